@@ -1,0 +1,266 @@
+/*
+ * phiray_cuda.h — the C ABI of phiray-b200: phiray's Rendered-mode hot path
+ * (LBVH build and refit, the 32-slot-stack path tracer, Skin, Denoise) as
+ * CUDA kernels for sm_100a behind plain C entry points.
+ *
+ * Every entry point replaces a piece of phiray's Rust API (gemphi/phiray);
+ * the citation beside each names the reference item it stands in for. A Rust
+ * FFI crate binds these one for one (`extern "C"` blocks, no bindgen), and
+ * wraps them in the same `Gpu`, `GpuArray`, `Pass`, `GpuBvh`, `Skin` and
+ * `Tracer` types, so callers such as phiber's `RaySkin` and
+ * `view3d/rendered.rs` keep their code.
+ *
+ * Conventions
+ *   - Every call returns int32 status: PHX_OK (0), a positive informational
+ *     code (PHX_REBUILD), or a negative PHX_ERR_*. The text of the last
+ *     error on the calling thread is available from phx_last_error.
+ *   - A context is one device and one CUDA stream; all work is stream-
+ *     ordered on it. A context is used by one host thread at a time
+ *     (phiray: `Gpu` is shared, `Tracer` is `&mut self`).
+ *   - Every host wait is bounded by a timeout in milliseconds and fails with
+ *     PHX_ERR_TIMEOUT instead of blocking forever (phiray `Gpu::wait_for`,
+ *     src/gpu/mod.rs:292-303). timeout_ms 0 means the default patience
+ *     (PHX_DEFAULT_WAIT_MS).
+ *   - Device pointers are passed as `void*` / typed pointers to device
+ *     memory; host pointers are documented as such.
+ *   - There is no CPU fallback: without a CUDA device every call that needs
+ *     one returns PHX_ERR_DEVICE.
+ */
+#ifndef PHIRAY_CUDA_H
+#define PHIRAY_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (phiray: Option/bool "declined", empty readback) ---- */
+#define PHX_OK 0
+#define PHX_REBUILD 1          /* GpuBvh::update returned false: rebuild instead */
+#define PHX_ERR_INVALID (-1)   /* bad argument (phiray panics on binding count)  */
+#define PHX_ERR_OOM (-2)
+#define PHX_ERR_TIMEOUT (-3)   /* phiray: empty readback, "device did not drain" */
+#define PHX_ERR_CANCELLED (-4) /* phiray: sample_in's `go` said no               */
+#define PHX_ERR_DEVICE (-5)    /* CUDA error, or no device                        */
+#define PHX_ERR_KERNEL (-6)    /* a kernel reported a status word (bounded wait)  */
+
+#define PHX_DEFAULT_WAIT_MS 5000u /* phiray WAIT_LIMIT, src/gpu/mod.rs:36 */
+
+/* ---- shared layouts (byte-identical to the reference's Pod types) ---- */
+
+/* bvh::Aabb, src/bvh/node.rs:60-66: 32 bytes, padded for WGSL. */
+typedef struct phx_aabb {
+    float lo[3];
+    float pad_a;
+    float hi[3];
+    float pad_b;
+} phx_aabb;
+
+/* bvh::Half, src/bvh/node.rs:12-16: a bound corner + index with leaf bit 31. */
+typedef struct phx_half {
+    float p[3];
+    uint32_t i;
+} phx_half;
+
+/* bvh::Node, src/bvh/node.rs:30-34. Inner: children lo.i, hi.i.
+ * Leaf: sorted slots [lo.i & ~LEAF, hi.i). */
+typedef struct phx_node {
+    phx_half lo;
+    phx_half hi;
+} phx_node;
+
+#define PHX_LEAF 0x80000000u /* bvh::LEAF, src/bvh/node.rs:7 */
+#define PHX_STACK 32u        /* bvh::STACK, src/bvh/node.rs:6 */
+
+/* bvh::Link, src/bvh/build.rs:8-14: Karras result for one internal node. */
+typedef struct phx_link {
+    uint32_t left, right, first, last;
+} phx_link;
+
+/* kernel::Pair, src/kernel/skin.rs:13-22. */
+typedef struct phx_pair {
+    uint32_t bone;
+    float weight;
+    uint32_t next;
+    float blend;
+} phx_pair;
+
+/* ---- context (phiray Gpu, src/gpu/mod.rs:84-99) ---- */
+typedef struct phx_ctx_s* phx_ctx;
+
+/* Gpu::new: open device `ordinal`, create its stream. */
+int32_t phx_ctx_create(int32_t ordinal, phx_ctx* out);
+int32_t phx_ctx_destroy(phx_ctx ctx);
+/* Gpu::wait_for (src/gpu/mod.rs:292-303): drain the stream, polling with a
+ * deadline; PHX_ERR_TIMEOUT when it does not drain in time. */
+int32_t phx_ctx_wait(phx_ctx ctx, uint32_t timeout_ms);
+/* The cudaStream_t work is enqueued on (as void*). */
+void* phx_ctx_stream(phx_ctx ctx);
+/* Enqueue on a caller's stream (e.g. one shared with another library);
+ * NULL returns to the context's own stream. */
+int32_t phx_ctx_set_stream(phx_ctx ctx, void* stream);
+/* Text of the calling thread's last error; returns its length. */
+int32_t phx_last_error(char* buf, size_t len);
+/* Library version string, for loaders. */
+const char* phx_version(void);
+/* Number of CUDA devices (0 when none), no context needed. */
+int32_t phx_device_count(void);
+
+/* ---- buffers (phiray GpuArray<T>, src/gpu/array.rs:20-187) ---- */
+typedef struct phx_buf_s* phx_buf;
+
+/* GpuArray::new / zeroed: `bytes` of device memory, zeroed. */
+int32_t phx_buf_alloc(phx_ctx ctx, uint64_t bytes, phx_buf* out);
+/* Borrow caller-owned device memory as a buffer (not freed by phx_buf_free). */
+int32_t phx_buf_wrap(phx_ctx ctx, void* device_ptr, uint64_t bytes, phx_buf* out);
+int32_t phx_buf_free(phx_buf buf);
+/* GpuArray::write_at (array.rs:99-107): host -> device, stream-ordered;
+ * returns when `src` may be reused. */
+int32_t phx_buf_write(phx_buf buf, uint64_t offset, const void* src, uint64_t bytes);
+/* GpuArray::write (array.rs:47-56): replace the contents with `bytes` from
+ * the host, reallocating when they do not fit; *reallocated = 1 then, which
+ * (as in phiray) means passes bound to the old buffer must be re-added. */
+int32_t phx_buf_assign(phx_buf buf, const void* src, uint64_t bytes, int32_t* reallocated);
+/* GpuArray::read_range (array.rs:148-187): device -> host, bounded wait. */
+int32_t phx_buf_read(phx_buf buf, uint64_t offset, void* dst, uint64_t bytes, uint32_t timeout_ms);
+uint64_t phx_buf_size(phx_buf buf);
+void* phx_buf_ptr(phx_buf buf);
+
+/* ---- kernels and recorded passes (phiray Kernel + Pass) ---- */
+
+/* Kernel ids stand in for Kernel::NAME/WGSL/key (src/kernel/mod.rs:51-105).
+ * Each kernel's params blob starts with {n, groups_x} as phiray's Param does;
+ * phx_pass_add fills those two words (Pass::add_over, src/gpu/pass.rs:70-101). */
+enum phx_kernel_id {
+    PHX_KERNEL_SKIN = 1,    /* kernel::Skin, src/kernel/skin.rs:34-66; params phx_skin_param; bufs rest, offsets, pairs, bones, out */
+    PHX_KERNEL_DENOISE = 2, /* kernel::Denoise, src/kernel/denoise.rs:53-64; params phx_denoise_param; bufs px */
+    PHX_KERNEL_MORTON = 3,  /* bvh::Morton, src/bvh/kernel.rs:21-51; params phx_morton_param; bufs prims, codes */
+    PHX_KERNEL_KARRAS = 4,  /* bvh::Karras, src/bvh/kernel.rs:65-117; params phx_karras_param; bufs codes, links */
+    PHX_KERNEL_REFIT = 5    /* bvh::Refit (one Jacobi step), src/bvh/kernel.rs:130-170; params phx_refit_param; bufs prims, order, src, dst */
+};
+
+/* kernel::SkinParam, src/kernel/skin.rs:24-32. */
+typedef struct phx_skin_param {
+    uint32_t n, groups_x;
+    float min;
+    uint32_t pad;
+} phx_skin_param;
+
+/* kernel::DenoiseParam, src/kernel/denoise.rs:24-51. */
+typedef struct phx_denoise_param {
+    uint32_t n, groups_x, w, h;
+    uint32_t step, round, last, keep;
+    float strength[4];
+    float view[4];
+} phx_denoise_param;
+
+/* bvh::MortonParam, src/bvh/kernel.rs:9-18. */
+typedef struct phx_morton_param {
+    uint32_t n, groups_x, pad0[2];
+    float lo[3];
+    float pad1;
+    float inv[3];
+    float pad2;
+} phx_morton_param;
+
+/* bvh::KarrasParam, src/bvh/kernel.rs:55-62. */
+typedef struct phx_karras_param {
+    uint32_t n, groups_x, leaves, pad;
+} phx_karras_param;
+
+/* bvh::RefitParam, src/bvh/kernel.rs:121-126. */
+typedef struct phx_refit_param {
+    uint32_t n, groups_x, pad[2];
+} phx_refit_param;
+
+typedef struct phx_pass_s* phx_pass;
+
+int32_t phx_pass_create(phx_ctx ctx, phx_pass* out);
+int32_t phx_pass_destroy(phx_pass pass);
+/* Pass::add_over (pass.rs:70-101): record kernel `id` over `items`
+ * invocations of a job of `n`; `params` (params_len bytes) is copied, its
+ * first two words set to {n, groups_x}. The buffer count must match the
+ * kernel's (phiray asserts; this returns PHX_ERR_INVALID). *step = index. */
+int32_t phx_pass_add(phx_pass pass, int32_t kernel_id, uint32_t n, uint32_t items, const void* params,
+                     uint32_t params_len, const phx_buf* bufs, uint32_t nbufs, uint32_t* step);
+/* Pass::set (pass.rs:104-106): overwrite `len` bytes of a step's params at
+ * `offset`, stream-ordered before the next run. */
+int32_t phx_pass_set(phx_pass pass, uint32_t step, uint32_t offset, const void* data, uint32_t len);
+/* Pass::run (pass.rs:109-113): replay every step, as one CUDA graph launch. */
+int32_t phx_pass_run(phx_pass pass);
+/* Pass::run_step (pass.rs:126-137). */
+int32_t phx_pass_run_step(phx_pass pass, uint32_t step);
+/* Pass::clear (pass.rs:139). */
+int32_t phx_pass_clear(phx_pass pass);
+/* Pass::len. */
+uint32_t phx_pass_len(phx_pass pass);
+/* Pass::compiled: distinct kernels this pass uses. */
+uint32_t phx_pass_compiled(phx_pass pass);
+
+/* ---- GpuBvh (src/bvh/gpu.rs:11-104) ---- */
+typedef struct phx_bvh_s* phx_bvh;
+
+/* GpuBvh::build (gpu.rs:23-74) from HOST prims: upload, then every stage on
+ * the device — bounds, Morton codes, stable radix sort, Karras links, leaf
+ * packing and depth, atomic bottom-up refit. No readback. n may be 0. */
+int32_t phx_bvh_build(phx_ctx ctx, const phx_aabb* host_prims, uint32_t n, uint32_t leaf, phx_bvh* out);
+/* The same from prims already in device memory (copied into the BVH). */
+int32_t phx_bvh_build_device(phx_ctx ctx, const phx_aabb* device_prims, uint32_t n, uint32_t leaf, phx_bvh* out);
+/* Rebuild an existing BVH in place over new prims (reuses its memory when
+ * the count fits). */
+int32_t phx_bvh_rebuild_device(phx_bvh bvh, const phx_aabb* device_prims, uint32_t n);
+/* GpuBvh::refit (gpu.rs:88-90): bounds again from the BVH's prims. */
+int32_t phx_bvh_refit(phx_bvh bvh);
+/* GpuBvh::update (gpu.rs:93-99): new HOST prims of the same count, then
+ * refit; PHX_REBUILD (no work done) when the count differs. */
+int32_t phx_bvh_update(phx_bvh bvh, const phx_aabb* host_prims, uint32_t n);
+/* The same with DEVICE prims. */
+int32_t phx_bvh_update_device(phx_bvh bvh, const phx_aabb* device_prims, uint32_t n);
+/* GpuBvh::download (gpu.rs:102-104): nodes (2n-1, host), order (n, host)
+ * and depth. Either array may be NULL. Bounded wait. */
+int32_t phx_bvh_download(phx_bvh bvh, phx_node* nodes, uint32_t* order, uint32_t* depth, uint32_t timeout_ms);
+/* Counts: prims, node slots (2n-1), leaf size, depth (waits for the build). */
+int32_t phx_bvh_info(phx_bvh bvh, uint32_t* n, uint32_t* nodes, uint32_t* leaf, uint32_t* depth);
+/* Device pointers of the BVH's arrays (GpuBvh's pub fields prims, order,
+ * nodes), plus the sorted Morton codes; any may be NULL. */
+int32_t phx_bvh_device(phx_bvh bvh, phx_aabb** prims, uint32_t** order, phx_node** nodes, uint32_t** codes);
+int32_t phx_bvh_destroy(phx_bvh bvh);
+
+/* Stage-by-stage entry points over device arrays (the reference's GPU build
+ * pieces, for tests and for callers that hold their own arrays). */
+/* bvh::Morton (kernel.rs:21-51) with Bvh::scene (build.rs:70-72) done on the
+ * device: codes[i] for prims[i]; scene box written to scene_out (device,
+ * may be NULL). */
+int32_t phx_morton(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t* codes, phx_aabb* scene_out);
+/* Bvh::sort_codes (build.rs:87-92) as a stable LSD radix sort: order[] and
+ * sorted[] (device) equal to sorting (code, index). */
+int32_t phx_sort_codes(phx_ctx ctx, const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted);
+/* bvh::Karras (kernel.rs:65-117): links[i] for i < n-1 from sorted codes. */
+int32_t phx_karras(phx_ctx ctx, const uint32_t* sorted, uint32_t n, phx_link* links);
+
+/* ---- Skin (src/kernel/skin.rs) ---- */
+/* kernel::Skin over device arrays: rest/out vec4 x n, offsets n+1, pairs,
+ * bones (column-major mat4 x nbones). Pairs naming a bone >= nbones are an
+ * error (PHX_ERR_KERNEL, from a status word the kernel sets). */
+int32_t phx_skin(phx_ctx ctx, const float* rest, const uint32_t* offsets, const phx_pair* pairs, const float* bones,
+                 uint32_t nbones, float* out, uint32_t n, float min);
+/* Face boxes for a refit: box f = Aabb::of_tri of vertices faces[f].xyz
+ * (phiray Pose::boxes, src/trace/pose.rs:45-51), from skinned positions. */
+int32_t phx_face_boxes(phx_ctx ctx, const float* verts, const uint32_t* faces, uint32_t nfaces, phx_aabb* boxes);
+
+/* ---- Denoise (src/kernel/denoise.rs, denoise.wgsl; Tracer::denoise_with,
+ * src/trace/read.rs:85-119) ---- */
+/* The four a-trous passes (steps 1, 2, 4, 8) over a px image of w*h pixels
+ * (34 w h + 1 words, phiray's Tracer::PX_LEN layout, device). `strength`
+ * and `view` as DenoiseParam; keep = Tracer::denoise_shown. Only the
+ * Standard view transform (view[0] == 0) is supported. */
+int32_t phx_denoise(phx_ctx ctx, uint32_t* px, uint32_t w, uint32_t h, const float strength[4], const float view[4],
+                    int32_t keep);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHIRAY_CUDA_H */

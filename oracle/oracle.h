@@ -1,0 +1,94 @@
+/*
+ * ORACLE — test infrastructure only. A CPU restatement, in C++, of
+ * gemphi/phiray's own CPU twins and WGSL for the Rendered-mode hot path.
+ * The reference is Rust + WGSL and cannot be built or run here (no Rust
+ * toolchain, no graphics stack), so this restatement is the checker the
+ * CUDA kernels are compared against, and the CPU baseline bench.py times.
+ * Nothing in the product links or calls it.
+ *
+ * Every function cites the reference file:line it follows. Pinned against
+ * the reference's own test vectors (see tests/test_oracle_*.py).
+ */
+#ifndef PHIRAY_ORACLE_H
+#define PHIRAY_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_aabb {
+    float lo[3];
+    float pad_a;
+    float hi[3];
+    float pad_b;
+} orc_aabb;
+
+typedef struct orc_half {
+    float p[3];
+    uint32_t i;
+} orc_half;
+
+typedef struct orc_node {
+    orc_half lo, hi;
+} orc_node;
+
+typedef struct orc_link {
+    uint32_t left, right, first, last;
+} orc_link;
+
+typedef struct orc_pair {
+    uint32_t bone;
+    float weight;
+    uint32_t next;
+    float blend;
+} orc_pair;
+
+int orc_threads(void);
+void orc_set_threads(int n);
+
+/* src/bvh/node.rs:96-105 morton(p, group) (64-bit, group in the high word). */
+uint64_t orc_morton(const float p[3], uint32_t group);
+/* src/bvh/build.rs:70-72 Bvh::scene. */
+void orc_scene(const orc_aabb* prims, uint32_t n, orc_aabb* out);
+/* src/bvh/build.rs:75-85 Bvh::codes. */
+void orc_codes(const orc_aabb* prims, uint32_t n, uint32_t* codes);
+/* src/bvh/build.rs:87-92 Bvh::sort_codes: order by (code, index). */
+void orc_sort_codes(const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted);
+/* src/bvh/sort.rs:127-150: the reference's sequential model of its GPU
+ * radix (8 LSD passes over the 64-bit key [index, code]). */
+void orc_radix_model(const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted);
+/* src/bvh/mod.rs:33-43 delta. */
+int32_t orc_delta(const uint32_t* codes, uint32_t n, int64_t i, int64_t j);
+/* src/bvh/build.rs:28-60 Link::of, for every internal node (n-1 links). */
+void orc_links(const uint32_t* sorted, uint32_t n, orc_link* links);
+/* src/bvh/build.rs:139-168 Bvh::assemble: nodes (2n-1), depth. */
+void orc_assemble(uint32_t n, const orc_link* links, uint32_t leaf, orc_node* nodes, uint32_t* depth);
+/* src/bvh/build.rs:180-194 Bvh::refit over `prims` through `order`. */
+void orc_refit(orc_node* nodes, uint32_t nnodes, const uint32_t* order, const orc_aabb* prims);
+/* src/bvh/build.rs:94-100 Bvh::build: nodes (2n-1), order (n), depth. */
+void orc_build(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order, uint32_t* depth);
+/* src/bvh/build.rs:104-136 Bvh::build_compact; returns the node count
+ * (nodes must hold 2n-1). */
+uint32_t orc_build_compact(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order,
+                           uint32_t* depth);
+/* src/bvh/shape.rs:8-37 Bvh::compact in place; returns the new count. */
+uint32_t orc_compact(orc_node* nodes, uint32_t nnodes);
+/* src/bvh/shape.rs:40-51 Bvh::reachable; returns the count written. */
+uint32_t orc_reachable(const orc_node* nodes, uint32_t nnodes, uint32_t* out);
+
+/* src/kernel/skin.rs:70-90 Skin::cpu. rest/out: vec4 x n; bones mat4 x k. */
+void orc_skin(const float* rest, const uint32_t* offsets, const orc_pair* pairs, const float* bones, float min,
+              uint32_t n, float* out);
+
+/* src/kernel/denoise.wgsl:47-134 + view.wgsl:62-99, run as
+ * Tracer::denoise_with (src/trace/read.rs:85-119) runs it: four passes,
+ * steps 1, 2, 4, 8, in place on a px buffer of 34 w h + 1 words. */
+void orc_denoise(uint32_t* px, uint32_t w, uint32_t h, const float strength[4], const float view[4], int keep);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

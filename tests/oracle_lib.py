@@ -1,0 +1,164 @@
+"""ctypes loader of the oracle (oracle/liboracle.so): the C++ restatement of
+phiray's CPU twins and WGSL that the CUDA kernels are checked against. Test
+infrastructure only; builds the library from oracle/Makefile if missing."""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent.parent / "oracle"
+LIB = ORACLE_DIR / "liboracle.so"
+
+vp, u32, i32, u64, f32 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64, C.c_float
+
+SIGS = {
+    "orc_threads": (C.c_int, []),
+    "orc_set_threads": (None, [C.c_int]),
+    "orc_morton": (u64, [vp, u32]),
+    "orc_scene": (None, [vp, u32, vp]),
+    "orc_codes": (None, [vp, u32, vp]),
+    "orc_sort_codes": (None, [vp, u32, vp, vp]),
+    "orc_radix_model": (None, [vp, u32, vp, vp]),
+    "orc_delta": (i32, [vp, u32, C.c_int64, C.c_int64]),
+    "orc_links": (None, [vp, u32, vp]),
+    "orc_assemble": (None, [u32, vp, u32, vp, C.POINTER(u32)]),
+    "orc_refit": (None, [vp, u32, vp, vp]),
+    "orc_build": (None, [vp, u32, u32, vp, vp, C.POINTER(u32)]),
+    "orc_build_compact": (u32, [vp, u32, u32, vp, vp, C.POINTER(u32)]),
+    "orc_compact": (u32, [vp, u32]),
+    "orc_reachable": (u32, [vp, u32, vp]),
+    "orc_skin": (None, [vp, vp, vp, vp, f32, u32, vp]),
+    "orc_denoise": (None, [vp, u32, u32, C.POINTER(f32), C.POINTER(f32), C.c_int]),
+}
+
+
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    deps = list(ORACLE_DIR.glob("*.cpp")) + list(ORACLE_DIR.glob("*.h"))
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+class Oracle:
+    def __init__(self, lib: C.CDLL):
+        self.lib = lib
+
+    # --- BVH (src/bvh/*.rs) ---
+    def morton(self, p, group=0) -> int:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        return self.lib.orc_morton(a.ctypes.data, group)
+
+    def scene(self, prims):
+        prims = np.ascontiguousarray(prims, dtype=np.float32)
+        out = np.zeros(8, dtype=np.float32)
+        self.lib.orc_scene(prims.ctypes.data, len(prims), out.ctypes.data)
+        return out
+
+    def codes(self, prims):
+        prims = np.ascontiguousarray(prims, dtype=np.float32)
+        out = np.zeros(len(prims), dtype=np.uint32)
+        self.lib.orc_codes(prims.ctypes.data, len(prims), out.ctypes.data)
+        return out
+
+    def sort_codes(self, codes):
+        codes = np.ascontiguousarray(codes, dtype=np.uint32)
+        order = np.zeros(len(codes), dtype=np.uint32)
+        sorted_ = np.zeros(len(codes), dtype=np.uint32)
+        self.lib.orc_sort_codes(codes.ctypes.data, len(codes), order.ctypes.data, sorted_.ctypes.data)
+        return order, sorted_
+
+    def radix_model(self, codes):
+        codes = np.ascontiguousarray(codes, dtype=np.uint32)
+        order = np.zeros(len(codes), dtype=np.uint32)
+        sorted_ = np.zeros(len(codes), dtype=np.uint32)
+        self.lib.orc_radix_model(codes.ctypes.data, len(codes), order.ctypes.data, sorted_.ctypes.data)
+        return order, sorted_
+
+    def links(self, sorted_codes):
+        s = np.ascontiguousarray(sorted_codes, dtype=np.uint32)
+        out = np.zeros((max(0, len(s) - 1), 4), dtype=np.uint32)
+        self.lib.orc_links(s.ctypes.data, len(s), out.ctypes.data)
+        return out
+
+    def build(self, prims, leaf=4):
+        prims = np.ascontiguousarray(prims, dtype=np.float32).reshape(-1, 8)
+        n = len(prims)
+        nodes = np.zeros((max(0, 2 * n - 1), 8), dtype=np.float32)
+        order = np.zeros(n, dtype=np.uint32)
+        depth = u32()
+        self.lib.orc_build(prims.ctypes.data, n, leaf, nodes.ctypes.data, order.ctypes.data, C.byref(depth))
+        return nodes, order, depth.value
+
+    def build_compact(self, prims, leaf=4):
+        prims = np.ascontiguousarray(prims, dtype=np.float32).reshape(-1, 8)
+        n = len(prims)
+        nodes = np.zeros((max(1, 2 * n - 1), 8), dtype=np.float32)
+        order = np.zeros(n, dtype=np.uint32)
+        depth = u32()
+        m = self.lib.orc_build_compact(prims.ctypes.data, n, leaf, nodes.ctypes.data, order.ctypes.data, C.byref(depth))
+        return nodes[:m].copy(), order, depth.value
+
+    def refit(self, nodes, order, prims):
+        nodes = np.ascontiguousarray(nodes, dtype=np.float32).copy()
+        order = np.ascontiguousarray(order, dtype=np.uint32)
+        prims = np.ascontiguousarray(prims, dtype=np.float32)
+        self.lib.orc_refit(nodes.ctypes.data, len(nodes), order.ctypes.data, prims.ctypes.data)
+        return nodes
+
+    def compact(self, nodes):
+        nodes = np.ascontiguousarray(nodes, dtype=np.float32).copy()
+        m = self.lib.orc_compact(nodes.ctypes.data, len(nodes))
+        return nodes[:m].copy()
+
+    def reachable(self, nodes):
+        nodes = np.ascontiguousarray(nodes, dtype=np.float32)
+        out = np.zeros(len(nodes), dtype=np.uint32)
+        m = self.lib.orc_reachable(nodes.ctypes.data, len(nodes), out.ctypes.data)
+        return out[:m].copy()
+
+    # --- Skin (src/kernel/skin.rs:70-90) ---
+    def skin(self, rest, offsets, pairs, bones, min_weight=1e-4):
+        rest = np.ascontiguousarray(rest, dtype=np.float32)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+        pairs = np.ascontiguousarray(pairs)
+        bones = np.ascontiguousarray(bones, dtype=np.float32)
+        out = np.zeros_like(rest)
+        self.lib.orc_skin(rest.ctypes.data, offsets.ctypes.data, pairs.ctypes.data, bones.ctypes.data,
+                          f32(min_weight), len(rest), out.ctypes.data)
+        return out
+
+    # --- Denoise (denoise.wgsl) ---
+    def denoise(self, px, w, h, strength=(64.0, 8.0, 40.0, 7.0), view=(0.0, 0.0, 1.0, 0.0), keep=False):
+        px = np.ascontiguousarray(px, dtype=np.uint32).copy()
+        s = (f32 * 4)(*strength)
+        v = (f32 * 4)(*view)
+        self.lib.orc_denoise(px.ctypes.data, w, h, s, v, 1 if keep else 0)
+        return px
+
+
+def build() -> Path:
+    if _stale():
+        subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    return LIB
+
+
+_cached = None
+
+
+def load() -> Oracle:
+    global _cached
+    if _cached is None:
+        build()
+        lib = C.CDLL(str(LIB))
+        for name, (res, args) in SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _cached = Oracle(lib)
+    return _cached
