@@ -457,7 +457,8 @@ __global__ void __launch_bounds__(256) k_pack(const uint4* __restrict__ links, c
 __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims, const uint32_t* __restrict__ order,
                                                const uint32_t* __restrict__ parent, float4* nodes,
                                                const uint32_t* __restrict__ starts,
-                                               const uint32_t* __restrict__ nstarts, uint32_t* counters) {
+                                               const uint32_t* __restrict__ nstarts, uint32_t* counters,
+                                               uint32_t* status) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= *nstarts) return;
     uint32_t i = starts[t];
@@ -476,7 +477,13 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims,
     }
     nodes[2 * (size_t)i] = make_float4(lx, ly, lz, a.w);
     nodes[2 * (size_t)i + 1] = make_float4(hx, hy, hz, b.w);
-    while (i != 0) {
+    // A Karras tree is at most 65 levels deep (delta grows strictly from
+    // -1 to 64 going down); a longer climb means a corrupt parent array.
+    for (int hops = 0; i != 0; hops++) {
+        if (hops > 80) {
+            atomicOr(status, STATUS_BAD_INDEX);
+            return;
+        }
         const uint32_t p = __ldg(parent + i);
         __threadfence();
         const uint32_t old = atomicAdd(counters + p, 1u);
@@ -639,7 +646,7 @@ int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf) {
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>(prims, (const uint32_t*)w.order.ptr,
                                                        (const uint32_t*)w.parent.ptr, (float4*)w.nodes.ptr,
                                                        (const uint32_t*)w.starts.ptr, w.nstarts(),
-                                                       (uint32_t*)w.counters.ptr);
+                                                       (uint32_t*)w.counters.ptr, c->status);
     return cuda_check(cudaGetLastError(), "bvh build");
 }
 
@@ -647,7 +654,7 @@ int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots) {
     if (n == 0) return PHX_OK;
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, c->stream>>>(
         (const float4*)w.prims.ptr, slots ? nullptr : (const uint32_t*)w.order.ptr, (const uint32_t*)w.parent.ptr,
-        (float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr, w.nstarts(), (uint32_t*)w.counters.ptr);
+        (float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr, w.nstarts(), (uint32_t*)w.counters.ptr, c->status);
     return cuda_check(cudaGetLastError(), "bvh refit");
 }
 
