@@ -259,6 +259,149 @@ int32_t phx_face_boxes(phx_ctx ctx, const float* verts, const uint32_t* faces, u
 int32_t phx_denoise(phx_ctx ctx, uint32_t* px, uint32_t w, uint32_t h, const float strength[4], const float view[4],
                     int32_t keep);
 
+
+/* ---- Tracer (src/trace/mod.rs, build.rs, sample.rs, read.rs) ---- */
+
+/* camera.wgsl `Light` (src/trace/light.rs:15-43): 80 bytes. kind 0 sun,
+ * 1 point, 2 spot, 3 area. */
+typedef struct phx_light {
+    float pos[3];
+    uint32_t kind;
+    float color[3];
+    float size;
+    float dir[3];
+    float cone;
+    float right[3];
+    float size_y;
+    uint32_t shape;
+    float blend;
+    float spot_scale[2];
+} phx_light;
+
+#define PHX_MAX_LIGHT 64
+
+/* trace::Camera (src/trace/camera.rs:12-230, camera.wgsl:3-54), byte for
+ * byte (5,776 bytes), so a Rust caller passes its `Camera` as is. The
+ * Rendered path reads the view, lights, env, view transform, bounces,
+ * limit and frame words; settings this build does not implement are
+ * refused with PHX_ERR_INVALID (see phx_tracer_sample). */
+typedef struct phx_camera {
+    uint32_t n, groups_x, w, h;
+    float right[3];
+    uint32_t persp;
+    float up[3];
+    float scale;
+    float back[3];
+    float units;
+    float pivot[3];
+    float aspect;
+    float sun[3];
+    float dist;
+    float sky[4];
+    float pan[2];
+    float ao, eps;
+    uint32_t frame;
+    float grid;
+    uint32_t count, glow;
+    float grid_color[4];
+    float env[4];
+    uint32_t split[4];
+    float view[4];
+    uint32_t envmap;
+    float env_rot;
+    uint32_t bounces, env_cdf;
+    float aperture, focus;
+    uint32_t blades;
+    float blade_spin;
+    float aperture_ratio;
+    uint32_t env_hidden;
+    float see_through;
+    uint32_t grid_hide;
+    uint32_t tile[4], film[4], preview[4], slice[4], insts[4], vis[4];
+    float taa[4], fx[4], outline[4];
+    uint32_t shade[4];
+    float single[4], cavity[4];
+    uint32_t ssao[4];
+    float shadow[4], shadow_fade[4];
+    uint32_t matcap[4];
+    float dof[4], outline_fx[4], outline_pick[4], outline_active[4], outline_move[4];
+    float adapt[4], limit[4];
+    uint32_t depth[4];
+    float integrator[4];
+    phx_light lights[PHX_MAX_LIGHT];
+} phx_camera;
+
+/* A scene as indexed HOST arrays (what trace::Scene packs, scene.rs:41-64):
+ * verts (nverts x 4 f32, xyz + 1), optional vertex normals (nverts x 4 f32,
+ * zero = flat face; may be NULL), faces (nfaces x 4 u32: v0, v1, v2,
+ * material), mats (nmats x 16 f32: color rgba, rough, metal, trans, ior,
+ * emit rgb, then zeros — trace::Mat's Rendered-path inputs). */
+typedef struct phx_scene {
+    const float* verts;
+    const float* normals;
+    const uint32_t* faces;
+    const float* mats;
+    uint32_t nverts, nfaces, nmats;
+    uint32_t leaf; /* LBVH leaf size (the tracer's 4, forest.rs:20) */
+} phx_scene;
+
+typedef struct phx_tracer_s* phx_tracer;
+
+/* PX_LEN (src/trace/read.rs:56): words per pixel of the image buffer. */
+#define PHX_PX_LEN 34u
+
+/* Tracer::new (src/trace/build.rs:11-24): upload the scene, build its LBVH
+ * on the device (the reference walks CPU-built SAH trees; here the GPU LBVH
+ * is the tracer's tree), gather triangles into leaf order, build the
+ * emitter table. */
+int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* scene, phx_tracer* out);
+int32_t phx_tracer_destroy(phx_tracer tr);
+/* Tracer::set_samples: the sample target `sample` stops at. */
+int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
+/* Tracer::sample / sample_in (src/trace/sample.rs:94-249): one more sample
+ * of `cam` at w x h — frame 0 on a new view, frame + 1 on the same one —
+ * in `slices` dispatches, polling `*cancel` (host memory, may be NULL)
+ * between them (PHX_ERR_CANCELLED: the sample is abandoned and the next
+ * starts over). *frame = the frame traced, *done = 1 once the target is
+ * reached (no work is done then). */
+int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t slices,
+                          const volatile int32_t* cancel, uint32_t* frame, int32_t* done);
+/* Tracer::render's loop as one launch: frames [first, first + spp) of `cam`
+ * into the image, each pixel's samples taken in order inside the kernel —
+ * the same sums as spp calls of sample. Stream-ordered, no wait. */
+int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first, uint32_t spp);
+/* Tracer::pixels / radiance / ... (read.rs:241-327): `count` words of the
+ * image buffer from word `offset` (plane p starts at p * w * h) into host
+ * memory; bounded wait. */
+int32_t phx_tracer_read(phx_tracer tr, uint64_t offset, uint32_t* dst, uint64_t count, uint32_t timeout_ms);
+/* Device pointer and size (words) of the image buffer. */
+int32_t phx_tracer_image(phx_tracer tr, uint32_t** px, uint64_t* words);
+/* Tracer::denoise / denoise_shown (read.rs:73-119) over the image. */
+int32_t phx_tracer_denoise(phx_tracer tr, int32_t keep);
+/* Tracer::time (sample.rs:253-255): GPU ms of the last sample/trace call,
+ * and the rays it traced (closest-hit and shadow). Waits for it. */
+int32_t phx_tracer_time(phx_tracer tr, float* gpu_ms, uint64_t* rays);
+/* Tracer::repose on the device (pose.rs:77-100, with the GPU frame path of
+ * jobs.md:22): new vertex positions (DEVICE, nverts x 4 f32), face boxes,
+ * then an LBVH refit (rebuild = 0) or rebuild (rebuild = 1). */
+int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebuild);
+/* The primary ray of frame `frame` per pixel (shade.wgsl:66-95, first
+ * trace): hit face id (0xFFFFFFFF for none) and t, into DEVICE arrays of
+ * w*h. For hit-id parity checks. */
+int32_t phx_tracer_primary(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame,
+                           uint32_t* ids, float* ts);
+/* Closest-hit (any_hit 0) or any-hit (1) walk of `n` rays from DEVICE
+ * arrays: rays[2i] = (origin.xyz, tmax), rays[2i+1] = (dir.xyz, 0);
+ * hits[i] = (t, face id bits, u, v) with face 0xFFFFFFFF for a miss. */
+int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit);
+/* The incoherent secondary rays of a frame: for each pixel's primary hit, one
+ * cosine-sampled diffuse ray (integrate.wgsl:6-11 cosine_dir) from the
+ * lifted hit point, drawn from that pixel's sample stream; written to a
+ * DEVICE ray buffer (format of phx_trace_rays, w*h rays; a pixel whose
+ * primary ray missed gets a ray with tmax 0). */
+int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame,
+                                  float* rays);
+
 #ifdef __cplusplus
 }
 #endif

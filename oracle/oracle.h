@@ -87,6 +87,23 @@ void orc_skin(const float* rest, const uint32_t* offsets, const orc_pair* pairs,
  * steps 1, 2, 4, 8, in place on a px buffer of 34 w h + 1 words. */
 void orc_denoise(uint32_t* px, uint32_t w, uint32_t h, const float strength[4], const float view[4], int keep);
 
+/* The Rendered-mode tracer (shade.wgsl main and what it calls) over one
+ * identity-instance scene: verts (x, y, z, 1) x V, faces (v0, v1, v2, mat)
+ * x F, mats 32 words (trace::Mat) each, optional vertex normals, LBVH leaf
+ * size. Frames [first, first + spp) of `cam` (a phx_camera, the reference's
+ * Camera) accumulated into px (34 w h + 1 words, in/out), rows
+ * [row0, row0 + rows) (rows 0 = all). *rays_out = rays traced. */
+struct phx_camera;
+void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
+               uint32_t leaf, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+               uint64_t* rays_out, uint32_t row0, uint32_t rows);
+/* Primary ray of frame `frame` per pixel: face id (0xFFFFFFFF none), t. */
+void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
+                 const struct phx_camera* cam, uint32_t frame, uint32_t* ids, float* ts);
+/* Closest / any hit of rays (o.xyz, tmax, d.xyz, 0): hits (t, face id, u, v). */
+void orc_trace_rays(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
+                    const float* rays, uint32_t n, float* hits, int any_hit);
+
 #ifdef __cplusplus
 }
 #endif

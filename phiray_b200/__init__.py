@@ -12,9 +12,13 @@ from ._native import PhxError, lib
 from .bvh import Bvh, GpuBvh, aabbs, of_tri
 from .gpu import Denoise, Gpu, GpuArray, Karras, Kernel, Morton, Pass, Refit, Skin, devptr
 from .kernels import denoise, face_boxes, skin
+from .tracer import CAMERA, Tracer, camera
 
 __all__ = [
     "Bvh",
+    "CAMERA",
+    "Tracer",
+    "camera",
     "Denoise",
     "Gpu",
     "GpuArray",

@@ -96,6 +96,19 @@ SIGNATURES: dict[str, tuple] = {
     "phx_skin": (i32, [vp, vp, vp, vp, vp, u32, vp, u32, C.c_float]),
     "phx_face_boxes": (i32, [vp, vp, vp, u32, vp]),
     "phx_denoise": (i32, [vp, vp, u32, u32, f32p, f32p, i32]),
+    "phx_tracer_create": (i32, [vp, vp, C.POINTER(vp)]),
+    "phx_tracer_destroy": (i32, [vp]),
+    "phx_tracer_set_samples": (i32, [vp, u32]),
+    "phx_tracer_sample": (i32, [vp, vp, u32, u32, u32, vp, C.POINTER(u32), C.POINTER(i32)]),
+    "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),
+    "phx_tracer_read": (i32, [vp, u64, vp, u64, u32]),
+    "phx_tracer_image": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
+    "phx_tracer_denoise": (i32, [vp, i32]),
+    "phx_tracer_time": (i32, [vp, C.POINTER(C.c_float), C.POINTER(u64)]),
+    "phx_tracer_repose_device": (i32, [vp, vp, i32]),
+    "phx_tracer_primary": (i32, [vp, vp, u32, u32, u32, vp, vp]),
+    "phx_tracer_secondary_rays": (i32, [vp, vp, u32, u32, u32, vp]),
+    "phx_trace_rays": (i32, [vp, vp, u32, vp, i32]),
 }
 
 _lib = None

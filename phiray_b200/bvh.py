@@ -75,6 +75,7 @@ class GpuBvh:
 
     def __init__(self, gpu: Gpu, handle: C.c_void_p, leaf: int):
         self.gpu, self.handle, self.leaf = gpu, handle, leaf
+        gpu.adopt(self)
 
     @classmethod
     def build(cls, gpu: Gpu, prims: np.ndarray, leaf: int = 4) -> "GpuBvh":

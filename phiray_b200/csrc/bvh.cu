@@ -28,7 +28,7 @@
 // the CPU builder exactly.
 #include <cfloat>
 
-#include "internal.cuh"
+#include "lbvh.cuh"
 
 namespace phx {
 namespace {
@@ -42,6 +42,7 @@ constexpr int RADIX_ITEMS = 16;
 constexpr int TILE = RADIX_THREADS * RADIX_ITEMS;
 constexpr int WARPS = RADIX_THREADS / 32;
 constexpr int PASSES = 4;
+static_assert(TILE == LBVH_TILE && PASSES == LBVH_PASSES, "lbvh.cuh and bvh.cu agree");
 constexpr uint32_t FLAG_AGG = 1u << 30;
 constexpr uint32_t FLAG_INC = 2u << 30;
 constexpr uint32_t VALUE_MASK = (1u << 30) - 1;
@@ -557,47 +558,29 @@ uint32_t grid_for(uint64_t items, uint32_t block, uint32_t cap) {
 
 }  // namespace
 
-// ---- the build, shared by GpuBvh and the stage entry points ----
-
-struct BvhWork {
-    uint32_t cap = 0;  // prims the arrays hold
-    DevMem prims, codes, sorted, order, alt_keys, alt_vals, partial, zeroed, links, parent, nodes, starts, counters,
-        scalars, scene;
-    uint32_t tiles = 0, nparts = 0;
-
-    int32_t reserve(uint32_t n, int sms) {
-        if (n <= cap && prims.ptr) return PHX_OK;
-        const size_t m = n ? n : 1;
-        tiles = (uint32_t)((m + TILE - 1) / TILE);
-        nparts = grid_for(m, 256, (uint32_t)sms * 4);
-        PHX_TRY(prims.reserve(m * sizeof(phx_aabb)));
-        PHX_TRY(codes.reserve(m * 4));
-        PHX_TRY(sorted.reserve(m * 4));
-        PHX_TRY(order.reserve(m * 4));
-        PHX_TRY(alt_keys.reserve(m * 4));
-        PHX_TRY(alt_vals.reserve(m * 4));
-        PHX_TRY(partial.reserve((size_t)nparts * 32));
-        PHX_TRY(zeroed.reserve(zeroed_bytes()));
-        PHX_TRY(links.reserve(m * sizeof(phx_link)));
-        PHX_TRY(parent.reserve((2 * m) * 4));
-        PHX_TRY(nodes.reserve((2 * m) * sizeof(phx_node)));
-        PHX_TRY(starts.reserve(m * 4));
-        PHX_TRY(counters.reserve(m * 4));
-        PHX_TRY(scalars.reserve(64));
-        PHX_TRY(scene.reserve(sizeof(phx_aabb)));
-        cap = (uint32_t)m;
-        return PHX_OK;
-    }
-    // [hist 4*256][tickets 4][pad to 16][look-back 4 * tiles * 256]
-    size_t zeroed_bytes() const { return (size_t)(PASSES * 256 + 16) * 4 + (size_t)PASSES * tiles * 256 * 4; }
-    uint32_t* hist() const { return (uint32_t*)zeroed.ptr; }
-    uint32_t* tickets() const { return (uint32_t*)zeroed.ptr + PASSES * 256; }
-    uint32_t* lookback(int pass) const {
-        return (uint32_t*)zeroed.ptr + PASSES * 256 + 16 + (size_t)pass * tiles * 256;
-    }
-    uint32_t* depth() const { return (uint32_t*)scalars.ptr; }
-    uint32_t* nstarts() const { return (uint32_t*)scalars.ptr + 1; }
-};
+int32_t BvhWork::reserve(uint32_t n, int sms) {
+    if (n <= cap && prims.ptr) return PHX_OK;
+    const size_t m = n ? n : 1;
+    tiles = (uint32_t)((m + TILE - 1) / TILE);
+    nparts = grid_for(m, 256, (uint32_t)sms * 4);
+    PHX_TRY(prims.reserve(m * sizeof(phx_aabb)));
+    PHX_TRY(codes.reserve(m * 4));
+    PHX_TRY(sorted.reserve(m * 4));
+    PHX_TRY(order.reserve(m * 4));
+    PHX_TRY(alt_keys.reserve(m * 4));
+    PHX_TRY(alt_vals.reserve(m * 4));
+    PHX_TRY(partial.reserve((size_t)nparts * 32));
+    PHX_TRY(zeroed.reserve(zeroed_bytes()));
+    PHX_TRY(links.reserve(m * sizeof(phx_link)));
+    PHX_TRY(parent.reserve((2 * m) * 4));
+    PHX_TRY(nodes.reserve((2 * m) * sizeof(phx_node)));
+    PHX_TRY(starts.reserve(m * 4));
+    PHX_TRY(counters.reserve(m * 4));
+    PHX_TRY(scalars.reserve(64));
+    PHX_TRY(scene.reserve(sizeof(phx_aabb)));
+    cap = (uint32_t)m;
+    return PHX_OK;
+}
 
 // Stable LSD sort of `codes` (n keys): sorted codes and order into `w`.
 static int32_t enqueue_sort(Ctx* c, BvhWork& w, const uint32_t* codes, uint32_t n, bool hist_ready) {
@@ -710,6 +693,7 @@ static int32_t bvh_new(phx_ctx ctx, uint32_t n, uint32_t leaf, phx_bvh* out) {
         delete b;
         return rc;
     }
+    ctx->c.live++;
     *out = b;
     return PHX_OK;
 }
@@ -728,7 +712,7 @@ int32_t phx_bvh_build(phx_ctx ctx, const phx_aabb* host_prims, uint32_t n, uint3
     // The host array is the caller's again on return.
     if (rc == PHX_OK) rc = wait_stream(b->ctx->stream, 0);
     if (rc != PHX_OK) {
-        delete b;
+        phx_bvh_destroy(b);
         return rc;
     }
     *out = b;
@@ -745,7 +729,7 @@ int32_t phx_bvh_build_device(phx_ctx ctx, const phx_aabb* device_prims, uint32_t
                            "copy prims");
     if (rc == PHX_OK) rc = enqueue_build(b->ctx, b->w, n, leaf);
     if (rc != PHX_OK) {
-        delete b;
+        phx_bvh_destroy(b);
         return rc;
     }
     *out = b;
@@ -839,6 +823,7 @@ int32_t phx_bvh_destroy(phx_bvh bvh) {
     if (!bvh) return PHX_OK;
     use(bvh->ctx);
     cudaStreamSynchronize(bvh->ctx->stream);
+    bvh->ctx->live--;
     delete bvh;
     return PHX_OK;
 }

@@ -38,6 +38,7 @@ struct Ctx {
     cudaStream_t capture = nullptr; // private stream for graph capture
     uint32_t* status = nullptr;     // device status word
     DevMem denoise_scratch;         // guide and ping-pong planes of phx_denoise
+    int live = 0;                   // buffers, passes, BVHs, tracers not yet freed
 };
 
 // Sets the thread's last error text and returns `code`.
@@ -60,6 +61,9 @@ int32_t launch_denoise_step(cudaStream_t s, const void* params, void* const* buf
 int32_t launch_morton_step(cudaStream_t s, const void* params, void* const* bufs, uint32_t items);
 int32_t launch_karras_step(cudaStream_t s, const void* params, void* const* bufs, uint32_t items);
 int32_t launch_refit_step(cudaStream_t s, const void* params, void* const* bufs, uint32_t items);
+
+// Face boxes (Aabb::of_tri) of vec4 vertices over uvec4 faces (skin.cu).
+int32_t launch_face_boxes(cudaStream_t s, const float* verts, const uint32_t* faces, uint32_t nfaces, phx_aabb* boxes);
 
 inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 

@@ -1,0 +1,36 @@
+// The LBVH build's device arrays and the enqueue functions that run it
+// (bvh.cu), shared with the tracer, which builds its tree over face boxes.
+#pragma once
+
+#include "internal.cuh"
+
+namespace phx {
+
+constexpr int LBVH_TILE = 4096;  // radix-sort tile (256 threads x 16 keys)
+constexpr int LBVH_PASSES = 4;   // 8-bit digits over the 30-bit Morton code
+
+struct BvhWork {
+    uint32_t cap = 0;  // prims the arrays hold
+    DevMem prims, codes, sorted, order, alt_keys, alt_vals, partial, zeroed, links, parent, nodes, starts, counters,
+        scalars, scene;
+    uint32_t tiles = 0, nparts = 0;
+
+    int32_t reserve(uint32_t n, int sms);
+    // [hist 4*256][tickets 4][pad to 16][look-back 4 * tiles * 256]
+    size_t zeroed_bytes() const { return (size_t)(LBVH_PASSES * 256 + 16) * 4 + (size_t)LBVH_PASSES * tiles * 256 * 4; }
+    uint32_t* hist() const { return (uint32_t*)zeroed.ptr; }
+    uint32_t* tickets() const { return (uint32_t*)zeroed.ptr + LBVH_PASSES * 256; }
+    uint32_t* lookback(int pass) const {
+        return (uint32_t*)zeroed.ptr + LBVH_PASSES * 256 + 16 + (size_t)pass * tiles * 256;
+    }
+    uint32_t* depth() const { return (uint32_t*)scalars.ptr; }
+    uint32_t* nstarts() const { return (uint32_t*)scalars.ptr + 1; }
+};
+
+// Every stage of Bvh::build over w.prims[0..n) on the context's stream.
+int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf);
+// Bvh::refit (slots = false: prims through order; true: prims already in
+// slot order, Bvh::refit_slots).
+int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots);
+
+}  // namespace phx

@@ -149,6 +149,9 @@ int32_t phx_ctx_create(int32_t ordinal, phx_ctx* out) {
 int32_t phx_ctx_destroy(phx_ctx ctx) {
     if (!ctx) return PHX_OK;
     Ctx& c = ctx->c;
+    // Everything made on a context holds a pointer to it: refuse to free it
+    // under them (the caller frees buffers, passes, BVHs, tracers first).
+    if (c.live > 0) return fail(PHX_ERR_INVALID, "context still has %d live objects", c.live);
     cudaSetDevice(c.device);
     if (c.own) cudaStreamSynchronize(c.own);
     if (c.status) cudaFree(c.status);
@@ -190,6 +193,7 @@ int32_t phx_buf_alloc(phx_ctx ctx, uint64_t bytes, phx_buf* out) {
     b->ptr = p;
     b->bytes = bytes;
     b->owned = true;
+    ctx->c.live++;
     *out = b;
     return PHX_OK;
 }
@@ -201,6 +205,7 @@ int32_t phx_buf_wrap(phx_ctx ctx, void* device_ptr, uint64_t bytes, phx_buf* out
     b->ptr = device_ptr;
     b->bytes = bytes;
     b->owned = false;
+    ctx->c.live++;
     *out = b;
     return PHX_OK;
 }
@@ -212,6 +217,7 @@ int32_t phx_buf_free(phx_buf buf) {
         cudaStreamSynchronize(buf->ctx->stream);
         cudaFree(buf->ptr);
     }
+    buf->ctx->live--;
     delete buf;
     return PHX_OK;
 }
@@ -328,6 +334,7 @@ int32_t phx_pass_create(phx_ctx ctx, phx_pass* out) {
     if (!ctx || !out) return fail(PHX_ERR_INVALID, "null argument");
     auto* p = new phx_pass_s();
     p->ctx = &ctx->c;
+    ctx->c.live++;
     *out = p;
     return PHX_OK;
 }
@@ -335,6 +342,7 @@ int32_t phx_pass_create(phx_ctx ctx, phx_pass* out) {
 int32_t phx_pass_destroy(phx_pass pass) {
     if (!pass) return PHX_OK;
     if (pass->exec) cudaGraphExecDestroy(pass->exec);
+    pass->ctx->live--;
     delete pass;
     return PHX_OK;
 }

@@ -1,0 +1,675 @@
+// The Rendered path's device code: the LBVH walk and the bounce loop.
+//
+// Reference: src/trace/wgsl/bvh.wgsl (box_t, ray_space, tri_t, safe_inv,
+// trace_blas/trace), shade.wgsl main (:41-373), integrate.wgsl (direct,
+// indirect, glow_mis, bounce_light, cosine_dir), light.wgsl (onb, cone_dir,
+// env_at, visible, lamp_query, area_query, spot_mask, lamp_reach,
+// lamp_chance, glow_query, hit_lift, through_lift), brdf.wgsl (GGX, Surf,
+// fresnel_of, dielectric_f0, under_layer(_real), env_brdf, brdf_w,
+// ggx_pdf, glossy_floor), util.wgsl (hash, rnd, unit_disk), view.wgsl.
+//
+// The scene is one identity instance (the configs place every mesh in world
+// space), so the reference's top-tree walk plus one trace_blas is a single
+// walk of the mesh tree here, in the same order: root box, near child
+// first, strict `t < best`. Features the configs do not use (textures,
+// procedural slots, environment images, depth of field, adaptive sampling,
+// the grid overlay, film transparency) are refused on the host.
+//
+// Layout the walk reads (built from the LBVH after every build/refit):
+//   nodes  4 float4 per inner node: both children's boxes, then their refs
+//          (inner node index, or first slot | LEAF)
+//   tris   3 float4 per sorted slot: a.xyz + face id, b.xyz + material id,
+//          c.xyz + flags (bit 0: last slot of its leaf; bit 1: a shadow
+//          ray passes it — glass or cut-out, bvh.wgsl:158-162)
+// so one step is one 64-byte node read and one triangle one 48-byte read.
+#pragma once
+
+#include "internal.cuh"
+#include "vec.cuh"
+
+namespace phx {
+namespace shade {
+
+constexpr uint32_t LEAF = 0x80000000u;
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr float INF = 3.0e38f;
+constexpr float PI = 3.14159265f;
+constexpr uint32_t FLAG_END = 1u;
+constexpr uint32_t FLAG_PASS = 2u;
+constexpr int STACK = 32;
+
+struct Scene {
+    const float4* __restrict__ nodes;
+    const float4* __restrict__ tris;
+    const float4* __restrict__ tnorm;  // 3 per slot, or null: flat faces
+    const float4* __restrict__ mats;   // 8 float4 (32 words, trace::Mat) per material
+    const uint32_t* __restrict__ lamp_slot;
+    const float* __restrict__ lamp_cdf;
+    const float4* __restrict__ info;   // root box + ref, extent, emitter count (device results of the build)
+    uint32_t lamp_count;
+    uint32_t root;  // inner node 0, or LEAF | 0 when the root is a leaf
+    f3 root_lo, root_hi;
+    float extent;
+};
+
+// Fills the build-dependent fields from the device info record, and the
+// frame's ray offsets from the extent (Tracer::sample_in, sample.rs:114-118:
+// ao = 8% of the extent when the camera leaves it 0, eps = 1e-5 of it).
+__device__ __forceinline__ void load_info(Scene& S) {
+    const float4 a = __ldg(S.info), b = __ldg(S.info + 1), c = __ldg(S.info + 2);
+    S.root_lo = mk(a.x, a.y, a.z);
+    S.root = __float_as_uint(a.w);
+    S.root_hi = mk(b.x, b.y, b.z);
+    S.extent = b.w;
+    S.lamp_count = __float_as_uint(c.x);
+}
+
+struct Hit {
+    float t;
+    uint32_t tri;  // sorted slot, NONE for a miss
+    float u, v;
+};
+
+struct Frame {
+    uint32_t w, h, n, frame0, spp, persp, count, bounces;
+    f3 right, up, back, pivot, env;
+    float scale, units, aspect, dist, pan_x, pan_y, ao, eps;  // ao: the camera's (0 = auto); eps set in-kernel
+    float sky[4];
+    float limit_d, limit_i, exposure, gamma;
+    const phx_light* __restrict__ lights;
+};
+
+// ---- util.wgsl ----
+
+__device__ __forceinline__ uint32_t hash(uint32_t x) {
+    uint32_t h = x * 747796405u + 2891336453u;
+    h = ((h >> ((h >> 28u) + 4u)) ^ h) * 277803737u;
+    return (h >> 22u) ^ h;
+}
+
+__device__ __forceinline__ float rnd(uint32_t& seed) {
+    seed = hash(seed);
+    return (float)seed / 4294967295.0f;
+}
+
+__device__ __forceinline__ float2 unit_disk(float ru, float rv) {
+    const float a = 2.0f * ru - 1.0f;
+    const float b = 2.0f * rv - 1.0f;
+    if (a == 0.0f && b == 0.0f) return make_float2(0.0f, 0.0f);
+    float r, phi;
+    if (a * a > b * b) {
+        r = a;
+        phi = (PI / 4.0f) * (b / a);
+    } else {
+        r = b;
+        phi = (PI / 2.0f) - (PI / 4.0f) * (a / b);
+    }
+    float s, c;
+    pm_sincos(phi, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+// ---- bvh.wgsl ----
+
+__device__ __forceinline__ float box_t(f3 lo, f3 hi, f3 o, f3 inv, float best) {
+    const f3 t1 = (lo - o) * inv;
+    const f3 t2 = (hi - o) * inv;
+    const float tmin = fmaxf(fmaxf(fminf(t1.x, t2.x), fminf(t1.y, t2.y)), fminf(t1.z, t2.z));
+    const float tmax = fminf(fminf(fmaxf(t1.x, t2.x), fmaxf(t1.y, t2.y)), fmaxf(t1.z, t2.z));
+    if (tmax >= fmaxf(tmin, 0.0f) && tmin < best) return fmaxf(tmin, 0.0f);
+    return INF;
+}
+
+struct RaySpace {
+    uint32_t kz;
+    bool flip;
+    f3 s;
+};
+
+__device__ __forceinline__ f3 ray_axes(f3 v, uint32_t kz, bool flip) {
+    const f3 p = kz == 2u ? v : (kz == 0u ? mk(v.y, v.z, v.x) : mk(v.z, v.x, v.y));
+    return flip ? mk(p.y, p.x, p.z) : p;
+}
+
+__device__ __forceinline__ RaySpace ray_space(f3 d) {
+    const f3 a = mk(fabsf(d.x), fabsf(d.y), fabsf(d.z));
+    const uint32_t kz = (a.x >= a.y && a.x >= a.z) ? 0u : (a.y >= a.z ? 1u : 2u);
+    const bool flip = ray_axes(d, kz, false).z < 0.0f;
+    const f3 dr = ray_axes(d, kz, flip);
+    const float sz = 1.0f / dr.z;
+    return RaySpace{kz, flip, mk(dr.x * sz, dr.y * sz, sz)};
+}
+
+// Watertight test (Woop et al. 2013): t, or INF for a miss; u, v the
+// weights of tb and tc.
+__device__ __forceinline__ float tri_t(f3 ta, f3 tb, f3 tc, f3 o, const RaySpace& r, float& u, float& v) {
+    const f3 a = ray_axes(ta - o, r.kz, r.flip);
+    const f3 b = ray_axes(tb - o, r.kz, r.flip);
+    const f3 c = ray_axes(tc - o, r.kz, r.flip);
+    const float ax = a.x - r.s.x * a.z;
+    const float ay = a.y - r.s.y * a.z;
+    const float bx = b.x - r.s.x * b.z;
+    const float by = b.y - r.s.y * b.z;
+    const float cx = c.x - r.s.x * c.z;
+    const float cy = c.y - r.s.y * c.z;
+    const float ea = cx * by - cy * bx;
+    const float eb = ax * cy - ay * cx;
+    const float ec = bx * ay - by * ax;
+    if ((ea < 0.0f || eb < 0.0f || ec < 0.0f) && (ea > 0.0f || eb > 0.0f || ec > 0.0f)) return INF;
+    const float det = ea + eb + ec;
+    if (det == 0.0f) return INF;
+    const float tt = ea * (r.s.z * a.z) + eb * (r.s.z * b.z) + ec * (r.s.z * c.z);
+    const float sg = det < 0.0f ? -1.0f : 1.0f;
+    if (tt * sg <= 0.0f) return INF;
+    const float inv = 1.0f / det;
+    u = eb * inv;
+    v = ec * inv;
+    return tt * inv;
+}
+
+__device__ __forceinline__ f3 safe_inv(f3 d) {
+    const float sx = d.x < 0.0f ? -1.0f : 1.0f, sy = d.y < 0.0f ? -1.0f : 1.0f, sz = d.z < 0.0f ? -1.0f : 1.0f;
+    return mk(1.0f / (fabsf(d.x) < 1e-9f ? sx * 1e-9f : d.x), 1.0f / (fabsf(d.y) < 1e-9f ? sy * 1e-9f : d.y),
+              1.0f / (fabsf(d.z) < 1e-9f ? sz * 1e-9f : d.z));
+}
+
+__device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
+
+// trace (bvh.wgsl:120-232) over the single-instance tree. `first`: any hit
+// (a shadow ray), which passes glass and cut-outs and stops at the first
+// opaque hit. The stack holds 32 refs; the builder caps the depth at 31.
+__device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first) {
+    Hit best{tmax, NONE, 0.0f, 0.0f};
+    const f3 inv = safe_inv(d);
+    if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return best;
+    const RaySpace rs = ray_space(d);
+    uint32_t stack[STACK];
+    int sp = 0;
+    uint32_t nd = S.root;
+    for (;;) {
+        if (nd & LEAF) {
+            for (uint32_t id = nd & ~LEAF;; id++) {
+                const float4 A = __ldg(S.tris + 3 * (size_t)id);
+                const float4 B = __ldg(S.tris + 3 * (size_t)id + 1);
+                const float4 Cc = __ldg(S.tris + 3 * (size_t)id + 2);
+                const uint32_t flags = __float_as_uint(Cc.w);
+                float u, v;
+                const float t = tri_t(xyz(A), xyz(B), xyz(Cc), o, rs, u, v);
+                if (t < best.t) {
+                    if (first) {
+                        if (!(flags & FLAG_PASS)) {
+                            best = Hit{t, id, u, v};
+                            return best;
+                        }
+                    } else {
+                        best = Hit{t, id, u, v};
+                    }
+                }
+                if (flags & FLAG_END) break;
+            }
+        } else {
+            const float4* q = S.nodes + 4 * (size_t)nd;
+            const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
+            const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);
+            const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
+            const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
+            if (tl < INF && tr < INF) {
+                if (tl <= tr) {
+                    stack[sp] = r;
+                    nd = l;
+                } else {
+                    stack[sp] = l;
+                    nd = r;
+                }
+                sp++;
+                continue;
+            }
+            if (tl < INF) {
+                nd = l;
+                continue;
+            }
+            if (tr < INF) {
+                nd = r;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        sp--;
+        nd = stack[sp];
+    }
+    return best;
+}
+
+// ---- scene records ----
+
+struct Mat {
+    float4 color;
+    float rough, metal, trans, ior;
+    f3 emit;
+    float sss;
+    f3 sss_radius;
+    float sheen, sheen_rough;
+    f3 sheen_tint;
+    float coat, coat_rough;
+};
+
+__device__ __forceinline__ Mat mat_at(const Scene& S, uint32_t m) {
+    const float4* q = S.mats + 8 * (size_t)m;
+    const float4 w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2), w4 = __ldg(q + 4), w5 = __ldg(q + 5),
+                 w6 = __ldg(q + 6);
+    Mat t;
+    t.color = w0;
+    t.rough = w1.x;
+    t.metal = w1.y;
+    t.trans = w1.z;
+    t.ior = w1.w;
+    t.emit = mk(w2.x, w2.y, w2.z);
+    t.sss = w4.y;
+    t.sss_radius = mk(w4.z, w4.w, w5.x);
+    t.sheen = w5.y;
+    t.sheen_rough = w5.z;
+    t.sheen_tint = mk(w5.w, w6.x, w6.y);
+    t.coat = w6.z;
+    t.coat_rough = w6.w;
+    return t;
+}
+
+struct Geo {
+    f3 a, b, c, na, nb, nc;
+    uint32_t face, mat;
+};
+
+__device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot) {
+    const float4 A = __ldg(S.tris + 3 * (size_t)slot), B = __ldg(S.tris + 3 * (size_t)slot + 1),
+                 Cc = __ldg(S.tris + 3 * (size_t)slot + 2);
+    Geo g;
+    g.a = xyz(A);
+    g.b = xyz(B);
+    g.c = xyz(Cc);
+    g.face = __float_as_uint(A.w);
+    g.mat = __float_as_uint(B.w);
+    if (S.tnorm) {
+        g.na = xyz(__ldg(S.tnorm + 3 * (size_t)slot));
+        g.nb = xyz(__ldg(S.tnorm + 3 * (size_t)slot + 1));
+        g.nc = xyz(__ldg(S.tnorm + 3 * (size_t)slot + 2));
+    } else {
+        g.na = g.nb = g.nc = mk(0.0f);
+    }
+    return g;
+}
+
+// ---- brdf.wgsl ----
+
+struct Surf {
+    f3 pos, n, v, albedo, f0;
+    float rough, bleed;
+    f3 sss_tint;
+    float sheen, sheen_rough;
+    f3 sheen_tint;
+    float coat, coat_rough, eta, dielectric;
+};
+
+__device__ __forceinline__ float ggx_lambda(float alpha2, float cos_n) {
+    const float t = alpha2 * fmaxf(1.0f / fmaxf(cos_n * cos_n, 1e-8f) - 1.0f, 0.0f);
+    return 0.5f * (sqrtf(1.0f + t) - 1.0f);
+}
+
+__device__ __forceinline__ f3 ggx_sample_vndf(f3 wi, float alpha, float r1, float r2) {
+    const f3 wi_ = normalize(mk(alpha * wi.x, alpha * wi.y, wi.z));
+    const float lensq = wi_.x * wi_.x + wi_.y * wi_.y;
+    f3 t1, t2;
+    if (lensq > 1e-7f) {
+        t1 = mk(-wi_.y, wi_.x, 0.0f) / sqrtf(lensq);
+        t2 = cross(wi_, t1);
+    } else {
+        t1 = mk(1.0f, 0.0f, 0.0f);
+        t2 = mk(0.0f, 1.0f, 0.0f);
+    }
+    float2 t = unit_disk(r1, r2);
+    t.y = mixf(sqrtf(fmaxf(1.0f - t.x * t.x, 0.0f)), t.y, 0.5f * (1.0f + wi_.z));
+    const f3 h_ = t1 * t.x + t2 * t.y + wi_ * sqrtf(fmaxf(0.0f, 1.0f - t.x * t.x - t.y * t.y));
+    return normalize(mk(alpha * h_.x, alpha * h_.y, fmaxf(0.0f, h_.z)));
+}
+
+__device__ __forceinline__ float ggx_weight(float alpha2, float cos_ni, float cos_no) {
+    const float li = ggx_lambda(alpha2, cos_ni);
+    const float lo = ggx_lambda(alpha2, cos_no);
+    return (1.0f + li) / (1.0f + li + lo);
+}
+
+__device__ __forceinline__ Surf plain_surf(f3 pos, f3 n, f3 v, f3 albedo, f3 f0, float rough) {
+    return Surf{pos, n, v, albedo, f0, rough, 0.0f, mk(1.0f), 0.0f, 0.5f, mk(1.0f), 0.0f, 0.03f, 0.0f, 0.0f};
+}
+
+// procedural.wgsl:73-81
+__device__ __forceinline__ float fresnel_dielectric_cos(float cosi, float eta) {
+    const float c = fabsf(cosi);
+    float g = eta * eta - 1.0f + c * c;
+    if (g <= 0.0f) return 1.0f;
+    g = sqrtf(g);
+    const float a = (g - c) / (g + c);
+    const float b = (c * (g + c) - 1.0f) / (c * (g - c) + 1.0f);
+    return 0.5f * a * a * (1.0f + b * b);
+}
+
+__device__ __forceinline__ f3 fresnel_of(const Surf& s, float cs) {
+    const float schlick = pm_pow(1.0f - cs, 5.0f);
+    f3 f = s.f0 + (mk(1.0f) - s.f0) * schlick;
+    if (s.eta > 1.0f && s.dielectric > 0.0f) {
+        const float r = (s.eta - 1.0f) / (s.eta + 1.0f);
+        const float face_on = r * r;
+        f += mk(s.dielectric * (fresnel_dielectric_cos(cs, s.eta) - face_on - (1.0f - face_on) * schlick));
+    }
+    return vmax(f, mk(0.0f));
+}
+
+__device__ __forceinline__ f3 scatter_tint(f3 radius) {
+    const float m = fmaxf(fmaxf(radius.x, radius.y), fmaxf(radius.z, 1e-6f));
+    return vmix(mk(1.0f), radius / m, 0.85f);
+}
+
+__device__ __forceinline__ float scatter_bleed(float weight, f3 radius) {
+    const float m = fmaxf(fmaxf(radius.x, radius.y), fmaxf(radius.z, 0.0f));
+    return clampf(weight, 0.0f, 1.0f) * clampf(m * 24.0f, 0.15f, 1.0f);
+}
+
+__device__ __forceinline__ float charlie(float nh, float rough) {
+    const float inv = 1.0f / fmaxf(rough * rough, 0.005f);
+    const float sin2 = fmaxf(1.0f - nh * nh, 0.0f);
+    return (2.0f + inv) * pm_pow(sin2, inv * 0.5f) / (2.0f * PI);
+}
+
+__device__ __forceinline__ f3 env_brdf(f3 f0, float rough, float nv) {
+    const float rx = rough * -1.0f + 1.0f, ry = rough * -0.0275f + 0.0425f, rz = rough * -0.572f + 1.04f,
+                rw = rough * 0.022f + -0.04f;
+    const float a004 = fminf(rx * rx, pm_exp2(-9.28f * nv)) * rx + ry;
+    const float abx = -1.04f * a004 + rz, aby = 1.04f * a004 + rw;
+    return f0 * abx + mk(aby);
+}
+
+__device__ __forceinline__ f3 dielectric_f0(float ior) {
+    const float r = (ior - 1.0f) / (ior + 1.0f);
+    return mk(r * r);
+}
+
+__device__ __forceinline__ float under_layer(f3 f0, float rough, float nv) {
+    const f3 e = env_brdf(f0, rough, nv);
+    return clampf(1.0f - fmaxf(e.x, fmaxf(e.y, e.z)), 0.0f, 1.0f);
+}
+
+__device__ __forceinline__ float under_layer_real(float eta, float rough, float nv) {
+    const float r = (eta - 1.0f) / (eta + 1.0f);
+    const float face_on = r * r;
+    const float climb = env_brdf(mk(0.0f), rough, nv).x;
+    const float flat = env_brdf(mk(1.0f), rough, nv).x - climb;
+    const float schlick = (1.0f - face_on) * pm_pow(1.0f - nv, 5.0f);
+    const float real = fresnel_dielectric_cos(nv, eta) - face_on;
+    const float scale = clampf(real / fmaxf(schlick, 1e-5f), 0.0f, 1.0f);
+    return clampf(1.0f - (face_on * flat + climb * scale), 0.0f, 1.0f);
+}
+
+// glossy_floor with phiray's own integrator (integrator.x 0): 0.3.
+__device__ __forceinline__ float glossy_floor() { return 0.3f; }
+
+__device__ __forceinline__ float ggx_pdf(const Surf& s, f3 l) {
+    const f3 h = normalize(l + s.v);
+    const float nh = fmaxf(dot(s.n, h), 0.0f);
+    const float a2 = fmaxf(s.rough * s.rough * s.rough * s.rough, 1e-4f);
+    const float dd = nh * nh * (a2 - 1.0f) + 1.0f;
+    const float dist = a2 / (PI * dd * dd);
+    const float nv = fmaxf(dot(s.n, s.v), 1e-4f);
+    const float g1 = 1.0f / (1.0f + ggx_lambda(a2, nv));
+    return g1 * dist / (4.0f * nv);
+}
+
+__device__ __forceinline__ f3 brdf_w(const Surf& s, f3 l, f3 e, float wd, float ws) {
+    const float raw = dot(s.n, l);
+    const float w = s.bleed * 0.75f;
+    const float nl = fmaxf((raw + w) / (1.0f + w), 0.0f) / (1.0f + w * 0.5f);
+    f3 thru = mk(0.0f);
+    if (s.bleed != 0.0f) thru = s.albedo * s.bleed * s.sss_tint * pm_pow(fmaxf(dot(s.v, -l), 0.0f), 3.0f) * 0.35f;
+    if (nl <= 0.0f) return thru * e * wd;
+    const f3 hv = normalize(l + s.v);
+    const float nh = fmaxf(dot(s.n, hv), 0.0f);
+    const float hvv = fmaxf(dot(hv, s.v), 0.0f);
+    const float a2 = fmaxf(s.rough * s.rough * s.rough * s.rough, 1e-4f);
+    const float dd = nh * nh * (a2 - 1.0f) + 1.0f;
+    const float dist = a2 / (PI * dd * dd);
+    const f3 fres = fresnel_of(s, hvv);
+    const float nv = fmaxf(dot(s.n, s.v), 1e-4f);
+    const float g2 = 1.0f / (1.0f + ggx_lambda(a2, nv) + ggx_lambda(a2, fmaxf(raw, 1e-4f)));
+    const f3 spec = fres * dist * g2 * 0.25f / nv;
+    const f3 diffuse = vmix(s.albedo, s.albedo * s.sss_tint, s.bleed) / PI;
+    f3 sum = diffuse * wd + spec * ws;
+    if (s.sheen != 0.0f) sum += s.sheen_tint * s.sheen * charlie(nh, s.sheen_rough);
+    if (s.coat != 0.0f) {
+        const float ca2 = fmaxf(s.coat_rough * s.coat_rough * s.coat_rough * s.coat_rough, 1e-4f);
+        const float cd = nh * nh * (ca2 - 1.0f) + 1.0f;
+        const float coat_f = 0.04f + 0.96f * pm_pow(1.0f - hvv, 5.0f);
+        const float coat = s.coat * coat_f * (ca2 / (PI * cd * cd)) * 0.25f;
+        const float under = 1.0f - s.coat * coat_f;
+        sum = sum * under + mk(coat);
+    }
+    f3 out = sum * e * nl;
+    if (s.bleed != 0.0f) out += thru * e * wd;
+    return out;
+}
+
+__device__ __forceinline__ f3 brdf(const Surf& s, f3 l, f3 e) { return brdf_w(s, l, e, 1.0f, 1.0f); }
+
+// ---- light.wgsl ----
+
+__device__ __forceinline__ f3 onb(f3 n, float a, float b) {
+    const f3 tx = normalize(fabsf(n.z) > 0.9f ? cross(n, mk(1.0f, 0.0f, 0.0f)) : cross(n, mk(0.0f, 0.0f, 1.0f)));
+    const f3 ty = cross(n, tx);
+    return tx * a + ty * b;
+}
+
+__device__ __forceinline__ f3 cone_dir(f3 axis, float ang, uint32_t& seed) {
+    if (ang <= 0.0f) return axis;
+    const float r = ang * sqrtf(rnd(seed));
+    const float ph = 2.0f * PI * rnd(seed);
+    float s, c;
+    pm_sincos(ph, &s, &c);
+    return normalize(axis + onb(axis, r * c, r * s));
+}
+
+__device__ __forceinline__ f3 cosine_dir(f3 n, uint32_t& seed) {
+    const float r1 = rnd(seed);
+    const float rr = sqrtf(r1);
+    const float ph = 2.0f * PI * rnd(seed);
+    float s, c;
+    pm_sincos(ph, &s, &c);
+    return normalize(onb(n, rr * c, rr * s) + n * sqrtf(fmaxf(0.0f, 1.0f - r1)));
+}
+
+struct Shadowed {
+    f3 c, dir;
+    float dist;
+};
+
+__device__ __forceinline__ Shadowed unshadowed() { return Shadowed{mk(0.0f), mk(0.0f, 0.0f, 1.0f), 0.0f}; }
+
+__device__ __forceinline__ float spot_mask(const phx_light& li, f3 l) {
+    const f3 dir = mk(li.dir[0], li.dir[1], li.dir[2]);
+    const float z = -dot(l, dir);
+    if (z <= 0.0f) return 0.0f;
+    float ellipse = z;
+    const f3 right = mk(li.right[0], li.right[1], li.right[2]);
+    const float ssx = li.spot_scale[0], ssy = li.spot_scale[1];
+    if (dot(right, right) > 1e-12f && ssx * ssx + ssy * ssy > 1e-12f) {
+        const f3 d = -l;
+        const float xx = dot(d, right) * ssx, yy = dot(d, cross(dir, right)) * ssy;
+        ellipse = 1.0f / sqrtf(1.0f + (xx * xx + yy * yy) / (z * z));
+    }
+    return smoothstepf(li.cone, li.cone + li.blend, ellipse);
+}
+
+__device__ __forceinline__ float lamp_reach(const phx_light& li, f3 at, float ao) {
+    const f3 color = mk(li.color[0], li.color[1], li.color[2]);
+    const float lum = dot(vmax(color, mk(0.0f)), mk(0.2126f, 0.7152f, 0.0722f));
+    if (li.kind == 0u) return lum;
+    const f3 to = mk(li.pos[0], li.pos[1], li.pos[2]) - at;
+    const float nr = fmaxf(li.size * 0.5f, ao * 0.05f);
+    return lum / ((4.0f * PI) * (dot(to, to) + nr * nr));
+}
+
+__device__ __forceinline__ Shadowed area_query(const Surf& s, const phx_light& li, float weight, float r1, float r2,
+                                               float pick) {
+    const f3 lpos = mk(li.pos[0], li.pos[1], li.pos[2]), ldir = mk(li.dir[0], li.dir[1], li.dir[2]),
+             lright = mk(li.right[0], li.right[1], li.right[2]);
+    const float height = dot(s.pos - lpos, ldir);
+    if (height <= 0.0f) return unshadowed();
+    const bool round = li.shape == 4u || li.shape == 5u;
+    const float hx = li.size * 0.5f, hy = li.size_y * 0.5f;
+    const float area = fmaxf(li.size * li.size_y * (round ? 0.25f * PI : 1.0f), 1e-8f);
+    const f3 up = cross(ldir, lright);
+    const f3 off = s.pos - lpos;
+    const float near = area / (area + PI * dot(off, off));
+    float onx, ony;
+    float sn, cs;
+    pm_sincos(2.0f * PI * r2, &sn, &cs);
+    if (pick < near) {
+        const float spread = sqrtf(r1 / fmaxf(1.0f - r1, 1e-6f)) * height;
+        onx = cs * spread + dot(off, lright);
+        ony = sn * spread + dot(off, up);
+        const float ux = onx / fmaxf(hx, 1e-8f), uy = ony / fmaxf(hy, 1e-8f);
+        const bool inside = round ? (ux * ux + uy * uy <= 1.0f) : (fmaxf(fabsf(ux), fabsf(uy)) <= 1.0f);
+        if (!inside) return unshadowed();
+    } else {
+        const float sq = sqrtf(r1);
+        if (round) {
+            onx = cs * sq * hx;
+            ony = sn * sq * hy;
+        } else {
+            onx = (r1 * 2.0f - 1.0f) * hx;
+            ony = (r2 * 2.0f - 1.0f) * hy;
+        }
+    }
+    const f3 to = lpos + lright * onx + up * ony - s.pos;
+    const float d2 = fmaxf(dot(to, to), 1e-6f);
+    const f3 l = to / sqrtf(d2);
+    const float facing = fmaxf(dot(-l, ldir), 0.0f);
+    const float pdf = (1.0f - near) / area + near * facing * facing / (PI * d2);
+    const f3 e = mk(li.color[0], li.color[1], li.color[2]) / (PI * area) * facing / d2 / fmaxf(pdf, 1e-12f);
+    if (maxc(e) < 1e-5f) return unshadowed();
+    return Shadowed{brdf(s, l, e) * weight, l, sqrtf(d2) * 0.999f};
+}
+
+__device__ __forceinline__ Shadowed lamp_query(const Frame& F, const Surf& s, uint32_t& seed) {
+    float total = 0.0f, held = 0.0f;
+    uint32_t idx = 0;
+    float u = rnd(seed);
+    for (uint32_t k = 0; k < F.count; k++) {
+        const float w = lamp_reach(F.lights[k], s.pos, F.ao);
+        if (w <= 0.0f) continue;
+        total += w;
+        const float share = w / total;
+        if (u < share) {
+            idx = k;
+            held = w;
+            u = u / share;
+        } else {
+            u = (u - share) / (1.0f - share);
+        }
+    }
+    if (total <= 0.0f || held <= 0.0f) return unshadowed();
+    const phx_light& li = F.lights[idx];
+    const float weight = total / held;
+    const f3 color = mk(li.color[0], li.color[1], li.color[2]);
+    if (li.kind == 0u) {
+        const f3 l = cone_dir(-mk(li.dir[0], li.dir[1], li.dir[2]), li.size * 0.5f, seed);
+        return Shadowed{brdf(s, l, color) * weight, l, INF};
+    }
+    const float r1 = rnd(seed);
+    const float r2 = rnd(seed);
+    if (li.kind == 3u) return area_query(s, li, weight, r1, r2, rnd(seed));
+    const f3 lpos = mk(li.pos[0], li.pos[1], li.pos[2]);
+    const f3 aim = lpos + onb(normalize(s.pos - lpos), (r1 - 0.5f) * li.size, (r2 - 0.5f) * li.size);
+    const f3 to = aim - s.pos;
+    const float d2 = fmaxf(dot(to, to), 1e-6f);
+    const f3 l = to / sqrtf(d2);
+    f3 e = color / ((4.0f * PI) * d2);
+    if (li.kind == 2u) e *= spot_mask(li, l);
+    if (maxc(e) < 1e-5f) return unshadowed();
+    return Shadowed{brdf(s, l, e) * weight, l, sqrtf(d2) * 0.999f};
+}
+
+__device__ __forceinline__ float lamp_chance(const Scene& S, uint32_t slot) {
+    const uint32_t count = S.lamp_count;
+    if (count == 0u) return 0.0f;
+    uint32_t lo = 0, hi = count - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (__ldg(S.lamp_slot + mid) < slot) lo = mid + 1u;
+        else hi = mid;
+    }
+    if (__ldg(S.lamp_slot + lo) != slot) return 0.0f;
+    const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
+    return __ldg(S.lamp_cdf + lo) - prev;
+}
+
+__device__ __forceinline__ Shadowed glow_query(const Scene& S, const Surf& s, uint32_t& seed) {
+    const uint32_t count = S.lamp_count;
+    if (count == 0u) return unshadowed();
+    const float u = rnd(seed);
+    uint32_t lo = 0, hi = count - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (__ldg(S.lamp_cdf + mid) < u) lo = mid + 1u;
+        else hi = mid;
+    }
+    const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
+    const float chance = fmaxf(__ldg(S.lamp_cdf + lo) - prev, 1e-8f);
+    const uint32_t f = __ldg(S.lamp_slot + lo);
+    const Geo g = geo_at(S, f);
+    const Mat t = mat_at(S, g.mat);
+    float a = rnd(seed);
+    float b = rnd(seed);
+    if (a + b > 1.0f) {
+        a = 1.0f - a;
+        b = 1.0f - b;
+    }
+    const f3 q = g.a + (g.b - g.a) * a + (g.c - g.a) * b;
+    const f3 cr = cross(g.b - g.a, g.c - g.a);
+    const float area = 0.5f * length(cr);
+    const f3 to = q - s.pos;
+    const float d2 = fmaxf(dot(to, to), 1e-6f);
+    const f3 l = to / sqrtf(d2);
+    const float cos_l = fabsf(dot(normalize(cr), l));
+    const f3 e = t.emit * cos_l * area / (chance * d2);
+    const float pl = chance * d2 / fmaxf(area * cos_l, 1e-8f);
+    const float pb = fmaxf(dot(s.n, l), 0.0f) / PI;
+    const float w = pl * pl / fmaxf(pl * pl + pb * pb, 1e-12f);
+    return Shadowed{brdf(s, l, e) * w, l, sqrtf(d2) * 0.999f};
+}
+
+__device__ __forceinline__ float hit_lift(const Frame& F, float t) {
+    const float start = 1.0e4f / F.units;
+    if (F.persp == 0u && t > start * 0.5f) return F.eps + fabsf(t - start) * 1e-5f + start * 2.4e-7f;
+    return F.eps + t * 1e-5f;
+}
+
+__device__ __forceinline__ float through_lift(const Frame& F, f3 pos, float t) {
+    const float reach = fmaxf(fmaxf(fabsf(pos.x), fabsf(pos.y)), fmaxf(fabsf(pos.z), 0.5f));
+    return hit_lift(F, t) - F.eps + reach * (256.0f / 8388608.0f);
+}
+
+__device__ __forceinline__ bool uses_rig(const Frame& F) { return F.count == 0u && !(dot(F.env, F.env) > 0.0f); }
+
+__device__ __forceinline__ Shadowed rig_query(const Frame& F, uint32_t k, const Surf& s, uint32_t& seed, f3 sun) {
+    if (k == 0u) {
+        const f3 key = cone_dir(sun, 0.06f, seed);
+        return Shadowed{brdf(s, key, mk(2.0f)), key, INF};
+    }
+    const f3 rim = normalize(F.up * 0.6f - F.back * 0.8f + F.right * 0.2f);
+    return Shadowed{brdf(s, rim, mk(0.9f)), rim, INF};
+}
+
+__device__ __forceinline__ f3 rig_fill(const Frame& F, const Surf& s) {
+    const f3 fill = normalize(-F.right * 0.8f + F.up * 0.2f + F.back * 0.6f);
+    return brdf(s, fill, mk(0.45f));
+}
+
+}  // namespace shade
+}  // namespace phx

@@ -102,6 +102,12 @@ int32_t launch_skin_step(cudaStream_t s, const void* params, void* const* bufs, 
                        p.min, status);
 }
 
+int32_t launch_face_boxes(cudaStream_t s, const float* verts, const uint32_t* faces, uint32_t nfaces, phx_aabb* boxes) {
+    if (nfaces == 0) return PHX_OK;
+    k_face_boxes<<<(nfaces + 255) / 256, 256, 0, s>>>((const float4*)verts, (const uint4*)faces, nfaces, (float4*)boxes);
+    return cuda_check(cudaGetLastError(), "face boxes");
+}
+
 }  // namespace phx
 
 using namespace phx;
@@ -117,11 +123,8 @@ int32_t phx_skin(phx_ctx ctx, const float* rest, const uint32_t* offsets, const 
 
 int32_t phx_face_boxes(phx_ctx ctx, const float* verts, const uint32_t* faces, uint32_t nfaces, phx_aabb* boxes) {
     if (!ctx || (nfaces && (!verts || !faces || !boxes))) return fail(PHX_ERR_INVALID, "null argument");
-    if (nfaces == 0) return PHX_OK;
     PHX_TRY(use(&ctx->c));
-    k_face_boxes<<<(nfaces + 255) / 256, 256, 0, ctx->c.stream>>>((const float4*)verts, (const uint4*)faces, nfaces,
-                                                                    (float4*)boxes);
-    return cuda_check(cudaGetLastError(), "face boxes");
+    return launch_face_boxes(ctx->c.stream, verts, faces, nfaces, boxes);
 }
 
 }  // extern "C"

@@ -1,0 +1,963 @@
+// The Rendered-mode tracer (phiray Tracer, src/trace/*.rs) on the device.
+//
+// A scene is uploaded once; its LBVH is built on the device over the face
+// boxes (bvh.cu) and re-encoded for the walk (shade.cuh): inner nodes with
+// both children's boxes inline, triangles gathered into leaf order. The
+// sample kernel runs shade.wgsl's main for every pixel and keeps the
+// per-pixel sums in registers across all the samples of a call, writing the
+// image planes once at the end — the same sums, in the same order, that the
+// reference's one-dispatch-per-sample loop leaves in its px buffer.
+#include <cfloat>
+#include <cstring>
+
+#include "lbvh.cuh"
+#include "shade.cuh"
+
+namespace phx {
+
+using namespace shade;
+
+namespace {
+
+// ---- scene preparation ----
+
+// tris in slot order (sorted by Morton code): positions, face id, material,
+// and the shadow-pass flag from the material (bvh.wgsl:158-162).
+__global__ void k_gather(const uint32_t* __restrict__ order, const uint4* __restrict__ faces,
+                         const float4* __restrict__ verts, const float4* __restrict__ vnorm,
+                         const float4* __restrict__ mats, uint32_t nmats, uint32_t n, float4* __restrict__ tris,
+                         float4* __restrict__ tnorm, uint32_t* status) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t f = __ldg(order + s);
+    const uint4 v = __ldg(faces + f);
+    const float4 a = __ldg(verts + v.x), b = __ldg(verts + v.y), c = __ldg(verts + v.z);
+    uint32_t m = v.w;
+    if (m >= nmats) {
+        atomicOr(status, STATUS_BAD_INDEX);
+        m = 0;
+    }
+    const float4 m0 = __ldg(mats + 8 * (size_t)m), m1 = __ldg(mats + 8 * (size_t)m + 1);
+    const uint32_t flags = (m1.z > 0.5f || m0.w < 0.5f) ? FLAG_PASS : 0u;
+    tris[3 * (size_t)s] = make_float4(a.x, a.y, a.z, __uint_as_float(f));
+    tris[3 * (size_t)s + 1] = make_float4(b.x, b.y, b.z, __uint_as_float(m));
+    tris[3 * (size_t)s + 2] = make_float4(c.x, c.y, c.z, __uint_as_float(flags));
+    if (tnorm) {
+        tnorm[3 * (size_t)s] = __ldg(vnorm + v.x);
+        tnorm[3 * (size_t)s + 1] = __ldg(vnorm + v.y);
+        tnorm[3 * (size_t)s + 2] = __ldg(vnorm + v.z);
+    }
+}
+
+// Marks the last slot of every reachable leaf (the refit's start list).
+__global__ void k_mark_ends(const float4* __restrict__ nodes, const uint32_t* __restrict__ starts,
+                            const uint32_t* __restrict__ nstarts, float4* tris) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *nstarts) return;
+    const uint32_t i = starts[t];
+    const uint32_t end = __float_as_uint(nodes[2 * (size_t)i + 1].w);
+    float4* c = tris + 3 * (size_t)(end - 1) + 2;
+    c->w = __uint_as_float(__float_as_uint(c->w) | FLAG_END);
+}
+
+// Inner node i -> both children's boxes and refs (leaf child: first | LEAF).
+__global__ void k_convert(const float4* __restrict__ nodes, uint32_t ninner, float4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninner) return;
+    const float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
+    const uint32_t li = __float_as_uint(a.w), ri = __float_as_uint(b.w);
+    if (li & LEAF) return;  // a packed leaf: never walked as an inner node
+    const float4 la = nodes[2 * (size_t)li], lb = nodes[2 * (size_t)li + 1];
+    const float4 ra = nodes[2 * (size_t)ri], rb = nodes[2 * (size_t)ri + 1];
+    const uint32_t lr = (__float_as_uint(la.w) & LEAF) ? __float_as_uint(la.w) : li;
+    const uint32_t rr = (__float_as_uint(ra.w) & LEAF) ? __float_as_uint(ra.w) : ri;
+    float4* q = out + 4 * (size_t)i;
+    q[0] = make_float4(la.x, la.y, la.z, lb.x);
+    q[1] = make_float4(lb.y, lb.z, ra.x, ra.y);
+    q[2] = make_float4(ra.z, rb.x, rb.y, rb.z);
+    q[3] = make_float4(__uint_as_float(lr), __uint_as_float(rr), 0.0f, 0.0f);
+}
+
+// Root box, root ref and the scene extent (Forest::extent, forest.rs:192-200:
+// the root box's diagonal, at least 1e-3).
+__global__ void k_root(const float4* __restrict__ nodes, uint32_t n, float4* info) {
+    const float4 a = nodes[0], b = nodes[1];
+    const uint32_t li = __float_as_uint(a.w);
+    const uint32_t root = (li & LEAF) ? li : 0u;
+    float e = 0.0f;
+    const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+    e = e + dx * dx;
+    e = e + dy * dy;
+    e = e + dz * dz;
+    const float ext = fmaxf(sqrtf(e), 1e-3f);
+    info[0] = make_float4(a.x, a.y, a.z, __uint_as_float(root));
+    info[1] = make_float4(b.x, b.y, b.z, ext);
+}
+
+// The emitter table (lamp.rs table_of, one instance): emissive slots in slot
+// order with their power (world area x emitted luminance) and its running
+// share. One block: counts per thread chunk, a block scan for positions,
+// then one thread sums in slot order so the CDF rounds as the CPU's does.
+__global__ void __launch_bounds__(1024) k_lamps(const float4* __restrict__ tris, const float4* __restrict__ mats,
+                                                uint32_t n, uint32_t* __restrict__ slots, float* __restrict__ power,
+                                                float* __restrict__ cdf, float4* info) {
+    __shared__ uint32_t s_count[1024];
+    const uint32_t T = blockDim.x, t = threadIdx.x;
+    const uint32_t chunk = (n + T - 1) / T;
+    const uint32_t lo = t * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    auto glow = [&](uint32_t s, float& p) -> bool {
+        const float4 A = __ldg(tris + 3 * (size_t)s), B = __ldg(tris + 3 * (size_t)s + 1),
+                     Cc = __ldg(tris + 3 * (size_t)s + 2);
+        const uint32_t m = __float_as_uint(B.w);
+        const float4 e = __ldg(mats + 8 * (size_t)m + 2);
+        const float lum = 0.2126f * e.x + 0.7152f * e.y + 0.0722f * e.z;
+        if (!(lum > 0.0f)) return false;
+        const float e1x = B.x - A.x, e1y = B.y - A.y, e1z = B.z - A.z;
+        const float e2x = Cc.x - A.x, e2y = Cc.y - A.y, e2z = Cc.z - A.z;
+        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        float sq = 0.0f;
+        sq = sq + cx * cx;
+        sq = sq + cy * cy;
+        sq = sq + cz * cz;
+        p = 0.5f * sqrtf(sq) * lum;
+        return p > 0.0f;
+    };
+    uint32_t c = 0;
+    for (uint32_t s = lo; s < hi; s++) {
+        float p;
+        if (glow(s, p)) c++;
+    }
+    s_count[t] = c;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < T; k++) {
+            const uint32_t v = s_count[k];
+            s_count[k] = run;
+            run += v;
+        }
+        info[2] = make_float4(__uint_as_float(run), 0.0f, 0.0f, 0.0f);
+    }
+    __syncthreads();
+    uint32_t at = s_count[t];
+    for (uint32_t s = lo; s < hi; s++) {
+        float p;
+        if (glow(s, p)) {
+            slots[at] = s;
+            power[at] = p;
+            at++;
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        const uint32_t count = __float_as_uint(info[2].x);
+        float total = 0.0f;
+        for (uint32_t k = 0; k < count; k++) total += power[k];
+        float run = 0.0f;
+        for (uint32_t k = 0; k < count; k++) {
+            run += power[k];
+            cdf[k] = run / total;
+        }
+    }
+}
+
+// ---- the sample kernel (shade.wgsl main) ----
+
+struct Sums {
+    f3 lin, grid, alb, nrm;
+    float cov, film, gone, dep;
+    uint32_t count, outline;
+};
+
+__device__ __forceinline__ float srgb_to_linear1(float c) {
+    return c <= 0.04045f ? c / 12.92f : pm_pow((c + 0.055f) / 1.055f, 2.4f);
+}
+
+__device__ __forceinline__ f3 env_at(const Frame& F) { return F.env; }
+
+// direct (integrate.wgsl:66-85): every light with its shadow ray.
+__device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s, uint32_t& seed, bool with_env,
+                                  f3 sun, uint32_t& rays) {
+    const bool rig = uses_rig(F);
+    f3 sum = rig ? rig_fill(F, s) : mk(0.0f);
+    for (uint32_t k = 0; k < 4u; k++) {
+        Shadowed q = unshadowed();
+        if (k == 0u) {
+            q = rig ? rig_query(F, 0u, s, seed, sun) : lamp_query(F, s, seed);
+        } else if (k == 1u) {
+            if (rig) q = rig_query(F, 1u, s, seed, sun);
+        } else if (k == 2u) {
+            q = glow_query(S, s, seed);
+        }
+        // k == 3: env_query needs an environment image's table (env_cdf),
+        // which the host refuses; it returns unshadowed without a draw.
+        if (maxc(q.c) > 0.0f) {
+            rays++;
+            const float vis = trace(S, s.pos, q.dir, q.dist, true).tri != NONE ? 0.0f : 1.0f;
+            sum += q.c * vis;
+        }
+    }
+    return sum;
+}
+
+// glow_mis (integrate.wgsl:15-23).
+__device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, const Hit& h, f3 from_n, f3 dir) {
+    const float chance = lamp_chance(S, h.tri);
+    if (chance <= 0.0f) return emit;
+    const f3 cr = cross(g.b - g.a, g.c - g.a);
+    const float pl = chance * h.t * h.t / fmaxf(0.5f * length(cr) * fabsf(dot(normalize(cr), dir)), 1e-8f);
+    const float pb = fmaxf(dot(from_n, dir), 0.0f) / PI;
+    return emit * pb * pb / fmaxf(pb * pb + pl * pl, 1e-12f);
+}
+
+// indirect (integrate.wgsl:111-230) with no environment image.
+__device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f3 n, uint32_t& seed, bool bounce,
+                                       f3 sun, uint32_t& rays) {
+    const bool lit = dot(F.env, F.env) > 0.0f;
+    if (S.lamp_count == 0u && !lit) {
+        const f3 dir = cosine_dir(n, seed);
+        // env_at(dir) * mix(0.25, 1, visible(pos, dir, ao)): with a black
+        // world the product is zero whatever the shadow ray finds, so the
+        // ray is only traced when the world has some colour.
+        if (F.env.x == 0.0f && F.env.y == 0.0f && F.env.z == 0.0f) return mk(0.0f);
+        rays++;
+        const float vis = trace(S, pos, dir, F.ao, true).tri != NONE ? 0.0f : 1.0f;
+        return env_at(F) * mixf(0.25f, 1.0f, vis);
+    }
+    const uint32_t depth = bounce ? (F.bounces != 0u ? F.bounces : 1u) : 1u;
+    f3 acc = mk(0.0f), thr = mk(1.0f), org = pos, nrm = n;
+    float min_pdf = 3.0e38f;
+    bool through = false;
+    f3 dir = mk(0.0f, 0.0f, 1.0f);
+    float pb = 1.0f;
+    for (uint32_t b = 0; b < depth; b++) {
+        if (!through) {
+            dir = cosine_dir(nrm, seed);
+            pb = fmaxf(dot(nrm, dir), 0.0f) / PI;
+        }
+        through = false;
+        min_pdf = fminf(min_pdf, pb);
+        rays++;
+        const Hit h = trace(S, org, dir, INF, false);
+        if (h.tri == NONE) {
+            acc += thr * env_at(F) * 1.0f;
+            break;
+        }
+        if (!bounce) break;
+        const Geo g = geo_at(S, h.tri);
+        const Mat t = mat_at(S, g.mat);
+        const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+        const f3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
+        const f3 hit = org + dir * h.t + ng * (F.eps + h.t * 1e-5f);
+        const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+        const float rough = fmaxf(t.rough, glossy_floor());
+        const f3 fd = dielectric_f0(t.ior);
+        const float metal = t.metal;
+        const float tw = t.trans * (1.0f - t.metal);
+        f3 albedo = base * (1.0f - t.metal) * (1.0f - tw);
+        if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -dir), 1e-4f));
+        acc += thr * glow_mis(S, g, t.emit, h, nrm, dir);
+        const float near = (!lit && h.t <= F.ao) ? 0.25f : 1.0f;
+        const Surf s = plain_surf(hit, ng, -dir, albedo, vmix(fd, base, metal), rough);
+        acc += thr * direct(S, F, s, seed, true, sun, rays) * near;
+        if (tw > 0.0f && rnd(seed) < tw) {
+            thr *= mk(sqrtf(base.x), sqrtf(base.y), sqrtf(base.z));
+            const f3 at = org + dir * h.t;
+            org = at - ng * through_lift(F, at, h.t);
+            through = true;
+            continue;
+        }
+        thr *= albedo;
+        if (b + 1u < depth) {
+            const float keep = clampf(maxc(thr), 0.0f, 0.95f);
+            if (keep < 1e-4f || rnd(seed) > keep) break;
+            thr = thr / keep;
+        }
+        org = hit;
+        nrm = ng;
+    }
+    return acc;
+}
+
+// bounce_light (integrate.wgsl:236-250).
+__device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const Hit& h, f3 org, f3 d,
+                                           uint32_t& seed, f3 sun, uint32_t& rays) {
+    const Geo g = geo_at(S, h.tri);
+    const Mat t = mat_at(S, g.mat);
+    const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+    const f3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
+    const f3 pos = org + d * h.t + ng * (F.eps + h.t * 1e-5f);
+    const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+    const float rough = fmaxf(t.rough, glossy_floor());
+    const f3 fd = dielectric_f0(t.ior);
+    f3 albedo = base * (1.0f - t.metal);
+    if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -d), 1e-4f));
+    const Surf s = plain_surf(pos, ng, -d, albedo, vmix(fd, base, t.metal), rough);
+    return direct(S, F, s, seed, false, sun, rays) + s.albedo * env_at(F) * 0.8f + t.emit;
+}
+
+__device__ __forceinline__ f3 clamp_light(f3 l, float limit) {
+    const float m = fmaxf(l.x, fmaxf(l.y, l.z));
+    if (limit <= 0.0f || m <= limit) return l;
+    return l * (limit / m);
+}
+
+struct CamRay {
+    f3 o, d;
+};
+
+__device__ __forceinline__ CamRay camera_ray(const Frame& F, uint32_t i, uint32_t& seed) {
+    const float su = ((float)(i % F.w) + 0.5f) / (float)F.w - 0.5f;
+    const float sv = ((float)(i / F.w) + 0.5f) / (float)F.h - 0.5f;
+    const float jox = rnd(seed) - 0.5f;
+    const float joy = rnd(seed) - 0.5f;
+    const float jx = jox / (float)F.w;
+    const float jy = joy / (float)F.h;
+    const float vx = (su + jx - F.pan_x) / F.scale;
+    const float vy = -((sv + jy) / F.aspect - F.pan_y) / F.scale;
+    CamRay r;
+    if (F.persp != 0u) {
+        r.o = F.pivot + F.back * (F.dist / F.units);
+        r.d = normalize(F.right * vx + F.up * vy - F.back * F.dist);
+    } else {
+        r.o = F.pivot + (F.right * vx + F.up * vy + F.back * 1.0e4f) / F.units;
+        r.d = -F.back;
+    }
+    return r;
+}
+
+// One sample of pixel i (shade.wgsl:41-373) added into `acc`.
+__device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t frame, f3 sun, Sums& acc,
+                       uint32_t& rays) {
+    uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
+    const CamRay cr = camera_ray(F, i, seed);
+    f3 o = cr.o, d = cr.d;
+    acc.outline = 0;
+    f3 col = mk(0.0f), thr = mk(1.0f);
+    const uint32_t see_through = 8u, through = 8u;
+    const bool glossy_on = true, diffuse_on = true;
+    uint32_t n_see = 0, n_through = 0;
+    const uint32_t passes = see_through + through + 1u;
+    for (uint32_t bounce = 0; bounce < passes; bounce++) {
+        rays++;
+        const Hit h = trace(S, o, d, INF, false);
+        if (h.tri == NONE) {
+            if (bounce == 0u) {
+                const float across = (float)(i % F.w) / fmaxf((float)F.w * 0.5f, 1.0f);
+                const float lift = F.sky[3] * (1.0f - clampf(across, 0.0f, 1.0f));
+                const f3 sky = mk(F.sky[0] + lift, F.sky[1] + lift, F.sky[2] + lift);
+                acc.alb += mk(srgb_to_linear1(sky.x), srgb_to_linear1(sky.y), srgb_to_linear1(sky.z));
+                acc.nrm += -d;
+                acc.dep += -1.0f;
+                acc.gone += 1.0f;
+                acc.count += 1u;
+                acc.film += 1.0f;
+                acc.lin += mk(0.0f);
+                acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                acc.cov += 1.0f;
+                return;
+            }
+            col += thr * env_at(F);
+            break;
+        }
+        if (bounce == 0u) acc.outline = 1u;
+        const Geo g = geo_at(S, h.tri);
+        const Mat t = mat_at(S, g.mat);
+        const float w = 1.0f - h.u - h.v;
+        const f3 hit = o + d * h.t;
+        const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+        const bool front = dot(ng0, d) < 0.0f;
+        const f3 ng = front ? ng0 : -ng0;
+        f3 n = g.na * w + g.nb * h.u + g.nc * h.v;
+        n = dot(n, n) > 1e-12f ? normalize(n) * (front ? 1.0f : -1.0f) : ng;
+        if (dot(n, -d) < 0.0f) n = ng;
+        const f3 off = ng * hit_lift(F, h.t);
+        const f3 past = ng * through_lift(F, hit, h.t);
+        const f3 pos = hit + off;
+        const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+        const float alpha = t.color.w;
+        const float rough = t.rough;
+        const float metal = t.metal;
+        const f3 emit = t.emit;
+        if (bounce == 0u) {
+            acc.alb += base;
+            acc.nrm += n;
+            acc.dep += h.t;
+        }
+        if (rnd(seed) >= alpha) {
+            n_see++;
+            if (n_see > see_through) break;
+            o = hit - past;
+            continue;
+        }
+        col += thr * emit;
+        const float bleed = scatter_bleed(t.sss, t.sss_radius);
+        const f3 fd = dielectric_f0(t.ior);
+        f3 diffuse = base * (1.0f - metal);
+        if (maxc(diffuse) > 0.0f) diffuse *= under_layer_real(t.ior, fmaxf(rough, 0.04f), fmaxf(dot(n, -d), 1e-4f));
+        const Surf s{pos,   n,      -d,        diffuse,         vmix(fd, base, metal), fmaxf(rough, 0.04f),
+                     bleed, scatter_tint(t.sss_radius), t.sheen, t.sheen_rough,    t.sheen_tint,
+                     t.coat, t.coat_rough, t.ior, 1.0f - metal};
+        const float opaque = 1.0f - t.trans * (1.0f - metal);
+        f3 c = mk(0.0f);
+        if (opaque > 0.0f) c = direct(S, F, s, seed, true, sun, rays) * opaque;
+        if (opaque < 1.0f) {
+            const Surf shine{pos, n, -d, mk(0.0f), s.f0, s.rough, 0.0f, mk(1.0f), 0.0f, t.sheen_rough,
+                             t.sheen_tint, t.coat, t.coat_rough, s.eta, s.dielectric};
+            c += direct(S, F, shine, seed, true, sun, rays) * (1.0f - opaque);
+        }
+        c = clamp_light(c, F.limit_d);
+        f3 bounced = mk(0.0f);
+        const f3 diffuse_weight = vmix(s.albedo, s.albedo * s.sss_tint, bleed) * opaque;
+        const f3 lw = mk(0.2126f, 0.7152f, 0.0722f);
+        const float ndv = fmaxf(dot(n, -d), 1e-4f);
+        const f3 gloss_guess = s.f0 + (mk(1.0f) - s.f0) * pm_pow(1.0f - ndv, 5.0f);
+        const float pd = dot(vmax(diffuse_weight, mk(0.0f)), lw);
+        const float pg = glossy_on ? dot(gloss_guess, lw) : 0.0f;
+        float p_diffuse = pd + pg > 0.0f ? pd / (pd + pg) : 1.0f;
+        if (pd > 0.0f && pg > 0.0f) p_diffuse = clampf(p_diffuse, 0.15f, 0.85f);
+        const bool take_diffuse = rnd(seed) < p_diffuse;
+        if (take_diffuse && pd > 0.0f)
+            bounced += diffuse_weight * indirect(S, F, pos, n, seed, diffuse_on, sun, rays) / p_diffuse;
+        const f3 v = -d;
+        const f3 tx = normalize(onb(n, 1.0f, 0.0f));
+        const f3 ty = cross(n, tx);
+        const float ggx_a = s.rough * s.rough;
+        const f3 wi_local = mk(dot(v, tx), dot(v, ty), dot(v, n));
+        const float r1 = rnd(seed);
+        const float r2 = rnd(seed);
+        const f3 h_local = ggx_sample_vndf(wi_local, ggx_a, r1, r2);
+        const f3 hw = normalize(tx * h_local.x + ty * h_local.y + n * h_local.z);
+        const f3 refl = reflect(d, hw);
+        const float cos_hi = fmaxf(dot(hw, v), 0.0f);
+        const float cos_no = dot(n, refl);
+        const f3 fres = fresnel_of(s, cos_hi);
+        if (!take_diffuse && glossy_on && dot(refl, ng) > 0.0f && cos_hi > 0.0f && cos_no > 0.0f) {
+            rays++;
+            const Hit rh = trace(S, pos, refl, INF, false);
+            f3 rc = env_at(F);
+            const float wg = 1.0f;
+            if (rh.tri != NONE) rc = bounce_light(S, F, rh, pos, refl, seed, sun, rays);
+            bounced += fres * rc * ggx_weight(ggx_a * ggx_a, fmaxf(dot(n, v), 1e-4f), cos_no) * wg / (1.0f - p_diffuse);
+        }
+        c += clamp_light(bounced, F.limit_i);
+        col += thr * c;
+        const float tw = t.trans * (1.0f - metal);
+        if (tw <= 0.0f) break;
+        n_through++;
+        if (n_through > through) break;
+        const float eta = front ? 1.0f / t.ior : t.ior;
+        f3 nd = refract(d, n, eta);
+        if (dot(nd, nd) < 1e-6f) {
+            nd = reflect(d, n);
+            o = hit + past;
+            thr *= tw;
+        } else {
+            o = hit - past;
+            thr *= mk(sqrtf(base.x), sqrtf(base.y), sqrtf(base.z)) * tw * (mk(1.0f) - fres);
+        }
+        d = cone_dir(normalize(nd), s.rough * s.rough, seed);
+        if (maxc(thr) < 0.01f) break;
+    }
+    // emit (util.wgsl:101-145) with no grid overlay: over = 0.
+    acc.gone += 0.0f;
+    acc.count += 1u;
+    acc.film += 1.0f;
+    acc.lin += col;
+    acc.grid += mk(0.0f);
+    acc.cov += 0.0f;
+}
+
+__device__ __forceinline__ void ld3(const uint32_t* px, uint32_t base, uint32_t i, f3& v) {
+    v = mk(__uint_as_float(px[base + 3 * i]), __uint_as_float(px[base + 3 * i + 1]),
+           __uint_as_float(px[base + 3 * i + 2]));
+}
+
+__device__ __forceinline__ void st3(uint32_t* px, uint32_t base, uint32_t i, f3 v) {
+    px[base + 3 * i] = __float_as_uint(v.x);
+    px[base + 3 * i + 1] = __float_as_uint(v.y);
+    px[base + 3 * i + 2] = __float_as_uint(v.z);
+}
+
+__device__ __forceinline__ void setup(Scene& S, Frame& F) {
+    load_info(S);
+    if (!(F.ao > 0.0f)) F.ao = S.extent * 0.08f;
+    F.eps = S.extent * 1e-5f;
+}
+
+__global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
+                                               uint32_t count, unsigned long long* ray_count) {
+    setup(S, F);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t rays = 0;
+    if (k < count) {
+        const uint32_t i = first + k;
+        const uint32_t n = F.n;
+        Sums acc;
+        if (F.frame0 > 0u) {
+            ld3(px, 1 * n, i, acc.lin);
+            ld3(px, 20 * n, i, acc.grid);
+            ld3(px, 7 * n, i, acc.alb);
+            ld3(px, 10 * n, i, acc.nrm);
+            acc.cov = __uint_as_float(px[23 * n + i]);
+            acc.film = __uint_as_float(px[24 * n + i]);
+            acc.gone = __uint_as_float(px[33 * n + i]);
+            acc.dep = __uint_as_float(px[13 * n + i]);
+            acc.count = px[31 * n + i];
+        } else {
+            acc.lin = acc.grid = acc.alb = acc.nrm = mk(0.0f);
+            acc.cov = acc.film = acc.gone = acc.dep = 0.0f;
+            acc.count = 0;
+            px[29 * n + i] = 0u;
+            px[30 * n + i] = 0u;
+        }
+        acc.outline = 0;
+        for (uint32_t s = 0; s < F.spp; s++) sample(S, F, i, F.frame0 + s, sun, acc, rays);
+        st3(px, 1 * n, i, acc.lin);
+        st3(px, 20 * n, i, acc.grid);
+        st3(px, 7 * n, i, acc.alb);
+        st3(px, 10 * n, i, acc.nrm);
+        px[23 * n + i] = __float_as_uint(acc.cov);
+        px[24 * n + i] = __float_as_uint(acc.film);
+        px[33 * n + i] = __float_as_uint(acc.gone);
+        px[13 * n + i] = __float_as_uint(acc.dep);
+        px[31 * n + i] = acc.count;
+        px[25 * n + i] = acc.outline;
+        const float kk = (float)acc.count;
+        const f3 shown = view_transform_std(acc.lin / fmaxf(kk - acc.gone, 1.0f), F.exposure, F.gamma) *
+                             (1.0f - acc.cov / kk) +
+                         acc.grid / kk;
+        st3(px, 4 * n, i, shown);
+        px[i] = pack_rgba(shown, acc.film / kk);
+    }
+    const uint32_t tot = __reduce_add_sync(0xffffffffu, rays);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(ray_count, (unsigned long long)tot);
+}
+
+// Primary ray of each pixel: face id and t.
+__global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict__ ids, float* __restrict__ ts) {
+    setup(S, F);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.n) return;
+    uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
+    const CamRay cr = camera_ray(F, i, seed);
+    const Hit h = trace(S, cr.o, cr.d, INF, false);
+    ids[i] = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
+    ts[i] = h.t;
+}
+
+// One cosine-sampled ray per primary hit (the incoherent set).
+__global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict__ rays) {
+    setup(S, F);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.n) return;
+    uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
+    const CamRay cr = camera_ray(F, i, seed);
+    const Hit h = trace(S, cr.o, cr.d, INF, false);
+    if (h.tri == NONE) {
+        rays[2 * (size_t)i] = make_float4(cr.o.x, cr.o.y, cr.o.z, 0.0f);
+        rays[2 * (size_t)i + 1] = make_float4(cr.d.x, cr.d.y, cr.d.z, 0.0f);
+        return;
+    }
+    const Geo g = geo_at(S, h.tri);
+    const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+    const f3 ng = dot(ng0, cr.d) < 0.0f ? ng0 : -ng0;
+    const f3 pos = cr.o + cr.d * h.t + ng * hit_lift(F, h.t);
+    const f3 dir = cosine_dir(ng, seed);
+    rays[2 * (size_t)i] = make_float4(pos.x, pos.y, pos.z, INF);
+    rays[2 * (size_t)i + 1] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+}
+
+template <bool ANY>
+__global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict__ rays, uint32_t n,
+                                              float4* __restrict__ hits) {
+    load_info(S);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+    const Hit h = trace(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY);
+    const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
+    hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
+}
+
+}  // namespace
+}  // namespace phx
+
+using namespace phx;
+
+struct phx_tracer_s {
+    Ctx* ctx = nullptr;
+    uint32_t nverts = 0, nfaces = 0, nmats = 0, leaf = 4;
+    bool has_normals = false;
+    DevMem verts, vnorm, faces, mats, tnodes, tris, tnorm, lamp_slot, lamp_power, lamp_cdf, info, px, rays, cam;
+    BvhWork bvh;
+    uint32_t w = 0, h = 0;
+    uint32_t frame = 0, target = 1024;
+    bool have_last = false;
+    phx_camera last;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int32_t prepare(phx_tracer tr) {
+    // After a build or refit: face boxes are in tr->bvh; gather, mark leaf
+    // ends, convert nodes, root info, emitter table.
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    const uint32_t n = tr->nfaces;
+    const BvhWork& w = tr->bvh;
+    k_gather<<<(n + 255) / 256, 256, 0, s>>>((const uint32_t*)w.order.ptr, (const uint4*)tr->faces.ptr,
+                                             (const float4*)tr->verts.ptr,
+                                             tr->has_normals ? (const float4*)tr->vnorm.ptr : nullptr,
+                                             (const float4*)tr->mats.ptr, tr->nmats, n, (float4*)tr->tris.ptr,
+                                             tr->has_normals ? (float4*)tr->tnorm.ptr : nullptr, c->status);
+    k_mark_ends<<<(n + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr,
+                                                w.nstarts(), (float4*)tr->tris.ptr);
+    if (n > 1)
+        k_convert<<<(n - 1 + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, n - 1, (float4*)tr->tnodes.ptr);
+    k_root<<<1, 1, 0, s>>>((const float4*)w.nodes.ptr, n, (float4*)tr->info.ptr);
+    k_lamps<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, n,
+                               (uint32_t*)tr->lamp_slot.ptr, (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr,
+                               (float4*)tr->info.ptr);
+    return cuda_check(cudaGetLastError(), "tracer prepare");
+}
+
+// The scene record the kernels take (build-dependent fields are read from
+// the device info record inside the kernel, so no host sync is needed).
+Scene scene_of(phx_tracer tr) {
+    Scene S;
+    memset(&S, 0, sizeof S);
+    S.nodes = (const float4*)tr->tnodes.ptr;
+    S.tris = (const float4*)tr->tris.ptr;
+    S.tnorm = tr->has_normals ? (const float4*)tr->tnorm.ptr : nullptr;
+    S.mats = (const float4*)tr->mats.ptr;
+    S.lamp_slot = (const uint32_t*)tr->lamp_slot.ptr;
+    S.lamp_cdf = (const float*)tr->lamp_cdf.ptr;
+    S.info = (const float4*)tr->info.ptr;
+    return S;
+}
+
+// Refuses Camera settings the device path does not implement.
+int32_t check_camera(const phx_camera* c) {
+    if (c->envmap != 0 || c->env_cdf != 0) return fail(PHX_ERR_INVALID, "environment images are not supported");
+    if (c->aperture > 0.0f) return fail(PHX_ERR_INVALID, "depth of field (aperture > 0) is not supported");
+    if (c->grid > 0.0f) return fail(PHX_ERR_INVALID, "the grid overlay is not supported");
+    if (c->film[0] != 0 || c->film[1] != 0) return fail(PHX_ERR_INVALID, "film transparency/world is not supported");
+    if (c->adapt[3] != 0.0f) return fail(PHX_ERR_INVALID, "adaptive sampling is not supported");
+    if (c->depth[0] != 0) return fail(PHX_ERR_INVALID, "Max Bounces rows (depth) are not supported");
+    if (c->integrator[0] != 0.0f) return fail(PHX_ERR_INVALID, "pixel filters other than phiray's own are not supported");
+    if (c->view[0] != 0.0f) return fail(PHX_ERR_INVALID, "only the Standard view transform is supported");
+    if (c->tile[2] != 0 || c->tile[3] != 0) return fail(PHX_ERR_INVALID, "tiles are not supported");
+    if (c->count > PHX_MAX_LIGHT) return fail(PHX_ERR_INVALID, "count %u > 64 lights", c->count);
+    if (!(c->scale != 0.0f) || !(c->units != 0.0f) || !(c->aspect != 0.0f))
+        return fail(PHX_ERR_INVALID, "scale, units and aspect must be non-zero");
+    return PHX_OK;
+}
+
+Frame frame_of(const phx_camera* c, uint32_t w, uint32_t h, const phx_light* dev_lights) {
+    Frame F;
+    F.w = w;
+    F.h = h;
+    F.n = w * h;
+    F.frame0 = 0;
+    F.spp = 1;
+    F.persp = c->persp;
+    F.count = c->count;
+    F.bounces = c->bounces;
+    F.right = mk(c->right[0], c->right[1], c->right[2]);
+    F.up = mk(c->up[0], c->up[1], c->up[2]);
+    F.back = mk(c->back[0], c->back[1], c->back[2]);
+    F.pivot = mk(c->pivot[0], c->pivot[1], c->pivot[2]);
+    F.env = mk(c->env[0], c->env[1], c->env[2]);
+    F.scale = c->scale;
+    F.units = c->units;
+    F.aspect = c->aspect;
+    F.dist = c->dist;
+    F.pan_x = c->pan[0];
+    F.pan_y = c->pan[1];
+    F.ao = c->ao;  // the kernel fills ao (when 0) and eps from the extent
+    F.eps = 0.0f;
+    for (int k = 0; k < 4; k++) F.sky[k] = c->sky[k];
+    F.limit_d = c->limit[0];
+    F.limit_i = c->limit[1];
+    F.exposure = c->view[1];
+    F.gamma = c->view[2];
+    F.lights = dev_lights;
+    return F;
+}
+
+int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
+    if (w == 0 || h == 0) return fail(PHX_ERR_INVALID, "image %ux%u", w, h);
+    const uint64_t n = (uint64_t)w * h;
+    if (n * PHX_PX_LEN + 1 > 0xFFFFFFFFull) return fail(PHX_ERR_INVALID, "image %ux%u is too large", w, h);
+    if (tr->w == w && tr->h == h && tr->px.ptr) return PHX_OK;
+    PHX_TRY(wait_stream(tr->ctx->stream, 0));
+    tr->px.release();
+    PHX_TRY(tr->px.reserve((n * PHX_PX_LEN + 1) * 4));
+    PHX_CUDA(cudaMemsetAsync(tr->px.ptr, 0, (n * PHX_PX_LEN + 1) * 4, tr->ctx->stream));
+    tr->w = w;
+    tr->h = h;
+    tr->have_last = false;
+    return PHX_OK;
+}
+
+int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp,
+                      uint32_t first_px, uint32_t count_px) {
+    Ctx* c = tr->ctx;
+    const Scene S = scene_of(tr);
+    PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, cam, sizeof(phx_camera), cudaMemcpyHostToDevice, c->stream));
+    Frame F = frame_of(cam, w, h, ((const phx_camera*)tr->cam.ptr)->lights);
+    F.frame0 = first_frame;
+    F.spp = spp;
+    const f3 sun = mk(cam->sun[0], cam->sun[1], cam->sun[2]);
+    k_render<<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px, count_px,
+                                                            (unsigned long long*)tr->rays.ptr);
+    return cuda_check(cudaGetLastError(), "render");
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
+    if (!ctx || !sc || !out) return fail(PHX_ERR_INVALID, "null argument");
+    if (sc->nfaces == 0) return fail(PHX_ERR_INVALID, "a tracer needs at least one face (Tracer::new declines an empty scene)");
+    if (!sc->verts || !sc->faces || !sc->mats || sc->nmats == 0 || sc->nverts == 0)
+        return fail(PHX_ERR_INVALID, "scene arrays missing");
+    if (sc->nfaces >= (1u << 30)) return fail(PHX_ERR_INVALID, "too many faces");
+    // Faces index vertices and materials: check on the host once.
+    for (uint32_t f = 0; f < sc->nfaces; f++) {
+        const uint32_t* q = sc->faces + 4 * (size_t)f;
+        if (q[0] >= sc->nverts || q[1] >= sc->nverts || q[2] >= sc->nverts || q[3] >= sc->nmats)
+            return fail(PHX_ERR_INVALID, "face %u names a vertex or material out of range", f);
+    }
+    for (uint32_t m = 0; m < sc->nmats; m++) {
+        const uint32_t* q = (const uint32_t*)(sc->mats + 32 * (size_t)m);
+        // tex, nmap, maps (Mat words 12..16) must be NO_TEX; second (30) NO_MAT.
+        for (int k = 12; k <= 16; k++)
+            if (q[k] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u uses a texture (not supported)", m);
+        if (q[30] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u has a second lobe (not supported)", m);
+    }
+    PHX_TRY(use(&ctx->c));
+    auto* tr = new phx_tracer_s();
+    tr->ctx = &ctx->c;
+    tr->nverts = sc->nverts;
+    tr->nfaces = sc->nfaces;
+    tr->nmats = sc->nmats;
+    tr->leaf = sc->leaf ? sc->leaf : 4;
+    tr->has_normals = sc->normals != nullptr;
+    ctx->c.live++;
+    cudaStream_t s = ctx->c.stream;
+    const size_t n = sc->nfaces;
+    int32_t rc = PHX_OK;
+    auto step = [&](int32_t r) {
+        if (rc == PHX_OK) rc = r;
+    };
+    step(tr->verts.reserve((size_t)sc->nverts * 16));
+    if (tr->has_normals) step(tr->vnorm.reserve((size_t)sc->nverts * 16));
+    step(tr->faces.reserve(n * 16));
+    step(tr->mats.reserve((size_t)sc->nmats * 128));
+    step(tr->tnodes.reserve((n > 1 ? n - 1 : 1) * 64));
+    step(tr->tris.reserve(n * 48));
+    if (tr->has_normals) step(tr->tnorm.reserve(n * 48));
+    step(tr->lamp_slot.reserve(n * 4));
+    step(tr->lamp_power.reserve(n * 4));
+    step(tr->lamp_cdf.reserve(n * 4));
+    step(tr->info.reserve(64));
+    step(tr->rays.reserve(8));
+    step(tr->cam.reserve(sizeof(phx_camera)));
+    step(tr->bvh.reserve(sc->nfaces, ctx->c.sms));
+    if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev0), "event");
+    if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev1), "event");
+    if (rc == PHX_OK)
+        rc = cuda_check(cudaMemcpyAsync(tr->verts.ptr, sc->verts, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK && tr->has_normals)
+        rc = cuda_check(cudaMemcpyAsync(tr->vnorm.ptr, sc->normals, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK) rc = cuda_check(cudaMemcpyAsync(tr->faces.ptr, sc->faces, n * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK)
+        rc = cuda_check(cudaMemcpyAsync(tr->mats.ptr, sc->mats, (size_t)sc->nmats * 128, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK) rc = cuda_check(cudaMemsetAsync(tr->rays.ptr, 0, 8, s), "zero");
+    if (rc == PHX_OK)
+        rc = launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, sc->nfaces,
+                               (phx_aabb*)tr->bvh.prims.ptr);
+    if (rc == PHX_OK) rc = enqueue_build(&ctx->c, tr->bvh, sc->nfaces, tr->leaf);
+    if (rc == PHX_OK) rc = prepare(tr);
+    if (rc == PHX_OK) rc = wait_stream(s, 0);
+    if (rc == PHX_OK) rc = read_status(&ctx->c);
+    if (rc != PHX_OK) {
+        phx_tracer_destroy(tr);
+        return rc;
+    }
+    *out = tr;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_destroy(phx_tracer tr) {
+    if (!tr) return PHX_OK;
+    use(tr->ctx);
+    cudaStreamSynchronize(tr->ctx->stream);
+    if (tr->ev0) cudaEventDestroy(tr->ev0);
+    if (tr->ev1) cudaEventDestroy(tr->ev1);
+    tr->ctx->live--;
+    delete tr;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    tr->target = samples ? samples : 1;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first, uint32_t spp) {
+    if (!tr || !cam) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    PHX_TRY(ensure_image(tr, w, h));
+    if (spp == 0) return PHX_OK;
+    Ctx* c = tr->ctx;
+    PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 8, c->stream));
+    PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));
+    PHX_TRY(launch_render(tr, cam, w, h, first, spp, 0, w * h));
+    PHX_CUDA(cudaEventRecord(tr->ev1, c->stream));
+    tr->frame = first + spp - 1;
+    tr->last = *cam;
+    tr->have_last = true;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t slices,
+                          const volatile int32_t* cancel, uint32_t* frame, int32_t* done) {
+    if (!tr || !cam) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    w = w ? w : 1;
+    h = h ? h : 1;
+    PHX_TRY(ensure_image(tr, w, h));
+    const uint32_t n = w * h;
+    slices = slices < 1 ? 1 : (slices > n ? n : slices);
+    // sample.rs:126-134: the same view (everything past n, groups_x) is the
+    // next frame; another view starts over.
+    const bool same = tr->have_last && memcmp((const char*)&tr->last + 8, (const char*)cam + 8, sizeof(phx_camera) - 8) == 0;
+    if (same && tr->frame + 1 >= tr->target) {
+        if (frame) *frame = tr->frame;
+        if (done) *done = 1;
+        return PHX_OK;
+    }
+    const uint32_t f = same ? tr->frame + 1 : 0;
+    Ctx* c = tr->ctx;
+    PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 8, c->stream));
+    PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));
+    for (uint32_t k = 0; k < slices; k++) {
+        const uint32_t a = (uint32_t)((uint64_t)n * k / slices), b = (uint32_t)((uint64_t)n * (k + 1) / slices);
+        PHX_TRY(launch_render(tr, cam, w, h, f, 1, a, b - a));
+        if (slices > 1) {
+            PHX_TRY(wait_stream(c->stream, 0));
+            if (cancel && *cancel) {
+                tr->have_last = false;  // a half-sampled frame is no frame
+                return fail(PHX_ERR_CANCELLED, "sample cancelled after slice %u of %u", k + 1, slices);
+            }
+        }
+    }
+    PHX_CUDA(cudaEventRecord(tr->ev1, c->stream));
+    tr->frame = f;
+    tr->last = *cam;
+    tr->have_last = true;
+    if (frame) *frame = f;
+    if (done) *done = (f + 1 >= tr->target) ? 1 : 0;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_read(phx_tracer tr, uint64_t offset, uint32_t* dst, uint64_t count, uint32_t timeout_ms) {
+    if (!tr || (!dst && count)) return fail(PHX_ERR_INVALID, "null argument");
+    const uint64_t words = (uint64_t)tr->w * tr->h * PHX_PX_LEN + 1;
+    if (!tr->px.ptr || offset + count > words) return fail(PHX_ERR_INVALID, "read past the image");
+    PHX_TRY(use(tr->ctx));
+    PHX_CUDA(cudaMemcpyAsync(dst, (const uint32_t*)tr->px.ptr + offset, count * 4, cudaMemcpyDeviceToHost, tr->ctx->stream));
+    PHX_TRY(wait_stream(tr->ctx->stream, timeout_ms));
+    return read_status(tr->ctx);
+}
+
+int32_t phx_tracer_image(phx_tracer tr, uint32_t** px, uint64_t* words) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (px) *px = (uint32_t*)tr->px.ptr;
+    if (words) *words = tr->px.ptr ? (uint64_t)tr->w * tr->h * PHX_PX_LEN + 1 : 0;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_denoise(phx_tracer tr, int32_t keep) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (!tr->px.ptr || !tr->have_last) return PHX_OK;  // nothing traced: read.rs:90
+    PHX_TRY(use(tr->ctx));
+    const float strength[4] = {64.0f, 8.0f, 40.0f, 7.0f};
+    return phx_denoise((phx_ctx)((char*)tr->ctx - offsetof(phx_ctx_s, c)), (uint32_t*)tr->px.ptr, tr->w, tr->h,
+                       strength, tr->last.view, keep);
+}
+
+int32_t phx_tracer_time(phx_tracer tr, float* gpu_ms, uint64_t* rays) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    PHX_TRY(use(tr->ctx));
+    PHX_TRY(wait_stream(tr->ctx->stream, 0));
+    if (gpu_ms) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, tr->ev0, tr->ev1) != cudaSuccess) {
+            cudaGetLastError();
+            ms = 0.0f;
+        }
+        *gpu_ms = ms;
+    }
+    if (rays) PHX_CUDA(cudaMemcpy(rays, tr->rays.ptr, 8, cudaMemcpyDeviceToHost));
+    return read_status(tr->ctx);
+}
+
+int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebuild) {
+    if (!tr || !verts) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(use(tr->ctx));
+    cudaStream_t s = tr->ctx->stream;
+    if ((const void*)verts != tr->verts.ptr)
+        PHX_CUDA(cudaMemcpyAsync(tr->verts.ptr, verts, (size_t)tr->nverts * 16, cudaMemcpyDeviceToDevice, s));
+    PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                              (phx_aabb*)tr->bvh.prims.ptr));
+    if (rebuild) PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf));
+    else PHX_TRY(enqueue_refit(tr->ctx, tr->bvh, tr->nfaces, false));
+    PHX_TRY(prepare(tr));
+    tr->have_last = false;  // a new pose starts the image over
+    return PHX_OK;
+}
+
+int32_t phx_tracer_primary(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame, uint32_t* ids,
+                           float* ts) {
+    if (!tr || !cam || !ids || !ts) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    const Scene S = scene_of(tr);
+    const Frame F = frame_of(cam, w, h, nullptr);
+    k_primary<<<(w * h + 127) / 128, 128, 0, tr->ctx->stream>>>(S, F, frame, ids, ts);
+    return cuda_check(cudaGetLastError(), "primary");
+}
+
+int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame,
+                                  float* rays) {
+    if (!tr || !cam || !rays) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    const Scene S = scene_of(tr);
+    const Frame F = frame_of(cam, w, h, nullptr);
+    k_secondary<<<(w * h + 127) / 128, 128, 0, tr->ctx->stream>>>(S, F, frame, (float4*)rays);
+    return cuda_check(cudaGetLastError(), "secondary rays");
+}
+
+int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit) {
+    if (!tr || (n && (!rays || !hits))) return fail(PHX_ERR_INVALID, "null argument");
+    if (n == 0) return PHX_OK;
+    PHX_TRY(use(tr->ctx));
+    const Scene S = scene_of(tr);
+    if (any_hit)
+        k_rays<true><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits);
+    else
+        k_rays<false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits);
+    return cuda_check(cudaGetLastError(), "trace rays");
+}
+
+}  // extern "C"

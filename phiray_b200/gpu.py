@@ -11,6 +11,7 @@ graph launch).
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -45,6 +46,11 @@ class Gpu:
         N.check(N.lib().phx_ctx_create(ordinal, C.byref(h)))
         self.handle = h
         self.ordinal = ordinal
+        self._children = weakref.WeakSet()
+
+    def adopt(self, obj) -> None:
+        """Track an object made on this context; close() releases it first."""
+        self._children.add(obj)
 
     @staticmethod
     def count() -> int:
@@ -63,6 +69,8 @@ class Gpu:
 
     def close(self) -> None:
         if self.handle:
+            for child in list(self._children):
+                child.close()
             N.lib().phx_ctx_destroy(self.handle)
             self.handle = None
 
@@ -84,6 +92,7 @@ class GpuArray:
             N.check(N.lib().phx_buf_wrap(gpu.handle, _wrap, int(nbytes), C.byref(h)))
         self.gpu = gpu
         self.handle = h
+        gpu.adopt(self)
 
     @classmethod
     def zeroed(cls, gpu: Gpu, nbytes: int) -> "GpuArray":
@@ -132,6 +141,8 @@ class GpuArray:
         if self.handle:
             N.lib().phx_buf_free(self.handle)
             self.handle = None
+
+    close = free
 
     def __del__(self):
         try:
@@ -193,6 +204,7 @@ class Pass:
         self.gpu = gpu
         self.handle = h
         self._keep: list = []
+        gpu.adopt(self)
 
     def add(self, kernel: Kernel, n: int, params: np.ndarray, buffers: list[GpuArray]) -> int:
         return self.add_over(kernel, n, n, params, buffers)

@@ -8,9 +8,12 @@ Scene arrays (the layout the tracer reads, phiray's scene contract in
 src/trace/scene.rs and layout.wgsl):
   verts  (V, 4) float32   position xyz, w = 1
   faces  (F, 4) uint32    v0, v1, v2, material id
-  mats   (M, 16) float32  Mat (src/trace/mat.rs) reduced to the inputs the
-                          Rendered path reads: color rgba, rough, metal,
-                          trans, ior, emit rgb, 0, 0, 0, 0, 0
+  mats   (M, 32) float32  trace::Mat's first 32 words (src/trace/mat.rs:9-40):
+                          color rgba, rough, metal, trans, ior, emit rgb,
+                          bump, tex, nmap, maps[3], sss, sss_radius[3],
+                          sheen, sheen_rough, sheen_tint[3], coat,
+                          coat_rough, aniso, aniso_rot, second, mix (the
+                          procedural slots after them are not used)
   lights (L, 20) float32  camera.wgsl `Light` records (80 bytes each)
 """
 
@@ -22,16 +25,26 @@ from dataclasses import dataclass, field
 import numpy as np
 
 SEED = 0x2545F491
-MAT_WORDS = 16
+MAT_WORDS = 32
+NO_TEX = 0xFFFFFFFF
 LIGHT_WORDS = 20
 
 
 def mat(color, rough=0.5, metal=0.0, trans=0.0, ior=1.5, emit=(0.0, 0.0, 0.0)) -> np.ndarray:
-    """One material row; defaults are Tri::new's (src/trace/kernel.rs)."""
+    """One material row; defaults are Tri::new's (src/trace/kernel.rs:55-57):
+    no textures, sss radius (0.05, 0.01, 0.005), sheen rough 0.5 and tint 1,
+    coat rough 0.03, no second lobe."""
     m = np.zeros(MAT_WORDS, dtype=np.float32)
+    w = m.view(np.uint32)
     m[0:4] = color
     m[4], m[5], m[6], m[7] = rough, metal, trans, ior
     m[8:11] = emit
+    w[12:17] = NO_TEX
+    m[18:21] = (0.05, 0.01, 0.005)
+    m[22] = 0.5
+    m[23:26] = 1.0
+    m[27] = 0.03
+    w[30] = NO_TEX
     return m
 
 
@@ -180,3 +193,98 @@ def c1_plain(ntris: int = 65536, width: int = 256, height: int = 256, spp: int =
     verts, faces = _assemble([(tri_v, tri_f), g, lq])
     view = View.look((0.5, 0.5, -1.5), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 45.0)
     return Scene("c1_plain", verts, faces, np.stack(mats), np.stack([light_off()]), view, width, height, spp, bounces)
+
+
+def _icosphere(levels: int):
+    """Unit icosphere: 20 * 4**levels faces, shared vertices."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array(
+        [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+         [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array(
+        [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2], [10, 7, 6],
+         [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+         [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    for _ in range(levels):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        uniq, inv = np.unique(e, axis=0, return_inverse=True)
+        mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(v)
+        v = np.concatenate([v, mid])
+        nf = len(f)
+        m01, m12, m20 = (inv[0:nf] + base, inv[nf:2 * nf] + base, inv[2 * nf:] + base)
+        a, b, c = f[:, 0], f[:, 1], f[:, 2]
+        f = np.concatenate([np.stack([a, m01, m20], 1), np.stack([b, m12, m01], 1), np.stack([c, m20, m12], 1),
+                            np.stack([m01, m12, m20], 1)])
+    return v, f
+
+
+def value_noise(p: np.ndarray, seed: int, octaves: int = 4) -> np.ndarray:
+    """Seeded 3D value noise (hashed lattice values, smoothstep-trilinear),
+    `octaves` octaves of doubling frequency and halving amplitude, in [-1, 1]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    table = rng.uniform(-1.0, 1.0, 1 << 16)
+    perm = rng.permutation(1 << 16)
+
+    def lattice(ix, iy, iz):
+        h = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791)
+        return table[perm[h & 0xFFFF]]
+
+    out = np.zeros(len(p))
+    amp, freq, norm = 1.0, 4.0, 0.0
+    for _ in range(octaves):
+        q = p * freq
+        i = np.floor(q).astype(np.int64)
+        fr = q - i
+        s = fr * fr * (3.0 - 2.0 * fr)
+        acc = np.zeros(len(p))
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    w = ((s[:, 0] if dx else 1 - s[:, 0]) * (s[:, 1] if dy else 1 - s[:, 1]) *
+                         (s[:, 2] if dz else 1 - s[:, 2]))
+                    acc += w * lattice(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)
+        out += amp * acc
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return out / norm
+
+
+def c2_mesh(levels: int = 8, width: int = 1920, height: int = 1080, spp: int = 64, bounces: int = 8,
+            env: float = 0.05) -> Scene:
+    """Config 2: an icosphere subdivided `levels` times (8: 1,310,720 faces),
+    radius 0.5 at the origin, displaced radially by seeded 4-octave value
+    noise of amplitude 0.05; a 2-face ground plane at y = -0.6; four 0.4 x
+    0.4 area lights (kind 3) above, facing down; albedo U(0.1, 0.9) per face,
+    30% of faces mirrors. The world is a dim uniform grey (`env`), so the
+    diffuse path runs its full `bounces` (with a black world and no emissive
+    faces the reference's `indirect` returns nothing, integrate.wgsl:111-121)."""
+    rng = np.random.Generator(np.random.PCG64(SEED + 1))
+    v, f = _icosphere(levels)
+    r = 0.5 * (1.0 + 0.05 * value_noise(v, SEED + 1))
+    pos = (v * r[:, None]).astype(np.float32)
+    nf = len(f)
+    tri_f = np.zeros((nf, 4), np.uint32)
+    tri_f[:, :3] = f
+    tri_f[:, 3] = np.arange(nf)
+    albedo = rng.uniform(0.1, 0.9, (nf, 3)).astype(np.float32)
+    is_mirror = rng.random(nf) < 0.3
+    mats = np.zeros((nf + 1, MAT_WORDS), np.float32)
+    lam = mat([0.5, 0.5, 0.5, 1.0], rough=1.0)
+    mir = mat([0.5, 0.5, 0.5, 1.0], rough=0.02, metal=1.0)
+    mats[:nf] = np.where(is_mirror[:, None], mir, lam)
+    mats[:nf, 0:3] = albedo
+    mats[nf] = lambert((0.6, 0.6, 0.6))
+    g = _quad((-3.0, -0.6, -3.0), (-3.0, -0.6, 3.0), (3.0, -0.6, 3.0), (3.0, -0.6, -3.0), nf)
+    verts, faces = _assemble([(pos, tri_f), g])
+    lights = [
+        light_area((x, 1.5, z), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.4, 0.4, (p, p, p))
+        for (x, z, p) in [(-0.8, -0.8, 30.0), (0.8, -0.8, 20.0), (-0.8, 0.8, 20.0), (0.8, 0.8, 15.0)]
+    ]
+    view = View.look((0.0, 0.3, -2.2), (0.0, -0.1, 1.0), (0.0, 1.0, 0.0), 40.0)
+    return Scene("c2_mesh", verts, faces, mats, np.stack(lights), view, width, height, spp, bounces,
+                 env=(env, env, env), meta={"levels": levels})

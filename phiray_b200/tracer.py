@@ -1,0 +1,198 @@
+"""``Tracer`` and ``Camera``: phiray's Rendered-mode tracer over the C ABI.
+
+Reference: src/trace/mod.rs (Tracer), build.rs (Tracer::new), sample.rs
+(sample, sample_in, time), read.rs (readbacks, denoise), pose.rs (repose),
+camera.rs (Camera). ``Camera`` is the reference's uniform byte for byte
+(5,776 bytes) as a numpy record, so the same bytes a Rust caller holds go
+through the ABI unchanged.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .gpu import Gpu, devptr
+
+PX_LEN = 34
+
+LIGHT = np.dtype(
+    [
+        ("pos", "<f4", 3),
+        ("kind", "<u4"),
+        ("color", "<f4", 3),
+        ("size", "<f4"),
+        ("dir", "<f4", 3),
+        ("cone", "<f4"),
+        ("right", "<f4", 3),
+        ("size_y", "<f4"),
+        ("shape", "<u4"),
+        ("blend", "<f4"),
+        ("spot_scale", "<f4", 2),
+    ]
+)
+
+CAMERA = np.dtype(
+    [
+        ("n", "<u4"), ("groups_x", "<u4"), ("w", "<u4"), ("h", "<u4"),
+        ("right", "<f4", 3), ("persp", "<u4"),
+        ("up", "<f4", 3), ("scale", "<f4"),
+        ("back", "<f4", 3), ("units", "<f4"),
+        ("pivot", "<f4", 3), ("aspect", "<f4"),
+        ("sun", "<f4", 3), ("dist", "<f4"),
+        ("sky", "<f4", 4),
+        ("pan", "<f4", 2), ("ao", "<f4"), ("eps", "<f4"),
+        ("frame", "<u4"), ("grid", "<f4"), ("count", "<u4"), ("glow", "<u4"),
+        ("grid_color", "<f4", 4), ("env", "<f4", 4), ("split", "<u4", 4), ("view", "<f4", 4),
+        ("envmap", "<u4"), ("env_rot", "<f4"), ("bounces", "<u4"), ("env_cdf", "<u4"),
+        ("aperture", "<f4"), ("focus", "<f4"), ("blades", "<u4"), ("blade_spin", "<f4"),
+        ("aperture_ratio", "<f4"), ("env_hidden", "<u4"), ("see_through", "<f4"), ("grid_hide", "<u4"),
+        ("tile", "<u4", 4), ("film", "<u4", 4), ("preview", "<u4", 4), ("slice", "<u4", 4),
+        ("insts", "<u4", 4), ("vis", "<u4", 4), ("taa", "<f4", 4), ("fx", "<f4", 4), ("outline", "<f4", 4),
+        ("shade", "<u4", 4), ("single", "<f4", 4), ("cavity", "<f4", 4), ("ssao", "<u4", 4),
+        ("shadow", "<f4", 4), ("shadow_fade", "<f4", 4), ("matcap", "<u4", 4), ("dof", "<f4", 4),
+        ("outline_fx", "<f4", 4), ("outline_pick", "<f4", 4), ("outline_active", "<f4", 4),
+        ("outline_move", "<f4", 4), ("adapt", "<f4", 4), ("limit", "<f4", 4), ("depth", "<u4", 4),
+        ("integrator", "<f4", 4),
+        ("lights", LIGHT, 64),
+    ]
+)
+assert CAMERA.itemsize == 5776
+
+
+def camera(scene) -> np.ndarray:
+    """A Camera record for a `scenes.Scene`: its view, lights, world colour,
+    diffuse bounces; Standard view transform, pinhole, no clamp."""
+    c = np.zeros(1, dtype=CAMERA)
+    v = scene.view
+    c["right"], c["up"], c["back"], c["pivot"] = v.right, v.up, v.back, v.pivot
+    c["persp"] = 1
+    c["dist"], c["scale"], c["units"] = v.dist, v.scale, v.units
+    c["aspect"] = scene.width / scene.height
+    c["env"][0, :3] = scene.env
+    c["view"] = (0.0, 0.0, 1.0, 0.0)
+    c["bounces"] = scene.bounces
+    c["sun"] = (0.0, 1.0, 0.0)
+    L = len(scene.lights)
+    c["count"] = L
+    raw = c["lights"].view(np.float32).reshape(1, 64, 20)
+    raw[0, :L] = scene.lights
+    return c
+
+
+class _Scene(C.Structure):
+    _fields_ = [
+        ("verts", C.c_void_p),
+        ("normals", C.c_void_p),
+        ("faces", C.c_void_p),
+        ("mats", C.c_void_p),
+        ("nverts", C.c_uint32),
+        ("nfaces", C.c_uint32),
+        ("nmats", C.c_uint32),
+        ("leaf", C.c_uint32),
+    ]
+
+
+class Tracer:
+    """The Rendered-mode path tracer (phiray ``Tracer``)."""
+
+    def __init__(self, gpu: Gpu, verts: np.ndarray, faces: np.ndarray, mats: np.ndarray, normals=None, leaf: int = 4):
+        self.gpu = gpu
+        self._host = [
+            np.ascontiguousarray(verts, dtype=np.float32),
+            np.ascontiguousarray(faces, dtype=np.uint32),
+            np.ascontiguousarray(mats, dtype=np.float32),
+            None if normals is None else np.ascontiguousarray(normals, dtype=np.float32),
+        ]
+        v, f, m, nrm = self._host
+        sc = _Scene(
+            v.ctypes.data, nrm.ctypes.data if nrm is not None else None, f.ctypes.data, m.ctypes.data,
+            len(v), len(f), len(m), leaf,
+        )
+        h = C.c_void_p()
+        N.check(N.lib().phx_tracer_create(gpu.handle, C.byref(sc), C.byref(h)))
+        self.handle = h
+        self.w = self.h = 0
+        gpu.adopt(self)
+
+    @classmethod
+    def of(cls, gpu: Gpu, scene, **kw) -> "Tracer":
+        return cls(gpu, scene.verts, scene.faces, scene.mats, **kw)
+
+    def set_samples(self, n: int) -> None:
+        N.check(N.lib().phx_tracer_set_samples(self.handle, n))
+
+    def sample(self, cam: np.ndarray, w: int, h: int, slices: int = 1, cancel=None) -> tuple[int, bool]:
+        """``Tracer::sample`` / ``sample_in``: (frame, done)."""
+        frame, done = C.c_uint32(), C.c_int32()
+        N.check(N.lib().phx_tracer_sample(self.handle, cam.ctypes.data, w, h, slices, cancel, C.byref(frame), C.byref(done)))
+        self.w, self.h = w, h
+        return frame.value, bool(done.value)
+
+    def trace(self, cam: np.ndarray, w: int, h: int, first: int, spp: int) -> None:
+        """Frames [first, first + spp) in one launch (stream-ordered)."""
+        N.check(N.lib().phx_tracer_trace(self.handle, cam.ctypes.data, w, h, first, spp))
+        self.w, self.h = w, h
+
+    def read(self, offset: int, count: int, timeout_ms: int = 0) -> np.ndarray:
+        out = np.empty(count, dtype=np.uint32)
+        N.check(N.lib().phx_tracer_read(self.handle, offset, out.ctypes.data, count, timeout_ms))
+        return out
+
+    def image(self) -> np.ndarray:
+        """The whole px buffer (34 w h + 1 words)."""
+        return self.read(0, PX_LEN * self.w * self.h + 1)
+
+    def pixels(self) -> np.ndarray:
+        """``Tracer::pixels``: packed RGBA8 (n,) uint32."""
+        return self.read(0, self.w * self.h)
+
+    def radiance(self) -> np.ndarray:
+        """``Tracer::radiance``: linear mean per pixel (h, w, 3) over the
+        samples that met something (read.rs:241-251)."""
+        n = self.w * self.h
+        px = self.read(0, PX_LEN * n + 1)
+        f = px.view(np.float32)
+        k = px[31 * n: 32 * n].astype(np.float32)
+        gone = f[33 * n: 34 * n]
+        lin = f[n: 4 * n].reshape(n, 3)
+        return (lin / np.maximum(k - gone, 1.0)[:, None]).reshape(self.h, self.w, 3)
+
+    def device_image(self) -> tuple[int, int]:
+        p, words = C.c_void_p(), C.c_uint64()
+        N.check(N.lib().phx_tracer_image(self.handle, C.byref(p), C.byref(words)))
+        return p.value or 0, words.value
+
+    def denoise(self, keep: bool = False) -> None:
+        N.check(N.lib().phx_tracer_denoise(self.handle, 1 if keep else 0))
+
+    def time(self) -> tuple[float, int]:
+        """``Tracer::time``: (GPU ms of the last call, rays traced)."""
+        ms, rays = C.c_float(), C.c_uint64()
+        N.check(N.lib().phx_tracer_time(self.handle, C.byref(ms), C.byref(rays)))
+        return ms.value, rays.value
+
+    def repose_device(self, verts, rebuild: bool = False) -> None:
+        N.check(N.lib().phx_tracer_repose_device(self.handle, devptr(verts), 1 if rebuild else 0))
+
+    def primary(self, cam: np.ndarray, w: int, h: int, frame: int, ids, ts) -> None:
+        N.check(N.lib().phx_tracer_primary(self.handle, cam.ctypes.data, w, h, frame, devptr(ids), devptr(ts)))
+
+    def secondary_rays(self, cam: np.ndarray, w: int, h: int, frame: int, rays) -> None:
+        N.check(N.lib().phx_tracer_secondary_rays(self.handle, cam.ctypes.data, w, h, frame, devptr(rays)))
+
+    def trace_rays(self, rays, n: int, hits, any_hit: bool = False) -> None:
+        N.check(N.lib().phx_trace_rays(self.handle, devptr(rays), n, devptr(hits), 1 if any_hit else 0))
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().phx_tracer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

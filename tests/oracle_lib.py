@@ -34,6 +34,9 @@ SIGS = {
     "orc_reachable": (u32, [vp, u32, vp]),
     "orc_skin": (None, [vp, vp, vp, vp, f32, u32, vp]),
     "orc_denoise": (None, [vp, u32, u32, C.POINTER(f32), C.POINTER(f32), C.c_int]),
+    "orc_trace": (None, [vp, vp, u32, vp, vp, u32, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
+    "orc_primary": (None, [vp, vp, u32, vp, u32, vp, u32, vp, vp]),
+    "orc_trace_rays": (None, [vp, vp, u32, vp, u32, vp, u32, vp, C.c_int]),
 }
 
 
@@ -140,6 +143,48 @@ class Oracle:
         v = (f32 * 4)(*view)
         self.lib.orc_denoise(px.ctypes.data, w, h, s, v, 1 if keep else 0)
         return px
+
+
+def _scene_args(scene):
+    v = np.ascontiguousarray(scene.verts, dtype=np.float32)
+    f = np.ascontiguousarray(scene.faces, dtype=np.uint32)
+    m = np.ascontiguousarray(scene.mats, dtype=np.float32)
+    return v, f, m
+
+
+class TraceOracle:
+    """The tracer restatement (oracle/trace.cpp) for a `scenes.Scene`."""
+
+    def __init__(self, orc: "Oracle", scene, leaf: int = 4):
+        self.lib = orc.lib
+        self.v, self.f, self.m = _scene_args(scene)
+        self.leaf = leaf
+
+    def trace(self, cam, first: int, spp: int, px=None, rows=None):
+        w, h = int(cam["w"][0]), int(cam["h"][0])
+        if px is None:
+            px = np.zeros(34 * w * h + 1, dtype=np.uint32)
+        rays = u64()
+        r0, nr = (0, 0) if rows is None else rows
+        self.lib.orc_trace(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, None, self.leaf,
+                           cam.ctypes.data, first, spp, px.ctypes.data, C.byref(rays), r0, nr)
+        return px, rays.value
+
+    def primary(self, cam, frame: int):
+        n = int(cam["w"][0]) * int(cam["h"][0])
+        ids = np.zeros(n, np.uint32)
+        ts = np.zeros(n, np.float32)
+        self.lib.orc_primary(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, self.leaf,
+                             cam.ctypes.data, frame, ids.ctypes.data, ts.ctypes.data)
+        return ids, ts
+
+    def trace_rays(self, rays, any_hit=False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        n = len(rays)
+        hits = np.zeros((n, 4), np.float32)
+        self.lib.orc_trace_rays(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, self.leaf,
+                                rays.ctypes.data, n, hits.ctypes.data, 1 if any_hit else 0)
+        return hits
 
 
 def build() -> Path:
