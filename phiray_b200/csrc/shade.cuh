@@ -46,6 +46,7 @@ struct Scene {
     const uint32_t* __restrict__ lamp_slot;
     const float* __restrict__ lamp_cdf;
     const float4* __restrict__ info;   // root box + ref, extent, emitter count (device results of the build)
+    uint32_t nslots;  // triangles: a leaf walk never reads past them
     uint32_t lamp_count;
     uint32_t root;  // inner node 0, or LEAF | 0 when the root is a leaf
     f3 root_lo, root_hi;
@@ -188,7 +189,7 @@ __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool f
     uint32_t nd = S.root;
     for (;;) {
         if (nd & LEAF) {
-            for (uint32_t id = nd & ~LEAF;; id++) {
+            for (uint32_t id = nd & ~LEAF; id < S.nslots; id++) {
                 const float4 A = __ldg(S.tris + 3 * (size_t)id);
                 const float4 B = __ldg(S.tris + 3 * (size_t)id + 1);
                 const float4 Cc = __ldg(S.tris + 3 * (size_t)id + 2);
@@ -214,14 +215,10 @@ __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool f
             const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
             const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
             if (tl < INF && tr < INF) {
-                if (tl <= tr) {
-                    stack[sp] = r;
-                    nd = l;
-                } else {
-                    stack[sp] = l;
-                    nd = r;
-                }
-                sp++;
+                // Depth <= 31 keeps sp below STACK; the check only guards a
+                // corrupt tree from writing past the stack.
+                if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
+                nd = tl <= tr ? l : r;
                 continue;
             }
             if (tl < INF) {

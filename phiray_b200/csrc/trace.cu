@@ -635,6 +635,7 @@ Scene scene_of(phx_tracer tr) {
     S.lamp_slot = (const uint32_t*)tr->lamp_slot.ptr;
     S.lamp_cdf = (const float*)tr->lamp_cdf.ptr;
     S.info = (const float4*)tr->info.ptr;
+    S.nslots = tr->nfaces;
     return S;
 }
 
@@ -929,6 +930,7 @@ int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebu
 int32_t phx_tracer_primary(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame, uint32_t* ids,
                            float* ts) {
     if (!tr || !cam || !ids || !ts) return fail(PHX_ERR_INVALID, "null argument");
+    if (w == 0 || h == 0) return fail(PHX_ERR_INVALID, "image %ux%u", w, h);
     PHX_TRY(check_camera(cam));
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
@@ -940,6 +942,7 @@ int32_t phx_tracer_primary(phx_tracer tr, const phx_camera* cam, uint32_t w, uin
 int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame,
                                   float* rays) {
     if (!tr || !cam || !rays) return fail(PHX_ERR_INVALID, "null argument");
+    if (w == 0 || h == 0) return fail(PHX_ERR_INVALID, "image %ux%u", w, h);
     PHX_TRY(check_camera(cam));
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
