@@ -1,0 +1,369 @@
+"""Benchmark: phiray's Rendered-mode hot path on the B200.
+
+Workload (the single-large-mesh configuration): an icosphere subdivided 8
+times (1,310,720 faces) displaced by seeded value noise, a ground plane, 4
+area lights, 30% mirror faces, 1920 x 1080, 64 samples per pixel, 8 diffuse
+bounces. One step is one frame: the LBVH rebuilt on the device over the
+mesh's face boxes, 64 samples traced, the a-trous denoise. Inputs are
+seeded synthetic (no dataset exists for this path).
+
+The headline `value` is Mrays/s over the whole frame step (every closest-hit
+and shadow ray the path tracer traced), whole job over all ranks. `e2e` is
+the same metric through the public API from pinned host arrays: create the
+tracer (scene upload + build), trace, denoise, read the packed image back.
+
+`--impl reference` times the reference's algorithm on the host cores (the
+C++ restatement of phiray's CPU twins and WGSL, oracle/, OpenMP over every
+core) on a bounded sample of the same frame.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p frames/s at equal relMSE vs 4096spp: denoised low-spp vs plain; Mrays/s"
+UNIT = "Mrays/s"
+WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 64 spp, 8 bounces, LBVH rebuild + trace + denoise per frame"
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (median SM clock, reasons)."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args) -> None:
+    """The reference's algorithm on the host cores (the oracle restatement)."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from phiray_b200 import scenes
+    from phiray_b200.tracer import camera
+    from tests import oracle_lib
+
+    orc = oracle_lib.load()
+    threads = orc.lib.orc_threads()
+    s = scenes.c2_mesh()
+    cam = camera(s)
+    cam["w"], cam["h"] = s.width, s.height
+    T = oracle_lib.TraceOracle(orc, s)
+    px = np.zeros(34 * s.width * s.height + 1, np.uint32)
+    rows = 64  # a bounded sample: 64 rows of the frame, one sample each
+    vals = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, rays = T.trace(cam, 0, 1, px, rows=(300 + 64 * (k % 8), rows))
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            vals.append(rays / dt / 1e6)
+    v = statistics.median(vals)
+    line = {
+        "metric": METRIC, "value": round(v, 3), "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{rows} rows of the 1080p frame at 1 spp per step (oracle/ C++ restatement, OpenMP)"},
+        "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(scene, cam) -> dict:
+    """The oracle traced on the host cores over a bounded sample (~10 s)."""
+    from tests import oracle_lib
+
+    orc = oracle_lib.load()
+    T = oracle_lib.TraceOracle(orc, scene)
+    px = np.zeros(34 * scene.width * scene.height + 1, np.uint32)
+    rays_total, t_total, row = 0, 0.0, 300
+    while t_total < 10.0 and row < scene.height:
+        t0 = time.perf_counter()
+        _, rays = T.trace(cam, 0, 1, px, rows=(row, 16))
+        t_total += time.perf_counter() - t0
+        rays_total += rays
+        row += 16
+    return {"value": round(rays_total / t_total / 1e6, 3), "unit": UNIT, "cores": orc.lib.orc_threads(), "kind": "port",
+            "sample": f"{row - 300} rows of the 1080p frame at 1 spp ({rays_total} rays, {t_total:.1f} s), oracle/ C++ OpenMP"}
+
+
+def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
+    """Warm-up and steps of one kernel family alone (for ncu launch lists and
+    captures): the frame render, the incoherent ray walk, or the LBVH build."""
+    import torch
+
+    if args.phase == "render":
+        fn = lambda: tr.trace(cam, W, H, 0, args.spp)  # noqa: E731
+    elif args.phase == "build":
+        fn = lambda: tr.repose_device(verts_dev, rebuild=True)  # noqa: E731
+    else:
+        rays = torch.empty((n, 8), dtype=torch.float32, device=f"cuda:{local}")
+        hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
+        tr.secondary_rays(cam, W, H, 0, rays)
+        fn = lambda: tr.trace_rays(rays, n, hits, False)  # noqa: E731
+    for _ in range(args.warmup):
+        fn()
+    gpu.wait(60000)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    gpu.wait(60000)
+    print(json.dumps({"phase": args.phase, "steps": args.steps, "ms": (time.perf_counter() - t0) * 1e3 / args.steps}))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build"],
+                    help="all: the benchmark; render/rays/build: only that kernel's launches (profiling runs)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+
+    s = scenes.c2_mesh(spp=args.spp)
+    cam = px.camera(s)
+    cam["w"], cam["h"] = s.width, s.height
+    W, H, n = s.width, s.height, s.width * s.height
+    gpu = px.Gpu(local)
+    stream = torch.cuda.ExternalStream(gpu.stream)
+    tr = px.Tracer.of(gpu, s)
+    verts_dev = torch.tensor(s.verts, device=f"cuda:{local}")
+
+    def step():
+        tr.repose_device(verts_dev, rebuild=True)  # LBVH rebuild on the device
+        tr.trace(cam, W, H, 0, args.spp)
+        tr.denoise()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        gpu.wait(60000)
+        torch.cuda.synchronize()
+
+    if args.phase != "all":
+        profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local)
+        gpu.close()
+        return
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    _, rays_per_frame = tr.time()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        barrier()
+    ms_step = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = rays_per_frame * world / (ms_step * 1e-3) / 1e6
+
+    # Phase timings (same device, outside the headline loop).
+    def timed(fn, reps):
+        fn()
+        gpu.wait(60000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        gpu.wait(60000)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    nf = s.ntris
+    build_ms = timed(lambda: tr.repose_device(verts_dev, rebuild=True), 10)
+    refit_ms = timed(lambda: tr.repose_device(verts_dev, rebuild=False), 10)
+    tr.trace(cam, W, H, 0, args.spp)
+    trace_ms, trace_rays = tr.time()
+    denoise_ms = timed(lambda: tr.denoise(), 5)
+    counts = tr.trace_stats(cam, W, H, 0, args.spp)  # same walks, counted
+    alg_bytes = counts[1] * 64 + counts[2] * 48
+    pk = peaks()
+    achieved = alg_bytes / (trace_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "trace_render_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tinfo = json.load(f)
+        traffic = tinfo.get("dram_bytes_per_launch_full")
+
+    rays = torch.empty((n, 8), dtype=torch.float32, device=f"cuda:{local}")
+    hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
+    tr.secondary_rays(cam, W, H, 0, rays)
+    inc_ms = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
+    ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
+    ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
+    prim_ms = timed(lambda: tr.primary(cam, W, H, 0, ids, ts), 10)
+
+    # End to end through the public API from pinned host memory.
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
+           (("v", s.verts), ("f", s.faces.view(np.int32)), ("m", s.mats))}
+    hv, hf, hm = pin["v"].numpy(), pin["f"].numpy().view(np.uint32), pin["m"].numpy()
+    h2d = hv.nbytes + hf.nbytes + hm.nbytes + cam.nbytes
+    d2h = n * 4
+
+    def e2e_step():
+        t = px.Tracer(gpu, hv, hf, hm)
+        t.trace(cam, W, H, 0, args.spp)
+        t.denoise()
+        img = t.pixels()
+        t.close()
+        return img
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(2, args.steps // 2)):
+        e2e_step()
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / max(2, args.steps // 2)
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = rays_per_frame * world / e2e_s / 1e6
+
+    out = None
+    if rank == 0:
+        cpu = None if args.no_cpu else cpu_baseline(s, cam)
+        out = {
+            "metric": METRIC,
+            "value": round(value, 2),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_step, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frame": f"{W}x{H}", "spp": args.spp, "bounces": s.bounces,
+                       "tris": nf, "parallelism": f"replicas x{world}",
+                       "l2": "scene ~300 MB of nodes/triangles/materials > 126 MB L2; the rebuild rewrites them each step"},
+            "frames_per_s": round(1000.0 / ms_step * world, 3),
+            "rays_per_frame": int(rays_per_frame),
+            "phases_ms": {"lbvh_build": round(build_ms, 3), "lbvh_refit": round(refit_ms, 3),
+                          "trace": round(trace_ms, 3), "denoise": round(denoise_ms, 3)},
+            "lbvh_build_gbs": round(412 * nf / (build_ms * 1e-3) / 1e9, 1),
+            "lbvh_refit_gbs": round(172 * nf / (refit_ms * 1e-3) / 1e9, 1),
+            "incoherent_grays": round(n / (inc_ms * 1e-3) / 1e9, 3),
+            "primary_grays": round(n / (prim_ms * 1e-3) / 1e9, 3),
+            "roofline": {"bound": "hbm", "kernel": "k_render (path-trace megakernel)", "achieved": round(achieved, 1),
+                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                         "traffic": traffic, "peak_source": pk["source"],
+                         "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": 21 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    gpu.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -394,6 +394,14 @@ int32_t phx_tracer_primary(phx_tracer tr, const phx_camera* cam, uint32_t w, uin
  * arrays: rays[2i] = (origin.xyz, tmax), rays[2i+1] = (dir.xyz, 0);
  * hits[i] = (t, face id bits, u, v) with face 0xFFFFFFFF for a miss. */
 int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit);
+/* The same walks, counted: counts = {rays, inner-node steps, triangle
+ * tests} — the work the walk's algorithmic bytes are computed from (one
+ * 64-byte node record a step, one 48-byte triangle a test). Waits. */
+int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit,
+                             uint64_t counts[3]);
+/* phx_tracer_trace, counted the same way (rays, steps, tests). Waits. */
+int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                               uint32_t spp, uint64_t counts[3]);
 /* The incoherent secondary rays of a frame: for each pixel's primary hit, one
  * cosine-sampled diffuse ray (integrate.wgsl:6-11 cosine_dir) from the
  * lifted hit point, drawn from that pixel's sample stream; written to a

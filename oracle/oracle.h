@@ -97,6 +97,12 @@ struct phx_camera;
 void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
                uint32_t leaf, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
                uint64_t* rays_out, uint32_t row0, uint32_t rows);
+/* The same with the scene (tree, emitter table) built once. */
+void* orc_scene_new(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
+                    uint32_t leaf);
+void orc_scene_free(void* scene);
+void orc_scene_trace(void* scene, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                     uint64_t* rays_out, uint32_t row0, uint32_t rows);
 /* Primary ray of frame `frame` per pixel: face id (0xFFFFFFFF none), t. */
 void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
                  const struct phx_camera* cam, uint32_t frame, uint32_t* ids, float* ts);

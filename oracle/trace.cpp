@@ -1054,21 +1054,33 @@ void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint3
 
 extern "C" {
 
-void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
-               uint32_t leaf, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px, uint64_t* rays_out,
-               uint32_t row0, uint32_t rows) {
+struct OrcScene {
     Shared S;
     World W0;
-    setup(S, W0, verts, faces, nfaces, mats, normals, leaf);
-    const uint32_t w = cam->w, h = cam->h;
-    const uint32_t n = w * h;
+};
+
+void* orc_scene_new(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
+                    uint32_t leaf) {
+    auto* h = new OrcScene();
+    setup(h->S, h->W0, verts, faces, nfaces, mats, normals, leaf);
+    return h;
+}
+
+void orc_scene_free(void* handle) { delete (OrcScene*)handle; }
+
+void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                     uint64_t* rays_out, uint32_t row0, uint32_t rows) {
+    const OrcScene* h = (const OrcScene*)handle;
+    const Shared& S = h->S;
+    const uint32_t w = cam->w, hh = cam->h;
+    const uint32_t n = w * hh;
     const float ao = cam->ao > 0.0f ? cam->ao : S.extent * 0.08f;
     const float eps = S.extent * 1e-5f;
-    const uint32_t r1 = rows ? (row0 + rows < h ? row0 + rows : h) : h;
+    const uint32_t r1 = rows ? (row0 + rows < hh ? row0 + rows : hh) : hh;
     uint64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
     for (int64_t y = row0; y < (int64_t)r1; y++) {
-        World W = W0;  // the scene is shared; counters are per thread
+        World W = h->W0;  // the scene is shared; counters are per thread
         W.p = cam;
         W.n = n;
         W.px = px;
@@ -1085,6 +1097,14 @@ void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const
         total += W.rays;
     }
     if (rays_out) *rays_out = total;
+}
+
+void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,
+               uint32_t leaf, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px, uint64_t* rays_out,
+               uint32_t row0, uint32_t rows) {
+    void* h = orc_scene_new(verts, faces, nfaces, mats, normals, leaf);
+    orc_scene_trace(h, cam, first, spp, px, rays_out, row0, rows);
+    orc_scene_free(h);
 }
 
 void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,

@@ -109,6 +109,8 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_primary": (i32, [vp, vp, u32, u32, u32, vp, vp]),
     "phx_tracer_secondary_rays": (i32, [vp, vp, u32, u32, u32, vp]),
     "phx_trace_rays": (i32, [vp, vp, u32, vp, i32]),
+    "phx_trace_rays_stats": (i32, [vp, vp, u32, vp, i32, C.POINTER(u64)]),
+    "phx_tracer_trace_stats": (i32, [vp, vp, u32, u32, u32, u32, C.POINTER(u64)]),
 }
 
 _lib = None

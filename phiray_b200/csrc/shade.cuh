@@ -71,6 +71,12 @@ struct Hit {
     float u, v;
 };
 
+// Rays traced by a thread, and (STATS builds) the walk's node steps and
+// triangle tests — the work the walk's bytes are counted from.
+struct Count {
+    uint32_t rays, steps, tests;
+};
+
 struct Frame {
     uint32_t w, h, n, frame0, spp, persp, count, bounces;
     f3 right, up, back, pivot, env;
@@ -179,7 +185,9 @@ __device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
 // trace (bvh.wgsl:120-232) over the single-instance tree. `first`: any hit
 // (a shadow ray), which passes glass and cut-outs and stops at the first
 // opaque hit. The stack holds 32 refs; the builder caps the depth at 31.
-__device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first) {
+template <bool STATS>
+__device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    cnt.rays++;
     Hit best{tmax, NONE, 0.0f, 0.0f};
     const f3 inv = safe_inv(d);
     if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return best;
@@ -194,6 +202,7 @@ __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool f
                 const float4 B = __ldg(S.tris + 3 * (size_t)id + 1);
                 const float4 Cc = __ldg(S.tris + 3 * (size_t)id + 2);
                 const uint32_t flags = __float_as_uint(Cc.w);
+                if (STATS) cnt.tests++;
                 float u, v;
                 const float t = tri_t(xyz(A), xyz(B), xyz(Cc), o, rs, u, v);
                 if (t < best.t) {
@@ -209,6 +218,7 @@ __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool f
                 if (flags & FLAG_END) break;
             }
         } else {
+            if (STATS) cnt.steps++;
             const float4* q = S.nodes + 4 * (size_t)nd;
             const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
             const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);

@@ -176,8 +176,9 @@ __device__ __forceinline__ float srgb_to_linear1(float c) {
 __device__ __forceinline__ f3 env_at(const Frame& F) { return F.env; }
 
 // direct (integrate.wgsl:66-85): every light with its shadow ray.
+template <bool STATS>
 __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s, uint32_t& seed, bool with_env,
-                                  f3 sun, uint32_t& rays) {
+                                  f3 sun, Count& cnt) {
     const bool rig = uses_rig(F);
     f3 sum = rig ? rig_fill(F, s) : mk(0.0f);
     for (uint32_t k = 0; k < 4u; k++) {
@@ -192,8 +193,7 @@ __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s,
         // k == 3: env_query needs an environment image's table (env_cdf),
         // which the host refuses; it returns unshadowed without a draw.
         if (maxc(q.c) > 0.0f) {
-            rays++;
-            const float vis = trace(S, s.pos, q.dir, q.dist, true).tri != NONE ? 0.0f : 1.0f;
+            const float vis = trace<STATS>(S, s.pos, q.dir, q.dist, true, cnt).tri != NONE ? 0.0f : 1.0f;
             sum += q.c * vis;
         }
     }
@@ -211,8 +211,9 @@ __device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, co
 }
 
 // indirect (integrate.wgsl:111-230) with no environment image.
+template <bool STATS>
 __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f3 n, uint32_t& seed, bool bounce,
-                                       f3 sun, uint32_t& rays) {
+                                       f3 sun, Count& cnt) {
     const bool lit = dot(F.env, F.env) > 0.0f;
     if (S.lamp_count == 0u && !lit) {
         const f3 dir = cosine_dir(n, seed);
@@ -220,8 +221,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
         // world the product is zero whatever the shadow ray finds, so the
         // ray is only traced when the world has some colour.
         if (F.env.x == 0.0f && F.env.y == 0.0f && F.env.z == 0.0f) return mk(0.0f);
-        rays++;
-        const float vis = trace(S, pos, dir, F.ao, true).tri != NONE ? 0.0f : 1.0f;
+        const float vis = trace<STATS>(S, pos, dir, F.ao, true, cnt).tri != NONE ? 0.0f : 1.0f;
         return env_at(F) * mixf(0.25f, 1.0f, vis);
     }
     const uint32_t depth = bounce ? (F.bounces != 0u ? F.bounces : 1u) : 1u;
@@ -237,8 +237,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
         }
         through = false;
         min_pdf = fminf(min_pdf, pb);
-        rays++;
-        const Hit h = trace(S, org, dir, INF, false);
+        const Hit h = trace<STATS>(S, org, dir, INF, false, cnt);
         if (h.tri == NONE) {
             acc += thr * env_at(F) * 1.0f;
             break;
@@ -259,7 +258,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
         acc += thr * glow_mis(S, g, t.emit, h, nrm, dir);
         const float near = (!lit && h.t <= F.ao) ? 0.25f : 1.0f;
         const Surf s = plain_surf(hit, ng, -dir, albedo, vmix(fd, base, metal), rough);
-        acc += thr * direct(S, F, s, seed, true, sun, rays) * near;
+        acc += thr * direct<STATS>(S, F, s, seed, true, sun, cnt) * near;
         if (tw > 0.0f && rnd(seed) < tw) {
             thr *= mk(sqrtf(base.x), sqrtf(base.y), sqrtf(base.z));
             const f3 at = org + dir * h.t;
@@ -280,8 +279,9 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
 }
 
 // bounce_light (integrate.wgsl:236-250).
+template <bool STATS>
 __device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const Hit& h, f3 org, f3 d,
-                                           uint32_t& seed, f3 sun, uint32_t& rays) {
+                                           uint32_t& seed, f3 sun, Count& cnt) {
     const Geo g = geo_at(S, h.tri);
     const Mat t = mat_at(S, g.mat);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -293,7 +293,7 @@ __device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const
     f3 albedo = base * (1.0f - t.metal);
     if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -d), 1e-4f));
     const Surf s = plain_surf(pos, ng, -d, albedo, vmix(fd, base, t.metal), rough);
-    return direct(S, F, s, seed, false, sun, rays) + s.albedo * env_at(F) * 0.8f + t.emit;
+    return direct<STATS>(S, F, s, seed, false, sun, cnt) + s.albedo * env_at(F) * 0.8f + t.emit;
 }
 
 __device__ __forceinline__ f3 clamp_light(f3 l, float limit) {
@@ -327,8 +327,9 @@ __device__ __forceinline__ CamRay camera_ray(const Frame& F, uint32_t i, uint32_
 }
 
 // One sample of pixel i (shade.wgsl:41-373) added into `acc`.
+template <bool STATS>
 __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t frame, f3 sun, Sums& acc,
-                       uint32_t& rays) {
+                       Count& cnt) {
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     f3 o = cr.o, d = cr.d;
@@ -339,8 +340,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
     uint32_t n_see = 0, n_through = 0;
     const uint32_t passes = see_through + through + 1u;
     for (uint32_t bounce = 0; bounce < passes; bounce++) {
-        rays++;
-        const Hit h = trace(S, o, d, INF, false);
+        const Hit h = trace<STATS>(S, o, d, INF, false, cnt);
         if (h.tri == NONE) {
             if (bounce == 0u) {
                 const float across = (float)(i % F.w) / fmaxf((float)F.w * 0.5f, 1.0f);
@@ -400,11 +400,11 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                      t.coat, t.coat_rough, t.ior, 1.0f - metal};
         const float opaque = 1.0f - t.trans * (1.0f - metal);
         f3 c = mk(0.0f);
-        if (opaque > 0.0f) c = direct(S, F, s, seed, true, sun, rays) * opaque;
+        if (opaque > 0.0f) c = direct<STATS>(S, F, s, seed, true, sun, cnt) * opaque;
         if (opaque < 1.0f) {
             const Surf shine{pos, n, -d, mk(0.0f), s.f0, s.rough, 0.0f, mk(1.0f), 0.0f, t.sheen_rough,
                              t.sheen_tint, t.coat, t.coat_rough, s.eta, s.dielectric};
-            c += direct(S, F, shine, seed, true, sun, rays) * (1.0f - opaque);
+            c += direct<STATS>(S, F, shine, seed, true, sun, cnt) * (1.0f - opaque);
         }
         c = clamp_light(c, F.limit_d);
         f3 bounced = mk(0.0f);
@@ -418,7 +418,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
         if (pd > 0.0f && pg > 0.0f) p_diffuse = clampf(p_diffuse, 0.15f, 0.85f);
         const bool take_diffuse = rnd(seed) < p_diffuse;
         if (take_diffuse && pd > 0.0f)
-            bounced += diffuse_weight * indirect(S, F, pos, n, seed, diffuse_on, sun, rays) / p_diffuse;
+            bounced += diffuse_weight * indirect<STATS>(S, F, pos, n, seed, diffuse_on, sun, cnt) / p_diffuse;
         const f3 v = -d;
         const f3 tx = normalize(onb(n, 1.0f, 0.0f));
         const f3 ty = cross(n, tx);
@@ -433,11 +433,10 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
         const float cos_no = dot(n, refl);
         const f3 fres = fresnel_of(s, cos_hi);
         if (!take_diffuse && glossy_on && dot(refl, ng) > 0.0f && cos_hi > 0.0f && cos_no > 0.0f) {
-            rays++;
-            const Hit rh = trace(S, pos, refl, INF, false);
+            const Hit rh = trace<STATS>(S, pos, refl, INF, false, cnt);
             f3 rc = env_at(F);
             const float wg = 1.0f;
-            if (rh.tri != NONE) rc = bounce_light(S, F, rh, pos, refl, seed, sun, rays);
+            if (rh.tri != NONE) rc = bounce_light<STATS>(S, F, rh, pos, refl, seed, sun, cnt);
             bounced += fres * rc * ggx_weight(ggx_a * ggx_a, fmaxf(dot(n, v), 1e-4f), cos_no) * wg / (1.0f - p_diffuse);
         }
         c += clamp_light(bounced, F.limit_i);
@@ -485,11 +484,12 @@ __device__ __forceinline__ void setup(Scene& S, Frame& F) {
     F.eps = S.extent * 1e-5f;
 }
 
+template <bool STATS>
 __global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
-                                               uint32_t count, unsigned long long* ray_count) {
+                                               uint32_t count, unsigned long long* counters) {
     setup(S, F);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t rays = 0;
+    Count cnt{0, 0, 0};
     if (k < count) {
         const uint32_t i = first + k;
         const uint32_t n = F.n;
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32
             px[30 * n + i] = 0u;
         }
         acc.outline = 0;
-        for (uint32_t s = 0; s < F.spp; s++) sample(S, F, i, F.frame0 + s, sun, acc, rays);
+        for (uint32_t s = 0; s < F.spp; s++) sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
         st3(px, 1 * n, i, acc.lin);
         st3(px, 20 * n, i, acc.grid);
         st3(px, 7 * n, i, acc.alb);
@@ -530,8 +530,16 @@ __global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32
         st3(px, 4 * n, i, shown);
         px[i] = pack_rgba(shown, acc.film / kk);
     }
-    const uint32_t tot = __reduce_add_sync(0xffffffffu, rays);
-    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(ray_count, (unsigned long long)tot);
+    const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counters, (unsigned long long)tot);
+    if (STATS) {
+        const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
+        const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 1, (unsigned long long)st);
+            atomicAdd(counters + 2, (unsigned long long)te);
+        }
+    }
 }
 
 // Primary ray of each pixel: face id and t.
@@ -541,7 +549,8 @@ __global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict
     if (i >= F.n) return;
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
-    const Hit h = trace(S, cr.o, cr.d, INF, false);
+    Count cnt{0, 0, 0};
+    const Hit h = trace<false>(S, cr.o, cr.d, INF, false, cnt);
     ids[i] = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
     ts[i] = h.t;
 }
@@ -553,7 +562,8 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     if (i >= F.n) return;
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
-    const Hit h = trace(S, cr.o, cr.d, INF, false);
+    Count cnt{0, 0, 0};
+    const Hit h = trace<false>(S, cr.o, cr.d, INF, false, cnt);
     if (h.tri == NONE) {
         rays[2 * (size_t)i] = make_float4(cr.o.x, cr.o.y, cr.o.z, 0.0f);
         rays[2 * (size_t)i + 1] = make_float4(cr.d.x, cr.d.y, cr.d.z, 0.0f);
@@ -568,16 +578,26 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     rays[2 * (size_t)i + 1] = make_float4(dir.x, dir.y, dir.z, 0.0f);
 }
 
-template <bool ANY>
+template <bool ANY, bool STATS>
 __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict__ rays, uint32_t n,
-                                              float4* __restrict__ hits) {
+                                              float4* __restrict__ hits, unsigned long long* counters) {
     load_info(S);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
-    const Hit h = trace(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY);
-    const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
-    hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
+    Count cnt{0, 0, 0};
+    if (i < n) {
+        const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+        const Hit h = trace<STATS>(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt);
+        const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
+        hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
+    }
+    if (STATS) {
+        const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
+        const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 1, (unsigned long long)st);
+            atomicAdd(counters + 2, (unsigned long long)te);
+        }
+    }
 }
 
 }  // namespace
@@ -704,7 +724,7 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
 }
 
 int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp,
-                      uint32_t first_px, uint32_t count_px) {
+                      uint32_t first_px, uint32_t count_px, bool stats = false) {
     Ctx* c = tr->ctx;
     const Scene S = scene_of(tr);
     PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, cam, sizeof(phx_camera), cudaMemcpyHostToDevice, c->stream));
@@ -712,8 +732,12 @@ int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t
     F.frame0 = first_frame;
     F.spp = spp;
     const f3 sun = mk(cam->sun[0], cam->sun[1], cam->sun[2]);
-    k_render<<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px, count_px,
-                                                            (unsigned long long*)tr->rays.ptr);
+    if (stats)
+        k_render<true><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
+                                                                      count_px, (unsigned long long*)tr->rays.ptr);
+    else
+        k_render<false><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
+                                                                       count_px, (unsigned long long*)tr->rays.ptr);
     return cuda_check(cudaGetLastError(), "render");
 }
 
@@ -766,7 +790,7 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     step(tr->lamp_power.reserve(n * 4));
     step(tr->lamp_cdf.reserve(n * 4));
     step(tr->info.reserve(64));
-    step(tr->rays.reserve(8));
+    step(tr->rays.reserve(24));
     step(tr->cam.reserve(sizeof(phx_camera)));
     step(tr->bvh.reserve(sc->nfaces, ctx->c.sms));
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev0), "event");
@@ -957,10 +981,49 @@ int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
     if (any_hit)
-        k_rays<true><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits);
+        k_rays<true, false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits, nullptr);
     else
-        k_rays<false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits);
+        k_rays<false, false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits, nullptr);
     return cuda_check(cudaGetLastError(), "trace rays");
+}
+
+int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit,
+                             uint64_t counts[3]) {
+    if (!tr || !counts || (n && (!rays || !hits))) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(use(tr->ctx));
+    cudaStream_t s = tr->ctx->stream;
+    PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
+    const Scene S = scene_of(tr);
+    if (n) {
+        if (any_hit)
+            k_rays<true, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits,
+                                                               (unsigned long long*)tr->rays.ptr);
+        else
+            k_rays<false, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits,
+                                                                (unsigned long long*)tr->rays.ptr);
+        PHX_CUDA(cudaGetLastError());
+    }
+    PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));
+    PHX_TRY(wait_stream(s, 0));
+    counts[0] = n;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                               uint32_t spp, uint64_t counts[3]) {
+    if (!tr || !cam || !counts) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    PHX_TRY(ensure_image(tr, w, h));
+    cudaStream_t s = tr->ctx->stream;
+    PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
+    if (spp) PHX_TRY(launch_render(tr, cam, w, h, first, spp, 0, w * h, true));
+    PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));
+    PHX_TRY(wait_stream(s, 0));
+    tr->frame = first + spp - 1;
+    tr->last = *cam;
+    tr->have_last = true;
+    return read_status(tr->ctx);
 }
 
 }  // extern "C"

@@ -186,6 +186,19 @@ class Tracer:
     def trace_rays(self, rays, n: int, hits, any_hit: bool = False) -> None:
         N.check(N.lib().phx_trace_rays(self.handle, devptr(rays), n, devptr(hits), 1 if any_hit else 0))
 
+    def trace_rays_stats(self, rays, n: int, hits, any_hit: bool = False) -> tuple[int, int, int]:
+        """(rays, inner-node steps, triangle tests) of the same walks."""
+        c = (C.c_uint64 * 3)()
+        N.check(N.lib().phx_trace_rays_stats(self.handle, devptr(rays), n, devptr(hits), 1 if any_hit else 0, c))
+        return c[0], c[1], c[2]
+
+    def trace_stats(self, cam: np.ndarray, w: int, h: int, first: int, spp: int) -> tuple[int, int, int]:
+        """``trace`` counted: (rays, inner-node steps, triangle tests)."""
+        c = (C.c_uint64 * 3)()
+        N.check(N.lib().phx_tracer_trace_stats(self.handle, cam.ctypes.data, w, h, first, spp, c))
+        self.w, self.h = w, h
+        return c[0], c[1], c[2]
+
     def close(self) -> None:
         if self.handle:
             N.lib().phx_tracer_destroy(self.handle)

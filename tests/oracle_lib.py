@@ -35,6 +35,9 @@ SIGS = {
     "orc_skin": (None, [vp, vp, vp, vp, f32, u32, vp]),
     "orc_denoise": (None, [vp, u32, u32, C.POINTER(f32), C.POINTER(f32), C.c_int]),
     "orc_trace": (None, [vp, vp, u32, vp, vp, u32, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
+    "orc_scene_new": (vp, [vp, vp, u32, vp, vp, u32]),
+    "orc_scene_free": (None, [vp]),
+    "orc_scene_trace": (None, [vp, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
     "orc_primary": (None, [vp, vp, u32, vp, u32, vp, u32, vp, vp]),
     "orc_trace_rays": (None, [vp, vp, u32, vp, u32, vp, u32, vp, C.c_int]),
 }
@@ -159,6 +162,14 @@ class TraceOracle:
         self.lib = orc.lib
         self.v, self.f, self.m = _scene_args(scene)
         self.leaf = leaf
+        self.handle = self.lib.orc_scene_new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data,
+                                             None, leaf)
+
+    def __del__(self):
+        try:
+            self.lib.orc_scene_free(self.handle)
+        except Exception:
+            pass
 
     def trace(self, cam, first: int, spp: int, px=None, rows=None):
         w, h = int(cam["w"][0]), int(cam["h"][0])
@@ -166,8 +177,7 @@ class TraceOracle:
             px = np.zeros(34 * w * h + 1, dtype=np.uint32)
         rays = u64()
         r0, nr = (0, 0) if rows is None else rows
-        self.lib.orc_trace(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, None, self.leaf,
-                           cam.ctypes.data, first, spp, px.ctypes.data, C.byref(rays), r0, nr)
+        self.lib.orc_scene_trace(self.handle, cam.ctypes.data, first, spp, px.ctypes.data, C.byref(rays), r0, nr)
         return px, rays.value
 
     def primary(self, cam, frame: int):

@@ -72,10 +72,11 @@ def test_samples_one_at_a_time_equal_one_launch(gpu):
     frames = []
     while True:
         f, done = a.sample(cam, s.width, s.height)
-        if done:
-            break
         frames.append(f)
+        if done:  # (frame, frame + 1 >= samples), sample.rs:223
+            break
     assert frames == [0, 1, 2, 3]
+    assert a.sample(cam, s.width, s.height) == (3, True)  # no more work
     b = px.Tracer.of(gpu, s)
     b.trace(cam, s.width, s.height, 0, 4)
     assert np.array_equal(a.image(), b.image())
