@@ -92,6 +92,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_bvh_destroy": (i32, [vp]),
     "phx_morton": (i32, [vp, vp, u32, vp, vp]),
     "phx_sort_codes": (i32, [vp, vp, u32, vp, vp]),
+    "phx_sort_codes_static": (i32, [vp, vp, u32, vp, vp]),
     "phx_karras": (i32, [vp, vp, u32, vp]),
     "phx_skin": (i32, [vp, vp, vp, vp, vp, u32, vp, u32, C.c_float]),
     "phx_face_boxes": (i32, [vp, vp, vp, u32, vp]),

@@ -606,6 +606,33 @@ static int32_t enqueue_sort(Ctx* c, BvhWork& w, const uint32_t* codes, uint32_t 
     return cuda_check(cudaGetLastError(), "radix sort");
 }
 
+// The stable sort over caller-provided arrays: alt_keys/alt_vals hold n
+// words each, hist 4 x 256 words, tickets 4 words and the look-back
+// 4 x `stride` x 256 words (stride >= ceil(n / 4096)); hist, tickets and the
+// look-back must be zero on entry.
+int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted,
+                         uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* hist, uint32_t* tickets, uint32_t* lookback,
+                         uint32_t stride) {
+    if (n == 0) return PHX_OK;
+    cudaStream_t s = c->stream;
+    const uint32_t tiles = (n + TILE - 1) / TILE;
+    k_hist<<<grid_for(n, 256, (uint32_t)c->sms * 4), 256, 0, s>>>(codes, n, hist);
+    for (int pass = 0; pass < PASSES; pass++) {
+        const uint32_t* kin = pass == 0 ? codes : (pass % 2 == 1 ? alt_keys : sorted);
+        const uint32_t* vin = pass % 2 == 1 ? alt_vals : order;
+        uint32_t* kout = pass % 2 == 0 ? alt_keys : sorted;
+        uint32_t* vout = pass % 2 == 0 ? alt_vals : order;
+        uint32_t* lb = lookback + (size_t)pass * stride * 256;
+        if (pass == 0)
+            k_radix_pass<true><<<tiles, RADIX_THREADS, 0, s>>>(kin, nullptr, kout, vout, n, 0, hist, lb, tickets,
+                                                                c->status);
+        else
+            k_radix_pass<false><<<tiles, RADIX_THREADS, 0, s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
+                                                                 lb, tickets + pass, c->status);
+    }
+    return cuda_check(cudaGetLastError(), "radix sort");
+}
+
 // Every stage of Bvh::build over w.prims[0..n) on the context's stream.
 int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf) {
     cudaStream_t s = c->stream;

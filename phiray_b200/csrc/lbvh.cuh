@@ -27,6 +27,12 @@ struct BvhWork {
     uint32_t* nstarts() const { return (uint32_t*)scalars.ptr + 1; }
 };
 
+// The stable radix sort of `codes` over caller-provided work arrays (see
+// bvh.cu): order and sorted codes out. Stream-ordered; no allocation.
+int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted,
+                         uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* hist, uint32_t* tickets, uint32_t* lookback,
+                         uint32_t stride);
+
 // Every stage of Bvh::build over w.prims[0..n) on the context's stream.
 int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf);
 // Bvh::refit (slots = false: prims through order; true: prims already in
