@@ -184,6 +184,64 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
     print(json.dumps({"phase": args.phase, "steps": args.steps, "ms": (time.perf_counter() - t0) * 1e3 / args.steps}))
 
 
+def run_c3(args) -> None:
+    """The skinned-animation configuration: 500k vertices / ~1M faces, 64
+    bones; per frame Skin -> face boxes -> LBVH refit (or full rebuild) ->
+    trace 1080p at 16 spp. Prints per-stage ms per frame (device events)."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+
+    frames = args.frames
+    s, rig = scenes.c3_skinned(spp=16)
+    cam = px.camera(s)
+    cam["w"], cam["h"] = s.width, s.height
+    gpu = px.Gpu(0)
+    st = torch.cuda.ExternalStream(gpu.stream)
+    tr = px.Tracer.of(gpu, s)
+    vptr, nv = tr.device_verts()
+    dev = {k: torch.tensor(np.ascontiguousarray(a).view(np.uint8), device="cuda")
+           for k, a in dict(rest=rig.rest, offsets=rig.offsets, pairs=rig.pairs).items()}
+    bones = [torch.tensor(rig.bones(f), device="cuda") for f in range(frames)]
+    gpu.wait(60000)
+    torch.cuda.synchronize()
+    res = {}
+    for mode in ("refit", "rebuild"):
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(frames)]
+        rays = 0
+        for f in range(frames + args.warmup):
+            k = f - args.warmup
+            e = ev[k] if k >= 0 else None
+            if e:
+                e[0].record(st)
+            px.skin(gpu, dev["rest"], dev["offsets"], dev["pairs"], bones[f % frames], rig.nbones, vptr, nv, 1e-4)
+            if e:
+                e[1].record(st)
+            tr.repose_device(vptr, rebuild=(mode == "rebuild"))
+            if e:
+                e[2].record(st)
+            tr.trace(cam, s.width, s.height, 0, s.spp)
+            if e:
+                e[3].record(st)
+            if k >= 0:
+                rays += tr.time()[1] if k == 0 else 0
+        gpu.wait(60000)
+        torch.cuda.synchronize()
+        skin = [e[0].elapsed_time(e[1]) for e in ev]
+        bvh = [e[1].elapsed_time(e[2]) for e in ev]
+        trace = [e[2].elapsed_time(e[3]) for e in ev]
+        res[mode] = {"skin_ms": round(statistics.mean(skin), 3), "boxes_and_bvh_ms": round(statistics.mean(bvh), 3),
+                     "trace_ms": round(statistics.mean(trace), 3),
+                     "frame_ms": round(statistics.mean(skin) + statistics.mean(bvh) + statistics.mean(trace), 3)}
+    nb = len(rig.rest)
+    out = {"workload": "c3_skinned: 500k verts / 999k tris, 64 bones, 1-4 influences, 1080p 16 spp",
+           "frames": frames, "per_frame": res,
+           "skin_gbs": round((16 + 4 + 16 * len(rig.pairs) / nb + 16) * nb / (res["refit"]["skin_ms"] * 1e-3) / 1e9, 1)}
+    print(json.dumps(out), flush=True)
+    gpu.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,11 +250,17 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                    help="c2: the headline frame benchmark; c3: the skinned-animation stage timings")
+    ap.add_argument("--frames", type=int, default=120, help="frames of the c3 workload")
     ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build"],
                     help="all: the benchmark; render/rays/build: only that kernel's launches (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload == "c3":
+        run_c3(args)
         return
 
     import torch

@@ -387,6 +387,10 @@ int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint3
  * image buffer from word `offset` (plane p starts at p * w * h) into host
  * memory; bounded wait. */
 int32_t phx_tracer_read(phx_tracer tr, uint64_t offset, uint32_t* dst, uint64_t count, uint32_t timeout_ms);
+/* Device pointer and count of the tracer's own vertex array (x, y, z, 1):
+ * a skinning kernel can write a new pose straight into it before
+ * phx_tracer_repose_device(tr, that pointer, ...), which then copies nothing. */
+int32_t phx_tracer_verts(phx_tracer tr, float** verts, uint32_t* nverts);
 /* Device pointer and size (words) of the image buffer. */
 int32_t phx_tracer_image(phx_tracer tr, uint32_t** px, uint64_t* words);
 /* Tracer::denoise / denoise_shown (read.rs:73-119) over the image. */

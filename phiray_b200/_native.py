@@ -104,6 +104,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),
     "phx_tracer_read": (i32, [vp, u64, vp, u64, u32]),
     "phx_tracer_image": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
+    "phx_tracer_verts": (i32, [vp, C.POINTER(vp), C.POINTER(u32)]),
     "phx_tracer_denoise": (i32, [vp, i32]),
     "phx_tracer_time": (i32, [vp, C.POINTER(C.c_float), C.POINTER(u64)]),
     "phx_tracer_repose_device": (i32, [vp, vp, i32]),

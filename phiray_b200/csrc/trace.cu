@@ -609,6 +609,7 @@ struct phx_tracer_s {
     Ctx* ctx = nullptr;
     uint32_t nverts = 0, nfaces = 0, nmats = 0, leaf = 4;
     bool has_normals = false;
+    bool emissive = false;  // some material emits: the emitter table is built
     DevMem verts, vnorm, faces, mats, tnodes, tris, tnorm, lamp_slot, lamp_power, lamp_cdf, info, px, rays, cam;
     BvhWork bvh;
     uint32_t w = 0, h = 0;
@@ -637,9 +638,12 @@ int32_t prepare(phx_tracer tr) {
     if (n > 1)
         k_convert<<<(n - 1 + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, n - 1, (float4*)tr->tnodes.ptr);
     k_root<<<1, 1, 0, s>>>((const float4*)w.nodes.ptr, n, (float4*)tr->info.ptr);
-    k_lamps<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, n,
-                               (uint32_t*)tr->lamp_slot.ptr, (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr,
-                               (float4*)tr->info.ptr);
+    if (tr->emissive)
+        k_lamps<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, n,
+                                   (uint32_t*)tr->lamp_slot.ptr, (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr,
+                                   (float4*)tr->info.ptr);
+    else  // no material emits: an empty table (the count word of info[2])
+        PHX_CUDA(cudaMemsetAsync((float4*)tr->info.ptr + 2, 0, sizeof(float4), s));
     return cuda_check(cudaGetLastError(), "tracer prepare");
 }
 
@@ -764,6 +768,11 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
             if (q[k] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u uses a texture (not supported)", m);
         if (q[30] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u has a second lobe (not supported)", m);
     }
+    bool emissive = false;
+    for (uint32_t m = 0; m < sc->nmats && !emissive; m++) {
+        const float* e = sc->mats + 32 * (size_t)m + 8;
+        emissive = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2] > 0.0f;
+    }
     PHX_TRY(use(&ctx->c));
     auto* tr = new phx_tracer_s();
     tr->ctx = &ctx->c;
@@ -772,6 +781,7 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     tr->nmats = sc->nmats;
     tr->leaf = sc->leaf ? sc->leaf : 4;
     tr->has_normals = sc->normals != nullptr;
+    tr->emissive = emissive;
     ctx->c.live++;
     cudaStream_t s = ctx->c.stream;
     const size_t n = sc->nfaces;
@@ -902,6 +912,13 @@ int32_t phx_tracer_read(phx_tracer tr, uint64_t offset, uint32_t* dst, uint64_t 
     PHX_CUDA(cudaMemcpyAsync(dst, (const uint32_t*)tr->px.ptr + offset, count * 4, cudaMemcpyDeviceToHost, tr->ctx->stream));
     PHX_TRY(wait_stream(tr->ctx->stream, timeout_ms));
     return read_status(tr->ctx);
+}
+
+int32_t phx_tracer_verts(phx_tracer tr, float** verts, uint32_t* nverts) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (verts) *verts = (float*)tr->verts.ptr;
+    if (nverts) *nverts = tr->nverts;
+    return PHX_OK;
 }
 
 int32_t phx_tracer_image(phx_tracer tr, uint32_t** px, uint64_t* words) {

@@ -288,3 +288,103 @@ def c2_mesh(levels: int = 8, width: int = 1920, height: int = 1080, spp: int = 6
     view = View.look((0.0, 0.3, -2.2), (0.0, -0.1, 1.0), (0.0, 1.0, 0.0), 40.0)
     return Scene("c2_mesh", verts, faces, mats, np.stack(lights), view, width, height, spp, bounces,
                  env=(env, env, env), meta={"levels": levels})
+
+
+def _rot(axis, ang):
+    axis = axis / np.linalg.norm(axis)
+    x, y, z = axis
+    c, s = math.cos(ang), math.sin(ang)
+    C_ = 1 - c
+    return np.array([[c + x * x * C_, x * y * C_ - z * s, x * z * C_ + y * s],
+                     [y * x * C_ + z * s, c + y * y * C_, y * z * C_ - x * s],
+                     [z * x * C_ - y * s, z * y * C_ + x * s, c + z * z * C_]])
+
+
+@dataclass
+class Rig:
+    """CSR linear-blend influences (kernel::Pair rows: bone, weight, next,
+    blend) over `rest` (V, 4), and the bone chain's joints."""
+
+    rest: np.ndarray
+    offsets: np.ndarray
+    pairs: np.ndarray
+    joints: np.ndarray
+    nbones: int
+
+    def bones(self, frame: int, max_deg: float = 15.0) -> np.ndarray:
+        """Column-major world matrices (nbones, 16) float32 for `frame`: each
+        bone turns at most `max_deg` degrees about its parent joint (seeded
+        per frame), composed down the chain."""
+        rng = np.random.Generator(np.random.PCG64(SEED + 2 + 7919 * frame))
+        world = np.eye(4)
+        out = np.zeros((self.nbones, 16), np.float32)
+        for b in range(self.nbones):
+            axis = rng.standard_normal(3)
+            ang = math.radians(max_deg) * rng.uniform(-1.0, 1.0)
+            j = self.joints[b]
+            local = np.eye(4)
+            local[:3, :3] = _rot(axis, ang)
+            local[:3, 3] = j - local[:3, :3] @ j
+            world = world @ local
+            out[b] = world.T.reshape(16).astype(np.float32)  # column-major
+        return out
+
+
+PAIR = np.dtype([("bone", "<u4"), ("weight", "<f4"), ("next", "<u4"), ("blend", "<f4")])
+
+
+def c3_skinned(rings: int = 1000, segments: int = 500, nbones: int = 64, width: int = 1920, height: int = 1080,
+               spp: int = 16, bounces: int = 4):
+    """Config 3: a `rings` x `segments` cylinder grid (500k vertices, ~1M
+    faces by default), radius 0.3, height 2, rigged with a chain of `nbones`
+    bones along its axis; each vertex takes 1-4 influences (uniform count)
+    from the bones nearest its height, weights Dirichlet(1). Returns the rest
+    Scene and its Rig. Lights: two area lights; a ground plane; a dim world."""
+    rng = np.random.Generator(np.random.PCG64(SEED + 2))
+    ys = np.linspace(0.0, 2.0, rings)
+    th = np.linspace(0.0, 2.0 * math.pi, segments, endpoint=False)
+    Y, T = np.meshgrid(ys, th, indexing="ij")
+    pos = np.stack([0.3 * np.cos(T), Y, 0.3 * np.sin(T)], -1).reshape(-1, 3).astype(np.float32)
+    r = np.arange(rings - 1)[:, None]
+    sgm = np.arange(segments)[None, :]
+    a = r * segments + sgm
+    b = r * segments + (sgm + 1) % segments
+    c = (r + 1) * segments + (sgm + 1) % segments
+    d = (r + 1) * segments + sgm
+    f1 = np.stack([a, b, c], -1).reshape(-1, 3)
+    f2 = np.stack([a, c, d], -1).reshape(-1, 3)
+    tri = np.concatenate([f1, f2])
+    nf = len(tri)
+    tri_f = np.zeros((nf, 4), np.uint32)
+    tri_f[:, :3] = tri
+    tri_f[:, 3] = (np.arange(nf) % 7).astype(np.uint32)
+    mats = [lambert(rng.uniform(0.2, 0.8, 3)) for _ in range(7)]
+    mats.append(lambert((0.6, 0.6, 0.6)))
+    g = _quad((-3.0, 0.0, -3.0), (-3.0, 0.0, 3.0), (3.0, 0.0, 3.0), (3.0, 0.0, -3.0), 7)
+    verts, faces = _assemble([(pos, tri_f), g])
+    # Rig: bone b spans heights [b, b + 1) * 2 / nbones, joint at its base.
+    nv = len(verts)
+    seg_h = 2.0 / nbones
+    vb = np.clip((verts[:, 1] / seg_h).astype(np.int64), 0, nbones - 1)
+    counts = rng.integers(1, 5, nv)
+    counts[len(pos):] = 0  # the ground is not skinned
+    offsets = np.zeros(nv + 1, np.uint32)
+    offsets[1:] = np.cumsum(counts)
+    k = int(offsets[-1])
+    pairs = np.zeros(k, PAIR)
+    rep = np.repeat(np.arange(nv), counts)
+    slot = np.arange(k) - np.repeat(offsets[:-1].astype(np.int64), counts)
+    bone = np.clip(vb[rep] + (slot + 1) // 2 * np.where(slot % 2 == 1, 1, -1), 0, nbones - 1)
+    pairs["bone"] = bone
+    pairs["next"] = bone
+    # Dirichlet(1) over each vertex's influences: normalised Exp(1) draws.
+    e = rng.exponential(1.0, k)
+    sums = np.add.reduceat(e, offsets[:-1][counts > 0].astype(np.int64))
+    pairs["weight"] = (e / np.repeat(sums, counts[counts > 0])).astype(np.float32)
+    joints = np.stack([np.zeros(nbones), np.arange(nbones) * seg_h, np.zeros(nbones)], -1)
+    lights = [light_area((-0.8, 2.8, -0.8), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.6, 0.6, (60.0, 60.0, 60.0)),
+              light_area((0.9, 2.5, -0.5), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.4, 0.4, (30.0, 30.0, 30.0))]
+    view = View.look((0.0, 1.0, -3.2), (0.0, 0.0, 1.0), (0.0, 1.0, 0.0), 45.0)
+    scene = Scene("c3_skinned", verts, faces, np.stack(mats), np.stack(lights), view, width, height, spp, bounces,
+                  env=(0.05, 0.05, 0.05))
+    return scene, Rig(verts.copy(), offsets, pairs, joints, nbones)

@@ -160,6 +160,12 @@ class Tracer:
         lin = f[n: 4 * n].reshape(n, 3)
         return (lin / np.maximum(k - gone, 1.0)[:, None]).reshape(self.h, self.w, 3)
 
+    def device_verts(self) -> tuple[int, int]:
+        """Device pointer and count of the tracer's own vertex array."""
+        p, nv = C.c_void_p(), C.c_uint32()
+        N.check(N.lib().phx_tracer_verts(self.handle, C.byref(p), C.byref(nv)))
+        return p.value or 0, nv.value
+
     def device_image(self) -> tuple[int, int]:
         p, words = C.c_void_p(), C.c_uint64()
         N.check(N.lib().phx_tracer_image(self.handle, C.byref(p), C.byref(words)))
