@@ -369,6 +369,26 @@ typedef struct phx_tracer_s* phx_tracer;
  * emitter table. */
 int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* scene, phx_tracer* out);
 int32_t phx_tracer_destroy(phx_tracer tr);
+/* Which kernel traces a frame. All compute the same image bit for bit:
+ * PHX_KERNEL_MEGAKERNEL is shade.wgsl's main as one thread per pixel with
+ * the walk called from every site that traces; PHX_KERNEL_STATE_MACHINE
+ * (the default) is a persistent kernel whose lanes take pixels from a
+ * counter and run the bounce loop as a state machine around one walk, so
+ * lanes at different points of their paths still traverse together. Its
+ * _6 and _8 forms cap registers for 6 or 8 resident 128-thread blocks per
+ * SM (more warps, path state spilled to local memory); phx_tracer_autotune
+ * times them on the scene and keeps the fastest. */
+#define PHX_KERNEL_MEGAKERNEL 0u
+#define PHX_KERNEL_STATE_MACHINE 1u
+#define PHX_KERNEL_STATE_MACHINE_6 2u
+#define PHX_KERNEL_STATE_MACHINE_8 3u
+int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
+/* The autotuner: times every render kernel (and register budget) above on
+ * `spp` samples of this scene and camera, keeps the fastest for the tracer
+ * and returns its id; ms (4 floats, may be NULL) gets each one's time. The
+ * image is overwritten (the next sample starts over). Waits. */
+int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                            uint32_t* chosen, float* ms);
 /* Tracer::set_samples: the sample target `sample` stops at. */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
 /* Tracer::sample / sample_in (src/trace/sample.rs:94-249): one more sample

@@ -100,6 +100,8 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_create": (i32, [vp, vp, C.POINTER(vp)]),
     "phx_tracer_destroy": (i32, [vp]),
     "phx_tracer_set_samples": (i32, [vp, u32]),
+    "phx_tracer_set_kernel": (i32, [vp, u32]),
+    "phx_tracer_autotune": (i32, [vp, vp, u32, u32, u32, C.POINTER(u32), C.POINTER(C.c_float)]),
     "phx_tracer_sample": (i32, [vp, vp, u32, u32, u32, vp, C.POINTER(u32), C.POINTER(i32)]),
     "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),
     "phx_tracer_read": (i32, [vp, u64, vp, u64, u32]),

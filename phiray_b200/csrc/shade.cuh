@@ -186,7 +186,7 @@ __device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
 // (a shadow ray), which passes glass and cut-outs and stops at the first
 // opaque hit. The stack holds 32 refs; the builder caps the depth at 31.
 template <bool STATS>
-__device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+__device__ __forceinline__ Hit walk(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     cnt.rays++;
     Hit best{tmax, NONE, 0.0f, 0.0f};
     const f3 inv = safe_inv(d);
@@ -245,6 +245,12 @@ __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool f
         nd = stack[sp];
     }
     return best;
+}
+
+// The walk behind a call, for code with several trace sites.
+template <bool STATS>
+__device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    return walk<STATS>(S, o, d, tmax, first, cnt);
 }
 
 // ---- scene records ----

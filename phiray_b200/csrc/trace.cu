@@ -7,6 +7,7 @@
 // per-pixel sums in registers across all the samples of a call, writing the
 // image planes once at the end — the same sums, in the same order, that the
 // reference's one-dispatch-per-sample loop leaves in its px buffer.
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 
@@ -542,6 +543,538 @@ __global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32
     }
 }
 
+// ---- the persistent state-machine render (one trace site) ----
+//
+// The same computation as k_render, restructured so every lane reaches the
+// traversal at one program point: a lane's work between two traces is a
+// phase of a state machine, and the loop head traces whatever ray the
+// lane's phase left (closest hit or shadow). Lanes whose paths are at
+// different points of the bounce loop then still walk the tree together.
+// direct()'s shadow rays are traced after all its light queries: the queries
+// draw every random number first and the shadow results only enter the sum,
+// so the draws and the sum happen in the reference's order. Lanes fetch
+// pixels from a counter and take each pixel's samples in order, so per-pixel
+// sums are added in frame order, as the reference's per-sample loop adds them.
+
+enum Phase : uint32_t {
+    PH_TRACE = 0,  // a ray is set: trace it, then go to `after`
+    PH_DONE,
+    PH_BEGIN_SAMPLE,
+    PH_ON_BOUNCE,
+    PH_SHINE_OR_LOBE,
+    PH_LOBE,
+    PH_IND_STEP,
+    PH_ON_IND_HIT,
+    PH_IND_AFTER_DIRECT,
+    PH_ON_IND_AO,
+    PH_AFTER_INDIRECT,
+    PH_GLOSSY,
+    PH_ON_GLOSSY,
+    PH_AFTER_GLOSSY,
+    PH_END_SHADING,
+    PH_EMIT_END,
+    PH_FINISH_SAMPLE,
+    PH_DIRECT_NEXT,
+    PH_ON_SHADOW,
+    PH_AFTER_DIRECT,
+};
+
+enum Cont : uint32_t { C_OPAQUE = 0, C_SHINE = 1, C_IND = 2, C_BOUNCE_LIGHT = 3 };
+
+struct Path {
+    // the ray the loop head traces next, and the phase that takes its hit
+    f3 ro, rd;
+    float rtmax;
+    uint32_t rany, after;
+    // pixel and sample
+    uint32_t i, frame, frame_end, seed;
+    f3 o, d, col, thr;
+    uint32_t bounce, n_see, n_through;
+    // the camera-path hit being shaded
+    f3 hit, past, base, ng;
+    uint32_t front;
+    float trans, metal, ior, opaque, p_diffuse;
+    uint32_t take_diffuse;
+    Surf s;
+    f3 c, bounced, diffuse_weight, aval;
+    // glossy ray
+    f3 fres;
+    float ggx_a, cos_no;
+    // direct(): queries with light, traced in order
+    f3 dpos, dsum;
+    f3 qc[4], qdir[4];
+    float qdist[4];
+    uint32_t qn, qk, cont;
+    // indirect()
+    f3 iacc, ithr, iorg, inrm, idir, ibase, ialbedo, ihit, ing;
+    uint32_t ib, idepth, ithrough, ibounce;
+    float imin_pdf, ipb, inear, itw, iht;
+    // bounce_light()
+    f3 balbedo, bemit;
+};
+
+__device__ __forceinline__ uint32_t set_ray(Path& P, f3 o, f3 d, float tmax, bool any, uint32_t after) {
+    P.ro = o;
+    P.rd = d;
+    P.rtmax = tmax;
+    P.rany = any ? 1u : 0u;
+    P.after = after;
+    return PH_TRACE;
+}
+
+// direct() up to its shadow rays: every query (and its draws) in order.
+__device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F, Path& P, const Surf& s, uint32_t cont,
+                                                 f3 sun) {
+    const bool rig = uses_rig(F);
+    P.dsum = rig ? rig_fill(F, s) : mk(0.0f);
+    P.qn = 0;
+    for (uint32_t k = 0; k < 4u; k++) {
+        Shadowed q = unshadowed();
+        if (k == 0u) {
+            q = rig ? rig_query(F, 0u, s, P.seed, sun) : lamp_query(F, s, P.seed);
+        } else if (k == 1u) {
+            if (rig) q = rig_query(F, 1u, s, P.seed, sun);
+        } else if (k == 2u) {
+            q = glow_query(S, s, P.seed);
+        }
+        if (maxc(q.c) > 0.0f) {
+            P.qc[P.qn] = q.c;
+            P.qdir[P.qn] = q.dir;
+            P.qdist[P.qn] = q.dist;
+            P.qn++;
+        }
+    }
+    P.dpos = s.pos;
+    P.qk = 0;
+    P.cont = cont;
+    return PH_DIRECT_NEXT;
+}
+
+template <bool STATS>
+__device__ uint32_t step(const Scene& S, const Frame& F, Path& P, uint32_t ph, const Hit& h, f3 sun, Sums& acc) {
+    const uint32_t see_through = 8u, through = 8u;
+    const uint32_t passes = see_through + through + 1u;
+    switch (ph) {
+        case PH_BEGIN_SAMPLE: {
+            P.seed = hash(P.i * 9781u + P.frame * 6271u + 1u);
+            const CamRay cr = camera_ray(F, P.i, P.seed);
+            P.o = cr.o;
+            P.d = cr.d;
+            acc.outline = 0;
+            P.col = mk(0.0f);
+            P.thr = mk(1.0f);
+            P.bounce = P.n_see = P.n_through = 0;
+            return set_ray(P, P.o, P.d, INF, false, PH_ON_BOUNCE);
+        }
+        case PH_ON_BOUNCE: {
+            if (h.tri == NONE) {
+                if (P.bounce == 0u) {
+                    const float across = (float)(P.i % F.w) / fmaxf((float)F.w * 0.5f, 1.0f);
+                    const float lift = F.sky[3] * (1.0f - clampf(across, 0.0f, 1.0f));
+                    const f3 sky = mk(F.sky[0] + lift, F.sky[1] + lift, F.sky[2] + lift);
+                    acc.alb += mk(srgb_to_linear1(sky.x), srgb_to_linear1(sky.y), srgb_to_linear1(sky.z));
+                    acc.nrm += -P.d;
+                    acc.dep += -1.0f;
+                    acc.gone += 1.0f;
+                    acc.count += 1u;
+                    acc.film += 1.0f;
+                    acc.lin += mk(0.0f);
+                    acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                    acc.cov += 1.0f;
+                    return PH_FINISH_SAMPLE;
+                }
+                P.col += P.thr * env_at(F);
+                return PH_EMIT_END;
+            }
+            if (P.bounce == 0u) acc.outline = 1u;
+            const Geo g = geo_at(S, h.tri);
+            const Mat t = mat_at(S, g.mat);
+            const float w = 1.0f - h.u - h.v;
+            const f3 hit = P.o + P.d * h.t;
+            const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+            const bool front = dot(ng0, P.d) < 0.0f;
+            const f3 ng = front ? ng0 : -ng0;
+            f3 n = g.na * w + g.nb * h.u + g.nc * h.v;
+            n = dot(n, n) > 1e-12f ? normalize(n) * (front ? 1.0f : -1.0f) : ng;
+            if (dot(n, -P.d) < 0.0f) n = ng;
+            const f3 off = ng * hit_lift(F, h.t);
+            const f3 past = ng * through_lift(F, hit, h.t);
+            const f3 pos = hit + off;
+            const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+            if (P.bounce == 0u) {
+                acc.alb += base;
+                acc.nrm += n;
+                acc.dep += h.t;
+            }
+            if (rnd(P.seed) >= t.color.w) {
+                P.n_see++;
+                if (P.n_see > see_through) return PH_EMIT_END;
+                P.o = hit - past;
+                P.bounce++;
+                if (P.bounce < passes) return set_ray(P, P.o, P.d, INF, false, PH_ON_BOUNCE);
+                return PH_EMIT_END;
+            }
+            P.col += P.thr * t.emit;
+            const float bleed = scatter_bleed(t.sss, t.sss_radius);
+            const f3 fd = dielectric_f0(t.ior);
+            f3 diffuse = base * (1.0f - t.metal);
+            if (maxc(diffuse) > 0.0f)
+                diffuse *= under_layer_real(t.ior, fmaxf(t.rough, 0.04f), fmaxf(dot(n, -P.d), 1e-4f));
+            P.s = Surf{pos,   n,      -P.d,   diffuse,    vmix(fd, base, t.metal), fmaxf(t.rough, 0.04f),
+                       bleed, scatter_tint(t.sss_radius), t.sheen, t.sheen_rough, t.sheen_tint,
+                       t.coat, t.coat_rough, t.ior, 1.0f - t.metal};
+            P.hit = hit;
+            P.past = past;
+            P.base = base;
+            P.ng = ng;
+            P.front = front ? 1u : 0u;
+            P.trans = t.trans;
+            P.metal = t.metal;
+            P.ior = t.ior;
+            P.opaque = 1.0f - t.trans * (1.0f - t.metal);
+            P.c = mk(0.0f);
+            if (P.opaque > 0.0f) return start_direct(S, F, P, P.s, C_OPAQUE, sun);
+            return PH_SHINE_OR_LOBE;
+        }
+        case PH_SHINE_OR_LOBE: {
+            if (P.opaque < 1.0f) {
+                const Surf shine{P.s.pos, P.s.n, P.s.v, mk(0.0f), P.s.f0, P.s.rough, 0.0f, mk(1.0f), 0.0f,
+                                 P.s.sheen_rough, P.s.sheen_tint, P.s.coat, P.s.coat_rough, P.s.eta, P.s.dielectric};
+                return start_direct(S, F, P, shine, C_SHINE, sun);
+            }
+            return PH_LOBE;
+        }
+        case PH_LOBE: {
+            P.c = clamp_light(P.c, F.limit_d);
+            P.bounced = mk(0.0f);
+            const Surf& s = P.s;
+            const float bleed = s.bleed;
+            P.diffuse_weight = vmix(s.albedo, s.albedo * s.sss_tint, bleed) * P.opaque;
+            const f3 lw = mk(0.2126f, 0.7152f, 0.0722f);
+            const float ndv = fmaxf(dot(s.n, -P.d), 1e-4f);
+            const f3 gloss_guess = s.f0 + (mk(1.0f) - s.f0) * pm_pow(1.0f - ndv, 5.0f);
+            const float pd = dot(vmax(P.diffuse_weight, mk(0.0f)), lw);
+            const float pg = dot(gloss_guess, lw);
+            float p_diffuse = pd + pg > 0.0f ? pd / (pd + pg) : 1.0f;
+            if (pd > 0.0f && pg > 0.0f) p_diffuse = clampf(p_diffuse, 0.15f, 0.85f);
+            P.p_diffuse = p_diffuse;
+            P.take_diffuse = rnd(P.seed) < p_diffuse ? 1u : 0u;
+            if (!(P.take_diffuse && pd > 0.0f)) return PH_GLOSSY;
+            // indirect(pos, n, seed, diffuse_on)
+            const bool lit = dot(F.env, F.env) > 0.0f;
+            if (S.lamp_count == 0u && !lit) {
+                const f3 dir = cosine_dir(s.n, P.seed);
+                if (F.env.x == 0.0f && F.env.y == 0.0f && F.env.z == 0.0f) {
+                    P.aval = mk(0.0f);
+                    return PH_AFTER_INDIRECT;
+                }
+                return set_ray(P, s.pos, dir, F.ao, true, PH_ON_IND_AO);
+            }
+            P.idepth = F.bounces != 0u ? F.bounces : 1u;
+            P.ibounce = 1u;
+            P.iacc = mk(0.0f);
+            P.ithr = mk(1.0f);
+            P.iorg = s.pos;
+            P.inrm = s.n;
+            P.imin_pdf = 3.0e38f;
+            P.ithrough = 0u;
+            P.idir = mk(0.0f, 0.0f, 1.0f);
+            P.ipb = 1.0f;
+            P.ib = 0;
+            return PH_IND_STEP;
+        }
+        case PH_IND_STEP: {
+            if (P.ib >= P.idepth) {
+                P.aval = P.iacc;
+                return PH_AFTER_INDIRECT;
+            }
+            if (!P.ithrough) {
+                P.idir = cosine_dir(P.inrm, P.seed);
+                P.ipb = fmaxf(dot(P.inrm, P.idir), 0.0f) / PI;
+            }
+            P.ithrough = 0u;
+            P.imin_pdf = fminf(P.imin_pdf, P.ipb);
+            return set_ray(P, P.iorg, P.idir, INF, false, PH_ON_IND_HIT);
+        }
+        case PH_ON_IND_HIT: {
+            if (h.tri == NONE) {
+                P.iacc += P.ithr * env_at(F) * 1.0f;
+                P.aval = P.iacc;
+                return PH_AFTER_INDIRECT;
+            }
+            if (!P.ibounce) {
+                P.aval = P.iacc;
+                return PH_AFTER_INDIRECT;
+            }
+            const Geo g = geo_at(S, h.tri);
+            const Mat t = mat_at(S, g.mat);
+            const f3 dir = P.idir;
+            const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+            const f3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
+            const f3 hit = P.iorg + dir * h.t + ng * (F.eps + h.t * 1e-5f);
+            const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+            const float rough = fmaxf(t.rough, glossy_floor());
+            const f3 fd = dielectric_f0(t.ior);
+            const float tw = t.trans * (1.0f - t.metal);
+            f3 albedo = base * (1.0f - t.metal) * (1.0f - tw);
+            if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -dir), 1e-4f));
+            P.iacc += P.ithr * glow_mis(S, g, t.emit, h, P.inrm, dir);
+            const bool lit = dot(F.env, F.env) > 0.0f;
+            P.inear = (!lit && h.t <= F.ao) ? 0.25f : 1.0f;
+            P.itw = tw;
+            P.ibase = base;
+            P.ialbedo = albedo;
+            P.ihit = hit;
+            P.ing = ng;
+            P.iht = h.t;
+            const Surf si = plain_surf(hit, ng, -dir, albedo, vmix(fd, base, t.metal), rough);
+            return start_direct(S, F, P, si, C_IND, sun);
+        }
+        case PH_IND_AFTER_DIRECT: {
+            if (P.itw > 0.0f && rnd(P.seed) < P.itw) {
+                P.ithr *= mk(sqrtf(P.ibase.x), sqrtf(P.ibase.y), sqrtf(P.ibase.z));
+                const f3 at = P.iorg + P.idir * P.iht;
+                P.iorg = at - P.ing * through_lift(F, at, P.iht);
+                P.ithrough = 1u;
+                P.ib++;
+                return PH_IND_STEP;
+            }
+            P.ithr *= P.ialbedo;
+            if (P.ib + 1u < P.idepth) {
+                const float keep = clampf(maxc(P.ithr), 0.0f, 0.95f);
+                if (keep < 1e-4f || rnd(P.seed) > keep) {
+                    P.aval = P.iacc;
+                    return PH_AFTER_INDIRECT;
+                }
+                P.ithr = P.ithr / keep;
+            }
+            P.iorg = P.ihit;
+            P.inrm = P.ing;
+            P.ib++;
+            return PH_IND_STEP;
+        }
+        case PH_ON_IND_AO: {
+            const float vis = h.tri != NONE ? 0.0f : 1.0f;
+            P.aval = env_at(F) * mixf(0.25f, 1.0f, vis);
+            return PH_AFTER_INDIRECT;
+        }
+        case PH_AFTER_INDIRECT: {
+            P.bounced += P.diffuse_weight * P.aval / P.p_diffuse;
+            return PH_GLOSSY;
+        }
+        case PH_GLOSSY: {
+            const Surf& s = P.s;
+            const f3 v = -P.d;
+            const f3 tx = normalize(onb(s.n, 1.0f, 0.0f));
+            const f3 ty = cross(s.n, tx);
+            P.ggx_a = s.rough * s.rough;
+            const f3 wi_local = mk(dot(v, tx), dot(v, ty), dot(v, s.n));
+            const float r1 = rnd(P.seed);
+            const float r2 = rnd(P.seed);
+            const f3 h_local = ggx_sample_vndf(wi_local, P.ggx_a, r1, r2);
+            const f3 hw = normalize(tx * h_local.x + ty * h_local.y + s.n * h_local.z);
+            const f3 refl = reflect(P.d, hw);
+            const float cos_hi = fmaxf(dot(hw, v), 0.0f);
+            P.cos_no = dot(s.n, refl);
+            P.fres = fresnel_of(s, cos_hi);
+            if (!P.take_diffuse && dot(refl, P.ng) > 0.0f && cos_hi > 0.0f && P.cos_no > 0.0f)
+                return set_ray(P, s.pos, refl, INF, false, PH_ON_GLOSSY);
+            return PH_END_SHADING;
+        }
+        case PH_ON_GLOSSY: {
+            if (h.tri == NONE) {
+                P.aval = env_at(F);
+                return PH_AFTER_GLOSSY;
+            }
+            // bounce_light (integrate.wgsl:236-250) up to its direct().
+            const Geo g = geo_at(S, h.tri);
+            const Mat t = mat_at(S, g.mat);
+            const f3 d = P.rd;
+            const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+            const f3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
+            const f3 pos = P.ro + d * h.t + ng * (F.eps + h.t * 1e-5f);
+            const f3 base = vmax(mk(t.color.x, t.color.y, t.color.z), mk(0.0f));
+            const float rough = fmaxf(t.rough, glossy_floor());
+            const f3 fd = dielectric_f0(t.ior);
+            f3 albedo = base * (1.0f - t.metal);
+            if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -d), 1e-4f));
+            const Surf s2 = plain_surf(pos, ng, -d, albedo, vmix(fd, base, t.metal), rough);
+            P.balbedo = s2.albedo;
+            P.bemit = t.emit;
+            return start_direct(S, F, P, s2, C_BOUNCE_LIGHT, sun);
+        }
+        case PH_AFTER_GLOSSY: {
+            const Surf& s = P.s;
+            P.bounced += P.fres * P.aval * ggx_weight(P.ggx_a * P.ggx_a, fmaxf(dot(s.n, -P.d), 1e-4f), P.cos_no) *
+                         1.0f / (1.0f - P.p_diffuse);
+            return PH_END_SHADING;
+        }
+        case PH_END_SHADING: {
+            P.c += clamp_light(P.bounced, F.limit_i);
+            P.col += P.thr * P.c;
+            const float tw = P.trans * (1.0f - P.metal);
+            if (tw <= 0.0f) return PH_EMIT_END;
+            P.n_through++;
+            if (P.n_through > through) return PH_EMIT_END;
+            const float eta = P.front ? 1.0f / P.ior : P.ior;
+            f3 nd = refract(P.d, P.s.n, eta);
+            if (dot(nd, nd) < 1e-6f) {
+                nd = reflect(P.d, P.s.n);
+                P.o = P.hit + P.past;
+                P.thr *= tw;
+            } else {
+                P.o = P.hit - P.past;
+                P.thr *= mk(sqrtf(P.base.x), sqrtf(P.base.y), sqrtf(P.base.z)) * tw * (mk(1.0f) - P.fres);
+            }
+            P.d = cone_dir(normalize(nd), P.s.rough * P.s.rough, P.seed);
+            if (maxc(P.thr) < 0.01f) return PH_EMIT_END;
+            P.bounce++;
+            if (P.bounce < passes) return set_ray(P, P.o, P.d, INF, false, PH_ON_BOUNCE);
+            return PH_EMIT_END;
+        }
+        case PH_EMIT_END: {
+            acc.gone += 0.0f;
+            acc.count += 1u;
+            acc.film += 1.0f;
+            acc.lin += P.col;
+            acc.grid += mk(0.0f);
+            acc.cov += 0.0f;
+            return PH_FINISH_SAMPLE;
+        }
+        case PH_DIRECT_NEXT: {
+            if (P.qk < P.qn) return set_ray(P, P.dpos, P.qdir[P.qk], P.qdist[P.qk], true, PH_ON_SHADOW);
+            return PH_AFTER_DIRECT;
+        }
+        case PH_ON_SHADOW: {
+            const float vis = h.tri != NONE ? 0.0f : 1.0f;
+            P.dsum += P.qc[P.qk] * vis;
+            P.qk++;
+            return PH_DIRECT_NEXT;
+        }
+        case PH_AFTER_DIRECT: {
+            const f3 D = P.dsum;
+            if (P.cont == C_OPAQUE) {
+                P.c = D * P.opaque;
+                return PH_SHINE_OR_LOBE;
+            }
+            if (P.cont == C_SHINE) {
+                P.c += D * (1.0f - P.opaque);
+                return PH_LOBE;
+            }
+            if (P.cont == C_IND) {
+                P.iacc += P.ithr * D * P.inear;
+                return PH_IND_AFTER_DIRECT;
+            }
+            P.aval = D + P.balbedo * env_at(F) * 0.8f + P.bemit;
+            return PH_AFTER_GLOSSY;
+        }
+    }
+    return PH_DONE;
+}
+
+__device__ __forceinline__ void load_sums(const uint32_t* px, uint32_t n, uint32_t i, bool keep, Sums& acc) {
+    if (keep) {
+        ld3(px, 1 * n, i, acc.lin);
+        ld3(px, 20 * n, i, acc.grid);
+        ld3(px, 7 * n, i, acc.alb);
+        ld3(px, 10 * n, i, acc.nrm);
+        acc.cov = __uint_as_float(px[23 * n + i]);
+        acc.film = __uint_as_float(px[24 * n + i]);
+        acc.gone = __uint_as_float(px[33 * n + i]);
+        acc.dep = __uint_as_float(px[13 * n + i]);
+        acc.count = px[31 * n + i];
+    } else {
+        acc.lin = acc.grid = acc.alb = acc.nrm = mk(0.0f);
+        acc.cov = acc.film = acc.gone = acc.dep = 0.0f;
+        acc.count = 0;
+    }
+    acc.outline = 0;
+}
+
+__device__ __forceinline__ void store_sums(uint32_t* px, uint32_t n, uint32_t i, bool first_frame, const Sums& acc,
+                                           const Frame& F) {
+    if (first_frame) {
+        px[29 * n + i] = 0u;
+        px[30 * n + i] = 0u;
+    }
+    st3(px, 1 * n, i, acc.lin);
+    st3(px, 20 * n, i, acc.grid);
+    st3(px, 7 * n, i, acc.alb);
+    st3(px, 10 * n, i, acc.nrm);
+    px[23 * n + i] = __float_as_uint(acc.cov);
+    px[24 * n + i] = __float_as_uint(acc.film);
+    px[33 * n + i] = __float_as_uint(acc.gone);
+    px[13 * n + i] = __float_as_uint(acc.dep);
+    px[31 * n + i] = acc.count;
+    px[25 * n + i] = acc.outline;
+    const float kk = (float)acc.count;
+    const f3 shown = view_transform_std(acc.lin / fmaxf(kk - acc.gone, 1.0f), F.exposure, F.gamma) *
+                         (1.0f - acc.cov / kk) +
+                     acc.grid / kk;
+    st3(px, 4 * n, i, shown);
+    px[i] = pack_rgba(shown, acc.film / kk);
+}
+
+// Persistent: every lane takes pixels from `next` until [first, first +
+// count) is done, tracing all of a pixel's samples in frame order.
+template <bool STATS, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
+                                                  uint32_t count, uint32_t* next, unsigned long long* counters) {
+    setup(S, F);
+    Count cnt{0, 0, 0};
+    Path P;
+    Sums acc;
+    uint32_t ph = PH_DONE;
+    uint32_t k = atomicAdd(next, 1u);
+    if (k < count) {
+        P.i = first + k;
+        P.frame = F.frame0;
+        P.frame_end = F.frame0 + F.spp;
+        load_sums(px, F.n, P.i, F.frame0 > 0u, acc);
+        ph = F.spp > 0u ? (uint32_t)PH_BEGIN_SAMPLE : (uint32_t)PH_FINISH_SAMPLE;
+    }
+    Hit h{INF, NONE, 0.0f, 0.0f};
+    for (;;) {
+        // run phases until the lane needs a ray or runs out of pixels
+        while (ph != PH_TRACE && ph != PH_DONE) {
+            if (ph == PH_FINISH_SAMPLE) {
+                P.frame++;
+                if (P.frame < P.frame_end) {
+                    ph = PH_BEGIN_SAMPLE;
+                    continue;
+                }
+                store_sums(px, F.n, P.i, F.frame0 == 0u, acc, F);
+                k = atomicAdd(next, 1u);
+                if (k >= count) {
+                    ph = PH_DONE;
+                    break;
+                }
+                P.i = first + k;
+                P.frame = F.frame0;
+                load_sums(px, F.n, P.i, F.frame0 > 0u, acc);
+                ph = PH_BEGIN_SAMPLE;
+                continue;
+            }
+            ph = step<STATS>(S, F, P, ph, h, sun, acc);
+        }
+        if (__all_sync(0xffffffffu, ph == PH_DONE)) break;
+        if (ph == PH_TRACE) {
+            h = walk<STATS>(S, P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
+            ph = P.after;
+        }
+    }
+    const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counters, (unsigned long long)tot);
+    if (STATS) {
+        const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
+        const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 1, (unsigned long long)st);
+            atomicAdd(counters + 2, (unsigned long long)te);
+        }
+    }
+}
+
 // Primary ray of each pixel: face id and t.
 __global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict__ ids, float* __restrict__ ts) {
     setup(S, F);
@@ -614,6 +1147,8 @@ struct phx_tracer_s {
     BvhWork bvh;
     uint32_t w = 0, h = 0;
     uint32_t frame = 0, target = 1024;
+    uint32_t kernel = PHX_KERNEL_STATE_MACHINE;  // which render kernel traces a frame
+    DevMem next;                                 // the state-machine kernel's pixel counter
     bool have_last = false;
     phx_camera last;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -736,6 +1271,30 @@ int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t
     F.frame0 = first_frame;
     F.spp = spp;
     const f3 sun = mk(cam->sun[0], cam->sun[1], cam->sun[2]);
+    if (tr->kernel != PHX_KERNEL_MEGAKERNEL) {
+        // state machine, at 4, 6 or 8 resident blocks of 128 per SM
+        const int minb = tr->kernel == 1u ? 4 : (tr->kernel == 2u ? 6 : 8);
+        const void* fn = minb == 4 ? (const void*)k_render_sm<false, 4>
+                                   : (minb == 6 ? (const void*)k_render_sm<false, 6> : (const void*)k_render_sm<false, 8>);
+        int per_sm = 0;
+        PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0));
+        const uint32_t grid = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)c->sms;
+        const uint32_t blocks = std::min<uint32_t>(grid, (count_px + 127) / 128);
+        PHX_CUDA(cudaMemsetAsync(tr->next.ptr, 0, 4, c->stream));
+        uint32_t* pxp = (uint32_t*)tr->px.ptr;
+        uint32_t* nx = (uint32_t*)tr->next.ptr;
+        unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
+        if (stats) {
+            if (minb == 4) k_render_sm<true, 4><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+            else if (minb == 6) k_render_sm<true, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+            else k_render_sm<true, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+        } else {
+            if (minb == 4) k_render_sm<false, 4><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+            else if (minb == 6) k_render_sm<false, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+            else k_render_sm<false, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
+        }
+        return cuda_check(cudaGetLastError(), "render");
+    }
     if (stats)
         k_render<true><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
                                                                       count_px, (unsigned long long*)tr->rays.ptr);
@@ -802,6 +1361,7 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     step(tr->info.reserve(64));
     step(tr->rays.reserve(24));
     step(tr->cam.reserve(sizeof(phx_camera)));
+    step(tr->next.reserve(16));
     step(tr->bvh.reserve(sc->nfaces, ctx->c.sms));
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev0), "event");
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev1), "event");
@@ -837,6 +1397,45 @@ int32_t phx_tracer_destroy(phx_tracer tr) {
     tr->ctx->live--;
     delete tr;
     return PHX_OK;
+}
+
+int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (kernel > PHX_KERNEL_STATE_MACHINE_8) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
+    tr->kernel = kernel;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                            uint32_t* chosen, float* ms) {
+    if (!tr || !cam) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    PHX_TRY(ensure_image(tr, w, h));
+    Ctx* c = tr->ctx;
+    float best = 0.0f;
+    uint32_t pick = PHX_KERNEL_STATE_MACHINE;
+    const uint32_t keep = tr->kernel;
+    for (uint32_t k = 0; k <= PHX_KERNEL_STATE_MACHINE_8; k++) {
+        tr->kernel = k;
+        PHX_TRY(launch_render(tr, cam, w, h, 0, spp ? spp : 1, 0, w * h));  // warm-up
+        PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));
+        PHX_TRY(launch_render(tr, cam, w, h, 0, spp ? spp : 1, 0, w * h));
+        PHX_CUDA(cudaEventRecord(tr->ev1, c->stream));
+        PHX_TRY(wait_stream(c->stream, 60000));
+        float t = 0.0f;
+        PHX_CUDA(cudaEventElapsedTime(&t, tr->ev0, tr->ev1));
+        if (ms) ms[k] = t;
+        if (k == 0 || t < best) {
+            best = t;
+            pick = k;
+        }
+    }
+    tr->kernel = pick;
+    (void)keep;
+    tr->have_last = false;  // the image holds the tuning frames: start over
+    if (chosen) *chosen = pick;
+    return read_status(c);
 }
 
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples) {

@@ -121,6 +121,23 @@ class Tracer:
     def of(cls, gpu: Gpu, scene, **kw) -> "Tracer":
         return cls(gpu, scene.verts, scene.faces, scene.mats, **kw)
 
+    MEGAKERNEL = 0
+    STATE_MACHINE = 1
+    STATE_MACHINE_6 = 2
+    STATE_MACHINE_8 = 3
+
+    def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
+        """Times every render kernel on this scene; keeps and returns the fastest."""
+        chosen = C.c_uint32()
+        ms = (C.c_float * 4)()
+        N.check(N.lib().phx_tracer_autotune(self.handle, cam.ctypes.data, w, h, spp, C.byref(chosen), ms))
+        self.w, self.h = w, h
+        return chosen.value, list(ms)
+
+    def set_kernel(self, kind: int) -> None:
+        """Render kernel: Tracer.MEGAKERNEL or Tracer.STATE_MACHINE (same image)."""
+        N.check(N.lib().phx_tracer_set_kernel(self.handle, kind))
+
     def set_samples(self, n: int) -> None:
         N.check(N.lib().phx_tracer_set_samples(self.handle, n))
 

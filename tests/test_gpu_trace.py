@@ -50,12 +50,14 @@ SCENES = {
 }
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3], ids=["megakernel", "state_machine", "sm6", "sm8"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_image_matches_oracle(gpu, orc, name):
+def test_image_matches_oracle(gpu, orc, name, kernel):
     s = SCENES[name]()
     cam = cam_of(s, s.width, s.height)
     want, orays = oracle_lib.TraceOracle(orc, s).trace(cam, 0, s.spp)
     tr = px.Tracer.of(gpu, s)
+    tr.set_kernel(kernel)
     tr.trace(cam, s.width, s.height, 0, s.spp)
     got = tr.image()
     check_image(got, want, s.width * s.height)
@@ -150,6 +152,17 @@ def test_ray_buffer_walks(gpu, orc):
         hit = want.view(np.uint32)[:, 1] != 0xFFFFFFFF
         if not any_hit:
             assert np.array_equal(got[hit], want[hit])
+
+
+def test_autotune_keeps_the_image(gpu, orc):
+    s = SCENES["c2_small"]()
+    cam = cam_of(s, s.width, s.height)
+    tr = px.Tracer.of(gpu, s)
+    chosen, ms = tr.autotune(cam, s.width, s.height, 2)
+    assert chosen in (0, 1, 2, 3) and all(t > 0 for t in ms)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    want, _ = oracle_lib.TraceOracle(orc, s).trace(cam, 0, s.spp)
+    check_image(tr.image(), want, s.width * s.height)
 
 
 def test_config1_full_image(gpu, orc):
