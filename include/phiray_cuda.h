@@ -389,6 +389,12 @@ int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
  * image is overwritten (the next sample starts over). Waits. */
 int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
                             uint32_t* chosen, float* ms);
+/* Where ray-buffer walks (phx_trace_rays) keep their 32-entry stack:
+ * PHX_STACK_LOCAL (per-thread local memory, the default) or PHX_STACK_SHARED
+ * (a column of a block-wide shared-memory array). Same hits either way. */
+#define PHX_STACK_LOCAL 0u
+#define PHX_STACK_SHARED 1u
+int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
 /* Tracer::set_samples: the sample target `sample` stops at. */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
 /* Tracer::sample / sample_in (src/trace/sample.rs:94-249): one more sample
@@ -446,6 +452,13 @@ int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w,
  * primary ray missed gets a ray with tmax 0). */
 int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t frame,
                                   float* rays);
+
+/* ---- BF16 tensor-core engine (learned denoiser; no reference counterpart:
+ * phiray has no learned denoiser, docs/reconstruct.md:61) ---- */
+/* D (fp32 M x N, row-major) = A (bf16 M x K, row-major) x B^T (bf16 N x K,
+ * row-major), on tcgen05 tensor cores with the accumulator in TMEM.
+ * M % 128 == 0, K % 64 == 0, N in {32, 64, 96, 128, 160}. Device pointers. */
+int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, float* D, uint32_t M, uint32_t N, uint32_t K);
 
 #ifdef __cplusplus
 }

@@ -94,6 +94,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_sort_codes": (i32, [vp, vp, u32, vp, vp]),
     "phx_sort_codes_static": (i32, [vp, vp, u32, vp, vp]),
     "phx_karras": (i32, [vp, vp, u32, vp]),
+    "phx_gemm_bf16": (i32, [vp, vp, vp, vp, u32, u32, u32]),
     "phx_skin": (i32, [vp, vp, vp, vp, vp, u32, vp, u32, C.c_float]),
     "phx_face_boxes": (i32, [vp, vp, vp, u32, vp]),
     "phx_denoise": (i32, [vp, vp, u32, u32, f32p, f32p, i32]),
@@ -101,6 +102,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_destroy": (i32, [vp]),
     "phx_tracer_set_samples": (i32, [vp, u32]),
     "phx_tracer_set_kernel": (i32, [vp, u32]),
+    "phx_tracer_set_stack": (i32, [vp, u32]),
     "phx_tracer_autotune": (i32, [vp, vp, u32, u32, u32, C.POINTER(u32), C.POINTER(C.c_float)]),
     "phx_tracer_sample": (i32, [vp, vp, u32, u32, u32, vp, C.POINTER(u32), C.POINTER(i32)]),
     "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),

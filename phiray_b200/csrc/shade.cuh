@@ -185,14 +185,41 @@ __device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
 // trace (bvh.wgsl:120-232) over the single-instance tree. `first`: any hit
 // (a shadow ray), which passes glass and cut-outs and stops at the first
 // opaque hit. The stack holds 32 refs; the builder caps the depth at 31.
-template <bool STATS>
-__device__ __forceinline__ Hit walk(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+// The arrays and root a walk reads, passed by value so they stay in
+// registers across the walk loop (a reference to a struct in local memory is
+// re-read every step when the loop's stack stores might alias it).
+struct Tree {
+    const float4* __restrict__ nodes;
+    const float4* __restrict__ tris;
+    uint32_t nslots, root;
+    f3 root_lo, root_hi;
+};
+
+__device__ __forceinline__ Tree tree_of(const Scene& S) {
+    return Tree{S.nodes, S.tris, S.nslots, S.root, S.root_lo, S.root_hi};
+}
+
+// The traversal stack: a per-thread array in local memory, or (SMEM) this
+// thread's column of a block-wide shared array, entry k at stk[k * stride].
+template <bool SMEM>
+struct Stack {
+    uint32_t local[SMEM ? 1 : STACK];
+    uint32_t* shared;
+    int stride;
+    __device__ __forceinline__ uint32_t& at(int k) { return SMEM ? shared[k * stride] : local[k]; }
+};
+
+template <bool STATS, bool SMEM = false>
+__device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool first, Count& cnt,
+                                    uint32_t* smem_stack = nullptr, int stride = 0) {
     cnt.rays++;
     Hit best{tmax, NONE, 0.0f, 0.0f};
     const f3 inv = safe_inv(d);
     if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return best;
     const RaySpace rs = ray_space(d);
-    uint32_t stack[STACK];
+    Stack<SMEM> stack;
+    stack.shared = smem_stack;
+    stack.stride = stride;
     int sp = 0;
     uint32_t nd = S.root;
     for (;;) {
@@ -227,7 +254,7 @@ __device__ __forceinline__ Hit walk(const Scene& S, f3 o, f3 d, float tmax, bool
             if (tl < INF && tr < INF) {
                 // Depth <= 31 keeps sp below STACK; the check only guards a
                 // corrupt tree from writing past the stack.
-                if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
+                if (sp < STACK) stack.at(sp++) = tl <= tr ? r : l;
                 nd = tl <= tr ? l : r;
                 continue;
             }
@@ -242,7 +269,7 @@ __device__ __forceinline__ Hit walk(const Scene& S, f3 o, f3 d, float tmax, bool
         }
         if (sp == 0) break;
         sp--;
-        nd = stack[sp];
+        nd = stack.at(sp);
     }
     return best;
 }
@@ -250,7 +277,7 @@ __device__ __forceinline__ Hit walk(const Scene& S, f3 o, f3 d, float tmax, bool
 // The walk behind a call, for code with several trace sites.
 template <bool STATS>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
-    return walk<STATS>(S, o, d, tmax, first, cnt);
+    return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 
 // ---- scene records ----

@@ -486,7 +486,7 @@ __device__ __forceinline__ void setup(Scene& S, Frame& F) {
 }
 
 template <bool STATS>
-__global__ void __launch_bounds__(128) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
+__global__ void __launch_bounds__(128, 4) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
                                                uint32_t count, unsigned long long* counters) {
     setup(S, F);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -600,11 +600,22 @@ struct Path {
     // glossy ray
     f3 fres;
     float ggx_a, cos_no;
-    // direct(): queries with light, traced in order
+    // direct(): queries with light, traced in order (four named slots, so no
+    // array is indexed at run time and the state can stay in registers)
     f3 dpos, dsum;
-    f3 qc[4], qdir[4];
-    float qdist[4];
+    f3 qc0, qc1, qc2, qc3, qd0, qd1, qd2, qd3;
+    float ql0, ql1, ql2, ql3;
     uint32_t qn, qk, cont;
+
+    __device__ __forceinline__ void put(uint32_t k, f3 c, f3 d, float l) {
+        if (k == 0) { qc0 = c; qd0 = d; ql0 = l; }
+        else if (k == 1) { qc1 = c; qd1 = d; ql1 = l; }
+        else if (k == 2) { qc2 = c; qd2 = d; ql2 = l; }
+        else { qc3 = c; qd3 = d; ql3 = l; }
+    }
+    __device__ __forceinline__ f3 qc(uint32_t k) const { return k == 0 ? qc0 : (k == 1 ? qc1 : (k == 2 ? qc2 : qc3)); }
+    __device__ __forceinline__ f3 qd(uint32_t k) const { return k == 0 ? qd0 : (k == 1 ? qd1 : (k == 2 ? qd2 : qd3)); }
+    __device__ __forceinline__ float ql(uint32_t k) const { return k == 0 ? ql0 : (k == 1 ? ql1 : (k == 2 ? ql2 : ql3)); }
     // indirect()
     f3 iacc, ithr, iorg, inrm, idir, ibase, ialbedo, ihit, ing;
     uint32_t ib, idepth, ithrough, ibounce;
@@ -638,9 +649,7 @@ __device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F,
             q = glow_query(S, s, P.seed);
         }
         if (maxc(q.c) > 0.0f) {
-            P.qc[P.qn] = q.c;
-            P.qdir[P.qn] = q.dir;
-            P.qdist[P.qn] = q.dist;
+            P.put(P.qn, q.c, q.dir, q.dist);
             P.qn++;
         }
     }
@@ -651,7 +660,8 @@ __device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F,
 }
 
 template <bool STATS>
-__device__ uint32_t step(const Scene& S, const Frame& F, Path& P, uint32_t ph, const Hit& h, f3 sun, Sums& acc) {
+__device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P, uint32_t ph, const Hit& h, f3 sun,
+                                         Sums& acc) {
     const uint32_t see_through = 8u, through = 8u;
     const uint32_t passes = see_through + through + 1u;
     switch (ph) {
@@ -942,12 +952,12 @@ __device__ uint32_t step(const Scene& S, const Frame& F, Path& P, uint32_t ph, c
             return PH_FINISH_SAMPLE;
         }
         case PH_DIRECT_NEXT: {
-            if (P.qk < P.qn) return set_ray(P, P.dpos, P.qdir[P.qk], P.qdist[P.qk], true, PH_ON_SHADOW);
+            if (P.qk < P.qn) return set_ray(P, P.dpos, P.qd(P.qk), P.ql(P.qk), true, PH_ON_SHADOW);
             return PH_AFTER_DIRECT;
         }
         case PH_ON_SHADOW: {
             const float vis = h.tri != NONE ? 0.0f : 1.0f;
-            P.dsum += P.qc[P.qk] * vis;
+            P.dsum += P.qc(P.qk) * vis;
             P.qk++;
             return PH_DIRECT_NEXT;
         }
@@ -1059,7 +1069,7 @@ __global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 su
         }
         if (__all_sync(0xffffffffu, ph == PH_DONE)) break;
         if (ph == PH_TRACE) {
-            h = walk<STATS>(S, P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
+            h = walk<STATS>(tree_of(S), P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
             ph = P.after;
         }
     }
@@ -1083,7 +1093,7 @@ __global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     Count cnt{0, 0, 0};
-    const Hit h = trace<false>(S, cr.o, cr.d, INF, false, cnt);
+    const Hit h = walk<false>(tree_of(S), cr.o, cr.d, INF, false, cnt);
     ids[i] = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
     ts[i] = h.t;
 }
@@ -1096,7 +1106,7 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     Count cnt{0, 0, 0};
-    const Hit h = trace<false>(S, cr.o, cr.d, INF, false, cnt);
+    const Hit h = walk<false>(tree_of(S), cr.o, cr.d, INF, false, cnt);
     if (h.tri == NONE) {
         rays[2 * (size_t)i] = make_float4(cr.o.x, cr.o.y, cr.o.z, 0.0f);
         rays[2 * (size_t)i + 1] = make_float4(cr.d.x, cr.d.y, cr.d.z, 0.0f);
@@ -1111,15 +1121,17 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     rays[2 * (size_t)i + 1] = make_float4(dir.x, dir.y, dir.z, 0.0f);
 }
 
-template <bool ANY, bool STATS>
+template <bool ANY, bool STATS, bool SMEM>
 __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict__ rays, uint32_t n,
                                               float4* __restrict__ hits, unsigned long long* counters) {
+    __shared__ uint32_t s_stack[SMEM ? STACK * 128 : 1];
     load_info(S);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt{0, 0, 0};
     if (i < n) {
         const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
-        const Hit h = trace<STATS>(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt);
+        const Hit h = walk<STATS, SMEM>(tree_of(S), mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt,
+                                        s_stack + threadIdx.x, 128);
         const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
         hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
     }
@@ -1131,6 +1143,15 @@ __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict_
             atomicAdd(counters + 2, (unsigned long long)te);
         }
     }
+}
+
+template <bool ANY, bool STATS>
+void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters, bool smem,
+                 cudaStream_t s) {
+    if (smem)
+        k_rays<ANY, STATS, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters);
+    else
+        k_rays<ANY, STATS, false><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters);
 }
 
 }  // namespace
@@ -1149,6 +1170,7 @@ struct phx_tracer_s {
     uint32_t frame = 0, target = 1024;
     uint32_t kernel = PHX_KERNEL_STATE_MACHINE;  // which render kernel traces a frame
     DevMem next;                                 // the state-machine kernel's pixel counter
+    bool smem_stack = false;                     // ray walks keep their stack in shared memory
     bool have_last = false;
     phx_camera last;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1438,6 +1460,13 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
     return read_status(c);
 }
 
+int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (place > PHX_STACK_SHARED) return fail(PHX_ERR_INVALID, "unknown stack placement %u", place);
+    tr->smem_stack = place == PHX_STACK_SHARED;
+    return PHX_OK;
+}
+
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
     tr->target = samples ? samples : 1;
@@ -1596,10 +1625,8 @@ int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits
     if (n == 0) return PHX_OK;
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
-    if (any_hit)
-        k_rays<true, false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits, nullptr);
-    else
-        k_rays<false, false><<<(n + 127) / 128, 128, 0, tr->ctx->stream>>>(S, (const float4*)rays, n, (float4*)hits, nullptr);
+    if (any_hit) launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream);
+    else launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream);
     return cuda_check(cudaGetLastError(), "trace rays");
 }
 
@@ -1611,12 +1638,8 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
     PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
     const Scene S = scene_of(tr);
     if (n) {
-        if (any_hit)
-            k_rays<true, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits,
-                                                               (unsigned long long*)tr->rays.ptr);
-        else
-            k_rays<false, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits,
-                                                                (unsigned long long*)tr->rays.ptr);
+        if (any_hit) launch_rays<true, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s);
+        else launch_rays<false, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s);
         PHX_CUDA(cudaGetLastError());
     }
     PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));

@@ -138,6 +138,10 @@ class Tracer:
         """Render kernel: Tracer.MEGAKERNEL or Tracer.STATE_MACHINE (same image)."""
         N.check(N.lib().phx_tracer_set_kernel(self.handle, kind))
 
+    def set_stack(self, shared: bool) -> None:
+        """Ray-buffer walks keep their stack in shared (True) or local memory."""
+        N.check(N.lib().phx_tracer_set_stack(self.handle, 1 if shared else 0))
+
     def set_samples(self, n: int) -> None:
         N.check(N.lib().phx_tracer_set_samples(self.handle, n))
 
