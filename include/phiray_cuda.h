@@ -460,6 +460,111 @@ int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t
  * M % 128 == 0, K % 64 == 0, N in {32, 64, 96, 128, 160}. Device pointers. */
 int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, float* D, uint32_t M, uint32_t N, uint32_t K);
 
+/* ---- Learned denoiser layers (no reference counterpart). Activations are
+ * NHWC bf16 with a pixel pitch and a channel offset (both multiples of 8
+ * elements), so a layer reads or writes one channel range of a wider buffer.
+ * 3x3 weights are [cout][Kp] bf16 with k = (3 ty + tx) cin + ci, zero from
+ * K = 9 cin up to Kp (a multiple of 64). All pointers are device pointers;
+ * every call is stream-ordered on the context's stream. ---- */
+
+/* Y[., yo + co] = act(conv3x3(X[., xo + ci]) + bias), stride 1, zero padding 1,
+ * cout (one launch's tile) in {32, 64, 96, 128, 160}; relu selects ReLU,
+ * out_f32 writes fp32 instead of bf16. */
+int32_t phx_nn_conv_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* W, int32_t Kp,
+                        const float* bias, void* Y, int32_t ys, int32_t yo, int32_t cout, int32_t B, int32_t H,
+                        int32_t Wd, int32_t relu, int32_t out_f32);
+/* dWt[k][co] += sum over pixels of im2col(X)[p][k] dY[p][dyo + co]; dWt is
+ * [Kp][cout] fp32 and must be zeroed by the caller. */
+int32_t phx_nn_conv_wgrad(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* dY,
+                          int32_t dys, int32_t dyo, int32_t cout, float* dWt, int32_t Kp, int32_t B, int32_t H,
+                          int32_t Wd);
+/* db[c] += sum over the P pixels of dY[p][dyo + c] (C <= 256). */
+int32_t phx_nn_bias_grad(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, int32_t C, int32_t P, float* db);
+/* dY[p][c] = 0 where Y[p][c] <= 0 (ReLU's gradient through its output). */
+int32_t phx_nn_relu_bwd(phx_ctx ctx, const void* Y, int32_t ys, int32_t yo, void* dY, int32_t dys, int32_t dyo,
+                        int32_t C, int32_t P);
+/* 2x2 average pooling of (B, H, W) into a contiguous (B, H/2, W/2, C). */
+int32_t phx_nn_pool_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t C, int32_t B, int32_t H, int32_t W,
+                        void* Y);
+/* Its gradient, ADDED into dX (B, H, W; pitch dxs, offset dxo). */
+int32_t phx_nn_pool_bwd(phx_ctx ctx, const void* dY, int32_t C, int32_t B, int32_t H, int32_t W, void* dX, int32_t dxs,
+                        int32_t dxo);
+/* Nearest 2x upsampling of a contiguous (B, H/2, W/2, C) into (B, H, W). */
+int32_t phx_nn_up_fwd(phx_ctx ctx, const void* X, int32_t C, int32_t B, int32_t H, int32_t W, void* Y, int32_t ys,
+                      int32_t yo);
+/* Its gradient: dX (B, H/2, W/2, C contiguous) = sum over each 2x2 block. */
+int32_t phx_nn_up_bwd(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, int32_t C, int32_t B, int32_t H, int32_t W,
+                      void* dX);
+/* W2[ci][(8 - tap) cout + co] = W[co][tap cin + ci]: the weights whose 3x3
+ * convolution of dY is the data gradient. W2 is [cin][Kp2]. */
+int32_t phx_nn_flip(phx_ctx ctx, const void* W, int32_t cout, int32_t cin, int32_t Kp, void* W2, int32_t Kp2);
+/* Per-pixel 5x5 kernels (softmax of logits 0..24, pitch 32 fp32) over the
+ * demodulated radiance irr (fp32 x 3), clamped to the valid h x w corner of
+ * the padded Hp x Wp images, remodulated by alb: out = alb * sum w irr.
+ * err = exp(logit 25) - 1e-3 (the error estimate). With ref: *loss += mean
+ * relative squared error (x - r)^2 / (r^2 + 0.01), and dlogits (bf16 pitch
+ * 32) = its gradient plus err_weight times that of the error head's squared
+ * log error. out, err, ref, dlogits, loss may be NULL. */
+int32_t phx_nn_kpn(phx_ctx ctx, const float* logits, const float* irr, const float* alb, const float* ref, int32_t B,
+                   int32_t Hp, int32_t Wp, int32_t h, int32_t w, float* out, float* err, void* dlogits, float* loss,
+                   float err_weight);
+/* Adam (bias-corrected, step >= 1) on a [rows][Kp] fp32 matrix whose first K
+ * columns are live; the gradient is [Kp][rows] when g_transposed, else
+ * [rows][Kp]. wb (nullable) receives the bf16 copy. */
+int32_t phx_nn_adam(phx_ctx ctx, float* w, const float* g, float* m, float* v, void* wb, int32_t rows, int32_t Kp,
+                    int32_t K, int32_t g_transposed, float lr, float b1, float b2, float eps, int32_t step);
+/* Network inputs from a traced px image (w x h) into padded Hp x Wp planes:
+ * feat (16 bf16 channels), irr and alb (fp32 x 3). */
+int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, int32_t w, int32_t h, int32_t Hp, int32_t Wp, void* feat,
+                        float* irr, float* alb);
+/* Per tile x tile block: mean error estimate into tile_err and the count of
+ * tiles above threshold into *fallback (device); every pixel of a tile within
+ * the threshold gets `out` written into the px planes (sums unless keep,
+ * shown, packed), the others keep what the a-trous Denoise wrote. */
+int32_t phx_nn_compose(phx_ctx ctx, uint32_t* px, int32_t w, int32_t h, int32_t Wp, const float* out, const float* err,
+                       int32_t tile, float threshold, int32_t keep, float exposure, float gamma, float* tile_err,
+                       uint32_t* fallback);
+
+/* ---- The learned denoiser: a kernel-predicting U-Net (5 levels of 32, 64,
+ * 96, 128, 160 channels, two 3x3 convolutions per level each way, 5x5
+ * per-pixel kernels) trained and run on the device. ---- */
+typedef struct phx_unet_s* phx_unet;
+/* A network with He-initialised weights drawn from `seed`. */
+int32_t phx_unet_create(phx_ctx ctx, uint64_t seed, phx_unet* out);
+int32_t phx_unet_destroy(phx_unet net);
+/* Parameters in the blob layout: per layer W [cout][9 cin] then b [cout]. */
+int32_t phx_unet_param_count(phx_unet net, uint64_t* count);
+/* Loads fp32 weights (host) and resets the optimiser. */
+int32_t phx_unet_set_params(phx_unet net, const float* params, uint64_t count);
+/* which = 0: the weights; 1: the gradients of the last phx_unet_grads. */
+int32_t phx_unet_get(phx_unet net, int32_t which, float* dst, uint64_t count);
+/* Forward over B padded images Hp x Wp (multiples of 16) of 16-channel
+ * features; out / err as phx_nn_kpn (nullable: logits only). */
+int32_t phx_unet_forward(phx_unet net, const void* feat, const float* irr, const float* alb, int32_t B, int32_t Hp,
+                         int32_t Wp, int32_t h, int32_t w, float* out, float* err);
+/* Forward, loss against ref (added to *loss, device) and all gradients. */
+int32_t phx_unet_grads(phx_unet net, const void* feat, const float* irr, const float* alb, const float* ref, int32_t B,
+                       int32_t Hp, int32_t Wp, int32_t h, int32_t w, float err_weight, float* loss);
+/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) with the last gradients. */
+int32_t phx_unet_adam(phx_unet net, float lr);
+/* phx_unet_grads then phx_unet_adam. */
+int32_t phx_unet_train_step(phx_unet net, const void* feat, const float* irr, const float* alb, const float* ref,
+                            int32_t B, int32_t Hp, int32_t Wp, int32_t h, int32_t w, float err_weight, float lr,
+                            float* loss);
+/* Device pointer of the last forward's head output ([B][Hp][Wp][32] fp32). */
+int32_t phx_unet_logits(phx_unet net, float** logits);
+/* Denoises a traced px image in place: features, network, the a-trous
+ * Denoise (phx_denoise, strength 64/8/40/7), then the learned result on every
+ * tile x tile block whose mean error estimate is <= threshold. With
+ * `fallback` non-NULL, waits and returns the number of tiles that kept the
+ * a-trous result. */
+int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, uint32_t w, uint32_t h, const float view[4], int32_t tile,
+                            float threshold, int32_t keep, uint32_t* fallback);
+/* Tracer::denoise with the learned denoiser (phx_unet_denoise_px on the
+ * tracer's image and last camera's view); nothing traced: no-op. */
+int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, int32_t tile, float threshold, int32_t keep,
+                                   uint32_t* fallback);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,31 @@ SIGNATURES: dict[str, tuple] = {
     "phx_sort_codes_static": (i32, [vp, vp, u32, vp, vp]),
     "phx_karras": (i32, [vp, vp, u32, vp]),
     "phx_gemm_bf16": (i32, [vp, vp, vp, vp, u32, u32, u32]),
+    "phx_nn_conv_fwd": (i32, [vp, vp, i32, i32, i32, vp, i32, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32]),
+    "phx_nn_conv_wgrad": (i32, [vp, vp, i32, i32, i32, vp, i32, i32, i32, vp, i32, i32, i32, i32]),
+    "phx_nn_bias_grad": (i32, [vp, vp, i32, i32, i32, i32, vp]),
+    "phx_nn_relu_bwd": (i32, [vp, vp, i32, i32, vp, i32, i32, i32, i32]),
+    "phx_nn_pool_fwd": (i32, [vp, vp, i32, i32, i32, i32, i32, i32, vp]),
+    "phx_nn_pool_bwd": (i32, [vp, vp, i32, i32, i32, i32, vp, i32, i32]),
+    "phx_nn_up_fwd": (i32, [vp, vp, i32, i32, i32, i32, vp, i32, i32]),
+    "phx_nn_up_bwd": (i32, [vp, vp, i32, i32, i32, i32, i32, i32, vp]),
+    "phx_nn_flip": (i32, [vp, vp, i32, i32, i32, vp, i32]),
+    "phx_nn_kpn": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, C.c_float]),
+    "phx_nn_adam": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, C.c_float, C.c_float, C.c_float, C.c_float, i32]),
+    "phx_nn_features": (i32, [vp, vp, i32, i32, i32, i32, vp, vp, vp]),
+    "phx_nn_compose": (i32, [vp, vp, i32, i32, i32, vp, vp, i32, C.c_float, i32, C.c_float, C.c_float, vp, vp]),
+    "phx_unet_create": (i32, [vp, u64, C.POINTER(vp)]),
+    "phx_unet_destroy": (i32, [vp]),
+    "phx_unet_param_count": (i32, [vp, C.POINTER(u64)]),
+    "phx_unet_set_params": (i32, [vp, vp, u64]),
+    "phx_unet_get": (i32, [vp, i32, vp, u64]),
+    "phx_unet_forward": (i32, [vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]),
+    "phx_unet_grads": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, C.c_float, vp]),
+    "phx_unet_adam": (i32, [vp, C.c_float]),
+    "phx_unet_train_step": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, C.c_float, C.c_float, vp]),
+    "phx_unet_logits": (i32, [vp, C.POINTER(vp)]),
+    "phx_unet_denoise_px": (i32, [vp, vp, u32, u32, f32p, i32, C.c_float, i32, C.POINTER(u32)]),
+    "phx_tracer_denoise_learned": (i32, [vp, vp, i32, C.c_float, i32, C.POINTER(u32)]),
     "phx_skin": (i32, [vp, vp, vp, vp, vp, u32, vp, u32, C.c_float]),
     "phx_face_boxes": (i32, [vp, vp, vp, u32, vp]),
     "phx_denoise": (i32, [vp, vp, u32, u32, f32p, f32p, i32]),

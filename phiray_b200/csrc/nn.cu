@@ -5,27 +5,41 @@
 // the engine's own parity check against a plain matrix product.
 #include <cuda_bf16.h>
 
+#include <atomic>
+
+#include "../../include/phiray_math.h"
 #include "internal.cuh"
 #include "tc.cuh"
+#include "vec.cuh"
 
 namespace phx {
 namespace {
 
 using bf16 = __nv_bfloat16;
 
-// Shared-memory plan of one CTA: A tile, room past it, B tile, room past it.
-// The room keeps every byte the MMAs could address inside the allocation
-// even if a descriptor's strides were read the other way round.
+// Shared-memory plan of one CTA: the A tile, then the B tile (the rooms
+// between them are spare space, zero since the descriptors were validated
+// against plain matrix products).
 template <int N>
 struct Plan {
     static constexpr int A_BYTES = tc::BM * tc::BK * 2;
     static constexpr int B_BYTES = N * tc::BK * 2;
-    static constexpr int A_ROOM = 16 * 1024;
-    static constexpr int B_ROOM = 64 * 1024;
+    static constexpr int A_ROOM = 0;
+    static constexpr int B_ROOM = 0;
     static constexpr int A_OFF = 0;
     static constexpr int B_OFF = A_BYTES + A_ROOM;
     static constexpr int TOTAL = B_OFF + B_BYTES + B_ROOM;
 };
+
+// Raises a kernel's dynamic shared-memory limit once per device.
+template <typename F>
+int32_t smem_limit(F* kernel, int bytes, int device, std::atomic<uint64_t>& done) {
+    const uint64_t bit = 1ull << (device & 63);
+    if (done.load(std::memory_order_acquire) & bit) return PHX_OK;
+    PHX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.fetch_or(bit, std::memory_order_release);
+    return PHX_OK;
+}
 
 __device__ __forceinline__ void fence_barrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -101,17 +115,750 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const bf16* __restrict__ A, c
 template <int N>
 int32_t launch_gemm(Ctx* c, const bf16* A, const bf16* B, float* D, int M, int K) {
     const int smem = Plan<N>::TOTAL;
-    PHX_CUDA(cudaFuncSetAttribute(k_gemm_bf16<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    static std::atomic<uint64_t> done{0};
+    PHX_TRY(smem_limit(k_gemm_bf16<N>, smem, c->device, done));
     k_gemm_bf16<N><<<M / tc::BM, 128, smem, c->stream>>>(A, B, D, M, K, c->status);
     return cuda_check(cudaGetLastError(), "gemm bf16");
 }
+
+// ---- 3x3 convolution as implicit GEMM on the engine ----
+//
+// Activations are NHWC bf16 with a pixel pitch and a channel offset, so a
+// layer can read one channel range of a wider buffer and write into another
+// (the U-Net's skip concatenations cost no copy). Weights are [cout][Kp] bf16,
+// k = (3 * ty + tx) * cin + ci, zero past K = 9 cin up to Kp (a multiple of 64).
+// cin, pitches and offsets are multiples of 8 (16-byte vectors).
+
+struct Geo {
+    int B, H, W;       // images and their size (stride 1, pad 1: same size out)
+    int cin, xs, xo;   // input channels, pixel pitch, channel offset
+    int cout, ys, yo;  // output channels (= the tile's N), pitch, offset
+    int K, Kp;         // 9 cin, padded to a multiple of 64
+};
+
+// A row of the im2col matrix: the pixel's image, y, x (or -1: past the end).
+struct PixRow {
+    int b, y, x;
+};
+
+__device__ __forceinline__ PixRow pix_row(int p, const Geo& g) {
+    const int P = g.B * g.H * g.W;
+    if (p >= P) return PixRow{-1, 0, 0};
+    const int hw = g.H * g.W;
+    const int b = p / hw, rem = p - b * hw;
+    return PixRow{b, rem / g.W, rem - (rem / g.W) * g.W};
+}
+
+// 8 consecutive k (one tap, 8 channels) of im2col row `pr`, 16 bytes.
+__device__ __forceinline__ uint4 im2col_vec(const bf16* __restrict__ X, const PixRow& pr, int k, const Geo& g) {
+    if (pr.b < 0 || k >= g.K) return make_uint4(0, 0, 0, 0);
+    const int tap = k / g.cin, ci = k - tap * g.cin;
+    const int y = pr.y + tap / 3 - 1, x = pr.x + tap % 3 - 1;
+    if (y < 0 || y >= g.H || x < 0 || x >= g.W) return make_uint4(0, 0, 0, 0);
+    return __ldg((const uint4*)(X + ((size_t)(pr.b * g.H + y) * g.W + x) * g.xs + g.xo + ci));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *(const uint32_t*)&v;
+}
+
+// Y = act(conv3x3(X, W) + bias). OUT_F32: fp32 output (the network's head).
+template <int N, bool RELU, bool OUT_F32>
+__global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
+                                                  const float* __restrict__ bias, void* __restrict__ Y, Geo g,
+                                                  uint32_t* status) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    using P = Plan<N>;
+    uint8_t* a_tile = smem + P::A_OFF;
+    uint8_t* b_tile = smem + P::B_OFF;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tc::tmem_alloc(&tmem_base, tc::tmem_cols(N));
+    if (tid == 0) {
+        tc::mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = tmem_base;
+    const int row0 = blockIdx.x * tc::BM;
+    // This thread stages k-vector c = tid % 8 of rows tid / 8 + 16 j.
+    const int c = tid & 7;
+    PixRow rows[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) rows[j] = pix_row(row0 + (tid >> 3) + 16 * j, g);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int kb = 0; kb < g.Kp && ok; kb += tc::BK) {
+        const int k = kb + c * 8;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int r = (tid >> 3) + 16 * j;
+            *(uint4*)(a_tile + tc::tile_off(r, c * 8, tc::BM)) = im2col_vec(X, rows[j], k, g);
+        }
+        for (int v = tid; v < N * 8; v += 128) {
+            const int r = v >> 3, cc = v & 7;
+            *(uint4*)(b_tile + tc::tile_off(r, cc * 8, N)) = __ldg((const uint4*)(Wt + (size_t)r * g.Kp + kb + cc * 8));
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            tc::mma_chunk<N>(tm, a_tile, b_tile, kb == 0);
+            tc::mma_commit(&bar);
+        }
+        ok = tc::mbar_wait(&bar, phase);
+        phase ^= 1u;
+        ok = __syncthreads_and(ok);
+    }
+    tc::fence_after_sync();
+    if (ok) {
+        const int p = row0 + warp * 32 + lane;
+        const bool live = p < g.B * g.H * g.W;
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (!live) continue;
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                v[j] += __ldg(bias + c0 + j);
+                if (RELU) v[j] = fmaxf(v[j], 0.0f);
+            }
+            if (OUT_F32) {
+                float4* o = (float4*)((float*)Y + (size_t)p * g.ys + g.yo + c0);
+#pragma unroll
+                for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                uint4* o = (uint4*)((bf16*)Y + (size_t)p * g.ys + g.yo + c0);
+                o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                  pack_bf16x2(v[6], v[7]));
+                o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                  pack_bf16x2(v[14], v[15]));
+            }
+        }
+    } else if (tid == 0) {
+        atomicOr(status, STATUS_SPIN_LIMIT);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tm, tc::tmem_cols(N));
+}
+
+// Weight gradient: dWt[k][co] += sum over pixels p of im2col(X)[p][k] dY[p][co].
+// GEMM rows = k (a 128-row block per CTA), N = cout, the reduction over the
+// pixel range of this CTA's split, 64 pixels a chunk; the tiles are written
+// transposed from the NHWC vectors. The split partial sums meet in dWt by
+// fp32 atomics. dY has pitch `dys` (cout channels at offset 0).
+template <int N>
+__global__ void __launch_bounds__(128) k_conv_wgrad(const bf16* __restrict__ X, const bf16* __restrict__ dY, int dys,
+                                                    int dyo, float* __restrict__ dWt, Geo g, int chunk_px,
+                                                    uint32_t* status) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    using P = Plan<N>;
+    uint8_t* a_tile = smem + P::A_OFF;
+    uint8_t* b_tile = smem + P::B_OFF;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tc::tmem_alloc(&tmem_base, tc::tmem_cols(N));
+    if (tid == 0) {
+        tc::mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = tmem_base;
+    const int k0 = blockIdx.x * tc::BM;
+    const int P0 = blockIdx.y * chunk_px;
+    const int Ptot = g.B * g.H * g.W;
+    const int P1 = min(P0 + chunk_px, Ptot);
+    // A: this thread stages k-vector rv = tid % 16 (rows rv*8..rv*8+7) at
+    // pixel columns tid / 16 + 8 j.
+    const int rv = tid & 15;
+    const int kv = k0 + rv * 8;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int pb = P0; pb < P1 && ok; pb += tc::BK) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int col = (tid >> 4) + 8 * j;
+            const PixRow pr = pix_row(pb + col < P1 ? pb + col : Ptot, g);
+            const uint4 val = im2col_vec(X, pr, kv, g);
+            const bf16* e = (const bf16*)&val;
+#pragma unroll
+            for (int q = 0; q < 8; q++) *(bf16*)(a_tile + tc::tile_off(rv * 8 + q, col, tc::BM)) = e[q];
+        }
+        for (int v = tid; v < N * 8; v += 128) {
+            const int bv = v % (N / 8), col = v / (N / 8);
+            const int p = pb + col;
+            uint4 val = make_uint4(0, 0, 0, 0);
+            if (p < P1) val = __ldg((const uint4*)(dY + (size_t)p * dys + dyo + bv * 8));
+            const bf16* e = (const bf16*)&val;
+#pragma unroll
+            for (int q = 0; q < 8; q++) *(bf16*)(b_tile + tc::tile_off(bv * 8 + q, col, N)) = e[q];
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            tc::mma_chunk<N>(tm, a_tile, b_tile, pb == P0);
+            tc::mma_commit(&bar);
+        }
+        ok = tc::mbar_wait(&bar, phase);
+        phase ^= 1u;
+        ok = __syncthreads_and(ok);
+    }
+    tc::fence_after_sync();
+    if (ok && P0 < P1) {
+        const int k = k0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (k < g.Kp) {
+#pragma unroll
+                for (int j = 0; j < 16; j++) atomicAdd(dWt + (size_t)k * N + c0 + j, v[j]);
+            }
+        }
+    } else if (!ok && tid == 0) {
+        atomicOr(status, STATUS_SPIN_LIMIT);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tm, tc::tmem_cols(N));
+}
+
+// ---- the network's other layers (elementwise, fp32 math on bf16 data) ----
+
+__device__ __forceinline__ float bf(const bf16 v) { return __bfloat162float(v); }
+
+// db[c] += sum over pixels of dY[p][dyo + c].
+__global__ void k_bias_grad(const bf16* __restrict__ dY, int dys, int dyo, int C, int P, float* __restrict__ db) {
+    const int c = threadIdx.x;  // blockDim.x = C (<= 256)
+    float acc = 0.0f;
+    for (int p = blockIdx.x; p < P; p += gridDim.x) acc += bf(dY[(size_t)p * dys + dyo + c]);
+    if (c < C) atomicAdd(db + c, acc);
+}
+
+// dY *= (Y > 0): ReLU's gradient through its output.
+__global__ void k_relu_bwd(const bf16* __restrict__ Y, int ys, int yo, bf16* dY, int dys, int dyo, int C, int P) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)P * C) return;
+    const size_t p = i / C;
+    const int c = (int)(i - p * C);
+    if (!(bf(Y[p * ys + yo + c]) > 0.0f)) dY[p * dys + dyo + c] = __float2bfloat16(0.0f);
+}
+
+// 2x2 average pool: X (B, H, W, pitch xs, offset xo) -> Y (B, H/2, W/2, C contiguous).
+__global__ void k_pool_fwd(const bf16* __restrict__ X, int xs, int xo, int C, int B, int H, int W, bf16* __restrict__ Y) {
+    const int h = H / 2, w = W / 2;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)B * h * w * C) return;
+    const int c = (int)(i % C);
+    const size_t q = i / C;
+    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
+    const size_t p00 = ((size_t)(b * H + 2 * y) * W + 2 * x);
+    const float s = bf(X[p00 * xs + xo + c]) + bf(X[(p00 + 1) * xs + xo + c]) + bf(X[(p00 + W) * xs + xo + c]) +
+                    bf(X[(p00 + W + 1) * xs + xo + c]);
+    Y[i] = __float2bfloat16(0.25f * s);
+}
+
+// Its gradient, added into dX (B, H, W, pitch dxs, offset dxo).
+__global__ void k_pool_bwd(const bf16* __restrict__ dY, int C, int B, int H, int W, bf16* dX, int dxs, int dxo) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)B * H * W * C) return;
+    const int c = (int)(i % C);
+    const size_t p = i / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+    const float g = 0.25f * bf(dY[((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]);
+    bf16* d = dX + p * dxs + dxo + c;
+    *d = __float2bfloat16(bf(*d) + g);
+}
+
+// Nearest 2x upsample: X (B, H/2, W/2, C contiguous) -> Y (B, H, W, pitch ys, offset yo).
+__global__ void k_up_fwd(const bf16* __restrict__ X, int C, int B, int H, int W, bf16* __restrict__ Y, int ys, int yo) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)B * H * W * C) return;
+    const int c = (int)(i % C);
+    const size_t p = i / C;
+    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+    Y[p * ys + yo + c] = X[((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c];
+}
+
+// Its gradient: dX (B, H/2, W/2, C contiguous) = sum of the 4 children.
+__global__ void k_up_bwd(const bf16* __restrict__ dY, int dys, int dyo, int C, int B, int H, int W, bf16* __restrict__ dX) {
+    const int h = H / 2, w = W / 2;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)B * h * w * C) return;
+    const int c = (int)(i % C);
+    const size_t q = i / C;
+    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
+    const size_t p00 = ((size_t)(b * H + 2 * y) * W + 2 * x);
+    const float s = bf(dY[p00 * dys + dyo + c]) + bf(dY[(p00 + 1) * dys + dyo + c]) + bf(dY[(p00 + W) * dys + dyo + c]) +
+                    bf(dY[(p00 + W + 1) * dys + dyo + c]);
+    dX[i] = __float2bfloat16(s);
+}
+
+// W2[ci][(8 - tap) * cout + co] = W[co][tap * cin + ci]: the weights of the
+// data-gradient convolution (a 3x3 convolution of dY).
+__global__ void k_flip(const bf16* __restrict__ W, int cout, int cin, int Kp, bf16* __restrict__ W2, int Kp2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)cin * Kp2) return;
+    const int ci = (int)(i / Kp2), k2 = (int)(i - (size_t)ci * Kp2);
+    float v = 0.0f;
+    if (k2 < 9 * cout) {
+        const int tap2 = k2 / cout, co = k2 - tap2 * cout;
+        v = bf(W[(size_t)co * Kp + (8 - tap2) * cin + ci]);
+    }
+    W2[i] = __float2bfloat16(v);
+}
+
+// Kernel prediction on demodulated radiance. Per pixel the softmax of
+// logits 0..24 weights the 5 x 5 neighbourhood (clamped to the valid h x w
+// image) of the irradiance irr = radiance / albedo', and the result is
+// remodulated: out = albedo' * sum_t w_t irr[nb_t]. Logit 25 is the
+// network's estimate e of log(relative error + 1e-3) at the pixel; `err`
+// receives exp(e) - 1e-3. With `ref`, adds to *loss the mean over valid
+// pixels and channels of (out - ref)^2 / (ref^2 + 0.01) and writes the
+// gradient of that loss plus err_weight * mean (e - log(rel_p + 1e-3))^2
+// (rel_p the pixel's own relative error, held constant) to dlogits (bf16,
+// pitch 32; zero on padding pixels and on logits 26..31).
+// Buffers are [B][Hp][Wp] x channels; pixels with y >= h or x >= w are padding.
+__global__ void k_kpn(const float* __restrict__ logits, const float* __restrict__ irr, const float* __restrict__ alb,
+                      const float* __restrict__ ref, int B, int Hp, int Wp, int h, int w, float* __restrict__ out,
+                      float* __restrict__ err, bf16* __restrict__ dlogits, float* loss, float scale, float err_weight) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int P = B * Hp * Wp;
+    float lsum = 0.0f;
+    if (p < P) {
+        const int x = p % Wp, y = (p / Wp) % Hp, b = p / (Wp * Hp);
+        const bool valid = y < h && x < w;
+        if (!valid) {
+            if (out)
+                for (int c = 0; c < 3; c++) out[(size_t)p * 3 + c] = 0.0f;
+            if (err) err[p] = 0.0f;
+            if (ref && dlogits)
+                for (int t = 0; t < 32; t++) dlogits[(size_t)p * 32 + t] = __float2bfloat16(0.0f);
+        } else {
+            float wt[25], mx = -3.0e38f;
+#pragma unroll
+            for (int t = 0; t < 25; t++) {
+                wt[t] = logits[(size_t)p * 32 + t];
+                mx = fmaxf(mx, wt[t]);
+            }
+            float z = 0.0f;
+#pragma unroll
+            for (int t = 0; t < 25; t++) {
+                wt[t] = pm_exp(wt[t] - mx);
+                z += wt[t];
+            }
+            const float iz = 1.0f / z;
+            float s[3] = {0.0f, 0.0f, 0.0f};
+            int nb[25];
+#pragma unroll
+            for (int t = 0; t < 25; t++) {
+                wt[t] *= iz;
+                const int yy = min(max(y + t / 5 - 2, 0), h - 1), xx = min(max(x + t % 5 - 2, 0), w - 1);
+                nb[t] = (b * Hp + yy) * Wp + xx;
+#pragma unroll
+                for (int c = 0; c < 3; c++) s[c] += wt[t] * irr[(size_t)nb[t] * 3 + c];
+            }
+            float a[3], o[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                a[c] = alb[(size_t)p * 3 + c];
+                o[c] = a[c] * s[c];
+            }
+            if (out)
+                for (int c = 0; c < 3; c++) out[(size_t)p * 3 + c] = o[c];
+            const float e = logits[(size_t)p * 32 + 25];
+            if (err) err[p] = fmaxf(pm_exp(e) - 1.0e-3f, 0.0f);
+            if (ref) {
+                float go[3], rel = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float r = ref[(size_t)p * 3 + c], d = o[c] - r, den = r * r + 0.01f;
+                    rel += d * d / den;
+                    go[c] = 2.0f * d / den * scale * a[c];
+                }
+                lsum = rel;
+                const float target = pm_log2(rel * (1.0f / 3.0f) + 1.0e-3f) * 0.693147182f;
+                const float ge = 2.0f * err_weight * (e - target) * (3.0f * scale);
+                float gw[25], dot = 0.0f;
+#pragma unroll
+                for (int t = 0; t < 25; t++) {
+                    const float* q = irr + (size_t)nb[t] * 3;
+                    gw[t] = go[0] * q[0] + go[1] * q[1] + go[2] * q[2];
+                    dot += wt[t] * gw[t];
+                }
+                if (dlogits) {
+                    bf16* d = dlogits + (size_t)p * 32;
+#pragma unroll
+                    for (int t = 0; t < 25; t++) d[t] = __float2bfloat16(wt[t] * (gw[t] - dot));
+                    d[25] = __float2bfloat16(ge);
+#pragma unroll
+                    for (int t = 26; t < 32; t++) d[t] = __float2bfloat16(0.0f);
+                }
+            }
+        }
+    }
+    if (ref && loss) {
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(loss, lsum * scale);
+    }
+}
+
+// Adam on a weight matrix held [rows][Kp] whose gradient is [Kp][rows]
+// (transposed), or on a plain vector (gt == false). Writes the bf16 copy.
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       bf16* __restrict__ wb, int rows, int Kp, int K, bool gt, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)rows * Kp) return;
+    const int r = (int)(i / Kp), k = (int)(i - (size_t)r * Kp);
+    if (k >= K) {
+        if (wb) wb[i] = __float2bfloat16(0.0f);
+        return;
+    }
+    const float gr = gt ? g[(size_t)k * rows + r] : g[i];
+    const float mm = b1 * m[i] + (1.0f - b1) * gr;
+    const float vv = b2 * v[i] + (1.0f - b2) * gr * gr;
+    m[i] = mm;
+    v[i] = vv;
+    const float upd = lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+    const float nw = w[i] - upd;
+    w[i] = nw;
+    if (wb) wb[i] = __float2bfloat16(nw);
+}
+
+__device__ __forceinline__ float finite_or_zero(float v) { return isfinite(v) ? v : 0.0f; }
+
+// Network inputs from a traced image (px planes, src/trace/read.rs:37-56).
+// Per pixel of the padded image (Hp x Wp; padding pixels all zero) 16 bf16
+// channels: log(1 + radiance) 3, log(1 + irradiance) 3, albedo 3, normal 3,
+// depth / (1 + |depth|), the fraction of samples that met something,
+// log2(samples) / 8, 0; a plane value that is not finite reads as 0. Radiance is the mean over the samples that met
+// something (Tracer::radiance, read.rs:241-251); albedo' = max(albedo, 0.05)
+// per channel; irradiance = radiance / albedo'. Also writes irr and albedo'
+// (fp32 x 3 each), the planes the predicted kernels filter and remodulate.
+__global__ void k_features(const uint32_t* __restrict__ px, int w, int h, int Hp, int Wp, bf16* __restrict__ feat,
+                           float* __restrict__ irr, float* __restrict__ alb) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Hp * Wp) return;
+    const int x = q % Wp, y = q / Wp;
+    float f[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) f[j] = 0.0f;
+    float ir[3] = {0.0f, 0.0f, 0.0f}, ad[3] = {0.0f, 0.0f, 0.0f};
+    if (x < w && y < h) {
+        const size_t n = (size_t)w * h, i = (size_t)y * w + x;
+        const uint32_t cnt = px[31 * n + i];
+        const float k = (float)max(cnt, 1u);
+        const float gone = __uint_as_float(px[33 * n + i]);
+        const float met = fmaxf(k - gone, 1.0f);
+        const float ln2 = 0.693147182f;
+        float nn = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            // a sample that overflowed (or a NaN) gives no input rather than a poisoned one
+            const float rad = finite_or_zero(fmaxf(__uint_as_float(px[n + 3 * i + c]) / met, 0.0f));
+            const float al = finite_or_zero(__uint_as_float(px[7 * n + 3 * i + c]) / k);
+            ad[c] = fmaxf(al, 0.05f);
+            ir[c] = rad / ad[c];
+            f[c] = pm_log2(1.0f + rad) * ln2;
+            f[3 + c] = pm_log2(1.0f + ir[c]) * ln2;
+            f[6 + c] = al;
+            f[9 + c] = finite_or_zero(__uint_as_float(px[10 * n + 3 * i + c]));
+            nn += f[9 + c] * f[9 + c];
+        }
+        const float inv = nn > 0.0f ? 1.0f / sqrtf(nn) : 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) f[9 + c] *= inv;
+        const float d = finite_or_zero(__uint_as_float(px[13 * n + i]) / k);
+        f[12] = d / (1.0f + fabsf(d));
+        f[13] = fmaxf(1.0f - gone / k, 0.0f);
+        f[14] = pm_log2(k) * 0.125f;
+    }
+    uint4* o = (uint4*)(feat + (size_t)q * 16);
+    o[0] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+    o[1] = make_uint4(pack_bf16x2(f[8], f[9]), pack_bf16x2(f[10], f[11]), pack_bf16x2(f[12], f[13]),
+                      pack_bf16x2(f[14], f[15]));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        irr[(size_t)q * 3 + c] = ir[c];
+        alb[(size_t)q * 3 + c] = ad[c];
+    }
+}
+
+// Mean of the per-pixel error estimate over each ts x ts tile of the valid
+// image (one block per tile); counts the tiles above `threshold`.
+__global__ void k_tile_err(const float* __restrict__ err, int w, int h, int Wp, int ts, float threshold,
+                           float* __restrict__ tile_err, uint32_t* fallback) {
+    const int tx = blockIdx.x, ty = blockIdx.y;
+    const int x0 = tx * ts, y0 = ty * ts;
+    const int tw = min(ts, w - x0), th = min(ts, h - y0);
+    float s = 0.0f;
+    for (int j = threadIdx.x; j < tw * th; j += blockDim.x) {
+        const int yy = y0 + j / tw, xx = x0 + j % tw;
+        s += err[(size_t)yy * Wp + xx];
+    }
+    __shared__ float part[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int j = 0; j < (int)(blockDim.x >> 5); j++) t += part[j];
+        t /= (float)(tw * th);
+        tile_err[ty * gridDim.x + tx] = t;
+        if (!(t <= threshold)) atomicAdd(fallback, 1u);
+    }
+}
+
+// Writes the learned result into the px planes for every pixel whose tile
+// estimate is within `threshold` (the rest keep what Denoise wrote):
+// the scene-linear sums so that Tracer::radiance returns `out` (unless
+// keep), the shown value and the packed display pixel, as the last Denoise
+// round does (denoise.wgsl, Standard view transform).
+__global__ void k_compose(const float* __restrict__ out, const float* __restrict__ tile_err, int w, int h, int Wp,
+                          int ts, float threshold, int keep, float exposure, float gamma, uint32_t* __restrict__ px) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int tiles_x = (w + ts - 1) / ts;
+    if (!(tile_err[(y / ts) * tiles_x + x / ts] <= threshold)) return;
+    const uint32_t n = (uint32_t)w * h, i = (uint32_t)y * w + x;
+    const uint32_t cnt = px[31 * n + i];
+    const float k = 1.0f / (float)(cnt > 1 ? cnt : 1);
+    const float gone = __uint_as_float(px[33 * n + i]);
+    const float met = 1.0f - gone * k;
+    const size_t q = (size_t)y * Wp + x;
+    f3 lin = mk(out[q * 3], out[q * 3 + 1], out[q * 3 + 2]);
+    if (!(met > 0.5f * k)) lin = mk(0.0f);
+    if (!keep) {
+        const float m = fmaxf((float)(cnt > 1 ? cnt : 1) - gone, 1.0f);
+        px[n + 3 * i] = __float_as_uint(lin.x * m);
+        px[n + 3 * i + 1] = __float_as_uint(lin.y * m);
+        px[n + 3 * i + 2] = __float_as_uint(lin.z * m);
+    }
+    const float cov = __uint_as_float(px[23 * n + i]) * k;
+    const f3 grid = mk(__uint_as_float(px[20 * n + 3 * i]), __uint_as_float(px[20 * n + 3 * i + 1]),
+                       __uint_as_float(px[20 * n + 3 * i + 2])) * k;
+    const f3 shown = view_transform_std(lin, exposure, gamma) * (1.0f - cov) + grid;
+    px[4 * n + 3 * i] = __float_as_uint(shown.x);
+    px[4 * n + 3 * i + 1] = __float_as_uint(shown.y);
+    px[4 * n + 3 * i + 2] = __float_as_uint(shown.z);
+    px[i] = pack_rgba(shown, __uint_as_float(px[24 * n + i]) * k);
+}
+
+template <int N, bool RELU, bool F32>
+int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
+    const int smem = Plan<N>::TOTAL;
+    static std::atomic<uint64_t> done{0};
+    PHX_TRY(smem_limit(k_conv_fwd<N, RELU, F32>, smem, c->device, done));
+    const int P = g.B * g.H * g.W;
+    k_conv_fwd<N, RELU, F32><<<(P + tc::BM - 1) / tc::BM, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
+    return cuda_check(cudaGetLastError(), "conv fwd");
+}
+
+template <bool RELU, bool F32>
+int32_t conv_fwd_any(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
+    switch (g.cout) {
+        case 32: return conv_fwd_n<32, RELU, F32>(c, X, W, bias, Y, g);
+        case 64: return conv_fwd_n<64, RELU, F32>(c, X, W, bias, Y, g);
+        case 96: return conv_fwd_n<96, RELU, F32>(c, X, W, bias, Y, g);
+        case 128: return conv_fwd_n<128, RELU, F32>(c, X, W, bias, Y, g);
+        case 160: return conv_fwd_n<160, RELU, F32>(c, X, W, bias, Y, g);
+    }
+    return fail(PHX_ERR_INVALID, "conv: output tile of %d channels (32, 64, 96, 128 or 160)", g.cout);
+}
+
+template <int N>
+int32_t wgrad_n(Ctx* c, const bf16* X, const bf16* dY, int dys, int dyo, float* dWt, const Geo& g) {
+    const int smem = Plan<N>::TOTAL;
+    static std::atomic<uint64_t> done{0};
+    PHX_TRY(smem_limit(k_conv_wgrad<N>, smem, c->device, done));
+    const int P = g.B * g.H * g.W;
+    // Split the pixel reduction so the grid covers the SMs a few times.
+    const int kblocks = (g.Kp + tc::BM - 1) / tc::BM;
+    int splits = (c->sms * 2 + kblocks - 1) / kblocks;
+    int chunk = (P + splits - 1) / splits;
+    chunk = (chunk + tc::BK - 1) / tc::BK * tc::BK;
+    splits = (P + chunk - 1) / chunk;
+    k_conv_wgrad<N><<<dim3(kblocks, splits), 128, smem, c->stream>>>(X, dY, dys, dyo, dWt, g, chunk, c->status);
+    return cuda_check(cudaGetLastError(), "conv wgrad");
+}
+
+int32_t check_geo(const Geo& g) {
+    if (g.B <= 0 || g.H <= 0 || g.W <= 0) return fail(PHX_ERR_INVALID, "conv: empty image");
+    if (g.cin % 8 || g.xs % 8 || g.xo % 8 || g.ys % 8 || g.yo % 8)
+        return fail(PHX_ERR_INVALID, "conv: channels, pitches and offsets must be multiples of 8");
+    if (g.Kp % 64 || g.Kp < g.K) return fail(PHX_ERR_INVALID, "conv: Kp %d must cover K %d in steps of 64", g.Kp, g.K);
+    if (g.xo < 0 || g.xo + g.cin > g.xs || g.yo < 0 || g.yo + g.cout > g.ys)
+        return fail(PHX_ERR_INVALID, "conv: channel window outside the pixel pitch");
+    return PHX_OK;
+}
+
+uint32_t blocks_for(size_t n) { return (uint32_t)((n + 255) / 256); }
 
 }  // namespace
 }  // namespace phx
 
 using namespace phx;
 
-extern "C" int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, float* D, uint32_t M, uint32_t N,
+extern "C" {
+
+int32_t phx_nn_conv_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* W, int32_t Kp,
+                        const float* bias, void* Y, int32_t ys, int32_t yo, int32_t cout, int32_t B, int32_t H,
+                        int32_t Wd, int32_t relu, int32_t out_f32) {
+    if (!ctx || !X || !W || !bias || !Y) return fail(PHX_ERR_INVALID, "null argument");
+    Geo g{B, H, Wd, cin, xs, xo, cout, ys, yo, 9 * cin, Kp};
+    PHX_TRY(check_geo(g));
+    PHX_TRY(use(&ctx->c));
+    const bf16* x = (const bf16*)X;
+    const bf16* w = (const bf16*)W;
+    if (out_f32) return relu ? conv_fwd_any<true, true>(&ctx->c, x, w, bias, Y, g)
+                             : conv_fwd_any<false, true>(&ctx->c, x, w, bias, Y, g);
+    return relu ? conv_fwd_any<true, false>(&ctx->c, x, w, bias, Y, g) : conv_fwd_any<false, false>(&ctx->c, x, w, bias, Y, g);
+}
+
+int32_t phx_nn_conv_wgrad(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* dY,
+                          int32_t dys, int32_t dyo, int32_t cout, float* dWt, int32_t Kp, int32_t B, int32_t H,
+                          int32_t Wd) {
+    if (!ctx || !X || !dY || !dWt) return fail(PHX_ERR_INVALID, "null argument");
+    Geo g{B, H, Wd, cin, xs, xo, cout, cout, 0, 9 * cin, Kp};
+    PHX_TRY(check_geo(g));
+    if (dys % 8 || dyo % 8 || dyo < 0 || dyo + cout > dys)
+        return fail(PHX_ERR_INVALID, "wgrad: dY pitch/offset must be multiples of 8 holding cout channels");
+    PHX_TRY(use(&ctx->c));
+    const bf16* x = (const bf16*)X;
+    const bf16* d = (const bf16*)dY;
+    switch (cout) {
+        case 32: return wgrad_n<32>(&ctx->c, x, d, dys, dyo, dWt, g);
+        case 64: return wgrad_n<64>(&ctx->c, x, d, dys, dyo, dWt, g);
+        case 96: return wgrad_n<96>(&ctx->c, x, d, dys, dyo, dWt, g);
+        case 128: return wgrad_n<128>(&ctx->c, x, d, dys, dyo, dWt, g);
+        case 160: return wgrad_n<160>(&ctx->c, x, d, dys, dyo, dWt, g);
+    }
+    return fail(PHX_ERR_INVALID, "wgrad: %d output channels (32, 64, 96, 128 or 160)", cout);
+}
+
+int32_t phx_nn_bias_grad(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, int32_t C, int32_t P, float* db) {
+    if (!ctx || !dY || !db || C <= 0 || C > 256 || P < 0 || dyo < 0 || dyo + C > dys)
+        return fail(PHX_ERR_INVALID, "bias grad arguments");
+    if (P == 0) return PHX_OK;
+    PHX_TRY(use(&ctx->c));
+    k_bias_grad<<<std::min(P, 1024), C, 0, ctx->c.stream>>>((const bf16*)dY, dys, dyo, C, P, db);
+    return cuda_check(cudaGetLastError(), "bias grad");
+}
+
+int32_t phx_nn_relu_bwd(phx_ctx ctx, const void* Y, int32_t ys, int32_t yo, void* dY, int32_t dys, int32_t dyo,
+                        int32_t C, int32_t P) {
+    if (!ctx || !Y || !dY || C <= 0 || P <= 0 || yo < 0 || yo + C > ys || dyo < 0 || dyo + C > dys)
+        return fail(PHX_ERR_INVALID, "relu bwd arguments");
+    PHX_TRY(use(&ctx->c));
+    k_relu_bwd<<<blocks_for((size_t)P * C), 256, 0, ctx->c.stream>>>((const bf16*)Y, ys, yo, (bf16*)dY, dys, dyo, C, P);
+    return cuda_check(cudaGetLastError(), "relu bwd");
+}
+
+int32_t phx_nn_pool_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t C, int32_t B, int32_t H, int32_t W,
+                        void* Y) {
+    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || xo < 0 || xo + C > xs)
+        return fail(PHX_ERR_INVALID, "pool arguments");
+    PHX_TRY(use(&ctx->c));
+    k_pool_fwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * C), 256, 0, ctx->c.stream>>>((const bf16*)X, xs, xo, C, B, H,
+                                                                                        W, (bf16*)Y);
+    return cuda_check(cudaGetLastError(), "pool fwd");
+}
+
+int32_t phx_nn_pool_bwd(phx_ctx ctx, const void* dY, int32_t C, int32_t B, int32_t H, int32_t W, void* dX, int32_t dxs,
+                        int32_t dxo) {
+    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || dxo < 0 || dxo + C > dxs)
+        return fail(PHX_ERR_INVALID, "pool arguments");
+    PHX_TRY(use(&ctx->c));
+    k_pool_bwd<<<blocks_for((size_t)B * H * W * C), 256, 0, ctx->c.stream>>>((const bf16*)dY, C, B, H, W, (bf16*)dX, dxs,
+                                                                              dxo);
+    return cuda_check(cudaGetLastError(), "pool bwd");
+}
+
+int32_t phx_nn_up_fwd(phx_ctx ctx, const void* X, int32_t C, int32_t B, int32_t H, int32_t W, void* Y, int32_t ys,
+                      int32_t yo) {
+    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || yo < 0 || yo + C > ys)
+        return fail(PHX_ERR_INVALID, "upsample arguments");
+    PHX_TRY(use(&ctx->c));
+    k_up_fwd<<<blocks_for((size_t)B * H * W * C), 256, 0, ctx->c.stream>>>((const bf16*)X, C, B, H, W, (bf16*)Y, ys, yo);
+    return cuda_check(cudaGetLastError(), "up fwd");
+}
+
+int32_t phx_nn_up_bwd(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, int32_t C, int32_t B, int32_t H, int32_t W,
+                      void* dX) {
+    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || dyo < 0 || dyo + C > dys)
+        return fail(PHX_ERR_INVALID, "upsample arguments");
+    PHX_TRY(use(&ctx->c));
+    k_up_bwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * C), 256, 0, ctx->c.stream>>>((const bf16*)dY, dys, dyo, C, B,
+                                                                                      H, W, (bf16*)dX);
+    return cuda_check(cudaGetLastError(), "up bwd");
+}
+
+int32_t phx_nn_flip(phx_ctx ctx, const void* W, int32_t cout, int32_t cin, int32_t Kp, void* W2, int32_t Kp2) {
+    if (!ctx || !W || !W2 || Kp2 < 9 * cout || Kp2 % 64) return fail(PHX_ERR_INVALID, "flip arguments");
+    PHX_TRY(use(&ctx->c));
+    k_flip<<<blocks_for((size_t)cin * Kp2), 256, 0, ctx->c.stream>>>((const bf16*)W, cout, cin, Kp, (bf16*)W2, Kp2);
+    return cuda_check(cudaGetLastError(), "flip");
+}
+
+int32_t phx_nn_kpn(phx_ctx ctx, const float* logits, const float* irr, const float* alb, const float* ref, int32_t B,
+                   int32_t Hp, int32_t Wp, int32_t h, int32_t w, float* out, float* err, void* dlogits, float* loss,
+                   float err_weight) {
+    if (!ctx || !logits || !irr || !alb) return fail(PHX_ERR_INVALID, "null argument");
+    if (B <= 0 || h <= 0 || w <= 0 || h > Hp || w > Wp) return fail(PHX_ERR_INVALID, "kpn: bad image size");
+    PHX_TRY(use(&ctx->c));
+    const int P = B * Hp * Wp;
+    const float scale = 1.0f / (3.0f * (float)B * (float)h * (float)w);
+    k_kpn<<<(P + 255) / 256, 256, 0, ctx->c.stream>>>(logits, irr, alb, ref, B, Hp, Wp, h, w, out, err, (bf16*)dlogits,
+                                                      loss, scale, err_weight);
+    return cuda_check(cudaGetLastError(), "kpn");
+}
+
+int32_t phx_nn_adam(phx_ctx ctx, float* w, const float* g, float* m, float* v, void* wb, int32_t rows, int32_t Kp,
+                    int32_t K, int32_t g_transposed, float lr, float b1, float b2, float eps, int32_t step) {
+    if (!ctx || !w || !g || !m || !v || step < 1) return fail(PHX_ERR_INVALID, "adam arguments");
+    PHX_TRY(use(&ctx->c));
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adam<<<blocks_for((size_t)rows * Kp), 256, 0, ctx->c.stream>>>(w, g, m, v, (bf16*)wb, rows, Kp, K, g_transposed != 0,
+                                                                    lr, b1, b2, eps, c1, c2);
+    return cuda_check(cudaGetLastError(), "adam");
+}
+
+int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, int32_t w, int32_t h, int32_t Hp, int32_t Wp, void* feat,
+                        float* irr, float* alb) {
+    if (!ctx || !px || !feat || !irr || !alb || w <= 0 || h <= 0 || Hp < h || Wp < w)
+        return fail(PHX_ERR_INVALID, "features arguments");
+    PHX_TRY(use(&ctx->c));
+    k_features<<<(Hp * Wp + 255) / 256, 256, 0, ctx->c.stream>>>(px, w, h, Hp, Wp, (bf16*)feat, irr, alb);
+    return cuda_check(cudaGetLastError(), "features");
+}
+
+int32_t phx_nn_compose(phx_ctx ctx, uint32_t* px, int32_t w, int32_t h, int32_t Wp, const float* out, const float* err,
+                       int32_t tile, float threshold, int32_t keep, float exposure, float gamma, float* tile_err,
+                       uint32_t* fallback) {
+    if (!ctx || !px || !out || !err || !tile_err || !fallback || tile <= 0 || w <= 0 || h <= 0 || Wp < w)
+        return fail(PHX_ERR_INVALID, "compose arguments");
+    PHX_TRY(use(&ctx->c));
+    const dim3 tiles((w + tile - 1) / tile, (h + tile - 1) / tile);
+    PHX_CUDA(cudaMemsetAsync(fallback, 0, sizeof(uint32_t), ctx->c.stream));
+    k_tile_err<<<tiles, 256, 0, ctx->c.stream>>>(err, w, h, Wp, tile, threshold, tile_err, fallback);
+    PHX_CUDA(cudaGetLastError());
+    const dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
+    k_compose<<<grid, block, 0, ctx->c.stream>>>(out, tile_err, w, h, Wp, tile, threshold, keep, exposure, gamma, px);
+    return cuda_check(cudaGetLastError(), "compose");
+}
+
+int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, float* D, uint32_t M, uint32_t N,
                                  uint32_t K) {
     if (!ctx || !A || !B || !D) return fail(PHX_ERR_INVALID, "null argument");
     if (M == 0 || M % 128 || K == 0 || K % 64)
@@ -128,3 +875,5 @@ extern "C" int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, floa
     }
     return fail(PHX_ERR_INVALID, "gemm: N %u must be 32, 64, 96, 128 or 160", N);
 }
+
+}  // extern "C"

@@ -1565,6 +1565,16 @@ int32_t phx_tracer_denoise(phx_tracer tr, int32_t keep) {
                        strength, tr->last.view, keep);
 }
 
+int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, int32_t tile, float threshold, int32_t keep,
+                                   uint32_t* fallback) {
+    if (!tr || !net) return fail(PHX_ERR_INVALID, "null argument");
+    if (fallback) *fallback = 0;
+    if (!tr->px.ptr || !tr->have_last) return PHX_OK;  // nothing traced: read.rs:90
+    PHX_TRY(use(tr->ctx));
+    return phx_unet_denoise_px(net, (uint32_t*)tr->px.ptr, tr->w, tr->h, tr->last.view, tile, threshold, keep,
+                               fallback);
+}
+
 int32_t phx_tracer_time(phx_tracer tr, float* gpu_ms, uint64_t* rays) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
     PHX_TRY(use(tr->ctx));

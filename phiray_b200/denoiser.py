@@ -1,0 +1,156 @@
+"""The learned denoiser over the C ABI: ``Unet`` (phx_unet_*) and the
+per-layer calls its parity tests drive one at a time (phx_nn_*).
+
+phiray has no learned denoiser; ``Unet.denoise(tracer)`` is the drop-in
+beside ``Tracer.denoise`` (src/trace/read.rs:78-119): the same px image is
+filtered in place, and every tile whose error estimate is above the
+threshold keeps the a-trous result of the plain ``Denoise``.
+
+Weights files (``.phxu``): magic ``PHXU``, u32 version 1, u64 count, then
+``count`` little-endian float32 in the blob layout (per layer W [cout][9 cin]
+with k = (3 ty + tx) cin + ci, then b [cout]).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import struct
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+from .gpu import Gpu, devptr
+
+HERE = Path(__file__).resolve().parent
+WEIGHTS = HERE / "weights" / "kpcn.phxu"
+SEED = 0x2545F491
+
+LAYERS = [(16, 32), (32, 32), (32, 64), (64, 64), (64, 96), (96, 96), (96, 128), (128, 128), (128, 160),
+          (160, 160), (288, 128), (128, 128), (224, 96), (96, 96), (160, 64), (64, 64), (96, 32), (32, 32), (32, 32)]
+FEATURES = 16
+HEAD = 32
+TILE = 16
+# Mean predicted relative error of a tile above which the a-trous result is kept.
+THRESHOLD = 0.05
+
+
+def padded(n: int) -> int:
+    """Image side padded to the network's multiple of 16."""
+    return (n + 15) // 16 * 16
+
+
+def flops_per_pixel() -> int:
+    """Multiply-adds x 2 of one forward pass per full-resolution pixel."""
+    lv = [0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 3, 3, 2, 2, 1, 1, 0, 0, 0]
+    mac = sum(9 * ci * co / 4 ** l for (ci, co), l in zip(LAYERS, lv))
+    return int(round(2 * mac))
+
+
+def read_weights(path) -> np.ndarray:
+    raw = Path(path).read_bytes()
+    magic, ver, count = struct.unpack_from("<4sIQ", raw, 0)
+    if magic != b"PHXU" or ver != 1:
+        raise ValueError(f"{path}: not a version-1 phxu weights file")
+    data = np.frombuffer(raw, dtype="<f4", count=count, offset=16)
+    return data.astype(np.float32)
+
+
+def write_weights(path, params: np.ndarray) -> None:
+    p = np.ascontiguousarray(params, dtype="<f4")
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    Path(path).write_bytes(struct.pack("<4sIQ", b"PHXU", 1, p.size) + p.tobytes())
+
+
+class Unet:
+    """The kernel-predicting U-Net on one Gpu (phx_unet)."""
+
+    def __init__(self, gpu: Gpu, seed: int = SEED, params: np.ndarray | None = None):
+        self.gpu = gpu
+        h = C.c_void_p()
+        N.check(N.lib().phx_unet_create(gpu.handle, seed, C.byref(h)))
+        self.handle = h
+        c = C.c_uint64()
+        N.check(N.lib().phx_unet_param_count(h, C.byref(c)))
+        self.count = c.value
+        gpu.adopt(self)
+        if params is not None:
+            self.set_params(params)
+
+    @classmethod
+    def pretrained(cls, gpu: Gpu, path=WEIGHTS) -> "Unet":
+        return cls(gpu, params=read_weights(path))
+
+    def set_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        N.check(N.lib().phx_unet_set_params(self.handle, p.ctypes.data, p.size))
+
+    def _get(self, which: int) -> np.ndarray:
+        out = np.empty(self.count, dtype=np.float32)
+        N.check(N.lib().phx_unet_get(self.handle, which, out.ctypes.data, out.size))
+        return out
+
+    def params(self) -> np.ndarray:
+        return self._get(0)
+
+    def grads(self) -> np.ndarray:
+        """Gradients of the last ``grads``/``train_step`` (blob layout)."""
+        return self._get(1)
+
+    def save(self, path) -> None:
+        write_weights(path, self.params())
+
+    def forward(self, feat, irr, alb, B: int, Hp: int, Wp: int, h: int, w: int, out=None, err=None) -> None:
+        N.check(N.lib().phx_unet_forward(self.handle, devptr(feat), devptr(irr), devptr(alb), B, Hp, Wp, h, w,
+                                         devptr(out), devptr(err)))
+
+    def logits(self) -> int:
+        p = C.c_void_p()
+        N.check(N.lib().phx_unet_logits(self.handle, C.byref(p)))
+        return p.value or 0
+
+    def compute_grads(self, feat, irr, alb, ref, B, Hp, Wp, h, w, loss, err_weight: float = 0.1) -> None:
+        N.check(N.lib().phx_unet_grads(self.handle, devptr(feat), devptr(irr), devptr(alb), devptr(ref), B, Hp, Wp,
+                                       h, w, err_weight, devptr(loss)))
+
+    def adam(self, lr: float) -> None:
+        N.check(N.lib().phx_unet_adam(self.handle, lr))
+
+    def train_step(self, feat, irr, alb, ref, B, Hp, Wp, h, w, loss, lr: float, err_weight: float = 0.1) -> None:
+        """One Adam step on a batch; the batch loss is ADDED to *loss (device fp32)."""
+        N.check(N.lib().phx_unet_train_step(self.handle, devptr(feat), devptr(irr), devptr(alb), devptr(ref), B, Hp,
+                                            Wp, h, w, err_weight, lr, devptr(loss)))
+
+    def denoise(self, tracer, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
+                count: bool = False) -> int | None:
+        """Learned ``Tracer::denoise``; with count=True waits and returns the
+        number of tiles that kept the a-trous result."""
+        fb = C.c_uint32()
+        N.check(N.lib().phx_tracer_denoise_learned(tracer.handle, self.handle, tile, threshold, 1 if keep else 0,
+                                                   C.byref(fb) if count else None))
+        return fb.value if count else None
+
+    def denoise_px(self, px, w: int, h: int, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
+                   view=(0.0, 0.0, 1.0, 0.0), count: bool = False) -> int | None:
+        """The same on any device px image (34 w h + 1 words)."""
+        fb = C.c_uint32()
+        v = (C.c_float * 4)(*view)
+        N.check(N.lib().phx_unet_denoise_px(self.handle, devptr(px), w, h, v, tile, threshold, 1 if keep else 0,
+                                            C.byref(fb) if count else None))
+        return fb.value if count else None
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().phx_unet_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def features(gpu: Gpu, px, w: int, h: int, Hp: int, Wp: int, feat, irr, alb) -> None:
+    """Network inputs of a traced px image (phx_nn_features)."""
+    N.check(N.lib().phx_nn_features(gpu.handle, devptr(px), w, h, Hp, Wp, devptr(feat), devptr(irr), devptr(alb)))

@@ -388,3 +388,127 @@ def c3_skinned(rings: int = 1000, segments: int = 500, nbones: int = 64, width: 
     scene = Scene("c3_skinned", verts, faces, np.stack(mats), np.stack(lights), view, width, height, spp, bounces,
                   env=(0.05, 0.05, 0.05))
     return scene, Rig(verts.copy(), offsets, pairs, joints, nbones)
+
+
+def _box(center, size, n):
+    """An axis-aligned box, each face an n x n grid of quads (12 n^2 faces)."""
+    t = np.linspace(-0.5, 0.5, n + 1)
+    U, V = np.meshgrid(t, t, indexing="ij")
+    verts, faces, base = [], [], 0
+    for axis in range(3):
+        for side in (-0.5, 0.5):
+            p = np.zeros((n + 1, n + 1, 3))
+            a1, a2 = (axis + 1) % 3, (axis + 2) % 3
+            p[..., axis] = side
+            p[..., a1] = U
+            p[..., a2] = V if side > 0 else -V
+            verts.append(p.reshape(-1, 3))
+            i = np.arange(n)[:, None] * (n + 1) + np.arange(n)[None, :]
+            q = np.stack([i, i + n + 1, i + n + 2, i + 1], -1).reshape(-1, 4) + base
+            faces.append(np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]]))
+            base += (n + 1) * (n + 1)
+    v = np.concatenate(verts) * np.asarray(size) + np.asarray(center)
+    return v, np.concatenate(faces)
+
+
+def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bounces: int | None = None) -> Scene:
+    """One seeded procedural scene of the learned denoiser's training set:
+    random boxes, spheres and noise-displaced spheres (plus a cloud of small
+    triangles) on a ground plane, 10k-500k faces in total (log-uniform
+    target), per-object or per-face albedo, some mirror objects, 1-4 area
+    lights and sometimes an emissive panel, a dim uniform world, and a camera
+    on a random orbit around the objects."""
+    rng = np.random.Generator(np.random.PCG64(SEED + 4 + 104729 * index))
+    target = int(math.exp(rng.uniform(math.log(1e4), math.log(5e5))))
+    parts, mats = [], []
+
+    def add(v, f, kind):
+        m0 = len(mats)
+        nf = len(f)
+        if kind == "mirror":
+            mats.append(mirror(rng.uniform(0.5, 1.0, 3)))
+            mid = np.full(nf, m0)
+        elif kind == "faces":  # per-face albedo, like a texture at triangle scale
+            k = min(nf, 4096)
+            for a in rng.uniform(0.05, 0.95, (k, 3)):
+                mats.append(lambert(a))
+            mid = m0 + rng.integers(0, k, nf)
+        elif kind == "mixed":  # per-face albedo with a share of mirror faces
+            k = min(nf, 2048)
+            share = rng.uniform(0.1, 0.4)
+            for a in rng.uniform(0.1, 0.9, (k, 3)):
+                mats.append(mirror(a) if rng.random() < share else lambert(a))
+            mid = m0 + rng.integers(0, k, nf)
+        else:
+            mats.append(lambert(rng.uniform(0.05, 0.95, 3)))
+            mid = np.full(nf, m0)
+        ff = np.zeros((nf, 4), np.uint32)
+        ff[:, :3] = f
+        ff[:, 3] = mid
+        parts.append((v.astype(np.float32), ff))
+
+    def kind():
+        return rng.choice(["plain", "faces", "mirror", "mixed"], p=[0.45, 0.25, 0.15, 0.15])
+
+    ground_y = -0.6
+    g = _quad((-4.0, ground_y, -4.0), (-4.0, ground_y, 4.0), (4.0, ground_y, 4.0), (4.0, ground_y, -4.0), 0)
+    mats.append(lambert(rng.uniform(0.2, 0.8, 3)))
+    parts.append((np.asarray(g[0], np.float32), g[1]))
+    if rng.random() < 0.5:  # a back wall
+        z = rng.uniform(1.2, 2.5)
+        w = _quad((-4.0, ground_y, z), (4.0, ground_y, z), (4.0, 3.0, z), (-4.0, 3.0, z), len(mats))
+        mats.append(lambert(rng.uniform(0.2, 0.8, 3)))
+        parts.append((np.asarray(w[0], np.float32), w[1]))
+    used = 0
+    for _ in range(int(rng.integers(2, 8))):
+        c = np.array([rng.uniform(-0.9, 0.9), 0.0, rng.uniform(-0.9, 0.9)])
+        s = rng.uniform(0.15, 0.5)
+        t = rng.random()
+        if t < 0.35:
+            n = int(rng.integers(2, 24))
+            size = s * rng.uniform(0.5, 1.5, 3)
+            c[1] = ground_y + size[1] / 2
+            v, f = _box(c, size, n)
+        else:
+            lv = int(rng.integers(2, 6))
+            v, f = _icosphere(lv)
+            if t > 0.65:  # displaced
+                r = 1.0 + rng.uniform(0.05, 0.25) * value_noise(v, int(rng.integers(1 << 30)))
+                v = v * r[:, None]
+            c[1] = ground_y + s * rng.uniform(0.7, 1.3)
+            v = v * s + c
+        add(v, f, kind())
+        used += len(f)
+    if used < target:  # fill the budget with a cloud of small triangles
+        nt = target - used
+        cen = np.array([0.0, ground_y + 0.5, 0.0]) + rng.uniform(-0.6, 0.6, (nt, 3)) * np.array([1.5, 0.8, 1.5])
+        e1 = _unit(rng, nt) * rng.uniform(0.01, 0.04, (nt, 1))
+        e2 = _unit(rng, nt) * rng.uniform(0.01, 0.04, (nt, 1))
+        a = cen - (e1 + e2) / 3.0
+        v = np.stack([a, a + e1, a + e2], 1).reshape(-1, 3)
+        f = np.arange(3 * nt).reshape(nt, 3)
+        add(v, f, rng.choice(["plain", "faces"]))
+    lights = []
+    for _ in range(int(rng.integers(1, 5))):
+        pos = (rng.uniform(-1.5, 1.5), rng.uniform(1.0, 2.5), rng.uniform(-1.5, 1.5))
+        sz = rng.uniform(0.15, 0.6)
+        p = rng.uniform(5.0, 40.0) * rng.uniform(0.7, 1.0, 3)
+        lights.append(light_area(pos, (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), sz, sz * rng.uniform(0.5, 1.5), tuple(p)))
+    if rng.random() < 0.3:  # an emissive panel seen by the camera and the paths
+        h_ = rng.uniform(0.1, 0.3)
+        y = rng.uniform(0.5, 1.5)
+        x0, z0 = rng.uniform(-1.0, 1.0, 2)
+        q = _quad((x0 - h_, y, z0 - h_), (x0 + h_, y, z0 - h_), (x0 + h_, y, z0 + h_), (x0 - h_, y, z0 + h_), len(mats))
+        mats.append(mat([0.0, 0.0, 0.0, 1.0], rough=1.0, emit=tuple(rng.uniform(3.0, 15.0) * np.ones(3))))
+        parts.append((np.asarray(q[0], np.float32), q[1]))
+    verts, faces = _assemble(parts)
+    az = rng.uniform(0.0, 2.0 * math.pi)
+    el = math.radians(rng.uniform(5.0, 40.0))
+    dist = rng.uniform(1.8, 3.2)
+    look = np.array([0.0, ground_y + 0.4, 0.0])
+    eye = look + dist * np.array([math.cos(el) * math.sin(az), math.sin(el), -math.cos(el) * math.cos(az)])
+    view = View.look(tuple(eye), tuple(look - eye), (0.0, 1.0, 0.0), rng.uniform(35.0, 55.0))
+    env = rng.uniform(0.0, 0.2)
+    b = int(rng.integers(4, 9)) if bounces is None else bounces
+    return Scene(f"procedural_{index}", verts, faces, np.stack(mats).astype(np.float32), np.stack(lights), view,
+                 width, height, spp, b, env=(env, env, env), meta={"index": index, "target": target})

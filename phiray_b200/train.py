@@ -1,0 +1,263 @@
+"""Trains the learned denoiser on the device, from pairs the tracer renders.
+
+``python -m phiray_b200.train --scenes 160 --ref-spp 1024 --steps 4000
+--out phiray_b200/weights/kpcn.phxu`` renders each seeded procedural scene
+(`scenes.procedural`) once as one continuous accumulation: several short
+segments (1-16 samples) whose px images, differenced from the running
+total, are independent noisy inputs, then `ref-spp` further samples whose
+difference is the reference. Every px plane the network reads (sums,
+albedo/normal/depth guides, sample and miss counts) accumulates linearly,
+so a difference of two accumulations is the image of the samples between
+them. The network then trains on random crops of those pairs with the
+project's own forward and backward kernels (``Unet.train_step``).
+
+Device memory for the data set and the crops is held in torch tensors on
+the context's stream; torch does no arithmetic of the network.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import kernels, scenes
+from .denoiser import THRESHOLD, TILE, Unet, features
+from .gpu import Gpu, GpuArray
+from .tracer import PX_LEN, Tracer, camera
+
+# planes that accumulate per sample: sums, guides, sample count, misses
+_F32_PLANES = [(1, 4), (7, 14), (33, 34)]
+_U32_PLANES = [(31, 32)]
+
+
+def px_diff(a: np.ndarray, b: np.ndarray | None, n: int) -> np.ndarray:
+    """The px image of the samples taken between accumulations b and a."""
+    out = np.zeros(PX_LEN * n + 1, dtype=np.uint32)
+    fo, fa = out.view(np.float32), a.view(np.float32)
+    fb = None if b is None else b.view(np.float32)
+    for lo, hi in _F32_PLANES:
+        s = slice(lo * n, hi * n)
+        fo[s] = fa[s] if fb is None else (fa[s].astype(np.float64) - fb[s]).astype(np.float32)
+    for lo, hi in _U32_PLANES:
+        s = slice(lo * n, hi * n)
+        out[s] = a[s] if b is None else a[s] - b[s]
+    return out
+
+
+def radiance(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """Tracer::radiance of a px image (read.rs:241-251): (h, w, 3) float32."""
+    n = w * h
+    f = px.view(np.float32)
+    k = px[31 * n:32 * n].astype(np.float32)
+    gone = f[33 * n:34 * n]
+    return (f[n:4 * n].reshape(n, 3) / np.maximum(k - gone, 1.0)[:, None]).reshape(h, w, 3)
+
+
+def relmse(x: np.ndarray, ref: np.ndarray) -> float:
+    """mean over pixels and channels of (x - r)^2 / (r^2 + 0.01)."""
+    x = x.astype(np.float64)
+    r = ref.astype(np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+
+
+def render_pairs(gpu: Gpu, scene, segments, ref_spp: int, chunk: int = 256):
+    """(noisy px images for each segment's spp, reference px image)."""
+    w, h = scene.width, scene.height
+    n = w * h
+    tr = Tracer.of(gpu, scene)
+    cam = camera(scene)
+    frame, prev, noisy = 0, None, []
+    for spp in segments:
+        tr.trace(cam, w, h, frame, spp)
+        frame += spp
+        img = tr.image()
+        noisy.append(px_diff(img, prev, n))
+        prev = img
+    left = ref_spp
+    while left > 0:
+        c = min(chunk, left)
+        tr.trace(cam, w, h, frame, c)
+        frame += c
+        left -= c
+    ref = px_diff(tr.image(), prev, n)
+    tr.close()
+    return noisy, ref
+
+
+class DataSet:
+    """Device-resident training pairs: features, demodulated radiance and
+    remodulation planes of each noisy image, and its reference radiance."""
+
+    def __init__(self, gpu: Gpu, count: int, size: int):
+        import torch
+
+        self.gpu, self.size, self.n = gpu, size, 0
+        dev = "cuda"
+        self.feat = torch.empty((count, size, size, 16), dtype=torch.bfloat16, device=dev)
+        self.irr = torch.empty((count, size, size, 3), dtype=torch.float32, device=dev)
+        self.alb = torch.empty((count, size, size, 3), dtype=torch.float32, device=dev)
+        self.ref = torch.empty((count, size, size, 3), dtype=torch.float32, device=dev)
+        self.spp = np.zeros(count, np.int32)
+        self.bad = 0
+
+    def add(self, noisy_px: np.ndarray, ref_rad: np.ndarray, spp: int) -> None:
+        """Appends one pair; a reference pixel that is not finite becomes 0
+        (counted in ``self.bad``)."""
+        import torch
+
+        fin = np.isfinite(ref_rad)
+        if not fin.all():
+            self.bad += int((~fin).sum())
+            ref_rad = np.where(fin, ref_rad, 0.0)
+
+        i, s = self.n, self.size
+        buf = GpuArray.from_(self.gpu, noisy_px)
+        features(self.gpu, buf, s, s, s, s, self.feat[i], self.irr[i], self.alb[i])
+        self.ref[i].copy_(torch.from_numpy(np.ascontiguousarray(ref_rad, dtype=np.float32)))
+        self.gpu.wait()
+        buf.free()
+        self.spp[i] = spp
+        self.n += 1
+
+    def nonfinite(self) -> dict:
+        """Count of values that are not finite in each device plane."""
+        import torch
+
+        return {k: int((~torch.isfinite(getattr(self, k)[:self.n].float())).sum().item())
+                for k in ("feat", "irr", "alb", "ref")}
+
+    def batch(self, rng, B: int, crop: int):
+        """B random crops (random flips and transposes) as contiguous tensors."""
+        import torch
+
+        idx = rng.integers(0, self.n, B)
+        s = self.size
+        outs = [[], [], [], []]
+        for i in idx:
+            y0, x0 = (int(v) for v in rng.integers(0, s - crop + 1, 2))
+            parts = [t[int(i), y0:y0 + crop, x0:x0 + crop] for t in (self.feat, self.irr, self.alb, self.ref)]
+            if rng.random() < 0.5:
+                parts = [torch.flip(p, (1,)) for p in parts]
+            if rng.random() < 0.5:
+                parts = [torch.flip(p, (0,)) for p in parts]
+            if rng.random() < 0.5:
+                parts = [p.transpose(0, 1) for p in parts]
+            for o, p in zip(outs, parts):
+                o.append(p)
+        return [torch.stack(o).contiguous() for o in outs]
+
+
+def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print):
+    ds = DataSet(gpu, len(indices) * len(segments), size)
+    refs, noisy_all = [], []
+    t0 = time.time()
+    for j, i in enumerate(indices):
+        sc = scenes.procedural(i, width=size, height=size)
+        noisy, ref = render_pairs(gpu, sc, segments, ref_spp)
+        rr = radiance(ref, size, size)
+        for spp, px in zip(segments, noisy):
+            ds.add(px, rr, spp)
+        refs.append(rr)
+        noisy_all.append(noisy)
+        if (j + 1) % 10 == 0:
+            log(f"rendered {j + 1}/{len(indices)} scenes ({time.time() - t0:.1f} s)")
+    return ds, refs, noisy_all
+
+
+def train(gpu: Gpu, ds: DataSet, steps: int, batch: int, crop: int, lr: float, seed: int = 1, log=print,
+          err_weight: float = 0.1) -> tuple[Unet, list]:
+    import torch
+
+    net = Unet(gpu, seed=seed)
+    rng = np.random.default_rng(seed)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    hist, acc, t0 = [], 0, time.time()
+    for step in range(steps):
+        warm = min(1.0, (step + 1) / 200)
+        rate = lr * warm * 0.5 * (1.0 + math.cos(math.pi * step / steps))
+        f, i, a, r = ds.batch(rng, batch, crop)
+        net.train_step(f, i, a, r, batch, crop, crop, crop, crop, loss, rate, err_weight)
+        acc += 1
+        if (step + 1) % 100 == 0 or step + 1 == steps or (step < 100 and (step + 1) % 10 == 0):
+            gpu.wait()
+            v = float(loss.item()) / acc
+            if not math.isfinite(v):
+                raise FloatingPointError(f"training loss became {v} by step {step + 1}")
+            hist.append((step + 1, v))
+            log(f"step {step + 1}: loss {v:.5f} lr {rate:.2e} ({time.time() - t0:.1f} s)")
+            loss.zero_()
+            acc = 0
+    gpu.wait()
+    return net, hist
+
+
+def evaluate(gpu: Gpu, net: Unet, noisy_px: np.ndarray, ref_rad: np.ndarray, w: int, h: int,
+             threshold: float = THRESHOLD) -> dict:
+    """relMSE against the reference of the noisy image, the a-trous Denoise,
+    and the learned denoiser (without and with the per-tile fallback)."""
+    out = {"noisy": relmse(radiance(noisy_px, w, h), ref_rad)}
+    buf = GpuArray.from_(gpu, noisy_px)
+    kernels.denoise(gpu, buf, w, h)
+    out["denoise"] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
+    for name, thr in (("learned", 1e30), ("learned_fallback", threshold)):
+        buf.write(noisy_px)
+        net.denoise_px(buf, w, h, TILE, thr)
+        out[name] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
+    buf.free()
+    return out
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--scenes", type=int, default=160)
+    ap.add_argument("--eval-scenes", type=int, default=8)
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--segments", default="1,2,4,4,8,16")
+    ap.add_argument("--ref-spp", type=int, default=1024)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--crop", type=int, default=128)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default="")
+    ap.add_argument("--report", default="")
+    args = ap.parse_args(argv)
+
+    import torch
+
+    gpu = Gpu(0)
+    gpu.set_stream(torch.cuda.current_stream().cuda_stream)
+    segments = [int(s) for s in args.segments.split(",")]
+    t0 = time.time()
+    ds, _, _ = build_data(gpu, range(args.scenes), args.size, segments, args.ref_spp)
+    t_data = time.time() - t0
+    print("non-finite values in the data set:", ds.nonfinite(), "in references (zeroed):", ds.bad)
+    t0 = time.time()
+    net, hist = train(gpu, ds, args.steps, args.batch, args.crop, args.lr, args.seed)
+    t_train = time.time() - t0
+    if args.out:
+        net.save(args.out)
+    held = range(100000, 100000 + args.eval_scenes)
+    rows = []
+    for i in held:
+        sc = scenes.procedural(i, width=args.size, height=args.size)
+        noisy, ref = render_pairs(gpu, sc, [4], args.ref_spp)
+        rows.append(evaluate(gpu, net, noisy[0], radiance(ref, args.size, args.size), args.size, args.size))
+    mean = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
+    report = {"scenes": args.scenes, "pairs": ds.n, "nonfinite_ref_values": ds.bad, "segments": segments, "ref_spp": args.ref_spp,
+              "steps": args.steps, "batch": args.batch, "crop": args.crop, "data_s": round(t_data, 1),
+              "train_s": round(t_train, 1), "loss": hist, "heldout_4spp_relmse": mean, "heldout_rows": rows}
+    print(json.dumps({k: v for k, v in report.items() if k not in ("loss", "heldout_rows")}))
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(report, f, indent=1)
+    net.close()
+    gpu.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -217,3 +217,13 @@ def load() -> Oracle:
             fn.argtypes = args
         _cached = Oracle(lib)
     return _cached
+
+
+def nn():
+    """The FP64 network oracle (oracle/nn.py) as a module."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("oracle_nn", ORACLE_DIR / "nn.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod

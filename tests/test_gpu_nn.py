@@ -1,12 +1,49 @@
-"""The tcgen05 BF16 engine and the denoiser network's kernels against plain
-fp32/fp64 products on the same bf16 inputs."""
+"""The tcgen05 BF16 engine and the learned denoiser's kernels against the
+FP64 oracle (oracle/nn.py) on the same bf16 inputs: each layer forward and
+backward, the per-pixel kernel step and its loss gradient, Adam, the
+feature planes, the whole network's logits and gradients, and the per-tile
+fallback to the a-trous Denoise."""
+
+import ctypes as C
 
 import numpy as np
 import pytest
 
 from phiray_b200 import _native as N
+from tests import oracle_lib
 
 pytestmark = pytest.mark.gpu
+nn = oracle_lib.nn()
+
+
+def _t(a, dtype=None):
+    """A CUDA tensor of a numpy array (bf16 from float64 via the oracle's rounding)."""
+    import torch
+
+    if dtype == "bf16":
+        bits = nn.bf16_bits(a).view(np.int16)
+        return torch.from_numpy(bits.copy()).cuda().view(torch.bfloat16)
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _np(t):
+    import torch
+
+    torch.cuda.synchronize()
+    if t.dtype == torch.bfloat16:
+        return nn.from_bf16_bits(t.view(torch.int16).cpu().numpy().view(np.uint16))
+    return t.cpu().numpy().astype(np.float64)
+
+
+def _sync(gpu):
+    import torch
+
+    torch.cuda.synchronize()
+    gpu.wait()
+
+
+def _round64(k):
+    return (k + 63) // 64 * 64
 
 
 @pytest.mark.parametrize("n", [32, 64, 96, 128, 160])
@@ -20,9 +57,424 @@ def test_gemm_bf16_matches_fp32_product(gpu, m, n, k):
     want = a.double() @ b.double().T
     da, db = a.cuda(), b.cuda()
     d = torch.empty(m, n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
     N.check(N.lib().phx_gemm_bf16(gpu.handle, da.data_ptr(), db.data_ptr(), d.data_ptr(), m, n, k))
     gpu.wait()
     got = d.cpu().double()
     err = (got - want).abs().max().item()
     scale = want.abs().max().item()
     assert err <= 1e-5 * scale + 1e-4, (err, scale)  # fp32 accumulation of exact bf16 products
+
+
+def _weights(rng, cout, cin):
+    K = 9 * cin
+    Kp = _round64(K)
+    w = nn.bf16(rng.normal(size=(cout, K)) * np.sqrt(2.0 / K))
+    wp = np.zeros((cout, Kp))
+    wp[:, :K] = w
+    return w, wp, Kp
+
+
+CONV_CASES = [
+    (16, 32, True, False),
+    (32, 64, True, False),
+    (64, 96, False, False),
+    (96, 128, True, False),
+    (128, 160, True, False),
+    (288, 128, True, False),
+    (224, 96, True, False),
+    (32, 32, False, True),
+]
+
+
+@pytest.mark.parametrize("cin,cout,relu,f32", CONV_CASES)
+def test_conv_fwd(gpu, cin, cout, relu, f32):
+    """Implicit-GEMM 3x3 convolution on the tensor cores, reading a channel
+    window of a wider buffer and writing into another: rounding of the
+    exact product only (bf16 out) or fp32 accumulation error (fp32 out);
+    the channels outside the window are untouched."""
+    import torch
+
+    rng = np.random.default_rng(cin * 1000 + cout)
+    B, H, W = 2, 12, 20  # 480 pixels: 3 full 128-row tiles and a partial one
+    xs, xo = cin + 16, 8
+    xbuf = nn.bf16(rng.normal(size=(B, H, W, xs)))
+    x = xbuf[..., xo:xo + cin]
+    w, wp, Kp = _weights(rng, cout, cin)
+    bias = rng.normal(size=cout).astype(np.float32) * 0.1
+    ys, yo = cout + 16, 8
+    X, Wt, bb = _t(xbuf, "bf16"), _t(wp, "bf16"), _t(bias)
+    sentinel = 1024.0  # exact in bf16 and fp32
+    if f32:
+        Y = torch.full((B, H, W, ys), sentinel, dtype=torch.float32, device="cuda")
+    else:
+        Y = torch.full((B, H, W, ys), sentinel, dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_conv_fwd(gpu.handle, X.data_ptr(), xs, xo, cin, Wt.data_ptr(), Kp, bb.data_ptr(),
+                                    Y.data_ptr(), ys, yo, cout, B, H, W, int(relu), int(f32)))
+    _sync(gpu)
+    got = _np(Y)
+    want = nn.conv(x, w, bias.astype(np.float64), relu)
+    mag = nn.conv(np.abs(x), np.abs(w), np.abs(bias), False)
+    g = got[..., yo:yo + cout]
+    if f32:
+        assert np.all(np.abs(g - want) <= 1e-5 * mag + 1e-30)
+    else:
+        assert np.all(np.abs(g - want) <= 2.0 ** -8 * np.abs(want) + 1e-5 * mag + 1e-30)
+    assert np.all(got[..., :yo] == sentinel) and np.all(got[..., yo + cout:] == np.float32(sentinel))
+
+
+@pytest.mark.parametrize("cin,cout,shape", [(16, 32, (2, 12, 20)), (96, 96, (1, 16, 24)), (288, 128, (2, 8, 8)),
+                                            (32, 160, (1, 64, 96)), (64, 64, (1, 64, 96))])
+def test_conv_wgrad(gpu, cin, cout, shape):
+    """Weight gradient: im2col(X)^T dY on the tensor cores, split over the
+    pixels with fp32 atomics; rows past K stay zero."""
+    import torch
+
+    rng = np.random.default_rng(cin * 7 + cout)
+    B, H, W = shape
+    xs, xo = cin + 8, 8
+    xbuf = nn.bf16(rng.normal(size=(B, H, W, xs)))
+    x = xbuf[..., xo:xo + cin]
+    dys, dyo = cout + 32, 16
+    dybuf = nn.bf16(rng.normal(size=(B, H, W, dys)))
+    dy = dybuf[..., dyo:dyo + cout]
+    K, Kp = 9 * cin, _round64(9 * cin)
+    X, DY = _t(xbuf, "bf16"), _t(dybuf, "bf16")
+    dWt = torch.zeros((Kp, cout), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_conv_wgrad(gpu.handle, X.data_ptr(), xs, xo, cin, DY.data_ptr(), dys, dyo, cout,
+                                      dWt.data_ptr(), Kp, B, H, W))
+    _sync(gpu)
+    got = _np(dWt)
+    want = nn.conv_wgrad(x, dy)  # (cout, K)
+    mag = nn.conv_wgrad(np.abs(x), np.abs(dy))
+    assert np.all(np.abs(got[:K].T - want) <= 1e-5 * mag + 1e-30)
+    assert np.all(got[K:] == 0.0)
+
+
+@pytest.mark.parametrize("cin,cout", [(32, 32), (96, 64), (160, 160), (64, 128)])
+def test_conv_dgrad_by_flipped_weights(gpu, cin, cout):
+    """Data gradient = the 3x3 convolution of dY by the flipped weights."""
+    import torch
+
+    rng = np.random.default_rng(cin + 31 * cout)
+    B, H, W = 2, 10, 14
+    w, wp, Kp = _weights(rng, cout, cin)
+    dy = nn.bf16(rng.normal(size=(B, H, W, cout)))
+    Kp2 = _round64(9 * cout)
+    Wt, DY = _t(wp, "bf16"), _t(dy, "bf16")
+    W2 = torch.empty((cin, Kp2), dtype=torch.bfloat16, device="cuda")
+    zero = torch.zeros(cin, dtype=torch.float32, device="cuda")
+    DX = torch.empty((B, H, W, cin), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_flip(gpu.handle, Wt.data_ptr(), cout, cin, Kp, W2.data_ptr(), Kp2))
+    N.check(N.lib().phx_nn_conv_fwd(gpu.handle, DY.data_ptr(), cout, 0, cout, W2.data_ptr(), Kp2, zero.data_ptr(),
+                                    DX.data_ptr(), cin, 0, cin, B, H, W, 0, 0))
+    _sync(gpu)
+    w2 = _np(W2)
+    assert np.array_equal(w2[:, :9 * cout], nn.flip(w, cin)) and np.all(w2[:, 9 * cout:] == 0)
+    got = _np(DX)
+    want = nn.conv_dgrad(dy, w, cin)
+    mag = nn.conv_dgrad(np.abs(dy), np.abs(w), cin)
+    assert np.all(np.abs(got - want) <= 2.0 ** -8 * np.abs(want) + 1e-5 * mag + 1e-30)
+
+
+def test_pool_up_relu_bias(gpu):
+    """The elementwise layers: pooling and upsampling (and their gradients,
+    pooling's added into a channel window), ReLU's gradient, bias gradient."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    B, H, W, C = 2, 8, 12, 32
+    pitch, off = 96, 64
+    buf = nn.bf16(rng.normal(size=(B, H, W, pitch)))
+    X = _t(buf, "bf16")
+    Y = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_pool_fwd(gpu.handle, X.data_ptr(), pitch, off, C, B, H, W, Y.data_ptr()))
+    _sync(gpu)
+    assert np.array_equal(_np(Y), nn.bf16(nn.pool(buf[..., off:off + C])))
+
+    dy = nn.bf16(rng.normal(size=(B, H // 2, W // 2, C)))
+    DY = _t(dy, "bf16")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_pool_bwd(gpu.handle, DY.data_ptr(), C, B, H, W, X.data_ptr(), pitch, off))
+    _sync(gpu)
+    got = _np(X)
+    want = buf.copy()
+    want[..., off:off + C] = nn.bf16(buf[..., off:off + C] + nn.pool_bwd(dy))
+    assert np.array_equal(got, want)
+
+    small = nn.bf16(rng.normal(size=(B, H // 2, W // 2, C)))
+    S = _t(small, "bf16")
+    U = torch.zeros((B, H, W, pitch), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_up_fwd(gpu.handle, S.data_ptr(), C, B, H, W, U.data_ptr(), pitch, 0))
+    _sync(gpu)
+    u = _np(U)
+    assert np.array_equal(u[..., :C], nn.up(small)) and np.all(u[..., C:] == 0)
+
+    D = torch.empty((B, H // 2, W // 2, C), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_up_bwd(gpu.handle, X.data_ptr(), pitch, off, C, B, H, W, D.data_ptr()))
+    _sync(gpu)
+    assert np.array_equal(_np(D), nn.bf16(nn.up_bwd(got[..., off:off + C])))
+
+    yv = nn.bf16(rng.normal(size=(B * H * W, pitch)))
+    dv = nn.bf16(rng.normal(size=(B * H * W, pitch)))
+    Yt, Dt = _t(yv, "bf16"), _t(dv, "bf16")
+    db = torch.zeros(C, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_relu_bwd(gpu.handle, Yt.data_ptr(), pitch, 8, Dt.data_ptr(), pitch, off, C, B * H * W))
+    N.check(N.lib().phx_nn_bias_grad(gpu.handle, Dt.data_ptr(), pitch, off, C, B * H * W, db.data_ptr()))
+    _sync(gpu)
+    want = dv.copy()
+    want[:, off:off + C] *= yv[:, 8:8 + C] > 0
+    assert np.array_equal(_np(Dt), want)
+    sums = want[:, off:off + C].sum(axis=0)
+    assert np.allclose(_np(db), sums, rtol=1e-5, atol=1e-4)
+
+
+def test_kpn_and_loss_gradient(gpu):
+    """Per-pixel 5x5 kernels on demodulated radiance, the error estimate, the
+    relMSE loss and its logit gradient, with padding pixels zero."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    B, Hp, Wp, h, w = 2, 16, 32, 13, 27
+    logits = rng.normal(size=(B, Hp, Wp, 32)).astype(np.float32)
+    irr = rng.gamma(1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    alb = rng.uniform(0.05, 1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    ref = rng.gamma(1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    L, I, A, R = _t(logits), _t(irr), _t(alb), _t(ref)
+    out = torch.empty((B, Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    err = torch.empty((B, Hp, Wp), dtype=torch.float32, device="cuda")
+    dl = torch.empty((B, Hp, Wp, 32), dtype=torch.bfloat16, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_kpn(gpu.handle, L.data_ptr(), I.data_ptr(), A.data_ptr(), R.data_ptr(), B, Hp, Wp, h, w,
+                               out.data_ptr(), err.data_ptr(), dl.data_ptr(), loss.data_ptr(), 0.25))
+    _sync(gpu)
+    o, e, lo, d = nn.kpn(logits.astype(np.float64), irr.astype(np.float64), alb.astype(np.float64), h, w,
+                         ref.astype(np.float64), 0.25)
+    assert np.allclose(_np(out), o, rtol=2e-5, atol=1e-6)
+    assert np.allclose(_np(err), e, rtol=2e-5, atol=1e-7)
+    assert abs(_np(loss)[0] - lo) <= 1e-4 * lo
+    got = _np(dl)
+    assert np.all(np.abs(got - d) <= 2.0 ** -8 * np.abs(d) + 1e-4 * np.abs(d).max())
+    assert np.all(got[:, h:] == 0) and np.all(got[:, :, w:] == 0) and np.all(got[..., 26:] == 0)
+
+
+def test_adam(gpu):
+    import torch
+
+    rng = np.random.default_rng(3)
+    rows, K, Kp = 32, 144, 192
+    w = rng.normal(size=(rows, Kp)).astype(np.float32)
+    w[:, K:] = 0
+    g = rng.normal(size=(Kp, rows)).astype(np.float32)
+    m = rng.normal(size=(rows, Kp)).astype(np.float32) * 0.1
+    v = rng.uniform(0, 0.1, size=(rows, Kp)).astype(np.float32)
+    Wd, G, M, V = _t(w), _t(g), _t(m), _t(v)
+    WB = torch.empty((rows, Kp), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_adam(gpu.handle, Wd.data_ptr(), G.data_ptr(), M.data_ptr(), V.data_ptr(), WB.data_ptr(),
+                                rows, Kp, K, 1, 1e-3, 0.9, 0.999, 1e-8, 7))
+    _sync(gpu)
+    b1, b2 = float(np.float32(0.9)), float(np.float32(0.999))  # the constants as the device holds them
+    nw, nm, nv = nn.adam(w[:, :K].astype(np.float64), g.T[:, :K].astype(np.float64), m[:, :K].astype(np.float64),
+                         v[:, :K].astype(np.float64), 1e-3, 7, b1, b2)
+    gw = _np(Wd)
+    assert np.allclose(gw[:, :K], nw, rtol=1e-6, atol=1e-6)
+    assert np.allclose(_np(M)[:, :K], nm, rtol=1e-5, atol=1e-7)
+    assert np.allclose(_np(V)[:, :K], nv, rtol=1e-5, atol=1e-9)
+    assert np.array_equal(_np(WB)[:, :K], nn.bf16(gw[:, :K])) and np.all(_np(WB)[:, K:] == 0)
+
+
+def _fake_px(rng, w, h):
+    """A px image with the planes the features read: sample counts 1..16,
+    missed samples, sums, albedo, normal and depth guides."""
+    n = w * h
+    px = np.zeros(34 * n + 1, dtype=np.uint32)
+    f = px.view(np.float32)
+    cnt = rng.integers(1, 17, size=n).astype(np.uint32)
+    px[31 * n:32 * n] = cnt
+    gone = np.minimum(rng.integers(0, 3, size=n), cnt).astype(np.float32)
+    f[33 * n:34 * n] = gone
+    f[n:4 * n] = (rng.gamma(0.5, size=(n, 3)) * cnt[:, None]).ravel()
+    f[7 * n:10 * n] = (rng.uniform(0, 1, size=(n, 3)) * cnt[:, None]).ravel()
+    f[10 * n:13 * n] = rng.normal(size=3 * n)
+    f[13 * n:14 * n] = rng.uniform(0.5, 5, size=n) * cnt
+    return px
+
+
+def test_features(gpu):
+    import torch
+
+    rng = np.random.default_rng(9)
+    w, h, Hp, Wp = 37, 21, 32, 48
+    px = _fake_px(rng, w, h)
+    P = _t(px.view(np.int32))
+    feat = torch.empty((Hp, Wp, 16), dtype=torch.bfloat16, device="cuda")
+    irr = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    alb = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_features(gpu.handle, P.data_ptr(), w, h, Hp, Wp, feat.data_ptr(), irr.data_ptr(),
+                                    alb.data_ptr()))
+    _sync(gpu)
+    f, i, a = nn.features(px, w, h, Hp, Wp)
+    assert np.all(np.abs(_np(feat) - f) <= 2.0 ** -8 * np.abs(f) + 1e-6)
+    assert np.allclose(_np(irr), i, rtol=1e-6, atol=0)
+    assert np.allclose(_np(alb), a, rtol=1e-6, atol=0)
+
+
+def _net_inputs(rng, B, H, W):
+    feat = nn.bf16(np.concatenate([rng.normal(size=(B, H, W, 15)) * 0.5, np.zeros((B, H, W, 1))], axis=-1))
+    irr = rng.gamma(1.0, size=(B, H, W, 3))
+    alb = rng.uniform(0.05, 1.0, size=(B, H, W, 3))
+    ref = irr * alb * rng.uniform(0.5, 1.5, size=(B, H, W, 3))
+    return feat, irr, alb, ref
+
+
+def _random_params(rng):
+    pairs = []
+    for cin, cout in nn.LAYERS:
+        pairs.append((rng.normal(size=(cout, 9 * cin)) * np.sqrt(2.0 / (9 * cin)), rng.normal(size=cout) * 0.05))
+    return nn.join_params(pairs).astype(np.float32)
+
+
+def test_unet_logits_and_gradients_match_fp64_oracle(gpu):
+    """The whole network on the device (19 tensor-core convolutions forward,
+    their weight and data gradients backward) against the FP64 oracle with
+    bf16 rounding at the same tensors: logits and every layer's gradients."""
+    import torch
+
+    from phiray_b200.denoiser import Unet
+
+    rng = np.random.default_rng(2024)
+    B, H, W = 2, 32, 48
+    feat, irr, alb, ref = _net_inputs(rng, B, H, W)
+    blob = _random_params(rng)
+    net = Unet(gpu, params=blob)
+    F, I, A, R = _t(feat, "bf16"), _t(irr.astype(np.float32)), _t(alb.astype(np.float32)), _t(ref.astype(np.float32))
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    net.compute_grads(F, I, A, R, B, H, W, H, W, loss, err_weight=0.1)
+    _sync(gpu)
+    from phiray_b200 import GpuArray
+
+    logits = GpuArray(gpu, B * H * W * 32 * 4, _wrap=net.logits()).read(np.float32).reshape(B, H, W, 32)
+    grads = net.grads()
+    params = nn.split_params(blob)
+    want_logits, act, P = nn.forward(params, feat, rounded=True)
+    scale = np.abs(want_logits).max()
+    assert np.abs(logits - want_logits).max() <= 1e-2 * scale
+    _, _, want_loss, dl = nn.kpn(logits.astype(np.float64), irr, alb, H, W, ref, 0.1)
+    assert abs(_np(loss)[0] - want_loss) <= 1e-4 * want_loss
+    want = nn.backward(P, act, dl, rounded=True)
+    got = nn.split_params(grads)
+    # The same network summed in fp32 instead of fp64 (same bf16 roundings):
+    # how far one valid summation order drifts from another once bf16 storage
+    # amplifies it (a rounding flip in one activation changes every sum
+    # downstream). The device's drift from fp64 must be of that size.
+    lg32, act32, P32 = nn.forward(params, feat, rounded=True, acc=np.float32)
+    alt = nn.backward(P32, act32, dl, rounded=True, acc=np.float32)
+
+    def rel(a, b):
+        return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+    dev = np.array([rel(g[0], w[0]) for g, w in zip(got, want)])
+    ref32 = np.array([rel(a[0], w[0]) for a, w in zip(alt, want)])
+    print("weight-gradient drift from fp64 per layer: device", np.round(dev, 4), "fp32 oracle", np.round(ref32, 4))
+    assert dev[-1] < 2e-3  # the head: its inputs agree, only accumulation order differs
+    assert np.all(dev <= 2.0 * ref32 + 0.01), (dev, ref32)
+    assert np.all([rel(g[1], w[1]) <= 2.0 * rel(a[1], w[1]) + 0.01 for g, w, a in zip(got, want, alt)])
+    net.close()
+
+
+def test_unet_training_lowers_the_loss(gpu):
+    """A few Adam steps on one batch lower its loss (the optimiser and the
+    gradients agree in sign and scale)."""
+    import torch
+
+    from phiray_b200.denoiser import Unet
+
+    rng = np.random.default_rng(77)
+    B, H, W = 2, 32, 32
+    feat, irr, alb, ref = _net_inputs(rng, B, H, W)
+    net = Unet(gpu, seed=1)
+    F, I, A, R = _t(feat, "bf16"), _t(irr.astype(np.float32)), _t(alb.astype(np.float32)), _t(ref.astype(np.float32))
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    hist = []
+    for _ in range(30):
+        loss.zero_()
+        net.train_step(F, I, A, R, B, H, W, H, W, loss, lr=2e-3)
+        _sync(gpu)
+        hist.append(float(_np(loss)[0]))
+    assert hist[-1] < 0.7 * hist[0], hist
+    net.close()
+
+
+def test_learned_denoise_fallback_tiles(gpu):
+    """Per-tile fallback: threshold below every estimate keeps the a-trous
+    Denoise bit for bit; above every estimate gives the network's own output;
+    in between, exactly the tiles over the threshold keep the a-trous result."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import GpuArray, scenes
+    from phiray_b200.denoiser import Unet, padded
+
+    s = scenes.c1_plain(ntris=4096, width=72, height=40, spp=4)
+    cam = px.camera(s)
+    w, h = s.width, s.height
+    tr = px.Tracer.of(gpu, s)
+    net = Unet(gpu, seed=3)
+
+    def traced():
+        tr.trace(cam, w, h, 0, 4)
+
+    traced()
+    tr.denoise()
+    plain = tr.image()
+    traced()
+    fb = net.denoise(tr, tile=16, threshold=-1.0, count=True)
+    assert fb == 3 * 5
+    assert np.array_equal(tr.image(), plain)
+
+    traced()
+    noisy = tr.image()
+    Hp, Wp = padded(h), padded(w)
+    feat = torch.empty((Hp, Wp, 16), dtype=torch.bfloat16, device="cuda")
+    irr = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    alb = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    out = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    err = torch.empty((Hp, Wp), dtype=torch.float32, device="cuda")
+    pptr, _ = tr.device_image()
+    torch.cuda.synchronize()
+    px.denoiser.features(gpu, pptr, w, h, Hp, Wp, feat, irr, alb)
+    net.forward(feat, irr, alb, 1, Hp, Wp, h, w, out, err)
+    _sync(gpu)
+    o, e = _np(out), _np(err)
+    fb = net.denoise(tr, tile=16, threshold=1e30, count=True)
+    assert fb == 0
+    rad = tr.radiance()
+    n = w * h
+    cnt = np.maximum(noisy[31 * n:32 * n].astype(np.float64), 1)
+    gone = noisy.view(np.float32)[33 * n:34 * n]
+    live = (1.0 - gone / cnt > 0.5 / cnt).reshape(h, w)
+    assert np.allclose(rad[live], o[:h, :w][live], rtol=1e-6, atol=1e-7)
+
+    tiles = sorted(e[j:min(j + 16, h), i:min(i + 16, w)].mean() for j in range(0, h, 16) for i in range(0, w, 16))
+    thr = float(0.5 * (tiles[7] + tiles[8]))
+    traced()
+    fb = net.denoise(tr, tile=16, threshold=thr, count=True)
+    mixed = tr.image()
+    _, mask = nn.compose(noisy, w, h, o, e[:h, :w], 16, thr)
+    assert fb == int((~mask).sum())
+    pm = np.repeat(np.repeat(mask, 16, 0), 16, 1)[:h, :w].reshape(n)
+    assert np.array_equal(mixed[:n][~pm], plain[:n][~pm])
+    net.close()
+    tr.close()
