@@ -242,6 +242,244 @@ def run_c3(args) -> None:
     gpu.close()
 
 
+def run_c4(args) -> None:
+    """The learned denoiser's network alone: one forward pass over a 1080p
+    frame (padded to 1088 x 1920) and one training step (forward, loss,
+    backward, Adam) on `batch` 128 x 128 crops, timed with CUDA events on
+    the context's stream; TFLOP/s counts the network's multiply-adds."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200.denoiser import Unet, flops_per_pixel
+
+    gpu = px.Gpu(0)
+    stream = torch.cuda.ExternalStream(gpu.stream)
+    net = Unet(gpu, seed=1)
+    Hp, Wp, h, w = 1088, 1920, 1080, 1920
+    g = torch.Generator(device="cpu").manual_seed(7)
+    feat = (torch.randn(Hp, Wp, 16, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    irr = torch.rand(Hp, Wp, 3, generator=g).cuda()
+    alb = (torch.rand(Hp, Wp, 3, generator=g) * 0.9 + 0.05).cuda()
+    out = torch.empty(Hp, Wp, 3, device="cuda")
+    err = torch.empty(Hp, Wp, device="cuda")
+    torch.cuda.synchronize()
+
+    def timed(fn, warm, reps):
+        for _ in range(warm):
+            fn()
+        gpu.wait(60000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        gpu.wait(60000)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    fwd = lambda: net.forward(feat, irr, alb, 1, Hp, Wp, h, w, out, err)  # noqa: E731
+    if args.phase == "nn":  # profiling runs: the launches alone
+        for _ in range(args.warmup + args.steps):
+            fwd()
+        gpu.wait(60000)
+        gpu.close()
+        return
+    with Clocks(0) as clk:
+        fwd_ms = timed(fwd, args.warmup, args.steps)
+    B, c = 12, 128
+    tf = (torch.randn(B, c, c, 16, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    ti, ta = torch.rand(B, c, c, 3, generator=g).cuda(), (torch.rand(B, c, c, 3, generator=g) * 0.9 + 0.05).cuda()
+    tref = torch.rand(B, c, c, 3, generator=g).cuda()
+    loss = torch.zeros(1, device="cuda")
+    torch.cuda.synchronize()
+    step_ms = timed(lambda: net.train_step(tf, ti, ta, tref, B, c, c, c, c, loss, 1e-4), args.warmup, args.steps)
+    fpp = flops_per_pixel()
+    fwd_tflops = fpp * Hp * Wp / (fwd_ms * 1e-3) / 1e12
+    train_tflops = 3 * fpp * B * c * c / (step_ms * 1e-3) / 1e12
+    pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = pk.get("bf16_tflops", 1590.0)
+    print(json.dumps({
+        "metric": "learned denoiser network TFLOP/s (bf16 tensor cores, fp32 accumulate)",
+        "value": round(fwd_tflops, 2), "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(fwd_ms, 3), "higher_is_better": True, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": "KPCN U-Net 32-64-96-128-160, forward over 1088x1920; training step on 12 x 128^2",
+                   "flops_per_pixel": fpp},
+        "forward_ms": round(fwd_ms, 3), "train_step_ms": round(step_ms, 3), "train_tflops": round(train_tflops, 2),
+        "roofline": {"bound": "tensor", "achieved": round(fwd_tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(fwd_tflops / peak, 4), "peak_source": "measured" if pk else "fallback"},
+        "clocks": clk.summary(),
+    }), flush=True)
+    net.close()
+    gpu.close()
+
+
+def run_c5(args) -> None:
+    """Batched serving: 64 procedural scenes (10k-2M faces, 256^2 to 1080p,
+    1/4/16 spp, 6 bounces) per frame: each scene's LBVH rebuilt or refit
+    (seeded coin per scene per frame), every scene traced in one persistent
+    launch, then the learned denoiser with its per-tile a-trous fallback;
+    the whole frame is one captured CUDA graph, replayed per frame with the
+    frame's rebuild/refit choices. Aggregate Mrays/s over the timed frames;
+    per-scene latency = completion after the frame's start (device clock)."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+    from phiray_b200.batch import Batch
+    from phiray_b200.denoiser import THRESHOLD, WEIGHTS, Unet
+
+    gpu = px.Gpu(0)
+    stream = torch.cuda.ExternalStream(gpu.stream)
+    t0 = time.time()
+    scs = scenes.c5_batch(args.scenes)
+    trs, b = [], Batch(gpu)
+    for sc in scs:
+        cam = px.camera(sc)
+        cam["w"], cam["h"] = sc.width, sc.height
+        tr = px.Tracer.of(gpu, sc)
+        trs.append(tr)
+        b.add(tr, cam, sc.width, sc.height, 0, sc.spp)
+    setup_s = time.time() - t0
+    cfg, tune_ms = b.autotune()
+    net = Unet.pretrained(gpu) if os.path.exists(WEIGHTS) else Unet(gpu)
+    b.capture(net, THRESHOLD)
+    rng = np.random.default_rng(5)
+    frames = [rng.integers(0, 2, len(scs)) for _ in range(args.warmup + args.steps)]
+    for m in frames[:args.warmup]:
+        b.replay(m)
+    gpu.wait(60000)
+    total_ms, rays, lats = 0.0, 0, []
+    with Clocks(0) as clk:
+        for m in frames[args.warmup:]:
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b.replay(m)
+            e.record(stream)
+            lat, r = b.results()
+            torch.cuda.synchronize()
+            total_ms += a.elapsed_time(e)
+            rays += int(r.sum())
+            lats.append(lat / 1e6)
+    lats = np.concatenate(lats)
+    ms = total_ms / args.steps
+    value = rays / (total_ms * 1e-3) / 1e6
+    print(json.dumps({
+        "metric": "batched serving aggregate Mrays/s (64 scenes, one persistent launch, captured frame graph)",
+        "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"c5_batch: {len(scs)} procedural scenes, faces log-uniform 10k-2M, "
+                               "256^2/512^2/720p/1080p, 1/4/16 spp, 6 bounces, rebuild or refit per scene per frame, "
+                               "learned denoise with a-trous fallback",
+                   "faces_total": int(sum(sc.ntris for sc in scs)),
+                   "pixels_total": int(sum(sc.width * sc.height for sc in scs)),
+                   "samples_total": int(sum(sc.width * sc.height * sc.spp for sc in scs))},
+        "frames_per_s": round(1000.0 / ms, 3),
+        "latency_ms": {"p50": round(float(np.percentile(lats, 50)), 3),
+                       "p99": round(float(np.percentile(lats, 99)), 3),
+                       "max": round(float(lats.max()), 3)},
+        "autotune": {"chosen": min(tune_ms, key=tune_ms.get), "kind_threads_stack": list(cfg),
+                     "trace_ms": {k: round(v, 3) for k, v in tune_ms.items()}},
+        "setup_s": round(setup_s, 1),
+        "clocks": clk.summary(),
+    }), flush=True)
+    b.close()
+    net.close()
+    gpu.close()
+
+
+def equal_relmse(args, gpu, s, cam, stream) -> dict:
+    """The headline comparison at 1080p against a 4096-spp render of the same
+    frame: plain tracing + the a-trous Denoise at `plain` spp against the
+    learned denoiser (with its per-tile Denoise fallback) at `learned` spp.
+    Every test image is an independent sample set: one accumulation runs the
+    reference's 4096 samples first and each test image is the difference of
+    two later accumulations (every plane the filters read accumulates
+    linearly). relMSE = mean (x - r)^2 / (r^2 + 0.01) over pixels and
+    channels of Tracer::radiance. Frame time = trace + filter, CUDA events."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import kernels
+    from phiray_b200 import train as T
+    from phiray_b200.denoiser import THRESHOLD, TILE, WEIGHTS, Unet
+
+    if not os.path.exists(WEIGHTS):
+        return {"unavailable": f"no trained weights at {os.path.relpath(WEIGHTS, ROOT)}"}
+    W, H, n = s.width, s.height, s.width * s.height
+    learned_spp = [1, 2, 4, 8, 16]
+    plain_spp = [64, 128, 256, 512]
+    tr = px.Tracer.of(gpu, s)
+    net = Unet.pretrained(gpu)
+    frame = 0
+    while frame < args.ref_spp:
+        c = min(64, args.ref_spp - frame)
+        tr.trace(cam, W, H, frame, c)
+        frame += c
+    prev = tr.image()
+    ref = T.radiance(T.px_diff(prev, None, n), W, H)
+    buf = px.GpuArray(gpu, (34 * n + 1) * 4)
+    rel_plain, rel_learned, kept = {}, {}, {}
+    tiles = ((W + TILE - 1) // TILE) * ((H + TILE - 1) // TILE)
+    for spp in learned_spp + plain_spp:
+        tr.trace(cam, W, H, frame, spp)
+        frame += spp
+        img = tr.image()
+        noisy = T.px_diff(img, prev, n)
+        prev = img
+        buf.write(noisy)
+        kernels.denoise(gpu, buf, W, H)
+        rel_plain[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
+        if spp in learned_spp:
+            buf.write(noisy)
+            kept[spp] = net.denoise_px(buf, W, H, TILE, THRESHOLD, count=True) / tiles
+            rel_learned[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
+    buf.free()
+
+    def frame_ms(spp, learned, reps):
+        def once():
+            tr.trace(cam, W, H, 0, spp)
+            if learned:
+                net.denoise(tr)
+            else:
+                tr.denoise()
+        once()
+        gpu.wait(60000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            once()
+        b.record(stream)
+        gpu.wait(60000)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_plain = frame_ms(args.plain_spp, False, 2)
+    target = rel_plain[args.plain_spp]
+    match = next((p for p in learned_spp if rel_learned[p] <= target), None)
+    out = {
+        "reference_spp": args.ref_spp,
+        "plain": {"spp": args.plain_spp, "relmse": round(target, 6), "frame_ms": round(t_plain, 3),
+                  "frames_per_s": round(1000.0 / t_plain, 3)},
+        "relmse_plain_denoise": {str(k): round(v, 6) for k, v in rel_plain.items()},
+        "relmse_learned": {str(k): round(v, 6) for k, v in rel_learned.items()},
+        "fallback_tile_share": {str(k): round(v, 4) for k, v in kept.items()},
+        "threshold": THRESHOLD,
+    }
+    if match is not None:
+        t_l = frame_ms(match, True, 5)
+        out["learned"] = {"spp": match, "relmse": round(rel_learned[match], 6), "frame_ms": round(t_l, 3),
+                          "frames_per_s": round(1000.0 / t_l, 3)}
+        out["speedup_at_equal_relmse"] = round(t_plain / t_l, 2)
+    else:
+        out["learned"] = None
+        out["speedup_at_equal_relmse"] = None
+    net.close()
+    tr.close()
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -250,10 +488,15 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
-                    help="c2: the headline frame benchmark; c3: the skinned-animation stage timings")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the headline frame benchmark; c3: the skinned-animation stage timings; "
+                         "c4: the learned denoiser's network alone; c5: batched serving")
+    ap.add_argument("--scenes", type=int, default=64, help="scenes of the c5 workload")
     ap.add_argument("--frames", type=int, default=120, help="frames of the c3 workload")
-    ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build"],
+    ap.add_argument("--ref-spp", type=int, default=4096, help="samples of the equal-relMSE reference render")
+    ap.add_argument("--plain-spp", type=int, default=256, help="samples of the plain tracer + Denoise")
+    ap.add_argument("--no-denoised", action="store_true", help="skip the equal-relMSE comparison")
+    ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build", "nn"],
                     help="all: the benchmark; render/rays/build: only that kernel's launches (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -261,6 +504,12 @@ def main() -> None:
         return
     if args.workload == "c3":
         run_c3(args)
+        return
+    if args.workload == "c4":
+        run_c4(args)
+        return
+    if args.workload == "c5":
+        run_c5(args)
         return
 
     import torch
@@ -387,6 +636,8 @@ def main() -> None:
         e2e_s = float(t.item())
     e2e = rays_per_frame * world / e2e_s / 1e6
 
+    denoised = None if args.no_denoised else equal_relmse(args, gpu, s, cam, stream)
+
     out = None
     if rank == 0:
         cpu = None if args.no_cpu else cpu_baseline(s, cam)
@@ -420,6 +671,7 @@ def main() -> None:
                          "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "denoised": denoised,
             "gpu_launches": 21 * args.steps,
             "clocks": clk.summary(),
         }

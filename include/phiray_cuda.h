@@ -565,6 +565,46 @@ int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, uint32_t w, uint32_t h, 
 int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, int32_t tile, float threshold, int32_t keep,
                                    uint32_t* fallback);
 
+/* ---- Batched serving: many tracers' frames in one persistent launch (no
+ * reference counterpart; phiber renders one Tracer per view). ---- */
+typedef struct phx_batch_s* phx_batch;
+/* PHX_BATCH_PERSISTENT: one launch whose warps take 32-pixel tiles of every
+ * job from one counter (costliest jobs first); PHX_BATCH_PER_SCENE: one
+ * launch per job with its tracer's own render kernel. Every job's image is
+ * bit for bit its tracer's own phx_tracer_trace. */
+#define PHX_BATCH_PERSISTENT 0u
+#define PHX_BATCH_PER_SCENE 1u
+int32_t phx_batch_create(phx_ctx ctx, phx_batch* out);
+int32_t phx_batch_destroy(phx_batch b);
+/* A job: frames [first, first + spp) of `cam` at w x h into tracer tr's image
+ * (one job per tracer). The camera is copied. */
+int32_t phx_batch_add(phx_batch b, phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                      uint32_t spp, uint32_t* index);
+int32_t phx_batch_clear(phx_batch b);
+/* Launch form, block size (64, 128, 256) and walk-stack placement
+ * (PHX_STACK_LOCAL / PHX_STACK_SHARED) of the persistent kernel. */
+int32_t phx_batch_set_config(phx_batch b, uint32_t kind, uint32_t threads, uint32_t stack);
+/* Every job's frame, stream-ordered. */
+int32_t phx_batch_trace(phx_batch b);
+/* The autotuner: times the persistent launch at each block size and stack
+ * placement, and per-scene launches of the megakernel and of the state
+ * machine, on the batch; keeps the fastest. ms (>= 8 floats, may be NULL)
+ * gets each configuration's time, *nconfigs their number. Waits. */
+int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint32_t* stack, float* ms,
+                           uint32_t* nconfigs);
+/* Records one serving frame as a CUDA graph: per job its face boxes, an LBVH
+ * rebuild and a refit each gated by the job's mode word, the tracer's
+ * preparation; the batch trace; per job the learned denoiser with the
+ * a-trous fallback (net non-NULL; one copy of the network per image shape)
+ * or the a-trous Denoise, then a completion time stamp. Runs one frame
+ * outside the capture first (sizing every buffer). */
+int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold);
+/* Replays the captured frame; modes (HOST, one per job): 1 rebuild, 0 refit. */
+int32_t phx_batch_replay(phx_batch b, const uint32_t* modes);
+/* After a replay: each job's completion time after the frame's start (ns,
+ * device clock) and rays traced (both nullable, one per job). Waits. */
+int32_t phx_batch_results(phx_batch b, uint64_t* latency_ns, uint64_t* rays);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,6 +120,17 @@ SIGNATURES: dict[str, tuple] = {
     "phx_unet_logits": (i32, [vp, C.POINTER(vp)]),
     "phx_unet_denoise_px": (i32, [vp, vp, u32, u32, f32p, i32, C.c_float, i32, C.POINTER(u32)]),
     "phx_tracer_denoise_learned": (i32, [vp, vp, i32, C.c_float, i32, C.POINTER(u32)]),
+    "phx_batch_create": (i32, [vp, C.POINTER(vp)]),
+    "phx_batch_destroy": (i32, [vp]),
+    "phx_batch_add": (i32, [vp, vp, vp, u32, u32, u32, u32, C.POINTER(u32)]),
+    "phx_batch_clear": (i32, [vp]),
+    "phx_batch_set_config": (i32, [vp, u32, u32, u32]),
+    "phx_batch_trace": (i32, [vp]),
+    "phx_batch_autotune": (i32, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_float),
+                                 C.POINTER(u32)]),
+    "phx_batch_capture": (i32, [vp, vp, C.c_float]),
+    "phx_batch_replay": (i32, [vp, vp]),
+    "phx_batch_results": (i32, [vp, vp, vp]),
     "phx_skin": (i32, [vp, vp, vp, vp, vp, u32, vp, u32, C.c_float]),
     "phx_face_boxes": (i32, [vp, vp, vp, u32, vp]),
     "phx_denoise": (i32, [vp, vp, u32, u32, f32p, f32p, i32]),

@@ -99,7 +99,16 @@ __device__ void block_minmax(float* v, float* s) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_bounds(const float4* __restrict__ prims, uint32_t n, float4* __restrict__ partial) {
+// Zeroes `words` words (the gated stand-in for a memset node).
+__global__ void k_fill(uint32_t* __restrict__ p, size_t words, Gate gate) {
+    if (gate.off()) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = 0u;
+}
+
+__global__ void __launch_bounds__(256) k_bounds(const float4* __restrict__ prims, uint32_t n, float4* __restrict__ partial,
+                                                  Gate gate) {
+    if (gate.off()) return;
     __shared__ float s[6];
     float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -123,7 +132,8 @@ __global__ void __launch_bounds__(256) k_bounds(const float4* __restrict__ prims
 __global__ void __launch_bounds__(256) k_morton_hist(const float4* __restrict__ prims, uint32_t n,
                                                      const float4* __restrict__ partial, uint32_t nparts,
                                                      uint32_t* __restrict__ codes, uint32_t* __restrict__ hist,
-                                                     float4* __restrict__ scene_out) {
+                                                     float4* __restrict__ scene_out, Gate gate) {
+    if (gate.off()) return;
     __shared__ float s[6];
     __shared__ uint32_t s_hist[PASSES * 256];
     float v[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -173,7 +183,8 @@ __global__ void k_morton_given(const float4* __restrict__ prims, uint32_t n, phx
     codes[i] = morton3((cx - p.lo[0]) * p.inv[0], (cy - p.lo[1]) * p.inv[1], (cz - p.lo[2]) * p.inv[2]);
 }
 
-__global__ void k_hist(const uint32_t* __restrict__ codes, uint32_t n, uint32_t* __restrict__ hist) {
+__global__ void k_hist(const uint32_t* __restrict__ codes, uint32_t n, uint32_t* __restrict__ hist, Gate gate) {
+    if (gate.off()) return;
     __shared__ uint32_t s_hist[PASSES * 256];
     for (int k = threadIdx.x; k < PASSES * 256; k += blockDim.x) s_hist[k] = 0;
     __syncthreads();
@@ -229,7 +240,8 @@ __global__ void __launch_bounds__(RADIX_THREADS) k_radix_pass(const uint32_t* __
                                                               uint32_t* __restrict__ vals_out, uint32_t n,
                                                               uint32_t shift, const uint32_t* __restrict__ hist,
                                                               uint32_t* lookback, uint32_t* ticket,
-                                                              uint32_t* status) {
+                                                              uint32_t* status, Gate gate) {
+    if (gate.off()) return;
     __shared__ uint32_t s_warp[WARPS][256];
     __shared__ uint32_t s_keys[TILE];
     __shared__ uint32_t s_vals[TILE];
@@ -368,7 +380,8 @@ __device__ __forceinline__ uint4 karras_link(const uint32_t* __restrict__ codes,
 }
 
 __global__ void __launch_bounds__(256) k_karras(const uint32_t* __restrict__ codes, uint32_t n, uint4* __restrict__ links,
-                                                uint32_t* __restrict__ parent) {
+                                                uint32_t* __restrict__ parent, Gate gate) {
+    if (gate.off()) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0 && parent) parent[0] = NONE;
     if (i + 1 >= n) return;
@@ -385,7 +398,8 @@ __global__ void __launch_bounds__(256) k_karras(const uint32_t* __restrict__ cod
 __global__ void __launch_bounds__(256) k_pack(const uint4* __restrict__ links, const uint32_t* __restrict__ parent,
                                               uint32_t n, uint32_t leaf, float4* __restrict__ nodes,
                                               uint32_t* __restrict__ starts, uint32_t* __restrict__ nstarts,
-                                              uint32_t* __restrict__ depth_out) {
+                                              uint32_t* __restrict__ depth_out, Gate gate) {
+    if (gate.off()) return;
     const uint32_t total = 2 * n - 1;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < total;
@@ -459,7 +473,8 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims,
                                                const uint32_t* __restrict__ parent, float4* nodes,
                                                const uint32_t* __restrict__ starts,
                                                const uint32_t* __restrict__ nstarts, uint32_t* counters,
-                                               uint32_t* status) {
+                                               uint32_t* status, Gate gate) {
+    if (gate.off()) return;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= *nstarts) return;
     uint32_t i = starts[t];
@@ -582,13 +597,23 @@ int32_t BvhWork::reserve(uint32_t n, int sms) {
     return PHX_OK;
 }
 
+// Zeroes `bytes` (a multiple of 4) on the stream: a memset node, or under a
+// gate a kernel that reads the gate first.
+static int32_t zero(Ctx* c, void* p, size_t bytes, Gate gate) {
+    if (!gate.word) return cuda_check(cudaMemsetAsync(p, 0, bytes, c->stream), "memset");
+    const size_t words = bytes / 4;
+    k_fill<<<grid_for(words, 256, (uint32_t)c->sms * 4), 256, 0, c->stream>>>((uint32_t*)p, words, gate);
+    return cuda_check(cudaGetLastError(), "fill");
+}
+
 // Stable LSD sort of `codes` (n keys): sorted codes and order into `w`.
-static int32_t enqueue_sort(Ctx* c, BvhWork& w, const uint32_t* codes, uint32_t n, bool hist_ready) {
+static int32_t enqueue_sort(Ctx* c, BvhWork& w, const uint32_t* codes, uint32_t n, bool hist_ready,
+                            Gate gate = Gate{}) {
     cudaStream_t s = c->stream;
     uint32_t tiles = (n + TILE - 1) / TILE;
     if (!hist_ready) {
-        PHX_CUDA(cudaMemsetAsync(w.zeroed.ptr, 0, w.zeroed_bytes(), s));
-        k_hist<<<grid_for(n, 256, (uint32_t)c->sms * 4), 256, 0, s>>>(codes, n, w.hist());
+        PHX_TRY(zero(c, w.zeroed.ptr, w.zeroed_bytes(), gate));
+        k_hist<<<grid_for(n, 256, (uint32_t)c->sms * 4), 256, 0, s>>>(codes, n, w.hist(), gate);
         PHX_CUDA(cudaGetLastError());
     }
     uint32_t* ak = (uint32_t*)w.alt_keys.ptr;
@@ -596,13 +621,13 @@ static int32_t enqueue_sort(Ctx* c, BvhWork& w, const uint32_t* codes, uint32_t 
     uint32_t* sk = (uint32_t*)w.sorted.ptr;
     uint32_t* sv = (uint32_t*)w.order.ptr;
     k_radix_pass<true><<<tiles, RADIX_THREADS, 0, s>>>(codes, nullptr, ak, av, n, 0, w.hist() + 0 * 256,
-                                                        w.lookback(0), w.tickets() + 0, c->status);
+                                                        w.lookback(0), w.tickets() + 0, c->status, gate);
     k_radix_pass<false><<<tiles, RADIX_THREADS, 0, s>>>(ak, av, sk, sv, n, 8, w.hist() + 1 * 256, w.lookback(1),
-                                                         w.tickets() + 1, c->status);
+                                                         w.tickets() + 1, c->status, gate);
     k_radix_pass<false><<<tiles, RADIX_THREADS, 0, s>>>(sk, sv, ak, av, n, 16, w.hist() + 2 * 256, w.lookback(2),
-                                                         w.tickets() + 2, c->status);
+                                                         w.tickets() + 2, c->status, gate);
     k_radix_pass<false><<<tiles, RADIX_THREADS, 0, s>>>(ak, av, sk, sv, n, 24, w.hist() + 3 * 256, w.lookback(3),
-                                                         w.tickets() + 3, c->status);
+                                                         w.tickets() + 3, c->status, gate);
     return cuda_check(cudaGetLastError(), "radix sort");
 }
 
@@ -616,7 +641,7 @@ int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* or
     if (n == 0) return PHX_OK;
     cudaStream_t s = c->stream;
     const uint32_t tiles = (n + TILE - 1) / TILE;
-    k_hist<<<grid_for(n, 256, (uint32_t)c->sms * 4), 256, 0, s>>>(codes, n, hist);
+    k_hist<<<grid_for(n, 256, (uint32_t)c->sms * 4), 256, 0, s>>>(codes, n, hist, Gate{});
     for (int pass = 0; pass < PASSES; pass++) {
         const uint32_t* kin = pass == 0 ? codes : (pass % 2 == 1 ? alt_keys : sorted);
         const uint32_t* vin = pass % 2 == 1 ? alt_vals : order;
@@ -625,46 +650,46 @@ int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* or
         uint32_t* lb = lookback + (size_t)pass * stride * 256;
         if (pass == 0)
             k_radix_pass<true><<<tiles, RADIX_THREADS, 0, s>>>(kin, nullptr, kout, vout, n, 0, hist, lb, tickets,
-                                                                c->status);
+                                                                c->status, Gate{});
         else
             k_radix_pass<false><<<tiles, RADIX_THREADS, 0, s>>>(kin, vin, kout, vout, n, 8 * pass, hist + 256 * pass,
-                                                                 lb, tickets + pass, c->status);
+                                                                 lb, tickets + pass, c->status, Gate{});
     }
     return cuda_check(cudaGetLastError(), "radix sort");
 }
 
 // Every stage of Bvh::build over w.prims[0..n) on the context's stream.
-int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf) {
+int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate) {
     cudaStream_t s = c->stream;
-    PHX_CUDA(cudaMemsetAsync(w.scalars.ptr, 0, 64, s));
+    PHX_TRY(zero(c, w.scalars.ptr, 64, gate));
     if (n == 0) return PHX_OK;
     const float4* prims = (const float4*)w.prims.ptr;
     const uint32_t nparts = grid_for(n, 256, (uint32_t)c->sms * 4);
-    k_bounds<<<nparts, 256, 0, s>>>(prims, n, (float4*)w.partial.ptr);
-    PHX_CUDA(cudaMemsetAsync(w.zeroed.ptr, 0, w.zeroed_bytes(), s));
+    k_bounds<<<nparts, 256, 0, s>>>(prims, n, (float4*)w.partial.ptr, gate);
+    PHX_TRY(zero(c, w.zeroed.ptr, w.zeroed_bytes(), gate));
     k_morton_hist<<<grid_for(n, 256, (uint32_t)c->sms * 8), 256, 0, s>>>(
-        prims, n, (const float4*)w.partial.ptr, nparts, (uint32_t*)w.codes.ptr, w.hist(), (float4*)w.scene.ptr);
+        prims, n, (const float4*)w.partial.ptr, nparts, (uint32_t*)w.codes.ptr, w.hist(), (float4*)w.scene.ptr, gate);
     PHX_CUDA(cudaGetLastError());
-    PHX_TRY(enqueue_sort(c, w, (const uint32_t*)w.codes.ptr, n, true));
+    PHX_TRY(enqueue_sort(c, w, (const uint32_t*)w.codes.ptr, n, true, gate));
     k_karras<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>((const uint32_t*)w.sorted.ptr, n, (uint4*)w.links.ptr,
-                                                        (uint32_t*)w.parent.ptr);
-    PHX_CUDA(cudaMemsetAsync(w.counters.ptr, 0, (size_t)n * 4, s));
+                                                        (uint32_t*)w.parent.ptr, gate);
+    PHX_TRY(zero(c, w.counters.ptr, (size_t)n * 4, gate));
     k_pack<<<grid_for(2ull * n - 1, 256, 1u << 30), 256, 0, s>>>((const uint4*)w.links.ptr,
                                                                 (const uint32_t*)w.parent.ptr, n, leaf,
                                                                 (float4*)w.nodes.ptr, (uint32_t*)w.starts.ptr,
-                                                                w.nstarts(), w.depth());
+                                                                w.nstarts(), w.depth(), gate);
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>(prims, (const uint32_t*)w.order.ptr,
                                                        (const uint32_t*)w.parent.ptr, (float4*)w.nodes.ptr,
                                                        (const uint32_t*)w.starts.ptr, w.nstarts(),
-                                                       (uint32_t*)w.counters.ptr, c->status);
+                                                       (uint32_t*)w.counters.ptr, c->status, gate);
     return cuda_check(cudaGetLastError(), "bvh build");
 }
 
-int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots) {
+int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots, Gate gate) {
     if (n == 0) return PHX_OK;
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, c->stream>>>(
         (const float4*)w.prims.ptr, slots ? nullptr : (const uint32_t*)w.order.ptr, (const uint32_t*)w.parent.ptr,
-        (float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr, w.nstarts(), (uint32_t*)w.counters.ptr, c->status);
+        (float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr, w.nstarts(), (uint32_t*)w.counters.ptr, c->status, gate);
     return cuda_check(cudaGetLastError(), "bvh refit");
 }
 
@@ -682,7 +707,7 @@ int32_t launch_karras_step(cudaStream_t s, const void* params, void* const* bufs
     memcpy(&p, params, sizeof p);
     if (items == 0 || p.leaves < 2) return PHX_OK;
     k_karras<<<grid_for(items, 256, 1u << 30), 256, 0, s>>>((const uint32_t*)bufs[0], p.leaves, (uint4*)bufs[1],
-                                                            nullptr);
+                                                            nullptr, Gate{});
     return cuda_check(cudaGetLastError(), "karras");
 }
 
@@ -866,10 +891,10 @@ int32_t phx_morton(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t* cod
     PHX_TRY(hist.reserve(PASSES * 256 * 4));
     PHX_TRY(scene.reserve(32));
     PHX_CUDA(cudaMemsetAsync(hist.ptr, 0, PASSES * 256 * 4, c->stream));
-    k_bounds<<<nparts, 256, 0, c->stream>>>((const float4*)prims, n, (float4*)partial.ptr);
+    k_bounds<<<nparts, 256, 0, c->stream>>>((const float4*)prims, n, (float4*)partial.ptr, Gate{});
     k_morton_hist<<<grid_for(n, 256, (uint32_t)c->sms * 8), 256, 0, c->stream>>>(
         (const float4*)prims, n, (const float4*)partial.ptr, nparts, codes, (uint32_t*)hist.ptr,
-        (float4*)(scene_out ? (void*)scene_out : scene.ptr));
+        (float4*)(scene_out ? (void*)scene_out : scene.ptr), Gate{});
     PHX_CUDA(cudaGetLastError());
     return wait_stream(c->stream, 0);
 }
@@ -894,7 +919,7 @@ int32_t phx_karras(phx_ctx ctx, const uint32_t* sorted, uint32_t n, phx_link* li
     if (n < 2) return PHX_OK;
     Ctx* c = &ctx->c;
     PHX_TRY(use(c));
-    k_karras<<<grid_for(n, 256, 1u << 30), 256, 0, c->stream>>>(sorted, n, (uint4*)links, nullptr);
+    k_karras<<<grid_for(n, 256, 1u << 30), 256, 0, c->stream>>>(sorted, n, (uint4*)links, nullptr, Gate{});
     PHX_CUDA(cudaGetLastError());
     return wait_stream(c->stream, 0);
 }

@@ -9,6 +9,18 @@ namespace phx {
 constexpr int LBVH_TILE = 4096;  // radix-sort tile (256 threads x 16 keys)
 constexpr int LBVH_PASSES = 4;   // 8-bit digits over the 30-bit Morton code
 
+// A device-side switch on a launch: the kernel does its work only when
+// *word == want (word NULL: always). A captured CUDA graph can then hold
+// both a rebuild and a refit and choose per replay by one word in device
+// memory, which every gated kernel reads before doing anything else.
+struct Gate {
+    const uint32_t* word = nullptr;
+    uint32_t want = 0;
+#ifdef __CUDACC__
+    __device__ __forceinline__ bool off() const { return word != nullptr && *word != want; }
+#endif
+};
+
 struct BvhWork {
     uint32_t cap = 0;  // prims the arrays hold
     DevMem prims, codes, sorted, order, alt_keys, alt_vals, partial, zeroed, links, parent, nodes, starts, counters,
@@ -34,9 +46,9 @@ int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* or
                          uint32_t stride);
 
 // Every stage of Bvh::build over w.prims[0..n) on the context's stream.
-int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf);
+int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate = Gate{});
 // Bvh::refit (slots = false: prims through order; true: prims already in
 // slot order, Bvh::refit_slots).
-int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots);
+int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots, Gate gate = Gate{});
 
 }  // namespace phx

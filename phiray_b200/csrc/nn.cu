@@ -163,21 +163,51 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *(const uint32_t*)&v;
 }
 
+// Asynchronous 16-byte global -> shared copy; src_bytes 0 fills zeros (the
+// source address must still be a valid one, it is not read).
+__device__ __forceinline__ void cp_async_ca16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_addr(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_cg16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+// Stages of the pipelined convolution: chunk c's tiles live in stage c % STAGES.
+constexpr int STAGES = 3;
+template <int N>
+struct Pipe {
+    static constexpr int A_BYTES = tc::BM * tc::BK * 2;
+    static constexpr int STAGE = A_BYTES + N * tc::BK * 2;
+    static constexpr int TOTAL = STAGES * STAGE;
+};
+
 // Y = act(conv3x3(X, W) + bias). OUT_F32: fp32 output (the network's head).
+//
+// One CTA: 128 pixels x N output channels, the K = 9 cin reduction in
+// chunks of 64 through a STAGES-deep ring of shared-memory tiles. Every
+// thread issues cp.async copies of its share of chunk c + STAGES - 1 (the
+// im2col rows, zero-filled at the image border and past K, and the weight
+// rows) while the tensor core works on chunk c; thread 0 issues chunk c's
+// four MMAs and commits them to the stage's mbarrier, which the threads
+// wait on before refilling that stage.
 template <int N, bool RELU, bool OUT_F32>
 __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
                                                   const float* __restrict__ bias, void* __restrict__ Y, Geo g,
                                                   uint32_t* status) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar[STAGES];
     __shared__ uint32_t tmem_base;
-    using P = Plan<N>;
-    uint8_t* a_tile = smem + P::A_OFF;
-    uint8_t* b_tile = smem + P::B_OFF;
+    using P = Pipe<N>;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tc::tmem_alloc(&tmem_base, tc::tmem_cols(N));
     if (tid == 0) {
-        tc::mbar_init(&bar, 1);
+        for (int i = 0; i < STAGES; i++) tc::mbar_init(&bar[i], 1);
         fence_barrier_init();
     }
     tc::fence_before_sync();
@@ -190,30 +220,58 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     PixRow rows[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) rows[j] = pix_row(row0 + (tid >> 3) + 16 * j, g);
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int kb = 0; kb < g.Kp && ok; kb += tc::BK) {
-        const int k = kb + c * 8;
+    const int nk = g.Kp / tc::BK;
+
+    auto issue = [&](int chunk) {
+        uint8_t* a = smem + (chunk % STAGES) * P::STAGE;
+        uint8_t* b = a + P::A_BYTES;
+        const int k = chunk * tc::BK + c * 8;
+        const bool kin = k < g.K;
+        const int tap = kin ? k / g.cin : 0;
+        const int ci = k - tap * g.cin;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const int r = (tid >> 3) + 16 * j;
-            *(uint4*)(a_tile + tc::tile_off(r, c * 8, tc::BM)) = im2col_vec(X, rows[j], k, g);
+            const int y = rows[j].y + dy, x = rows[j].x + dx;
+            const bool ok = kin && rows[j].b >= 0 && y >= 0 && y < g.H && x >= 0 && x < g.W;
+            const bf16* src = ok ? X + ((size_t)(rows[j].b * g.H + y) * g.W + x) * g.xs + g.xo + ci : X;
+            cp_async_ca16(a + tc::tile_off(r, c * 8, tc::BM), src, ok ? 16u : 0u);
         }
         for (int v = tid; v < N * 8; v += 128) {
             const int r = v >> 3, cc = v & 7;
-            *(uint4*)(b_tile + tc::tile_off(r, cc * 8, N)) = __ldg((const uint4*)(Wt + (size_t)r * g.Kp + kb + cc * 8));
+            cp_async_cg16(b + tc::tile_off(r, cc * 8, N), Wt + (size_t)r * g.Kp + chunk * tc::BK + cc * 8);
         }
-        tc::fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            tc::mma_chunk<N>(tm, a_tile, b_tile, kb == 0);
-            tc::mma_commit(&bar);
-        }
-        ok = tc::mbar_wait(&bar, phase);
-        phase ^= 1u;
-        ok = __syncthreads_and(ok);
+    };
+
+    // Prologue: STAGES - 1 groups, empty past the last chunk, so that chunk c
+    // is always commit group c.
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < nk) issue(s);
+        cp_async_commit();
     }
+    bool ok = true;
+    for (int chunk = 0; chunk < nk; chunk++) {
+        cp_async_wait<STAGES - 2>();  // this thread's copies of `chunk` landed
+        tc::fence_async_smem();
+        __syncthreads();              // and everyone's
+        if (tid == 0) {
+            uint8_t* a = smem + (chunk % STAGES) * P::STAGE;
+            tc::fence_after_sync();
+            tc::mma_chunk<N>(tm, a, a + P::A_BYTES, chunk == 0);
+            tc::mma_commit(&bar[chunk % STAGES]);
+        }
+        const int next = chunk + STAGES - 1;
+        if (next < nk) {
+            // the stage `next` reuses held chunk - 1: its MMAs must be done
+            if (chunk >= 1) ok = tc::mbar_wait(&bar[(chunk - 1) % STAGES], ((chunk - 1) / STAGES) & 1) && ok;
+            issue(next);
+        }
+        cp_async_commit();
+    }
+    ok = tc::mbar_wait(&bar[(nk - 1) % STAGES], ((nk - 1) / STAGES) & 1) && ok;
+    ok = __syncthreads_and(ok);
     tc::fence_after_sync();
     if (ok) {
         const int p = row0 + warp * 32 + lane;
@@ -657,7 +715,7 @@ __global__ void k_compose(const float* __restrict__ out, const float* __restrict
 
 template <int N, bool RELU, bool F32>
 int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
-    const int smem = Plan<N>::TOTAL;
+    const int smem = Pipe<N>::TOTAL;
     static std::atomic<uint64_t> done{0};
     PHX_TRY(smem_limit(k_conv_fwd<N, RELU, F32>, smem, c->device, done));
     const int P = g.B * g.H * g.W;

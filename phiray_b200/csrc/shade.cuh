@@ -51,6 +51,10 @@ struct Scene {
     uint32_t root;  // inner node 0, or LEAF | 0 when the root is a leaf
     f3 root_lo, root_hi;
     float extent;
+    // The walks' 32-entry stacks: per-thread local memory (0), or (1) this
+    // thread's column of the launch's dynamic shared memory, which must then
+    // hold 32 words per thread.
+    uint32_t smem_stack;
 };
 
 // Fills the build-dependent fields from the device info record, and the
@@ -277,6 +281,10 @@ __device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool f
 // The walk behind a call, for code with several trace sites.
 template <bool STATS>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    if (S.smem_stack) {
+        extern __shared__ uint32_t walk_stacks[];
+        return walk<STATS, true>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
+    }
     return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 

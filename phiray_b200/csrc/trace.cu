@@ -8,8 +8,10 @@
 // image planes once at the end — the same sums, in the same order, that the
 // reference's one-dispatch-per-sample loop leaves in its px buffer.
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cstring>
+#include <vector>
 
 #include "lbvh.cuh"
 #include "shade.cuh"
@@ -485,52 +487,54 @@ __device__ __forceinline__ void setup(Scene& S, Frame& F) {
     F.eps = S.extent * 1e-5f;
 }
 
+// One pixel's samples [F.frame0, F.frame0 + F.spp): its sums read back (or
+// started over on frame 0), shade.wgsl's main once per sample, the planes
+// written once (util.wgsl's guide/emit over the whole run of samples).
 template <bool STATS>
-__global__ void __launch_bounds__(128, 4) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
-                                               uint32_t count, unsigned long long* counters) {
-    setup(S, F);
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    Count cnt{0, 0, 0};
-    if (k < count) {
-        const uint32_t i = first + k;
-        const uint32_t n = F.n;
-        Sums acc;
-        if (F.frame0 > 0u) {
-            ld3(px, 1 * n, i, acc.lin);
-            ld3(px, 20 * n, i, acc.grid);
-            ld3(px, 7 * n, i, acc.alb);
-            ld3(px, 10 * n, i, acc.nrm);
-            acc.cov = __uint_as_float(px[23 * n + i]);
-            acc.film = __uint_as_float(px[24 * n + i]);
-            acc.gone = __uint_as_float(px[33 * n + i]);
-            acc.dep = __uint_as_float(px[13 * n + i]);
-            acc.count = px[31 * n + i];
-        } else {
-            acc.lin = acc.grid = acc.alb = acc.nrm = mk(0.0f);
-            acc.cov = acc.film = acc.gone = acc.dep = 0.0f;
-            acc.count = 0;
-            px[29 * n + i] = 0u;
-            px[30 * n + i] = 0u;
-        }
-        acc.outline = 0;
-        for (uint32_t s = 0; s < F.spp; s++) sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
-        st3(px, 1 * n, i, acc.lin);
-        st3(px, 20 * n, i, acc.grid);
-        st3(px, 7 * n, i, acc.alb);
-        st3(px, 10 * n, i, acc.nrm);
-        px[23 * n + i] = __float_as_uint(acc.cov);
-        px[24 * n + i] = __float_as_uint(acc.film);
-        px[33 * n + i] = __float_as_uint(acc.gone);
-        px[13 * n + i] = __float_as_uint(acc.dep);
-        px[31 * n + i] = acc.count;
-        px[25 * n + i] = acc.outline;
-        const float kk = (float)acc.count;
-        const f3 shown = view_transform_std(acc.lin / fmaxf(kk - acc.gone, 1.0f), F.exposure, F.gamma) *
-                             (1.0f - acc.cov / kk) +
-                         acc.grid / kk;
-        st3(px, 4 * n, i, shown);
-        px[i] = pack_rgba(shown, acc.film / kk);
+__device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun, uint32_t* __restrict__ px,
+                                          uint32_t i, Count& cnt) {
+    const uint32_t n = F.n;
+    Sums acc;
+    if (F.frame0 > 0u) {
+        ld3(px, 1 * n, i, acc.lin);
+        ld3(px, 20 * n, i, acc.grid);
+        ld3(px, 7 * n, i, acc.alb);
+        ld3(px, 10 * n, i, acc.nrm);
+        acc.cov = __uint_as_float(px[23 * n + i]);
+        acc.film = __uint_as_float(px[24 * n + i]);
+        acc.gone = __uint_as_float(px[33 * n + i]);
+        acc.dep = __uint_as_float(px[13 * n + i]);
+        acc.count = px[31 * n + i];
+    } else {
+        acc.lin = acc.grid = acc.alb = acc.nrm = mk(0.0f);
+        acc.cov = acc.film = acc.gone = acc.dep = 0.0f;
+        acc.count = 0;
+        px[29 * n + i] = 0u;
+        px[30 * n + i] = 0u;
     }
+    acc.outline = 0;
+    for (uint32_t s = 0; s < F.spp; s++) sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
+    st3(px, 1 * n, i, acc.lin);
+    st3(px, 20 * n, i, acc.grid);
+    st3(px, 7 * n, i, acc.alb);
+    st3(px, 10 * n, i, acc.nrm);
+    px[23 * n + i] = __float_as_uint(acc.cov);
+    px[24 * n + i] = __float_as_uint(acc.film);
+    px[33 * n + i] = __float_as_uint(acc.gone);
+    px[13 * n + i] = __float_as_uint(acc.dep);
+    px[31 * n + i] = acc.count;
+    px[25 * n + i] = acc.outline;
+    const float kk = (float)acc.count;
+    const f3 shown = view_transform_std(acc.lin / fmaxf(kk - acc.gone, 1.0f), F.exposure, F.gamma) *
+                         (1.0f - acc.cov / kk) +
+                     acc.grid / kk;
+    st3(px, 4 * n, i, shown);
+    px[i] = pack_rgba(shown, acc.film / kk);
+}
+
+// Adds a warp's ray count (and STATS: steps, tests) to counters[0..2].
+template <bool STATS>
+__device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long long* counters) {
     const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counters, (unsigned long long)tot);
     if (STATS) {
@@ -540,6 +544,73 @@ __global__ void __launch_bounds__(128, 4) k_render(Scene S, Frame F, f3 sun, uin
             atomicAdd(counters + 1, (unsigned long long)st);
             atomicAdd(counters + 2, (unsigned long long)te);
         }
+    }
+}
+
+template <bool STATS>
+__global__ void __launch_bounds__(128, 4) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
+                                               uint32_t count, unsigned long long* counters) {
+    setup(S, F);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    Count cnt{0, 0, 0};
+    if (k < count) render_px<STATS>(S, F, sun, px, first + k, cnt);
+    flush_counts<STATS>(cnt, counters);
+}
+
+// ---- many scenes in one persistent launch ----
+//
+// A job is one tracer's frame: its scene, camera frame, image and ray
+// counters. Its pixels are cut into tiles of 32 (one warp each); the tiles
+// of all jobs are numbered in one range, the costliest jobs first. Each
+// warp of a grid sized to the resident capacity takes the next tile from a
+// counter, finds its job by binary search over the jobs' first tiles, copies
+// the job record to its slot of shared memory, and renders the tile's
+// pixels: the same per-pixel computation as k_render, so every job's image
+// is bit for bit its single-scene render.
+struct Job {
+    Scene S;
+    Frame F;
+    f3 sun;
+    uint32_t* px;
+    unsigned long long* counters;
+    uint32_t tile0;  // first tile of this job in the launch's numbering
+    uint32_t npx;
+};
+
+template <bool STATS, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
+                                                                         uint32_t ntiles, uint32_t* next) {
+    constexpr int WARPS = THREADS / 32;
+    constexpr int WORDS = (int)(sizeof(Job) / 4);
+    __shared__ __align__(16) Job sj[WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Job& J = sj[warp];
+    uint32_t cur = 0xFFFFFFFFu;
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(next, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= ntiles) break;
+        uint32_t lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(&jobs[mid].tile0) <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        if (lo != cur) {
+            __syncwarp();
+            const uint32_t* src = (const uint32_t*)(jobs + lo);
+            uint32_t* dst = (uint32_t*)&J;
+            for (int k = lane; k < WORDS; k += 32) dst[k] = __ldg(src + k);
+            __syncwarp();
+            if (lane == 0) setup(J.S, J.F);
+            __syncwarp();
+            cur = lo;
+        }
+        const uint32_t p = (t - J.tile0) * 32u + (uint32_t)lane;
+        Count cnt{0, 0, 0};
+        if (p < J.npx) render_px<STATS>(J.S, J.F, J.sun, J.px, p, cnt);
+        flush_counts<STATS>(cnt, J.counters);
     }
 }
 
@@ -1284,15 +1355,12 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
     return PHX_OK;
 }
 
-int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp,
-                      uint32_t first_px, uint32_t count_px, bool stats = false) {
+// Launches the tracer's render kernel over pixels [first_px, first_px +
+// count_px) of frame F, whose camera is already in tr->cam (no host copy:
+// the launch can be recorded into a graph).
+int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, uint32_t count_px, bool stats) {
     Ctx* c = tr->ctx;
     const Scene S = scene_of(tr);
-    PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, cam, sizeof(phx_camera), cudaMemcpyHostToDevice, c->stream));
-    Frame F = frame_of(cam, w, h, ((const phx_camera*)tr->cam.ptr)->lights);
-    F.frame0 = first_frame;
-    F.spp = spp;
-    const f3 sun = mk(cam->sun[0], cam->sun[1], cam->sun[2]);
     if (tr->kernel != PHX_KERNEL_MEGAKERNEL) {
         // state machine, at 4, 6 or 8 resident blocks of 128 per SM
         const int minb = tr->kernel == 1u ? 4 : (tr->kernel == 2u ? 6 : 8);
@@ -1324,6 +1392,21 @@ int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t
         k_render<false><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
                                                                        count_px, (unsigned long long*)tr->rays.ptr);
     return cuda_check(cudaGetLastError(), "render");
+}
+
+// The frame record of `cam` for tr, whose lights the kernels read from tr->cam.
+Frame frame_for(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp) {
+    Frame F = frame_of(cam, w, h, ((const phx_camera*)tr->cam.ptr)->lights);
+    F.frame0 = first_frame;
+    F.spp = spp;
+    return F;
+}
+
+int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp,
+                      uint32_t first_px, uint32_t count_px, bool stats = false) {
+    PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, cam, sizeof(phx_camera), cudaMemcpyHostToDevice, tr->ctx->stream));
+    const Frame F = frame_for(tr, cam, w, h, first_frame, spp);
+    return launch_frame(tr, F, mk(cam->sun[0], cam->sun[1], cam->sun[2]), first_px, count_px, stats);
 }
 
 }  // namespace
@@ -1673,6 +1756,410 @@ int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w,
     tr->last = *cam;
     tr->have_last = true;
     return read_status(tr->ctx);
+}
+
+}  // extern "C"
+
+// ---- batched serving: many tracers' frames in one persistent launch ----
+
+namespace phx {
+namespace {
+
+__global__ void k_stamp(unsigned long long* dst) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *dst = t;
+}
+
+struct BatchJob {
+    phx_tracer tr;
+    phx_camera cam;
+    uint32_t w, h, first, spp;
+};
+
+}  // namespace
+}  // namespace phx
+
+struct phx_batch_s {
+    phx_ctx handle = nullptr;
+    Ctx* ctx = nullptr;
+    std::vector<BatchJob> jobs;
+    std::vector<uint32_t> order;  // jobs by decreasing per-tile cost
+    uint32_t kind = PHX_BATCH_PERSISTENT, threads = 128, stack = PHX_STACK_LOCAL;
+    DevMem djobs, next, counters, stamps, modes;
+    uint32_t* host_modes = nullptr;  // pinned: the graph's per-replay copy source
+    uint32_t ntiles = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<phx_unet> nets;  // one network per padded image shape
+    std::vector<int> net_of;     // job -> nets index (-1: the a-trous Denoise)
+};
+
+namespace phx {
+namespace {
+
+template <int THREADS>
+int32_t launch_batch(phx_batch b) {
+    Ctx* c = b->ctx;
+    const void* fn = (const void*)k_render_batch<false, THREADS>;
+    const int smem = b->stack == PHX_STACK_SHARED ? STACK * 4 * THREADS : 0;
+    static std::atomic<uint64_t> done{0};
+    const uint64_t bit = 1ull << (c->device & 63);
+    if (smem && !(done.load() & bit)) {
+        PHX_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, STACK * 4 * THREADS));
+        done.fetch_or(bit);
+    }
+    int per_sm = 0;
+    PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, THREADS, smem));
+    const uint32_t warps_needed = b->ntiles;
+    uint32_t grid = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)c->sms;
+    grid = std::min<uint32_t>(grid, (warps_needed + THREADS / 32 - 1) / (THREADS / 32));
+    PHX_CUDA(cudaMemsetAsync(b->next.ptr, 0, 4, c->stream));
+    k_render_batch<false, THREADS><<<grid, THREADS, smem, c->stream>>>((const Job*)b->djobs.ptr,
+                                                                        (uint32_t)b->jobs.size(), b->ntiles,
+                                                                        (uint32_t*)b->next.ptr);
+    return cuda_check(cudaGetLastError(), "batch render");
+}
+
+// Uploads cameras and the job table (host copies: not inside a capture).
+int32_t batch_prepare(phx_batch b) {
+    Ctx* c = b->ctx;
+    const size_t nj = b->jobs.size();
+    PHX_TRY(b->counters.reserve(nj * 3 * sizeof(unsigned long long)));
+    PHX_TRY(b->stamps.reserve((nj + 1) * sizeof(unsigned long long)));
+    PHX_TRY(b->next.reserve(4));
+    PHX_TRY(b->modes.reserve(nj * 4));
+    b->order.resize(nj);
+    for (size_t j = 0; j < nj; j++) b->order[j] = (uint32_t)j;
+    std::stable_sort(b->order.begin(), b->order.end(),
+                     [&](uint32_t x, uint32_t y) { return b->jobs[x].spp > b->jobs[y].spp; });
+    std::vector<Job> host(nj);
+    uint32_t tile = 0;
+    for (size_t k = 0; k < nj; k++) {
+        const uint32_t j = b->order[k];
+        BatchJob& bj = b->jobs[j];
+        phx_tracer tr = bj.tr;
+        PHX_TRY(ensure_image(tr, bj.w, bj.h));
+        PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, &bj.cam, sizeof(phx_camera), cudaMemcpyHostToDevice, c->stream));
+        Job& J = host[k];
+        memset(&J, 0, sizeof J);
+        J.S = scene_of(tr);
+        J.S.smem_stack = b->stack == PHX_STACK_SHARED ? 1u : 0u;
+        J.F = frame_for(tr, &bj.cam, bj.w, bj.h, bj.first, bj.spp);
+        J.sun = mk(bj.cam.sun[0], bj.cam.sun[1], bj.cam.sun[2]);
+        J.px = (uint32_t*)tr->px.ptr;
+        J.counters = (unsigned long long*)b->counters.ptr + 3 * j;
+        J.tile0 = tile;
+        J.npx = bj.w * bj.h;
+        tile += (J.npx + 31) / 32;
+    }
+    b->ntiles = tile;
+    PHX_TRY(b->djobs.reserve(nj * sizeof(Job)));
+    PHX_CUDA(cudaMemcpyAsync(b->djobs.ptr, host.data(), nj * sizeof(Job), cudaMemcpyHostToDevice, c->stream));
+    return wait_stream(c->stream, 0);  // the pageable sources are released on return
+}
+
+// The frame's traces, stream-ordered (capturable once batch_prepare ran).
+int32_t batch_trace(phx_batch b) {
+    Ctx* c = b->ctx;
+    PHX_CUDA(cudaMemsetAsync(b->counters.ptr, 0, b->jobs.size() * 3 * sizeof(unsigned long long), c->stream));
+    if (b->kind == PHX_BATCH_PER_SCENE) {
+        for (size_t j = 0; j < b->jobs.size(); j++) {
+            BatchJob& bj = b->jobs[j];
+            const Frame F = frame_for(bj.tr, &bj.cam, bj.w, bj.h, bj.first, bj.spp);
+            PHX_CUDA(cudaMemsetAsync(bj.tr->rays.ptr, 0, 8, c->stream));
+            PHX_TRY(launch_frame(bj.tr, F, mk(bj.cam.sun[0], bj.cam.sun[1], bj.cam.sun[2]), 0, bj.w * bj.h, false));
+            PHX_CUDA(cudaMemcpyAsync((unsigned long long*)b->counters.ptr + 3 * j, bj.tr->rays.ptr, 8,
+                                     cudaMemcpyDeviceToDevice, c->stream));
+        }
+        return PHX_OK;
+    }
+    switch (b->threads) {
+        case 64: return launch_batch<64>(b);
+        case 128: return launch_batch<128>(b);
+        case 256: return launch_batch<256>(b);
+    }
+    return fail(PHX_ERR_INVALID, "batch block size %u (64, 128 or 256)", b->threads);
+}
+
+void batch_mark_traced(phx_batch b) {
+    for (BatchJob& bj : b->jobs) {
+        bj.tr->frame = bj.first + bj.spp - 1;
+        bj.tr->last = bj.cam;
+        bj.tr->have_last = true;
+    }
+}
+
+void batch_drop_graph(phx_batch b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+}
+
+int32_t clone_net(phx_ctx ctx, phx_unet src, phx_unet* out) {
+    uint64_t count = 0;
+    PHX_TRY(phx_unet_param_count(src, &count));
+    std::vector<float> p(count);
+    PHX_TRY(phx_unet_get(src, 0, p.data(), count));
+    PHX_TRY(phx_unet_create(ctx, 1, out));
+    const int32_t rc = phx_unet_set_params(*out, p.data(), count);
+    if (rc < 0) {
+        phx_unet_destroy(*out);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+}  // namespace
+}  // namespace phx
+
+extern "C" {
+
+int32_t phx_batch_create(phx_ctx ctx, phx_batch* out) {
+    if (!ctx || !out) return fail(PHX_ERR_INVALID, "null argument");
+    PHX_TRY(use(&ctx->c));
+    phx_batch b = new phx_batch_s();
+    b->handle = ctx;
+    b->ctx = &ctx->c;
+    if (cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+        delete b;
+        return fail(PHX_ERR_DEVICE, "event create");
+    }
+    ctx->c.live++;
+    *out = b;
+    return PHX_OK;
+}
+
+int32_t phx_batch_clear(phx_batch b) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    PHX_TRY(use(b->ctx));
+    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    batch_drop_graph(b);
+    for (phx_unet n : b->nets) phx_unet_destroy(n);
+    b->nets.clear();
+    b->net_of.clear();
+    b->jobs.clear();
+    b->ntiles = 0;
+    return PHX_OK;
+}
+
+int32_t phx_batch_destroy(phx_batch b) {
+    if (!b) return PHX_OK;
+    phx_batch_clear(b);
+    if (b->host_modes) cudaFreeHost(b->host_modes);
+    if (b->done) cudaEventDestroy(b->done);
+    b->ctx->live--;
+    delete b;
+    return PHX_OK;
+}
+
+int32_t phx_batch_add(phx_batch b, phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                      uint32_t spp, uint32_t* index) {
+    if (!b || !tr || !cam) return fail(PHX_ERR_INVALID, "null argument");
+    if (tr->ctx != b->ctx) return fail(PHX_ERR_INVALID, "the tracer belongs to another context");
+    if (w == 0 || h == 0 || spp == 0) return fail(PHX_ERR_INVALID, "empty job %ux%u x %u spp", w, h, spp);
+    if ((uint64_t)w * h * PHX_PX_LEN + 1 > 0xFFFFFFFFull) return fail(PHX_ERR_INVALID, "image %ux%u too large", w, h);
+    for (const BatchJob& bj : b->jobs)
+        if (bj.tr == tr) return fail(PHX_ERR_INVALID, "a tracer can hold one job of a batch");
+    PHX_TRY(check_camera(cam));
+    batch_drop_graph(b);
+    b->jobs.push_back(BatchJob{tr, *cam, w, h, first, spp});
+    if (index) *index = (uint32_t)(b->jobs.size() - 1);
+    return PHX_OK;
+}
+
+int32_t phx_batch_set_config(phx_batch b, uint32_t kind, uint32_t threads, uint32_t stack) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    if (kind > PHX_BATCH_PER_SCENE) return fail(PHX_ERR_INVALID, "unknown batch kind %u", kind);
+    if (threads != 64 && threads != 128 && threads != 256) return fail(PHX_ERR_INVALID, "block size %u", threads);
+    if (stack > PHX_STACK_SHARED) return fail(PHX_ERR_INVALID, "stack placement %u", stack);
+    batch_drop_graph(b);
+    b->kind = kind;
+    b->threads = threads;
+    b->stack = stack;
+    return PHX_OK;
+}
+
+int32_t phx_batch_trace(phx_batch b) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    if (b->jobs.empty()) return PHX_OK;
+    PHX_TRY(use(b->ctx));
+    PHX_TRY(batch_prepare(b));
+    PHX_TRY(batch_trace(b));
+    batch_mark_traced(b);
+    return PHX_OK;
+}
+
+int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint32_t* stack, float* ms,
+                           uint32_t* nconfigs) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    if (b->jobs.empty()) return fail(PHX_ERR_INVALID, "empty batch");
+    PHX_TRY(use(b->ctx));
+    struct Cfg {
+        uint32_t kind, threads, stack, tracer_kernel;
+    };
+    std::vector<Cfg> cfgs;
+    for (uint32_t t : {64u, 128u, 256u})
+        for (uint32_t st : {PHX_STACK_LOCAL, PHX_STACK_SHARED}) cfgs.push_back({PHX_BATCH_PERSISTENT, t, st, 0});
+    cfgs.push_back({PHX_BATCH_PER_SCENE, 128, PHX_STACK_LOCAL, PHX_KERNEL_MEGAKERNEL});
+    cfgs.push_back({PHX_BATCH_PER_SCENE, 128, PHX_STACK_LOCAL, PHX_KERNEL_STATE_MACHINE});
+    std::vector<uint32_t> saved;
+    for (const BatchJob& bj : b->jobs) saved.push_back(bj.tr->kernel);
+    cudaEvent_t e0, e1;
+    PHX_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(PHX_ERR_DEVICE, "event create");
+    }
+    float best = 3.0e38f;
+    size_t pick = 0;
+    int32_t rc = PHX_OK;
+    for (size_t k = 0; k < cfgs.size() && rc == PHX_OK; k++) {
+        const Cfg& cf = cfgs[k];
+        b->kind = cf.kind;
+        b->threads = cf.threads;
+        b->stack = cf.stack;
+        if (cf.kind == PHX_BATCH_PER_SCENE)
+            for (BatchJob& bj : b->jobs) bj.tr->kernel = cf.tracer_kernel;
+        if ((rc = batch_prepare(b)) < 0 || (rc = batch_trace(b)) < 0) break;  // warm-up
+        cudaEventRecord(e0, b->ctx->stream);
+        if ((rc = batch_trace(b)) < 0) break;
+        cudaEventRecord(e1, b->ctx->stream);
+        if ((rc = wait_stream(b->ctx->stream, 0)) < 0) break;
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        if (ms) ms[k] = t;
+        if (t < best) {
+            best = t;
+            pick = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (size_t j = 0; j < b->jobs.size(); j++)
+        b->jobs[j].tr->kernel = cfgs[pick].kind == PHX_BATCH_PER_SCENE ? cfgs[pick].tracer_kernel : saved[j];
+    PHX_TRY(rc);
+    batch_drop_graph(b);
+    b->kind = cfgs[pick].kind;
+    b->threads = cfgs[pick].threads;
+    b->stack = cfgs[pick].stack;
+    if (kind) *kind = b->kind;
+    if (threads) *threads = b->threads;
+    if (stack) *stack = b->stack;
+    if (nconfigs) *nconfigs = (uint32_t)cfgs.size();
+    for (BatchJob& bj : b->jobs) bj.tr->have_last = false;  // the images hold tuning frames
+    return read_status(b->ctx);
+}
+
+int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    if (b->jobs.empty()) return fail(PHX_ERR_INVALID, "empty batch");
+    PHX_TRY(use(b->ctx));
+    Ctx* c = b->ctx;
+    PHX_TRY(wait_stream(c->stream, 0));
+    batch_drop_graph(b);
+    for (phx_unet n : b->nets) phx_unet_destroy(n);
+    b->nets.clear();
+    b->net_of.assign(b->jobs.size(), -1);
+    PHX_TRY(batch_prepare(b));
+    if (!b->host_modes) PHX_CUDA(cudaHostAlloc((void**)&b->host_modes, b->jobs.size() * 4, cudaHostAllocDefault));
+    // One network per padded image shape (each holds buffers for its shape;
+    // nothing may be allocated while the frame is recorded), and a first
+    // frame outside the capture that sizes every scratch buffer.
+    std::vector<std::pair<uint32_t, uint32_t>> shapes;
+    const float strength[4] = {64.0f, 8.0f, 40.0f, 7.0f};
+    for (size_t j = 0; j < b->jobs.size(); j++) {
+        BatchJob& bj = b->jobs[j];
+        if (net) {
+            const std::pair<uint32_t, uint32_t> sh{(bj.h + 15) / 16, (bj.w + 15) / 16};
+            size_t k = 0;
+            while (k < shapes.size() && shapes[k] != sh) k++;
+            if (k == shapes.size()) {
+                shapes.push_back(sh);
+                phx_unet cl = nullptr;
+                PHX_TRY(clone_net(b->handle, net, &cl));
+                b->nets.push_back(cl);
+            }
+            b->net_of[j] = (int)k;
+        }
+    }
+    PHX_TRY(batch_trace(b));
+    for (size_t j = 0; j < b->jobs.size(); j++) {
+        BatchJob& bj = b->jobs[j];
+        if (b->net_of[j] >= 0)
+            PHX_TRY(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, bj.cam.view, 16,
+                                        threshold, 0, nullptr));
+        else
+            PHX_TRY(phx_denoise(b->handle, (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, strength, bj.cam.view, 0));
+    }
+    PHX_TRY(wait_stream(c->stream, 0));
+    PHX_TRY(read_status(c));
+
+    cudaGraph_t graph = nullptr;
+    PHX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int32_t rc = PHX_OK;
+    auto step = [&](int32_t r) {
+        if (rc == PHX_OK && r < 0) rc = r;
+    };
+    unsigned long long* stamps = (unsigned long long*)b->stamps.ptr;
+    k_stamp<<<1, 1, 0, c->stream>>>(stamps);
+    step(cuda_check(cudaMemcpyAsync(b->modes.ptr, b->host_modes, b->jobs.size() * 4, cudaMemcpyHostToDevice,
+                                    c->stream), "modes"));
+    for (size_t j = 0; j < b->jobs.size() && rc == PHX_OK; j++) {
+        phx_tracer tr = b->jobs[j].tr;
+        const uint32_t* mode = (const uint32_t*)b->modes.ptr + j;
+        step(launch_face_boxes(c->stream, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                               (phx_aabb*)tr->bvh.prims.ptr));
+        step(enqueue_build(c, tr->bvh, tr->nfaces, tr->leaf, Gate{mode, 1u}));
+        step(enqueue_refit(c, tr->bvh, tr->nfaces, false, Gate{mode, 0u}));
+        step(prepare(tr));
+    }
+    if (rc == PHX_OK) step(batch_trace(b));
+    for (size_t j = 0; j < b->jobs.size() && rc == PHX_OK; j++) {
+        BatchJob& bj = b->jobs[j];
+        if (b->net_of[j] >= 0)
+            step(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, bj.cam.view, 16,
+                                     threshold, 0, nullptr));
+        else
+            step(phx_denoise(b->handle, (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, strength, bj.cam.view, 0));
+        k_stamp<<<1, 1, 0, c->stream>>>(stamps + 1 + j);
+    }
+    const cudaError_t end = cudaStreamEndCapture(c->stream, &graph);
+    if (rc == PHX_OK) rc = cuda_check(end, "end capture");
+    if (rc == PHX_OK) rc = cuda_check(cudaGraphInstantiate(&b->exec, graph, 0), "instantiate frame graph");
+    if (graph) cudaGraphDestroy(graph);
+    if (rc < 0) batch_drop_graph(b);
+    return rc;
+}
+
+int32_t phx_batch_replay(phx_batch b, const uint32_t* modes) {
+    if (!b || !modes) return fail(PHX_ERR_INVALID, "null argument");
+    if (!b->exec) return fail(PHX_ERR_INVALID, "no captured frame (phx_batch_capture)");
+    PHX_TRY(use(b->ctx));
+    // the previous replay has read its modes before they are overwritten
+    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    for (size_t j = 0; j < b->jobs.size(); j++) b->host_modes[j] = modes[j] ? 1u : 0u;
+    PHX_CUDA(cudaGraphLaunch(b->exec, b->ctx->stream));
+    PHX_CUDA(cudaEventRecord(b->done, b->ctx->stream));
+    batch_mark_traced(b);
+    return PHX_OK;
+}
+
+int32_t phx_batch_results(phx_batch b, uint64_t* latency_ns, uint64_t* rays) {
+    if (!b) return fail(PHX_ERR_INVALID, "null batch");
+    PHX_TRY(use(b->ctx));
+    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    const size_t nj = b->jobs.size();
+    if (latency_ns && b->stamps.ptr) {
+        std::vector<unsigned long long> st(nj + 1);
+        PHX_CUDA(cudaMemcpy(st.data(), b->stamps.ptr, (nj + 1) * 8, cudaMemcpyDeviceToHost));
+        for (size_t j = 0; j < nj; j++) latency_ns[j] = st[1 + j] - st[0];
+    }
+    if (rays && b->counters.ptr) {
+        std::vector<unsigned long long> ct(nj * 3);
+        PHX_CUDA(cudaMemcpy(ct.data(), b->counters.ptr, nj * 24, cudaMemcpyDeviceToHost));
+        for (size_t j = 0; j < nj; j++) rays[j] = ct[3 * j];
+    }
+    return read_status(b->ctx);
 }
 
 }  // extern "C"

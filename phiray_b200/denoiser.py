@@ -32,7 +32,7 @@ FEATURES = 16
 HEAD = 32
 TILE = 16
 # Mean predicted relative error of a tile above which the a-trous result is kept.
-THRESHOLD = 0.05
+THRESHOLD = 0.1
 
 
 def padded(n: int) -> int:

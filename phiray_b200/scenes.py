@@ -411,15 +411,18 @@ def _box(center, size, n):
     return v, np.concatenate(faces)
 
 
-def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bounces: int | None = None) -> Scene:
+def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bounces: int | None = None,
+               target: int | None = None) -> Scene:
     """One seeded procedural scene of the learned denoiser's training set:
     random boxes, spheres and noise-displaced spheres (plus a cloud of small
     triangles) on a ground plane, 10k-500k faces in total (log-uniform
     target), per-object or per-face albedo, some mirror objects, 1-4 area
     lights and sometimes an emissive panel, a dim uniform world, and a camera
-    on a random orbit around the objects."""
+    on a random orbit around the objects. `target` overrides the drawn face
+    budget (the cloud of small triangles fills up to it)."""
     rng = np.random.Generator(np.random.PCG64(SEED + 4 + 104729 * index))
-    target = int(math.exp(rng.uniform(math.log(1e4), math.log(5e5))))
+    drawn = int(math.exp(rng.uniform(math.log(1e4), math.log(5e5))))
+    target = drawn if target is None else int(target)
     parts, mats = [], []
 
     def add(v, f, kind):
@@ -512,3 +515,20 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
     b = int(rng.integers(4, 9)) if bounces is None else bounces
     return Scene(f"procedural_{index}", verts, faces, np.stack(mats).astype(np.float32), np.stack(lights), view,
                  width, height, spp, b, env=(env, env, env), meta={"index": index, "target": target})
+
+
+RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+
+
+def c5_batch(count: int = 64):
+    """Config 5's scenes: `count` procedural scenes with face counts
+    log-uniform over 10k-2M, resolutions drawn from 256^2, 512^2, 720p and
+    1080p, 1, 4 or 16 samples per pixel, 6 bounces (seeded)."""
+    rng = np.random.Generator(np.random.PCG64(SEED + 5))
+    out = []
+    for k in range(count):
+        tris = int(math.exp(rng.uniform(math.log(1e4), math.log(2e6))))
+        w, h = RESOLUTIONS[int(rng.integers(0, len(RESOLUTIONS)))]
+        spp = int(rng.choice([1, 4, 16]))
+        out.append(procedural(200000 + k, width=w, height=h, spp=spp, bounces=6, target=tris))
+    return out

@@ -25,7 +25,7 @@ import time
 import numpy as np
 
 from . import kernels, scenes
-from .denoiser import THRESHOLD, TILE, Unet, features
+from .denoiser import TILE, Unet, features
 from .gpu import Gpu, GpuArray
 from .tracer import PX_LEN, Tracer, camera
 
@@ -195,18 +195,21 @@ def train(gpu: Gpu, ds: DataSet, steps: int, batch: int, crop: int, lr: float, s
     return net, hist
 
 
-def evaluate(gpu: Gpu, net: Unet, noisy_px: np.ndarray, ref_rad: np.ndarray, w: int, h: int,
-             threshold: float = THRESHOLD) -> dict:
+def evaluate(gpu: Gpu, net: Unet, noisy_px: np.ndarray, ref_rad: np.ndarray, w: int, h: int) -> dict:
     """relMSE against the reference of the noisy image, the a-trous Denoise,
-    and the learned denoiser (without and with the per-tile fallback)."""
+    and the learned denoiser without and with the per-tile fallback at a few
+    thresholds (with the share of tiles that kept the a-trous result)."""
     out = {"noisy": relmse(radiance(noisy_px, w, h), ref_rad)}
     buf = GpuArray.from_(gpu, noisy_px)
     kernels.denoise(gpu, buf, w, h)
     out["denoise"] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
-    for name, thr in (("learned", 1e30), ("learned_fallback", threshold)):
+    tiles = ((w + TILE - 1) // TILE) * ((h + TILE - 1) // TILE)
+    for name, thr in [("learned", 1e30)] + [(f"fallback_{t:g}", t) for t in (0.02, 0.05, 0.1, 0.2, 0.5)]:
         buf.write(noisy_px)
-        net.denoise_px(buf, w, h, TILE, thr)
+        kept = net.denoise_px(buf, w, h, TILE, thr, count=True)
         out[name] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
+        if name != "learned":
+            out[name + "_tiles"] = kept / tiles
     buf.free()
     return out
 
