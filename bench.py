@@ -40,6 +40,9 @@ UNIT = "Mrays/s"
 WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 64 spp, 8 bounces, LBVH rebuild + trace + denoise per frame"
 
 
+KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8"]
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -104,6 +107,26 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def max_over_ranks(value: float, device: str = "cuda") -> float:
+    """The largest `value` over all ranks of the default process group (the
+    timing rule: a multi-GPU step takes as long as its slowest rank); the
+    value itself when there is no group."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, ms_max: float) -> float:
+    """Whole-job throughput of replicas: every rank processes `units_per_rank`
+    in (at most) ms_max milliseconds."""
+    return units_per_rank * world / (ms_max * 1e-3)
 
 
 def reference_arm(args) -> None:
@@ -408,7 +431,7 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     if not os.path.exists(WEIGHTS):
         return {"unavailable": f"no trained weights at {os.path.relpath(WEIGHTS, ROOT)}"}
     W, H, n = s.width, s.height, s.width * s.height
-    learned_spp = [1, 2, 4, 8, 16]
+    learned_spp = [1, 2, 4, 8, 16, 32, 64]
     plain_spp = [64, 128, 256, 512]
     tr = px.Tracer.of(gpu, s)
     net = Unet.pretrained(gpu)
@@ -468,10 +491,24 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
         "threshold": THRESHOLD,
     }
     if match is not None:
-        t_l = frame_ms(match, True, 5)
+        t_l = frame_ms(match, True, 3)
         out["learned"] = {"spp": match, "relmse": round(rel_learned[match], 6), "frame_ms": round(t_l, 3),
                           "frames_per_s": round(1000.0 / t_l, 3)}
         out["speedup_at_equal_relmse"] = round(t_plain / t_l, 2)
+        # the spp where the learned curve crosses the target (log-log between the
+        # measured neighbours), with the frame time scaled by samples: a
+        # finer estimate than the measured grid point, reported beside it
+        k = learned_spp.index(match)
+        if k > 0:
+            s0, s1 = learned_spp[k - 1], match
+            r0, r1 = rel_learned[s0], rel_learned[s1]
+            f = (np.log(target) - np.log(r0)) / (np.log(r1) - np.log(r0))
+            s_eq = float(np.exp(np.log(s0) + f * (np.log(s1) - np.log(s0))))
+            t_net = frame_ms(1, True, 3) - frame_ms(1, False, 3) + 0.0
+            t_trace_1 = (frame_ms(match, False, 2) - frame_ms(1, False, 3)) / max(match - 1, 1)
+            t_eq = frame_ms(1, False, 3) + t_trace_1 * (s_eq - 1) + t_net
+            out["interpolated"] = {"spp": round(s_eq, 2), "frame_ms": round(t_eq, 3),
+                                   "speedup": round(t_plain / t_eq, 2)}
     else:
         out["learned"] = None
         out["speedup_at_equal_relmse"] = None
@@ -551,6 +588,7 @@ def main() -> None:
         gpu.close()
         return
 
+    chosen, tune_ms = tr.autotune(cam, W, H, 1)  # the render kernel for this scene (keeps the image contract)
     for _ in range(args.warmup):
         step()
     barrier()
@@ -563,12 +601,8 @@ def main() -> None:
             step()
         e1.record(stream)
         barrier()
-    ms_step = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
-    value = rays_per_frame * world / (ms_step * 1e-3) / 1e6
+    ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps, f"cuda:{local}")
+    value = whole_job_rate(rays_per_frame, world, ms_step) / 1e6
 
     # Phase timings (same device, outside the headline loop).
     def timed(fn, reps):
@@ -629,12 +663,8 @@ def main() -> None:
     for _ in range(max(2, args.steps // 2)):
         e2e_step()
     barrier()
-    e2e_s = (time.perf_counter() - t0) / max(2, args.steps // 2)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = rays_per_frame * world / e2e_s / 1e6
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(2, args.steps // 2), f"cuda:{local}")
+    e2e = whole_job_rate(rays_per_frame, world, e2e_s * 1e3) / 1e6
 
     denoised = None if args.no_denoised else equal_relmse(args, gpu, s, cam, stream)
 
@@ -657,6 +687,8 @@ def main() -> None:
             "config": {"workload": WORKLOAD, "frame": f"{W}x{H}", "spp": args.spp, "bounces": s.bounces,
                        "tris": nf, "parallelism": f"replicas x{world}",
                        "l2": "scene ~300 MB of nodes/triangles/materials > 126 MB L2; the rebuild rewrites them each step"},
+            "render_kernel": {"chosen": KERNEL_NAMES[chosen],
+                              "ms_1spp": {KERNEL_NAMES[k]: round(v, 3) for k, v in enumerate(tune_ms)}},
             "frames_per_s": round(1000.0 / ms_step * world, 3),
             "rays_per_frame": int(rays_per_frame),
             "phases_ms": {"lbvh_build": round(build_ms, 3), "lbvh_refit": round(refit_ms, 3),

@@ -370,9 +370,9 @@ typedef struct phx_tracer_s* phx_tracer;
 int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* scene, phx_tracer* out);
 int32_t phx_tracer_destroy(phx_tracer tr);
 /* Which kernel traces a frame. All compute the same image bit for bit:
- * PHX_KERNEL_MEGAKERNEL is shade.wgsl's main as one thread per pixel with
- * the walk called from every site that traces; PHX_KERNEL_STATE_MACHINE
- * (the default) is a persistent kernel whose lanes take pixels from a
+ * PHX_KERNEL_MEGAKERNEL (the default) is shade.wgsl's main as one thread per
+ * pixel with the walk called from every site that traces;
+ * PHX_KERNEL_STATE_MACHINE is a persistent kernel whose lanes take pixels from a
  * counter and run the bounce loop as a state machine around one walk, so
  * lanes at different points of their paths still traverse together. Its
  * _6 and _8 forms cap registers for 6 or 8 resident 128-thread blocks per

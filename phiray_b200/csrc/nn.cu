@@ -178,32 +178,47 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
 }
 
-// Stages of the pipelined convolution: chunk c's tiles live in stage c % STAGES.
-constexpr int STAGES = 3;
-template <int N>
-struct Pipe {
-    static constexpr int A_BYTES = tc::BM * tc::BK * 2;
-    static constexpr int STAGE = A_BYTES + N * tc::BK * 2;
+// ---- the convolution forward: shifted descriptors over a staged patch ----
+//
+// One CTA computes a 16 x 8 block of output pixels of one image (M = 128:
+// m = 8 ty + tx, so each 8-row group of the MMA is one image row of 8
+// pixels) for N output channels. Input channels are taken CC at a time: the
+// (16 + 2) x (8 + 2) input patch of those channels is staged once in shared
+// memory in the canonical K-major layout — 16-byte pixel vectors of 8
+// channels, a patch row of 10 pixels every ROWB = 160 bytes, the 8-channel
+// groups LBO = 18 * 160 bytes apart — and the A operand of tap (dy, dx) is
+// the same patch seen through a descriptor whose start moves by
+// dy * ROWB + dx * 16 bytes (SBO = ROWB). The nine taps' MMAs read one
+// staged patch instead of nine gathered copies of it. The weights of the
+// nine taps for the CC channels (B tiles N x CC each) are staged beside it.
+// Chunks go through a STAGES-deep ring filled by cp.async (zero-filled
+// outside the image), each stage refilled after the mbarrier of the MMAs
+// that last read it.
+constexpr int TY = 16, TX = 8;
+constexpr int PY = TY + 2, PX = TX + 2;
+constexpr int ROWB = PX * 16;  // bytes of one patch row of one 8-channel group
+
+template <int N, int CC>
+struct Conv {
+    static constexpr int KG = CC / 8;                 // 8-channel groups a chunk
+    static constexpr int LBO_A = PY * ROWB;           // between channel groups of the patch
+    static constexpr int PATCH = KG * LBO_A;          // patch bytes
+    static constexpr int BTAP = N * CC * 2;           // one tap's weight tile
+    static constexpr int STAGE = (PATCH + 9 * BTAP + 127) / 128 * 128;
+    static constexpr int STAGES = N <= 32 ? 3 : 2;
     static constexpr int TOTAL = STAGES * STAGE;
 };
 
 // Y = act(conv3x3(X, W) + bias). OUT_F32: fp32 output (the network's head).
-//
-// One CTA: 128 pixels x N output channels, the K = 9 cin reduction in
-// chunks of 64 through a STAGES-deep ring of shared-memory tiles. Every
-// thread issues cp.async copies of its share of chunk c + STAGES - 1 (the
-// im2col rows, zero-filled at the image border and past K, and the weight
-// rows) while the tensor core works on chunk c; thread 0 issues chunk c's
-// four MMAs and commits them to the stage's mbarrier, which the threads
-// wait on before refilling that stage.
-template <int N, bool RELU, bool OUT_F32>
+template <int N, int CC, bool RELU, bool OUT_F32>
 __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
                                                   const float* __restrict__ bias, void* __restrict__ Y, Geo g,
                                                   uint32_t* status) {
+    using C = Conv<N, CC>;
+    constexpr int STAGES = C::STAGES;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar[STAGES];
     __shared__ uint32_t tmem_base;
-    using P = Pipe<N>;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tc::tmem_alloc(&tmem_base, tc::tmem_cols(N));
     if (tid == 0) {
@@ -214,57 +229,61 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tm = tmem_base;
-    const int row0 = blockIdx.x * tc::BM;
-    // This thread stages k-vector c = tid % 8 of rows tid / 8 + 16 j.
-    const int c = tid & 7;
-    PixRow rows[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) rows[j] = pix_row(row0 + (tid >> 3) + 16 * j, g);
-    const int nk = g.Kp / tc::BK;
+    const int tiles_x = (g.W + TX - 1) / TX, tiles_y = (g.H + TY - 1) / TY;
+    const int bx = blockIdx.x % tiles_x, by = (blockIdx.x / tiles_x) % tiles_y, img = blockIdx.x / (tiles_x * tiles_y);
+    const int y0 = by * TY, x0 = bx * TX;
+    const int nk = g.cin / CC;
 
     auto issue = [&](int chunk) {
-        uint8_t* a = smem + (chunk % STAGES) * P::STAGE;
-        uint8_t* b = a + P::A_BYTES;
-        const int k = chunk * tc::BK + c * 8;
-        const bool kin = k < g.K;
-        const int tap = kin ? k / g.cin : 0;
-        const int ci = k - tap * g.cin;
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int r = (tid >> 3) + 16 * j;
-            const int y = rows[j].y + dy, x = rows[j].x + dx;
-            const bool ok = kin && rows[j].b >= 0 && y >= 0 && y < g.H && x >= 0 && x < g.W;
-            const bf16* src = ok ? X + ((size_t)(rows[j].b * g.H + y) * g.W + x) * g.xs + g.xo + ci : X;
-            cp_async_ca16(a + tc::tile_off(r, c * 8, tc::BM), src, ok ? 16u : 0u);
+        uint8_t* patch = smem + (chunk % STAGES) * C::STAGE;
+        uint8_t* wb = patch + C::PATCH;
+        const int c0 = chunk * CC;
+        for (int v = tid; v < PY * PX * C::KG; v += 128) {
+            const int kg = v % C::KG, q = v / C::KG;
+            const int py = q / PX, px = q - py * PX;
+            const int y = y0 + py - 1, x = x0 + px - 1;
+            const bool ok = y >= 0 && y < g.H && x >= 0 && x < g.W;
+            const bf16* src = ok ? X + ((size_t)(img * g.H + y) * g.W + x) * g.xs + g.xo + c0 + kg * 8 : X;
+            cp_async_ca16(patch + kg * C::LBO_A + py * ROWB + px * 16, src, ok ? 16u : 0u);
         }
-        for (int v = tid; v < N * 8; v += 128) {
-            const int r = v >> 3, cc = v & 7;
-            cp_async_cg16(b + tc::tile_off(r, cc * 8, N), Wt + (size_t)r * g.Kp + chunk * tc::BK + cc * 8);
+        for (int v = tid; v < 9 * N * C::KG; v += 128) {
+            const int kg = v % C::KG, q = v / C::KG;
+            const int r = q % N, tap = q / N;
+            cp_async_cg16(wb + tap * C::BTAP + tc::tile_off(r, kg * 8, N),
+                          Wt + (size_t)r * g.Kp + tap * g.cin + c0 + kg * 8);
         }
     };
 
-    // Prologue: STAGES - 1 groups, empty past the last chunk, so that chunk c
-    // is always commit group c.
 #pragma unroll
     for (int s = 0; s < STAGES - 1; s++) {
         if (s < nk) issue(s);
         cp_async_commit();
     }
     bool ok = true;
+    constexpr uint32_t idesc = tc::instr_desc_bf16(tc::BM, N);
+    constexpr uint32_t b_lbo = (N / 8) * 128;
     for (int chunk = 0; chunk < nk; chunk++) {
-        cp_async_wait<STAGES - 2>();  // this thread's copies of `chunk` landed
+        cp_async_wait<STAGES - 2>();
         tc::fence_async_smem();
-        __syncthreads();              // and everyone's
+        __syncthreads();
         if (tid == 0) {
-            uint8_t* a = smem + (chunk % STAGES) * P::STAGE;
+            const uint32_t patch = tc::smem_addr(smem + (chunk % STAGES) * C::STAGE);
+            const uint32_t wb = patch + C::PATCH;
             tc::fence_after_sync();
-            tc::mma_chunk<N>(tm, a, a + P::A_BYTES, chunk == 0);
+#pragma unroll
+            for (int tap = 0; tap < 9; tap++) {
+                const uint32_t a0 = patch + (tap / 3) * ROWB + (tap % 3) * 16;
+#pragma unroll
+                for (int s = 0; s < CC / 16; s++) {
+                    const uint64_t da = tc::smem_desc(a0 + 2 * s * C::LBO_A, C::LBO_A, ROWB);
+                    const uint64_t db = tc::smem_desc(wb + tap * C::BTAP + 2 * s * b_lbo, b_lbo, 128);
+                    tc::mma_bf16(tm, da, db, idesc, (chunk == 0 && tap == 0 && s == 0) ? 0u : 1u);
+                }
+            }
             tc::mma_commit(&bar[chunk % STAGES]);
         }
         const int next = chunk + STAGES - 1;
         if (next < nk) {
-            // the stage `next` reuses held chunk - 1: its MMAs must be done
             if (chunk >= 1) ok = tc::mbar_wait(&bar[(chunk - 1) % STAGES], ((chunk - 1) / STAGES) & 1) && ok;
             issue(next);
         }
@@ -274,8 +293,10 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     ok = __syncthreads_and(ok);
     tc::fence_after_sync();
     if (ok) {
-        const int p = row0 + warp * 32 + lane;
-        const bool live = p < g.B * g.H * g.W;
+        const int m = warp * 32 + lane;
+        const int y = y0 + m / TX, x = x0 + m % TX;
+        const bool live = y < g.H && x < g.W;
+        const size_t p = ((size_t)img * g.H + y) * g.W + x;
 #pragma unroll 1
         for (int c0 = 0; c0 < N; c0 += 16) {
             float v[16];
@@ -287,11 +308,11 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
                 if (RELU) v[j] = fmaxf(v[j], 0.0f);
             }
             if (OUT_F32) {
-                float4* o = (float4*)((float*)Y + (size_t)p * g.ys + g.yo + c0);
+                float4* o = (float4*)((float*)Y + p * g.ys + g.yo + c0);
 #pragma unroll
                 for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             } else {
-                uint4* o = (uint4*)((bf16*)Y + (size_t)p * g.ys + g.yo + c0);
+                uint4* o = (uint4*)((bf16*)Y + p * g.ys + g.yo + c0);
                 o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
                                   pack_bf16x2(v[6], v[7]));
                 o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
@@ -403,63 +424,116 @@ __global__ void k_bias_grad(const bf16* __restrict__ dY, int dys, int dyo, int C
     if (c < C) atomicAdd(db + c, acc);
 }
 
+// The elementwise layers move 8 channels (one 16-byte vector) per thread;
+// every channel count, pitch and offset is a multiple of 8.
+union V8 {
+    uint4 u;
+    __nv_bfloat162 h[4];
+};
+
+__device__ __forceinline__ void unpack8(const uint4 u, float* f) {
+    V8 v;
+    v.u = u;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 t = __bfloat1622float2(v.h[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+
+__device__ __forceinline__ uint4 pack8(const float* f) {
+    return make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]),
+                      pack_bf16x2(f[6], f[7]));
+}
+
+__device__ __forceinline__ uint4 ld8(const bf16* p) { return *(const uint4*)p; }
+__device__ __forceinline__ void st8(bf16* p, uint4 v) { *(uint4*)p = v; }
+
 // dY *= (Y > 0): ReLU's gradient through its output.
 __global__ void k_relu_bwd(const bf16* __restrict__ Y, int ys, int yo, bf16* dY, int dys, int dyo, int C, int P) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)P * C) return;
-    const size_t p = i / C;
-    const int c = (int)(i - p * C);
-    if (!(bf(Y[p * ys + yo + c]) > 0.0f)) dY[p * dys + dyo + c] = __float2bfloat16(0.0f);
+    const int cv = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * cv) return;
+    const int p = i / cv, c = (i - p * cv) * 8;
+    float y[8], d[8];
+    unpack8(ld8(Y + (size_t)p * ys + yo + c), y);
+    bf16* dp = dY + (size_t)p * dys + dyo + c;
+    unpack8(ld8(dp), d);
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+        if (!(y[j] > 0.0f)) d[j] = 0.0f;
+    st8(dp, pack8(d));
 }
 
 // 2x2 average pool: X (B, H, W, pitch xs, offset xo) -> Y (B, H/2, W/2, C contiguous).
 __global__ void k_pool_fwd(const bf16* __restrict__ X, int xs, int xo, int C, int B, int H, int W, bf16* __restrict__ Y) {
-    const int h = H / 2, w = W / 2;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)B * h * w * C) return;
-    const int c = (int)(i % C);
-    const size_t q = i / C;
-    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
-    const size_t p00 = ((size_t)(b * H + 2 * y) * W + 2 * x);
-    const float s = bf(X[p00 * xs + xo + c]) + bf(X[(p00 + 1) * xs + xo + c]) + bf(X[(p00 + W) * xs + xo + c]) +
-                    bf(X[(p00 + W + 1) * xs + xo + c]);
-    Y[i] = __float2bfloat16(0.25f * s);
+    const int h = H / 2, w = W / 2, cv = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * h * w * cv) return;
+    const int q = i / cv, c = (i - q * cv) * 8;
+    const int x = q % w, y = (q / w) % h, b = q / (w * h);
+    const size_t p00 = (size_t)(b * H + 2 * y) * W + 2 * x;
+    float s[8], t[8];
+    unpack8(ld8(X + p00 * xs + xo + c), s);
+    unpack8(ld8(X + (p00 + 1) * xs + xo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(ld8(X + (p00 + W) * xs + xo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(ld8(X + (p00 + W + 1) * xs + xo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] = 0.25f * (s[j] + t[j]);
+    st8(Y + (size_t)q * C + c, pack8(s));
 }
 
 // Its gradient, added into dX (B, H, W, pitch dxs, offset dxo).
 __global__ void k_pool_bwd(const bf16* __restrict__ dY, int C, int B, int H, int W, bf16* dX, int dxs, int dxo) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)B * H * W * C) return;
-    const int c = (int)(i % C);
-    const size_t p = i / C;
-    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-    const float g = 0.25f * bf(dY[((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]);
-    bf16* d = dX + p * dxs + dxo + c;
-    *d = __float2bfloat16(bf(*d) + g);
+    const int cv = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * H * W * cv) return;
+    const int p = i / cv, c = (i - p * cv) * 8;
+    const int x = p % W, y = (p / W) % H, b = p / (W * H);
+    float g[8], d[8];
+    unpack8(ld8(dY + ((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c), g);
+    bf16* dp = dX + (size_t)p * dxs + dxo + c;
+    unpack8(ld8(dp), d);
+#pragma unroll
+    for (int j = 0; j < 8; j++) d[j] += 0.25f * g[j];
+    st8(dp, pack8(d));
 }
 
 // Nearest 2x upsample: X (B, H/2, W/2, C contiguous) -> Y (B, H, W, pitch ys, offset yo).
 __global__ void k_up_fwd(const bf16* __restrict__ X, int C, int B, int H, int W, bf16* __restrict__ Y, int ys, int yo) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)B * H * W * C) return;
-    const int c = (int)(i % C);
-    const size_t p = i / C;
-    const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-    Y[p * ys + yo + c] = X[((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c];
+    const int cv = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * H * W * cv) return;
+    const int p = i / cv, c = (i - p * cv) * 8;
+    const int x = p % W, y = (p / W) % H, b = p / (W * H);
+    st8(Y + (size_t)p * ys + yo + c, ld8(X + ((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c));
 }
 
 // Its gradient: dX (B, H/2, W/2, C contiguous) = sum of the 4 children.
 __global__ void k_up_bwd(const bf16* __restrict__ dY, int dys, int dyo, int C, int B, int H, int W, bf16* __restrict__ dX) {
-    const int h = H / 2, w = W / 2;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)B * h * w * C) return;
-    const int c = (int)(i % C);
-    const size_t q = i / C;
-    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
-    const size_t p00 = ((size_t)(b * H + 2 * y) * W + 2 * x);
-    const float s = bf(dY[p00 * dys + dyo + c]) + bf(dY[(p00 + 1) * dys + dyo + c]) + bf(dY[(p00 + W) * dys + dyo + c]) +
-                    bf(dY[(p00 + W + 1) * dys + dyo + c]);
-    dX[i] = __float2bfloat16(s);
+    const int h = H / 2, w = W / 2, cv = C / 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * h * w * cv) return;
+    const int q = i / cv, c = (i - q * cv) * 8;
+    const int x = q % w, y = (q / w) % h, b = q / (w * h);
+    const size_t p00 = (size_t)(b * H + 2 * y) * W + 2 * x;
+    float s[8], t[8];
+    unpack8(ld8(dY + p00 * dys + dyo + c), s);
+    unpack8(ld8(dY + (p00 + 1) * dys + dyo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(ld8(dY + (p00 + W) * dys + dyo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(ld8(dY + (p00 + W + 1) * dys + dyo + c), t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    st8(dX + (size_t)q * C + c, pack8(s));
 }
 
 // W2[ci][(8 - tap) * cout + co] = W[co][tap * cin + ci]: the weights of the
@@ -713,24 +787,31 @@ __global__ void k_compose(const float* __restrict__ out, const float* __restrict
     px[i] = pack_rgba(shown, __uint_as_float(px[24 * n + i]) * k);
 }
 
-template <int N, bool RELU, bool F32>
+template <int N, int CC, bool RELU, bool F32>
 int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
-    const int smem = Pipe<N>::TOTAL;
+    const int smem = Conv<N, CC>::TOTAL;
     static std::atomic<uint64_t> done{0};
-    PHX_TRY(smem_limit(k_conv_fwd<N, RELU, F32>, smem, c->device, done));
-    const int P = g.B * g.H * g.W;
-    k_conv_fwd<N, RELU, F32><<<(P + tc::BM - 1) / tc::BM, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
+    PHX_TRY(smem_limit(k_conv_fwd<N, CC, RELU, F32>, smem, c->device, done));
+    const uint32_t blocks = (uint32_t)g.B * ((g.H + TY - 1) / TY) * ((g.W + TX - 1) / TX);
+    k_conv_fwd<N, CC, RELU, F32><<<blocks, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
     return cuda_check(cudaGetLastError(), "conv fwd");
+}
+
+// Channels a chunk: 32 where they divide cin and the stage stays small, else 16.
+template <int N, bool RELU, bool F32>
+int32_t conv_fwd_cc(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
+    if (N <= 64 && g.cin % 32 == 0) return conv_fwd_n<N, 32, RELU, F32>(c, X, W, bias, Y, g);
+    return conv_fwd_n<N, 16, RELU, F32>(c, X, W, bias, Y, g);
 }
 
 template <bool RELU, bool F32>
 int32_t conv_fwd_any(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
     switch (g.cout) {
-        case 32: return conv_fwd_n<32, RELU, F32>(c, X, W, bias, Y, g);
-        case 64: return conv_fwd_n<64, RELU, F32>(c, X, W, bias, Y, g);
-        case 96: return conv_fwd_n<96, RELU, F32>(c, X, W, bias, Y, g);
-        case 128: return conv_fwd_n<128, RELU, F32>(c, X, W, bias, Y, g);
-        case 160: return conv_fwd_n<160, RELU, F32>(c, X, W, bias, Y, g);
+        case 32: return conv_fwd_cc<32, RELU, F32>(c, X, W, bias, Y, g);
+        case 64: return conv_fwd_cc<64, RELU, F32>(c, X, W, bias, Y, g);
+        case 96: return conv_fwd_cc<96, RELU, F32>(c, X, W, bias, Y, g);
+        case 128: return conv_fwd_cc<128, RELU, F32>(c, X, W, bias, Y, g);
+        case 160: return conv_fwd_cc<160, RELU, F32>(c, X, W, bias, Y, g);
     }
     return fail(PHX_ERR_INVALID, "conv: output tile of %d channels (32, 64, 96, 128 or 160)", g.cout);
 }
@@ -753,8 +834,8 @@ int32_t wgrad_n(Ctx* c, const bf16* X, const bf16* dY, int dys, int dyo, float* 
 
 int32_t check_geo(const Geo& g) {
     if (g.B <= 0 || g.H <= 0 || g.W <= 0) return fail(PHX_ERR_INVALID, "conv: empty image");
-    if (g.cin % 8 || g.xs % 8 || g.xo % 8 || g.ys % 8 || g.yo % 8)
-        return fail(PHX_ERR_INVALID, "conv: channels, pitches and offsets must be multiples of 8");
+    if (g.cin % 16 || g.xs % 8 || g.xo % 8 || g.ys % 8 || g.yo % 8)
+        return fail(PHX_ERR_INVALID, "conv: cin a multiple of 16, pitches and offsets multiples of 8");
     if (g.Kp % 64 || g.Kp < g.K) return fail(PHX_ERR_INVALID, "conv: Kp %d must cover K %d in steps of 64", g.Kp, g.K);
     if (g.xo < 0 || g.xo + g.cin > g.xs || g.yo < 0 || g.yo + g.cout > g.ys)
         return fail(PHX_ERR_INVALID, "conv: channel window outside the pixel pitch");
@@ -816,48 +897,53 @@ int32_t phx_nn_bias_grad(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, 
 
 int32_t phx_nn_relu_bwd(phx_ctx ctx, const void* Y, int32_t ys, int32_t yo, void* dY, int32_t dys, int32_t dyo,
                         int32_t C, int32_t P) {
-    if (!ctx || !Y || !dY || C <= 0 || P <= 0 || yo < 0 || yo + C > ys || dyo < 0 || dyo + C > dys)
+    if (!ctx || !Y || !dY || C <= 0 || C % 8 || P <= 0 || yo < 0 || yo + C > ys || dyo < 0 || dyo + C > dys ||
+        (ys | yo | dys | dyo) % 8)
         return fail(PHX_ERR_INVALID, "relu bwd arguments");
     PHX_TRY(use(&ctx->c));
-    k_relu_bwd<<<blocks_for((size_t)P * C), 256, 0, ctx->c.stream>>>((const bf16*)Y, ys, yo, (bf16*)dY, dys, dyo, C, P);
+    k_relu_bwd<<<blocks_for((size_t)P * (C / 8)), 256, 0, ctx->c.stream>>>((const bf16*)Y, ys, yo, (bf16*)dY, dys, dyo, C, P);
     return cuda_check(cudaGetLastError(), "relu bwd");
 }
 
 int32_t phx_nn_pool_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t C, int32_t B, int32_t H, int32_t W,
                         void* Y) {
-    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || xo < 0 || xo + C > xs)
+    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || C % 8 || H % 2 || W % 2 || xo < 0 ||
+        xo + C > xs || (xs | xo) % 8)
         return fail(PHX_ERR_INVALID, "pool arguments");
     PHX_TRY(use(&ctx->c));
-    k_pool_fwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * C), 256, 0, ctx->c.stream>>>((const bf16*)X, xs, xo, C, B, H,
+    k_pool_fwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * (C / 8)), 256, 0, ctx->c.stream>>>((const bf16*)X, xs, xo, C, B, H,
                                                                                         W, (bf16*)Y);
     return cuda_check(cudaGetLastError(), "pool fwd");
 }
 
 int32_t phx_nn_pool_bwd(phx_ctx ctx, const void* dY, int32_t C, int32_t B, int32_t H, int32_t W, void* dX, int32_t dxs,
                         int32_t dxo) {
-    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || dxo < 0 || dxo + C > dxs)
+    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || C % 8 || H % 2 || W % 2 || dxo < 0 ||
+        dxo + C > dxs || (dxs | dxo) % 8)
         return fail(PHX_ERR_INVALID, "pool arguments");
     PHX_TRY(use(&ctx->c));
-    k_pool_bwd<<<blocks_for((size_t)B * H * W * C), 256, 0, ctx->c.stream>>>((const bf16*)dY, C, B, H, W, (bf16*)dX, dxs,
+    k_pool_bwd<<<blocks_for((size_t)B * H * W * (C / 8)), 256, 0, ctx->c.stream>>>((const bf16*)dY, C, B, H, W, (bf16*)dX, dxs,
                                                                               dxo);
     return cuda_check(cudaGetLastError(), "pool bwd");
 }
 
 int32_t phx_nn_up_fwd(phx_ctx ctx, const void* X, int32_t C, int32_t B, int32_t H, int32_t W, void* Y, int32_t ys,
                       int32_t yo) {
-    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || yo < 0 || yo + C > ys)
+    if (!ctx || !X || !Y || B <= 0 || H <= 0 || W <= 0 || C <= 0 || C % 8 || H % 2 || W % 2 || yo < 0 ||
+        yo + C > ys || (ys | yo) % 8)
         return fail(PHX_ERR_INVALID, "upsample arguments");
     PHX_TRY(use(&ctx->c));
-    k_up_fwd<<<blocks_for((size_t)B * H * W * C), 256, 0, ctx->c.stream>>>((const bf16*)X, C, B, H, W, (bf16*)Y, ys, yo);
+    k_up_fwd<<<blocks_for((size_t)B * H * W * (C / 8)), 256, 0, ctx->c.stream>>>((const bf16*)X, C, B, H, W, (bf16*)Y, ys, yo);
     return cuda_check(cudaGetLastError(), "up fwd");
 }
 
 int32_t phx_nn_up_bwd(phx_ctx ctx, const void* dY, int32_t dys, int32_t dyo, int32_t C, int32_t B, int32_t H, int32_t W,
                       void* dX) {
-    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || H % 2 || W % 2 || dyo < 0 || dyo + C > dys)
+    if (!ctx || !dY || !dX || B <= 0 || H <= 0 || W <= 0 || C <= 0 || C % 8 || H % 2 || W % 2 || dyo < 0 ||
+        dyo + C > dys || (dys | dyo) % 8)
         return fail(PHX_ERR_INVALID, "upsample arguments");
     PHX_TRY(use(&ctx->c));
-    k_up_bwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * C), 256, 0, ctx->c.stream>>>((const bf16*)dY, dys, dyo, C, B,
+    k_up_bwd<<<blocks_for((size_t)B * (H / 2) * (W / 2) * (C / 8)), 256, 0, ctx->c.stream>>>((const bf16*)dY, dys, dyo, C, B,
                                                                                       H, W, (bf16*)dX);
     return cuda_check(cudaGetLastError(), "up bwd");
 }

@@ -1239,7 +1239,7 @@ struct phx_tracer_s {
     BvhWork bvh;
     uint32_t w = 0, h = 0;
     uint32_t frame = 0, target = 1024;
-    uint32_t kernel = PHX_KERNEL_STATE_MACHINE;  // which render kernel traces a frame
+    uint32_t kernel = PHX_KERNEL_MEGAKERNEL;  // which render kernel traces a frame (the fastest measured)
     DevMem next;                                 // the state-machine kernel's pixel counter
     bool smem_stack = false;                     // ray walks keep their stack in shared memory
     bool have_last = false;
@@ -1765,6 +1765,10 @@ int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w,
 namespace phx {
 namespace {
 
+// A serving frame of many scenes can take seconds: the batch's host waits
+// allow two minutes before they report PHX_ERR_TIMEOUT.
+constexpr uint32_t BATCH_WAIT_MS = 120000;
+
 __global__ void k_stamp(unsigned long long* dst) {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1856,7 +1860,7 @@ int32_t batch_prepare(phx_batch b) {
     b->ntiles = tile;
     PHX_TRY(b->djobs.reserve(nj * sizeof(Job)));
     PHX_CUDA(cudaMemcpyAsync(b->djobs.ptr, host.data(), nj * sizeof(Job), cudaMemcpyHostToDevice, c->stream));
-    return wait_stream(c->stream, 0);  // the pageable sources are released on return
+    return wait_stream(c->stream, BATCH_WAIT_MS);  // the pageable sources are released on return
 }
 
 // The frame's traces, stream-ordered (capturable once batch_prepare ran).
@@ -1932,7 +1936,7 @@ int32_t phx_batch_create(phx_ctx ctx, phx_batch* out) {
 int32_t phx_batch_clear(phx_batch b) {
     if (!b) return fail(PHX_ERR_INVALID, "null batch");
     PHX_TRY(use(b->ctx));
-    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    PHX_TRY(wait_stream(b->ctx->stream, BATCH_WAIT_MS));
     batch_drop_graph(b);
     for (phx_unet n : b->nets) phx_unet_destroy(n);
     b->nets.clear();
@@ -2024,7 +2028,7 @@ int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint3
         cudaEventRecord(e0, b->ctx->stream);
         if ((rc = batch_trace(b)) < 0) break;
         cudaEventRecord(e1, b->ctx->stream);
-        if ((rc = wait_stream(b->ctx->stream, 0)) < 0) break;
+        if ((rc = wait_stream(b->ctx->stream, BATCH_WAIT_MS)) < 0) break;
         float t = 0.0f;
         cudaEventElapsedTime(&t, e0, e1);
         if (ms) ms[k] = t;
@@ -2055,7 +2059,7 @@ int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
     if (b->jobs.empty()) return fail(PHX_ERR_INVALID, "empty batch");
     PHX_TRY(use(b->ctx));
     Ctx* c = b->ctx;
-    PHX_TRY(wait_stream(c->stream, 0));
+    PHX_TRY(wait_stream(c->stream, BATCH_WAIT_MS));
     batch_drop_graph(b);
     for (phx_unet n : b->nets) phx_unet_destroy(n);
     b->nets.clear();
@@ -2091,7 +2095,7 @@ int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
         else
             PHX_TRY(phx_denoise(b->handle, (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, strength, bj.cam.view, 0));
     }
-    PHX_TRY(wait_stream(c->stream, 0));
+    PHX_TRY(wait_stream(c->stream, BATCH_WAIT_MS));
     PHX_TRY(read_status(c));
 
     cudaGraph_t graph = nullptr;
@@ -2136,7 +2140,7 @@ int32_t phx_batch_replay(phx_batch b, const uint32_t* modes) {
     if (!b->exec) return fail(PHX_ERR_INVALID, "no captured frame (phx_batch_capture)");
     PHX_TRY(use(b->ctx));
     // the previous replay has read its modes before they are overwritten
-    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    PHX_TRY(wait_stream(b->ctx->stream, BATCH_WAIT_MS));
     for (size_t j = 0; j < b->jobs.size(); j++) b->host_modes[j] = modes[j] ? 1u : 0u;
     PHX_CUDA(cudaGraphLaunch(b->exec, b->ctx->stream));
     PHX_CUDA(cudaEventRecord(b->done, b->ctx->stream));
@@ -2147,7 +2151,7 @@ int32_t phx_batch_replay(phx_batch b, const uint32_t* modes) {
 int32_t phx_batch_results(phx_batch b, uint64_t* latency_ns, uint64_t* rays) {
     if (!b) return fail(PHX_ERR_INVALID, "null batch");
     PHX_TRY(use(b->ctx));
-    PHX_TRY(wait_stream(b->ctx->stream, 0));
+    PHX_TRY(wait_stream(b->ctx->stream, BATCH_WAIT_MS));
     const size_t nj = b->jobs.size();
     if (latency_ns && b->stamps.ptr) {
         std::vector<unsigned long long> st(nj + 1);
