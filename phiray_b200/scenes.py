@@ -415,7 +415,9 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
                target: int | None = None) -> Scene:
     """One seeded procedural scene of the learned denoiser's training set:
     random boxes, spheres and noise-displaced spheres (plus a cloud of small
-    triangles) on a ground plane, 10k-500k faces in total (log-uniform
+    triangles; in about a third of the scenes a finely tessellated displaced
+    sphere with per-face albedo and mirror faces fills much of the view) on a
+    ground plane, 10k-500k faces in total (log-uniform
     target), per-object or per-face albedo, some mirror objects, 1-4 area
     lights and sometimes an emissive panel, a dim uniform world, and a camera
     on a random orbit around the objects. `target` overrides the drawn face
@@ -463,7 +465,15 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
         mats.append(lambert(rng.uniform(0.2, 0.8, 3)))
         parts.append((np.asarray(w[0], np.float32), w[1]))
     used = 0
-    for _ in range(int(rng.integers(2, 8))):
+    hero = rng.random() < 0.35
+    if hero:  # a finely tessellated, noise-displaced sphere filling much of the view
+        v, f = _icosphere(6 if rng.random() < 0.6 else 7)
+        r = 1.0 + rng.uniform(0.03, 0.1) * value_noise(v, int(rng.integers(1 << 30)))
+        s_h = rng.uniform(0.4, 0.65)
+        v = v * (r * s_h)[:, None] + np.array([0.0, ground_y + s_h * 1.05, 0.0])
+        add(v, f, "mixed" if rng.random() < 0.7 else "faces")
+        used += len(f)
+    for _ in range(int(rng.integers(2, 8) if not hero else rng.integers(0, 4))):
         c = np.array([rng.uniform(-0.9, 0.9), 0.0, rng.uniform(-0.9, 0.9)])
         s = rng.uniform(0.15, 0.5)
         t = rng.random()
@@ -507,14 +517,14 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
     verts, faces = _assemble(parts)
     az = rng.uniform(0.0, 2.0 * math.pi)
     el = math.radians(rng.uniform(5.0, 40.0))
-    dist = rng.uniform(1.8, 3.2)
+    dist = rng.uniform(1.4, 2.2) if hero else rng.uniform(1.8, 3.2)
     look = np.array([0.0, ground_y + 0.4, 0.0])
     eye = look + dist * np.array([math.cos(el) * math.sin(az), math.sin(el), -math.cos(el) * math.cos(az)])
     view = View.look(tuple(eye), tuple(look - eye), (0.0, 1.0, 0.0), rng.uniform(35.0, 55.0))
     env = rng.uniform(0.0, 0.2)
     b = int(rng.integers(4, 9)) if bounces is None else bounces
     return Scene(f"procedural_{index}", verts, faces, np.stack(mats).astype(np.float32), np.stack(lights), view,
-                 width, height, spp, b, env=(env, env, env), meta={"index": index, "target": target})
+                 width, height, spp, b, env=(env, env, env), meta={"index": index, "target": target, "hero": hero})
 
 
 RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
