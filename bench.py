@@ -196,6 +196,7 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
         rays = torch.empty((n, 8), dtype=torch.float32, device=f"cuda:{local}")
         hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
         tr.secondary_rays(cam, W, H, 0, rays)
+        tr.set_walk(args.walk)
         fn = lambda: tr.trace_rays(rays, n, hits, False)  # noqa: E731
     for _ in range(args.warmup):
         fn()
@@ -533,6 +534,7 @@ def main() -> None:
     ap.add_argument("--ref-spp", type=int, default=4096, help="samples of the equal-relMSE reference render")
     ap.add_argument("--plain-spp", type=int, default=256, help="samples of the plain tracer + Denoise")
     ap.add_argument("--no-denoised", action="store_true", help="skip the equal-relMSE comparison")
+    ap.add_argument("--walk", type=int, default=0, help="ray walk of --phase rays: 0 a thread per ray, 1 persistent")
     ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build", "nn"],
                     help="all: the benchmark; render/rays/build: only that kernel's launches (profiling runs)")
     args = ap.parse_args()
@@ -637,7 +639,11 @@ def main() -> None:
     rays = torch.empty((n, 8), dtype=torch.float32, device=f"cuda:{local}")
     hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
     tr.secondary_rays(cam, W, H, 0, rays)
-    inc_ms = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
+    walk_ms = {}
+    for name, mode in (("thread_per_ray", px.Tracer.WALK_THREAD), ("persistent_fetch", px.Tracer.WALK_FETCH)):
+        tr.set_walk(mode)
+        walk_ms[name] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
+    inc_ms = min(walk_ms.values())
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
     ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
     prim_ms = timed(lambda: tr.primary(cam, W, H, 0, ids, ts), 10)
@@ -696,6 +702,7 @@ def main() -> None:
             "lbvh_build_gbs": round(412 * nf / (build_ms * 1e-3) / 1e9, 1),
             "lbvh_refit_gbs": round(172 * nf / (refit_ms * 1e-3) / 1e9, 1),
             "incoherent_grays": round(n / (inc_ms * 1e-3) / 1e9, 3),
+            "incoherent_grays_by_walk": {k: round(n / (v * 1e-3) / 1e9, 3) for k, v in walk_ms.items()},
             "primary_grays": round(n / (prim_ms * 1e-3) / 1e9, 3),
             "roofline": {"bound": "hbm", "kernel": "k_render (path-trace megakernel)", "achieved": round(achieved, 1),
                          "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),

@@ -395,6 +395,13 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
 #define PHX_STACK_LOCAL 0u
 #define PHX_STACK_SHARED 1u
 int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
+/* How ray-buffer walks (phx_trace_rays) are scheduled: PHX_WALK_THREAD, one
+ * thread per ray (the default); PHX_WALK_FETCH, persistent warps whose idle
+ * lanes take the next rays from a counter between rounds of 16 visits. Each
+ * ray is walked in the same order either way: the same hits. */
+#define PHX_WALK_THREAD 0u
+#define PHX_WALK_FETCH 1u
+int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
 /* Tracer::set_samples: the sample target `sample` stops at. */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
 /* Tracer::sample / sample_in (src/trace/sample.rs:94-249): one more sample

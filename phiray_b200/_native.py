@@ -139,6 +139,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_set_samples": (i32, [vp, u32]),
     "phx_tracer_set_kernel": (i32, [vp, u32]),
     "phx_tracer_set_stack": (i32, [vp, u32]),
+    "phx_tracer_set_walk": (i32, [vp, u32]),
     "phx_tracer_autotune": (i32, [vp, vp, u32, u32, u32, C.POINTER(u32), C.POINTER(C.c_float)]),
     "phx_tracer_sample": (i32, [vp, vp, u32, u32, u32, vp, C.POINTER(u32), C.POINTER(i32)]),
     "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),

@@ -5,6 +5,7 @@
 // the engine's own parity check against a plain matrix product.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "../../include/phiray_math.h"
@@ -327,6 +328,153 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     if (warp == 0) tc::tmem_free(tm, tc::tmem_cols(N));
 }
 
+// ---- the same convolution, persistent and weight-stationary ----
+//
+// Used when the layer's weights (9 taps x N x cin bf16) and two input
+// patches fit in shared memory. Each CTA loads the weights once and walks
+// the output tiles blockIdx.x, + gridDim.x, ...; the tensor memory holds two
+// accumulators of N columns (at column 0 and at the power of two >= N). Iteration i: thread 0 issues tile i's MMAs
+// (9 taps x cin / 16, shifted descriptors over patch buffer i & 1) into
+// accumulator i & 1 and commits them to mbarrier i & 1; meanwhile every
+// thread waits for tile i - 1's MMAs, refills patch buffer (i + 1) & 1
+// with tile i + 1's patch and writes tile i - 1's outputs from accumulator
+// (i - 1) & 1. So the copies and the epilogue of neighbouring tiles run
+// under the current tile's MMAs.
+template <int N>
+struct ConvWS {
+    static constexpr int W_BYTES_PER_CIN = 9 * N * 2;  // x cin
+    static constexpr int PATCH_PER_CIN = PY * ROWB / 8; // x cin (= 360 bytes a channel)
+    static size_t bytes(int cin) { return (size_t)cin * (W_BYTES_PER_CIN + 2 * PATCH_PER_CIN); }
+};
+
+template <int N, bool RELU, bool OUT_F32>
+__global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
+                                                 const float* __restrict__ bias, void* __restrict__ Y, Geo g,
+                                                 uint32_t* status) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // accumulator b at column b * ACC (a power of two: aligned like a whole allocation)
+    constexpr uint32_t ACC = tc::tmem_cols(N);
+    constexpr uint32_t COLS = 2 * ACC;
+    if (warp == 0) tc::tmem_alloc(&tmem_base, COLS);
+    if (tid == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        fence_barrier_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = tmem_base;
+    const int KG = g.cin / 8;
+    const int LBO_A = PY * ROWB;
+    const int PATCH = KG * LBO_A;
+    const int BTAP = N * g.cin * 2;
+    uint8_t* wsm = smem;
+    uint8_t* patch0 = smem + 9 * BTAP;
+    const int tiles_x = (g.W + TX - 1) / TX, tiles_y = (g.H + TY - 1) / TY;
+    const int ntiles = g.B * tiles_x * tiles_y;
+
+    // the weights, once
+    for (int v = tid; v < 9 * N * KG; v += 128) {
+        const int kg = v % KG, q = v / KG;
+        const int r = q % N, tap = q / N;
+        cp_async_cg16(wsm + tap * BTAP + tc::tile_off(r, kg * 8, N), Wt + (size_t)r * g.Kp + tap * g.cin + kg * 8);
+    }
+    cp_async_commit();
+    auto issue_patch = [&](int tile, int buf) {
+        const int bx = tile % tiles_x, by = (tile / tiles_x) % tiles_y, img = tile / (tiles_x * tiles_y);
+        const int y0 = by * TY, x0 = bx * TX;
+        uint8_t* patch = patch0 + buf * PATCH;
+        for (int v = tid; v < PY * PX * KG; v += 128) {
+            const int kg = v % KG, q = v / KG;
+            const int py = q / PX, px = q - py * PX;
+            const int y = y0 + py - 1, x = x0 + px - 1;
+            const bool ok = y >= 0 && y < g.H && x >= 0 && x < g.W;
+            const bf16* src = ok ? X + ((size_t)(img * g.H + y) * g.W + x) * g.xs + g.xo + kg * 8 : X;
+            cp_async_ca16(patch + kg * LBO_A + py * ROWB + px * 16, src, ok ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    auto epilogue = [&](int tile, int buf) {
+        const int bx = tile % tiles_x, by = (tile / tiles_x) % tiles_y, img = tile / (tiles_x * tiles_y);
+        const int m = warp * 32 + lane;
+        const int y = by * TY + m / TX, x = bx * TX + m % TX;
+        const bool live = y < g.H && x < g.W;
+        const size_t p = ((size_t)img * g.H + y) * g.W + x;
+#pragma unroll 1
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)buf * ACC + (uint32_t)c0, v);
+            if (!live) continue;
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                v[j] += __ldg(bias + c0 + j);
+                if (RELU) v[j] = fmaxf(v[j], 0.0f);
+            }
+            if (OUT_F32) {
+                float4* o = (float4*)((float*)Y + p * g.ys + g.yo + c0);
+#pragma unroll
+                for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                uint4* o = (uint4*)((bf16*)Y + p * g.ys + g.yo + c0);
+                o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                  pack_bf16x2(v[6], v[7]));
+                o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                  pack_bf16x2(v[14], v[15]));
+            }
+        }
+        tc::fence_before_sync();
+    };
+
+    constexpr uint32_t idesc = tc::instr_desc_bf16(tc::BM, N);
+    constexpr uint32_t b_lbo = (N / 8) * 128;
+    bool ok = true;
+    int i = 0, prev = -1;
+    if ((int)blockIdx.x < ntiles) issue_patch(blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
+        const int b = i & 1;
+        cp_async_wait<0>();  // this thread's copies of tile i (and the weights)
+        tc::fence_async_smem();
+        __syncthreads();     // everyone's; and the last epilogue's TMEM reads
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t pa = tc::smem_addr(patch0 + b * PATCH);
+            const uint32_t wa = tc::smem_addr(wsm);
+            const uint32_t acc = tm + (uint32_t)b * ACC;
+            for (int tap = 0; tap < 9; tap++) {
+                const uint32_t a0 = pa + (tap / 3) * ROWB + (tap % 3) * 16;
+                for (int s = 0; s < g.cin / 16; s++) {
+                    const uint64_t da = tc::smem_desc(a0 + 2 * s * LBO_A, LBO_A, ROWB);
+                    const uint64_t db = tc::smem_desc(wa + tap * BTAP + 2 * s * b_lbo, b_lbo, 128);
+                    tc::mma_bf16(acc, da, db, idesc, (tap == 0 && s == 0) ? 0u : 1u);
+                }
+            }
+            tc::mma_commit(&bar[b]);
+        }
+        if (i >= 1) ok = tc::mbar_wait(&bar[b ^ 1], ((i - 1) >> 1) & 1) && ok;  // tile i - 1's MMAs done
+        const int next = tile + gridDim.x;
+        if (next < ntiles) issue_patch(next, b ^ 1);
+        if (i >= 1) {
+            tc::fence_after_sync();
+            epilogue(prev, b ^ 1);
+        }
+        prev = tile;
+    }
+    if (i >= 1) {
+        ok = tc::mbar_wait(&bar[(i - 1) & 1], ((i - 1) >> 1) & 1) && ok;
+        tc::fence_after_sync();
+        epilogue(prev, (i - 1) & 1);
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) atomicOr(status, STATUS_SPIN_LIMIT);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tm, COLS);
+}
+
 // Weight gradient: dWt[k][co] += sum over pixels p of im2col(X)[p][k] dY[p][co].
 // GEMM rows = k (a 128-row block per CTA), N = cout, the reduction over the
 // pixel range of this CTA's split, 64 pixels a chunk; the tiles are written
@@ -561,27 +709,54 @@ __global__ void k_flip(const bf16* __restrict__ W, int cout, int cin, int Kp, bf
 // (rel_p the pixel's own relative error, held constant) to dlogits (bf16,
 // pitch 32; zero on padding pixels and on logits 26..31).
 // Buffers are [B][Hp][Wp] x channels; pixels with y >= h or x >= w are padding.
-__global__ void k_kpn(const float* __restrict__ logits, const float* __restrict__ irr, const float* __restrict__ alb,
-                      const float* __restrict__ ref, int B, int Hp, int Wp, int h, int w, float* __restrict__ out,
-                      float* __restrict__ err, bf16* __restrict__ dlogits, float* loss, float scale, float err_weight) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int P = B * Hp * Wp;
+__global__ void __launch_bounds__(256) k_kpn(const float* __restrict__ logits, const float* __restrict__ irr,
+                                             const float* __restrict__ alb, const float* __restrict__ ref, int B,
+                                             int Hp, int Wp, int h, int w, float* __restrict__ out,
+                                             float* __restrict__ err, bf16* __restrict__ dlogits, float* loss,
+                                             float scale, float err_weight) {
+    // The 20 x 20 clamped neighbourhood of this block's 16 x 16 pixels.
+    __shared__ float tile[20][20][3];
+    const int bx = blockIdx.x * 16, by = blockIdx.y * 16, b = blockIdx.z;
+    for (int k = threadIdx.x; k < 400; k += 256) {
+        const int ly = k / 20, lx = k - ly * 20;
+        const int yy = min(max(by + ly - 2, 0), h - 1), xx = min(max(bx + lx - 2, 0), w - 1);
+        const float* q = irr + ((size_t)(b * Hp + yy) * Wp + xx) * 3;
+        tile[ly][lx][0] = q[0];
+        tile[ly][lx][1] = q[1];
+        tile[ly][lx][2] = q[2];
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x = bx + tx, y = by + ty;
+    const bool inside = x < Wp && y < Hp;
+    const size_t p = ((size_t)b * Hp + y) * Wp + x;
     float lsum = 0.0f;
-    if (p < P) {
-        const int x = p % Wp, y = (p / Wp) % Hp, b = p / (Wp * Hp);
+    if (inside) {
         const bool valid = y < h && x < w;
         if (!valid) {
             if (out)
-                for (int c = 0; c < 3; c++) out[(size_t)p * 3 + c] = 0.0f;
+                for (int c = 0; c < 3; c++) out[p * 3 + c] = 0.0f;
             if (err) err[p] = 0.0f;
             if (ref && dlogits)
-                for (int t = 0; t < 32; t++) dlogits[(size_t)p * 32 + t] = __float2bfloat16(0.0f);
+                for (int t = 0; t < 32; t++) dlogits[p * 32 + t] = __float2bfloat16(0.0f);
         } else {
             float wt[25], mx = -3.0e38f;
+            const float4* lg = (const float4*)(logits + p * 32);
+            float e = 0.0f;
 #pragma unroll
-            for (int t = 0; t < 25; t++) {
-                wt[t] = logits[(size_t)p * 32 + t];
-                mx = fmaxf(mx, wt[t]);
+            for (int q = 0; q < 7; q++) {
+                const float4 v = __ldg(lg + q);
+                const float f[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int t = 4 * q + j;
+                    if (t < 25) {
+                        wt[t] = f[j];
+                        mx = fmaxf(mx, f[j]);
+                    } else if (t == 25) {
+                        e = f[j];
+                    }
+                }
             }
             float z = 0.0f;
 #pragma unroll
@@ -590,31 +765,28 @@ __global__ void k_kpn(const float* __restrict__ logits, const float* __restrict_
                 z += wt[t];
             }
             const float iz = 1.0f / z;
-            float s[3] = {0.0f, 0.0f, 0.0f};
-            int nb[25];
+            float sm[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
             for (int t = 0; t < 25; t++) {
                 wt[t] *= iz;
-                const int yy = min(max(y + t / 5 - 2, 0), h - 1), xx = min(max(x + t % 5 - 2, 0), w - 1);
-                nb[t] = (b * Hp + yy) * Wp + xx;
+                const float* nb = tile[ty + t / 5][tx + t % 5];
 #pragma unroll
-                for (int c = 0; c < 3; c++) s[c] += wt[t] * irr[(size_t)nb[t] * 3 + c];
+                for (int c = 0; c < 3; c++) sm[c] += wt[t] * nb[c];
             }
             float a[3], o[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                a[c] = alb[(size_t)p * 3 + c];
-                o[c] = a[c] * s[c];
+                a[c] = alb[p * 3 + c];
+                o[c] = a[c] * sm[c];
             }
             if (out)
-                for (int c = 0; c < 3; c++) out[(size_t)p * 3 + c] = o[c];
-            const float e = logits[(size_t)p * 32 + 25];
+                for (int c = 0; c < 3; c++) out[p * 3 + c] = o[c];
             if (err) err[p] = fmaxf(pm_exp(e) - 1.0e-3f, 0.0f);
             if (ref) {
                 float go[3], rel = 0.0f;
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const float r = ref[(size_t)p * 3 + c], d = o[c] - r, den = r * r + 0.01f;
+                    const float r = ref[p * 3 + c], d = o[c] - r, den = r * r + 0.01f;
                     rel += d * d / den;
                     go[c] = 2.0f * d / den * scale * a[c];
                 }
@@ -624,12 +796,12 @@ __global__ void k_kpn(const float* __restrict__ logits, const float* __restrict_
                 float gw[25], dot = 0.0f;
 #pragma unroll
                 for (int t = 0; t < 25; t++) {
-                    const float* q = irr + (size_t)nb[t] * 3;
-                    gw[t] = go[0] * q[0] + go[1] * q[1] + go[2] * q[2];
+                    const float* nb = tile[ty + t / 5][tx + t % 5];
+                    gw[t] = go[0] * nb[0] + go[1] * nb[1] + go[2] * nb[2];
                     dot += wt[t] * gw[t];
                 }
                 if (dlogits) {
-                    bf16* d = dlogits + (size_t)p * 32;
+                    bf16* d = dlogits + p * 32;
 #pragma unroll
                     for (int t = 0; t < 25; t++) d[t] = __float2bfloat16(wt[t] * (gw[t] - dot));
                     d[25] = __float2bfloat16(ge);
@@ -797,9 +969,28 @@ int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void
     return cuda_check(cudaGetLastError(), "conv fwd");
 }
 
-// Channels a chunk: 32 where they divide cin and the stage stays small, else 16.
+constexpr size_t WS_MAX_SMEM = 200 * 1024;
+
+template <int N, bool RELU, bool F32>
+int32_t conv_ws_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
+    const int smem = (int)ConvWS<N>::bytes(g.cin);
+    static std::atomic<uint64_t> done{0};
+    PHX_TRY(smem_limit(k_conv_ws<N, RELU, F32>, (int)WS_MAX_SMEM, c->device, done));
+    int per_sm = 0;
+    PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_ws<N, RELU, F32>, 128, smem));
+    // two accumulators of N columns per CTA share the SM's 512 TMEM columns
+    per_sm = std::min(per_sm > 0 ? per_sm : 1, (int)(512 / (2 * tc::tmem_cols(N))));
+    const int ntiles = g.B * ((g.H + TY - 1) / TY) * ((g.W + TX - 1) / TX);
+    const int grid = std::min(ntiles, per_sm * c->sms);
+    k_conv_ws<N, RELU, F32><<<grid, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
+    return cuda_check(cudaGetLastError(), "conv fwd (weight-stationary)");
+}
+
+// The weight-stationary form where its smem fits (N <= 128), else chunks of
+// 32 channels where they divide cin and the stage stays small, else 16.
 template <int N, bool RELU, bool F32>
 int32_t conv_fwd_cc(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
+    if (N <= 128 && ConvWS<N>::bytes(g.cin) <= WS_MAX_SMEM) return conv_ws_n<N, RELU, F32>(c, X, W, bias, Y, g);
     if (N <= 64 && g.cin % 32 == 0) return conv_fwd_n<N, 32, RELU, F32>(c, X, W, bias, Y, g);
     return conv_fwd_n<N, 16, RELU, F32>(c, X, W, bias, Y, g);
 }
@@ -961,10 +1152,10 @@ int32_t phx_nn_kpn(phx_ctx ctx, const float* logits, const float* irr, const flo
     if (!ctx || !logits || !irr || !alb) return fail(PHX_ERR_INVALID, "null argument");
     if (B <= 0 || h <= 0 || w <= 0 || h > Hp || w > Wp) return fail(PHX_ERR_INVALID, "kpn: bad image size");
     PHX_TRY(use(&ctx->c));
-    const int P = B * Hp * Wp;
     const float scale = 1.0f / (3.0f * (float)B * (float)h * (float)w);
-    k_kpn<<<(P + 255) / 256, 256, 0, ctx->c.stream>>>(logits, irr, alb, ref, B, Hp, Wp, h, w, out, err, (bf16*)dlogits,
-                                                      loss, scale, err_weight);
+    const dim3 grid((Wp + 15) / 16, (Hp + 15) / 16, B);
+    k_kpn<<<grid, 256, 0, ctx->c.stream>>>(logits, irr, alb, ref, B, Hp, Wp, h, w, out, err, (bf16*)dlogits, loss,
+                                           scale, err_weight);
     return cuda_check(cudaGetLastError(), "kpn");
 }
 

@@ -1216,9 +1216,151 @@ __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict_
     }
 }
 
+// The same walks on persistent warps that refill idle lanes: every lane
+// keeps one ray's traversal state (position in the tree, its 32-entry stack,
+// best hit) and advances it STEPS node or leaf visits at a time; between
+// rounds the lanes whose ray finished take the next rays from one counter
+// (one atomic per warp). Each ray is walked in exactly its own order, so the
+// hits are those of k_rays; the warp no longer idles while its longest ray
+// finishes.
+constexpr int RAY_STEPS = 16;
+
+template <bool ANY, bool STATS>
+__global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __restrict__ rays, uint32_t n,
+                                                    float4* __restrict__ hits, unsigned long long* counters,
+                                                    uint32_t* next) {
+    load_info(S);
+    const Tree T = tree_of(S);
+    const int lane = threadIdx.x & 31;
+    Count cnt{0, 0, 0};
+    uint32_t stack[STACK];
+    bool active = false;
+    uint32_t idx = 0, nd = 0;
+    int sp = 0;
+    f3 o = mk(0.0f), inv = mk(0.0f);
+    RaySpace rs;
+    rs.kz = 2u;
+    rs.flip = false;
+    rs.s = mk(0.0f);
+    Hit best{0.0f, NONE, 0.0f, 0.0f};
+    for (;;) {
+        const uint32_t need = __ballot_sync(0xffffffffu, !active);
+        if (need) {
+            const int leader = __ffs(need) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next, (uint32_t)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active) {
+                idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                if (idx < n) {
+                    const float4 a = __ldg(rays + 2 * (size_t)idx), b = __ldg(rays + 2 * (size_t)idx + 1);
+                    o = mk(a.x, a.y, a.z);
+                    const f3 d = mk(b.x, b.y, b.z);
+                    cnt.rays++;
+                    best = Hit{a.w, NONE, 0.0f, 0.0f};
+                    inv = safe_inv(d);
+                    rs = ray_space(d);
+                    sp = 0;
+                    nd = T.root;
+                    active = box_t(T.root_lo, T.root_hi, o, inv, best.t) < INF;
+                    if (!active) {
+                        hits[idx] = make_float4(best.t, __uint_as_float(NONE), 0.0f, 0.0f);
+                    }
+                    // a ray that misses the root box is written and the lane asks again next round
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) {
+            // nothing in flight: done once the counter has passed n
+            uint32_t seen = 0;
+            if (lane == 0) seen = atomicAdd(next, 0u);
+            seen = __shfl_sync(0xffffffffu, seen, 0);
+            if (seen >= n) break;
+            continue;
+        }
+        for (int it = 0; it < RAY_STEPS && active; it++) {
+            bool done = false;
+            if (nd & LEAF) {
+                for (uint32_t id = nd & ~LEAF; id < T.nslots; id++) {
+                    const float4 A = __ldg(T.tris + 3 * (size_t)id);
+                    const float4 B = __ldg(T.tris + 3 * (size_t)id + 1);
+                    const float4 Cc = __ldg(T.tris + 3 * (size_t)id + 2);
+                    const uint32_t flags = __float_as_uint(Cc.w);
+                    if (STATS) cnt.tests++;
+                    float u, v;
+                    const float t = tri_t(xyz(A), xyz(B), xyz(Cc), o, rs, u, v);
+                    if (t < best.t) {
+                        if (ANY) {
+                            if (!(flags & FLAG_PASS)) {
+                                best = Hit{t, id, u, v};
+                                done = true;
+                                break;
+                            }
+                        } else {
+                            best = Hit{t, id, u, v};
+                        }
+                    }
+                    if (flags & FLAG_END) break;
+                }
+            } else {
+                if (STATS) cnt.steps++;
+                const float4* q = T.nodes + 4 * (size_t)nd;
+                const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
+                const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);
+                const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
+                const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
+                if (tl < INF && tr < INF) {
+                    if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
+                    nd = tl <= tr ? l : r;
+                    continue;
+                }
+                if (tl < INF) {
+                    nd = l;
+                    continue;
+                }
+                if (tr < INF) {
+                    nd = r;
+                    continue;
+                }
+            }
+            if (!done) {
+                if (sp == 0) {
+                    done = true;
+                } else {
+                    sp--;
+                    nd = stack[sp];
+                }
+            }
+            if (done) {
+                const uint32_t face = best.tri == NONE ? NONE : __float_as_uint(__ldg(T.tris + 3 * (size_t)best.tri).w);
+                hits[idx] = make_float4(best.t, __uint_as_float(face), best.u, best.v);
+                active = false;
+            }
+        }
+    }
+    const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
+    (void)tot;
+    if (STATS) {
+        const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
+        const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
+        if (lane == 0) {
+            atomicAdd(counters + 1, (unsigned long long)st);
+            atomicAdd(counters + 2, (unsigned long long)te);
+        }
+    }
+}
+
 template <bool ANY, bool STATS>
 void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters, bool smem,
-                 cudaStream_t s) {
+                 cudaStream_t s, uint32_t* next = nullptr, int sms = 0) {
+    if (next) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rays_fetch<ANY, STATS>, 128, 0);
+        const uint32_t grid = std::min<uint32_t>((uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms, (n + 127) / 128);
+        cudaMemsetAsync(next, 0, 4, s);
+        k_rays_fetch<ANY, STATS><<<grid, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters, next);
+        return;
+    }
     if (smem)
         k_rays<ANY, STATS, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters);
     else
@@ -1242,6 +1384,7 @@ struct phx_tracer_s {
     uint32_t kernel = PHX_KERNEL_MEGAKERNEL;  // which render kernel traces a frame (the fastest measured)
     DevMem next;                                 // the state-machine kernel's pixel counter
     bool smem_stack = false;                     // ray walks keep their stack in shared memory
+    uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, or persistent warps
     bool have_last = false;
     phx_camera last;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1550,6 +1693,13 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
     return PHX_OK;
 }
 
+int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode) {
+    if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
+    if (mode > PHX_WALK_FETCH) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
+    tr->walk = mode;
+    return PHX_OK;
+}
+
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
     tr->target = samples ? samples : 1;
@@ -1718,8 +1868,9 @@ int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits
     if (n == 0) return PHX_OK;
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
-    if (any_hit) launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream);
-    else launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream);
+    uint32_t* nx = tr->walk == PHX_WALK_FETCH ? (uint32_t*)tr->next.ptr : nullptr;
+    if (any_hit) launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms);
+    else launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms);
     return cuda_check(cudaGetLastError(), "trace rays");
 }
 
@@ -1731,8 +1882,11 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
     PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
     const Scene S = scene_of(tr);
     if (n) {
-        if (any_hit) launch_rays<true, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s);
-        else launch_rays<false, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s);
+        uint32_t* nx = tr->walk == PHX_WALK_FETCH ? (uint32_t*)tr->next.ptr : nullptr;
+        if (any_hit)
+            launch_rays<true, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s, nx, tr->ctx->sms);
+        else
+            launch_rays<false, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s, nx, tr->ctx->sms);
         PHX_CUDA(cudaGetLastError());
     }
     PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));

@@ -142,6 +142,14 @@ class Tracer:
         """Ray-buffer walks keep their stack in shared (True) or local memory."""
         N.check(N.lib().phx_tracer_set_stack(self.handle, 1 if shared else 0))
 
+    WALK_THREAD = 0
+    WALK_FETCH = 1
+
+    def set_walk(self, mode: int) -> None:
+        """Ray-buffer walks: Tracer.WALK_THREAD (a thread per ray) or
+        Tracer.WALK_FETCH (persistent warps refilling idle lanes); same hits."""
+        N.check(N.lib().phx_tracer_set_walk(self.handle, mode))
+
     def set_samples(self, n: int) -> None:
         N.check(N.lib().phx_tracer_set_samples(self.handle, n))
 

@@ -124,6 +124,31 @@ def test_conv_fwd(gpu, cin, cout, relu, f32):
     assert np.all(got[..., :yo] == sentinel) and np.all(got[..., yo + cout:] == np.float32(sentinel))
 
 
+@pytest.mark.parametrize("cin,cout,shape", [(16, 32, (2, 256, 384)), (32, 64, (1, 256, 256)),
+                                            (96, 32, (1, 256, 256))])
+def test_conv_fwd_many_tiles_per_block(gpu, cin, cout, shape):
+    """Images with more 16 x 8 tiles than resident blocks: the persistent,
+    weight-stationary form walks several tiles per block through its two
+    patch buffers and two tensor-memory accumulators."""
+    import torch
+
+    rng = np.random.default_rng(cin * 31 + cout)
+    B, H, W = shape
+    x = nn.bf16(rng.normal(size=(B, H, W, cin)))
+    w, wp, Kp = _weights(rng, cout, cin)
+    bias = rng.normal(size=cout).astype(np.float32) * 0.1
+    X, Wt, bb = _t(x, "bf16"), _t(wp, "bf16"), _t(bias)
+    Y = torch.empty((B, H, W, cout), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().phx_nn_conv_fwd(gpu.handle, X.data_ptr(), cin, 0, cin, Wt.data_ptr(), Kp, bb.data_ptr(),
+                                    Y.data_ptr(), cout, 0, cout, B, H, W, 1, 0))
+    _sync(gpu)
+    got = _np(Y)
+    want = nn.conv(x, w, bias.astype(np.float64), True)
+    mag = nn.conv(np.abs(x), np.abs(w), np.abs(bias), False)
+    assert np.all(np.abs(got - want) <= 2.0 ** -8 * np.abs(want) + 1e-5 * mag + 1e-30)
+
+
 @pytest.mark.parametrize("cin,cout,shape", [(16, 32, (2, 12, 20)), (96, 96, (1, 16, 24)), (288, 128, (2, 8, 8)),
                                             (32, 160, (1, 64, 96)), (64, 64, (1, 64, 96))])
 def test_conv_wgrad(gpu, cin, cout, shape):

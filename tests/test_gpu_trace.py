@@ -127,7 +127,8 @@ def test_primary_hit_ids(gpu, orc, name):
     assert np.array_equal(ts.cpu().numpy(), want_t)
 
 
-def test_ray_buffer_walks(gpu, orc):
+@pytest.mark.parametrize("walk", [0, 1], ids=["thread_per_ray", "persistent_fetch"])
+def test_ray_buffer_walks(gpu, orc, walk):
     import torch
 
     s = SCENES["c2_small"]()
@@ -140,6 +141,7 @@ def test_ray_buffer_walks(gpu, orc):
     rays[:, 0:3], rays[:, 3], rays[:, 4:7] = o, 3.0e38, d
     rays[::5, 3] = 0.3  # some bounded rays
     tr = px.Tracer.of(gpu, s)
+    tr.set_walk(walk)
     dr = torch.tensor(rays, device="cuda")
     hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
     T = oracle_lib.TraceOracle(orc, s)
