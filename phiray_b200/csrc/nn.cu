@@ -32,12 +32,14 @@ struct Plan {
     static constexpr int TOTAL = B_OFF + B_BYTES + B_ROOM;
 };
 
-// Raises a kernel's dynamic shared-memory limit once per device.
+// Raises a kernel's dynamic shared-memory limit (and carveout) once per device.
 template <typename F>
 int32_t smem_limit(F* kernel, int bytes, int device, std::atomic<uint64_t>& done) {
     const uint64_t bit = 1ull << (device & 63);
     if (done.load(std::memory_order_acquire) & bit) return PHX_OK;
     PHX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    // the largest shared-memory carveout, so that several blocks fit an SM
+    PHX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     done.fetch_or(bit, std::memory_order_release);
     return PHX_OK;
 }
@@ -976,10 +978,12 @@ int32_t conv_ws_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void*
     const int smem = (int)ConvWS<N>::bytes(g.cin);
     static std::atomic<uint64_t> done{0};
     PHX_TRY(smem_limit(k_conv_ws<N, RELU, F32>, (int)WS_MAX_SMEM, c->device, done));
-    int per_sm = 0;
-    PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_ws<N, RELU, F32>, 128, smem));
-    // two accumulators of N columns per CTA share the SM's 512 TMEM columns
-    per_sm = std::min(per_sm > 0 ? per_sm : 1, (int)(512 / (2 * tc::tmem_cols(N))));
+    // Blocks per SM: by shared memory (the SM's 228 KB less 1 KB per block,
+    // this kernel's 1 KB of static data), by the 512 TMEM columns (two
+    // accumulators a block) and by threads.
+    const int by_smem = (228 * 1024) / (smem + 2 * 1024);
+    const int by_tmem = (int)(512 / (2 * tc::tmem_cols(N)));
+    const int per_sm = std::max(1, std::min(std::min(by_smem, by_tmem), 16));
     const int ntiles = g.B * ((g.H + TY - 1) / TY) * ((g.W + TX - 1) / TX);
     const int grid = std::min(ntiles, per_sm * c->sms);
     k_conv_ws<N, RELU, F32><<<grid, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);

@@ -88,6 +88,45 @@ def render_pairs(gpu: Gpu, scene, segments, ref_spp: int, chunk: int = 256):
     return noisy, ref
 
 
+def render_group(gpu: Gpu, scs, segments, ref_spp: int, chunk: int = 256):
+    """render_pairs for several scenes at once: every pass traces all the
+    scenes' frames in one persistent batch launch (a single 256 x 256 image
+    cannot fill the GPU on its own)."""
+    from .batch import Batch
+
+    trs = [Tracer.of(gpu, sc) for sc in scs]
+    cams = [camera(sc) for sc in scs]
+    b = Batch(gpu)
+
+    def run(first: int, spp: int) -> None:
+        b.clear()
+        for sc, tr, cam in zip(scs, trs, cams):
+            b.add(tr, cam, sc.width, sc.height, first, spp)
+        b.trace()
+
+    frame = 0
+    prev = [None] * len(scs)
+    noisy = [[] for _ in scs]
+    for spp in segments:
+        run(frame, spp)
+        frame += spp
+        for k, (sc, tr) in enumerate(zip(scs, trs)):
+            img = tr.image()
+            noisy[k].append(px_diff(img, prev[k], sc.width * sc.height))
+            prev[k] = img
+    left = ref_spp
+    while left > 0:
+        c = min(chunk, left)
+        run(frame, c)
+        frame += c
+        left -= c
+    refs = [px_diff(tr.image(), prev[k], sc.width * sc.height) for k, (sc, tr) in enumerate(zip(scs, trs))]
+    b.close()
+    for tr in trs:
+        tr.close()
+    return noisy, refs
+
+
 class DataSet:
     """Device-resident training pairs: features, demodulated radiance and
     remodulation planes of each noisy image, and its reference radiance."""
@@ -151,20 +190,62 @@ class DataSet:
         return [torch.stack(o).contiguous() for o in outs]
 
 
-def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print):
+def _scene(i: int, size: int):
+    return scenes.procedural(i, width=size, height=size)
+
+
+def scene_stream(indices, size: int, workers: int):
+    """Procedural scenes in order, generated ahead on `workers` host
+    processes (spawned, so no CUDA state is inherited) while the GPU renders."""
+    indices = list(indices)
+    if workers <= 1:
+        for i in indices:
+            yield _scene(i, size)
+        return
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        ahead = 2 * workers
+        futs = [ex.submit(_scene, i, size) for i in indices[:ahead]]
+        for k in range(len(indices)):
+            if k + ahead < len(indices):
+                futs.append(ex.submit(_scene, indices[k + ahead], size))
+            yield futs[k].result()
+            futs[k] = None
+
+
+GROUP = 16  # scenes rendered together in one batch launch
+
+
+def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, workers: int = 0):
+    indices = list(indices)
     ds = DataSet(gpu, len(indices) * len(segments), size)
     refs, noisy_all = [], []
     t0 = time.time()
-    for j, i in enumerate(indices):
-        sc = scenes.procedural(i, width=size, height=size)
-        noisy, ref = render_pairs(gpu, sc, segments, ref_spp)
-        rr = radiance(ref, size, size)
-        for spp, px in zip(segments, noisy):
-            ds.add(px, rr, spp)
-        refs.append(rr)
-        noisy_all.append(noisy)
-        if (j + 1) % 10 == 0:
-            log(f"rendered {j + 1}/{len(indices)} scenes ({time.time() - t0:.1f} s)")
+    if workers <= 0:
+        import os
+
+        workers = max(1, min(8, (os.cpu_count() or 2) - 1))
+    group = []
+
+    def flush():
+        noisy_g, refs_g = render_group(gpu, group, segments, ref_spp)
+        for noisy, ref in zip(noisy_g, refs_g):
+            rr = radiance(ref, size, size)
+            for spp, px in zip(segments, noisy):
+                ds.add(px, rr, spp)
+            refs.append(rr)
+            noisy_all.append(noisy)
+        group.clear()
+        log(f"rendered {len(refs)}/{len(indices)} scenes ({time.time() - t0:.1f} s)")
+
+    for sc in scene_stream(indices, size, workers):
+        group.append(sc)
+        if len(group) == GROUP:
+            flush()
+    if group:
+        flush()
     return ds, refs, noisy_all
 
 
