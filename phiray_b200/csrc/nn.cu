@@ -346,7 +346,8 @@ template <int N>
 struct ConvWS {
     static constexpr int W_BYTES_PER_CIN = 9 * N * 2;  // x cin
     static constexpr int PATCH_PER_CIN = PY * ROWB / 8; // x cin (= 360 bytes a channel)
-    static size_t bytes(int cin) { return (size_t)cin * (W_BYTES_PER_CIN + 2 * PATCH_PER_CIN); }
+    static constexpr int PATCHES = 3;  // the tile being multiplied and the next two in flight
+    static size_t bytes(int cin) { return (size_t)cin * (W_BYTES_PER_CIN + PATCHES * PATCH_PER_CIN); }
 };
 
 template <int N, bool RELU, bool OUT_F32>
@@ -433,17 +434,24 @@ __global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, con
 
     constexpr uint32_t idesc = tc::instr_desc_bf16(tc::BM, N);
     constexpr uint32_t b_lbo = (N / 8) * 128;
+    constexpr int NP = ConvWS<N>::PATCHES;
     bool ok = true;
     int i = 0, prev = -1;
-    if ((int)blockIdx.x < ntiles) issue_patch(blockIdx.x, 0);
+    // Prologue: tiles 0 and 1 of this block in flight (commit groups 1, 2 after
+    // the weights' group 0; an empty group stands in for a missing tile).
+    for (int k = 0; k < NP - 1; k++) {
+        const int t = blockIdx.x + k * gridDim.x;
+        if (t < ntiles) issue_patch(t, k);
+        else cp_async_commit();
+    }
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, i++) {
         const int b = i & 1;
-        cp_async_wait<0>();  // this thread's copies of tile i (and the weights)
+        cp_async_wait<NP - 2>();  // this thread's copies of tile i (and the weights) landed
         tc::fence_async_smem();
-        __syncthreads();     // everyone's; and the last epilogue's TMEM reads
+        __syncthreads();          // everyone's; and the last epilogue's TMEM reads
         if (tid == 0) {
             tc::fence_after_sync();
-            const uint32_t pa = tc::smem_addr(patch0 + b * PATCH);
+            const uint32_t pa = tc::smem_addr(patch0 + (i % NP) * PATCH);
             const uint32_t wa = tc::smem_addr(wsm);
             const uint32_t acc = tm + (uint32_t)b * ACC;
             for (int tap = 0; tap < 9; tap++) {
@@ -457,8 +465,10 @@ __global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, con
             tc::mma_commit(&bar[b]);
         }
         if (i >= 1) ok = tc::mbar_wait(&bar[b ^ 1], ((i - 1) >> 1) & 1) && ok;  // tile i - 1's MMAs done
-        const int next = tile + gridDim.x;
-        if (next < ntiles) issue_patch(next, b ^ 1);
+        // tile i + 2 into the patch buffer tile i - 1 used
+        const int ahead = tile + (NP - 1) * gridDim.x;
+        if (ahead < ntiles) issue_patch(ahead, (i + NP - 1) % NP);
+        else cp_async_commit();
         if (i >= 1) {
             tc::fence_after_sync();
             epilogue(prev, b ^ 1);

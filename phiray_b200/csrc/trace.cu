@@ -1224,7 +1224,6 @@ __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict_
 // hits are those of k_rays; the warp no longer idles while its longest ray
 // finishes.
 constexpr int RAY_STEPS = 16;
-constexpr uint32_t SENT = 0xFFFFFFFFu;  // no node: the stack ran empty
 
 template <bool ANY, bool STATS>
 __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __restrict__ rays, uint32_t n,
@@ -1280,40 +1279,9 @@ __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __res
             continue;
         }
         for (int it = 0; it < RAY_STEPS && active; it++) {
-            // Inner nodes first; the first leaf found is postponed and the
-            // lane keeps traversing until it finds a second one or every
-            // converged lane holds a leaf, so the leaf tests run together.
-            // Leaves are still tested in the order they are found, hence
-            // the same hits as the one-visit-at-a-time walk.
-            uint32_t pl = SENT;
-            while (nd != SENT) {
-                if (nd & LEAF) {
-                    if (pl != SENT) break;
-                    pl = nd;
-                    nd = sp > 0 ? stack[--sp] : SENT;
-                } else {
-                    if (STATS) cnt.steps++;
-                    const float4* q = T.nodes + 4 * (size_t)nd;
-                    const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
-                    const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);
-                    const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
-                    const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
-                    if (tl < INF && tr < INF) {
-                        if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
-                        nd = tl <= tr ? l : r;
-                    } else if (tl < INF) {
-                        nd = l;
-                    } else if (tr < INF) {
-                        nd = r;
-                    } else {
-                        nd = sp > 0 ? stack[--sp] : SENT;
-                    }
-                }
-                if (__all_sync(__activemask(), pl != SENT)) break;
-            }
             bool done = false;
-            if (pl != SENT) {
-                for (uint32_t id = pl & ~LEAF; id < T.nslots; id++) {
+            if (nd & LEAF) {
+                for (uint32_t id = nd & ~LEAF; id < T.nslots; id++) {
                     const float4 A = __ldg(T.tris + 3 * (size_t)id);
                     const float4 B = __ldg(T.tris + 3 * (size_t)id + 1);
                     const float4 Cc = __ldg(T.tris + 3 * (size_t)id + 2);
@@ -1334,8 +1302,35 @@ __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __res
                     }
                     if (flags & FLAG_END) break;
                 }
+            } else {
+                if (STATS) cnt.steps++;
+                const float4* q = T.nodes + 4 * (size_t)nd;
+                const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
+                const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);
+                const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
+                const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
+                if (tl < INF && tr < INF) {
+                    if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
+                    nd = tl <= tr ? l : r;
+                    continue;
+                }
+                if (tl < INF) {
+                    nd = l;
+                    continue;
+                }
+                if (tr < INF) {
+                    nd = r;
+                    continue;
+                }
             }
-            if (nd == SENT) done = true;  // nothing left to visit
+            if (!done) {
+                if (sp == 0) {
+                    done = true;
+                } else {
+                    sp--;
+                    nd = stack[sp];
+                }
+            }
             if (done) {
                 const uint32_t face = best.tri == NONE ? NONE : __float_as_uint(__ldg(T.tris + 3 * (size_t)best.tri).w);
                 hits[idx] = make_float4(best.t, __uint_as_float(face), best.u, best.v);
