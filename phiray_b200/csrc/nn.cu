@@ -271,15 +271,15 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
         __syncthreads();
         if (tid == 0) {
             const uint32_t patch = tc::smem_addr(smem + (chunk % STAGES) * C::STAGE);
-            const uint32_t wb = patch + C::PATCH;
             tc::fence_after_sync();
+            const uint64_t da0 = tc::smem_desc(patch, C::LBO_A, ROWB);
+            const uint64_t db0 = tc::smem_desc(patch + C::PATCH, b_lbo, 128);
 #pragma unroll
             for (int tap = 0; tap < 9; tap++) {
-                const uint32_t a0 = patch + (tap / 3) * ROWB + (tap % 3) * 16;
 #pragma unroll
                 for (int s = 0; s < CC / 16; s++) {
-                    const uint64_t da = tc::smem_desc(a0 + 2 * s * C::LBO_A, C::LBO_A, ROWB);
-                    const uint64_t db = tc::smem_desc(wb + tap * C::BTAP + 2 * s * b_lbo, b_lbo, 128);
+                    const uint64_t da = da0 + (uint64_t)(((tap / 3) * ROWB + (tap % 3) * 16 + 2 * s * C::LBO_A) >> 4);
+                    const uint64_t db = db0 + (uint64_t)((tap * C::BTAP + 2 * s * b_lbo) >> 4);
                     tc::mma_bf16(tm, da, db, idesc, (chunk == 0 && tap == 0 && s == 0) ? 0u : 1u);
                 }
             }
@@ -451,15 +451,21 @@ __global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, con
         __syncthreads();          // everyone's; and the last epilogue's TMEM reads
         if (tid == 0) {
             tc::fence_after_sync();
-            const uint32_t pa = tc::smem_addr(patch0 + (i % NP) * PATCH);
-            const uint32_t wa = tc::smem_addr(wsm);
             const uint32_t acc = tm + (uint32_t)b * ACC;
+            // Descriptors are built once; a step along K or to another tap
+            // adds its byte offset / 16 to the start-address field.
+            const uint64_t da0 = tc::smem_desc(tc::smem_addr(patch0 + (i % NP) * PATCH), LBO_A, ROWB);
+            const uint64_t db0 = tc::smem_desc(tc::smem_addr(wsm), b_lbo, 128);
+            const uint64_t a_step = (uint64_t)((2 * LBO_A) >> 4), b_step = (uint64_t)((2 * b_lbo) >> 4);
+            const int ks = g.cin / 16;
+#pragma unroll
             for (int tap = 0; tap < 9; tap++) {
-                const uint32_t a0 = pa + (tap / 3) * ROWB + (tap % 3) * 16;
-                for (int s = 0; s < g.cin / 16; s++) {
-                    const uint64_t da = tc::smem_desc(a0 + 2 * s * LBO_A, LBO_A, ROWB);
-                    const uint64_t db = tc::smem_desc(wa + tap * BTAP + 2 * s * b_lbo, b_lbo, 128);
+                uint64_t da = da0 + (uint64_t)(((tap / 3) * ROWB + (tap % 3) * 16) >> 4);
+                uint64_t db = db0 + (uint64_t)((tap * BTAP) >> 4);
+                for (int s = 0; s < ks; s++) {
                     tc::mma_bf16(acc, da, db, idesc, (tap == 0 && s == 0) ? 0u : 1u);
+                    da += a_step;
+                    db += b_step;
                 }
             }
             tc::mma_commit(&bar[b]);

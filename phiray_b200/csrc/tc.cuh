@@ -124,12 +124,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* out) {
 template <int N>
 __device__ __forceinline__ void mma_chunk(uint32_t tmem_d, const uint8_t* a_tile, const uint8_t* b_tile, bool first) {
     constexpr uint32_t idesc = instr_desc_bf16(BM, N);
-    const uint32_t a0 = smem_addr(a_tile), b0 = smem_addr(b_tile);
     constexpr uint32_t a_lbo = (BM / 8) * 128, b_lbo = (N / 8) * 128;
+    // one descriptor per operand; each K = 16 step adds 2 * LBO / 16 to its
+    // start-address field (shared-memory offsets stay below 2^18 bytes, so the
+    // 14-bit field does not carry)
+    const uint64_t da0 = smem_desc(smem_addr(a_tile), a_lbo, 128);
+    const uint64_t db0 = smem_desc(smem_addr(b_tile), b_lbo, 128);
 #pragma unroll
     for (int s = 0; s < BK / 16; s++) {
-        const uint64_t da = smem_desc(a0 + s * 2 * a_lbo, a_lbo, 128);
-        const uint64_t db = smem_desc(b0 + s * 2 * b_lbo, b_lbo, 128);
+        const uint64_t da = da0 + (uint64_t)((s * 2 * a_lbo) >> 4);
+        const uint64_t db = db0 + (uint64_t)((s * 2 * b_lbo) >> 4);
         mma_bf16(tmem_d, da, db, idesc, (first && s == 0) ? 0u : 1u);
     }
 }

@@ -415,7 +415,7 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
                target: int | None = None) -> Scene:
     """One seeded procedural scene of the learned denoiser's training set:
     random boxes, spheres and noise-displaced spheres (plus a cloud of small
-    triangles; in about a third of the scenes a finely tessellated displaced
+    triangles; in about half of the scenes a finely tessellated displaced
     sphere with per-face albedo and mirror faces fills much of the view) on a
     ground plane, 10k-500k faces in total (log-uniform
     target), per-object or per-face albedo, some mirror objects, 1-4 area
@@ -465,7 +465,7 @@ def procedural(index: int, width: int = 256, height: int = 256, spp: int = 4, bo
         mats.append(lambert(rng.uniform(0.2, 0.8, 3)))
         parts.append((np.asarray(w[0], np.float32), w[1]))
     used = 0
-    hero = rng.random() < 0.35
+    hero = rng.random() < 0.5
     if hero:  # a finely tessellated, noise-displaced sphere filling much of the view
         v, f = _icosphere(6 if rng.random() < 0.6 else 7)
         r = 1.0 + rng.uniform(0.03, 0.1) * value_noise(v, int(rng.integers(1 << 30)))
