@@ -40,7 +40,7 @@ UNIT = "Mrays/s"
 WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 64 spp, 8 bounces, LBVH rebuild + trace + denoise per frame"
 
 
-KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8"]
+KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8", "megakernel/3", "megakernel/2"]
 
 
 def peaks() -> dict:
@@ -644,6 +644,9 @@ def main() -> None:
         tr.set_walk(mode)
         walk_ms[name] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
     inc_ms = min(walk_ms.values())
+    tr.set_walk(px.Tracer.WALK_FETCH if walk_ms["persistent_fetch"] <= walk_ms["thread_per_ray"] else px.Tracer.WALK_THREAD)
+    _, inc_steps, inc_tests = tr.trace_rays_stats(rays, n, hits, False)
+    inc_bytes = inc_steps * 64 + inc_tests * 48
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
     ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
     prim_ms = timed(lambda: tr.primary(cam, W, H, 0, ids, ts), 10)
@@ -703,6 +706,9 @@ def main() -> None:
             "lbvh_refit_gbs": round(172 * nf / (refit_ms * 1e-3) / 1e9, 1),
             "incoherent_grays": round(n / (inc_ms * 1e-3) / 1e9, 3),
             "incoherent_grays_by_walk": {k: round(n / (v * 1e-3) / 1e9, 3) for k, v in walk_ms.items()},
+            "incoherent_walk": {"steps_per_ray": round(inc_steps / n, 2), "tests_per_ray": round(inc_tests / n, 2),
+                                "achieved_gbs": round(inc_bytes / (inc_ms * 1e-3) / 1e9, 1),
+                                "frac_of_hbm": round(inc_bytes / (inc_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)},
             "primary_grays": round(n / (prim_ms * 1e-3) / 1e9, 3),
             "roofline": {"bound": "hbm", "kernel": "k_render (path-trace megakernel)", "achieved": round(achieved, 1),
                          "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),

@@ -382,10 +382,14 @@ int32_t phx_tracer_destroy(phx_tracer tr);
 #define PHX_KERNEL_STATE_MACHINE 1u
 #define PHX_KERNEL_STATE_MACHINE_6 2u
 #define PHX_KERNEL_STATE_MACHINE_8 3u
+/* The megakernel with a register budget for 3 or 2 resident blocks (more
+ * registers a thread, fewer spills, fewer warps). */
+#define PHX_KERNEL_MEGAKERNEL_3 4u
+#define PHX_KERNEL_MEGAKERNEL_2 5u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer
- * and returns its id; ms (4 floats, may be NULL) gets each one's time. The
+ * and returns its id; ms (6 floats, may be NULL) gets each one's time. The
  * image is overwritten (the next sample starts over). Waits. */
 int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
                             uint32_t* chosen, float* ms);

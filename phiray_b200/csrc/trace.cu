@@ -547,9 +547,11 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
     }
 }
 
-template <bool STATS>
-__global__ void __launch_bounds__(128, 4) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
-                                               uint32_t count, unsigned long long* counters) {
+// MINB: resident 128-thread blocks per SM the register budget is set for
+// (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills).
+template <bool STATS, int MINB = 4>
+__global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px,
+                                                  uint32_t first, uint32_t count, unsigned long long* counters) {
     setup(S, F);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt{0, 0, 0};
@@ -1504,7 +1506,7 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
 int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, uint32_t count_px, bool stats) {
     Ctx* c = tr->ctx;
     const Scene S = scene_of(tr);
-    if (tr->kernel != PHX_KERNEL_MEGAKERNEL) {
+    if (tr->kernel >= PHX_KERNEL_STATE_MACHINE && tr->kernel <= PHX_KERNEL_STATE_MACHINE_8) {
         // state machine, at 4, 6 or 8 resident blocks of 128 per SM
         const int minb = tr->kernel == 1u ? 4 : (tr->kernel == 2u ? 6 : 8);
         const void* fn = minb == 4 ? (const void*)k_render_sm<false, 4>
@@ -1528,12 +1530,19 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
         }
         return cuda_check(cudaGetLastError(), "render");
     }
-    if (stats)
-        k_render<true><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
-                                                                      count_px, (unsigned long long*)tr->rays.ptr);
-    else
-        k_render<false><<<(count_px + 127) / 128, 128, 0, c->stream>>>(S, F, sun, (uint32_t*)tr->px.ptr, first_px,
-                                                                       count_px, (unsigned long long*)tr->rays.ptr);
+    const uint32_t blocks = (count_px + 127) / 128;
+    uint32_t* pxp = (uint32_t*)tr->px.ptr;
+    unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
+    if (tr->kernel == PHX_KERNEL_MEGAKERNEL_3) {
+        if (stats) k_render<true, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2) {
+        if (stats) k_render<true, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else {
+        if (stats) k_render<true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    }
     return cuda_check(cudaGetLastError(), "render");
 }
 
@@ -1649,7 +1658,7 @@ int32_t phx_tracer_destroy(phx_tracer tr) {
 
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (kernel > PHX_KERNEL_STATE_MACHINE_8) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
+    if (kernel > PHX_KERNEL_MEGAKERNEL_2) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
     tr->kernel = kernel;
     return PHX_OK;
 }
@@ -1664,7 +1673,7 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
     float best = 0.0f;
     uint32_t pick = PHX_KERNEL_STATE_MACHINE;
     const uint32_t keep = tr->kernel;
-    for (uint32_t k = 0; k <= PHX_KERNEL_STATE_MACHINE_8; k++) {
+    for (uint32_t k = 0; k <= PHX_KERNEL_MEGAKERNEL_2; k++) {
         tr->kernel = k;
         PHX_TRY(launch_render(tr, cam, w, h, 0, spp ? spp : 1, 0, w * h));  // warm-up
         PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));
