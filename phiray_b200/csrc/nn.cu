@@ -987,7 +987,9 @@ int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void
     return cuda_check(cudaGetLastError(), "conv fwd");
 }
 
-constexpr size_t WS_MAX_SMEM = 200 * 1024;
+// The weight-stationary form only where two blocks fit an SM: with one,
+// nothing covers its per-tile synchronisation and the chunked form is faster.
+constexpr size_t WS_MAX_SMEM = 110 * 1024;
 
 template <int N, bool RELU, bool F32>
 int32_t conv_ws_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
