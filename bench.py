@@ -640,11 +640,13 @@ def main() -> None:
     hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
     tr.secondary_rays(cam, W, H, 0, rays)
     walk_ms = {}
-    for name, mode in (("thread_per_ray", px.Tracer.WALK_THREAD), ("persistent_fetch", px.Tracer.WALK_FETCH)):
+    walks = {"thread_per_ray": px.Tracer.WALK_THREAD, "persistent_fetch": px.Tracer.WALK_FETCH,
+             "sorted_fetch": px.Tracer.WALK_SORTED}
+    for name, mode in walks.items():
         tr.set_walk(mode)
-        walk_ms[name] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
+        walk_ms[name] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)  # the sort is inside the timing
     inc_ms = min(walk_ms.values())
-    tr.set_walk(px.Tracer.WALK_FETCH if walk_ms["persistent_fetch"] <= walk_ms["thread_per_ray"] else px.Tracer.WALK_THREAD)
+    tr.set_walk(walks[min(walk_ms, key=walk_ms.get)])
     _, inc_steps, inc_tests = tr.trace_rays_stats(rays, n, hits, False)
     inc_bytes = inc_steps * 64 + inc_tests * 48
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")

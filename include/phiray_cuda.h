@@ -405,6 +405,10 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
  * ray is walked in the same order either way: the same hits. */
 #define PHX_WALK_THREAD 0u
 #define PHX_WALK_FETCH 1u
+/* PHX_WALK_SORTED: PHX_WALK_FETCH over the rays in the order of a stable
+ * radix sort by (direction octant, Morton code of the origin), each hit
+ * still written at its ray's index. */
+#define PHX_WALK_SORTED 2u
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
 /* Tracer::set_samples: the sample target `sample` stops at. */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);

@@ -1230,7 +1230,7 @@ constexpr int RAY_STEPS = 16;
 template <bool ANY, bool STATS>
 __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __restrict__ rays, uint32_t n,
                                                     float4* __restrict__ hits, unsigned long long* counters,
-                                                    uint32_t* next) {
+                                                    uint32_t* next, const uint32_t* __restrict__ order) {
     load_info(S);
     const Tree T = tree_of(S);
     const int lane = threadIdx.x & 31;
@@ -1255,6 +1255,7 @@ __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __res
             if (!active) {
                 idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
                 if (idx < n) {
+                    if (order) idx = __ldg(order + idx);  // walk in the sorted order, answer in place
                     const float4 a = __ldg(rays + 2 * (size_t)idx), b = __ldg(rays + 2 * (size_t)idx + 1);
                     o = mk(a.x, a.y, a.z);
                     const f3 d = mk(b.x, b.y, b.z);
@@ -1352,15 +1353,43 @@ __global__ void __launch_bounds__(128) k_rays_fetch(Scene S, const float4* __res
     }
 }
 
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 9 bits -> every third of 27
+    uint32_t x = v & 0x1FFu;
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+// A ray's sort key: its direction's octant above the 27-bit Morton code of
+// its origin in the scene box, so that sorted rays leave nearby points in
+// similar directions and walk similar parts of the tree.
+__global__ void k_ray_keys(Scene S, const float4* __restrict__ rays, uint32_t n, uint32_t* __restrict__ keys) {
+    load_info(S);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+    const f3 ext = S.root_hi - S.root_lo;
+    const float ux = ext.x > 0.0f ? (a.x - S.root_lo.x) / ext.x : 0.0f;
+    const float uy = ext.y > 0.0f ? (a.y - S.root_lo.y) / ext.y : 0.0f;
+    const float uz = ext.z > 0.0f ? (a.z - S.root_lo.z) / ext.z : 0.0f;
+    const uint32_t qx = (uint32_t)(fminf(fmaxf(ux, 0.0f), 1.0f) * 511.0f);
+    const uint32_t qy = (uint32_t)(fminf(fmaxf(uy, 0.0f), 1.0f) * 511.0f);
+    const uint32_t qz = (uint32_t)(fminf(fmaxf(uz, 0.0f), 1.0f) * 511.0f);
+    const uint32_t oct = (b.x < 0.0f ? 1u : 0u) | (b.y < 0.0f ? 2u : 0u) | (b.z < 0.0f ? 4u : 0u);
+    keys[i] = (oct << 27) | (spread3(qx) << 2) | (spread3(qy) << 1) | spread3(qz);
+}
+
 template <bool ANY, bool STATS>
 void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters, bool smem,
-                 cudaStream_t s, uint32_t* next = nullptr, int sms = 0) {
+                 cudaStream_t s, uint32_t* next = nullptr, int sms = 0, const uint32_t* order = nullptr) {
     if (next) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rays_fetch<ANY, STATS>, 128, 0);
         const uint32_t grid = std::min<uint32_t>((uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms, (n + 127) / 128);
         cudaMemsetAsync(next, 0, 4, s);
-        k_rays_fetch<ANY, STATS><<<grid, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters, next);
+        k_rays_fetch<ANY, STATS><<<grid, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters, next, order);
         return;
     }
     if (smem)
@@ -1386,7 +1415,8 @@ struct phx_tracer_s {
     uint32_t kernel = PHX_KERNEL_MEGAKERNEL;  // which render kernel traces a frame (the fastest measured)
     DevMem next;                                 // the state-machine kernel's pixel counter
     bool smem_stack = false;                     // ray walks keep their stack in shared memory
-    uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, or persistent warps
+    uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, persistent warps, sorted first
+    DevMem rkeys, rsorted, rorder, ralt_k, ralt_v, rzero;  // the sorted walk's keys and radix-sort scratch
     bool have_last = false;
     phx_camera last;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -1704,7 +1734,7 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
 
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (mode > PHX_WALK_FETCH) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
+    if (mode > PHX_WALK_SORTED) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
     tr->walk = mode;
     return PHX_OK;
 }
@@ -1872,14 +1902,45 @@ int32_t phx_tracer_secondary_rays(phx_tracer tr, const phx_camera* cam, uint32_t
     return cuda_check(cudaGetLastError(), "secondary rays");
 }
 
+namespace phx {
+namespace {
+// Sorts the rays' keys (k_ray_keys) with the stable radix sort: the order
+// the sorted walk takes them in. Stream-ordered.
+int32_t sort_rays(phx_tracer tr, const Scene& S, const float* rays, uint32_t n, const uint32_t** order) {
+    Ctx* c = tr->ctx;
+    const uint32_t stride = (n + 4095) / 4096;
+    const size_t zero_words = 4 * 256 + 16 + (size_t)4 * stride * 256;
+    PHX_TRY(tr->rkeys.reserve((size_t)n * 4));
+    PHX_TRY(tr->rsorted.reserve((size_t)n * 4));
+    PHX_TRY(tr->rorder.reserve((size_t)n * 4));
+    PHX_TRY(tr->ralt_k.reserve((size_t)n * 4));
+    PHX_TRY(tr->ralt_v.reserve((size_t)n * 4));
+    PHX_TRY(tr->rzero.reserve(zero_words * 4));
+    PHX_CUDA(cudaMemsetAsync(tr->rzero.ptr, 0, zero_words * 4, c->stream));
+    k_ray_keys<<<(n + 255) / 256, 256, 0, c->stream>>>(S, (const float4*)rays, n, (uint32_t*)tr->rkeys.ptr);
+    PHX_CUDA(cudaGetLastError());
+    uint32_t* z = (uint32_t*)tr->rzero.ptr;
+    PHX_TRY(enqueue_sort_raw(c, (const uint32_t*)tr->rkeys.ptr, n, (uint32_t*)tr->rorder.ptr,
+                             (uint32_t*)tr->rsorted.ptr, (uint32_t*)tr->ralt_k.ptr, (uint32_t*)tr->ralt_v.ptr, z,
+                             z + 4 * 256, z + 4 * 256 + 16, stride));
+    *order = (const uint32_t*)tr->rorder.ptr;
+    return PHX_OK;
+}
+}  // namespace
+}  // namespace phx
+
 int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit) {
     if (!tr || (n && (!rays || !hits))) return fail(PHX_ERR_INVALID, "null argument");
     if (n == 0) return PHX_OK;
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
-    uint32_t* nx = tr->walk == PHX_WALK_FETCH ? (uint32_t*)tr->next.ptr : nullptr;
-    if (any_hit) launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms);
-    else launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms);
+    uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
+    const uint32_t* order = nullptr;
+    if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));
+    if (any_hit)
+        launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms, order);
+    else
+        launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms, order);
     return cuda_check(cudaGetLastError(), "trace rays");
 }
 
@@ -1891,11 +1952,12 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
     PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
     const Scene S = scene_of(tr);
     if (n) {
-        uint32_t* nx = tr->walk == PHX_WALK_FETCH ? (uint32_t*)tr->next.ptr : nullptr;
-        if (any_hit)
-            launch_rays<true, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s, nx, tr->ctx->sms);
-        else
-            launch_rays<false, true>(S, rays, n, hits, (unsigned long long*)tr->rays.ptr, tr->smem_stack, s, nx, tr->ctx->sms);
+        uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
+        const uint32_t* order = nullptr;
+        if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));
+        unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
+        if (any_hit) launch_rays<true, true>(S, rays, n, hits, ct, tr->smem_stack, s, nx, tr->ctx->sms, order);
+        else launch_rays<false, true>(S, rays, n, hits, ct, tr->smem_stack, s, nx, tr->ctx->sms, order);
         PHX_CUDA(cudaGetLastError());
     }
     PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));

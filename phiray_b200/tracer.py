@@ -146,10 +146,13 @@ class Tracer:
 
     WALK_THREAD = 0
     WALK_FETCH = 1
+    WALK_SORTED = 2
 
     def set_walk(self, mode: int) -> None:
-        """Ray-buffer walks: Tracer.WALK_THREAD (a thread per ray) or
-        Tracer.WALK_FETCH (persistent warps refilling idle lanes); same hits."""
+        """Ray-buffer walks: Tracer.WALK_THREAD (a thread per ray),
+        Tracer.WALK_FETCH (persistent warps refilling idle lanes) or
+        Tracer.WALK_SORTED (the same over rays sorted by direction octant and
+        origin); same hits."""
         N.check(N.lib().phx_tracer_set_walk(self.handle, mode))
 
     def set_samples(self, n: int) -> None:

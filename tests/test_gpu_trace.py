@@ -127,7 +127,7 @@ def test_primary_hit_ids(gpu, orc, name):
     assert np.array_equal(ts.cpu().numpy(), want_t)
 
 
-@pytest.mark.parametrize("walk", [0, 1], ids=["thread_per_ray", "persistent_fetch"])
+@pytest.mark.parametrize("walk", [0, 1, 2], ids=["thread_per_ray", "persistent_fetch", "sorted"])
 def test_ray_buffer_walks(gpu, orc, walk):
     import torch
 
