@@ -386,10 +386,14 @@ int32_t phx_tracer_destroy(phx_tracer tr);
  * registers a thread, fewer spills, fewer warps). */
 #define PHX_KERNEL_MEGAKERNEL_3 4u
 #define PHX_KERNEL_MEGAKERNEL_2 5u
+/* The megakernel (4 or 2 resident blocks) with each warp's lanes waiting for
+ * each other after every sample, so samples start together. */
+#define PHX_KERNEL_MEGAKERNEL_SYNC 6u
+#define PHX_KERNEL_MEGAKERNEL_2_SYNC 7u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer
- * and returns its id; ms (6 floats, may be NULL) gets each one's time. The
+ * and returns its id; ms (8 floats, may be NULL) gets each one's time. The
  * image is overwritten (the next sample starts over). Waits. */
 int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
                             uint32_t* chosen, float* ms);

@@ -490,9 +490,13 @@ __device__ __forceinline__ void setup(Scene& S, Frame& F) {
 // One pixel's samples [F.frame0, F.frame0 + F.spp): its sums read back (or
 // started over on frame 0), shade.wgsl's main once per sample, the planes
 // written once (util.wgsl's guide/emit over the whole run of samples).
-template <bool STATS>
+// SYNC: the lanes that entered wait for each other after every sample, so
+// each sample's camera ray and first bounces start together (the same sums
+// either way: a lane's own samples keep their order).
+template <bool STATS, bool SYNC = false>
 __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun, uint32_t* __restrict__ px,
                                           uint32_t i, Count& cnt) {
+    const unsigned lanes = __activemask();
     const uint32_t n = F.n;
     Sums acc;
     if (F.frame0 > 0u) {
@@ -513,7 +517,10 @@ __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun
         px[30 * n + i] = 0u;
     }
     acc.outline = 0;
-    for (uint32_t s = 0; s < F.spp; s++) sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
+    for (uint32_t s = 0; s < F.spp; s++) {
+        sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
+        if (SYNC) __syncwarp(lanes);
+    }
     st3(px, 1 * n, i, acc.lin);
     st3(px, 20 * n, i, acc.grid);
     st3(px, 7 * n, i, acc.alb);
@@ -549,13 +556,13 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
 
 // MINB: resident 128-thread blocks per SM the register budget is set for
 // (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills).
-template <bool STATS, int MINB = 4>
+template <bool STATS, int MINB = 4, bool SYNC = false>
 __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px,
                                                   uint32_t first, uint32_t count, unsigned long long* counters) {
     setup(S, F);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt{0, 0, 0};
-    if (k < count) render_px<STATS>(S, F, sun, px, first + k, cnt);
+    if (k < count) render_px<STATS, SYNC>(S, F, sun, px, first + k, cnt);
     flush_counts<STATS>(cnt, counters);
 }
 
@@ -1563,7 +1570,13 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
     const uint32_t blocks = (count_px + 127) / 128;
     uint32_t* pxp = (uint32_t*)tr->px.ptr;
     unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
-    if (tr->kernel == PHX_KERNEL_MEGAKERNEL_3) {
+    if (tr->kernel == PHX_KERNEL_MEGAKERNEL_SYNC) {
+        if (stats) k_render<true, 4, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 4, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2_SYNC) {
+        if (stats) k_render<true, 2, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 2, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_3) {
         if (stats) k_render<true, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
     } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2) {
@@ -1688,7 +1701,7 @@ int32_t phx_tracer_destroy(phx_tracer tr) {
 
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (kernel > PHX_KERNEL_MEGAKERNEL_2) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
+    if (kernel > PHX_KERNEL_MEGAKERNEL_2_SYNC) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
     tr->kernel = kernel;
     return PHX_OK;
 }
@@ -1703,7 +1716,7 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
     float best = 0.0f;
     uint32_t pick = PHX_KERNEL_STATE_MACHINE;
     const uint32_t keep = tr->kernel;
-    for (uint32_t k = 0; k <= PHX_KERNEL_MEGAKERNEL_2; k++) {
+    for (uint32_t k = 0; k <= PHX_KERNEL_MEGAKERNEL_2_SYNC; k++) {
         tr->kernel = k;
         PHX_TRY(launch_render(tr, cam, w, h, 0, spp ? spp : 1, 0, w * h));  // warm-up
         PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));

@@ -127,11 +127,13 @@ class Tracer:
     STATE_MACHINE_8 = 3
     MEGAKERNEL_3 = 4
     MEGAKERNEL_2 = 5
+    MEGAKERNEL_SYNC = 6
+    MEGAKERNEL_2_SYNC = 7
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
         chosen = C.c_uint32()
-        ms = (C.c_float * 6)()
+        ms = (C.c_float * 8)()
         N.check(N.lib().phx_tracer_autotune(self.handle, cam.ctypes.data, w, h, spp, C.byref(chosen), ms))
         self.w, self.h = w, h
         return chosen.value, list(ms)

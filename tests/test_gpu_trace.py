@@ -50,7 +50,8 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5], ids=["megakernel", "state_machine", "sm6", "sm8", "mk3", "mk2"])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7],
+                         ids=["megakernel", "state_machine", "sm6", "sm8", "mk3", "mk2", "mk_sync", "mk2_sync"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_image_matches_oracle(gpu, orc, name, kernel):
     s = SCENES[name]()
@@ -161,7 +162,7 @@ def test_autotune_keeps_the_image(gpu, orc):
     cam = cam_of(s, s.width, s.height)
     tr = px.Tracer.of(gpu, s)
     chosen, ms = tr.autotune(cam, s.width, s.height, 2)
-    assert chosen in range(6) and all(t > 0 for t in ms)
+    assert chosen in range(8) and all(t > 0 for t in ms)
     tr.trace(cam, s.width, s.height, 0, s.spp)
     want, _ = oracle_lib.TraceOracle(orc, s).trace(cam, 0, s.spp)
     check_image(tr.image(), want, s.width * s.height)
