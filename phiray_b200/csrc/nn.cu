@@ -199,31 +199,39 @@ __device__ __forceinline__ void cp_async_wait() {
 // that last read it.
 constexpr int TY = 16, TX = 8;
 constexpr int PY = TY + 2, PX = TX + 2;
-constexpr int ROWB = PX * 16;  // bytes of one patch row of one 8-channel group
+constexpr int ROWB = PX * 16;  // bytes of one patch row of one 8-channel group (one 16 x 8 tile)
 
-template <int N, int CC>
+// T tiles side by side: the block covers 16 x 8T pixels, stages one
+// (16 + 2) x (8T + 2) patch a chunk, and keeps T accumulators of N columns;
+// tile t's A operand of tap (dy, dx) starts dy * ROWT + (8 t + dx) * 16 bytes
+// into the patch. The weight chunk is read once for the T tiles.
+template <int N, int CC, int T>
 struct Conv {
     static constexpr int KG = CC / 8;                 // 8-channel groups a chunk
-    static constexpr int LBO_A = PY * ROWB;           // between channel groups of the patch
+    static constexpr int PXT = TX * T + 2;            // patch width
+    static constexpr int ROWT = PXT * 16;             // bytes of a patch row of one channel group
+    static constexpr int LBO_A = PY * ROWT;           // between channel groups of the patch
     static constexpr int PATCH = KG * LBO_A;          // patch bytes
     static constexpr int BTAP = N * CC * 2;           // one tap's weight tile
     static constexpr int STAGE = (PATCH + 9 * BTAP + 127) / 128 * 128;
-    static constexpr int STAGES = N <= 32 ? 3 : 2;
+    static constexpr int STAGES = STAGE <= 40 * 1024 ? 3 : 2;
     static constexpr int TOTAL = STAGES * STAGE;
+    static constexpr uint32_t ACC = tc::tmem_cols(N);  // accumulator stride in TMEM columns
+    static constexpr uint32_t COLS = tc::tmem_cols(T * ACC);
 };
 
 // Y = act(conv3x3(X, W) + bias). OUT_F32: fp32 output (the network's head).
-template <int N, int CC, bool RELU, bool OUT_F32>
+template <int N, int CC, int T, bool RELU, bool OUT_F32>
 __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
                                                   const float* __restrict__ bias, void* __restrict__ Y, Geo g,
                                                   uint32_t* status) {
-    using C = Conv<N, CC>;
+    using C = Conv<N, CC, T>;
     constexpr int STAGES = C::STAGES;
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar[STAGES];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (warp == 0) tc::tmem_alloc(&tmem_base, tc::tmem_cols(N));
+    if (warp == 0) tc::tmem_alloc(&tmem_base, C::COLS);
     if (tid == 0) {
         for (int i = 0; i < STAGES; i++) tc::mbar_init(&bar[i], 1);
         fence_barrier_init();
@@ -232,22 +240,22 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tm = tmem_base;
-    const int tiles_x = (g.W + TX - 1) / TX, tiles_y = (g.H + TY - 1) / TY;
+    const int tiles_x = (g.W + TX * T - 1) / (TX * T), tiles_y = (g.H + TY - 1) / TY;
     const int bx = blockIdx.x % tiles_x, by = (blockIdx.x / tiles_x) % tiles_y, img = blockIdx.x / (tiles_x * tiles_y);
-    const int y0 = by * TY, x0 = bx * TX;
+    const int y0 = by * TY, x0 = bx * TX * T;
     const int nk = g.cin / CC;
 
     auto issue = [&](int chunk) {
         uint8_t* patch = smem + (chunk % STAGES) * C::STAGE;
         uint8_t* wb = patch + C::PATCH;
         const int c0 = chunk * CC;
-        for (int v = tid; v < PY * PX * C::KG; v += 128) {
+        for (int v = tid; v < PY * C::PXT * C::KG; v += 128) {
             const int kg = v % C::KG, q = v / C::KG;
-            const int py = q / PX, px = q - py * PX;
+            const int py = q / C::PXT, px = q - py * C::PXT;
             const int y = y0 + py - 1, x = x0 + px - 1;
             const bool ok = y >= 0 && y < g.H && x >= 0 && x < g.W;
             const bf16* src = ok ? X + ((size_t)(img * g.H + y) * g.W + x) * g.xs + g.xo + c0 + kg * 8 : X;
-            cp_async_ca16(patch + kg * C::LBO_A + py * ROWB + px * 16, src, ok ? 16u : 0u);
+            cp_async_ca16(patch + kg * C::LBO_A + py * C::ROWT + px * 16, src, ok ? 16u : 0u);
         }
         for (int v = tid; v < 9 * N * C::KG; v += 128) {
             const int kg = v % C::KG, q = v / C::KG;
@@ -272,15 +280,20 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
         if (tid == 0) {
             const uint32_t patch = tc::smem_addr(smem + (chunk % STAGES) * C::STAGE);
             tc::fence_after_sync();
-            const uint64_t da0 = tc::smem_desc(patch, C::LBO_A, ROWB);
+            const uint64_t da0 = tc::smem_desc(patch, C::LBO_A, C::ROWT);
             const uint64_t db0 = tc::smem_desc(patch + C::PATCH, b_lbo, 128);
 #pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
+            for (int t = 0; t < T; t++) {
 #pragma unroll
-                for (int s = 0; s < CC / 16; s++) {
-                    const uint64_t da = da0 + (uint64_t)(((tap / 3) * ROWB + (tap % 3) * 16 + 2 * s * C::LBO_A) >> 4);
-                    const uint64_t db = db0 + (uint64_t)((tap * C::BTAP + 2 * s * b_lbo) >> 4);
-                    tc::mma_bf16(tm, da, db, idesc, (chunk == 0 && tap == 0 && s == 0) ? 0u : 1u);
+                for (int tap = 0; tap < 9; tap++) {
+#pragma unroll
+                    for (int s = 0; s < CC / 16; s++) {
+                        const uint64_t da =
+                            da0 + (uint64_t)(((tap / 3) * C::ROWT + (TX * t + tap % 3) * 16 + 2 * s * C::LBO_A) >> 4);
+                        const uint64_t db = db0 + (uint64_t)((tap * C::BTAP + 2 * s * b_lbo) >> 4);
+                        tc::mma_bf16(tm + (uint32_t)t * C::ACC, da, db, idesc,
+                                     (chunk == 0 && tap == 0 && s == 0) ? 0u : 1u);
+                    }
                 }
             }
             tc::mma_commit(&bar[chunk % STAGES]);
@@ -297,29 +310,32 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     tc::fence_after_sync();
     if (ok) {
         const int m = warp * 32 + lane;
-        const int y = y0 + m / TX, x = x0 + m % TX;
-        const bool live = y < g.H && x < g.W;
-        const size_t p = ((size_t)img * g.H + y) * g.W + x;
 #pragma unroll 1
-        for (int c0 = 0; c0 < N; c0 += 16) {
-            float v[16];
-            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (!live) continue;
+        for (int t = 0; t < T; t++) {
+            const int y = y0 + m / TX, x = x0 + TX * t + m % TX;
+            const bool live = y < g.H && x < g.W;
+            const size_t p = ((size_t)img * g.H + y) * g.W + x;
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)t * C::ACC + (uint32_t)c0, v);
+                if (!live) continue;
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                v[j] += __ldg(bias + c0 + j);
-                if (RELU) v[j] = fmaxf(v[j], 0.0f);
-            }
-            if (OUT_F32) {
-                float4* o = (float4*)((float*)Y + p * g.ys + g.yo + c0);
+                for (int j = 0; j < 16; j++) {
+                    v[j] += __ldg(bias + c0 + j);
+                    if (RELU) v[j] = fmaxf(v[j], 0.0f);
+                }
+                if (OUT_F32) {
+                    float4* o = (float4*)((float*)Y + p * g.ys + g.yo + c0);
 #pragma unroll
-                for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            } else {
-                uint4* o = (uint4*)((bf16*)Y + p * g.ys + g.yo + c0);
-                o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                                  pack_bf16x2(v[6], v[7]));
-                o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
-                                  pack_bf16x2(v[14], v[15]));
+                    for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                } else {
+                    uint4* o = (uint4*)((bf16*)Y + p * g.ys + g.yo + c0);
+                    o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                      pack_bf16x2(v[6], v[7]));
+                    o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                      pack_bf16x2(v[14], v[15]));
+                }
             }
         }
     } else if (tid == 0) {
@@ -327,7 +343,7 @@ __global__ void __launch_bounds__(128) k_conv_fwd(const bf16* __restrict__ X, co
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_free(tm, tc::tmem_cols(N));
+    if (warp == 0) tc::tmem_free(tm, C::COLS);
 }
 
 // ---- the same convolution, persistent and weight-stationary ----
@@ -977,18 +993,16 @@ __global__ void k_compose(const float* __restrict__ out, const float* __restrict
     px[i] = pack_rgba(shown, __uint_as_float(px[24 * n + i]) * k);
 }
 
-template <int N, int CC, bool RELU, bool F32>
+template <int N, int CC, int T, bool RELU, bool F32>
 int32_t conv_fwd_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
-    const int smem = Conv<N, CC>::TOTAL;
+    const int smem = Conv<N, CC, T>::TOTAL;
     static std::atomic<uint64_t> done{0};
-    PHX_TRY(smem_limit(k_conv_fwd<N, CC, RELU, F32>, smem, c->device, done));
-    const uint32_t blocks = (uint32_t)g.B * ((g.H + TY - 1) / TY) * ((g.W + TX - 1) / TX);
-    k_conv_fwd<N, CC, RELU, F32><<<blocks, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
+    PHX_TRY(smem_limit(k_conv_fwd<N, CC, T, RELU, F32>, smem, c->device, done));
+    const uint32_t blocks = (uint32_t)g.B * ((g.H + TY - 1) / TY) * ((g.W + TX * T - 1) / (TX * T));
+    k_conv_fwd<N, CC, T, RELU, F32><<<blocks, 128, smem, c->stream>>>(X, W, bias, Y, g, c->status);
     return cuda_check(cudaGetLastError(), "conv fwd");
 }
 
-// The weight-stationary form only where two blocks fit an SM: with one,
-// nothing covers its per-tile synchronisation and the chunked form is faster.
 constexpr size_t WS_MAX_SMEM = 110 * 1024;
 
 template <int N, bool RELU, bool F32>
@@ -1008,13 +1022,14 @@ int32_t conv_ws_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void*
     return cuda_check(cudaGetLastError(), "conv fwd (weight-stationary)");
 }
 
-// The weight-stationary form where its smem fits (N <= 128), else chunks of
-// 32 channels where they divide cin and the stage stays small, else 16.
+// The weight-stationary form where two of its blocks fit an SM, else the
+// chunked form over 16 channels a chunk.
 template <int N, bool RELU, bool F32>
 int32_t conv_fwd_cc(Ctx* c, const bf16* X, const bf16* W, const float* bias, void* Y, const Geo& g) {
     if (N <= 128 && ConvWS<N>::bytes(g.cin) <= WS_MAX_SMEM) return conv_ws_n<N, RELU, F32>(c, X, W, bias, Y, g);
-    if (N <= 64 && g.cin % 32 == 0) return conv_fwd_n<N, 32, RELU, F32>(c, X, W, bias, Y, g);
-    return conv_fwd_n<N, 16, RELU, F32>(c, X, W, bias, Y, g);
+    // chunked: several tiles a block where N is small (their weights read once)
+    constexpr int T = N <= 32 ? 4 : (N <= 64 ? 2 : 1);
+    return conv_fwd_n<N, 16, T, RELU, F32>(c, X, W, bias, Y, g);
 }
 
 template <bool RELU, bool F32>

@@ -84,6 +84,8 @@ CONV_CASES = [
     (288, 128, True, False),
     (224, 96, True, False),
     (32, 32, False, True),
+    (96, 32, True, False),
+    (160, 64, True, False),
 ]
 
 
