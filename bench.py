@@ -661,16 +661,29 @@ def main() -> None:
     h2d = hv.nbytes + hf.nbytes + hm.nbytes + cam.nbytes
     d2h = n * 4
 
+    e2e_parts = {"create_ms": 0.0, "trace_denoise_ms": 0.0, "read_ms": 0.0, "close_ms": 0.0}
+
     def e2e_step():
+        t0 = time.perf_counter()
         t = px.Tracer(gpu, hv, hf, hm)
+        gpu.wait(60000)
+        t1 = time.perf_counter()
         t.trace(cam, W, H, 0, args.spp)
         t.denoise()
+        gpu.wait(60000)
+        t2 = time.perf_counter()
         img = t.pixels()
+        t3 = time.perf_counter()
         t.close()
+        t4 = time.perf_counter()
+        for k, a, b in (("create_ms", t0, t1), ("trace_denoise_ms", t1, t2), ("read_ms", t2, t3), ("close_ms", t3, t4)):
+            e2e_parts[k] += (b - a) * 1e3
         return img
 
     e2e_step()
     barrier()
+    for k in e2e_parts:
+        e2e_parts[k] = 0.0
     t0 = time.perf_counter()
     for _ in range(max(2, args.steps // 2)):
         e2e_step()
@@ -718,7 +731,8 @@ def main() -> None:
                          "traffic": traffic, "peak_source": pk["source"],
                          "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "phases_ms": {k: round(v / max(2, args.steps // 2), 1) for k, v in e2e_parts.items()}},
             "denoised": denoised,
             "gpu_launches": 21 * args.steps,
             "clocks": clk.summary(),
