@@ -492,6 +492,12 @@ int32_t phx_gemm_bf16(phx_ctx ctx, const void* A, const void* B, float* D, uint3
 int32_t phx_nn_conv_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* W, int32_t Kp,
                         const float* bias, void* Y, int32_t ys, int32_t yo, int32_t cout, int32_t B, int32_t H,
                         int32_t Wd, int32_t relu, int32_t out_f32);
+/* The network's head (32 outputs, no ReLU) fused with phx_nn_kpn's forward:
+ * out and err exactly as phx_nn_conv_fwd (out_f32) followed by phx_nn_kpn,
+ * without writing the logits. */
+int32_t phx_nn_conv_kpn(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* W, int32_t Kp,
+                        const float* bias, const float* irr, const float* alb, int32_t B, int32_t Hp, int32_t Wp,
+                        int32_t h, int32_t w, float* out, float* err);
 /* dWt[k][co] += sum over pixels of im2col(X)[p][k] dY[p][dyo + co]; dWt is
  * [Kp][cout] fp32 and must be zeroed by the caller. */
 int32_t phx_nn_conv_wgrad(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* dY,

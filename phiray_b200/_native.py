@@ -96,6 +96,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_karras": (i32, [vp, vp, u32, vp]),
     "phx_gemm_bf16": (i32, [vp, vp, vp, vp, u32, u32, u32]),
     "phx_nn_conv_fwd": (i32, [vp, vp, i32, i32, i32, vp, i32, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32]),
+    "phx_nn_conv_kpn": (i32, [vp, vp, i32, i32, i32, vp, i32, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp]),
     "phx_nn_conv_wgrad": (i32, [vp, vp, i32, i32, i32, vp, i32, i32, i32, vp, i32, i32, i32, i32]),
     "phx_nn_bias_grad": (i32, [vp, vp, i32, i32, i32, i32, vp]),
     "phx_nn_relu_bwd": (i32, [vp, vp, i32, i32, vp, i32, i32, i32, i32]),

@@ -366,10 +366,55 @@ struct ConvWS {
     static size_t bytes(int cin) { return (size_t)cin * (W_BYTES_PER_CIN + PATCHES * PATCH_PER_CIN); }
 };
 
-template <int N, bool RELU, bool OUT_F32>
+// The kernel-prediction step as a head convolution's epilogue (inference):
+// the 32 head outputs of a pixel go from TMEM through the softmax and the
+// 5 x 5 filter straight to out / err, and no logits are written.
+struct KpnOut {
+    const float* irr;
+    const float* alb;
+    float* out;
+    float* err;
+    int h, w;  // the valid corner of the padded H x W images
+};
+
+__device__ __forceinline__ void kpn_pixel(const float* lg, const KpnOut& k, int img, int y, int x, int Hp, int Wp,
+                                          size_t p) {
+    if (!(y < k.h && x < k.w)) {
+        for (int c = 0; c < 3; c++) k.out[p * 3 + c] = 0.0f;
+        k.err[p] = 0.0f;
+        return;
+    }
+    float wt[25], mx = -3.0e38f;
+#pragma unroll
+    for (int t = 0; t < 25; t++) {
+        wt[t] = lg[t];
+        mx = fmaxf(mx, wt[t]);
+    }
+    float z = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 25; t++) {
+        wt[t] = pm_exp(wt[t] - mx);
+        z += wt[t];
+    }
+    const float iz = 1.0f / z;
+    float sm[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int t = 0; t < 25; t++) {
+        const int yy = min(max(y + t / 5 - 2, 0), k.h - 1), xx = min(max(x + t % 5 - 2, 0), k.w - 1);
+        const float* q = k.irr + ((size_t)(img * Hp + yy) * Wp + xx) * 3;
+        const float wv = wt[t] * iz;
+#pragma unroll
+        for (int c = 0; c < 3; c++) sm[c] += wv * __ldg(q + c);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) k.out[p * 3 + c] = __ldg(k.alb + p * 3 + c) * sm[c];
+    k.err[p] = fmaxf(pm_exp(lg[25]) - 1.0e-3f, 0.0f);
+}
+
+template <int N, bool RELU, bool OUT_F32, bool KPN = false>
 __global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, const bf16* __restrict__ Wt,
                                                  const float* __restrict__ bias, void* __restrict__ Y, Geo g,
-                                                 uint32_t* status) {
+                                                 uint32_t* status, KpnOut kp = KpnOut{}) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar[2];
     __shared__ uint32_t tmem_base;
@@ -423,6 +468,18 @@ __global__ void __launch_bounds__(128) k_conv_ws(const bf16* __restrict__ X, con
         const int y = by * TY + m / TX, x = bx * TX + m % TX;
         const bool live = y < g.H && x < g.W;
         const size_t p = ((size_t)img * g.H + y) * g.W + x;
+        if (KPN) {
+            float lg[32];
+            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)buf * ACC, lg);
+            tc::tmem_ld16(tm + ((uint32_t)(warp * 32) << 16) + (uint32_t)buf * ACC + 16u, lg + 16);
+            if (live) {
+#pragma unroll
+                for (int j = 0; j < 26; j++) lg[j] += __ldg(bias + j);
+                kpn_pixel(lg, kp, img, y, x, g.H, g.W, p);
+            }
+            tc::fence_before_sync();
+            return;
+        }
 #pragma unroll 1
         for (int c0 = 0; c0 < N; c0 += 16) {
             float v[16];
@@ -1022,6 +1079,20 @@ int32_t conv_ws_n(Ctx* c, const bf16* X, const bf16* W, const float* bias, void*
     return cuda_check(cudaGetLastError(), "conv fwd (weight-stationary)");
 }
 
+// The head (32 outputs, no ReLU) with the kernel-prediction epilogue.
+int32_t conv_kpn(Ctx* c, const bf16* X, const bf16* W, const float* bias, const Geo& g, const KpnOut& kp) {
+    const int smem = (int)ConvWS<32>::bytes(g.cin);
+    if ((size_t)smem > WS_MAX_SMEM) return fail(PHX_ERR_INVALID, "conv+kpn: %d input channels do not fit", g.cin);
+    static std::atomic<uint64_t> done{0};
+    PHX_TRY(smem_limit(k_conv_ws<32, false, true, true>, (int)WS_MAX_SMEM, c->device, done));
+    const int by_smem = (228 * 1024) / (smem + 2 * 1024);
+    const int per_sm = std::max(1, std::min(std::min(by_smem, (int)(512 / (2 * tc::tmem_cols(32)))), 16));
+    const int ntiles = g.B * ((g.H + TY - 1) / TY) * ((g.W + TX - 1) / TX);
+    const int grid = std::min(ntiles, per_sm * c->sms);
+    k_conv_ws<32, false, true, true><<<grid, 128, smem, c->stream>>>(X, W, bias, nullptr, g, c->status, kp);
+    return cuda_check(cudaGetLastError(), "conv + kpn");
+}
+
 // The weight-stationary form where two of its blocks fit an SM, else the
 // chunked form over 16 channels a chunk.
 template <int N, bool RELU, bool F32>
@@ -1091,6 +1162,17 @@ int32_t phx_nn_conv_fwd(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int3
     if (out_f32) return relu ? conv_fwd_any<true, true>(&ctx->c, x, w, bias, Y, g)
                              : conv_fwd_any<false, true>(&ctx->c, x, w, bias, Y, g);
     return relu ? conv_fwd_any<true, false>(&ctx->c, x, w, bias, Y, g) : conv_fwd_any<false, false>(&ctx->c, x, w, bias, Y, g);
+}
+
+int32_t phx_nn_conv_kpn(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* W, int32_t Kp,
+                        const float* bias, const float* irr, const float* alb, int32_t B, int32_t Hp, int32_t Wp,
+                        int32_t h, int32_t w, float* out, float* err) {
+    if (!ctx || !X || !W || !bias || !irr || !alb || !out || !err) return fail(PHX_ERR_INVALID, "null argument");
+    if (h <= 0 || w <= 0 || h > Hp || w > Wp) return fail(PHX_ERR_INVALID, "conv+kpn: bad valid region");
+    Geo g{B, Hp, Wp, cin, xs, xo, 32, 32, 0, 9 * cin, Kp};
+    PHX_TRY(check_geo(g));
+    PHX_TRY(use(&ctx->c));
+    return conv_kpn(&ctx->c, (const bf16*)X, (const bf16*)W, bias, g, KpnOut{irr, alb, out, err, h, w});
 }
 
 int32_t phx_nn_conv_wgrad(phx_ctx ctx, const void* X, int32_t xs, int32_t xo, int32_t cin, const void* dY,

@@ -158,7 +158,8 @@ int32_t relu_bwd(phx_unet_s* n, View y, View dy, int C, const Shape& s, int leve
 
 View v(DevMem& m, int pitch, int off = 0) { return View{m.ptr, pitch, off}; }
 
-int32_t forward(phx_unet_s* n, const void* feat, const Shape& s) {
+// Every layer up to the head's input (Db[0]); with_head: the head too (fp32 logits).
+int32_t forward(phx_unet_s* n, const void* feat, const Shape& s, bool with_head = true) {
     View x{(void*)feat, FEAT, 0};
     for (int l = 0; l < 4; l++) {
         PHX_TRY(layer_fwd(n, 2 * l, x, v(n->A[l], LEVEL_CH[l]), s, l));
@@ -179,6 +180,7 @@ int32_t forward(phx_unet_s* n, const void* feat, const Shape& s) {
         below = v(n->Db[l], LEVEL_CH[l]);
         below_ch = LEVEL_CH[l];
     }
+    if (!with_head) return PHX_OK;
     return layer_fwd(n, 18, below, View{n->logits.ptr, HEAD, 0}, s, 0);
 }
 
@@ -410,6 +412,13 @@ int32_t phx_unet_forward(phx_unet net, const void* feat, const float* irr, const
     PHX_TRY(check_shape(s));
     PHX_TRY(use(net->ctx));
     PHX_TRY(ensure(net, s));
+    if (out && err) {
+        // inference: the head's epilogue applies the predicted kernels (no logits)
+        PHX_TRY(forward(net, feat, s, false));
+        const Conv& c = net->L[NL - 1];
+        return phx_nn_conv_kpn(net->handle, net->Db[0].ptr, 32, 0, c.cin, c.wb.ptr, c.Kp, (const float*)c.b32.ptr,
+                               irr, alb, B, Hp, Wp, h, w, out, err);
+    }
     PHX_TRY(forward(net, feat, s));
     if (!out && !err) return PHX_OK;
     return phx_nn_kpn(net->handle, (const float*)net->logits.ptr, irr, alb, nullptr, B, Hp, Wp, h, w, out, err,

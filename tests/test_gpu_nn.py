@@ -293,6 +293,39 @@ def test_kpn_and_loss_gradient(gpu):
     assert np.all(got[:, h:] == 0) and np.all(got[:, :, w:] == 0) and np.all(got[..., 26:] == 0)
 
 
+def test_head_with_kpn_epilogue_equals_head_then_kpn(gpu):
+    """The fused head + kernel-prediction step gives the outputs of the head
+    convolution (fp32 logits) followed by the kernel-prediction kernel."""
+    import torch
+
+    rng = np.random.default_rng(21)
+    B, Hp, Wp, h, w = 2, 32, 48, 29, 41
+    x = nn.bf16(rng.normal(size=(B, Hp, Wp, 32)) * 0.5)
+    wgt, wp, Kp = _weights(rng, 32, 32)
+    bias = (rng.normal(size=32) * 0.1).astype(np.float32)
+    irr = rng.gamma(1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    alb = rng.uniform(0.05, 1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    X, Wt, bb, I, A = _t(x, "bf16"), _t(wp, "bf16"), _t(bias), _t(irr), _t(alb)
+    logits = torch.empty((B, Hp, Wp, 32), dtype=torch.float32, device="cuda")
+    o1 = torch.empty((B, Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    e1 = torch.empty((B, Hp, Wp), dtype=torch.float32, device="cuda")
+    o2 = torch.empty_like(o1)
+    e2 = torch.empty_like(e1)
+    torch.cuda.synchronize()
+    L = N.lib()
+    N.check(L.phx_nn_conv_fwd(gpu.handle, X.data_ptr(), 32, 0, 32, Wt.data_ptr(), Kp, bb.data_ptr(), logits.data_ptr(),
+                              32, 0, 32, B, Hp, Wp, 0, 1))
+    N.check(L.phx_nn_kpn(gpu.handle, logits.data_ptr(), I.data_ptr(), A.data_ptr(), None, B, Hp, Wp, h, w,
+                         o1.data_ptr(), e1.data_ptr(), None, None, 0.0))
+    N.check(L.phx_nn_conv_kpn(gpu.handle, X.data_ptr(), 32, 0, 32, Wt.data_ptr(), Kp, bb.data_ptr(), I.data_ptr(),
+                              A.data_ptr(), B, Hp, Wp, h, w, o2.data_ptr(), e2.data_ptr()))
+    _sync(gpu)
+    assert np.allclose(_np(o1), _np(o2), rtol=1e-6, atol=1e-7)
+    assert np.allclose(_np(e1), _np(e2), rtol=1e-6, atol=1e-9)
+    o, e = nn.kpn(nn.conv(x, wgt, bias.astype(np.float64), False), irr.astype(np.float64), alb.astype(np.float64), h, w)
+    assert np.allclose(_np(o2), o, rtol=1e-4, atol=1e-6)
+
+
 def test_adam(gpu):
     import torch
 
