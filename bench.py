@@ -428,7 +428,7 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     import phiray_b200 as px
     from phiray_b200 import kernels
     from phiray_b200 import train as T
-    from phiray_b200.denoiser import THRESHOLD, TILE, WEIGHTS, Unet
+    from phiray_b200.denoiser import THRESHOLD, TILE, WEIGHTS, Unet, snapshot_host
 
     if not os.path.exists(WEIGHTS):
         return {"unavailable": f"no trained weights at {os.path.relpath(WEIGHTS, ROOT)}"}
@@ -445,29 +445,47 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     prev = tr.image()
     ref = T.radiance(T.px_diff(prev, None, n), W, H)
     buf = px.GpuArray(gpu, (34 * n + 1) * 4)
+    hbuf = px.GpuArray(gpu, n * 16)
     rel_plain, rel_learned, kept = {}, {}, {}
     tiles = ((W + TILE - 1) // TILE) * ((H + TILE - 1) // TILE)
     for spp in learned_spp + plain_spp:
-        tr.trace(cam, W, H, frame, spp)
+        # traced in two halves: the first half's image is the learned
+        # denoiser's part-way snapshot (the plain method ignores it)
+        first = spp // 2
+        mid = None
+        if first > 0:
+            tr.trace(cam, W, H, frame, first)
+            mid = tr.image()
+        tr.trace(cam, W, H, frame + first, spp - first)
         frame += spp
         img = tr.image()
         noisy = T.px_diff(img, prev, n)
+        half = None if mid is None else snapshot_host(T.px_diff(mid, prev, n), W, H)
         prev = img
         buf.write(noisy)
         kernels.denoise(gpu, buf, W, H)
         rel_plain[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
         if spp in learned_spp:
             buf.write(noisy)
-            kept[spp] = net.denoise_px(buf, W, H, TILE, THRESHOLD, count=True) / tiles
+            if half is not None:
+                hbuf.write(half)
+            kept[spp] = net.denoise_px(buf, W, H, half=hbuf if half is not None else None, tile=TILE,
+                                       threshold=THRESHOLD, count=True) / tiles
             rel_learned[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
     buf.free()
 
     def frame_ms(spp, learned, reps):
         def once():
-            tr.trace(cam, W, H, 0, spp)
-            if learned:
+            if learned and spp >= 2:
+                tr.trace(cam, W, H, 0, spp // 2)
+                tr.snapshot(hbuf)
+                tr.trace(cam, W, H, spp // 2, spp - spp // 2)
+                net.denoise(tr, half=hbuf)
+            elif learned:
+                tr.trace(cam, W, H, 0, spp)
                 net.denoise(tr)
             else:
+                tr.trace(cam, W, H, 0, spp)
                 tr.denoise()
         once()
         gpu.wait(60000)
@@ -514,6 +532,7 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     else:
         out["learned"] = None
         out["speedup_at_equal_relmse"] = None
+    hbuf.free()
     net.close()
     tr.close()
     return out

@@ -539,9 +539,14 @@ int32_t phx_nn_kpn(phx_ctx ctx, const float* logits, const float* irr, const flo
 int32_t phx_nn_adam(phx_ctx ctx, float* w, const float* g, float* m, float* v, void* wb, int32_t rows, int32_t Kp,
                     int32_t K, int32_t g_transposed, float lr, float b1, float b2, float eps, int32_t step);
 /* Network inputs from a traced px image (w x h) into padded Hp x Wp planes:
- * feat (16 bf16 channels), irr and alb (fp32 x 3). */
-int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, int32_t w, int32_t h, int32_t Hp, int32_t Wp, void* feat,
-                        float* irr, float* alb);
+ * feat (16 bf16 channels), irr and alb (fp32 x 3). half (nullable): a
+ * phx_nn_snapshot of the same image taken part way through its samples,
+ * from which the pixels' own sample spread is read. */
+int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, const float* half, int32_t w, int32_t h, int32_t Hp,
+                        int32_t Wp, void* feat, float* irr, float* alb);
+/* A snapshot of a px image's linear sums and met-sample counts (w * h x 4
+ * floats, device): the `half` input of phx_nn_features. */
+int32_t phx_nn_snapshot(phx_ctx ctx, const uint32_t* px, uint32_t w, uint32_t h, float* snap);
 /* Per tile x tile block: mean error estimate into tile_err and the count of
  * tiles above threshold into *fallback (device); every pixel of a tile within
  * the threshold gets `out` written into the px planes (sums unless keep,
@@ -578,17 +583,22 @@ int32_t phx_unet_train_step(phx_unet net, const void* feat, const float* irr, co
                             float* loss);
 /* Device pointer of the last forward's head output ([B][Hp][Wp][32] fp32). */
 int32_t phx_unet_logits(phx_unet net, float** logits);
-/* Denoises a traced px image in place: features, network, the a-trous
+/* Denoises a traced px image in place (`half`: nullable snapshot, as
+ * phx_nn_features): features, network, the a-trous
  * Denoise (phx_denoise, strength 64/8/40/7), then the learned result on every
  * tile x tile block whose mean error estimate is <= threshold. With
  * `fallback` non-NULL, waits and returns the number of tiles that kept the
  * a-trous result. */
-int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, uint32_t w, uint32_t h, const float view[4], int32_t tile,
-                            float threshold, int32_t keep, uint32_t* fallback);
+int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint32_t w, uint32_t h,
+                            const float view[4], int32_t tile, float threshold, int32_t keep, uint32_t* fallback);
+/* phx_nn_snapshot of the tracer's image as it is now (take it half way
+ * through a frame's samples and pass it to phx_tracer_denoise_learned). */
+int32_t phx_tracer_snapshot(phx_tracer tr, float* snap);
 /* Tracer::denoise with the learned denoiser (phx_unet_denoise_px on the
- * tracer's image and last camera's view); nothing traced: no-op. */
-int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, int32_t tile, float threshold, int32_t keep,
-                                   uint32_t* fallback);
+ * tracer's image, `half` (nullable) and the last camera's view); nothing
+ * traced: no-op. */
+int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, const float* half, int32_t tile, float threshold,
+                                   int32_t keep, uint32_t* fallback);
 
 /* ---- Batched serving: many tracers' frames in one persistent launch (no
  * reference counterpart; phiber renders one Tracer per view). ---- */

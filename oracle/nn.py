@@ -147,15 +147,18 @@ def _fin(a):
     return np.where(np.isfinite(a), a, 0.0)
 
 
-def features(px: np.ndarray, w: int, h: int, Hp: int, Wp: int):
-    """(feat (Hp, Wp, 16), irr (Hp, Wp, 3), alb (Hp, Wp, 3)) from px planes."""
+def features(px: np.ndarray, w: int, h: int, Hp: int, Wp: int, half: np.ndarray | None = None):
+    """(feat (Hp, Wp, 16), irr (Hp, Wp, 3), alb (Hp, Wp, 3)) from px planes;
+    `half` (n, 4): sums and met-sample counts part way through the samples."""
     n = w * h
     f = px.view(np.float32).astype(np.float64)
-    cnt = np.maximum(px[31 * n:32 * n].astype(np.float64), 1.0)
+    cnt_raw = px[31 * n:32 * n].astype(np.float64)
+    cnt = np.maximum(cnt_raw, 1.0)
     gone = f[33 * n:34 * n]
     met = np.maximum(cnt - gone, 1.0)
-    with np.errstate(invalid="ignore", over="ignore"):
-        rad = _fin(np.maximum(f[n:4 * n].reshape(n, 3) / met[:, None], 0.0))
+    sums = f[n:4 * n].reshape(n, 3)
+    with np.errstate(invalid="ignore", over="ignore", divide="ignore"):
+        rad = _fin(np.maximum(sums / met[:, None], 0.0))
         al = _fin(f[7 * n:10 * n].reshape(n, 3) / cnt[:, None])
     ad = np.maximum(al, 0.05)
     ir = rad / ad
@@ -165,7 +168,16 @@ def features(px: np.ndarray, w: int, h: int, Hp: int, Wp: int):
     d = _fin(f[13 * n:14 * n] / cnt)
     feat = np.zeros((Hp, Wp, 16))
     v = feat[:h, :w]
-    v[..., 0:3] = np.log1p(rad).reshape(h, w, 3)
+    if half is not None:
+        hs = half.astype(np.float64)
+        met_total = cnt_raw - gone
+        spread = (hs[:, 3] >= 1.0) & (met_total - hs[:, 3] >= 1.0)
+        with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+            ra = np.maximum(hs[:, :3] / hs[:, 3:4], 0.0)
+            rb = np.maximum((sums - hs[:, :3]) / (met_total - hs[:, 3])[:, None], 0.0)
+            sp = _fin(np.abs(ra - rb) * 0.5 / np.maximum(al, 0.05))
+        v[..., 0:3] = np.where(spread[:, None], np.log1p(np.where(spread[:, None], sp, 0.0)), 0.0).reshape(h, w, 3)
+        v[..., 15] = spread.astype(np.float64).reshape(h, w)
     v[..., 3:6] = np.log1p(ir).reshape(h, w, 3)
     v[..., 6:9] = al.reshape(h, w, 3)
     v[..., 9:12] = nr.reshape(h, w, 3)

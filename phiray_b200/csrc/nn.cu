@@ -935,14 +935,19 @@ __device__ __forceinline__ float finite_or_zero(float v) { return isfinite(v) ? 
 
 // Network inputs from a traced image (px planes, src/trace/read.rs:37-56).
 // Per pixel of the padded image (Hp x Wp; padding pixels all zero) 16 bf16
-// channels: log(1 + radiance) 3, log(1 + irradiance) 3, albedo 3, normal 3,
-// depth / (1 + |depth|), the fraction of samples that met something,
-// log2(samples) / 8, 0; a plane value that is not finite reads as 0. Radiance is the mean over the samples that met
-// something (Tracer::radiance, read.rs:241-251); albedo' = max(albedo, 0.05)
-// per channel; irradiance = radiance / albedo'. Also writes irr and albedo'
-// (fp32 x 3 each), the planes the predicted kernels filter and remodulate.
-__global__ void k_features(const uint32_t* __restrict__ px, int w, int h, int Hp, int Wp, bf16* __restrict__ feat,
-                           float* __restrict__ irr, float* __restrict__ alb) {
+// channels: log(1 + |irr_a - irr_b| / 2) 3, log(1 + irradiance) 3, albedo 3,
+// normal 3, depth / (1 + |depth|), the fraction of samples that met
+// something, log2(samples) / 8, and 1 where the first channels hold a
+// spread, 0 where they do not. Radiance is the mean over the samples that
+// met something (Tracer::radiance, read.rs:241-251); albedo' = max(albedo,
+// 0.05) per channel; irradiance = radiance / albedo'. irr_a / irr_b are the
+// irradiances of the samples before and after `half` (a snapshot of the
+// sums and met-sample count taken part way, phx_nn_snapshot; NULL: none) —
+// their difference is the pixel's own sample spread. A plane value that is
+// not finite reads as 0. Also writes irr and albedo' (fp32 x 3 each), the
+// planes the predicted kernels filter and remodulate.
+__global__ void k_features(const uint32_t* __restrict__ px, const float4* __restrict__ half, int w, int h, int Hp,
+                           int Wp, bf16* __restrict__ feat, float* __restrict__ irr, float* __restrict__ alb) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= Hp * Wp) return;
     const int x = q % Wp, y = q / Wp;
@@ -957,15 +962,25 @@ __global__ void k_features(const uint32_t* __restrict__ px, int w, int h, int Hp
         const float gone = __uint_as_float(px[33 * n + i]);
         const float met = fmaxf(k - gone, 1.0f);
         const float ln2 = 0.693147182f;
+        float4 hs = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (half) hs = half[i];
+        const float met_total = (float)cnt - gone;
+        const bool spread = half && hs.w >= 1.0f && met_total - hs.w >= 1.0f;
+        const float hsum[3] = {hs.x, hs.y, hs.z};
         float nn = 0.0f;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             // a sample that overflowed (or a NaN) gives no input rather than a poisoned one
-            const float rad = finite_or_zero(fmaxf(__uint_as_float(px[n + 3 * i + c]) / met, 0.0f));
+            const float sum = __uint_as_float(px[n + 3 * i + c]);
+            const float rad = finite_or_zero(fmaxf(sum / met, 0.0f));
             const float al = finite_or_zero(__uint_as_float(px[7 * n + 3 * i + c]) / k);
             ad[c] = fmaxf(al, 0.05f);
             ir[c] = rad / ad[c];
-            f[c] = pm_log2(1.0f + rad) * ln2;
+            if (spread) {
+                const float ra = fmaxf(hsum[c] / hs.w, 0.0f);
+                const float rb = fmaxf((sum - hsum[c]) / (met_total - hs.w), 0.0f);
+                f[c] = pm_log2(1.0f + finite_or_zero(fabsf(ra - rb) * 0.5f / ad[c])) * ln2;
+            }
             f[3 + c] = pm_log2(1.0f + ir[c]) * ln2;
             f[6 + c] = al;
             f[9 + c] = finite_or_zero(__uint_as_float(px[10 * n + 3 * i + c]));
@@ -978,6 +993,7 @@ __global__ void k_features(const uint32_t* __restrict__ px, int w, int h, int Hp
         f[12] = d / (1.0f + fabsf(d));
         f[13] = fmaxf(1.0f - gone / k, 0.0f);
         f[14] = pm_log2(k) * 0.125f;
+        f[15] = spread ? 1.0f : 0.0f;
     }
     uint4* o = (uint4*)(feat + (size_t)q * 16);
     o[0] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
@@ -988,6 +1004,16 @@ __global__ void k_features(const uint32_t* __restrict__ px, int w, int h, int Hp
         irr[(size_t)q * 3 + c] = ir[c];
         alb[(size_t)q * 3 + c] = ad[c];
     }
+}
+
+// The sums and met-sample count of a px image now: the `half` snapshot of
+// k_features (float4 per pixel: linear sums xyz, samples - missed).
+__global__ void k_snapshot(const uint32_t* __restrict__ px, uint32_t n, float4* __restrict__ snap) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    snap[i] = make_float4(__uint_as_float(px[n + 3 * i]), __uint_as_float(px[n + 3 * i + 1]),
+                          __uint_as_float(px[n + 3 * i + 2]),
+                          (float)px[31 * (size_t)n + i] - __uint_as_float(px[33 * (size_t)n + i]));
 }
 
 // Mean of the per-pixel error estimate over each ts x ts tile of the valid
@@ -1288,13 +1314,23 @@ int32_t phx_nn_adam(phx_ctx ctx, float* w, const float* g, float* m, float* v, v
     return cuda_check(cudaGetLastError(), "adam");
 }
 
-int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, int32_t w, int32_t h, int32_t Hp, int32_t Wp, void* feat,
-                        float* irr, float* alb) {
+int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, const float* half, int32_t w, int32_t h, int32_t Hp,
+                        int32_t Wp, void* feat, float* irr, float* alb) {
     if (!ctx || !px || !feat || !irr || !alb || w <= 0 || h <= 0 || Hp < h || Wp < w)
         return fail(PHX_ERR_INVALID, "features arguments");
     PHX_TRY(use(&ctx->c));
-    k_features<<<(Hp * Wp + 255) / 256, 256, 0, ctx->c.stream>>>(px, w, h, Hp, Wp, (bf16*)feat, irr, alb);
+    k_features<<<(Hp * Wp + 255) / 256, 256, 0, ctx->c.stream>>>(px, (const float4*)half, w, h, Hp, Wp, (bf16*)feat,
+                                                                 irr, alb);
     return cuda_check(cudaGetLastError(), "features");
+}
+
+int32_t phx_nn_snapshot(phx_ctx ctx, const uint32_t* px, uint32_t w, uint32_t h, float* snap) {
+    if (!ctx || !px || !snap) return fail(PHX_ERR_INVALID, "null argument");
+    const uint32_t n = w * h;
+    if (n == 0) return PHX_OK;
+    PHX_TRY(use(&ctx->c));
+    k_snapshot<<<(n + 255) / 256, 256, 0, ctx->c.stream>>>(px, n, (float4*)snap);
+    return cuda_check(cudaGetLastError(), "snapshot");
 }
 
 int32_t phx_nn_compose(phx_ctx ctx, uint32_t* px, int32_t w, int32_t h, int32_t Wp, const float* out, const float* err,

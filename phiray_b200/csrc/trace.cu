@@ -1850,13 +1850,21 @@ int32_t phx_tracer_denoise(phx_tracer tr, int32_t keep) {
                        strength, tr->last.view, keep);
 }
 
-int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, int32_t tile, float threshold, int32_t keep,
-                                   uint32_t* fallback) {
+int32_t phx_tracer_snapshot(phx_tracer tr, float* snap) {
+    if (!tr || !snap) return fail(PHX_ERR_INVALID, "null argument");
+    if (!tr->px.ptr) return fail(PHX_ERR_INVALID, "nothing traced");
+    PHX_TRY(use(tr->ctx));
+    return phx_nn_snapshot((phx_ctx)((char*)tr->ctx - offsetof(phx_ctx_s, c)), (const uint32_t*)tr->px.ptr, tr->w,
+                           tr->h, snap);
+}
+
+int32_t phx_tracer_denoise_learned(phx_tracer tr, phx_unet net, const float* half, int32_t tile, float threshold,
+                                   int32_t keep, uint32_t* fallback) {
     if (!tr || !net) return fail(PHX_ERR_INVALID, "null argument");
     if (fallback) *fallback = 0;
     if (!tr->px.ptr || !tr->have_last) return PHX_OK;  // nothing traced: read.rs:90
     PHX_TRY(use(tr->ctx));
-    return phx_unet_denoise_px(net, (uint32_t*)tr->px.ptr, tr->w, tr->h, tr->last.view, tile, threshold, keep,
+    return phx_unet_denoise_px(net, (uint32_t*)tr->px.ptr, half, tr->w, tr->h, tr->last.view, tile, threshold, keep,
                                fallback);
 }
 
@@ -2328,8 +2336,8 @@ int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
     for (size_t j = 0; j < b->jobs.size(); j++) {
         BatchJob& bj = b->jobs[j];
         if (b->net_of[j] >= 0)
-            PHX_TRY(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, bj.cam.view, 16,
-                                        threshold, 0, nullptr));
+            PHX_TRY(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, nullptr, bj.w, bj.h,
+                                        bj.cam.view, 16, threshold, 0, nullptr));
         else
             PHX_TRY(phx_denoise(b->handle, (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, strength, bj.cam.view, 0));
     }
@@ -2359,8 +2367,8 @@ int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
     for (size_t j = 0; j < b->jobs.size() && rc == PHX_OK; j++) {
         BatchJob& bj = b->jobs[j];
         if (b->net_of[j] >= 0)
-            step(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, bj.cam.view, 16,
-                                     threshold, 0, nullptr));
+            step(phx_unet_denoise_px(b->nets[b->net_of[j]], (uint32_t*)bj.tr->px.ptr, nullptr, bj.w, bj.h,
+                                     bj.cam.view, 16, threshold, 0, nullptr));
         else
             step(phx_denoise(b->handle, (uint32_t*)bj.tr->px.ptr, bj.w, bj.h, strength, bj.cam.view, 0));
         k_stamp<<<1, 1, 0, c->stream>>>(stamps + 1 + j);

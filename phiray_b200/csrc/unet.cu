@@ -465,8 +465,8 @@ int32_t phx_unet_logits(phx_unet net, float** logits) {
     return PHX_OK;
 }
 
-int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, uint32_t w, uint32_t h, const float view[4], int32_t tile,
-                            float threshold, int32_t keep, uint32_t* fallback) {
+int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint32_t w, uint32_t h,
+                            const float view[4], int32_t tile, float threshold, int32_t keep, uint32_t* fallback) {
     if (!net || !px || !view) return fail(PHX_ERR_INVALID, "null argument");
     if (w == 0 || h == 0) return PHX_OK;
     if (tile <= 0) return fail(PHX_ERR_INVALID, "unet: tile %d", tile);
@@ -480,7 +480,7 @@ int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, uint32_t w, uint32_t h, 
     PHX_TRY(net->err.reserve(P * 4));
     PHX_TRY(net->tile_err.reserve((size_t)((w + tile - 1) / tile) * ((h + tile - 1) / tile) * 4));
     PHX_TRY(net->fallback.reserve(4));
-    PHX_TRY(phx_nn_features(net->handle, px, (int)w, (int)h, Hp, Wp, net->feat.ptr, (float*)net->irr.ptr,
+    PHX_TRY(phx_nn_features(net->handle, px, half, (int)w, (int)h, Hp, Wp, net->feat.ptr, (float*)net->irr.ptr,
                             (float*)net->alb.ptr));
     PHX_TRY(phx_unet_forward(net, net->feat.ptr, (const float*)net->irr.ptr, (const float*)net->alb.ptr, 1, Hp, Wp,
                              (int)h, (int)w, (float*)net->out.ptr, (float*)net->err.ptr));

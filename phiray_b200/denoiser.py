@@ -121,22 +121,23 @@ class Unet:
         N.check(N.lib().phx_unet_train_step(self.handle, devptr(feat), devptr(irr), devptr(alb), devptr(ref), B, Hp,
                                             Wp, h, w, err_weight, lr, devptr(loss)))
 
-    def denoise(self, tracer, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
+    def denoise(self, tracer, half=None, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
                 count: bool = False) -> int | None:
-        """Learned ``Tracer::denoise``; with count=True waits and returns the
-        number of tiles that kept the a-trous result."""
+        """Learned ``Tracer::denoise``; `half`: a snapshot (``Tracer.snapshot``)
+        taken part way through the frame's samples, or None. With count=True
+        waits and returns the number of tiles that kept the a-trous result."""
         fb = C.c_uint32()
-        N.check(N.lib().phx_tracer_denoise_learned(tracer.handle, self.handle, tile, threshold, 1 if keep else 0,
-                                                   C.byref(fb) if count else None))
+        N.check(N.lib().phx_tracer_denoise_learned(tracer.handle, self.handle, devptr(half), tile, threshold,
+                                                   1 if keep else 0, C.byref(fb) if count else None))
         return fb.value if count else None
 
-    def denoise_px(self, px, w: int, h: int, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
-                   view=(0.0, 0.0, 1.0, 0.0), count: bool = False) -> int | None:
+    def denoise_px(self, px, w: int, h: int, half=None, tile: int = TILE, threshold: float = THRESHOLD,
+                   keep: bool = False, view=(0.0, 0.0, 1.0, 0.0), count: bool = False) -> int | None:
         """The same on any device px image (34 w h + 1 words)."""
         fb = C.c_uint32()
         v = (C.c_float * 4)(*view)
-        N.check(N.lib().phx_unet_denoise_px(self.handle, devptr(px), w, h, v, tile, threshold, 1 if keep else 0,
-                                            C.byref(fb) if count else None))
+        N.check(N.lib().phx_unet_denoise_px(self.handle, devptr(px), devptr(half), w, h, v, tile, threshold,
+                                            1 if keep else 0, C.byref(fb) if count else None))
         return fb.value if count else None
 
     def close(self) -> None:
@@ -151,6 +152,23 @@ class Unet:
             pass
 
 
-def features(gpu: Gpu, px, w: int, h: int, Hp: int, Wp: int, feat, irr, alb) -> None:
-    """Network inputs of a traced px image (phx_nn_features)."""
-    N.check(N.lib().phx_nn_features(gpu.handle, devptr(px), w, h, Hp, Wp, devptr(feat), devptr(irr), devptr(alb)))
+def features(gpu: Gpu, px, w: int, h: int, Hp: int, Wp: int, feat, irr, alb, half=None) -> None:
+    """Network inputs of a traced px image (phx_nn_features); `half`: a
+    snapshot taken part way through its samples, or None."""
+    N.check(N.lib().phx_nn_features(gpu.handle, devptr(px), devptr(half), w, h, Hp, Wp, devptr(feat), devptr(irr),
+                                    devptr(alb)))
+
+
+def snapshot(gpu: Gpu, px, w: int, h: int, snap) -> None:
+    """phx_nn_snapshot: the sums and met-sample counts of a px image now."""
+    N.check(N.lib().phx_nn_snapshot(gpu.handle, devptr(px), w, h, devptr(snap)))
+
+
+def snapshot_host(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """The same snapshot from a host px image: (w h, 4) float32."""
+    n = w * h
+    f = px.view(np.float32)
+    out = np.empty((n, 4), np.float32)
+    out[:, :3] = f[n:4 * n].reshape(n, 3)
+    out[:, 3] = px[31 * n:32 * n].astype(np.float32) - f[33 * n:34 * n]
+    return out

@@ -207,6 +207,11 @@ class Tracer:
         N.check(N.lib().phx_tracer_image(self.handle, C.byref(p), C.byref(words)))
         return p.value or 0, words.value
 
+    def snapshot(self, snap) -> None:
+        """The image's sums and met-sample counts now, into a device array of
+        w h x 4 floats (the learned denoiser's `half` input)."""
+        N.check(N.lib().phx_tracer_snapshot(self.handle, devptr(snap)))
+
     def denoise(self, keep: bool = False) -> None:
         N.check(N.lib().phx_tracer_denoise(self.handle, 1 if keep else 0))
 

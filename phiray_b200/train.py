@@ -3,9 +3,10 @@
 ``python -m phiray_b200.train --scenes 160 --ref-spp 1024 --steps 4000
 --out phiray_b200/weights/kpcn.phxu`` renders each seeded procedural scene
 (`scenes.procedural`) once as one continuous accumulation: several short
-segments (1-16 samples) whose px images, differenced from the running
-total, are independent noisy inputs, then `ref-spp` further samples whose
-difference is the reference. Every px plane the network reads (sums,
+segments (1-64 samples) whose px images, differenced from the running
+total, are independent noisy inputs (each traced in two halves, the first
+half's image giving the part-way snapshot of its sample spread), then
+`ref-spp` further samples whose difference is the reference. Every px plane the network reads (sums,
 albedo/normal/depth guides, sample and miss counts) accumulates linearly,
 so a difference of two accumulations is the image of the samples between
 them. The network then trains on random crops of those pairs with the
@@ -25,7 +26,7 @@ import time
 import numpy as np
 
 from . import kernels, scenes
-from .denoiser import TILE, Unet, features
+from .denoiser import TILE, Unet, features, snapshot_host
 from .gpu import Gpu, GpuArray
 from .tracer import PX_LEN, Tracer, camera
 
@@ -64,34 +65,11 @@ def relmse(x: np.ndarray, ref: np.ndarray) -> float:
     return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
 
 
-def render_pairs(gpu: Gpu, scene, segments, ref_spp: int, chunk: int = 256):
-    """(noisy px images for each segment's spp, reference px image)."""
-    w, h = scene.width, scene.height
-    n = w * h
-    tr = Tracer.of(gpu, scene)
-    cam = camera(scene)
-    frame, prev, noisy = 0, None, []
-    for spp in segments:
-        tr.trace(cam, w, h, frame, spp)
-        frame += spp
-        img = tr.image()
-        noisy.append(px_diff(img, prev, n))
-        prev = img
-    left = ref_spp
-    while left > 0:
-        c = min(chunk, left)
-        tr.trace(cam, w, h, frame, c)
-        frame += c
-        left -= c
-    ref = px_diff(tr.image(), prev, n)
-    tr.close()
-    return noisy, ref
-
-
 def render_group(gpu: Gpu, scs, segments, ref_spp: int, chunk: int = 256):
-    """render_pairs for several scenes at once: every pass traces all the
-    scenes' frames in one persistent batch launch (a single 256 x 256 image
-    cannot fill the GPU on its own)."""
+    """Noisy images (one per segment, each with its part-way snapshot or None),
+    and the reference image, of several scenes: one continuous accumulation
+    per scene, every pass tracing all the scenes' frames in one persistent
+    batch launch (a single 256 x 256 image cannot fill the GPU on its own)."""
     from .batch import Batch
 
     trs = [Tracer.of(gpu, sc) for sc in scs]
@@ -107,12 +85,23 @@ def render_group(gpu: Gpu, scs, segments, ref_spp: int, chunk: int = 256):
     frame = 0
     prev = [None] * len(scs)
     noisy = [[] for _ in scs]
+    halves = [[] for _ in scs]
     for spp in segments:
-        run(frame, spp)
+        # a segment of two or more samples is traced in two halves: the first
+        # half's image is its part-way snapshot (the pixels' sample spread)
+        first = spp // 2
+        mid = [None] * len(scs)
+        if first > 0:
+            run(frame, first)
+            mid = [tr.image() for tr in trs]
+        run(frame + first, spp - first)
         frame += spp
         for k, (sc, tr) in enumerate(zip(scs, trs)):
+            n = sc.width * sc.height
             img = tr.image()
-            noisy[k].append(px_diff(img, prev[k], sc.width * sc.height))
+            noisy[k].append(px_diff(img, prev[k], n))
+            halves[k].append(None if mid[k] is None else snapshot_host(px_diff(mid[k], prev[k], n), sc.width,
+                                                                        sc.height))
             prev[k] = img
     left = ref_spp
     while left > 0:
@@ -124,7 +113,7 @@ def render_group(gpu: Gpu, scs, segments, ref_spp: int, chunk: int = 256):
     b.close()
     for tr in trs:
         tr.close()
-    return noisy, refs
+    return noisy, halves, refs
 
 
 class DataSet:
@@ -143,9 +132,9 @@ class DataSet:
         self.spp = np.zeros(count, np.int32)
         self.bad = 0
 
-    def add(self, noisy_px: np.ndarray, ref_rad: np.ndarray, spp: int) -> None:
-        """Appends one pair; a reference pixel that is not finite becomes 0
-        (counted in ``self.bad``)."""
+    def add(self, noisy_px: np.ndarray, half: np.ndarray | None, ref_rad: np.ndarray, spp: int) -> None:
+        """Appends one pair (`half`: the part-way snapshot, or None); a
+        reference pixel that is not finite becomes 0 (counted in ``self.bad``)."""
         import torch
 
         fin = np.isfinite(ref_rad)
@@ -155,10 +144,13 @@ class DataSet:
 
         i, s = self.n, self.size
         buf = GpuArray.from_(self.gpu, noisy_px)
-        features(self.gpu, buf, s, s, s, s, self.feat[i], self.irr[i], self.alb[i])
+        hbuf = GpuArray.from_(self.gpu, np.ascontiguousarray(half, np.float32)) if half is not None else None
+        features(self.gpu, buf, s, s, s, s, self.feat[i], self.irr[i], self.alb[i], half=hbuf)
         self.ref[i].copy_(torch.from_numpy(np.ascontiguousarray(ref_rad, dtype=np.float32)))
         self.gpu.wait()
         buf.free()
+        if hbuf is not None:
+            hbuf.free()
         self.spp[i] = spp
         self.n += 1
 
@@ -216,6 +208,7 @@ def scene_stream(indices, size: int, workers: int):
 
 
 GROUP = 16  # scenes rendered together in one batch launch
+DROP_HALF = 0.15  # share of training pairs given no part-way snapshot
 
 
 def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, workers: int = 0):
@@ -229,12 +222,16 @@ def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, 
         workers = max(1, min(8, (os.cpu_count() or 2) - 1))
     group = []
 
+    drop = np.random.default_rng(12345)
+
     def flush():
-        noisy_g, refs_g = render_group(gpu, group, segments, ref_spp)
-        for noisy, ref in zip(noisy_g, refs_g):
+        noisy_g, halves_g, refs_g = render_group(gpu, group, segments, ref_spp)
+        for noisy, halves, ref in zip(noisy_g, halves_g, refs_g):
             rr = radiance(ref, size, size)
-            for spp, px in zip(segments, noisy):
-                ds.add(px, rr, spp)
+            for spp, px, half in zip(segments, noisy, halves):
+                # some pairs go without the snapshot, so the network also
+                # serves callers that have none
+                ds.add(px, None if drop.random() < DROP_HALF else half, rr, spp)
             refs.append(rr)
             noisy_all.append(noisy)
         group.clear()
@@ -276,22 +273,25 @@ def train(gpu: Gpu, ds: DataSet, steps: int, batch: int, crop: int, lr: float, s
     return net, hist
 
 
-def evaluate(gpu: Gpu, net: Unet, noisy_px: np.ndarray, ref_rad: np.ndarray, w: int, h: int) -> dict:
+def evaluate(gpu: Gpu, net: Unet, noisy_px: np.ndarray, ref_rad: np.ndarray, w: int, h: int, half=None) -> dict:
     """relMSE against the reference of the noisy image, the a-trous Denoise,
     and the learned denoiser without and with the per-tile fallback at a few
     thresholds (with the share of tiles that kept the a-trous result)."""
     out = {"noisy": relmse(radiance(noisy_px, w, h), ref_rad)}
     buf = GpuArray.from_(gpu, noisy_px)
+    hbuf = GpuArray.from_(gpu, np.ascontiguousarray(half, np.float32)) if half is not None else None
     kernels.denoise(gpu, buf, w, h)
     out["denoise"] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
     tiles = ((w + TILE - 1) // TILE) * ((h + TILE - 1) // TILE)
     for name, thr in [("learned", 1e30)] + [(f"fallback_{t:g}", t) for t in (0.02, 0.05, 0.1, 0.2, 0.5)]:
         buf.write(noisy_px)
-        kept = net.denoise_px(buf, w, h, TILE, thr, count=True)
+        kept = net.denoise_px(buf, w, h, half=hbuf, tile=TILE, threshold=thr, count=True)
         out[name] = relmse(radiance(buf.read(np.uint32), w, h), ref_rad)
         if name != "learned":
             out[name + "_tiles"] = kept / tiles
     buf.free()
+    if hbuf is not None:
+        hbuf.free()
     return out
 
 
@@ -329,8 +329,9 @@ def main(argv=None) -> None:
     rows = []
     for i in held:
         sc = scenes.procedural(i, width=args.size, height=args.size)
-        noisy, ref = render_pairs(gpu, sc, [4], args.ref_spp)
-        rows.append(evaluate(gpu, net, noisy[0], radiance(ref, args.size, args.size), args.size, args.size))
+        noisy, halves, refs = render_group(gpu, [sc], [4], args.ref_spp)
+        rows.append(evaluate(gpu, net, noisy[0][0], radiance(refs[0], args.size, args.size), args.size, args.size,
+                             halves[0][0]))
     mean = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
     report = {"scenes": args.scenes, "pairs": ds.n, "nonfinite_ref_values": ds.bad, "segments": segments, "ref_spp": args.ref_spp,
               "steps": args.steps, "batch": args.batch, "crop": args.crop, "data_s": round(t_data, 1),

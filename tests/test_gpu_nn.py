@@ -369,24 +369,46 @@ def _fake_px(rng, w, h):
     return px
 
 
-def test_features(gpu):
+@pytest.mark.parametrize("with_half", [False, True])
+def test_features(gpu, with_half):
+    """Feature planes from px planes, with and without the part-way snapshot
+    (the snapshot taken on the device equals the host restatement's)."""
     import torch
+
+    from phiray_b200.denoiser import snapshot_host
 
     rng = np.random.default_rng(9)
     w, h, Hp, Wp = 37, 21, 32, 48
     px = _fake_px(rng, w, h)
+    n = w * h
+    half = None
+    if with_half:
+        early = px.copy()  # a part-way image: fewer samples, part of the sums
+        early[31 * n:32 * n] = px[31 * n:32 * n] // 2
+        fe = early.view(np.float32)
+        fe[n:4 * n] *= 0.4
+        fe[33 * n:34 * n] = np.minimum(fe[33 * n:34 * n], early[31 * n:32 * n].astype(np.float32))
+        E = _t(early.view(np.int32))
+        S = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        N.check(N.lib().phx_nn_snapshot(gpu.handle, E.data_ptr(), w, h, S.data_ptr()))
+        _sync(gpu)
+        half = snapshot_host(early, w, h)
+        assert np.array_equal(_np(S).astype(np.float32), half)
     P = _t(px.view(np.int32))
+    H_ = _t(half) if half is not None else None
     feat = torch.empty((Hp, Wp, 16), dtype=torch.bfloat16, device="cuda")
     irr = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
     alb = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
-    N.check(N.lib().phx_nn_features(gpu.handle, P.data_ptr(), w, h, Hp, Wp, feat.data_ptr(), irr.data_ptr(),
-                                    alb.data_ptr()))
+    N.check(N.lib().phx_nn_features(gpu.handle, P.data_ptr(), H_.data_ptr() if H_ is not None else None, w, h, Hp, Wp,
+                                    feat.data_ptr(), irr.data_ptr(), alb.data_ptr()))
     _sync(gpu)
-    f, i, a = nn.features(px, w, h, Hp, Wp)
+    f, i, a = nn.features(px, w, h, Hp, Wp, half)
     assert np.all(np.abs(_np(feat) - f) <= 2.0 ** -8 * np.abs(f) + 1e-6)
     assert np.allclose(_np(irr), i, rtol=1e-6, atol=0)
     assert np.allclose(_np(alb), a, rtol=1e-6, atol=0)
+    assert (f[..., 15] > 0).any() == with_half
 
 
 def _net_inputs(rng, B, H, W):
