@@ -21,10 +21,17 @@ enum : uint32_t {
     STATUS_STACK_OVERFLOW = 1u << 2,
 };
 
-// A growable device allocation.
+struct Ctx;
+
+// A growable device allocation. Reserved inside a context's call (after
+// use()), it comes from the context's stream-ordered pool on the context's
+// stream, and its release is a free ordered on that stream: the pool keeps
+// the memory mapped, so the next object of the context reuses it without a
+// cudaMalloc/cudaFree round trip through the driver. Otherwise cudaMalloc.
 struct DevMem {
     void* ptr = nullptr;
     size_t bytes = 0;
+    Ctx* owner = nullptr;          // the context whose pool holds ptr, or null
     int32_t reserve(size_t want);  // grows, discarding contents
     void release();
     ~DevMem() { release(); }
@@ -37,6 +44,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;  // where work goes (own, or a caller's)
     cudaStream_t capture = nullptr; // private stream for graph capture
     uint32_t* status = nullptr;     // device status word
+    cudaMemPool_t pool = nullptr;   // device memory of the context's objects
     DevMem denoise_scratch;         // guide and ping-pong planes of phx_denoise
     int live = 0;                   // buffers, passes, BVHs, tracers not yet freed
 };
@@ -50,8 +58,13 @@ int32_t cuda_check(cudaError_t e, const char* what);
 int32_t read_status(Ctx* c);
 // Bounded drain of `stream` (polls an event with a deadline).
 int32_t wait_stream(cudaStream_t s, uint32_t timeout_ms);
-// Ensures ctx's device is current on this thread.
+// Ensures ctx's device is current on this thread and makes ctx the one whose
+// pool this thread's DevMem reservations draw on.
 int32_t use(Ctx* c);
+// Device allocation from the context's pool, ordered on its stream (cudaMalloc
+// when the context has no pool); the matching free.
+int32_t ctx_alloc(Ctx* c, void** p, size_t bytes);
+void ctx_free(Ctx* c, void* p);
 
 // Kernel launches the Pass layer replays (one per phx_kernel_id), defined in
 // the kernel files. `params` is the step's params blob, `bufs` its buffers.

@@ -6,13 +6,25 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <thread>
+#include <unordered_set>
 
 #include "internal.cuh"
 
 namespace phx {
 
 static thread_local std::string g_last_error;
+// The context of this thread's last use(): DevMem::reserve draws on its pool.
+static thread_local Ctx* t_current = nullptr;
+// Contexts not yet destroyed (a stale t_current is never dereferenced).
+static std::mutex g_ctx_mutex;
+static std::unordered_set<Ctx*> g_ctxs;
+
+static bool ctx_alive(Ctx* c) {
+    std::lock_guard<std::mutex> lock(g_ctx_mutex);
+    return g_ctxs.count(c) != 0;
+}
 
 int32_t fail(int32_t code, const char* fmt, ...) {
     char buf[512];
@@ -37,7 +49,34 @@ int32_t use(Ctx* c) {
     if (!c) return fail(PHX_ERR_INVALID, "null context");
     int cur = -1;
     if (cudaGetDevice(&cur) != cudaSuccess || cur != c->device) PHX_CUDA(cudaSetDevice(c->device));
+    t_current = c;
     return PHX_OK;
+}
+
+int32_t ctx_alloc(Ctx* c, void** p, size_t bytes) {
+    *p = nullptr;
+    if (!c->pool) return cuda_check(cudaMalloc(p, bytes), "cudaMalloc");
+    // An allocation recorded into a graph would belong to the graph: refuse
+    // one made while the context's stream is being captured.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PHX_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        return fail(PHX_ERR_INVALID, "allocation of %zu bytes while the stream is captured", bytes);
+    PHX_CUDA(cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream));
+    // Kernels stage rows with 16-byte copies and vector loads: keep the
+    // 256-byte alignment cudaMalloc gives.
+    if ((uintptr_t)*p & 255u) {
+        cudaFreeAsync(*p, c->stream);
+        *p = nullptr;
+        return fail(PHX_ERR_DEVICE, "pool allocation of %zu bytes not 256-byte aligned", bytes);
+    }
+    return PHX_OK;
+}
+
+void ctx_free(Ctx* c, void* p) {
+    if (!p) return;
+    if (c && c->pool) cudaFreeAsync(p, c->stream);
+    else cudaFree(p);
 }
 
 int32_t wait_stream(cudaStream_t s, uint32_t timeout_ms) {
@@ -84,15 +123,23 @@ int32_t DevMem::reserve(size_t want) {
     if (want <= bytes && ptr) return PHX_OK;
     release();
     if (want == 0) return PHX_OK;
-    PHX_CUDA(cudaMalloc(&ptr, want));
+    Ctx* c = t_current;
+    int cur = -1;
+    if (c && ctx_alive(c) && cudaGetDevice(&cur) == cudaSuccess && cur == c->device) {
+        PHX_TRY(ctx_alloc(c, &ptr, want));
+        owner = c;
+    } else {
+        PHX_CUDA(cudaMalloc(&ptr, want));
+    }
     bytes = want;
     return PHX_OK;
 }
 
 void DevMem::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) ctx_free(owner, ptr);
     ptr = nullptr;
     bytes = 0;
+    owner = nullptr;
 }
 
 }  // namespace phx
@@ -133,6 +180,31 @@ int32_t phx_ctx_create(int32_t ordinal, phx_ctx* out) {
     Ctx& c = h->c;
     c.device = ordinal;
     cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, ordinal);
+    {
+        std::lock_guard<std::mutex> lock(g_ctx_mutex);
+        g_ctxs.insert(&c);
+    }
+    // The context's memory pool: freed blocks stay mapped (up to a quarter of
+    // the device) for the context's next objects. Without stream-ordered
+    // allocation support the context uses cudaMalloc.
+    int pools = 0;
+    cudaDeviceGetAttribute(&pools, cudaDevAttrMemoryPoolsSupported, ordinal);
+    if (pools) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ordinal;
+        if (cudaMemPoolCreate(&c.pool, &props) == cudaSuccess) {
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            uint64_t keep = total_b / 4;
+            cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            cudaGetLastError();
+            c.pool = nullptr;
+        }
+    }
     int32_t rc = cuda_check(cudaStreamCreateWithFlags(&c.own, cudaStreamNonBlocking), "stream");
     if (rc == PHX_OK) rc = cuda_check(cudaStreamCreateWithFlags(&c.capture, cudaStreamNonBlocking), "stream");
     if (rc == PHX_OK) rc = cuda_check(cudaMalloc(&c.status, 4), "status");
@@ -153,10 +225,18 @@ int32_t phx_ctx_destroy(phx_ctx ctx) {
     // under them (the caller frees buffers, passes, BVHs, tracers first).
     if (c.live > 0) return fail(PHX_ERR_INVALID, "context still has %d live objects", c.live);
     cudaSetDevice(c.device);
+    {
+        std::lock_guard<std::mutex> lock(g_ctx_mutex);
+        g_ctxs.erase(&c);
+    }
+    if (t_current == &c) t_current = nullptr;
+    if (c.stream) c.denoise_scratch.release();
+    if (c.stream) cudaStreamSynchronize(c.stream);
     if (c.own) cudaStreamSynchronize(c.own);
     if (c.status) cudaFree(c.status);
     if (c.capture) cudaStreamDestroy(c.capture);
     if (c.own) cudaStreamDestroy(c.own);
+    if (c.pool) cudaMemPoolDestroy(c.pool);
     delete ctx;
     return PHX_OK;
 }
@@ -172,7 +252,14 @@ void* phx_ctx_stream(phx_ctx ctx) { return ctx ? (void*)ctx->c.stream : nullptr;
 
 int32_t phx_ctx_set_stream(phx_ctx ctx, void* stream) {
     if (!ctx) return fail(PHX_ERR_INVALID, "null context");
-    ctx->c.stream = stream ? (cudaStream_t)stream : ctx->c.own;
+    cudaStream_t next = stream ? (cudaStream_t)stream : ctx->c.own;
+    if (next != ctx->c.stream) {
+        // Frees of the context's memory are ordered on its stream: drain the
+        // old one so nothing still running there reads a block freed on the new.
+        PHX_TRY(use(&ctx->c));
+        PHX_TRY(wait_stream(ctx->c.stream, 0));
+    }
+    ctx->c.stream = next;
     return PHX_OK;
 }
 
@@ -181,10 +268,10 @@ int32_t phx_buf_alloc(phx_ctx ctx, uint64_t bytes, phx_buf* out) {
     PHX_TRY(use(&ctx->c));
     void* p = nullptr;
     if (bytes) {
-        PHX_CUDA(cudaMalloc(&p, bytes));
+        PHX_TRY(ctx_alloc(&ctx->c, &p, bytes));
         int32_t rc = cuda_check(cudaMemsetAsync(p, 0, bytes, ctx->c.stream), "zero");
         if (rc != PHX_OK) {
-            cudaFree(p);
+            ctx_free(&ctx->c, p);
             return rc;
         }
     }
@@ -215,7 +302,7 @@ int32_t phx_buf_free(phx_buf buf) {
     if (buf->owned && buf->ptr) {
         use(buf->ctx);
         cudaStreamSynchronize(buf->ctx->stream);
-        cudaFree(buf->ptr);
+        ctx_free(buf->ctx, buf->ptr);
     }
     buf->ctx->live--;
     delete buf;
@@ -243,8 +330,8 @@ int32_t phx_buf_assign(phx_buf buf, const void* src, uint64_t bytes, int32_t* re
         PHX_TRY(use(buf->ctx));
         cudaStreamSynchronize(buf->ctx->stream);
         void* p = nullptr;
-        PHX_CUDA(cudaMalloc(&p, bytes));
-        if (buf->ptr) cudaFree(buf->ptr);
+        PHX_TRY(ctx_alloc(buf->ctx, &p, bytes));
+        ctx_free(buf->ctx, buf->ptr);
         buf->ptr = p;
         buf->bytes = bytes;
         re = 1;
