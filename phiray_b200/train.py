@@ -26,7 +26,7 @@ import time
 import numpy as np
 
 from . import kernels, scenes
-from .denoiser import TILE, Unet, features, snapshot_host
+from .denoiser import TILE, Unet, features, read_weights, snapshot_host
 from .gpu import Gpu, GpuArray
 from .tracer import PX_LEN, Tracer, camera
 
@@ -161,11 +161,22 @@ class DataSet:
         return {k: int((~torch.isfinite(getattr(self, k)[:self.n].float())).sum().item())
                 for k in ("feat", "irr", "alb", "ref")}
 
-    def batch(self, rng, B: int, crop: int):
-        """B random crops (random flips and transposes) as contiguous tensors."""
+    def weights(self, spp_bias: float) -> np.ndarray | None:
+        """Pair probabilities proportional to spp ** spp_bias (None: uniform).
+        The loss of a low-spp pair is many times that of a high-spp one, so
+        under uniform draws the few-sample images dominate the gradient; a
+        positive bias draws the many-sample images more often."""
+        if spp_bias == 0.0:
+            return None
+        w = self.spp[:self.n].astype(np.float64) ** spp_bias
+        return w / w.sum()
+
+    def batch(self, rng, B: int, crop: int, p: np.ndarray | None = None):
+        """B random crops (random flips and transposes) as contiguous tensors;
+        `p`: pair probabilities (``weights``), or None for uniform draws."""
         import torch
 
-        idx = rng.integers(0, self.n, B)
+        idx = rng.integers(0, self.n, B) if p is None else rng.choice(self.n, B, p=p)
         s = self.size
         outs = [[], [], [], []]
         for i in idx:
@@ -211,7 +222,11 @@ GROUP = 16  # scenes rendered together in one batch launch
 DROP_HALF = 0.15  # share of training pairs given no part-way snapshot
 
 
-def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, workers: int = 0):
+def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, workers: int = 0,
+               keep: bool = True):
+    """The data set of the scenes `indices`; with keep, also every scene's
+    reference radiance and noisy px images on the host (8.9 MB an image at
+    256 x 256: pass keep=False for large sets)."""
     indices = list(indices)
     ds = DataSet(gpu, len(indices) * len(segments), size)
     refs, noisy_all = [], []
@@ -223,6 +238,7 @@ def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, 
     group = []
 
     drop = np.random.default_rng(12345)
+    done = [0]
 
     def flush():
         noisy_g, halves_g, refs_g = render_group(gpu, group, segments, ref_spp)
@@ -232,10 +248,12 @@ def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, 
                 # some pairs go without the snapshot, so the network also
                 # serves callers that have none
                 ds.add(px, None if drop.random() < DROP_HALF else half, rr, spp)
-            refs.append(rr)
-            noisy_all.append(noisy)
+            if keep:
+                refs.append(rr)
+                noisy_all.append(noisy)
+        done[0] += len(group)
         group.clear()
-        log(f"rendered {len(refs)}/{len(indices)} scenes ({time.time() - t0:.1f} s)")
+        log(f"rendered {done[0]}/{len(indices)} scenes ({time.time() - t0:.1f} s)")
 
     for sc in scene_stream(indices, size, workers):
         group.append(sc)
@@ -247,17 +265,21 @@ def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, 
 
 
 def train(gpu: Gpu, ds: DataSet, steps: int, batch: int, crop: int, lr: float, seed: int = 1, log=print,
-          err_weight: float = 0.1) -> tuple[Unet, list]:
+          err_weight: float = 0.1, init: np.ndarray | None = None, spp_bias: float = 0.0) -> tuple[Unet, list]:
+    """Adam with a 200-step warm-up and a cosine decay; `init`: starting
+    parameters (fine-tuning), else the seeded initialisation; `spp_bias`:
+    see ``DataSet.weights``."""
     import torch
 
-    net = Unet(gpu, seed=seed)
+    net = Unet(gpu, seed=seed, params=init)
     rng = np.random.default_rng(seed)
+    p = ds.weights(spp_bias)
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
     hist, acc, t0 = [], 0, time.time()
     for step in range(steps):
         warm = min(1.0, (step + 1) / 200)
         rate = lr * warm * 0.5 * (1.0 + math.cos(math.pi * step / steps))
-        f, i, a, r = ds.batch(rng, batch, crop)
+        f, i, a, r = ds.batch(rng, batch, crop, p)
         net.train_step(f, i, a, r, batch, crop, crop, crop, crop, loss, rate, err_weight)
         acc += 1
         if (step + 1) % 100 == 0 or step + 1 == steps or (step < 100 and (step + 1) % 10 == 0):
@@ -307,6 +329,10 @@ def main(argv=None) -> None:
     ap.add_argument("--crop", type=int, default=128)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--first-scene", type=int, default=0, help="index of the first procedural scene")
+    ap.add_argument("--init", default="", help="weights to fine-tune from (.phxu)")
+    ap.add_argument("--spp-bias", type=float, default=0.0, help="draw pairs with probability ~ spp ** bias")
+    ap.add_argument("--eval-ref-spp", type=int, default=4096, help="samples of the held-out references")
     ap.add_argument("--out", default="")
     ap.add_argument("--report", default="")
     args = ap.parse_args(argv)
@@ -317,11 +343,14 @@ def main(argv=None) -> None:
     gpu.set_stream(torch.cuda.current_stream().cuda_stream)
     segments = [int(s) for s in args.segments.split(",")]
     t0 = time.time()
-    ds, _, _ = build_data(gpu, range(args.scenes), args.size, segments, args.ref_spp)
+    ds, _, _ = build_data(gpu, range(args.first_scene, args.first_scene + args.scenes), args.size, segments,
+                          args.ref_spp, keep=False)
     t_data = time.time() - t0
     print("non-finite values in the data set:", ds.nonfinite(), "in references (zeroed):", ds.bad)
     t0 = time.time()
-    net, hist = train(gpu, ds, args.steps, args.batch, args.crop, args.lr, args.seed)
+    init = read_weights(args.init) if args.init else None
+    net, hist = train(gpu, ds, args.steps, args.batch, args.crop, args.lr, args.seed, init=init,
+                      spp_bias=args.spp_bias)
     t_train = time.time() - t0
     if args.out:
         net.save(args.out)
@@ -329,12 +358,13 @@ def main(argv=None) -> None:
     rows = []
     for i in held:
         sc = scenes.procedural(i, width=args.size, height=args.size)
-        noisy, halves, refs = render_group(gpu, [sc], [4], args.ref_spp)
+        noisy, halves, refs = render_group(gpu, [sc], [4], args.eval_ref_spp)
         rows.append(evaluate(gpu, net, noisy[0][0], radiance(refs[0], args.size, args.size), args.size, args.size,
                              halves[0][0]))
     mean = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
-    report = {"scenes": args.scenes, "pairs": ds.n, "nonfinite_ref_values": ds.bad, "segments": segments, "ref_spp": args.ref_spp,
-              "steps": args.steps, "batch": args.batch, "crop": args.crop, "data_s": round(t_data, 1),
+    report = {"scenes": args.scenes, "first_scene": args.first_scene, "pairs": ds.n, "nonfinite_ref_values": ds.bad,
+              "segments": segments, "ref_spp": args.ref_spp, "eval_ref_spp": args.eval_ref_spp,
+              "init": args.init or None, "spp_bias": args.spp_bias, "lr": args.lr, "steps": args.steps, "batch": args.batch, "crop": args.crop, "data_s": round(t_data, 1),
               "train_s": round(t_train, 1), "loss": hist, "heldout_4spp_relmse": mean, "heldout_rows": rows}
     print(json.dumps({k: v for k, v in report.items() if k not in ("loss", "heldout_rows")}))
     if args.report:
