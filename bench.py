@@ -41,7 +41,7 @@ WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 6
 
 
 KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8", "megakernel/3", "megakernel/2",
-                "megakernel/sync", "megakernel/2/sync"]
+                "megakernel/sync", "megakernel/2/sync", "megakernel/5", "megakernel/6", "megakernel/6/sync"]
 
 
 def peaks() -> dict:
@@ -190,6 +190,8 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
     import torch
 
     if args.phase == "render":
+        if args.kernel >= 0:
+            tr.set_kernel(args.kernel)
         fn = lambda: tr.trace(cam, W, H, 0, args.spp)  # noqa: E731
     elif args.phase == "build":
         fn = lambda: tr.repose_device(verts_dev, rebuild=True)  # noqa: E731
@@ -433,7 +435,7 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     if not os.path.exists(WEIGHTS):
         return {"unavailable": f"no trained weights at {os.path.relpath(WEIGHTS, ROOT)}"}
     W, H, n = s.width, s.height, s.width * s.height
-    learned_spp = [1, 2, 4, 8, 16, 32, 64]
+    learned_spp = [1, 2, 4, 8, 16, 24, 32, 48, 64]
     plain_spp = [64, 128, 256, 512]
     tr = px.Tracer.of(gpu, s)
     net = Unet.pretrained(gpu)
@@ -448,31 +450,41 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     hbuf = px.GpuArray(gpu, n * 16)
     rel_plain, rel_learned, kept = {}, {}, {}
     tiles = ((W + TILE - 1) // TILE) * ((H + TILE - 1) // TILE)
-    for spp in learned_spp + plain_spp:
-        # traced in two halves: the first half's image is the learned
-        # denoiser's part-way snapshot (the plain method ignores it)
-        first = spp // 2
-        mid = None
-        if first > 0:
-            tr.trace(cam, W, H, frame, first)
-            mid = tr.image()
-        tr.trace(cam, W, H, frame + first, spp - first)
-        frame += spp
-        img = tr.image()
-        noisy = T.px_diff(img, prev, n)
-        half = None if mid is None else snapshot_host(T.px_diff(mid, prev, n), W, H)
-        prev = img
-        buf.write(noisy)
-        kernels.denoise(gpu, buf, W, H)
-        rel_plain[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
-        if spp in learned_spp:
+    # relMSE of one frame swings by ~10 % between sample sets (a few bright
+    # paths decide it): every figure is the mean over `relmse_frames`
+    # independent frames
+    for _ in range(args.relmse_frames):
+        for spp in learned_spp + plain_spp:
+            # traced in two halves: the first half's image is the learned
+            # denoiser's part-way snapshot (the plain method ignores it)
+            first = spp // 2
+            mid = None
+            if first > 0:
+                tr.trace(cam, W, H, frame, first)
+                mid = tr.image()
+            tr.trace(cam, W, H, frame + first, spp - first)
+            frame += spp
+            img = tr.image()
+            noisy = T.px_diff(img, prev, n)
+            half = None if mid is None else snapshot_host(T.px_diff(mid, prev, n), W, H)
+            prev = img
             buf.write(noisy)
-            if half is not None:
-                hbuf.write(half)
-            kept[spp] = net.denoise_px(buf, W, H, half=hbuf if half is not None else None, tile=TILE,
-                                       threshold=THRESHOLD, count=True) / tiles
-            rel_learned[spp] = T.relmse(T.radiance(buf.read(np.uint32), W, H), ref)
+            kernels.denoise(gpu, buf, W, H)
+            rel_plain.setdefault(spp, []).append(T.relmse(T.radiance(buf.read(np.uint32), W, H), ref))
+            if spp in learned_spp:
+                buf.write(noisy)
+                if half is not None:
+                    hbuf.write(half)
+                kept.setdefault(spp, []).append(
+                    net.denoise_px(buf, W, H, half=hbuf if half is not None else None, tile=TILE,
+                                   threshold=THRESHOLD, count=True) / tiles)
+                rel_learned.setdefault(spp, []).append(T.relmse(T.radiance(buf.read(np.uint32), W, H), ref))
     buf.free()
+    spread = {"plain": {str(k): [round(x, 6) for x in v] for k, v in rel_plain.items() if k == args.plain_spp},
+              "learned": {str(k): [round(x, 6) for x in v] for k, v in rel_learned.items() if k in (24, 32, 48)}}
+    rel_plain = {k: float(np.mean(v)) for k, v in rel_plain.items()}
+    rel_learned = {k: float(np.mean(v)) for k, v in rel_learned.items()}
+    kept = {k: float(np.mean(v)) for k, v in kept.items()}
 
     def frame_ms(spp, learned, reps):
         def once():
@@ -503,6 +515,8 @@ def equal_relmse(args, gpu, s, cam, stream) -> dict:
     match = next((p for p in learned_spp if rel_learned[p] <= target), None)
     out = {
         "reference_spp": args.ref_spp,
+        "frames": args.relmse_frames,
+        "relmse_per_frame": spread,
         "plain": {"spp": args.plain_spp, "relmse": round(target, 6), "frame_ms": round(t_plain, 3),
                   "frames_per_s": round(1000.0 / t_plain, 3)},
         "relmse_plain_denoise": {str(k): round(v, 6) for k, v in rel_plain.items()},
@@ -554,7 +568,11 @@ def main() -> None:
     ap.add_argument("--ref-spp", type=int, default=4096, help="samples of the equal-relMSE reference render")
     ap.add_argument("--plain-spp", type=int, default=256, help="samples of the plain tracer + Denoise")
     ap.add_argument("--no-denoised", action="store_true", help="skip the equal-relMSE comparison")
+    ap.add_argument("--relmse-frames", type=int, default=3,
+                    help="independent frames each equal-relMSE figure is averaged over")
     ap.add_argument("--walk", type=int, default=0, help="ray walk of --phase rays: 0 a thread per ray, 1 persistent")
+    ap.add_argument("--kernel", type=int, default=-1,
+                    help="render kernel id of --phase render (KERNEL_NAMES order; default: the tracer's default)")
     ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build", "nn"],
                     help="all: the benchmark; render/rays/build: only that kernel's launches (profiling runs)")
     args = ap.parse_args()

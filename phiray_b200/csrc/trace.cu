@@ -1582,6 +1582,15 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
     } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2) {
         if (stats) k_render<true, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_5) {
+        if (stats) k_render<true, 5><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 5><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_6) {
+        if (stats) k_render<true, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_6_SYNC) {
+        if (stats) k_render<true, 6, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 6, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
     } else {
         if (stats) k_render<true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
@@ -1701,7 +1710,7 @@ int32_t phx_tracer_destroy(phx_tracer tr) {
 
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (kernel > PHX_KERNEL_MEGAKERNEL_2_SYNC) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
+    if (kernel >= PHX_KERNEL_COUNT) return fail(PHX_ERR_INVALID, "unknown render kernel %u", kernel);
     tr->kernel = kernel;
     return PHX_OK;
 }
@@ -1716,7 +1725,7 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
     float best = 0.0f;
     uint32_t pick = PHX_KERNEL_STATE_MACHINE;
     const uint32_t keep = tr->kernel;
-    for (uint32_t k = 0; k <= PHX_KERNEL_MEGAKERNEL_2_SYNC; k++) {
+    for (uint32_t k = 0; k < PHX_KERNEL_COUNT; k++) {
         tr->kernel = k;
         PHX_TRY(launch_render(tr, cam, w, h, 0, spp ? spp : 1, 0, w * h));  // warm-up
         PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));

@@ -129,11 +129,15 @@ class Tracer:
     MEGAKERNEL_2 = 5
     MEGAKERNEL_SYNC = 6
     MEGAKERNEL_2_SYNC = 7
+    MEGAKERNEL_5 = 8
+    MEGAKERNEL_6 = 9
+    MEGAKERNEL_6_SYNC = 10
+    KERNELS = 11
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
         chosen = C.c_uint32()
-        ms = (C.c_float * 8)()
+        ms = (C.c_float * self.KERNELS)()
         N.check(N.lib().phx_tracer_autotune(self.handle, cam.ctypes.data, w, h, spp, C.byref(chosen), ms))
         self.w, self.h = w, h
         return chosen.value, list(ms)
