@@ -390,10 +390,18 @@ int32_t phx_tracer_destroy(phx_tracer tr);
  * each other after every sample, so samples start together. */
 #define PHX_KERNEL_MEGAKERNEL_SYNC 6u
 #define PHX_KERNEL_MEGAKERNEL_2_SYNC 7u
+/* The megakernel with a register budget for 5 or 6 resident blocks (more
+ * warps to hide the walk's load latency, more spills), and the 6-block form
+ * with the per-sample warp wait. */
+#define PHX_KERNEL_MEGAKERNEL_5 8u
+#define PHX_KERNEL_MEGAKERNEL_6 9u
+#define PHX_KERNEL_MEGAKERNEL_6_SYNC 10u
+/* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
+#define PHX_KERNEL_COUNT 11u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer
- * and returns its id; ms (8 floats, may be NULL) gets each one's time. The
+ * and returns its id; ms (PHX_KERNEL_COUNT floats, may be NULL) gets each one's time. The
  * image is overwritten (the next sample starts over). Waits. */
 int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
                             uint32_t* chosen, float* ms);
@@ -577,6 +585,14 @@ int32_t phx_unet_grads(phx_unet net, const void* feat, const float* irr, const f
                        int32_t Hp, int32_t Wp, int32_t h, int32_t w, float err_weight, float* loss);
 /* One Adam step (b1 0.9, b2 0.999, eps 1e-8) with the last gradients. */
 int32_t phx_unet_adam(phx_unet net, float lr);
+/* Every layer's gradients as one device array of *count fp32 (per layer the
+ * weight gradient [Kp][cout], Kp = 9 cin rounded up to 64, then the bias
+ * gradient [cout], each starting at a multiple of 64 floats; the padding is
+ * zero). Data-parallel training reduces this one array across ranks between
+ * phx_unet_grads and phx_unet_adam (an all-reduce average), so every rank
+ * takes the same Adam step. No reference counterpart: phiray trains no
+ * network. */
+int32_t phx_unet_grad_arena(phx_unet net, float** grads, uint64_t* count);
 /* phx_unet_grads then phx_unet_adam. */
 int32_t phx_unet_train_step(phx_unet net, const void* feat, const float* irr, const float* alb, const float* ref,
                             int32_t B, int32_t Hp, int32_t Wp, int32_t h, int32_t w, float err_weight, float lr,

@@ -120,6 +120,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_unet_adam": (i32, [vp, C.c_float]),
     "phx_unet_train_step": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, C.c_float, C.c_float, vp]),
     "phx_unet_logits": (i32, [vp, C.POINTER(vp)]),
+    "phx_unet_grad_arena": (i32, [vp, C.POINTER(vp), C.POINTER(C.c_uint64)]),
     "phx_unet_denoise_px": (i32, [vp, vp, vp, u32, u32, f32p, i32, C.c_float, i32, C.POINTER(u32)]),
     "phx_tracer_snapshot": (i32, [vp, vp]),
     "phx_tracer_denoise_learned": (i32, [vp, vp, vp, i32, C.c_float, i32, C.POINTER(u32)]),

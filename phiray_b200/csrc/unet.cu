@@ -43,8 +43,25 @@ int round64(int k) { return (k + 63) / 64 * 64; }
 
 struct Conv {
     int cin = 0, cout = 0, K = 0, Kp = 0, Kp2 = 0;
-    DevMem w32, wb, b32, mw, vw, mb, vb, gw, gb, w2;
+    DevMem w32, wb, b32, mw, vw, mb, vb, w2;
+    float* gw = nullptr;  // weight gradient [Kp][cout], in the network's gradient arena
+    float* gb = nullptr;  // bias gradient [cout], in the arena
 };
+
+// Offsets (in floats, each a multiple of 64) of every layer's weight and bias
+// gradients in one arena, so a data-parallel trainer reduces all gradients
+// with one collective; the arena's total length in floats.
+size_t grad_layout(size_t* off_w, size_t* off_b) {
+    size_t at = 0;
+    for (int i = 0; i < NL; i++) {
+        const size_t w = (size_t)COUT[i] * (size_t)((9 * CIN[i] + 63) / 64 * 64);
+        if (off_w) off_w[i] = at;
+        at += (w + 63) / 64 * 64;
+        if (off_b) off_b[i] = at;
+        at += ((size_t)COUT[i] + 63) / 64 * 64;
+    }
+    return at;
+}
 
 // A bf16 NHWC view: base, pixel pitch, channel offset.
 struct View {
@@ -65,6 +82,7 @@ struct phx_unet_s {
     phx_ctx handle = nullptr;
     phx::Ctx* ctx = nullptr;
     phx::Conv L[phx::NL];
+    phx::DevMem grads;  // every layer's weight and bias gradients (grad_layout)
     phx::DevMem zero_bias;
     phx::Shape shape;
     // activations
@@ -144,8 +162,8 @@ int32_t layer_bwd(phx_unet_s* n, int i, View x, View dy, View* dx, const Shape& 
     Conv& c = n->L[i];
     const int H = s.H >> level, W = s.W >> level;
     PHX_TRY(phx_nn_conv_wgrad(n->handle, x.p, x.pitch, x.off, c.cin, dy.p, dy.pitch, dy.off, c.cout,
-                              (float*)c.gw.ptr, c.Kp, s.B, H, W));
-    PHX_TRY(phx_nn_bias_grad(n->handle, dy.p, dy.pitch, dy.off, c.cout, s.B * H * W, (float*)c.gb.ptr));
+                              c.gw, c.Kp, s.B, H, W));
+    PHX_TRY(phx_nn_bias_grad(n->handle, dy.p, dy.pitch, dy.off, c.cout, s.B * H * W, c.gb));
     if (dx)
         PHX_TRY(conv(n, dy, c.cout, c.w2.ptr, c.Kp2, (const float*)n->zero_bias.ptr, *dx, c.cin, s, level, false,
                      false));
@@ -186,10 +204,7 @@ int32_t forward(phx_unet_s* n, const void* feat, const Shape& s, bool with_head 
 
 int32_t backward(phx_unet_s* n, const void* feat, const Shape& s) {
     cudaStream_t st = n->ctx->stream;
-    for (int i = 0; i < NL; i++) {
-        PHX_CUDA(cudaMemsetAsync(n->L[i].gw.ptr, 0, n->L[i].gw.bytes, st));
-        PHX_CUDA(cudaMemsetAsync(n->L[i].gb.ptr, 0, n->L[i].gb.bytes, st));
-    }
+    PHX_CUDA(cudaMemsetAsync(n->grads.ptr, 0, n->grads.bytes, st));
     // head
     View dy{n->dlogits.ptr, HEAD, 0};
     View dx = v(n->dDb[0], 32);
@@ -271,8 +286,8 @@ int32_t load(phx_unet_s* n, const float* blob) {
         PHX_CUDA(cudaMemsetAsync(c.mb.ptr, 0, c.mb.bytes, st));
         PHX_CUDA(cudaMemsetAsync(c.vb.ptr, 0, c.vb.bytes, st));
         // bf16 copy: an Adam step of rate 0 with a zero gradient
-        PHX_CUDA(cudaMemsetAsync(c.gw.ptr, 0, c.gw.bytes, st));
-        PHX_TRY(phx_nn_adam(n->handle, (float*)c.w32.ptr, (const float*)c.gw.ptr, (float*)c.mw.ptr, (float*)c.vw.ptr,
+        PHX_CUDA(cudaMemsetAsync(c.gw, 0, (size_t)c.cout * c.Kp * sizeof(float), st));
+        PHX_TRY(phx_nn_adam(n->handle, (float*)c.w32.ptr, c.gw, (float*)c.mw.ptr, (float*)c.vw.ptr,
                             c.wb.ptr, c.cout, c.Kp, c.K, 1, 0.0f, n->b1, n->b2, n->eps, 1));
     }
     n->step = 0;
@@ -340,10 +355,20 @@ int32_t phx_unet_create(phx_ctx ctx, uint64_t seed, phx_unet* out) {
         c.Kp2 = round64(9 * c.cout);
         const size_t W = (size_t)c.cout * c.Kp;
         if ((rc = c.w32.reserve(W * 4)) < 0 || (rc = c.wb.reserve(W * 2)) < 0 || (rc = c.mw.reserve(W * 4)) < 0 ||
-            (rc = c.vw.reserve(W * 4)) < 0 || (rc = c.gw.reserve(W * 4)) < 0 || (rc = c.b32.reserve(c.cout * 4)) < 0 ||
+            (rc = c.vw.reserve(W * 4)) < 0 || (rc = c.b32.reserve(c.cout * 4)) < 0 ||
             (rc = c.mb.reserve(c.cout * 4)) < 0 || (rc = c.vb.reserve(c.cout * 4)) < 0 ||
-            (rc = c.gb.reserve(c.cout * 4)) < 0 || (rc = c.w2.reserve((size_t)c.cin * c.Kp2 * 2)) < 0)
+            (rc = c.w2.reserve((size_t)c.cin * c.Kp2 * 2)) < 0)
             break;
+    }
+    if (rc == PHX_OK) {
+        size_t off_w[NL], off_b[NL];
+        const size_t total = grad_layout(off_w, off_b);
+        rc = n->grads.reserve(total * sizeof(float));
+        if (rc == PHX_OK) rc = cuda_check(cudaMemsetAsync(n->grads.ptr, 0, total * sizeof(float), ctx->c.stream), "grads");
+        for (int i = 0; i < NL && rc == PHX_OK; i++) {
+            n->L[i].gw = (float*)n->grads.ptr + off_w[i];
+            n->L[i].gb = (float*)n->grads.ptr + off_b[i];
+        }
     }
     if (rc == PHX_OK && (rc = n->zero_bias.reserve(288 * 4)) == PHX_OK)
         rc = cuda_check(cudaMemsetAsync(n->zero_bias.ptr, 0, 288 * 4, ctx->c.stream), "zero bias");
@@ -394,12 +419,12 @@ int32_t phx_unet_get(phx_unet net, int32_t which, float* dst, uint64_t count) {
     for (int i = 0; i < NL; i++) {
         Conv& c = net->L[i];
         std::vector<float> w((size_t)c.cout * c.Kp);
-        PHX_CUDA(cudaMemcpy(w.data(), which == 0 ? c.w32.ptr : c.gw.ptr, w.size() * 4, cudaMemcpyDeviceToHost));
+        PHX_CUDA(cudaMemcpy(w.data(), which == 0 ? c.w32.ptr : (const void*)c.gw, w.size() * 4, cudaMemcpyDeviceToHost));
         for (int r = 0; r < c.cout; r++)
             for (int k = 0; k < c.K; k++)
                 q[(size_t)r * c.K + k] = which == 0 ? w[(size_t)r * c.Kp + k] : w[(size_t)k * c.cout + r];
         q += (size_t)c.cout * c.K;
-        PHX_CUDA(cudaMemcpy(q, which == 0 ? c.b32.ptr : c.gb.ptr, c.cout * 4, cudaMemcpyDeviceToHost));
+        PHX_CUDA(cudaMemcpy(q, which == 0 ? c.b32.ptr : (const void*)c.gb, c.cout * 4, cudaMemcpyDeviceToHost));
         q += c.cout;
     }
     return PHX_OK;
@@ -444,9 +469,9 @@ int32_t phx_unet_adam(phx_unet net, float lr) {
     const int t = ++net->step;
     for (int i = 0; i < NL; i++) {
         Conv& c = net->L[i];
-        PHX_TRY(phx_nn_adam(net->handle, (float*)c.w32.ptr, (const float*)c.gw.ptr, (float*)c.mw.ptr,
+        PHX_TRY(phx_nn_adam(net->handle, (float*)c.w32.ptr, c.gw, (float*)c.mw.ptr,
                             (float*)c.vw.ptr, c.wb.ptr, c.cout, c.Kp, c.K, 1, lr, net->b1, net->b2, net->eps, t));
-        PHX_TRY(phx_nn_adam(net->handle, (float*)c.b32.ptr, (const float*)c.gb.ptr, (float*)c.mb.ptr,
+        PHX_TRY(phx_nn_adam(net->handle, (float*)c.b32.ptr, c.gb, (float*)c.mb.ptr,
                             (float*)c.vb.ptr, nullptr, 1, c.cout, c.cout, 0, lr, net->b1, net->b2, net->eps, t));
     }
     return flip_all(net);
@@ -457,6 +482,13 @@ int32_t phx_unet_train_step(phx_unet net, const void* feat, const float* irr, co
                             float* loss) {
     PHX_TRY(phx_unet_grads(net, feat, irr, alb, ref, B, Hp, Wp, h, w, err_weight, loss));
     return phx_unet_adam(net, lr);
+}
+
+int32_t phx_unet_grad_arena(phx_unet net, float** grads, uint64_t* count) {
+    if (!net || !grads || !count) return fail(PHX_ERR_INVALID, "null argument");
+    *grads = (float*)net->grads.ptr;
+    *count = grad_layout(nullptr, nullptr);
+    return PHX_OK;
 }
 
 int32_t phx_unet_logits(phx_unet net, float** logits) {

@@ -109,6 +109,24 @@ class Unet:
         N.check(N.lib().phx_unet_logits(self.handle, C.byref(p)))
         return p.value or 0
 
+    def grad_arena(self) -> tuple[int, int]:
+        """(device pointer, fp32 count) of the array holding every layer's
+        gradients (phx_unet_grad_arena): what data-parallel ranks reduce."""
+        p, c = C.c_void_p(), C.c_uint64()
+        N.check(N.lib().phx_unet_grad_arena(self.handle, C.byref(p), C.byref(c)))
+        return p.value or 0, c.value
+
+    def grad_tensor(self):
+        """The gradient arena as a torch fp32 tensor sharing its memory."""
+        import torch
+
+        ptr, count = self.grad_arena()
+
+        class _Arena:
+            __cuda_array_interface__ = {"shape": (count,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+        return torch.as_tensor(_Arena(), device=f"cuda:{self.gpu.ordinal}")
+
     def compute_grads(self, feat, irr, alb, ref, B, Hp, Wp, h, w, loss, err_weight: float = 0.1) -> None:
         N.check(N.lib().phx_unet_grads(self.handle, devptr(feat), devptr(irr), devptr(alb), devptr(ref), B, Hp, Wp,
                                        h, w, err_weight, devptr(loss)))

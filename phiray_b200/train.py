@@ -264,23 +264,64 @@ def build_data(gpu: Gpu, indices, size: int, segments, ref_spp: int, log=print, 
     return ds, refs, noisy_all
 
 
+def world() -> tuple[int, int]:
+    """(rank, world size) of the initialised process group, else (0, 1)."""
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(), dist.get_world_size()
+    return 0, 1
+
+
+def shard(indices, rank: int, size: int) -> list:
+    """The scenes one data-parallel rank renders: every size-th from its rank
+    (disjoint, together all of them)."""
+    return list(indices)[rank::size]
+
+
+def average_grads(t, size: int) -> None:
+    """In-place all-reduce average of a gradient tensor over the process
+    group: NCCL's AVG where the backend has it, else a sum and a division."""
+    import torch.distributed as dist
+
+    if size <= 1:
+        return
+    if dist.get_backend() == "nccl":
+        dist.all_reduce(t, op=dist.ReduceOp.AVG)
+    else:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        t.div_(size)
+
+
 def train(gpu: Gpu, ds: DataSet, steps: int, batch: int, crop: int, lr: float, seed: int = 1, log=print,
           err_weight: float = 0.1, init: np.ndarray | None = None, spp_bias: float = 0.0) -> tuple[Unet, list]:
     """Adam with a 200-step warm-up and a cosine decay; `init`: starting
     parameters (fine-tuning), else the seeded initialisation; `spp_bias`:
-    see ``DataSet.weights``."""
+    see ``DataSet.weights``. Under an initialised process group each rank
+    draws its crops from its own data set, and the gradient arena is
+    averaged across ranks before every Adam step: every rank holds the same
+    weights throughout (same start, same averaged gradients, same update)."""
     import torch
 
+    rank, size = world()
     net = Unet(gpu, seed=seed, params=init)
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(seed + 7919 * rank)
     p = ds.weights(spp_bias)
-    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device=f"cuda:{gpu.ordinal}")
+    arena = net.grad_tensor() if size > 1 else None
     hist, acc, t0 = [], 0, time.time()
     for step in range(steps):
         warm = min(1.0, (step + 1) / 200)
         rate = lr * warm * 0.5 * (1.0 + math.cos(math.pi * step / steps))
         f, i, a, r = ds.batch(rng, batch, crop, p)
-        net.train_step(f, i, a, r, batch, crop, crop, crop, crop, loss, rate, err_weight)
+        if arena is None:
+            net.train_step(f, i, a, r, batch, crop, crop, crop, crop, loss, rate, err_weight)
+        else:
+            # the network's stream is torch's current one, so the collective
+            # follows the gradients and the Adam step follows the collective
+            net.compute_grads(f, i, a, r, batch, crop, crop, crop, crop, loss, err_weight)
+            average_grads(arena, size)
+            net.adam(rate)
         acc += 1
         if (step + 1) % 100 == 0 or step + 1 == steps or (step < 100 and (step + 1) % 10 == 0):
             gpu.wait()
@@ -337,14 +378,29 @@ def main(argv=None) -> None:
     ap.add_argument("--report", default="")
     args = ap.parse_args(argv)
 
+    import os
+
     import torch
 
-    gpu = Gpu(0)
+    size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if size > 1:
+        # data parallel, one process per GPU (torchrun): each rank renders its
+        # share of the scenes; gradients are averaged over NCCL every step
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    rank, size = world()
+    gpu = Gpu(local)
     gpu.set_stream(torch.cuda.current_stream().cuda_stream)
     segments = [int(s) for s in args.segments.split(",")]
     t0 = time.time()
-    ds, _, _ = build_data(gpu, range(args.first_scene, args.first_scene + args.scenes), args.size, segments,
-                          args.ref_spp, keep=False)
+    mine = shard(range(args.first_scene, args.first_scene + args.scenes), rank, size)
+    ds, _, _ = build_data(gpu, mine, args.size, segments, args.ref_spp, keep=False,
+                          log=print if rank == 0 else (lambda *a: None))
     t_data = time.time() - t0
     print("non-finite values in the data set:", ds.nonfinite(), "in references (zeroed):", ds.bad)
     t0 = time.time()
@@ -352,6 +408,21 @@ def main(argv=None) -> None:
     net, hist = train(gpu, ds, args.steps, args.batch, args.crop, args.lr, args.seed, init=init,
                       spp_bias=args.spp_bias)
     t_train = time.time() - t0
+    lockstep = True
+    if size > 1:
+        # every rank must hold the same weights: compare a checksum of each
+        import torch.distributed as dist
+
+        mine_sum = torch.tensor([float(np.sum(net.params(), dtype=np.float64))], dtype=torch.float64,
+                                device=f"cuda:{local}")
+        sums = [torch.zeros_like(mine_sum) for _ in range(size)]
+        dist.all_gather(sums, mine_sum)
+        lockstep = all(float(x.item()) == float(sums[0].item()) for x in sums)
+        if rank != 0:
+            net.close()
+            gpu.close()
+            dist.destroy_process_group()
+            return
     if args.out:
         net.save(args.out)
     held = range(100000, 100000 + args.eval_scenes)
@@ -362,7 +433,8 @@ def main(argv=None) -> None:
         rows.append(evaluate(gpu, net, noisy[0][0], radiance(refs[0], args.size, args.size), args.size, args.size,
                              halves[0][0]))
     mean = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
-    report = {"scenes": args.scenes, "first_scene": args.first_scene, "pairs": ds.n, "nonfinite_ref_values": ds.bad,
+    report = {"scenes": args.scenes, "first_scene": args.first_scene, "ranks": size, "ranks_in_lockstep": lockstep,
+              "pairs_rank0": ds.n, "nonfinite_ref_values": ds.bad,
               "segments": segments, "ref_spp": args.ref_spp, "eval_ref_spp": args.eval_ref_spp,
               "init": args.init or None, "spp_bias": args.spp_bias, "lr": args.lr, "steps": args.steps, "batch": args.batch, "crop": args.crop, "data_s": round(t_data, 1),
               "train_s": round(t_train, 1), "loss": hist, "heldout_4spp_relmse": mean, "heldout_rows": rows}
@@ -372,6 +444,10 @@ def main(argv=None) -> None:
             json.dump(report, f, indent=1)
     net.close()
     gpu.close()
+    if size > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -59,3 +59,56 @@ def test_reference_arm_runs_on_rank_zero_only(capsys, monkeypatch):
     monkeypatch.setenv("WORLD_SIZE", "2")
     bench.reference_arm(argparse.Namespace(steps=1, warmup=0))
     assert capsys.readouterr().out == ""
+
+
+def _train_rank(rank: int, world: int, port: int, out) -> None:
+    """One data-parallel training rank on CPU: its own gradients, the
+    all-reduce average of phiray_b200.train, then the oracle's Adam step."""
+    import datetime
+    import sys
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), ".."))
+    from oracle import nn as O
+    from phiray_b200 import train as T
+
+    r, size = T.world()
+    rng = np.random.default_rng(100 + rank)
+    w = np.random.default_rng(5).standard_normal(257).astype(np.float32)  # same start on every rank
+    m = np.zeros_like(w)
+    v = np.zeros_like(w)
+    seen = []
+    for step in range(1, 4):
+        g_local = rng.standard_normal(257).astype(np.float32)  # this rank's own batch
+        t = torch.from_numpy(g_local.copy())
+        T.average_grads(t, size)
+        everyone = [torch.zeros(257) for _ in range(size)]
+        dist.all_gather(everyone, torch.from_numpy(g_local))
+        seen.append(float(np.abs(t.numpy() - np.mean([e.numpy() for e in everyone], axis=0)).max()))
+        w, m, v = O.adam(w, t.numpy(), m, v, 1e-3, step)
+    out.put((rank, r, size, T.shard(range(10), r, size), seen, float(np.sum(w, dtype=np.float64))))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_data_parallel_training_ranks_stay_in_lockstep():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_train_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, r0, s0, sh0, seen0, sum0), (_, r1, s1, sh1, seen1, sum1) = res
+    assert (r0, r1, s0, s1) == (0, 1, 2, 2)
+    assert sorted(sh0 + sh1) == list(range(10)) and not set(sh0) & set(sh1)  # disjoint scene shards
+    assert max(seen0 + seen1) < 1e-6  # the reduced gradient is the mean of the ranks' gradients
+    assert sum0 == sum1  # same start, same averaged gradient, same Adam: identical weights

@@ -560,3 +560,90 @@ def test_learned_denoise_fallback_tiles(gpu):
     assert np.array_equal(mixed[:n][~pm], plain[:n][~pm])
     net.close()
     tr.close()
+
+
+def test_unet_data_parallel_step_equals_one_batch(gpu):
+    """Data-parallel training emulated on one GPU: two networks with the same
+    weights take the gradients of two half batches, their gradient arenas are
+    averaged (what the NCCL all-reduce average does between ranks) and each
+    takes its Adam step. Both then hold identical weights, and the averaged
+    gradient equals the whole batch's gradient on one network up to fp32
+    summation order (the loss is a mean over the batch). The arena holds
+    exactly the gradients phx_unet_get reports, in its own layout."""
+    import torch
+
+    from phiray_b200.denoiser import Unet
+
+    rng = np.random.default_rng(31)
+    B, H, W = 4, 32, 32
+    feat, irr, alb, ref = _net_inputs(rng, B, H, W)
+    blob = _random_params(rng)
+    nets = [Unet(gpu, params=blob) for _ in range(3)]
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+
+    def inputs(sl):
+        return (_t(feat[sl], "bf16"), _t(irr[sl].astype(np.float32)), _t(alb[sl].astype(np.float32)),
+                _t(ref[sl].astype(np.float32)))
+
+    parts = [inputs(slice(0, 2)), inputs(slice(2, 4)), inputs(slice(0, 4))]
+    torch.cuda.synchronize()
+    for net, (F, I, A, R), b in zip(nets, parts, (2, 2, 4)):
+        net.compute_grads(F, I, A, R, b, H, W, H, W, loss, err_weight=0.1)
+    _sync(gpu)
+    arenas = [n.grad_tensor() for n in nets]
+    count = nets[0].grad_arena()[1]
+    assert all(a.numel() == count for a in arenas)
+
+    # the arena layout: per layer [Kp][cout] then [cout], each at a multiple of 64 floats
+    host = arenas[0].cpu().numpy()
+    want = nets[0].grads()
+    at, q = 0, 0
+    for cin, cout in nn.LAYERS:
+        K, Kp = 9 * cin, _round64(9 * cin)
+        gw = host[at:at + Kp * cout].reshape(Kp, cout)
+        assert np.array_equal(gw[:K].T.reshape(-1), want[q:q + cout * K])
+        assert not gw[K:].any()
+        q += cout * K
+        at += (Kp * cout + 63) // 64 * 64
+        assert np.array_equal(host[at:at + cout], want[q:q + cout])
+        q += cout
+        at += (cout + 63) // 64 * 64
+    assert at == count and q == want.size
+
+    avg = (arenas[0] + arenas[1]) / 2
+    whole = arenas[2]
+    assert float(torch.linalg.norm(avg - whole) / torch.linalg.norm(whole)) < 1e-3
+    arenas[0].copy_(avg)
+    arenas[1].copy_(avg)
+    torch.cuda.synchronize()
+    for net in nets[:2]:
+        net.adam(1e-3)
+    _sync(gpu)
+    p0, p1 = nets[0].params(), nets[1].params()
+    assert np.array_equal(p0, p1)
+    assert not np.array_equal(p0, blob)
+    for net in nets:
+        net.close()
+
+
+def test_shipped_weights_beat_the_atrous_denoise_on_held_out_scenes(gpu):
+    """The trained weights in the package on procedural scenes the training
+    never saw (indices 100000 and 100003): at 4 spp with the part-way
+    snapshot, the learned denoiser's relMSE against a 1024-spp reference is
+    well below the a-trous Denoise's, which is below the noisy image's."""
+    from phiray_b200 import scenes
+    from phiray_b200 import train as T
+    from phiray_b200.denoiser import Unet
+
+    net = Unet.pretrained(gpu)
+    scs = [scenes.procedural(i, width=256, height=256) for i in (100000, 100003)]
+    noisy, halves, refs = T.render_group(gpu, scs, [4], 1024)
+    ratios = []
+    for k in range(len(scs)):
+        r = T.evaluate(gpu, net, noisy[k][0], T.radiance(refs[k], 256, 256), 256, 256, halves[k][0])
+        print(scs[k].name if hasattr(scs[k], "name") else k, {q: round(v, 5) for q, v in r.items()})
+        assert r["learned"] < r["denoise"] < r["noisy"], r
+        assert r["fallback_0.1"] < r["denoise"], r
+        ratios.append(r["learned"] / r["denoise"])
+    assert np.mean(ratios) < 0.75, ratios
+    net.close()
