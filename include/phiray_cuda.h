@@ -390,14 +390,16 @@ int32_t phx_tracer_destroy(phx_tracer tr);
  * each other after every sample, so samples start together. */
 #define PHX_KERNEL_MEGAKERNEL_SYNC 6u
 #define PHX_KERNEL_MEGAKERNEL_2_SYNC 7u
-/* The megakernel with a register budget for 5 or 6 resident blocks (more
- * warps to hide the walk's load latency, more spills), and the 6-block form
- * with the per-sample warp wait. */
+/* The megakernel with a register budget for 5, 6 or 8 resident blocks (more
+ * warps to hide the walk's load latency, more spills), and the 6- and
+ * 8-block forms with the per-sample warp wait. */
 #define PHX_KERNEL_MEGAKERNEL_5 8u
 #define PHX_KERNEL_MEGAKERNEL_6 9u
 #define PHX_KERNEL_MEGAKERNEL_6_SYNC 10u
+#define PHX_KERNEL_MEGAKERNEL_8 11u
+#define PHX_KERNEL_MEGAKERNEL_8_SYNC 12u
 /* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
-#define PHX_KERNEL_COUNT 11u
+#define PHX_KERNEL_COUNT 13u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer

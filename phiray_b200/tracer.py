@@ -132,7 +132,9 @@ class Tracer:
     MEGAKERNEL_5 = 8
     MEGAKERNEL_6 = 9
     MEGAKERNEL_6_SYNC = 10
-    KERNELS = 11
+    MEGAKERNEL_8 = 11
+    MEGAKERNEL_8_SYNC = 12
+    KERNELS = 13
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
