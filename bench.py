@@ -569,7 +569,7 @@ def main() -> None:
     ap.add_argument("--ref-spp", type=int, default=4096, help="samples of the equal-relMSE reference render")
     ap.add_argument("--plain-spp", type=int, default=256, help="samples of the plain tracer + Denoise")
     ap.add_argument("--no-denoised", action="store_true", help="skip the equal-relMSE comparison")
-    ap.add_argument("--relmse-frames", type=int, default=3,
+    ap.add_argument("--relmse-frames", type=int, default=5,
                     help="independent frames each equal-relMSE figure is averaged over")
     ap.add_argument("--walk", type=int, default=0, help="ray walk of --phase rays: 0 a thread per ray, 1 persistent")
     ap.add_argument("--kernel", type=int, default=-1,

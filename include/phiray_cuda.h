@@ -554,6 +554,12 @@ int32_t phx_nn_adam(phx_ctx ctx, float* w, const float* g, float* m, float* v, v
  * from which the pixels' own sample spread is read. */
 int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, const float* half, int32_t w, int32_t h, int32_t Hp,
                         int32_t Wp, void* feat, float* irr, float* alb);
+/* The a-trous Denoise's first-round firefly clamp (denoise.wgsl:47-134) on B
+ * padded Hp x Wp images of fp32 x 3 irradiance, inside the h x w image: a
+ * pixel brighter in luma than 1.5 x its brightest 8-neighbour + 0.05 takes
+ * their mean. out must not alias irr. */
+int32_t phx_nn_firefly(phx_ctx ctx, const float* irr, float* out, int32_t B, int32_t Hp, int32_t Wp, int32_t h,
+                       int32_t w);
 /* A snapshot of a px image's linear sums and met-sample counts (w * h x 4
  * floats, device): the `half` input of phx_nn_features. */
 int32_t phx_nn_snapshot(phx_ctx ctx, const uint32_t* px, uint32_t w, uint32_t h, float* snap);
@@ -601,8 +607,12 @@ int32_t phx_unet_train_step(phx_unet net, const void* feat, const float* irr, co
                             float* loss);
 /* Device pointer of the last forward's head output ([B][Hp][Wp][32] fp32). */
 int32_t phx_unet_logits(phx_unet net, float** logits);
+/* Whether phx_unet_denoise_px's predicted kernels filter the irradiance
+ * after phx_nn_firefly (on) or as it is (0, the default). */
+int32_t phx_unet_set_clamp(phx_unet net, int32_t on);
 /* Denoises a traced px image in place (`half`: nullable snapshot, as
- * phx_nn_features): features, network, the a-trous
+ * phx_nn_features): features, network (its kernels filtering the
+ * firefly-clamped irradiance if phx_unet_set_clamp turned that on), the a-trous
  * Denoise (phx_denoise, strength 64/8/40/7), then the learned result on every
  * tile x tile block whose mean error estimate is <= threshold. With
  * `fallback` non-NULL, waits and returns the number of tiles that kept the

@@ -193,6 +193,41 @@ def features(px: np.ndarray, w: int, h: int, Hp: int, Wp: int, half: np.ndarray 
 
 # ---- the network ----
 
+def firefly(irr: np.ndarray, h: int, w: int) -> np.ndarray:
+    """The a-trous Denoise's first-round firefly clamp (denoise.wgsl:47-134,
+    its FIRST pass) on padded (B, Hp, Wp, 3) irradiance, in float32 with the
+    device's order of operations: inside the h x w image, a pixel whose luma
+    0.2126 r + 0.7152 g + 0.0722 b exceeds 1.5 x the brightest in-image
+    8-neighbour's + 0.05 takes the neighbours' mean (summed row by row);
+    other pixels are copied."""
+    x = np.asarray(irr, dtype=np.float32)
+    out = x.copy()
+    B = x.shape[0]
+    k = [np.float32(0.2126), np.float32(0.7152), np.float32(0.0722)]
+
+    def luma(v):
+        return (v[..., 0] * k[0] + v[..., 1] * k[1]) + v[..., 2] * k[2]
+
+    top = np.zeros((B, h, w), np.float32)
+    acc = np.zeros((B, h, w, 3), np.float32)
+    cnt = np.zeros((B, h, w), np.float32)
+    for dy in (-1, 0, 1):
+        for dx in (-1, 0, 1):
+            if dy == 0 and dx == 0:
+                continue
+            ys, xs = np.arange(h) + dy, np.arange(w) + dx
+            ok = ((ys >= 0) & (ys < h))[:, None] & ((xs >= 0) & (xs < w))[None, :]
+            nb = x[:, np.clip(ys, 0, h - 1)][:, :, np.clip(xs, 0, w - 1)]
+            top = np.where(ok, np.maximum(top, luma(nb)), top)
+            acc = np.where(ok[..., None], acc + nb, acc)
+            cnt = np.where(ok, cnt + np.float32(1.0), cnt)
+    centre = x[:, :h, :w]
+    hit = (cnt > 0) & (luma(centre) > np.float32(1.5) * top + np.float32(0.05))
+    mean = acc / np.maximum(cnt, np.float32(1.0))[..., None]
+    out[:, :h, :w] = np.where(hit[..., None], mean, centre)
+    return out
+
+
 def split_params(blob: np.ndarray):
     """Blob (per layer W (cout, 9 cin) then b (cout,)) -> [(W, b)]."""
     out, o = [], 0

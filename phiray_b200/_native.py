@@ -109,6 +109,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_nn_adam": (i32, [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, C.c_float, C.c_float, C.c_float, C.c_float, i32]),
     "phx_nn_features": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, vp, vp]),
     "phx_nn_snapshot": (i32, [vp, vp, u32, u32, vp]),
+    "phx_nn_firefly": (i32, [vp, vp, vp, i32, i32, i32, i32, i32]),
     "phx_nn_compose": (i32, [vp, vp, i32, i32, i32, vp, vp, i32, C.c_float, i32, C.c_float, C.c_float, vp, vp]),
     "phx_unet_create": (i32, [vp, u64, C.POINTER(vp)]),
     "phx_unet_destroy": (i32, [vp]),
@@ -121,6 +122,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_unet_train_step": (i32, [vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, C.c_float, C.c_float, vp]),
     "phx_unet_logits": (i32, [vp, C.POINTER(vp)]),
     "phx_unet_grad_arena": (i32, [vp, C.POINTER(vp), C.POINTER(C.c_uint64)]),
+    "phx_unet_set_clamp": (i32, [vp, i32]),
     "phx_unet_denoise_px": (i32, [vp, vp, vp, u32, u32, f32p, i32, C.c_float, i32, C.POINTER(u32)]),
     "phx_tracer_snapshot": (i32, [vp, vp]),
     "phx_tracer_denoise_learned": (i32, [vp, vp, vp, i32, C.c_float, i32, C.POINTER(u32)]),

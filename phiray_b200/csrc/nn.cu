@@ -934,6 +934,45 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
 __device__ __forceinline__ float finite_or_zero(float v) { return isfinite(v) ? v : 0.0f; }
 
 // Network inputs from a traced image (px planes, src/trace/read.rs:37-56).
+// The a-trous Denoise's first-round firefly clamp (denoise.wgsl:47-134, the
+// rule k_round<FIRST> applies) on B padded images of irradiance (fp32 x 3 a
+// pixel): a pixel inside the h x w image whose luma exceeds 1.5 x the
+// brightest of its in-image 8-neighbours + 0.05 takes those neighbours'
+// mean; every other pixel is copied. Luma and the mean are summed in the
+// order k_round sums them.
+__global__ void k_firefly(const float* __restrict__ irr, float* __restrict__ out, int B, int Hp, int Wp, int h,
+                          int w) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)B * Hp * Wp) return;
+    const int x = (int)(q % (size_t)Wp), y = (int)((q / (size_t)Wp) % (size_t)Hp);
+    const size_t img = q - (size_t)y * Wp - x;  // first pixel of this image
+    float r = __ldg(irr + 3 * q), g = __ldg(irr + 3 * q + 1), b = __ldg(irr + 3 * q + 2);
+    if (x < w && y < h) {
+        float top = 0.0f, sr = 0.0f, sg = 0.0f, sb = 0.0f, nn = 0.0f;
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dx = -1; dx <= 1; dx++) {
+                const int sx = x + dx, sy = y + dy;
+                if ((dx == 0 && dy == 0) || sx < 0 || sy < 0 || sx >= w || sy >= h) continue;
+                const float* c = irr + 3 * (img + (size_t)sy * Wp + sx);
+                const float cr = __ldg(c), cg = __ldg(c + 1), cb = __ldg(c + 2);
+                top = fmaxf(top, cr * 0.2126f + cg * 0.7152f + cb * 0.0722f);
+                sr += cr;
+                sg += cg;
+                sb += cb;
+                nn += 1.0f;
+            }
+        }
+        if (nn > 0.0f && r * 0.2126f + g * 0.7152f + b * 0.0722f > 1.5f * top + 0.05f) {
+            r = sr / nn;
+            g = sg / nn;
+            b = sb / nn;
+        }
+    }
+    out[3 * q] = r;
+    out[3 * q + 1] = g;
+    out[3 * q + 2] = b;
+}
+
 // Per pixel of the padded image (Hp x Wp; padding pixels all zero) 16 bf16
 // channels: log(1 + |irr_a - irr_b| / 2) 3, log(1 + irradiance) 3, albedo 3,
 // normal 3, depth / (1 + |depth|), the fraction of samples that met
@@ -1322,6 +1361,16 @@ int32_t phx_nn_features(phx_ctx ctx, const uint32_t* px, const float* half, int3
     k_features<<<(Hp * Wp + 255) / 256, 256, 0, ctx->c.stream>>>(px, (const float4*)half, w, h, Hp, Wp, (bf16*)feat,
                                                                  irr, alb);
     return cuda_check(cudaGetLastError(), "features");
+}
+
+int32_t phx_nn_firefly(phx_ctx ctx, const float* irr, float* out, int32_t B, int32_t Hp, int32_t Wp, int32_t h,
+                       int32_t w) {
+    if (!ctx || !irr || !out || irr == out || B <= 0 || h <= 0 || w <= 0 || Hp < h || Wp < w)
+        return fail(PHX_ERR_INVALID, "firefly arguments");
+    PHX_TRY(use(&ctx->c));
+    const size_t total = (size_t)B * Hp * Wp;
+    k_firefly<<<(unsigned)((total + 255) / 256), 256, 0, ctx->c.stream>>>(irr, out, B, Hp, Wp, h, w);
+    return cuda_check(cudaGetLastError(), "firefly");
 }
 
 int32_t phx_nn_snapshot(phx_ctx ctx, const uint32_t* px, uint32_t w, uint32_t h, float* snap) {

@@ -90,7 +90,8 @@ struct phx_unet_s {
     // gradients
     phx::DevMem dA[5], dcat[4], dpool[5], dB4, dDa[4], dDb[4], dlogits;
     // tracer-facing scratch
-    phx::DevMem feat, irr, alb, out, err, tile_err, fallback;
+    phx::DevMem feat, irr, irr_clamped, alb, out, err, tile_err, fallback;
+    bool clamp = false;  // firefly clamp on the irradiance the predicted kernels filter
     int step = 0;
     float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
 };
@@ -497,6 +498,12 @@ int32_t phx_unet_logits(phx_unet net, float** logits) {
     return PHX_OK;
 }
 
+int32_t phx_unet_set_clamp(phx_unet net, int32_t on) {
+    if (!net) return fail(PHX_ERR_INVALID, "null network");
+    net->clamp = on != 0;
+    return PHX_OK;
+}
+
 int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint32_t w, uint32_t h,
                             const float view[4], int32_t tile, float threshold, int32_t keep, uint32_t* fallback) {
     if (!net || !px || !view) return fail(PHX_ERR_INVALID, "null argument");
@@ -514,8 +521,19 @@ int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint3
     PHX_TRY(net->fallback.reserve(4));
     PHX_TRY(phx_nn_features(net->handle, px, half, (int)w, (int)h, Hp, Wp, net->feat.ptr, (float*)net->irr.ptr,
                             (float*)net->alb.ptr));
-    PHX_TRY(phx_unet_forward(net, net->feat.ptr, (const float*)net->irr.ptr, (const float*)net->alb.ptr, 1, Hp, Wp,
-                             (int)h, (int)w, (float*)net->out.ptr, (float*)net->err.ptr));
+    // With the clamp on, the network reads the features as they are and the
+    // kernels it predicts filter the irradiance after the a-trous firefly
+    // clamp (off by default: on the C2 frame at 24-40 spp it raised relMSE
+    // by about 1 %: the network already gives lone bright samples little
+    // weight, and the clamp also darkens true highlights).
+    const float* filtered = (const float*)net->irr.ptr;
+    if (net->clamp) {
+        PHX_TRY(net->irr_clamped.reserve(P * 12));
+        PHX_TRY(phx_nn_firefly(net->handle, filtered, (float*)net->irr_clamped.ptr, 1, Hp, Wp, (int)h, (int)w));
+        filtered = (const float*)net->irr_clamped.ptr;
+    }
+    PHX_TRY(phx_unet_forward(net, net->feat.ptr, filtered, (const float*)net->alb.ptr, 1, Hp, Wp, (int)h, (int)w,
+                             (float*)net->out.ptr, (float*)net->err.ptr));
     // The a-trous filter everywhere first; the learned result then replaces it
     // on every tile whose estimate is within the threshold.
     const float strength[4] = {64.0f, 8.0f, 40.0f, 7.0f};

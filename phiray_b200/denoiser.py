@@ -139,6 +139,11 @@ class Unet:
         N.check(N.lib().phx_unet_train_step(self.handle, devptr(feat), devptr(irr), devptr(alb), devptr(ref), B, Hp,
                                             Wp, h, w, err_weight, lr, devptr(loss)))
 
+    def set_clamp(self, on: bool) -> None:
+        """Whether the predicted kernels filter the firefly-clamped irradiance
+        or the irradiance as it is (the default; phx_unet_set_clamp)."""
+        N.check(N.lib().phx_unet_set_clamp(self.handle, 1 if on else 0))
+
     def denoise(self, tracer, half=None, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
                 count: bool = False) -> int | None:
         """Learned ``Tracer::denoise``; `half`: a snapshot (``Tracer.snapshot``)
@@ -175,6 +180,12 @@ def features(gpu: Gpu, px, w: int, h: int, Hp: int, Wp: int, feat, irr, alb, hal
     snapshot taken part way through its samples, or None."""
     N.check(N.lib().phx_nn_features(gpu.handle, devptr(px), devptr(half), w, h, Hp, Wp, devptr(feat), devptr(irr),
                                     devptr(alb)))
+
+
+def firefly(gpu: Gpu, irr, out, B: int, Hp: int, Wp: int, h: int, w: int) -> None:
+    """phx_nn_firefly: the a-trous Denoise's firefly clamp on padded fp32 x 3
+    irradiance planes."""
+    N.check(N.lib().phx_nn_firefly(gpu.handle, devptr(irr), devptr(out), B, Hp, Wp, h, w))
 
 
 def snapshot(gpu: Gpu, px, w: int, h: int, snap) -> None:

@@ -647,3 +647,75 @@ def test_shipped_weights_beat_the_atrous_denoise_on_held_out_scenes(gpu):
         ratios.append(r["learned"] / r["denoise"])
     assert np.mean(ratios) < 0.75, ratios
     net.close()
+
+
+def test_firefly_clamp_matches_the_oracle(gpu):
+    """phx_nn_firefly against the oracle's float32 restatement, bit for bit:
+    planted single-pixel fireflies (corners and edges included) take their
+    neighbours' mean, a pixel no brighter than its neighbours is kept, and
+    the padding outside the h x w image is copied."""
+    import torch
+
+    from phiray_b200.denoiser import firefly
+
+    rng = np.random.default_rng(9)
+    B, Hp, Wp, h, w = 2, 32, 48, 30, 45
+    irr = rng.gamma(1.0, size=(B, Hp, Wp, 3)).astype(np.float32)
+    for b, y, x in [(0, 0, 0), (0, 29, 44), (1, 15, 0), (1, 7, 22), (0, 12, 33)]:
+        irr[b, y, x] = 1000.0  # a firefly
+    irr[1, 20, 20] = irr[1, 19:22, 19:22].reshape(-1, 3).max(axis=0)  # no brighter than its neighbours
+    src = torch.from_numpy(irr).cuda()
+    dst = torch.full_like(src, -1.0)
+    torch.cuda.synchronize()
+    firefly(gpu, src, dst, B, Hp, Wp, h, w)
+    _sync(gpu)
+    got = dst.cpu().numpy()
+    want = nn.firefly(irr, h, w)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    changed = (got != irr).any(axis=-1)
+    assert changed[0, 0, 0] and changed[0, 29, 44] and changed[1, 15, 0] and changed[1, 7, 22]
+    assert not changed[1, 20, 20]
+    assert not changed[:, h:, :].any() and not changed[:, :, w:].any()
+
+
+def test_learned_denoise_with_the_clamp_filters_clamped_irradiance(gpu):
+    """With phx_unet_set_clamp on, the learned denoise equals the network run
+    on the features with its kernels applied to the firefly-clamped
+    irradiance (no tile falling back)."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+    from phiray_b200.denoiser import Unet, padded
+
+    s = scenes.c1_plain(ntris=4096, width=72, height=40, spp=4)
+    cam = px.camera(s)
+    w, h = s.width, s.height
+    tr = px.Tracer.of(gpu, s)
+    net = Unet(gpu, seed=3)
+    net.set_clamp(True)
+    tr.trace(cam, w, h, 0, 4)
+    noisy = tr.image()
+    Hp, Wp = padded(h), padded(w)
+    feat = torch.empty((Hp, Wp, 16), dtype=torch.bfloat16, device="cuda")
+    irr = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    alb = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    clamped = torch.empty_like(irr)
+    out = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    err = torch.empty((Hp, Wp), dtype=torch.float32, device="cuda")
+    pptr, _ = tr.device_image()
+    torch.cuda.synchronize()
+    px.denoiser.features(gpu, pptr, w, h, Hp, Wp, feat, irr, alb)
+    px.denoiser.firefly(gpu, irr, clamped, 1, Hp, Wp, h, w)
+    net.forward(feat, clamped, alb, 1, Hp, Wp, h, w, out, err)
+    _sync(gpu)
+    o = _np(out)
+    assert net.denoise(tr, tile=16, threshold=1e30, count=True) == 0
+    rad = tr.radiance()
+    n = w * h
+    cnt = np.maximum(noisy[31 * n:32 * n].astype(np.float64), 1)
+    gone = noisy.view(np.float32)[33 * n:34 * n]
+    live = (1.0 - gone / cnt > 0.5 / cnt).reshape(h, w)
+    assert np.allclose(rad[live], o[:h, :w][live], rtol=1e-6, atol=1e-7)
+    net.close()
+    tr.close()
