@@ -398,8 +398,12 @@ int32_t phx_tracer_destroy(phx_tracer tr);
 #define PHX_KERNEL_MEGAKERNEL_6_SYNC 10u
 #define PHX_KERNEL_MEGAKERNEL_8 11u
 #define PHX_KERNEL_MEGAKERNEL_8_SYNC 12u
+/* The same with the per-sample warp wait at 10 and 12 resident blocks (48
+ * and 40 registers a thread). */
+#define PHX_KERNEL_MEGAKERNEL_10_SYNC 13u
+#define PHX_KERNEL_MEGAKERNEL_12_SYNC 14u
 /* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
-#define PHX_KERNEL_COUNT 13u
+#define PHX_KERNEL_COUNT 15u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer

@@ -556,7 +556,8 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
 
 // MINB: resident 128-thread blocks per SM the register budget is set for
 // (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills;
-// 5: 96, 6: 80, 8: 64 — more warps to hide the walk's loads, more spills).
+// 5: 96, 6: 80, 8: 64, 10: 48, 12: 40 — more warps to hide the walk's
+// loads, more spills).
 template <bool STATS, int MINB = 4, bool SYNC = false>
 __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px,
                                                   uint32_t first, uint32_t count, unsigned long long* counters) {
@@ -1600,6 +1601,12 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
     } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_8_SYNC) {
         if (stats) k_render<true, 8, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false, 8, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_10_SYNC) {
+        if (stats) k_render<true, 10, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 10, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_12_SYNC) {
+        if (stats) k_render<true, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
     } else {
         if (stats) k_render<true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);

@@ -134,7 +134,9 @@ class Tracer:
     MEGAKERNEL_6_SYNC = 10
     MEGAKERNEL_8 = 11
     MEGAKERNEL_8_SYNC = 12
-    KERNELS = 13
+    MEGAKERNEL_10_SYNC = 13
+    MEGAKERNEL_12_SYNC = 14
+    KERNELS = 15
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
