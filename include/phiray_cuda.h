@@ -398,12 +398,13 @@ int32_t phx_tracer_destroy(phx_tracer tr);
 #define PHX_KERNEL_MEGAKERNEL_6_SYNC 10u
 #define PHX_KERNEL_MEGAKERNEL_8 11u
 #define PHX_KERNEL_MEGAKERNEL_8_SYNC 12u
-/* The same with the per-sample warp wait at 10 and 12 resident blocks (48
- * and 40 registers a thread). */
+/* The same with the per-sample warp wait at 10, 12 and 16 resident blocks
+ * (48, 40 and 32 registers a thread). */
 #define PHX_KERNEL_MEGAKERNEL_10_SYNC 13u
 #define PHX_KERNEL_MEGAKERNEL_12_SYNC 14u
+#define PHX_KERNEL_MEGAKERNEL_16_SYNC 15u
 /* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
-#define PHX_KERNEL_COUNT 15u
+#define PHX_KERNEL_COUNT 16u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer

@@ -556,8 +556,8 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
 
 // MINB: resident 128-thread blocks per SM the register budget is set for
 // (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills;
-// 5: 96, 6: 80, 8: 64, 10: 48, 12: 40 — more warps to hide the walk's
-// loads, more spills).
+// 5: 96, 6: 80, 8: 64, 10: 48, 12: 40, 16: 32 — more warps to hide the
+// walk's loads, more spills).
 template <bool STATS, int MINB = 4, bool SYNC = false>
 __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px,
                                                   uint32_t first, uint32_t count, unsigned long long* counters) {
@@ -588,10 +588,11 @@ struct Job {
     uint32_t npx;
 };
 
-// Registers are budgeted for 768 resident threads an SM (80 a thread), a
-// budget at which the single-scene megakernel runs faster than at 512.
+// Registers are budgeted for 1536 resident threads an SM (40 a thread): the
+// walk is latency-bound, and the single-scene megakernel runs fastest with
+// that many warps resident although it spills more.
 template <bool STATS, int THREADS>
-__global__ void __launch_bounds__(THREADS, 768 / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
+__global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
                                                                          uint32_t ntiles, uint32_t* next) {
     constexpr int WARPS = THREADS / 32;
     constexpr int WORDS = (int)(sizeof(Job) / 4);
@@ -1607,6 +1608,9 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
     } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_12_SYNC) {
         if (stats) k_render<true, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_16_SYNC) {
+        if (stats) k_render<true, 16, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
+        else k_render<false, 16, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
     } else {
         if (stats) k_render<true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
         else k_render<false><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);

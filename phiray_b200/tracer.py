@@ -136,7 +136,8 @@ class Tracer:
     MEGAKERNEL_8_SYNC = 12
     MEGAKERNEL_10_SYNC = 13
     MEGAKERNEL_12_SYNC = 14
-    KERNELS = 15
+    MEGAKERNEL_16_SYNC = 15
+    KERNELS = 16
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
