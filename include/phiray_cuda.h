@@ -443,6 +443,21 @@ int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint
  * into the image, each pixel's samples taken in order inside the kernel —
  * the same sums as spp calls of sample. Stream-ordered, no wait. */
 int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first, uint32_t spp);
+/* Tracer::set_adaptive (src/trace/mod.rs:235-240): Adaptive Sampling as
+ * [threshold, min samples, step, on], stamped on every frame this tracer
+ * traces in place of the camera's own adapt field (sample.rs:119). With it
+ * on, a frame's samples skip the pixels that have settled: at the end of a
+ * sample that is a step boundary past the minimum the convergence check of
+ * adapt.wgsl runs (full vs half image), then the dilation and the
+ * open-pixel list (gather.wgsl) the next samples trace. The image planes
+ * are phiray's (half image 26n, flags 29n/30n, list 32n, its length at 34n).
+ * A change of setting starts the next sample over. Adaptive frames run on
+ * the megakernel forms and whole (no pixel slices); batches refuse them. */
+int32_t phx_tracer_set_adaptive(phx_tracer tr, const float adapt[4]);
+/* Tracer::unconverged (src/trace/mod.rs:224-233): the number of pixels not
+ * yet settled after the last sample's tail; PHX_ERR_INVALID when adaptive
+ * sampling is off. Bounded wait. */
+int32_t phx_tracer_unconverged(phx_tracer tr, uint32_t* count, uint32_t timeout_ms);
 /* Tracer::pixels / radiance / ... (read.rs:241-327): `count` words of the
  * image buffer from word `offset` (plane p starts at p * w * h) into host
  * memory; bounded wait. */

@@ -11,6 +11,7 @@
 // (textures, procedural slots, environment images, depth of field, adaptive
 // sampling, the grid, film transparency, other pixel filters and view
 // transforms) must be off in the Camera.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -828,6 +829,15 @@ void emit(World& W, uint32_t i, V3 lin, V3 over_rgb, float over_a, float cover, 
     px[g + 1] = u_of(gs.y);
     px[g + 2] = u_of(gs.z);
     px[gc] = u_of(cov);
+    // util.wgsl:126-132: Adaptive Sampling's half image takes the odd
+    // samples at double weight.
+    if (W.p->adapt[3] != 0.0f && (W.frame & 1u)) {
+        const uint32_t x = 26 * N + 3 * i;
+        const V3 half = (keep ? v3(f_of(px[x]), f_of(px[x + 1]), f_of(px[x + 2])) : v3(0.0f)) + lin * 2.0f;
+        px[x] = u_of(half.x);
+        px[x + 1] = u_of(half.y);
+        px[x + 2] = u_of(half.z);
+    }
     const V3 shown = view_transform_of(l / fmaxw(k - gone, 1.0f), W.p->view) * (1.0f - cov / k) + gs / k;
     const uint32_t b = 4 * N + 3 * i;
     px[b] = u_of(shown.x);
@@ -875,6 +885,9 @@ void shade_main(World& W, uint32_t i) {
         px[29 * N + i] = 0u;
         px[30 * N + i] = 0u;
     }
+    // shade.wgsl:44-64: past frame 0 only the open pixels are traced (the
+    // list gather.wgsl built from the settled flags of the last tail).
+    if (p->adapt[3] != 0.0f && px[30 * N + i] != 0u) return;
     uint32_t seed = hash(i * 9781u + W.frame * 6271u + 1u);
     const CamRay cr = camera_ray(W, i, &seed);
     V3 o = cr.o, d = cr.d;
@@ -1068,9 +1081,72 @@ void* orc_scene_new(const float* verts, const uint32_t* faces, uint32_t nfaces, 
 
 void orc_scene_free(void* handle) { delete (OrcScene*)handle; }
 
+// adapt.wgsl and gather.wgsl: the tail after `sample` — the convergence
+// check at a step boundary past the minimum, the dilation over the four
+// neighbours, and the open-pixel list (pixel order) with its length at 34n.
+static void adapt_tail(const phx_camera* cam, uint32_t* px, uint32_t sample) {
+    const uint32_t w = cam->w, h = cam->h, n = w * h;
+    const uint32_t min_samples = cam->adapt[1] > 0.0f ? (uint32_t)cam->adapt[1] : 0u;
+    const uint32_t step = cam->adapt[2] >= 1.0f ? (uint32_t)cam->adapt[2] : 1u;
+    if (sample > min_samples && (sample & (step - 1u)) == step - 1u) {
+        for (uint32_t i = 0; i < n; i++) {
+            if (px[29 * n + i] != 0u) continue;
+            const uint32_t a = n + 3 * i, x = 26 * n + 3 * i;
+            const float fr = f_of(px[a]), fg = f_of(px[a + 1]), fb = f_of(px[a + 2]);
+            const float hr = f_of(px[x]), hg = f_of(px[x + 1]), hb = f_of(px[x + 2]);
+            const uint32_t taken = px[31 * n + i] > 1u ? px[31 * n + i] : 1u;
+            const float scale = 1.0f / (float)taken;
+            const float error_difference = (std::fabs(fr - hr) + std::fabs(fg - hg) + std::fabs(fb - hb)) * scale;
+            const float intensity = (fr + fg + fb) * scale;
+            const float error_normalize = intensity < 1.0f ? std::sqrt(intensity) : intensity;
+            const float error = error_difference / (0.0001f + error_normalize);
+            if (error < cam->adapt[0]) px[29 * n + i] = 1u;
+        }
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t x = i % w, y = i / w;
+        const uint32_t* f = px + 29 * (size_t)n;
+        uint32_t all = f[i];
+        if (x > 0u) all = std::min(all, f[i - 1]);
+        if (x + 1u < w) all = std::min(all, f[i + 1]);
+        if (y > 0u) all = std::min(all, f[i - w]);
+        if (y + 1u < h) all = std::min(all, f[i + w]);
+        px[30 * (size_t)n + i] = all;
+    }
+    uint32_t open = 0;
+    for (uint32_t i = 0; i < n; i++)
+        if (px[30 * (size_t)n + i] == 0u) px[32 * (size_t)n + open++] = i;
+    px[34 * (size_t)n] = open;
+}
+
 void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
                      uint64_t* rays_out, uint32_t row0, uint32_t rows) {
     const OrcScene* h = (const OrcScene*)handle;
+    if (cam->adapt[3] != 0.0f) {
+        // Adaptive Sampling couples neighbouring pixels between samples:
+        // whole frames, sample by sample, each followed by its tail.
+        const Shared& S = h->S;
+        const uint32_t n = cam->w * cam->h;
+        uint64_t total = 0;
+        for (uint32_t f = first; f < first + spp; f++) {
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+            for (int64_t i = 0; i < (int64_t)n; i++) {
+                World W = h->W0;
+                W.p = cam;
+                W.n = n;
+                W.px = px;
+                W.ao = cam->ao > 0.0f ? cam->ao : S.extent * 0.08f;
+                W.eps = S.extent * 1e-5f;
+                W.rays = 0;
+                W.frame = f;
+                shade_main(W, (uint32_t)i);
+                total += W.rays;
+            }
+            adapt_tail(cam, px, f);
+        }
+        if (rays_out) *rays_out = total;
+        return;
+    }
     const Shared& S = h->S;
     const uint32_t w = cam->w, hh = cam->h;
     const uint32_t n = w * hh;

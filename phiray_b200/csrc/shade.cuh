@@ -88,6 +88,12 @@ struct Frame {
     float sky[4];
     float limit_d, limit_i, exposure, gamma;
     const phx_light* __restrict__ lights;
+    // Adaptive Sampling (util.wgsl:61-99): on, the convergence threshold,
+    // the minimum samples and the step; `list`: this launch traces the
+    // open-pixel list (px word 32n + k, its length at 34n) instead of
+    // pixel k.
+    uint32_t adapt_on, adapt_min, adapt_step, adapt_list;
+    float adapt_thr;
 };
 
 // ---- util.wgsl ----

@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(1024) k_lamps(const float4* __restrict__ tris,
 
 struct Sums {
     f3 lin, grid, alb, nrm;
+    f3 half;  // Adaptive Sampling's half image: every odd sample at double weight
     float cov, film, gone, dep;
     uint32_t count, outline;
 };
@@ -356,6 +357,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                 acc.count += 1u;
                 acc.film += 1.0f;
                 acc.lin += mk(0.0f);
+                if (F.adapt_on && (frame & 1u)) acc.half = acc.half + mk(0.0f) * 2.0f;
                 acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
                 acc.cov += 1.0f;
                 return;
@@ -466,6 +468,8 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
     acc.count += 1u;
     acc.film += 1.0f;
     acc.lin += col;
+    // the half image takes the odd samples at double weight (util.wgsl:126-132)
+    if (F.adapt_on && (frame & 1u)) acc.half = acc.half + col * 2.0f;
     acc.grid += mk(0.0f);
     acc.cov += 0.0f;
 }
@@ -516,6 +520,10 @@ __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun
         px[29 * n + i] = 0u;
         px[30 * n + i] = 0u;
     }
+    // The half image is read whatever the frame: the first odd sample adds
+    // to what the plane holds, as util.wgsl's emit does (`keep` is true
+    // from frame 1 on, and frame 0 never writes the plane).
+    if (F.adapt_on) ld3(px, 26 * n, i, acc.half);
     acc.outline = 0;
     for (uint32_t s = 0; s < F.spp; s++) {
         sample<STATS>(S, F, i, F.frame0 + s, sun, acc, cnt);
@@ -531,6 +539,7 @@ __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun
     px[13 * n + i] = __float_as_uint(acc.dep);
     px[31 * n + i] = acc.count;
     px[25 * n + i] = acc.outline;
+    if (F.adapt_on) st3(px, 26 * n, i, acc.half);
     const float kk = (float)acc.count;
     const f3 shown = view_transform_std(acc.lin / fmaxf(kk - acc.gone, 1.0f), F.exposure, F.gamma) *
                          (1.0f - acc.cov / kk) +
@@ -564,8 +573,70 @@ __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, 
     setup(S, F);
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt{0, 0, 0};
-    if (k < count) render_px<STATS, SYNC>(S, F, sun, px, first + k, cnt);
+    if (F.adapt_list) {
+        // shade.wgsl:44-50: thread k takes the k-th pixel still open
+        if (k < px[34u * F.n]) render_px<STATS, SYNC>(S, F, sun, px, px[32u * F.n + k], cnt);
+    } else if (k < count) {
+        render_px<STATS, SYNC>(S, F, sun, px, first + k, cnt);
+    }
     flush_counts<STATS>(cnt, counters);
+}
+
+// ---- Adaptive Sampling (adapt.wgsl, gather.wgsl) ----
+
+// adapt.wgsl's main: Cycles' convergence check at the end of `sample`, a
+// step boundary past the minimum. The full and half images estimate the
+// same mean; their disagreement scaled by the pixel's own sample count and
+// normalised by its intensity (by its square root below 1) is the error.
+__global__ void k_adapt_check(uint32_t* __restrict__ px, uint32_t n, float thr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || px[29u * n + i] != 0u) return;
+    const uint32_t a = n + 3u * i, x = 26u * n + 3u * i;
+    const f3 full = mk(__uint_as_float(px[a]), __uint_as_float(px[a + 1u]), __uint_as_float(px[a + 2u]));
+    const f3 half = mk(__uint_as_float(px[x]), __uint_as_float(px[x + 1u]), __uint_as_float(px[x + 2u]));
+    const uint32_t taken = max(px[31u * n + i], 1u);
+    const float scale = 1.0f / (float)taken;
+    const f3 d = mk(fabsf(full.x - half.x), fabsf(full.y - half.y), fabsf(full.z - half.z));
+    const float error_difference = (d.x + d.y + d.z) * scale;
+    const float intensity = (full.x + full.y + full.z) * scale;
+    const float error_normalize = intensity < 1.0f ? sqrtf(intensity) : intensity;
+    const float error = error_difference / (0.0001f + error_normalize);
+    if (error < thr) px[29u * n + i] = 1u;
+}
+
+// adapt.wgsl's dilate: a pixel counts as settled only when it and its four
+// neighbours are; the flag the tracer obeys.
+__global__ void k_adapt_dilate(uint32_t* __restrict__ px, uint32_t w, uint32_t h) {
+    const uint32_t n = w * h, i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t x = i % w, y = i / w;
+    const uint32_t* f = px + 29u * n;
+    uint32_t all = f[i];
+    if (x > 0u) all = min(all, f[i - 1u]);
+    if (x + 1u < w) all = min(all, f[i + 1u]);
+    if (y > 0u) all = min(all, f[i - w]);
+    if (y + 1u < h) all = min(all, f[i + w]);
+    px[30u * n + i] = all;
+}
+
+// gather.wgsl: the list of pixels not settled, each block appending its
+// open pixels as one run in the order they lie (the list's order decides
+// only which thread traces which pixel, never a result).
+__global__ void __launch_bounds__(256) k_adapt_gather(uint32_t* __restrict__ px, uint32_t n) {
+    __shared__ uint32_t held, run;
+    if (threadIdx.x == 0) held = 0u;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool open = i < n && px[30u * n + i] == 0u;
+    const unsigned ballot = __ballot_sync(0xffffffffu, open);
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0 && ballot) base = atomicAdd(&held, (uint32_t)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) run = atomicAdd(px + 34u * n, held);
+    __syncthreads();
+    if (open) px[32u * n + run + base + __popc(ballot & ((1u << lane) - 1u))] = i;
 }
 
 // ---- many scenes in one persistent launch ----
@@ -1430,6 +1501,10 @@ struct phx_tracer_s {
     uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, persistent warps, sorted first
     DevMem rkeys, rsorted, rorder, ralt_k, ralt_v, rzero;  // the sorted walk's keys and radix-sort scratch
     bool have_last = false;
+    // Adaptive Sampling, [threshold, min samples, step, on] (Tracer::adapt,
+    // set_adaptive): every frame this tracer traces takes it in place of the
+    // camera's own (sample.rs:119, `cam.adapt = self.adapt`).
+    float adapt[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     phx_camera last;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -1484,7 +1559,6 @@ int32_t check_camera(const phx_camera* c) {
     if (c->aperture > 0.0f) return fail(PHX_ERR_INVALID, "depth of field (aperture > 0) is not supported");
     if (c->grid > 0.0f) return fail(PHX_ERR_INVALID, "the grid overlay is not supported");
     if (c->film[0] != 0 || c->film[1] != 0) return fail(PHX_ERR_INVALID, "film transparency/world is not supported");
-    if (c->adapt[3] != 0.0f) return fail(PHX_ERR_INVALID, "adaptive sampling is not supported");
     if (c->depth[0] != 0) return fail(PHX_ERR_INVALID, "Max Bounces rows (depth) are not supported");
     if (c->integrator[0] != 0.0f) return fail(PHX_ERR_INVALID, "pixel filters other than phiray's own are not supported");
     if (c->view[0] != 0.0f) return fail(PHX_ERR_INVALID, "only the Standard view transform is supported");
@@ -1524,6 +1598,13 @@ Frame frame_of(const phx_camera* c, uint32_t w, uint32_t h, const phx_light* dev
     F.exposure = c->view[1];
     F.gamma = c->view[2];
     F.lights = dev_lights;
+    // sample.rs:119 passes the resolved Adaptive Sampling setting through;
+    // adapt.wgsl reads min and step as u32(adapt.y), max(u32(adapt.z), 1).
+    F.adapt_on = c->adapt[3] != 0.0f ? 1u : 0u;
+    F.adapt_thr = c->adapt[0];
+    F.adapt_min = c->adapt[1] > 0.0f ? (uint32_t)c->adapt[1] : 0u;
+    F.adapt_step = c->adapt[2] >= 1.0f ? (uint32_t)c->adapt[2] : 1u;
+    F.adapt_list = 0u;
     return F;
 }
 
@@ -1548,6 +1629,17 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
 int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, uint32_t count_px, bool stats) {
     Ctx* c = tr->ctx;
     const Scene S = scene_of(tr);
+    // Adaptive Sampling runs on the megakernel forms (the state machine
+    // fetches pixels by index, not from the open list); they all compute
+    // the same image, so an adaptive frame takes the default form instead.
+    const uint32_t keep_kernel = tr->kernel;
+    if (F.adapt_on && tr->kernel >= PHX_KERNEL_STATE_MACHINE && tr->kernel <= PHX_KERNEL_STATE_MACHINE_8)
+        tr->kernel = PHX_KERNEL_MEGAKERNEL;
+    struct Restore {
+        phx_tracer t;
+        uint32_t k;
+        ~Restore() { t->kernel = k; }
+    } restore{tr, keep_kernel};
     if (tr->kernel >= PHX_KERNEL_STATE_MACHINE && tr->kernel <= PHX_KERNEL_STATE_MACHINE_8) {
         // state machine, at 4, 6 or 8 resident blocks of 128 per SM
         const int minb = tr->kernel == 1u ? 4 : (tr->kernel == 2u ? 6 : 8);
@@ -1626,11 +1718,56 @@ Frame frame_for(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, ui
     return F;
 }
 
+// Adaptive Sampling's tail after a sample (sample.rs `BTail::Adapt`):
+// the convergence check when `sample` is a step boundary past the minimum
+// (adapt.wgsl's need_filter), then the dilation and the open-pixel list.
+bool adapt_boundary(const Frame& F, uint32_t sample) {
+    return sample > F.adapt_min && (sample & (F.adapt_step - 1u)) == F.adapt_step - 1u;
+}
+
+int32_t adapt_tail(phx_tracer tr, const Frame& F, bool check, uint32_t sample) {
+    cudaStream_t s = tr->ctx->stream;
+    uint32_t* px = (uint32_t*)tr->px.ptr;
+    const uint32_t blocks = (F.n + 255) / 256;
+    if (check && adapt_boundary(F, sample)) k_adapt_check<<<blocks, 256, 0, s>>>(px, F.n, F.adapt_thr);
+    k_adapt_dilate<<<blocks, 256, 0, s>>>(px, F.w, F.h);
+    PHX_CUDA(cudaMemsetAsync(px + 34ull * F.n, 0, 4, s));
+    k_adapt_gather<<<blocks, 256, 0, s>>>(px, F.n);
+    return cuda_check(cudaGetLastError(), "adaptive sampling tail");
+}
+
 int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first_frame, uint32_t spp,
                       uint32_t first_px, uint32_t count_px, bool stats = false) {
+    phx_camera view = *cam;
+    std::memcpy(view.adapt, tr->adapt, sizeof view.adapt);
+    cam = &view;
+    // pageable source: the copy is staged before the call returns
     PHX_CUDA(cudaMemcpyAsync(tr->cam.ptr, cam, sizeof(phx_camera), cudaMemcpyHostToDevice, tr->ctx->stream));
     const Frame F = frame_for(tr, cam, w, h, first_frame, spp);
-    return launch_frame(tr, F, mk(cam->sun[0], cam->sun[1], cam->sun[2]), first_px, count_px, stats);
+    const f3 sun = mk(cam->sun[0], cam->sun[1], cam->sun[2]);
+    if (!F.adapt_on) return launch_frame(tr, F, sun, first_px, count_px, stats);
+    if (first_px != 0 || count_px != F.n)
+        return fail(PHX_ERR_INVALID, "adaptive sampling traces whole frames (no pixel slices)");
+    // The samples run in launches that end at step boundaries: between two
+    // boundaries no pixel's flag changes, so every sample of a launch traces
+    // the same open pixels (the reference re-gathers after every sample and
+    // gets the same list). Past frame 0 a launch starts from the open list,
+    // which is rebuilt first from the flags as they stand.
+    uint32_t f = first_frame;
+    const uint32_t end = first_frame + spp;
+    if (f > 0) PHX_TRY(adapt_tail(tr, F, false, 0));
+    while (f < end) {
+        uint32_t e = f;
+        while (e + 1 < end && !adapt_boundary(F, e)) e++;
+        Frame G = F;
+        G.frame0 = f;
+        G.spp = e - f + 1;
+        G.adapt_list = f > 0 ? 1u : 0u;
+        PHX_TRY(launch_frame(tr, G, sun, 0, F.n, stats));
+        PHX_TRY(adapt_tail(tr, F, true, e));
+        f = e + 1;
+    }
+    return PHX_OK;
 }
 
 }  // namespace
@@ -1800,6 +1937,7 @@ int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint3
     PHX_CUDA(cudaEventRecord(tr->ev1, c->stream));
     tr->frame = first + spp - 1;
     tr->last = *cam;
+    std::memcpy(tr->last.adapt, tr->adapt, sizeof tr->adapt);
     tr->have_last = true;
     return PHX_OK;
 }
@@ -1814,8 +1952,13 @@ int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint
     PHX_TRY(ensure_image(tr, w, h));
     const uint32_t n = w * h;
     slices = slices < 1 ? 1 : (slices > n ? n : slices);
-    // sample.rs:126-134: the same view (everything past n, groups_x) is the
-    // next frame; another view starts over.
+    if (tr->adapt[3] != 0.0f) slices = 1;  // an adaptive sample traces the open list whole
+    // sample.rs:119-134: the tracer's Adaptive Sampling setting stamped on
+    // the view; the same view (everything past n, groups_x) is the next
+    // frame, another view starts over.
+    phx_camera view = *cam;
+    std::memcpy(view.adapt, tr->adapt, sizeof view.adapt);
+    cam = &view;
     const bool same = tr->have_last && memcmp((const char*)&tr->last + 8, (const char*)cam + 8, sizeof(phx_camera) - 8) == 0;
     if (same && tr->frame + 1 >= tr->target) {
         if (frame) *frame = tr->frame;
@@ -1844,6 +1987,26 @@ int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint
     if (frame) *frame = f;
     if (done) *done = (f + 1 >= tr->target) ? 1 : 0;
     return PHX_OK;
+}
+
+int32_t phx_tracer_set_adaptive(phx_tracer tr, const float adapt[4]) {
+    if (!tr || !adapt) return fail(PHX_ERR_INVALID, "null argument");
+    if (std::memcmp(tr->adapt, adapt, sizeof tr->adapt) != 0) {
+        std::memcpy(tr->adapt, adapt, sizeof tr->adapt);
+        tr->have_last = false;  // another setting is another view: the next sample starts over
+    }
+    return PHX_OK;
+}
+
+int32_t phx_tracer_unconverged(phx_tracer tr, uint32_t* count, uint32_t timeout_ms) {
+    if (!tr || !count) return fail(PHX_ERR_INVALID, "null argument");
+    if (tr->adapt[3] == 0.0f) return fail(PHX_ERR_INVALID, "adaptive sampling is off");
+    if (!tr->px.ptr) return fail(PHX_ERR_INVALID, "nothing traced yet");
+    PHX_TRY(use(tr->ctx));
+    const uint64_t n = (uint64_t)tr->w * tr->h;
+    PHX_CUDA(cudaMemcpyAsync(count, (const uint32_t*)tr->px.ptr + 34 * n, 4, cudaMemcpyDeviceToHost, tr->ctx->stream));
+    PHX_TRY(wait_stream(tr->ctx->stream, timeout_ms));
+    return read_status(tr->ctx);
 }
 
 int32_t phx_tracer_read(phx_tracer tr, uint64_t offset, uint32_t* dst, uint64_t count, uint32_t timeout_ms) {
@@ -2029,6 +2192,7 @@ int32_t phx_tracer_trace_stats(phx_tracer tr, const phx_camera* cam, uint32_t w,
     PHX_TRY(wait_stream(s, 0));
     tr->frame = first + spp - 1;
     tr->last = *cam;
+    std::memcpy(tr->last.adapt, tr->adapt, sizeof tr->adapt);
     tr->have_last = true;
     return read_status(tr->ctx);
 }
@@ -2240,8 +2404,11 @@ int32_t phx_batch_add(phx_batch b, phx_tracer tr, const phx_camera* cam, uint32_
     for (const BatchJob& bj : b->jobs)
         if (bj.tr == tr) return fail(PHX_ERR_INVALID, "a tracer can hold one job of a batch");
     PHX_TRY(check_camera(cam));
+    if (tr->adapt[3] != 0.0f)
+        return fail(PHX_ERR_INVALID, "adaptive sampling runs on single-scene traces (phx_tracer_trace/sample)");
     batch_drop_graph(b);
     b->jobs.push_back(BatchJob{tr, *cam, w, h, first, spp});
+    std::memset(b->jobs.back().cam.adapt, 0, sizeof b->jobs.back().cam.adapt);  // the tracer's setting rules
     if (index) *index = (uint32_t)(b->jobs.size() - 1);
     return PHX_OK;
 }

@@ -169,6 +169,21 @@ class Tracer:
     def set_samples(self, n: int) -> None:
         N.check(N.lib().phx_tracer_set_samples(self.handle, n))
 
+    def set_adaptive(self, adapt) -> None:
+        """``Tracer::set_adaptive``: [threshold, min samples, step, on]."""
+        a = (C.c_float * 4)(*[float(v) for v in adapt])
+        N.check(N.lib().phx_tracer_set_adaptive(self.handle, a))
+
+    def unconverged(self, timeout_ms: int = 0) -> int | None:
+        """``Tracer::unconverged``: pixels not settled after the last sample,
+        or None when adaptive sampling is off."""
+        c = C.c_uint32()
+        rc = N.lib().phx_tracer_unconverged(self.handle, C.byref(c), timeout_ms)
+        if rc == N.PHX_ERR_INVALID:
+            return None
+        N.check(rc)
+        return c.value
+
     def sample(self, cam: np.ndarray, w: int, h: int, slices: int = 1, cancel=None) -> tuple[int, bool]:
         """``Tracer::sample`` / ``sample_in``: (frame, done)."""
         frame, done = C.c_uint32(), C.c_int32()

@@ -196,3 +196,60 @@ def test_refit_after_repose_matches_a_fresh_tracer(gpu):
     f = px.Tracer.of(gpu, s2)
     f.trace(cam, s.width, s.height, 0, 2)
     assert np.array_equal(t.image(), f.image())
+
+
+ADAPT = [0.03, 4.0, 4.0, 1.0]  # Adaptive Sampling: threshold, min samples, step, on
+
+
+def _check_adaptive(got, want, n):
+    # every plane bit for bit but the open list, whose order is the GPU's;
+    # the list as a set, and its length
+    assert np.array_equal(got[:32 * n], want[:32 * n])
+    assert np.array_equal(got[33 * n:34 * n], want[33 * n:34 * n])
+    m = int(want[34 * n])
+    assert int(got[34 * n]) == m and 0 < m < n
+    assert np.array_equal(np.sort(got[32 * n:32 * n + m]), want[32 * n:32 * n + m])
+    return m
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 12, 15], ids=["megakernel", "state_machine", "mk8_sync", "mk16_sync"])
+def test_adaptive_sampling_matches_oracle(gpu, orc, kernel):
+    """Adaptive Sampling (set_adaptive): the samples of one frame over two
+    calls, settled pixels skipped through the open list, the convergence
+    check and dilation at each step boundary — the image equals the
+    oracle's, which runs the reference's per-sample tail, bit for bit."""
+    s = scenes.c1_plain(ntris=2048, width=48, height=32, spp=4)
+    w, h = s.width, s.height
+    n = w * h
+    cam = cam_of(s, w, h)
+    ocam = cam.copy()
+    ocam["adapt"] = ADAPT
+    want, _ = oracle_lib.TraceOracle(orc, s).trace(ocam, 0, 32)
+    tr = px.Tracer.of(gpu, s)
+    tr.set_kernel(kernel)
+    assert tr.unconverged() is None  # off
+    tr.set_adaptive(ADAPT)
+    tr.trace(cam, w, h, 0, 13)
+    tr.trace(cam, w, h, 13, 19)
+    m = _check_adaptive(tr.image(), want, n)
+    assert tr.unconverged() == m
+    tr.close()
+
+
+def test_adaptive_sampling_sample_by_sample(gpu, orc):
+    """Tracer::sample under Adaptive Sampling (slices are ignored: an
+    adaptive sample traces the open list whole) == the oracle."""
+    s = scenes.c1_plain(ntris=2048, width=48, height=32, spp=4)
+    w, h = s.width, s.height
+    cam = cam_of(s, w, h)
+    ocam = cam.copy()
+    ocam["adapt"] = ADAPT
+    want, _ = oracle_lib.TraceOracle(orc, s).trace(ocam, 0, 20)
+    tr = px.Tracer.of(gpu, s)
+    tr.set_adaptive(ADAPT)
+    tr.set_samples(20)
+    for k in range(20):
+        frame, done = tr.sample(cam, w, h, slices=3)
+        assert frame == k and done == (k == 19)
+    _check_adaptive(tr.image(), want, w * h)
+    tr.close()
