@@ -425,7 +425,9 @@ def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
     reference's 4096 samples first and each test image is the difference of
     two later accumulations (every plane the filters read accumulates
     linearly). relMSE = mean (x - r)^2 / (r^2 + 0.01) over pixels and
-    channels of Tracer::radiance. Frame time = trace + filter, CUDA events."""
+    channels of the linear mean over the samples that met something (the
+    value the view transform shows; Tracer::radiance wherever every sample
+    met something). Frame time = trace + filter, CUDA events."""
     import torch
 
     import phiray_b200 as px

@@ -454,6 +454,13 @@ int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint3
  * A change of setting starts the next sample over. Adaptive frames run on
  * the megakernel forms and whole (no pixel slices); batches refuse them. */
 int32_t phx_tracer_set_adaptive(phx_tracer tr, const float adapt[4]);
+/* Tracer::show (src/trace/read.rs:182-216, show.wgsl): `count` linear rgb
+ * triples (host, row 0 first; missing pixels read as 0) become the image's
+ * sums, scaled by the samples each pixel took, and the display step of
+ * emit runs over them (shown planes and packed pixels), so a composited
+ * image is shown through the same view transform. PHX_ERR_INVALID before
+ * any frame was traced. Waits. */
+int32_t phx_tracer_show(phx_tracer tr, const float* linear, uint64_t count);
 /* Tracer::unconverged (src/trace/mod.rs:224-233): the number of pixels not
  * yet settled after the last sample's tail; PHX_ERR_INVALID when adaptive
  * sampling is off. Bounded wait. */

@@ -104,6 +104,8 @@ void orc_scene_free(void* scene);
 void orc_scene_trace(void* scene, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
                      uint64_t* rays_out, uint32_t row0, uint32_t rows);
 /* Primary ray of frame `frame` per pixel: face id (0xFFFFFFFF none), t. */
+// show.wgsl: emit's display tail (shown planes, packed pixels) over the sums in px.
+void orc_show(const struct phx_camera* cam, uint32_t* px);
 void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
                  const struct phx_camera* cam, uint32_t frame, uint32_t* ids, float* ts);
 /* Closest / any hit of rays (o.xyz, tmax, d.xyz, 0): hits (t, face id, u, v). */

@@ -1183,6 +1183,24 @@ void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const
     orc_scene_free(h);
 }
 
+// show.wgsl: emit's display tail over the sums already in px.
+void orc_show(const phx_camera* cam, uint32_t* px) {
+    const uint32_t n = cam->w * cam->h;
+    for (uint32_t i = 0; i < n; i++) {
+        const float k = (float)(px[31 * n + i] > 1u ? px[31 * n + i] : 1u);
+        const uint32_t a = n + 3 * i, g = 20 * n + 3 * i;
+        const V3 l = v3(f_of(px[a]), f_of(px[a + 1]), f_of(px[a + 2]));
+        const V3 gs = v3(f_of(px[g]), f_of(px[g + 1]), f_of(px[g + 2]));
+        const float cov = f_of(px[23 * n + i]), film = f_of(px[24 * n + i]), gone = f_of(px[33 * n + i]);
+        const V3 shown = view_transform_of(l / fmaxw(k - gone, 1.0f), cam->view) * (1.0f - cov / k) + gs / k;
+        const uint32_t b = 4 * n + 3 * i;
+        px[b] = u_of(shown.x);
+        px[b + 1] = u_of(shown.y);
+        px[b + 2] = u_of(shown.z);
+        px[i] = pack(shown, film / k);
+    }
+}
+
 void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
                  const phx_camera* cam, uint32_t frame, uint32_t* ids, float* ts) {
     Shared S;

@@ -151,6 +151,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_trace": (i32, [vp, vp, u32, u32, u32, u32]),
     "phx_tracer_read": (i32, [vp, u64, vp, u64, u32]),
     "phx_tracer_set_adaptive": (i32, [vp, vp]),
+    "phx_tracer_show": (i32, [vp, vp, u64]),
     "phx_tracer_unconverged": (i32, [vp, C.POINTER(u32), u32]),
     "phx_tracer_image": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
     "phx_tracer_verts": (i32, [vp, C.POINTER(vp), C.POINTER(u32)]),

@@ -978,7 +978,7 @@ __global__ void k_firefly(const float* __restrict__ irr, float* __restrict__ out
 // normal 3, depth / (1 + |depth|), the fraction of samples that met
 // something, log2(samples) / 8, and 1 where the first channels hold a
 // spread, 0 where they do not. Radiance is the mean over the samples that
-// met something (Tracer::radiance, read.rs:241-251); albedo' = max(albedo,
+// met something (util.wgsl's emit: light sum / max(k - gone, 1)); albedo' = max(albedo,
 // 0.05) per channel; irradiance = radiance / albedo'. irr_a / irr_b are the
 // irradiances of the samples before and after `half` (a snapshot of the
 // sums and met-sample count taken part way, phx_nn_snapshot; NULL: none) —
@@ -1082,7 +1082,8 @@ __global__ void k_tile_err(const float* __restrict__ err, int w, int h, int Wp, 
 
 // Writes the learned result into the px planes for every pixel whose tile
 // estimate is within `threshold` (the rest keep what Denoise wrote):
-// the scene-linear sums so that Tracer::radiance returns `out` (unless
+// the scene-linear sums so that their mean over the samples that met
+// something (emit's light sum / max(k - gone, 1)) is `out` (unless
 // keep), the shown value and the packed display pixel, as the last Denoise
 // round does (denoise.wgsl, Standard view transform).
 __global__ void k_compose(const float* __restrict__ out, const float* __restrict__ tile_err, int w, int h, int Wp,

@@ -582,6 +582,25 @@ __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, 
     flush_counts<STATS>(cnt, counters);
 }
 
+// show.wgsl: the display step of emit on its own, over the linear sums
+// already in the image (Tracer::show writes a composited image there):
+// the view transform of the mean over the samples that met something,
+// the overlay laid over by its coverage, the packed pixel.
+__global__ void k_show(uint32_t* __restrict__ px, uint32_t n, float exposure, float gamma) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float k = (float)max(px[31u * n + i], 1u);
+    f3 l, gs;
+    ld3(px, 1 * n, i, l);
+    ld3(px, 20 * n, i, gs);
+    const float cov = __uint_as_float(px[23u * n + i]);
+    const float film = __uint_as_float(px[24u * n + i]);
+    const float gone = __uint_as_float(px[33u * n + i]);
+    const f3 shown = view_transform_std(l / fmaxf(k - gone, 1.0f), exposure, gamma) * (1.0f - cov / k) + gs / k;
+    st3(px, 4 * n, i, shown);
+    px[i] = pack_rgba(shown, film / k);
+}
+
 // ---- Adaptive Sampling (adapt.wgsl, gather.wgsl) ----
 
 // adapt.wgsl's main: Cycles' convergence check at the end of `sample`, a
@@ -1987,6 +2006,33 @@ int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint
     if (frame) *frame = f;
     if (done) *done = (f + 1 >= tr->target) ? 1 : 0;
     return PHX_OK;
+}
+
+int32_t phx_tracer_show(phx_tracer tr, const float* linear, uint64_t count) {
+    if (!tr || (!linear && count)) return fail(PHX_ERR_INVALID, "null argument");
+    if (!tr->px.ptr || !tr->have_last) return fail(PHX_ERR_INVALID, "no image to show yet");
+    PHX_TRY(use(tr->ctx));
+    const uint64_t n = (uint64_t)tr->w * tr->h;
+    cudaStream_t s = tr->ctx->stream;
+    // read.rs:182-216: the sums are k times the mean, k the samples each
+    // pixel took (counts: frame + 1, or the pixel's own count under
+    // Adaptive Sampling); missing pixels of `linear` read as 0.
+    std::vector<uint32_t> cnt;
+    if (tr->adapt[3] != 0.0f) {
+        cnt.resize(n);
+        PHX_CUDA(cudaMemcpyAsync(cnt.data(), (const uint32_t*)tr->px.ptr + 31 * n, n * 4, cudaMemcpyDeviceToHost, s));
+        PHX_TRY(wait_stream(s, 0));
+    }
+    std::vector<float> sums(3 * n, 0.0f);
+    for (uint64_t i = 0; i < n; i++) {
+        const float k = tr->adapt[3] != 0.0f ? (float)(cnt[i] > 1u ? cnt[i] : 1u) : (float)(tr->frame + 1);
+        for (int c = 0; c < 3; c++) sums[3 * i + c] = i < count ? linear[3 * i + c] * k : 0.0f * k;
+    }
+    PHX_CUDA(cudaMemcpyAsync((uint32_t*)tr->px.ptr + n, sums.data(), 3 * n * 4, cudaMemcpyHostToDevice, s));
+    k_show<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((uint32_t*)tr->px.ptr, (uint32_t)n, tr->last.view[1],
+                                                       tr->last.view[2]);
+    PHX_TRY(cuda_check(cudaGetLastError(), "show"));
+    return wait_stream(s, 0);  // `linear` is the caller's: the copy has read it
 }
 
 int32_t phx_tracer_set_adaptive(phx_tracer tr, const float adapt[4]) {

@@ -95,6 +95,57 @@ class _Scene(C.Structure):
     ]
 
 
+def _counts(px: np.ndarray, n: int) -> np.ndarray:
+    """Samples each pixel took (read.rs `counts`: the count plane, at least 1)."""
+    return np.maximum(px[31 * n:32 * n], 1).astype(np.float32)
+
+
+def radiance_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """``Tracer::radiance`` of a host px image: sums / samples taken."""
+    n = w * h
+    lin = px.view(np.float32)[n:4 * n].reshape(n, 3)
+    return (lin / _counts(px, n)[:, None]).reshape(h, w, 3)
+
+
+def lit_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """The linear mean over the samples that met something (util.wgsl's emit:
+    l / max(k - gone, 1)), the value the view transform is applied to."""
+    n = w * h
+    f = px.view(np.float32)
+    k = px[31 * n:32 * n].astype(np.float32)
+    return (f[n:4 * n].reshape(n, 3) / np.maximum(k - f[33 * n:34 * n], 1.0)[:, None]).reshape(h, w, 3)
+
+
+def display_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """``Tracer::display``: the shown plane (no division: it is a mean)."""
+    n = w * h
+    return px.view(np.float32)[4 * n:7 * n].reshape(h, w, 3).copy()
+
+
+def albedo_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """``Tracer::albedo``: the albedo guide sums / samples taken."""
+    n = w * h
+    return (px.view(np.float32)[7 * n:10 * n].reshape(n, 3) / _counts(px, n)[:, None]).reshape(h, w, 3)
+
+
+def normal_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """``Tracer::normal``: the normal guide mean, re-normalised (0 where its
+    length is 1e-9 or less)."""
+    n = w * h
+    v = px.view(np.float32)[10 * n:13 * n].reshape(n, 3) / _counts(px, n)[:, None]
+    ln = np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2])
+    out = np.where((ln > 1e-9)[:, None], v / np.where(ln > 1e-9, ln, 1.0)[:, None], 0.0)
+    return out.astype(np.float32).reshape(h, w, 3)
+
+
+def depth_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
+    """``Tracer::depth``: the depth guide mean, 1e10 where it is <= 0 (a
+    miss records -1 a sample)."""
+    n = w * h
+    mean = px.view(np.float32)[13 * n:14 * n] / _counts(px, n)
+    return np.where(mean <= 0.0, np.float32(1.0e10), mean).astype(np.float32).reshape(h, w)
+
+
 class Tracer:
     """The Rendered-mode path tracer (phiray ``Tracer``)."""
 
@@ -210,15 +261,37 @@ class Tracer:
         return self.read(0, self.w * self.h)
 
     def radiance(self) -> np.ndarray:
-        """``Tracer::radiance``: linear mean per pixel (h, w, 3) over the
-        samples that met something (read.rs:241-251)."""
-        n = self.w * self.h
-        px = self.read(0, PX_LEN * n + 1)
-        f = px.view(np.float32)
-        k = px[31 * n: 32 * n].astype(np.float32)
-        gone = f[33 * n: 34 * n]
-        lin = f[n: 4 * n].reshape(n, 3)
-        return (lin / np.maximum(k - gone, 1.0)[:, None]).reshape(self.h, self.w, 3)
+        """``Tracer::radiance`` (read.rs:240-251): the linear sums over the
+        samples each pixel took, (h, w, 3)."""
+        return radiance_of(self.image(), self.w, self.h)
+
+    def lit(self) -> np.ndarray:
+        """The linear mean over the samples that met something (what emit
+        hands the view transform), (h, w, 3)."""
+        return lit_of(self.image(), self.w, self.h)
+
+    def display(self) -> np.ndarray:
+        """``Tracer::display`` (read.rs:253-262): the shown values, (h, w, 3)."""
+        return display_of(self.image(), self.w, self.h)
+
+    def albedo(self) -> np.ndarray:
+        """``Tracer::albedo`` (read.rs:264-271): the diffuse-colour guide, (h, w, 3)."""
+        return albedo_of(self.image(), self.w, self.h)
+
+    def normal(self) -> np.ndarray:
+        """``Tracer::normal`` (read.rs:273-285): the normal guide made unit, (h, w, 3)."""
+        return normal_of(self.image(), self.w, self.h)
+
+    def depth(self) -> np.ndarray:
+        """``Tracer::depth`` (read.rs:287-309): distance to the first hit, 1e10
+        where nothing was met, (h, w)."""
+        return depth_of(self.image(), self.w, self.h)
+
+    def show(self, linear) -> None:
+        """``Tracer::show`` (read.rs:182-216): a composited linear image shown
+        through the tracer's view transform (phx_tracer_show)."""
+        lin = np.ascontiguousarray(np.asarray(linear, dtype=np.float32).reshape(-1, 3))
+        N.check(N.lib().phx_tracer_show(self.handle, lin.ctypes.data, lin.shape[0]))
 
     def device_verts(self) -> tuple[int, int]:
         """Device pointer and count of the tracer's own vertex array."""

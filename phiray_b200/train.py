@@ -50,7 +50,10 @@ def px_diff(a: np.ndarray, b: np.ndarray | None, n: int) -> np.ndarray:
 
 
 def radiance(px: np.ndarray, w: int, h: int) -> np.ndarray:
-    """Tracer::radiance of a px image (read.rs:241-251): (h, w, 3) float32."""
+    """The linear mean over the samples that met something (util.wgsl's emit:
+    light sum / max(k - gone, 1)) of a px image, (h, w, 3) float32 — the value
+    the view transform shows; equal to Tracer::radiance (read.rs:240-251,
+    sum / k) wherever every sample met something."""
     n = w * h
     f = px.view(np.float32)
     k = px[31 * n:32 * n].astype(np.float32)

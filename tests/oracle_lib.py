@@ -39,6 +39,7 @@ SIGS = {
     "orc_scene_free": (None, [vp]),
     "orc_scene_trace": (None, [vp, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
     "orc_primary": (None, [vp, vp, u32, vp, u32, vp, u32, vp, vp]),
+    "orc_show": (None, [vp, vp]),
     "orc_trace_rays": (None, [vp, vp, u32, vp, u32, vp, u32, vp, C.c_int]),
 }
 

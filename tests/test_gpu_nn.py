@@ -542,7 +542,7 @@ def test_learned_denoise_fallback_tiles(gpu):
     o, e = _np(out), _np(err)
     fb = net.denoise(tr, tile=16, threshold=1e30, count=True)
     assert fb == 0
-    rad = tr.radiance()
+    rad = tr.lit()
     n = w * h
     cnt = np.maximum(noisy[31 * n:32 * n].astype(np.float64), 1)
     gone = noisy.view(np.float32)[33 * n:34 * n]
@@ -711,7 +711,7 @@ def test_learned_denoise_with_the_clamp_filters_clamped_irradiance(gpu):
     _sync(gpu)
     o = _np(out)
     assert net.denoise(tr, tile=16, threshold=1e30, count=True) == 0
-    rad = tr.radiance()
+    rad = tr.lit()
     n = w * h
     cnt = np.maximum(noisy[31 * n:32 * n].astype(np.float64), 1)
     gone = noisy.view(np.float32)[33 * n:34 * n]

@@ -253,3 +253,27 @@ def test_adaptive_sampling_sample_by_sample(gpu, orc):
         assert frame == k and done == (k == 19)
     _check_adaptive(tr.image(), want, w * h)
     tr.close()
+
+
+def test_show_matches_oracle(gpu, orc):
+    """Tracer::show (phx_tracer_show): a composited linear image written back
+    as sums scaled by the samples taken, then show.wgsl's display step —
+    the sums, shown planes and packed pixels equal the oracle's bit for bit."""
+    s = SCENES["c1_small"]()
+    w, h = s.width, s.height
+    n = w * h
+    cam = cam_of(s, w, h)
+    tr = px.Tracer.of(gpu, s)
+    tr.trace(cam, w, h, 0, 5)
+    before = tr.image()
+    linear = (px.tracer.radiance_of(before, w, h) * np.float32(0.5)).reshape(n, 3).astype(np.float32)
+    linear[::7] = 0.0
+    tr.show(linear[: n - 10])  # the last pixels missing read as 0
+    got = tr.image()
+    want = before.copy()
+    full = np.zeros((n, 3), np.float32)
+    full[: n - 10] = linear[: n - 10]
+    want.view(np.float32)[n:4 * n] = (full * np.float32(5.0)).reshape(-1)
+    orc.lib.orc_show(cam.ctypes.data, want.ctypes.data)
+    assert np.array_equal(got, want)
+    tr.close()
