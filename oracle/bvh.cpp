@@ -303,6 +303,157 @@ void orc_refit(orc_node* nodes, uint32_t nnodes, const uint32_t* order, const or
     }
 }
 
+// ---- the binned SAH builder (src/bvh/sah.rs:25-189): the tree phiray's
+// tracer walks (forest.rs:49, 216). Bins, sweeps and the in-place partition
+// in the reference's order, so the tree is the reference's node for node.
+namespace {
+
+const uint32_t SAH_BINS = 16;      // sah.rs:26 BIN_COUNT
+const float SAH_TRAVERSE = 1.0f;   // sah.rs:30 TRAVERSE
+
+// sah.rs:32-35 area (of an Aabb; negative extents count as 0).
+float sah_area(const orc_aabb& b) {
+    float d[3];
+    for (int k = 0; k < 3; k++) d[k] = rmax(b.hi[k] - b.lo[k], 0.0f);
+    return 2.0f * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+}
+
+// sah.rs:68-79 Grid: a centroid's bin along one axis (Rust `as usize`
+// truncates and saturates; NaN gives 0).
+struct SahGrid {
+    float lo[3], scale[3];
+    uint32_t bin(const float* c, int k) const {
+        const float v = (c[k] - lo[k]) * scale[k];
+        uint64_t b = (v != v || v <= 0.0f) ? 0u : (v >= 1.8e19f ? UINT64_MAX : (uint64_t)v);
+        return (uint32_t)std::min<uint64_t>(b, SAH_BINS - 1);
+    }
+};
+
+orc_aabb point_box(const float* c) {
+    orc_aabb b;
+    std::memset(&b, 0, sizeof b);
+    for (int k = 0; k < 3; k++) b.lo[k] = b.hi[k] = c[k];
+    return b;
+}
+
+// sah.rs:114-189 split: the left count m after reordering `slots`, or -1
+// for a leaf. Histogram merges are exact (integer counts, min/max bounds),
+// so the reference's parallel fill gives what this serial one gives.
+int64_t sah_split(const orc_aabb* prims, const std::vector<float>& centres, uint32_t* slots, uint32_t count,
+                  uint32_t leaf) {
+    if (count <= 1) return -1;
+    orc_aabb cbox = aabb_default();
+    for (uint32_t j = 0; j < count; j++) cbox = aabb_union(cbox, point_box(&centres[3 * (size_t)slots[j]]));
+    SahGrid grid;
+    bool flat = true;
+    for (int k = 0; k < 3; k++) {
+        const float e = cbox.hi[k] - cbox.lo[k];
+        grid.lo[k] = cbox.lo[k];
+        grid.scale[k] = e > 0.0f ? (float)SAH_BINS * (1.0f - 1e-5f) / e : 0.0f;
+        if (grid.scale[k] != 0.0f) flat = false;
+    }
+    if (flat) return count > leaf ? (int64_t)(count / 2) : -1;
+    uint32_t bcount[3][SAH_BINS] = {};
+    orc_aabb bbox[3][SAH_BINS];
+    for (int k = 0; k < 3; k++)
+        for (uint32_t b = 0; b < SAH_BINS; b++) bbox[k][b] = aabb_default();
+    for (uint32_t j = 0; j < count; j++) {
+        const uint32_t i = slots[j];
+        for (int k = 0; k < 3; k++) {
+            const uint32_t at = grid.bin(&centres[3 * (size_t)i], k);
+            bcount[k][at] += 1;
+            bbox[k][at] = aabb_union(bbox[k][at], prims[i]);
+        }
+    }
+    bool have = false;
+    float best_cost = 0.0f;
+    int best_k = 0;
+    uint32_t best_at = 0;
+    for (int k = 0; k < 3; k++) {
+        if (grid.scale[k] == 0.0f) continue;
+        float right_area[SAH_BINS] = {};
+        uint32_t right_count[SAH_BINS] = {};
+        orc_aabb b = aabb_default();
+        uint32_t c = 0;
+        for (uint32_t at = SAH_BINS - 1; at >= 1; at--) {
+            b = aabb_union(b, bbox[k][at]);
+            c += bcount[k][at];
+            right_area[at] = sah_area(b);
+            right_count[at] = c;
+        }
+        b = aabb_default();
+        c = 0;
+        for (uint32_t at = 0; at + 1 < SAH_BINS; at++) {
+            b = aabb_union(b, bbox[k][at]);
+            c += bcount[k][at];
+            const float ra = right_area[at + 1];
+            const uint32_t rc = right_count[at + 1];
+            if (c == 0 || rc == 0) continue;
+            const float cost = sah_area(b) * (float)c + ra * (float)rc;
+            if (!have || cost < best_cost) {
+                have = true;
+                best_cost = cost;
+                best_k = k;
+                best_at = at;
+            }
+        }
+    }
+    orc_aabb bounds = aabb_default();
+    for (uint32_t b = 0; b < SAH_BINS; b++) bounds = aabb_union(bounds, bbox[0][b]);
+    if (!have) return count > leaf ? (int64_t)(count / 2) : -1;
+    const float parent = rmax(sah_area(bounds), FLT_MIN);
+    if (count <= leaf && SAH_TRAVERSE + best_cost / parent >= (float)count) return -1;
+    uint32_t m = 0;
+    for (uint32_t j = 0; j < count; j++) {
+        if (grid.bin(&centres[3 * (size_t)slots[j]], best_k) <= best_at) {
+            std::swap(slots[j], slots[m]);
+            m++;
+        }
+    }
+    return (m == 0 || m == count) ? (int64_t)(count / 2) : (int64_t)m;
+}
+
+}  // namespace
+
+uint32_t orc_build_sah(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order,
+                       uint32_t* depth_out) {
+    // sah.rs:84-109 Bvh::build_sah: a work stack of (slot, start, end, depth),
+    // left child taken first, leaves at the depth cap, then refit.
+    *depth_out = 0;
+    if (n == 0) return 0;
+    std::vector<float> centres(3 * (size_t)n);
+    for (uint32_t i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) centres[3 * (size_t)i + k] = 0.5f * (prims[i].lo[k] + prims[i].hi[k]);
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
+    uint32_t count = 1;
+    nodes[0] = node_inner(0, 0);
+    uint32_t depth = 0;
+    struct Work {
+        uint32_t slot, start, end, d;
+    };
+    std::vector<Work> work{{0, 0, n, 0}};
+    while (!work.empty()) {
+        const Work wk = work.back();
+        work.pop_back();
+        depth = std::max(depth, wk.d);
+        const int64_t cut = wk.d + 1 >= STACK ? -1 : sah_split(prims, centres, order + wk.start, wk.end - wk.start, leaf);
+        if (cut < 0) {
+            nodes[wk.slot] = node_leaf(wk.start, wk.end);
+        } else {
+            const uint32_t at = count;
+            nodes[count++] = node_inner(0, 0);
+            nodes[count++] = node_inner(0, 0);
+            nodes[wk.slot] = node_inner(at, at + 1);
+            const uint32_t m = (uint32_t)cut;
+            work.push_back({at + 1, wk.start + m, wk.end, wk.d + 1});
+            work.push_back({at, wk.start, wk.start + m, wk.d + 1});
+        }
+    }
+    *depth_out = depth;
+    orc_refit(nodes, count, order, prims);
+    return count;
+}
+
 void orc_build(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order, uint32_t* depth) {
     // build.rs:94-100
     *depth = 0;

@@ -73,6 +73,10 @@ void orc_build(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes
  * (nodes must hold 2n-1). */
 uint32_t orc_build_compact(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order,
                            uint32_t* depth);
+/* src/bvh/sah.rs:84-189 Bvh::build_sah, the binned SAH tree phiray's tracer
+ * walks: nodes (room for 2n-1), order (n), depth; returns the node count. */
+uint32_t orc_build_sah(const orc_aabb* prims, uint32_t n, uint32_t leaf, orc_node* nodes, uint32_t* order,
+                       uint32_t* depth);
 /* src/bvh/shape.rs:8-37 Bvh::compact in place; returns the new count. */
 uint32_t orc_compact(orc_node* nodes, uint32_t nnodes);
 /* src/bvh/shape.rs:40-51 Bvh::reachable; returns the count written. */

@@ -29,6 +29,7 @@ SIGS = {
     "orc_assemble": (None, [u32, vp, u32, vp, C.POINTER(u32)]),
     "orc_refit": (None, [vp, u32, vp, vp]),
     "orc_build": (None, [vp, u32, u32, vp, vp, C.POINTER(u32)]),
+    "orc_build_sah": (u32, [vp, u32, u32, vp, vp, C.POINTER(u32)]),
     "orc_build_compact": (u32, [vp, u32, u32, vp, vp, C.POINTER(u32)]),
     "orc_compact": (u32, [vp, u32]),
     "orc_reachable": (u32, [vp, u32, vp]),
@@ -109,6 +110,16 @@ class Oracle:
         order = np.zeros(n, dtype=np.uint32)
         depth = u32()
         m = self.lib.orc_build_compact(prims.ctypes.data, n, leaf, nodes.ctypes.data, order.ctypes.data, C.byref(depth))
+        return nodes[:m].copy(), order, depth.value
+
+    def build_sah(self, prims, leaf=4):
+        """src/bvh/sah.rs Bvh::build_sah: (nodes, order, depth)."""
+        prims = np.ascontiguousarray(prims, dtype=np.float32).reshape(-1, 8)
+        n = len(prims)
+        nodes = np.zeros((max(1, 2 * n - 1), 8), dtype=np.float32)
+        order = np.zeros(n, dtype=np.uint32)
+        depth = u32()
+        m = self.lib.orc_build_sah(prims.ctypes.data, n, leaf, nodes.ctypes.data, order.ctypes.data, C.byref(depth))
         return nodes[:m].copy(), order, depth.value
 
     def refit(self, nodes, order, prims):

@@ -148,3 +148,47 @@ def test_golden_fixture(orc):
     nodes, order, depth = orc.build(p, 4)
     assert np.array_equal(order, g["order"]) and depth == int(g["depth"])
     assert np.array_equal(nodes.view(np.uint32), g["nodes"].view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 100, 5000, 70000])
+@pytest.mark.parametrize("leaf", [1, 4])
+def test_sah_builds_valid_trees(orc, n, leaf):
+    # test.rs:79-91: the binned SAH tree (sah.rs) the reference's tracer walks
+    p = gen.test_prims(n)
+    nodes, order, depth = orc.build_sah(p, leaf)
+    gen.check_tree(nodes, order, depth, p, orc.reachable(nodes))
+    assert len(orc.reachable(nodes)) == len(nodes)  # built compact: no unreachable nodes
+
+
+def test_sah_empty_and_flat(orc):
+    nodes, order, depth = orc.build_sah(np.zeros((0, 8), np.float32), 4)
+    assert len(nodes) == 0 and len(order) == 0 and depth == 0
+    # every centre in one point: no plane to split on, still a valid tree
+    flat = np.tile(np.array([0, 0, 0, 0, 1, 1, 1, 0], np.float32), (1000, 1))
+    nodes, order, depth = orc.build_sah(flat, 4)
+    gen.check_tree(nodes, order, depth, flat, orc.reachable(nodes))
+
+
+def _sah_cost(nodes):
+    # test.rs:97-112 cost: each node's area against the root's, times what it holds
+    w = nodes.view(np.uint32)
+
+    def area(i):
+        d = np.maximum(nodes[i, 4:7] - nodes[i, 0:3], 0.0).astype(np.float32)
+        return np.float32(2.0) * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0])
+
+    root = area(0)
+    total = 0.0
+    for i in range(len(nodes)):
+        lo, hi = int(w[i, 3]), int(w[i, 7])
+        held = (hi - (lo & 0x7FFFFFFF)) if lo & 0x80000000 else 1
+        total += float(area(i) / root) * held
+    return total
+
+
+def test_sah_trees_are_cheaper_to_walk_than_morton_ones(orc):
+    # test.rs:94-116
+    p = gen.test_prims(20000)
+    sah = _sah_cost(orc.build_sah(p, 4)[0])
+    morton = _sah_cost(orc.build_compact(p, 4)[0])
+    assert sah < morton * 0.9, (sah, morton)
