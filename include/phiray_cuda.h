@@ -296,7 +296,7 @@ typedef struct phx_light {
 /* trace::Camera (src/trace/camera.rs:12-230, camera.wgsl:3-54), byte for
  * byte (5,776 bytes), so a Rust caller passes its `Camera` as is. The
  * Rendered path reads the view, lights, env, view transform, bounces,
- * limit and frame words; settings this build does not implement are
+ * limit and frame words; settings this library does not implement are
  * refused with PHX_ERR_INVALID (see phx_tracer_sample). */
 typedef struct phx_camera {
     uint32_t n, groups_x, w, h;
