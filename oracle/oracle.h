@@ -107,6 +107,13 @@ void* orc_scene_new(const float* verts, const uint32_t* faces, uint32_t nfaces, 
 void orc_scene_free(void* scene);
 void orc_scene_trace(void* scene, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
                      uint64_t* rays_out, uint32_t row0, uint32_t rows);
+/* The same scene with the binned SAH tree (sah.rs) in place of the Morton one. */
+void* orc_scene_new_sah(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
+                        const float* normals, uint32_t leaf);
+/* orc_scene_trace that also counts the walks' inner-node visits (walk[0]) and
+ * triangle tests (walk[1]). */
+void orc_scene_trace_walk(void* scene, const struct phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                          uint64_t* rays, uint32_t row0, uint32_t rows, uint64_t* walk);
 /* Primary ray of frame `frame` per pixel: face id (0xFFFFFFFF none), t. */
 // show.wgsl: emit's display tail (shown planes, packed pixels) over the sums in px.
 void orc_show(const struct phx_camera* cam, uint32_t* px);

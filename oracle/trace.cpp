@@ -83,6 +83,7 @@ struct World {
     float ao, eps;
     uint32_t* px;
     uint64_t rays;
+    mutable uint64_t steps = 0, tests = 0;  // inner-node visits and triangle tests of the walks
 
     const uint32_t* face(uint32_t slot) const { return faces + 4 * (size_t)S->order[slot]; }
     V3 vert(uint32_t v) const { return v3(verts[4 * (size_t)v], verts[4 * (size_t)v + 1], verts[4 * (size_t)v + 2]); }
@@ -206,6 +207,7 @@ void trace_blas(const World& W, V3 o, V3 d, bool first, Hit* best) {
         if ((nd.lo.i & LEAF) != 0u) {
             for (uint32_t id = nd.lo.i & ~LEAF; id < nd.hi.i; id++) {
                 const uint32_t* v = W.face(id);
+                W.tests++;
                 float h[3];
                 tri_t(W.vert(v[0]), W.vert(v[1]), W.vert(v[2]), o, rs, h);
                 if (h[0] < best->t) {
@@ -219,6 +221,7 @@ void trace_blas(const World& W, V3 o, V3 d, bool first, Hit* best) {
                 }
             }
         } else {
+            W.steps++;
             const orc_node nl = W.S->nodes[nd.lo.i];
             const orc_node nr = W.S->nodes[nd.hi.i];
             const float tl = box_t(nl, o, inv, best->t);
@@ -1006,7 +1009,7 @@ void shade_main(World& W, uint32_t i) {
 }
 
 void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
-           const float* normals, uint32_t leaf) {
+           const float* normals, uint32_t leaf, bool sah = false) {
     W.S = &S;
     std::vector<orc_aabb> boxes(nfaces);
     for (uint32_t f = 0; f < nfaces; f++) {
@@ -1023,7 +1026,12 @@ void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint3
     S.nodes.assign(2 * (size_t)nfaces - 1, orc_node{});
     S.order.assign(nfaces, 0);
     uint32_t depth = 0;
-    orc_build(boxes.data(), nfaces, leaf ? leaf : 4, S.nodes.data(), S.order.data(), &depth);
+    if (sah) {
+        // the binned SAH tree phiray's tracer builds (forest.rs:49 build_sah)
+        S.nodes.resize(orc_build_sah(boxes.data(), nfaces, leaf ? leaf : 4, S.nodes.data(), S.order.data(), &depth));
+    } else {
+        orc_build(boxes.data(), nfaces, leaf ? leaf : 4, S.nodes.data(), S.order.data(), &depth);
+    }
     W.verts = verts;
     W.normals = normals;
     W.faces = faces;
@@ -1079,6 +1087,13 @@ void* orc_scene_new(const float* verts, const uint32_t* faces, uint32_t nfaces, 
     return h;
 }
 
+void* orc_scene_new_sah(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
+                        const float* normals, uint32_t leaf) {
+    auto* h = new OrcScene();
+    setup(h->S, h->W0, verts, faces, nfaces, mats, normals, leaf, true);
+    return h;
+}
+
 void orc_scene_free(void* handle) { delete (OrcScene*)handle; }
 
 // adapt.wgsl and gather.wgsl: the tail after `sample` — the convergence
@@ -1119,9 +1134,25 @@ static void adapt_tail(const phx_camera* cam, uint32_t* px, uint32_t sample) {
     px[34 * (size_t)n] = open;
 }
 
+static void scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                        uint64_t* rays_out, uint32_t row0, uint32_t rows, uint64_t* walk);
+
 void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
                      uint64_t* rays_out, uint32_t row0, uint32_t rows) {
+    scene_trace(handle, cam, first, spp, px, rays_out, row0, rows, nullptr);
+}
+
+// The same, also counting the walks' inner-node visits and triangle tests
+// (walk[0], walk[1]): a tree's cost on a real ray load.
+void orc_scene_trace_walk(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                          uint64_t* rays_out, uint32_t row0, uint32_t rows, uint64_t* walk) {
+    scene_trace(handle, cam, first, spp, px, rays_out, row0, rows, walk);
+}
+
+static void scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32_t spp, uint32_t* px,
+                        uint64_t* rays_out, uint32_t row0, uint32_t rows, uint64_t* walk) {
     const OrcScene* h = (const OrcScene*)handle;
+    uint64_t steps_sum = 0, tests_sum = 0;
     if (cam->adapt[3] != 0.0f) {
         // Adaptive Sampling couples neighbouring pixels between samples:
         // whole frames, sample by sample, each followed by its tail.
@@ -1129,7 +1160,7 @@ void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32
         const uint32_t n = cam->w * cam->h;
         uint64_t total = 0;
         for (uint32_t f = first; f < first + spp; f++) {
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total, steps_sum, tests_sum)
             for (int64_t i = 0; i < (int64_t)n; i++) {
                 World W = h->W0;
                 W.p = cam;
@@ -1141,10 +1172,16 @@ void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32
                 W.frame = f;
                 shade_main(W, (uint32_t)i);
                 total += W.rays;
+                steps_sum += W.steps;
+                tests_sum += W.tests;
             }
             adapt_tail(cam, px, f);
         }
         if (rays_out) *rays_out = total;
+        if (walk) {
+            walk[0] = steps_sum;
+            walk[1] = tests_sum;
+        }
         return;
     }
     const Shared& S = h->S;
@@ -1154,7 +1191,7 @@ void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32
     const float eps = S.extent * 1e-5f;
     const uint32_t r1 = rows ? (row0 + rows < hh ? row0 + rows : hh) : hh;
     uint64_t total = 0;
-#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total, steps_sum, tests_sum)
     for (int64_t y = row0; y < (int64_t)r1; y++) {
         World W = h->W0;  // the scene is shared; counters are per thread
         W.p = cam;
@@ -1171,8 +1208,14 @@ void orc_scene_trace(void* handle, const phx_camera* cam, uint32_t first, uint32
             }
         }
         total += W.rays;
+        steps_sum += W.steps;
+        tests_sum += W.tests;
     }
     if (rays_out) *rays_out = total;
+    if (walk) {
+        walk[0] = steps_sum;
+        walk[1] = tests_sum;
+    }
 }
 
 void orc_trace(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, const float* normals,

@@ -37,6 +37,8 @@ SIGS = {
     "orc_denoise": (None, [vp, u32, u32, C.POINTER(f32), C.POINTER(f32), C.c_int]),
     "orc_trace": (None, [vp, vp, u32, vp, vp, u32, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
     "orc_scene_new": (vp, [vp, vp, u32, vp, vp, u32]),
+    "orc_scene_new_sah": (vp, [vp, vp, u32, vp, vp, u32]),
+    "orc_scene_trace_walk": (None, [vp, vp, u32, u32, vp, C.POINTER(u64), u32, u32, vp]),
     "orc_scene_free": (None, [vp]),
     "orc_scene_trace": (None, [vp, vp, u32, u32, vp, C.POINTER(u64), u32, u32]),
     "orc_primary": (None, [vp, vp, u32, vp, u32, vp, u32, vp, vp]),
@@ -170,12 +172,12 @@ def _scene_args(scene):
 class TraceOracle:
     """The tracer restatement (oracle/trace.cpp) for a `scenes.Scene`."""
 
-    def __init__(self, orc: "Oracle", scene, leaf: int = 4):
+    def __init__(self, orc: "Oracle", scene, leaf: int = 4, sah: bool = False):
         self.lib = orc.lib
         self.v, self.f, self.m = _scene_args(scene)
         self.leaf = leaf
-        self.handle = self.lib.orc_scene_new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data,
-                                             None, leaf)
+        new = self.lib.orc_scene_new_sah if sah else self.lib.orc_scene_new
+        self.handle = new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, None, leaf)
 
     def __del__(self):
         try:
@@ -191,6 +193,17 @@ class TraceOracle:
         r0, nr = (0, 0) if rows is None else rows
         self.lib.orc_scene_trace(self.handle, cam.ctypes.data, first, spp, px.ctypes.data, C.byref(rays), r0, nr)
         return px, rays.value
+
+    def trace_walk(self, cam, first: int, spp: int, rows=None):
+        """trace, also returning the walks' (inner-node visits, triangle tests)."""
+        w, h = int(cam["w"][0]), int(cam["h"][0])
+        px = np.zeros(34 * w * h + 1, dtype=np.uint32)
+        rays = u64()
+        walk = np.zeros(2, np.uint64)
+        r0, nr = (0, 0) if rows is None else rows
+        self.lib.orc_scene_trace_walk(self.handle, cam.ctypes.data, first, spp, px.ctypes.data, C.byref(rays), r0, nr,
+                                      walk.ctypes.data)
+        return px, rays.value, int(walk[0]), int(walk[1])
 
     def primary(self, cam, frame: int):
         n = int(cam["w"][0]) * int(cam["h"][0])

@@ -192,3 +192,22 @@ def test_sah_trees_are_cheaper_to_walk_than_morton_ones(orc):
     sah = _sah_cost(orc.build_sah(p, 4)[0])
     morton = _sah_cost(orc.build_compact(p, 4)[0])
     assert sah < morton * 0.9, (sah, morton)
+
+
+@pytest.mark.parametrize("which", ["c1", "c2"])
+def test_sah_tree_traces_the_same_image(orc, which):
+    """The tree decides only which nodes a walk visits: with the SAH tree
+    the oracle's image is the Morton tree's word for word, with fewer
+    triangle tests."""
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+    from tests import oracle_lib
+
+    s = (scenes.c1_plain(ntris=4096, width=64, height=64, spp=4) if which == "c1"
+         else scenes.c2_mesh(levels=4, width=64, height=48, spp=4))
+    cam = px.camera(s)
+    cam["w"], cam["h"] = s.width, s.height
+    a, ra, _, ta = oracle_lib.TraceOracle(orc, s).trace_walk(cam, 0, 4)
+    b, rb, _, tb = oracle_lib.TraceOracle(orc, s, sah=True).trace_walk(cam, 0, 4)
+    assert ra == rb and np.array_equal(a, b)
+    assert tb < ta
