@@ -202,6 +202,18 @@ uint32_t phx_pass_compiled(phx_pass pass);
 /* ---- GpuBvh (src/bvh/gpu.rs:11-104) ---- */
 typedef struct phx_bvh_s* phx_bvh;
 
+/* Bvh::build_sah (src/bvh/sah.rs:84-189) on the device: the binned SAH tree
+ * phiray's tracer walks (forest.rs:49, 216), node for node — 16 centroid
+ * bins per axis, the cheapest of the 45 planes, a leaf where splitting
+ * costs more than testing what the node holds or at depth 31, the
+ * reference's in-place partition of each node's slots and its node
+ * numbering, bounds refit bottom up. All pointers are DEVICE memory:
+ * prims (n phx_aabb), nodes (room for 2n - 1), order (n). Writes the node
+ * count and depth; stream-ordered, waits once per tree level. One thread
+ * builds each node of a level, so the first levels run on few threads. */
+int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t leaf, phx_node* nodes,
+                          uint32_t* order, uint32_t* node_count, uint32_t* depth);
+
 /* GpuBvh::build (gpu.rs:23-74) from HOST prims: upload, then every stage on
  * the device — bounds, Morton codes, stable radix sort, Karras links, leaf
  * packing and depth, atomic bottom-up refit. No readback. n may be 0. */

@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_pass_len": (u32, [vp]),
     "phx_pass_compiled": (u32, [vp]),
     "phx_bvh_build": (i32, [vp, vp, u32, u32, C.POINTER(vp)]),
+    "phx_bvh_build_sah": (i32, [vp, vp, u32, u32, vp, vp, C.POINTER(u32), C.POINTER(u32)]),
     "phx_bvh_build_device": (i32, [vp, vp, u32, u32, C.POINTER(vp)]),
     "phx_bvh_rebuild_device": (i32, [vp, vp, u32]),
     "phx_bvh_refit": (i32, [vp]),

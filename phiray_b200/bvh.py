@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
-from .gpu import Gpu, devptr
+from .gpu import Gpu, GpuArray, devptr
 
 LEAF = N.LEAF
 STACK = N.STACK
@@ -68,6 +68,27 @@ class Bvh:
             if not lo & LEAF:
                 stack.extend([lo, hi])
         return out
+
+
+def build_sah(gpu: Gpu, prims: np.ndarray, leaf: int = 4, timeout_ms: int = 0) -> "Bvh":
+    """``Bvh::build_sah`` (src/bvh/sah.rs) on the device from host prims:
+    the binned SAH tree phiray's tracer walks, read back as a ``Bvh``."""
+    prims = np.ascontiguousarray(prims, dtype=np.float32).reshape(-1, 8)
+    n = len(prims)
+    if n == 0:
+        return Bvh(np.zeros((0, 8), np.float32), np.zeros(0, np.uint32), 0)
+    src = GpuArray.from_(gpu, prims)
+    nodes = GpuArray(gpu, (2 * n - 1) * 32)
+    order = GpuArray(gpu, n * 4)
+    count, depth = C.c_uint32(), C.c_uint32()
+    N.check(N.lib().phx_bvh_build_sah(gpu.handle, devptr(src), n, leaf, devptr(nodes), devptr(order),
+                                      C.byref(count), C.byref(depth)))
+    m = count.value
+    out = Bvh(nodes.read(np.float32, timeout_ms=timeout_ms).reshape(-1, 8)[:m].copy(),
+              order.read(np.uint32, timeout_ms=timeout_ms), depth.value)
+    for a in (src, nodes, order):
+        a.free()
+    return out
 
 
 class GpuBvh:

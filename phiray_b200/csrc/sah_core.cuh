@@ -1,0 +1,248 @@
+// The binned SAH builder's per-node steps (phiray src/bvh/sah.rs:25-189),
+// written once for the device kernels of sah.cu and for a host build of
+// the same code: every function here is plain arithmetic on one node or
+// one tree entry, so a host loop over the entries computes exactly what a
+// launch over them computes.
+//
+// The tree equals the reference's node for node: the same bins, sweep and
+// leaf rule per node, the same in-place (swap) partition of the node's
+// slots, and node indices in the order the reference's work stack hands
+// them out (children of the k-th inner node in depth-first, left-first
+// order at 2k + 1 and 2k + 2).
+#pragma once
+
+#include <stdint.h>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+#define SAH_HD __host__ __device__ __forceinline__
+
+namespace phx {
+namespace sah {
+
+constexpr uint32_t BINS = 16;        // sah.rs:26 BIN_COUNT
+constexpr float TRAVERSE = 1.0f;     // sah.rs:30
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+constexpr uint32_t LEAF_BIT = 0x80000000u;
+constexpr uint32_t MAX_DEPTH = 32;   // node.rs STACK: a node at depth 31 is a leaf
+
+// Rust f32::min / max: the argument that is not NaN wins.
+SAH_HD float rmin(float a, float b) { return a != a ? b : (b != b ? a : (a < b ? a : b)); }
+SAH_HD float rmax(float a, float b) { return a != a ? b : (b != b ? a : (a > b ? a : b)); }
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+SAH_HD Box empty_box() {
+    Box b;
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = 3.402823466e38f;    // f32::MAX
+        b.hi[k] = -3.402823466e38f;   // f32::MIN
+    }
+    return b;
+}
+
+SAH_HD void grow(Box& b, const Box& o) {
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = rmin(b.lo[k], o.lo[k]);
+        b.hi[k] = rmax(b.hi[k], o.hi[k]);
+    }
+}
+
+// A primitive's box from phiray's Aabb layout: lo.xyz, pad, hi.xyz, pad.
+SAH_HD Box prim_box(const float* aabb8) {
+    Box b;
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = aabb8[k];
+        b.hi[k] = aabb8[4 + k];
+    }
+    return b;
+}
+
+// sah.rs:32-35
+SAH_HD float area(const Box& b) {
+    float d[3];
+    for (int k = 0; k < 3; k++) d[k] = rmax(b.hi[k] - b.lo[k], 0.0f);
+    return 2.0f * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+}
+
+// sah.rs:68-79: the bin of centre c along axis k (Rust `as usize`
+// truncates toward zero and saturates; NaN gives 0).
+SAH_HD uint32_t bin_of(const float* c, const float* lo, const float* scale, int k) {
+    const float v = (c[k] - lo[k]) * scale[k];
+    const uint32_t b = (v != v || v <= 0.0f) ? 0u : (v >= 16.0f ? BINS - 1 : (uint32_t)v);
+    return b < BINS - 1 ? b : BINS - 1;
+}
+
+// sah.rs:114-189 split: the left count after reordering slots[0, count), or
+// NONE for a leaf. Serial over the node's slots.
+SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots, uint32_t count, uint32_t leaf) {
+    if (count <= 1) return NONE;
+    Box cbox = empty_box();
+    for (uint32_t j = 0; j < count; j++) {
+        const float* c = centres + 3 * (uint64_t)slots[j];
+        Box p;
+        for (int k = 0; k < 3; k++) p.lo[k] = p.hi[k] = c[k];
+        grow(cbox, p);
+    }
+    float lo[3], scale[3];
+    bool flat = true;
+    for (int k = 0; k < 3; k++) {
+        const float e = cbox.hi[k] - cbox.lo[k];
+        lo[k] = cbox.lo[k];
+        scale[k] = e > 0.0f ? (float)BINS * (1.0f - 1e-5f) / e : 0.0f;
+        if (scale[k] != 0.0f) flat = false;
+    }
+    if (flat) return count > leaf ? count / 2 : NONE;
+    uint32_t bcount[3][BINS];
+    Box bbox[3][BINS];
+    for (int k = 0; k < 3; k++)
+        for (uint32_t b = 0; b < BINS; b++) {
+            bcount[k][b] = 0;
+            bbox[k][b] = empty_box();
+        }
+    for (uint32_t j = 0; j < count; j++) {
+        const uint32_t i = slots[j];
+        const Box pb = prim_box(prims + 8 * (uint64_t)i);
+        for (int k = 0; k < 3; k++) {
+            const uint32_t at = bin_of(centres + 3 * (uint64_t)i, lo, scale, k);
+            bcount[k][at] += 1;
+            grow(bbox[k][at], pb);
+        }
+    }
+    bool have = false;
+    float best = 0.0f;
+    int best_k = 0;
+    uint32_t best_at = 0;
+    for (int k = 0; k < 3; k++) {
+        if (scale[k] == 0.0f) continue;
+        float right_area[BINS];
+        uint32_t right_count[BINS];
+        Box b = empty_box();
+        uint32_t c = 0;
+        for (uint32_t at = BINS - 1; at >= 1; at--) {
+            grow(b, bbox[k][at]);
+            c += bcount[k][at];
+            right_area[at] = area(b);
+            right_count[at] = c;
+        }
+        b = empty_box();
+        c = 0;
+        for (uint32_t at = 0; at + 1 < BINS; at++) {
+            grow(b, bbox[k][at]);
+            c += bcount[k][at];
+            const uint32_t rc = right_count[at + 1];
+            if (c == 0 || rc == 0) continue;
+            const float cost = area(b) * (float)c + right_area[at + 1] * (float)rc;
+            if (!have || cost < best) {
+                have = true;
+                best = cost;
+                best_k = k;
+                best_at = at;
+            }
+        }
+    }
+    Box bounds = empty_box();
+    for (uint32_t b = 0; b < BINS; b++) grow(bounds, bbox[0][b]);
+    if (!have) return count > leaf ? count / 2 : NONE;
+    const float parent = rmax(area(bounds), 1.17549435e-38f);  // f32::MIN_POSITIVE
+    if (count <= leaf && TRAVERSE + best / parent >= (float)count) return NONE;
+    uint32_t m = 0;
+    for (uint32_t j = 0; j < count; j++) {
+        if (bin_of(centres + 3 * (uint64_t)slots[j], lo, scale, best_k) <= best_at) {
+            const uint32_t t = slots[j];
+            slots[j] = slots[m];
+            slots[m] = t;
+            m++;
+        }
+    }
+    return (m == 0 || m == count) ? count / 2 : m;
+}
+
+// One node of the tree under construction (temporary numbering).
+struct TNode {
+    uint32_t start, end, depth;
+    uint32_t left, right;  // temporary ids of the children; NONE for a leaf
+};
+
+// Where to put new nodes: a counter of temporary ids and the next level's
+// list. `add` is an atomic add on the device and a plain one on the host.
+template <class Add>
+SAH_HD void process(uint32_t t, TNode* tn, const float* prims, const float* centres, uint32_t* order, uint32_t leaf,
+                    uint32_t* tcount, uint32_t* next, uint32_t* next_count, Add add) {
+    TNode nd = tn[t];
+    const uint32_t m = nd.depth + 1 >= MAX_DEPTH
+                           ? NONE
+                           : split(prims, centres, order + nd.start, nd.end - nd.start, leaf);
+    if (m == NONE) {
+        nd.left = nd.right = NONE;
+    } else {
+        const uint32_t c = add(tcount, 2u);
+        tn[c] = TNode{nd.start, nd.start + m, nd.depth + 1, NONE, NONE};
+        tn[c + 1] = TNode{nd.start + m, nd.end, nd.depth + 1, NONE, NONE};
+        nd.left = c;
+        nd.right = c + 1;
+        const uint32_t p = add(next_count, 2u);
+        next[p] = c;
+        next[p + 1] = c + 1;
+    }
+    tn[t] = nd;
+}
+
+// Inner nodes in t's subtree, t included (children's counts first).
+SAH_HD void count_inner(uint32_t t, const TNode* tn, uint32_t* inner) {
+    const TNode nd = tn[t];
+    inner[t] = nd.left == NONE ? 0u : 1u + inner[nd.left] + inner[nd.right];
+}
+
+// Top down: an inner node of depth-first rank r has its children at final
+// indices 2r + 1 and 2r + 2 (sah.rs:95-105's work stack pops the left child
+// first and hands out two indices per inner node).
+SAH_HD void place(uint32_t t, const TNode* tn, const uint32_t* inner, uint32_t* rank, uint32_t* final_index) {
+    const TNode nd = tn[t];
+    if (nd.left == NONE) return;
+    const uint32_t r = rank[t];
+    rank[nd.left] = r + 1;
+    rank[nd.right] = r + 1 + inner[nd.left];
+    final_index[nd.left] = 2 * r + 1;
+    final_index[nd.right] = 2 * r + 2;
+}
+
+// The node at its final index, bounds from its children or its primitives
+// (Bvh::refit, build.rs:180-194: unions, exact in any order). `boxes` holds
+// each temporary node's bounds for its parent; children come first.
+SAH_HD void emit(uint32_t t, const TNode* tn, const uint32_t* final_index, const float* prims, const uint32_t* order,
+                 Box* boxes, float* nodes) {
+    const TNode nd = tn[t];
+    Box b = empty_box();
+    uint32_t lo_i, hi_i;
+    if (nd.left == NONE) {
+        for (uint32_t s = nd.start; s < nd.end; s++) grow(b, prim_box(prims + 8 * (uint64_t)order[s]));
+        lo_i = nd.start | LEAF_BIT;
+        hi_i = nd.end;
+    } else {
+        b = boxes[nd.left];
+        grow(b, boxes[nd.right]);
+        lo_i = final_index[nd.left];
+        hi_i = final_index[nd.right];
+    }
+    boxes[t] = b;
+    float* o = nodes + 8 * (uint64_t)final_index[t];
+    uint32_t* u = (uint32_t*)o;
+    o[0] = b.lo[0];
+    o[1] = b.lo[1];
+    o[2] = b.lo[2];
+    u[3] = lo_i;
+    o[4] = b.hi[0];
+    o[5] = b.hi[1];
+    o[6] = b.hi[2];
+    u[7] = hi_i;
+}
+
+}  // namespace sah
+}  // namespace phx

@@ -189,3 +189,28 @@ def test_pass_replays_reference_kernels(gpu, orc):
     for i in orc.reachable(nodes):
         assert np.array_equal(got[i], nodes[i])
     assert ps.compiled() == 1
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 5000, 70000])
+@pytest.mark.parametrize("leaf", [1, 4])
+def test_sah_build_equals_the_reference_tree(gpu, orc, n, leaf):
+    """phx_bvh_build_sah == Bvh::build_sah's restatement, word for word:
+    nodes with their bounds, slot order, depth."""
+    from phiray_b200.bvh import build_sah
+
+    p = gen.test_prims(n)
+    want_nodes, want_order, want_depth = orc.build_sah(p, leaf)
+    got = build_sah(gpu, p, leaf)
+    assert got.depth == want_depth
+    assert np.array_equal(got.order, want_order)
+    assert np.array_equal(got.nodes.view(np.uint32), want_nodes.view(np.uint32))
+
+
+def test_sah_build_on_a_mesh(gpu, orc):
+    from phiray_b200.bvh import build_sah
+
+    p = gen.bvh_prims(20000, 0.0)
+    want_nodes, want_order, want_depth = orc.build_sah(p, 4)
+    got = build_sah(gpu, p, 4)
+    assert got.depth == want_depth and np.array_equal(got.order, want_order)
+    assert np.array_equal(got.nodes.view(np.uint32), want_nodes.view(np.uint32))
