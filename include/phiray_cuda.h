@@ -251,15 +251,20 @@ int32_t phx_morton(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t* cod
 int32_t phx_sort_codes(phx_ctx ctx, const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted);
 /* phx_sort_codes without allocating: no counterpart in the reference. For
  * callers that cannot allocate device memory at call time — a host that
- * hands the renderer a fixed, pre-reserved budget, a frame loop that must not
- * stall on cudaMalloc/cudaFree, or work recorded into a CUDA graph. The
- * sort's working memory is one array compiled into the library
- * (~9.4 MB, held on every GPU that loads it until the process exits), so n
- * is at most PHX_SORT_STATIC_MAX (larger n: PHX_ERR_INVALID). The first call
- * on a device looks up that array's device address; make it before any
- * stream capture. Stream-ordered and does not wait: synchronise before
- * reading order/sorted. All calls share the array, so calls whose work
- * overlaps on the GPU (other streams, other host threads) race. */
+ * hands the renderer a fixed, pre-reserved budget and owns every other byte
+ * of the device, or a frame loop that must not stall on cudaMalloc/cudaFree
+ * (both can wait for the whole device). The sort's working memory is one
+ * array compiled into the library (~9.4 MB, held on every GPU that loads it
+ * until the process exits), so n is at most PHX_SORT_STATIC_MAX (larger n:
+ * PHX_ERR_INVALID, nothing launched). The first call on a device looks up
+ * that array's device address and keeps it for the life of the process: make
+ * that first call before any stream capture, and do not reset the device
+ * (cudaDeviceReset) while the library is loaded. Stream-ordered and does not
+ * wait: synchronise before reading order/sorted. A failure inside the sort's
+ * kernels (a look-back wait that gave up) is reported by the next call that
+ * reads the context's status, such as phx_ctx_wait. All calls share the
+ * array, so calls whose work overlaps on the GPU (other streams, other host
+ * threads) race. */
 #define PHX_SORT_STATIC_MAX (1u << 20)
 int32_t phx_sort_codes_static(phx_ctx ctx, const uint32_t* codes, uint32_t n, uint32_t* order, uint32_t* sorted);
 /* bvh::Karras (kernel.rs:65-117): links[i] for i < n-1 from sorted codes. */

@@ -111,7 +111,7 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
         const uint32_t next = off[lv] + len[lv];
         PHX_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, s));
         k_sah_level<<<blocks_of(len[lv], 64), 64, 0, s>>>(L + off[lv], len[lv], T, P, (const float*)centres.ptr, order,
-                                                         leaf ? leaf : 4, cnt, L + next, cnt + 1);
+                                                         leaf, cnt, L + next, cnt + 1);
         PHX_CUDA(cudaGetLastError());
         uint32_t opened = 0;
         PHX_CUDA(cudaMemcpyAsync(&opened, cnt + 1, 4, cudaMemcpyDeviceToHost, s));

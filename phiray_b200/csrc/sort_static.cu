@@ -2,10 +2,9 @@
 // allocation at call time.
 //
 // Who needs it: code that must not call cudaMalloc — a host that reserved
-// its device memory up front and hands the renderer a fixed budget, a
+// its device memory up front and hands the renderer a fixed budget, or a
 // frame loop that must not stall (cudaMalloc and cudaFree can wait for the
-// whole device), or work being recorded into a CUDA graph, where allocating
-// calls are not allowed. Such callers pass their input and output arrays;
+// whole device). Such callers pass their input and output arrays;
 // the sort's working memory (the ping-pong key/value arrays, the digit
 // histograms, the tile tickets and the look-back words) comes from one
 // array of fixed size compiled into this library.
@@ -34,7 +33,10 @@ constexpr size_t TOTAL_WORDS = ZERO_WORDS + 2 * (size_t)MAX_KEYS;
 static __device__ __align__(256) uint32_t g_sort_scratch[TOTAL_WORDS];
 
 std::mutex g_lock;
-uint32_t* g_addr[64] = {};  // device address of g_sort_scratch, per device
+// Device address of g_sort_scratch, per device, looked up once for the life
+// of the process. A device reset unloads the module and leaves these stale,
+// so the library must not outlive a cudaDeviceReset of a device it sorted on.
+uint32_t* g_addr[64] = {};
 
 // The device address of the array on the current device, looked up once per
 // device (the first call on a device does this; make that first call before
@@ -72,5 +74,8 @@ extern "C" int32_t phx_sort_codes_static(phx_ctx ctx, const uint32_t* codes, uin
     uint32_t* alt_vals = alt_keys + MAX_KEYS;
     // The array keeps the last call's contents: the counters start at zero.
     PHX_CUDA(cudaMemsetAsync(base, 0, ZERO_WORDS * 4, c->stream));
+    // Launch errors come back here; a look-back wait that gives up inside the
+    // kernels sets the context's status word, which the next status read
+    // (phx_ctx_wait) reports.
     return phx::enqueue_sort_raw(c, codes, n, order, sorted, alt_keys, alt_vals, hist, tickets, lookback, MAX_TILES);
 }

@@ -37,7 +37,7 @@ extern "C" uint32_t emul_build_sah(const float* prims, uint32_t n, uint32_t leaf
         const uint32_t next = off[lv] + len[lv];
         uint32_t opened = 0;
         for (uint32_t k = 0; k < len[lv]; k++)
-            process(lists[off[lv] + k], tn.data(), prims, centres.data(), order, leaf ? leaf : 4, &tcount,
+            process(lists[off[lv] + k], tn.data(), prims, centres.data(), order, leaf, &tcount,
                     lists.data() + next, &opened, add);
         if (opened == 0) break;
         off.push_back(next);

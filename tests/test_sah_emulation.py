@@ -38,7 +38,7 @@ def emul(tmp_path_factory):
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 7, 100, 5000, 70000])
-@pytest.mark.parametrize("leaf", [1, 4])
+@pytest.mark.parametrize("leaf", [0, 1, 4])
 def test_device_steps_build_the_reference_tree(orc, emul, n, leaf):
     p = gen.test_prims(n)
     want_nodes, want_order, want_depth = orc.build_sah(p, leaf)

@@ -1,9 +1,9 @@
 """phx_sort_codes_static: the radix sort that allocates nothing at call time.
 
 Some callers cannot allocate device memory when they sort — a host that gave
-the renderer a fixed budget up front, a frame loop that must not stall on
-cudaMalloc/cudaFree, work recorded into a CUDA graph. This entry point takes
-its working memory from one fixed array compiled into the library instead.
+the renderer a fixed budget up front, or a frame loop that must not stall on
+cudaMalloc/cudaFree. This entry point takes its working memory from one fixed
+array compiled into the library instead.
 Its output must be the allocating sort's (phx_sort_codes), bit for bit, on
 two calls in a row (the shared array keeps the first call's contents, so the
 second call shows that everything that must start at zero does). This file
@@ -42,6 +42,8 @@ def test_static_sort_matches_the_allocating_sort_twice():
             d = torch.tensor(codes.view(np.int32), device="cuda")
             want = _sort(lib, ctx, lib.phx_sort_codes, d, n, torch)
             got = _sort(lib, ctx, lib.phx_sort_codes_static, d, n, torch)
+            # errors inside the sort's kernels surface at the next status read
+            assert lib.phx_ctx_wait(ctx, 0) == 0
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
             assert np.array_equal(got[0], np.argsort(codes, kind="stable").astype(np.uint32))
         # beyond the stated maximum: a clear error, nothing launched
