@@ -101,6 +101,14 @@ void* phx_ctx_stream(phx_ctx ctx);
 /* Enqueue on a caller's stream (e.g. one shared with another library);
  * NULL returns to the context's own stream. */
 int32_t phx_ctx_set_stream(phx_ctx ctx, void* stream);
+/* The library's bounded device waits made to run out, for tests of the
+ * failure path (no reference counterpart: phiray's WGSL never waits on
+ * another invocation). which 0: the mbarrier wait of the tensor-core engine;
+ * 1: the radix sort's look-back wait. The wait polls a flag nothing sets
+ * (satisfied = 0) at most `limit` times, sets the context's status word and
+ * returns; the call then reports PHX_ERR_KERNEL ("spin limit") and the
+ * context stays usable. satisfied = 1 sets the flag first: PHX_OK. Waits. */
+int32_t phx_selftest_wait(phx_ctx ctx, int32_t which, uint32_t limit, int32_t satisfied);
 /* Text of the calling thread's last error; returns its length. */
 int32_t phx_last_error(char* buf, size_t len);
 /* Library version string, for loaders. */
@@ -446,7 +454,8 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
  * still written at its ray's index. */
 #define PHX_WALK_SORTED 2u
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
-/* Tracer::set_samples: the sample target `sample` stops at. */
+/* Tracer::set_samples: the sample target `sample` stops at (32 until set,
+ * Tracer::SAMPLE_COUNT, src/trace/mod.rs:129). */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
 /* Tracer::sample / sample_in (src/trace/sample.rs:94-249): one more sample
  * of `cam` at w x h — frame 0 on a new view, frame + 1 on the same one —

@@ -20,8 +20,14 @@
  *   - sin/cos: Cody-Waite reduction by pi/2 in three parts, then the
  *     Taylor series on [-pi/4, pi/4] and a quadrant swap.
  *   - pow(x, y) = exp2(y log2 x) for x > 0; exp(x) = exp2(x log2 e).
- * Accuracy is a few ulp over the ranges the kernels use, which is more
- * than a path tracer needs; the point is sameness, not the last ulp.
+ * Accuracy against float64, measured over 400,000 arguments a function
+ * (tests/test_math_accuracy.py holds these bounds): exp2 <= 1.5 ulp on
+ * [-126, 127]; log2 <= 3.5 ulp on [1e-30, 1e30]; sin and cos <= 1.5 x 2^-24
+ * absolute on [-100, 100]; pow(x, y) <= 5 + 1.5 |y log2 x| ulp and exp(x)
+ * <= 3 + 1.5 |x log2 e| ulp (the product's rounding is carried into the
+ * exponent: ~10 ulp for the sRGB curve's pow(x, 1/2.4), more for large
+ * results). More than a path tracer needs; the point is sameness, not the
+ * last ulp: the device build returns the host build's bits.
  *
  * Build rule: every file that includes this must be compiled without
  * floating-point contraction (nvcc --fmad=false, gcc -ffp-contract=off),

@@ -123,6 +123,12 @@ void orc_primary(const float* verts, const uint32_t* faces, uint32_t nfaces, con
 void orc_trace_rays(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats, uint32_t leaf,
                     const float* rays, uint32_t n, float* hits, int any_hit);
 
+/* tri.rs:51-114: the watertight test of one ray against one triangle;
+ * returns 1 with out = (t, u, v) on a hit. */
+int orc_tri_hit(const float* a, const float* b, const float* c, const float* o, const float* d, float* out);
+/* phiray_math.h on the host: fn 0 exp2, 1 log2, 2 sin, 3 cos, 4 pow, 5 exp. */
+void orc_math(int fn, const float* x, const float* y, float* out, uint32_t n);
+
 #ifdef __cplusplus
 }
 #endif

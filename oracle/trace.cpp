@@ -8,9 +8,9 @@
 // util.wgsl's emit and guide do (read-modify-write per sample).
 //
 // Only the features the synthetic configs use are restated; the rest
-// (textures, procedural slots, environment images, depth of field, adaptive
-// sampling, the grid, film transparency, other pixel filters and view
-// transforms) must be off in the Camera.
+// (textures, procedural slots, environment images, depth of field, film
+// transparency, other pixel filters and view transforms) must be off in the
+// Camera.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -851,6 +851,83 @@ void emit(World& W, uint32_t i, V3 lin, V3 over_rgb, float over_a, float cover, 
 
 float srgb_to_linear1(float c) { return c <= 0.04045f ? c / 12.92f : pm_pow((c + 0.055f) / 1.055f, 2.4f); }
 
+// ---- util.wgsl:185-272 the floor grid overlay ----
+
+struct Over {
+    V3 c;
+    float a;
+};
+
+// floor_over: the floor's lines and its X and Y axes, premultiplied.
+Over floor_over(const phx_camera* p, V3 o, V3 d, float t_hit, float px_) {
+    if (p->grid <= 0.0f || std::fabs(d.z) < 1e-6f) return Over{v3(0.0f), 0.0f};
+    const float t = -o.z / d.z;
+    if (t <= 0.0f || t >= t_hit) return Over{v3(0.0f), 0.0f};
+    const V3 q = o + d * t;
+    float foot = px_;
+    if (p->persp != 0u) foot = px_ * t * p->units / p->dist;
+    const float want = foot * 24.0f;
+    const float lg = pm_log2(fmaxw(want, 1e-9f)) / pm_log2(10.0f);
+    const float lvl = std::floor(lg);
+    const float f = lg - lvl;
+    const float g0 = pm_pow(10.0f, lvl);
+    const float g1 = g0 * 10.0f;
+    const float half_w = foot * 0.5f;
+    const float aa = foot;
+    const float c0x = q.x / g0, c0y = q.y / g0;
+    const float c1x = q.x / g1, c1y = q.y / g1;
+    // WGSL round: to nearest, ties to even
+    const float d0x = std::fabs(c0x - std::nearbyint(c0x)) * g0, d0y = std::fabs(c0y - std::nearbyint(c0y)) * g0;
+    const float d1x = std::fabs(c1x - std::nearbyint(c1x)) * g1, d1y = std::fabs(c1y - std::nearbyint(c1y)) * g1;
+    const float l0 = fmaxw(1.0f - smoothstep(half_w, half_w + aa, d0x), 1.0f - smoothstep(half_w, half_w + aa, d0y));
+    const float l1 = fmaxw(1.0f - smoothstep(half_w, half_w + aa, d1x), 1.0f - smoothstep(half_w, half_w + aa, d1y));
+    const float fine = (1.0f - f) * (1.0f - f);
+    const float line = fmaxw(l0 * fine * 0.6f, l1);
+    const float horizon = clampf(std::fabs(d.z) * 4.0f, 0.0f, 1.0f);
+    float depth = 1.0f;
+    if (p->persp != 0u) {
+        const float r = t * p->units / (p->dist * 6.0f);
+        depth = 1.0f / (1.0f + r * r);
+    }
+    const float fade = horizon * depth;
+    const float w0 = line * p->grid_color[3] * fade * ((p->grid_hide & 1u) != 0u ? 0.0f : 1.0f);
+    V3 c = v3(p->grid_color[0], p->grid_color[1], p->grid_color[2]) * w0;
+    float a = w0;
+    const float ax = 1.0f - smoothstep(half_w, half_w + aa, std::fabs(q.y));
+    const float ay = 1.0f - smoothstep(half_w, half_w + aa, std::fabs(q.x));
+    const float w1 = ax * 0.85f * fade * ((p->grid_hide & 2u) != 0u ? 0.0f : 1.0f);
+    c = c * (1.0f - w1) + v3(0.85f, 0.3f, 0.33f) * w1;
+    a = a * (1.0f - w1) + w1;
+    const float w2 = ay * 0.85f * fade * ((p->grid_hide & 4u) != 0u ? 0.0f : 1.0f);
+    c = c * (1.0f - w2) + v3(0.47f, 0.72f, 0.2f) * w2;
+    a = a * (1.0f - w2) + w2;
+    return Over{c, a};
+}
+
+// z_axis_over: the vertical line through the origin.
+Over z_axis_over(const phx_camera* p, V3 o, V3 d, float t_hit, float px_) {
+    const float a = d.x * d.x + d.y * d.y;
+    if (a < 1e-12f) return Over{v3(0.0f), 0.0f};
+    const float t = -(o.x * d.x + o.y * d.y) / a;
+    if (t <= 0.0f || t >= t_hit) return Over{v3(0.0f), 0.0f};
+    float foot = px_;
+    if (p->persp != 0u) foot = px_ * t * p->units / p->dist;
+    const V3 at = o + d * t;
+    const float r = std::sqrt(at.x * at.x + at.y * at.y);
+    const float w = (1.0f - smoothstep(foot * 0.5f, foot * 1.5f, r)) * 0.85f;
+    return Over{v3(0.25f, 0.53f, 0.92f) * w, w};
+}
+
+// grid_over: the floor, then the Z axis laid over it when asked for.
+Over grid_over(const phx_camera* p, V3 o, V3 d, float t_hit, float px_) {
+    Over g = floor_over(p, o, d, t_hit, px_);
+    if (p->grid > 0.0f && (p->grid_hide & 8u) != 0u) {
+        const Over z = z_axis_over(p, o, d, t_hit, px_);
+        g = Over{g.c * (1.0f - z.a) + z.c, g.a * (1.0f - z.a) + z.a};
+    }
+    return g;
+}
+
 struct CamRay {
     V3 o, d;
 };
@@ -894,6 +971,11 @@ void shade_main(World& W, uint32_t i) {
     uint32_t seed = hash(i * 9781u + W.frame * 6271u + 1u);
     const CamRay cr = camera_ray(W, i, &seed);
     V3 o = cr.o, d = cr.d;
+    // shade.wgsl:96-103: a pixel's footprint for the grid, the first ray and
+    // the first surface's distance
+    const float pix = 1.0f / (p->scale * p->units * (float)p->w);
+    const V3 o0 = o, d0 = d;
+    float first_t = INF;
     const float across = (float)(i % p->w) / fmaxw((float)p->w * 0.5f, 1.0f);
     const V3 sky = v3(p->sky[0], p->sky[1], p->sky[2]) + v3(p->sky[3]) * (1.0f - clampf(across, 0.0f, 1.0f));
     px[25 * N + i] = 0u;  // outline_store(i, 0)
@@ -906,14 +988,18 @@ void shade_main(World& W, uint32_t i) {
         const Hit h = trace(W, o, d, INF, false);
         if (h.tri == NONE) {
             if (bounce == 0u) {
+                const Over g = grid_over(p, o, d, INF, pix);
                 guide(W, i, v3(srgb_to_linear1(sky.x), srgb_to_linear1(sky.y), srgb_to_linear1(sky.z)), -d, -1.0f);
-                emit(W, i, v3(0.0f), sky * (1.0f - 0.0f) + v3(0.0f), 1.0f, 1.0f, 1.0f);
+                emit(W, i, v3(0.0f), sky * (1.0f - g.a) + g.c, 1.0f, 1.0f, 1.0f);
                 return;
             }
             col += thr * env_at(W, d);
             break;
         }
-        if (bounce == 0u) px[25 * N + i] = h.inst + 1u;
+        if (bounce == 0u) {
+            first_t = h.t;
+            px[25 * N + i] = h.inst + 1u;
+        }
         const Tri t = tri_of(W, h.tri);
         const float w = 1.0f - h.u - h.v;
         const V3 hit = o + d * h.t;
@@ -1005,7 +1091,8 @@ void shade_main(World& W, uint32_t i) {
         d = cone_dir(normalize(nd), s.rough * s.rough, &seed);
         if (maxc(thr) < 0.01f) break;
     }
-    emit(W, i, col, v3(0.0f), 0.0f, 1.0f, 0.0f);
+    const Over g = grid_over(p, o0, d0, first_t, pix);
+    emit(W, i, col, g.c, g.a, 1.0f, 0.0f);
 }
 
 void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
@@ -1279,6 +1366,33 @@ void orc_trace_rays(const float* verts, const uint32_t* faces, uint32_t nfaces, 
         hits[4 * i + 1] = f_of(h.tri == NONE ? NONE : S.order[h.tri]);
         hits[4 * i + 2] = h.u;
         hits[4 * i + 3] = h.v;
+    }
+}
+
+// The watertight ray/triangle test alone (tri.rs:51-114, bvh.wgsl
+// ray_space + tri_t): 1 and (t, u, v) on a hit, 0 otherwise.
+int orc_tri_hit(const float* a, const float* b, const float* c, const float* o, const float* d, float* out) {
+    float h[3];
+    tri_t(v3(a[0], a[1], a[2]), v3(b[0], b[1], b[2]), v3(c[0], c[1], c[2]), v3(o[0], o[1], o[2]),
+          ray_space(v3(d[0], d[1], d[2])), h);
+    out[0] = h[0];
+    out[1] = h[1];
+    out[2] = h[2];
+    return h[0] < INF ? 1 : 0;
+}
+
+// The shared transcendental functions (phiray_math.h) on the host, for
+// their accuracy tests: fn 0 exp2, 1 log2, 2 sin, 3 cos, 4 pow(x, y), 5 exp.
+void orc_math(int fn, const float* x, const float* y, float* out, uint32_t n) {
+    for (uint32_t i = 0; i < n; i++) {
+        switch (fn) {
+            case 0: out[i] = pm_exp2(x[i]); break;
+            case 1: out[i] = pm_log2(x[i]); break;
+            case 2: out[i] = pm_sin(x[i]); break;
+            case 3: out[i] = pm_cos(x[i]); break;
+            case 4: out[i] = pm_pow(x[i], y[i]); break;
+            default: out[i] = pm_exp(x[i]); break;
+        }
     }
 }
 

@@ -93,6 +93,23 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     return OUT
 
 
+def build_test_probe(verbose: bool = False) -> Path:
+    """The tests' device probe of the shared math (tests/mathprobe.cu) as
+    tests/libmathprobe.so, with the library's flags. Test infrastructure:
+    nothing in the package loads it."""
+    src = HERE.parent / "tests" / "mathprobe.cu"
+    out = src.with_name("libmathprobe.so")
+    deps = [src, HERE.parent / "include" / "phiray_math.h"]
+    if _stale(out, deps):
+        cmd = [nvcc(), *flags(), "-shared", "-o", str(out), str(src), "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode != 0:
+            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed on tests/mathprobe.cu")
+    return out
+
+
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv, force="--force" in sys.argv, ptxas_info="--ptxas" in sys.argv)
     print(OUT)

@@ -43,21 +43,11 @@ constexpr int TILE = RADIX_THREADS * RADIX_ITEMS;
 constexpr int WARPS = RADIX_THREADS / 32;
 constexpr int PASSES = 4;
 static_assert(TILE == LBVH_TILE && PASSES == LBVH_PASSES, "lbvh.cuh and bvh.cu agree");
-constexpr uint32_t FLAG_AGG = 1u << 30;
-constexpr uint32_t FLAG_INC = 2u << 30;
-constexpr uint32_t VALUE_MASK = (1u << 30) - 1;
+constexpr uint32_t FLAG_AGG = LOOKBACK_AGG;
+constexpr uint32_t FLAG_INC = LOOKBACK_INC;
+constexpr uint32_t VALUE_MASK = LOOKBACK_VALUE;
 constexpr uint32_t SPIN_LIMIT = 1u << 22;
 constexpr uint32_t MAX_PRIMS = 1u << 30;  // look-back words hold 30-bit counts
-
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 
 // morton's spread (node.rs:98-104; WGSL kernel.rs:33-39). fmaxf(NaN, 0) is
 // 0, as Rust's `NaN as u64` is.
@@ -295,23 +285,7 @@ __global__ void __launch_bounds__(RADIX_THREADS) k_radix_pass(const uint32_t* __
         st_relaxed(mine, FLAG_INC | run);
     } else {
         st_relaxed(mine, FLAG_AGG | run);
-        int t = (int)tile - 1;
-        uint32_t spins = 0;
-        while (t >= 0) {
-            const uint32_t v = ld_relaxed(lookback + (size_t)t * 256 + d);
-            const uint32_t flag = v & ~VALUE_MASK;
-            if (flag == 0) {
-                if (++spins > SPIN_LIMIT) {
-                    atomicOr(status, STATUS_SPIN_LIMIT);
-                    break;
-                }
-                if (spins > 32) __nanosleep(64);
-                continue;
-            }
-            prefix += v & VALUE_MASK;
-            if (flag == FLAG_INC) break;
-            t--;
-        }
+        prefix = lookback_prefix(lookback, tile, d, SPIN_LIMIT, status);
         st_relaxed(mine, FLAG_INC | ((prefix + run) & VALUE_MASK));
     }
     const uint32_t tile_off = block_exclusive_scan(run, s_tmp);

@@ -21,6 +21,52 @@ struct Gate {
 #endif
 };
 
+#ifdef __CUDACC__
+// Decoupled look-back words of the radix sort: a tile's count for one digit
+// with a flag — its own count only (AGG) or the inclusive prefix (INC).
+constexpr uint32_t LOOKBACK_AGG = 1u << 30;
+constexpr uint32_t LOOKBACK_INC = 2u << 30;
+constexpr uint32_t LOOKBACK_VALUE = (1u << 30) - 1;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// The exclusive prefix of digit d for tile `tile` (> 0): walks back over
+// the earlier tiles' words (256 per tile), adding aggregates until an
+// inclusive prefix. A word not yet written is polled again, at most `limit`
+// times in all; past that the wait gives up, sets STATUS_SPIN_LIMIT in
+// *status and returns what it has (the caller's result is then wrong and the
+// host reports the status instead of it).
+__device__ __forceinline__ uint32_t lookback_prefix(const uint32_t* lookback, uint32_t tile, uint32_t d,
+                                                    uint32_t limit, uint32_t* status) {
+    uint32_t prefix = 0, spins = 0;
+    int t = (int)tile - 1;
+    while (t >= 0) {
+        const uint32_t v = ld_relaxed(lookback + (size_t)t * 256 + d);
+        const uint32_t flag = v & ~LOOKBACK_VALUE;
+        if (flag == 0) {
+            if (++spins > limit) {
+                atomicOr(status, STATUS_SPIN_LIMIT);
+                break;
+            }
+            if (spins > 32) __nanosleep(64);
+            continue;
+        }
+        prefix += v & LOOKBACK_VALUE;
+        if (flag == LOOKBACK_INC) break;
+        t--;
+    }
+    return prefix;
+}
+#endif
+
 struct BvhWork {
     uint32_t cap = 0;  // prims the arrays hold
     DevMem prims, codes, sorted, order, alt_keys, alt_vals, partial, zeroed, links, parent, nodes, starts, counters,

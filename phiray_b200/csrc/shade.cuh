@@ -94,6 +94,11 @@ struct Frame {
     // pixel k.
     uint32_t adapt_on, adapt_min, adapt_step, adapt_list;
     float adapt_thr;
+    // The floor grid overlay (util.wgsl:185-272): Camera.grid (0 = off),
+    // grid_color, grid_hide.
+    float grid;
+    float4 grid_color;
+    uint32_t grid_hide;
 };
 
 // ---- util.wgsl ----
@@ -718,6 +723,85 @@ __device__ __forceinline__ Shadowed rig_query(const Frame& F, uint32_t k, const 
     }
     const f3 rim = normalize(F.up * 0.6f - F.back * 0.8f + F.right * 0.2f);
     return Shadowed{brdf(s, rim, mk(0.9f)), rim, INF};
+}
+
+// ---- util.wgsl:185-272: the floor grid as an overlay, premultiplied ----
+
+struct Over {
+    f3 c;
+    float a;
+};
+
+// floor_over: Blender's floor grid on z = 0 (lines every power of ten, the
+// finer level fading as its cells shrink, anti-aliased over one pixel's
+// footprint, faded toward the horizon) and its X and Y axes.
+__device__ __forceinline__ Over floor_over(const Frame& F, f3 o, f3 d, float t_hit, float px) {
+    if (F.grid <= 0.0f || fabsf(d.z) < 1e-6f) return Over{mk(0.0f), 0.0f};
+    const float t = -o.z / d.z;
+    if (t <= 0.0f || t >= t_hit) return Over{mk(0.0f), 0.0f};
+    const f3 q = o + d * t;
+    float foot = px;
+    if (F.persp != 0u) foot = px * t * F.units / F.dist;
+    const float want = foot * 24.0f;
+    const float lg = pm_log2(fmaxf(want, 1e-9f)) / pm_log2(10.0f);
+    const float lvl = floorf(lg);
+    const float f = lg - lvl;
+    const float g0 = pm_pow(10.0f, lvl);
+    const float g1 = g0 * 10.0f;
+    const float half_w = foot * 0.5f;
+    const float aa = foot;
+    const float c0x = q.x / g0, c0y = q.y / g0, c1x = q.x / g1, c1y = q.y / g1;
+    // WGSL round(): to nearest, ties to even, as rintf
+    const float d0x = fabsf(c0x - rintf(c0x)) * g0, d0y = fabsf(c0y - rintf(c0y)) * g0;
+    const float d1x = fabsf(c1x - rintf(c1x)) * g1, d1y = fabsf(c1y - rintf(c1y)) * g1;
+    const float l0 = fmaxf(1.0f - smoothstepf(half_w, half_w + aa, d0x), 1.0f - smoothstepf(half_w, half_w + aa, d0y));
+    const float l1 = fmaxf(1.0f - smoothstepf(half_w, half_w + aa, d1x), 1.0f - smoothstepf(half_w, half_w + aa, d1y));
+    const float fine = (1.0f - f) * (1.0f - f);
+    const float line = fmaxf(l0 * fine * 0.6f, l1);
+    const float horizon = clampf(fabsf(d.z) * 4.0f, 0.0f, 1.0f);
+    float depth = 1.0f;
+    if (F.persp != 0u) {
+        const float r = t * F.units / (F.dist * 6.0f);
+        depth = 1.0f / (1.0f + r * r);
+    }
+    const float fade = horizon * depth;
+    const float w0 = line * F.grid_color.w * fade * ((F.grid_hide & 1u) != 0u ? 0.0f : 1.0f);
+    f3 c = mk(F.grid_color.x, F.grid_color.y, F.grid_color.z) * w0;
+    float a = w0;
+    const float ax = 1.0f - smoothstepf(half_w, half_w + aa, fabsf(q.y));
+    const float ay = 1.0f - smoothstepf(half_w, half_w + aa, fabsf(q.x));
+    const float w1 = ax * 0.85f * fade * ((F.grid_hide & 2u) != 0u ? 0.0f : 1.0f);
+    c = c * (1.0f - w1) + mk(0.85f, 0.3f, 0.33f) * w1;
+    a = a * (1.0f - w1) + w1;
+    const float w2 = ay * 0.85f * fade * ((F.grid_hide & 4u) != 0u ? 0.0f : 1.0f);
+    c = c * (1.0f - w2) + mk(0.47f, 0.72f, 0.2f) * w2;
+    a = a * (1.0f - w2) + w2;
+    return Over{c, a};
+}
+
+// z_axis_over: the vertical line through the origin, within half a pixel.
+__device__ __forceinline__ Over z_axis_over(const Frame& F, f3 o, f3 d, float t_hit, float px) {
+    const float a = d.x * d.x + d.y * d.y;
+    if (a < 1e-12f) return Over{mk(0.0f), 0.0f};
+    const float t = -(o.x * d.x + o.y * d.y) / a;
+    if (t <= 0.0f || t >= t_hit) return Over{mk(0.0f), 0.0f};
+    float foot = px;
+    if (F.persp != 0u) foot = px * t * F.units / F.dist;
+    const f3 at = o + d * t;
+    const float r = sqrtf(at.x * at.x + at.y * at.y);
+    const float w = (1.0f - smoothstepf(foot * 0.5f, foot * 1.5f, r)) * 0.85f;
+    return Over{mk(0.25f, 0.53f, 0.92f) * w, w};
+}
+
+// grid_over: nothing unless the camera turns the grid on.
+__device__ __noinline__ Over grid_over(const Frame& F, f3 o, f3 d, float t_hit) {
+    const float px = 1.0f / (F.scale * F.units * (float)F.w);
+    Over g = floor_over(F, o, d, t_hit, px);
+    if (F.grid > 0.0f && (F.grid_hide & 8u) != 0u) {
+        const Over z = z_axis_over(F, o, d, t_hit, px);
+        g = Over{g.c * (1.0f - z.a) + z.c, g.a * (1.0f - z.a) + z.a};
+    }
+    return g;
 }
 
 __device__ __forceinline__ f3 rig_fill(const Frame& F, const Surf& s) {

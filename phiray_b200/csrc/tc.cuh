@@ -74,10 +74,15 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
 }
 
-// Bounded wait on an mbarrier phase; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+// One arrival on an mbarrier (this thread's).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false when `limit` polls ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t limit = WAIT_LIMIT) {
     const uint32_t a = smem_addr(bar);
-    for (uint32_t it = 0; it < WAIT_LIMIT; it++) {
+    for (uint32_t it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

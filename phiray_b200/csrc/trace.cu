@@ -358,14 +358,29 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                 acc.film += 1.0f;
                 acc.lin += mk(0.0f);
                 if (F.adapt_on && (frame & 1u)) acc.half = acc.half + mk(0.0f) * 2.0f;
-                acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                if (F.grid > 0.0f) {
+                    const Over g = grid_over(F, o, d, INF);
+                    acc.grid += sky * (1.0f - g.a) + g.c;
+                } else {
+                    acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                }
                 acc.cov += 1.0f;
                 return;
             }
             col += thr * env_at(F);
             break;
         }
-        if (bounce == 0u) acc.outline = 1u;
+        if (bounce == 0u) {
+            acc.outline = 1u;
+            // emit's overlay term grid_over(o0, d0, first_t) is a function of
+            // the first ray and hit alone: added once per sample here, where
+            // they are at hand, instead of at emit (util.wgsl:101-145)
+            if (F.grid > 0.0f) {
+                const Over gr = grid_over(F, o, d, h.t);
+                acc.grid += gr.c;
+                acc.cov += gr.a;
+            }
+        }
         const Geo g = geo_at(S, h.tri);
         const Mat t = mat_at(S, g.mat);
         const float w = 1.0f - h.u - h.v;
@@ -463,15 +478,13 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
         d = cone_dir(normalize(nd), s.rough * s.rough, seed);
         if (maxc(thr) < 0.01f) break;
     }
-    // emit (util.wgsl:101-145) with no grid overlay: over = 0.
+    // emit (util.wgsl:101-145); the overlay was added at the first hit.
     acc.gone += 0.0f;
     acc.count += 1u;
     acc.film += 1.0f;
     acc.lin += col;
     // the half image takes the odd samples at double weight (util.wgsl:126-132)
     if (F.adapt_on && (frame & 1u)) acc.half = acc.half + col * 2.0f;
-    acc.grid += mk(0.0f);
-    acc.cov += 0.0f;
 }
 
 __device__ __forceinline__ void ld3(const uint32_t* px, uint32_t base, uint32_t i, f3& v) {
@@ -864,14 +877,26 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                     acc.count += 1u;
                     acc.film += 1.0f;
                     acc.lin += mk(0.0f);
-                    acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                    if (F.grid > 0.0f) {
+                        const Over gr = grid_over(F, P.o, P.d, INF);
+                        acc.grid += sky * (1.0f - gr.a) + gr.c;
+                    } else {
+                        acc.grid += sky * (1.0f - 0.0f) + mk(0.0f);
+                    }
                     acc.cov += 1.0f;
                     return PH_FINISH_SAMPLE;
                 }
                 P.col += P.thr * env_at(F);
                 return PH_EMIT_END;
             }
-            if (P.bounce == 0u) acc.outline = 1u;
+            if (P.bounce == 0u) {
+                acc.outline = 1u;
+                if (F.grid > 0.0f) {  // emit's overlay, as in sample()
+                    const Over gr = grid_over(F, P.o, P.d, h.t);
+                    acc.grid += gr.c;
+                    acc.cov += gr.a;
+                }
+            }
             const Geo g = geo_at(S, h.tri);
             const Mat t = mat_at(S, g.mat);
             const float w = 1.0f - h.u - h.v;
@@ -1122,8 +1147,6 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
             acc.count += 1u;
             acc.film += 1.0f;
             acc.lin += P.col;
-            acc.grid += mk(0.0f);
-            acc.cov += 0.0f;
             return PH_FINISH_SAMPLE;
         }
         case PH_DIRECT_NEXT: {
@@ -1513,7 +1536,7 @@ struct phx_tracer_s {
     DevMem verts, vnorm, faces, mats, tnodes, tris, tnorm, lamp_slot, lamp_power, lamp_cdf, info, px, rays, cam;
     BvhWork bvh;
     uint32_t w = 0, h = 0;
-    uint32_t frame = 0, target = 1024;
+    uint32_t frame = 0, target = 32;  // Tracer::SAMPLE_COUNT (src/trace/mod.rs:129) until set_samples
     uint32_t kernel = PHX_KERNEL_MEGAKERNEL;  // which render kernel traces a frame (the fastest measured)
     DevMem next;                                 // the state-machine kernel's pixel counter
     bool smem_stack = false;                     // ray walks keep their stack in shared memory
@@ -1576,7 +1599,6 @@ Scene scene_of(phx_tracer tr) {
 int32_t check_camera(const phx_camera* c) {
     if (c->envmap != 0 || c->env_cdf != 0) return fail(PHX_ERR_INVALID, "environment images are not supported");
     if (c->aperture > 0.0f) return fail(PHX_ERR_INVALID, "depth of field (aperture > 0) is not supported");
-    if (c->grid > 0.0f) return fail(PHX_ERR_INVALID, "the grid overlay is not supported");
     if (c->film[0] != 0 || c->film[1] != 0) return fail(PHX_ERR_INVALID, "film transparency/world is not supported");
     if (c->depth[0] != 0) return fail(PHX_ERR_INVALID, "Max Bounces rows (depth) are not supported");
     if (c->integrator[0] != 0.0f) return fail(PHX_ERR_INVALID, "pixel filters other than phiray's own are not supported");
@@ -1624,6 +1646,9 @@ Frame frame_of(const phx_camera* c, uint32_t w, uint32_t h, const phx_light* dev
     F.adapt_min = c->adapt[1] > 0.0f ? (uint32_t)c->adapt[1] : 0u;
     F.adapt_step = c->adapt[2] >= 1.0f ? (uint32_t)c->adapt[2] : 1u;
     F.adapt_list = 0u;
+    F.grid = c->grid;
+    F.grid_color = make_float4(c->grid_color[0], c->grid_color[1], c->grid_color[2], c->grid_color[3]);
+    F.grid_hide = c->grid_hide;
     return F;
 }
 

@@ -72,6 +72,42 @@ def light_area(pos, direction, right, size, size_y, power, shape=0) -> np.ndarra
     return l
 
 
+def light_sun(direction, power, angle=0.0) -> np.ndarray:
+    """camera.wgsl Light, kind 0 (sun): colour x power arriving along
+    `direction`, spread over a cone of `angle` radians (Light.size)."""
+    l = np.zeros(LIGHT_WORDS, dtype=np.float32)
+    l.view(np.uint32)[3] = 0
+    l[4:7] = power
+    l[7] = angle
+    l[8:11] = direction
+    return l
+
+
+def light_point(pos, power, size=0.0) -> np.ndarray:
+    """camera.wgsl Light, kind 1 (point): colour x power from `pos`, a ball of
+    diameter `size`."""
+    l = np.zeros(LIGHT_WORDS, dtype=np.float32)
+    l[0:3] = pos
+    l.view(np.uint32)[3] = 1
+    l[4:7] = power
+    l[7] = size
+    return l
+
+
+def light_spot(pos, direction, power, cone, blend, size=0.0, right=(0.0, 0.0, 0.0), scale=(0.0, 0.0)) -> np.ndarray:
+    """camera.wgsl Light, kind 2 (spot): a point lamp masked to the cone
+    whose cosine is `cone`, softened over `blend`; a non-zero `right` and
+    `scale` make the cone elliptical (light.wgsl spot_mask)."""
+    l = light_point(pos, power, size)
+    l.view(np.uint32)[3] = 2
+    l[8:11] = direction
+    l[11] = cone
+    l[12:15] = right
+    l[17] = blend
+    l[18:20] = scale
+    return l
+
+
 def light_off() -> np.ndarray:
     """A zero-power point lamp: keeps Camera.count at 1 so the studio rig
     (light.wgsl:87-90, used only when count == 0 and the world is black)
@@ -123,6 +159,8 @@ class Scene:
     bounces: int
     env: tuple = (0.0, 0.0, 0.0)
     meta: dict = field(default_factory=dict)
+    normals: np.ndarray | None = None  # (V, 4) float32 vertex normals, or None: flat faces
+    sun: tuple = (0.0, 1.0, 0.0)  # Camera.sun: the studio rig's key light direction
 
     @property
     def ntris(self) -> int:
@@ -542,3 +580,127 @@ def c5_batch(count: int = 64):
         spp = int(rng.choice([1, 4, 16]))
         out.append(procedural(200000 + k, width=w, height=h, spp=spp, bounces=6, target=tris))
     return out
+
+
+def _smooth_normals(verts: np.ndarray, faces: np.ndarray) -> np.ndarray:
+    """Area-weighted vertex normals (V, 4), w = 0."""
+    p = verts[:, :3].astype(np.float64)
+    a, b, c = p[faces[:, 0]], p[faces[:, 1]], p[faces[:, 2]]
+    fn = np.cross(b - a, c - a)
+    acc = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(acc, faces[:, k], fn)
+    ln = np.linalg.norm(acc, axis=1, keepdims=True)
+    out = np.zeros((len(p), 4), np.float32)
+    out[:, :3] = np.where(ln > 0, acc / np.where(ln > 0, ln, 1.0), 0.0)
+    return out
+
+
+def features(kind: str, width: int = 64, height: int = 48, spp: int = 4, bounces: int = 4) -> Scene:
+    """Small scenes that reach the Rendered shader's paths the benchmark
+    configurations leave unused, each a seeded arrangement of a ground
+    quad, a back wall, a smooth (vertex-normal) icosphere, a box and a
+    small triangle cloud:
+
+      "lamps"   a sun with an angular size, a point lamp with a radius, an
+                elliptical spot lamp and a round area lamp (light.wgsl
+                lamp_query, spot_mask, area_query's disc branch);
+      "rig"     no lamps and a black world: the studio rig lights the scene
+                (light.wgsl uses_rig, rig_query, rig_fill);
+      "glass"   a glass sphere, a tinted glass panel, a half-transmissive
+                box, an alpha cut-out card and an emissive quad seen through
+                them (shade.wgsl's see-through and through loop, refraction
+                and total internal reflection; bvh.wgsl's shadow rays
+                passing glass and cut-outs; integrate.wgsl's through step);
+      "layers"  coat, sheen, subsurface and part-metal materials on the
+                smooth sphere and the box (brdf.wgsl brdf_w's coat, sheen
+                and bleed terms, fresnel_of's dielectric term).
+    """
+    rng = np.random.Generator(np.random.PCG64(SEED + 6 + {"lamps": 0, "rig": 1, "glass": 2, "layers": 3}[kind]))
+    parts, mats, nparts = [], [], []
+
+    def add(v, f, m, normals=None):
+        ff = np.zeros((len(f), 4), np.uint32)
+        ff[:, :3] = f
+        ff[:, 3] = m
+        parts.append((np.asarray(v, np.float32), ff))
+        nparts.append(normals)
+
+    def material(row):
+        mats.append(row)
+        return len(mats) - 1
+
+    g = _quad((-2.0, 0.0, -2.0), (-2.0, 0.0, 2.0), (2.0, 0.0, 2.0), (2.0, 0.0, -2.0), 0)
+    add(g[0], g[1][:, :3], material(lambert((0.6, 0.6, 0.55))))
+    w = _quad((-2.0, 0.0, 1.2), (2.0, 0.0, 1.2), (2.0, 2.0, 1.2), (-2.0, 2.0, 1.2), 0)
+    add(w[0], w[1][:, :3], material(lambert((0.5, 0.55, 0.6))))
+    sv, sf = _icosphere(3)
+    sphere_c = np.array([-0.35, 0.32, 0.3])
+    sv = sv * 0.3 + sphere_c
+    bv, bf = _box((0.4, 0.25, 0.45), (0.35, 0.5, 0.35), 3)
+    cl_n = 300
+    cen = rng.uniform(-0.6, 0.6, (cl_n, 3)) * np.array([1.0, 0.3, 0.4]) + np.array([0.0, 0.9, 0.2])
+    e1 = _unit(rng, cl_n) * rng.uniform(0.02, 0.05, (cl_n, 1))
+    e2 = _unit(rng, cl_n) * rng.uniform(0.02, 0.05, (cl_n, 1))
+    a0 = cen - (e1 + e2) / 3.0
+    cv = np.stack([a0, a0 + e1, a0 + e2], 1).reshape(-1, 3)
+    cf = np.arange(3 * cl_n).reshape(cl_n, 3)
+    lights = [light_off()]
+    env = (0.0, 0.0, 0.0)
+    sun = (0.0, 1.0, 0.0)
+    smooth_sphere = True
+    if kind == "lamps":
+        add(sv, sf, material(mat([0.7, 0.3, 0.2, 1.0], rough=0.35)), "smooth")
+        add(bv, bf, material(mat([0.3, 0.6, 0.3, 1.0], rough=0.6, metal=0.2)))
+        add(cv, cf, material(lambert((0.8, 0.8, 0.3))))
+        lights = [
+            light_sun((-0.3, -1.0, 0.4), (1.5, 1.4, 1.2), angle=0.08),
+            light_point((0.8, 1.4, -0.6), (18.0, 16.0, 14.0), size=0.15),
+            light_spot((-0.9, 1.6, -0.5), (0.45, -0.85, 0.3), (40.0, 40.0, 45.0), cone=0.85, blend=0.08, size=0.05,
+                       right=(1.0, 0.0, 0.0), scale=(1.0, 1.6)),
+            light_area((0.0, 1.9, 0.2), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.5, 0.3, (8.0, 8.0, 8.0), shape=4),
+        ]
+        env = (0.02, 0.02, 0.03)
+    elif kind == "rig":
+        add(sv, sf, material(mat([0.6, 0.6, 0.65, 1.0], rough=0.3)), "smooth")
+        add(bv, bf, material(mat([0.8, 0.3, 0.3, 1.0], rough=0.7)))
+        add(cv, cf, material(mirror((0.9, 0.9, 0.9))))
+        lights = np.zeros((0, LIGHT_WORDS), np.float32)
+        sun = tuple(np.array([0.4, 0.8, -0.45]) / np.linalg.norm([0.4, 0.8, -0.45]))
+    elif kind == "glass":
+        add(sv, sf, material(mat([0.95, 0.95, 1.0, 1.0], rough=0.02, trans=1.0, ior=1.5)), "smooth")
+        add(bv, bf, material(mat([0.8, 0.5, 0.2, 1.0], rough=0.4, trans=0.5, ior=1.33)))
+        add(cv, cf, material(mat([0.3, 0.7, 0.9, 0.4], rough=0.8)))  # alpha 0.4: a cut-out
+        pv, pf = _quad((-0.9, 0.05, -0.45), (0.1, 0.05, -0.45), (0.1, 0.75, -0.55), (-0.9, 0.75, -0.55), 0)
+        add(pv, pf[:, :3], material(mat([0.6, 0.9, 0.7, 1.0], rough=0.15, trans=0.9, ior=1.7)))
+        ev, ef = _quad((0.5, 1.5, 0.0), (0.9, 1.5, 0.0), (0.9, 1.5, 0.4), (0.5, 1.5, 0.4), 0)
+        add(ev, ef[:, :3], material(mat([0.0, 0.0, 0.0, 1.0], rough=1.0, emit=(12.0, 11.0, 9.0))))
+        lights = [light_area((-0.5, 1.8, -0.3), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.6, 0.6, (14.0, 14.0, 14.0))]
+        env = (0.05, 0.06, 0.08)
+    elif kind == "layers":
+        coat = mat([0.7, 0.15, 0.1, 1.0], rough=0.5)
+        coat[26], coat[27] = 0.8, 0.08
+        add(sv, sf, material(coat), "smooth")
+        sheen = mat([0.2, 0.25, 0.6, 1.0], rough=0.9)
+        sheen[21], sheen[22], sheen[23:26] = 0.8, 0.3, (1.0, 0.9, 0.8)
+        sheen[17], sheen[18:21] = 0.6, (0.2, 0.08, 0.04)  # subsurface weight and radius
+        add(bv, bf, material(sheen))
+        part = mat([0.9, 0.8, 0.5, 1.0], rough=0.25, metal=0.5)
+        part[26], part[27] = 0.3, 0.2
+        add(cv, cf, material(part))
+        lights = [light_area((-0.6, 1.8, -0.6), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.5, 0.5, (16.0, 15.0, 14.0)),
+                  light_point((0.9, 1.2, -0.8), (6.0, 6.0, 7.0), size=0.1)]
+        env = (0.04, 0.04, 0.05)
+    else:
+        raise ValueError(kind)
+    verts, faces = _assemble(parts)
+    normals = np.zeros((len(verts), 4), np.float32)
+    at = 0
+    for (v, f), nrm in zip(parts, nparts):
+        if nrm == "smooth" and smooth_sphere:
+            normals[at:at + len(v)] = _smooth_normals(np.c_[v, np.ones(len(v))], f[:, :3].astype(np.int64))
+        at += len(v)
+    view = View.look((0.1, 0.75, -1.9), (-0.05, -0.25, 1.0), (0.0, 1.0, 0.0), 50.0)
+    lights = np.asarray(lights, np.float32).reshape(-1, LIGHT_WORDS)
+    return Scene(f"features_{kind}", verts, faces, np.stack(mats).astype(np.float32), lights, view, width, height,
+                 spp, bounces, env=env, normals=normals, sun=sun)

@@ -74,7 +74,7 @@ def camera(scene) -> np.ndarray:
     c["env"][0, :3] = scene.env
     c["view"] = (0.0, 0.0, 1.0, 0.0)
     c["bounces"] = scene.bounces
-    c["sun"] = (0.0, 1.0, 0.0)
+    c["sun"] = getattr(scene, "sun", (0.0, 1.0, 0.0))
     L = len(scene.lights)
     c["count"] = L
     raw = c["lights"].view(np.float32).reshape(1, 64, 20)
@@ -170,6 +170,7 @@ class Tracer:
 
     @classmethod
     def of(cls, gpu: Gpu, scene, **kw) -> "Tracer":
+        kw.setdefault("normals", getattr(scene, "normals", None))
         return cls(gpu, scene.verts, scene.faces, scene.mats, **kw)
 
     MEGAKERNEL = 0

@@ -44,6 +44,8 @@ SIGS = {
     "orc_primary": (None, [vp, vp, u32, vp, u32, vp, u32, vp, vp]),
     "orc_show": (None, [vp, vp]),
     "orc_trace_rays": (None, [vp, vp, u32, vp, u32, vp, u32, vp, C.c_int]),
+    "orc_tri_hit": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "orc_math": (None, [C.c_int, vp, vp, vp, u32]),
 }
 
 
@@ -153,6 +155,23 @@ class Oracle:
                           f32(min_weight), len(rest), out.ctypes.data)
         return out
 
+    # --- the watertight triangle test (tri.rs:51-114) and the shared math ---
+    def tri_hit(self, a, b, c, o, d):
+        """(t, u, v) of the watertight test, or None for a miss."""
+        args = [np.ascontiguousarray(v, dtype=np.float32) for v in (a, b, c, o, d)]
+        out = np.zeros(3, np.float32)
+        hit = self.lib.orc_tri_hit(*[v.ctypes.data for v in args], out.ctypes.data)
+        return (float(out[0]), float(out[1]), float(out[2])) if hit else None
+
+    MATH = {"exp2": 0, "log2": 1, "sin": 2, "cos": 3, "pow": 4, "exp": 5}
+
+    def math(self, fn: str, x, y=None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(np.zeros_like(x) if y is None else y, dtype=np.float32)
+        out = np.zeros_like(x)
+        self.lib.orc_math(self.MATH[fn], x.ctypes.data, y.ctypes.data, out.ctypes.data, len(x))
+        return out
+
     # --- Denoise (denoise.wgsl) ---
     def denoise(self, px, w, h, strength=(64.0, 8.0, 40.0, 7.0), view=(0.0, 0.0, 1.0, 0.0), keep=False):
         px = np.ascontiguousarray(px, dtype=np.uint32).copy()
@@ -175,9 +194,12 @@ class TraceOracle:
     def __init__(self, orc: "Oracle", scene, leaf: int = 4, sah: bool = False):
         self.lib = orc.lib
         self.v, self.f, self.m = _scene_args(scene)
+        nrm = getattr(scene, "normals", None)
+        self.nrm = None if nrm is None else np.ascontiguousarray(nrm, dtype=np.float32)
         self.leaf = leaf
         new = self.lib.orc_scene_new_sah if sah else self.lib.orc_scene_new
-        self.handle = new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, None, leaf)
+        self.handle = new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data,
+                          None if self.nrm is None else self.nrm.ctypes.data, leaf)
 
     def __del__(self):
         try:
