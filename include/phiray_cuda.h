@@ -383,6 +383,23 @@ typedef struct phx_scene {
     uint32_t leaf; /* LBVH leaf size (the tracer's 4, forest.rs:20) */
 } phx_scene;
 
+/* trace::Mesh (src/trace/mesh.rs:12-22): faces [face_lo, face_hi) of the
+ * scene's face array, kept in the mesh's own space under a tree of its own. */
+typedef struct phx_mesh {
+    uint32_t face_lo, face_hi;
+} phx_mesh;
+
+/* trace::Instance (src/trace/instance.rs:20-37): one placement of a mesh.
+ * world is object -> world in Blender's layout, m[col][row] at
+ * world[4 * col + row] (translation in world[12..14]). casts_shadow 0: shadow
+ * rays pass it (Cycles' Ray Visibility > Shadow). 32-byte aligned record. */
+typedef struct phx_instance {
+    float world[16];
+    uint32_t mesh;
+    uint32_t casts_shadow;
+    uint32_t pad[6];
+} phx_instance;
+
 typedef struct phx_tracer_s* phx_tracer;
 
 /* PX_LEN (src/trace/read.rs:56): words per pixel of the image buffer. */
@@ -393,6 +410,25 @@ typedef struct phx_tracer_s* phx_tracer;
  * is the tracer's tree), gather triangles into leaf order, build the
  * emitter table. */
 int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* scene, phx_tracer* out);
+/* Tracer::new over meshes placed by instances (src/trace/forest.rs:44-61,
+ * 126-158; instance.rs): each mesh's faces [face_lo, face_hi) get an LBVH of
+ * their own in the mesh's space (the vertices stay there), the instances'
+ * world boxes a top tree (one instance a leaf); the walk takes each ray
+ * through the top tree and into each instance's mesh by its inverse
+ * (bvh.wgsl:115-232), a hit remembers its instance, shading places the face
+ * in the world by it (layout.wgsl tri_of, world_ng for mirroring matrices),
+ * shadow rays pass instances that cast none, and the emitter table holds an
+ * entry per (emissive face, instance) (lamp.rs table_of). Meshes must name
+ * ascending, disjoint ranges; faces in no mesh are never hit. Vertex w is
+ * taken as 1. */
+int32_t phx_tracer_create_instanced(phx_ctx ctx, const phx_scene* scene, const phx_mesh* meshes, uint32_t nmeshes,
+                                    const phx_instance* insts, uint32_t ninsts, phx_tracer* out);
+/* Tracer::reinstance (src/trace/pose.rs:105-120): the same instances placed
+ * by new matrices (and shadow flags); the top tree is rebuilt on the device,
+ * the emitter table again, the image starts over. PHX_ERR_INVALID when the
+ * count or an instance's mesh differs (build the tracer again) or the tracer
+ * has no instances. Stream-ordered. */
+int32_t phx_tracer_reinstance(phx_tracer tr, const phx_instance* insts, uint32_t ninsts);
 int32_t phx_tracer_destroy(phx_tracer tr);
 /* Which kernel traces a frame. All compute the same image bit for bit:
  * PHX_KERNEL_MEGAKERNEL (the default) is shade.wgsl's main as one thread per
@@ -469,6 +505,20 @@ int32_t phx_tracer_sample(phx_tracer tr, const phx_camera* cam, uint32_t w, uint
  * into the image, each pixel's samples taken in order inside the kernel —
  * the same sums as spp calls of sample. Stream-ordered, no wait. */
 int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first, uint32_t spp);
+/* phx_tracer_trace over rows [row0, row0 + rows) of the w x h frame only: the
+ * other rows' planes are left as they are. For a frame split across GPUs by
+ * rows (each rank traces its rows, then the finished rows are gathered to
+ * the presenting rank: phx_tracer_copy_rows). Not with adaptive sampling. */
+int32_t phx_tracer_trace_rows(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                              uint32_t spp, uint32_t row0, uint32_t rows);
+/* PHX_ROW_WORDS words a pixel of the planes a traced row carries (packed,
+ * linear sums, shown, albedo, normal, depth, overlay, coverage, film,
+ * outline, sample count, missed — read.rs:37-56): copies rows [row0,
+ * row0 + rows) of them between the image and `packed` (DEVICE, plane by
+ * plane, PHX_ROW_WORDS * rows * w words), into the image when into_image.
+ * Stream-ordered. */
+#define PHX_ROW_WORDS 22u
+int32_t phx_tracer_copy_rows(phx_tracer tr, uint32_t row0, uint32_t rows, uint32_t* packed, int32_t into_image);
 /* Tracer::set_adaptive (src/trace/mod.rs:235-240): Adaptive Sampling as
  * [threshold, min samples, step, on], stamped on every frame this tracer
  * traces in place of the camera's own adapt field (sample.rs:119). With it
@@ -713,7 +763,8 @@ int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint3
  * preparation; the batch trace; per job the learned denoiser with the
  * a-trous fallback (net non-NULL; one copy of the network per image shape)
  * or the a-trous Denoise, then a completion time stamp. Runs one frame
- * outside the capture first (sizing every buffer). */
+ * outside the capture first (sizing every buffer). Tracers of instances are
+ * refused (PHX_ERR_INVALID): phx_batch_trace takes them. */
 int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold);
 /* Replays the captured frame; modes (HOST, one per job): 1 rebuild, 0 refit. */
 int32_t phx_batch_replay(phx_batch b, const uint32_t* modes);

@@ -39,6 +39,7 @@ struct Hit {
 // A triangle record as layout.wgsl's tri_of assembles it.
 struct Tri {
     V3 a, b, c, na, nb, nc;
+    bool mirror;  // placed by an instance whose matrix mirrors (word 27, bit 2)
     float rough, trans, metal, ior;
     float color[4];
     V3 emit;
@@ -63,13 +64,38 @@ struct Shadowed {
     float dist;
 };
 
+// One placement of a mesh (instance.rs Instance::words): the world matrix's
+// rows, the inverse's rows, the mesh, and flags — bit 0 at the identity,
+// bit 1 casts no shadow, bit 2 mirrors.
+struct Inst {
+    float row[3][4];
+    float inv[3][4];
+    uint32_t mesh;
+    uint32_t flags;
+};
+
+// One mesh's tree (forest.rs blas): faces [lo, hi) of the scene, nodes over
+// them in the mesh's own space, leaf ranges mesh-local.
+struct MeshTree {
+    uint32_t lo = 0, hi = 0;
+    std::vector<orc_node> nodes;
+};
+
 // The scene shared by every pixel: the tree, leaf order, emitter table.
+// With `meshes` empty the scene is one identity instance whose tree is
+// `nodes`; otherwise `nodes` is the top tree over the instances' world boxes
+// (its slots named by inst_order) and each mesh has its own tree.
 struct Shared {
     std::vector<orc_node> nodes;
     std::vector<uint32_t> order;
     std::vector<uint32_t> lamp_face;  // light table (lamp.rs table_of): slots
+    std::vector<uint32_t> lamp_inst;  // and the instance of each
     std::vector<float> lamp_cdf;
     float extent = 0.0f;
+    std::vector<MeshTree> meshes;
+    std::vector<Inst> insts;
+    std::vector<uint32_t> inst_order;
+    uint32_t leaf = 4;
 };
 
 struct World {
@@ -252,14 +278,130 @@ void trace_blas(const World& W, V3 o, V3 d, bool first, Hit* best) {
     }
 }
 
-// trace (bvh.wgsl:194-232): the top tree holds the one instance, whose box
-// is the mesh tree's root box.
+// A row of an instance matrix applied to a point (w = 1) or a direction.
+float row_point(const float r[4], V3 p) { return ((r[0] * p.x + r[1] * p.y) + r[2] * p.z) + r[3] * 1.0f; }
+float row_dir(const float r[4], V3 d) { return (r[0] * d.x + r[1] * d.y) + r[2] * d.z; }
+
+// trace_blas (bvh.wgsl:115-190) for instance i of a scene with a top tree:
+// the ray taken into the mesh's space by the instance's inverse (direction
+// unnormalised, so t is the world's), the mesh's tree walked there.
+void trace_blas_inst(const World& W, uint32_t i, V3 ow, V3 dw, bool first, Hit* best) {
+    const Inst& in = W.S->insts[i];
+    const MeshTree& mt = W.S->meshes[in.mesh];
+    if (mt.nodes.empty()) return;
+    if (first && (in.flags & 2u) != 0u) return;
+    V3 o = ow, d = dw;
+    if ((in.flags & 1u) == 0u) {
+        o = v3(row_point(in.inv[0], ow), row_point(in.inv[1], ow), row_point(in.inv[2], ow));
+        d = v3(row_dir(in.inv[0], dw), row_dir(in.inv[1], dw), row_dir(in.inv[2], dw));
+    }
+    const V3 inv = safe_inv(d);
+    const orc_node top = mt.nodes[0];
+    if (box_t(top, o, inv, best->t) >= INF) return;
+    const RaySpace rs = ray_space(d);
+    uint32_t stack[32];
+    uint32_t sp = 0;
+    orc_node nd = top;
+    for (;;) {
+        if ((nd.lo.i & LEAF) != 0u) {
+            for (uint32_t id = (nd.lo.i & ~LEAF) + mt.lo; id < nd.hi.i + mt.lo; id++) {
+                const uint32_t* v = W.face(id);
+                W.tests++;
+                float h[3];
+                tri_t(W.vert(v[0]), W.vert(v[1]), W.vert(v[2]), o, rs, h);
+                if (h[0] < best->t) {
+                    if (first) {
+                        const float* m = W.mat(v[3]);
+                        if (m[6] > 0.5f || m[3] < 0.5f) continue;
+                        *best = Hit{h[0], id, h[1], h[2], i};
+                        return;
+                    }
+                    *best = Hit{h[0], id, h[1], h[2], i};
+                }
+            }
+        } else {
+            W.steps++;
+            const orc_node nl = mt.nodes[nd.lo.i];
+            const orc_node nr = mt.nodes[nd.hi.i];
+            const float tl = box_t(nl, o, inv, best->t);
+            const float tr = box_t(nr, o, inv, best->t);
+            if (tl < INF && tr < INF) {
+                if (tl <= tr) {
+                    stack[sp] = nd.hi.i;
+                    nd = nl;
+                } else {
+                    stack[sp] = nd.lo.i;
+                    nd = nr;
+                }
+                sp++;
+                continue;
+            }
+            if (tl < INF) {
+                nd = nl;
+                continue;
+            }
+            if (tr < INF) {
+                nd = nr;
+                continue;
+            }
+        }
+        if (sp == 0u) break;
+        sp--;
+        nd = mt.nodes[stack[sp]];
+    }
+}
+
+// trace (bvh.wgsl:194-232). One identity instance: its tree is `nodes`.
+// With instances: the top tree over their world boxes, each leaf's
+// instances walked in slot order; an any-hit ray stops at the first.
 Hit trace(World& W, V3 o, V3 d, float tmax, bool first) {
     W.rays++;
     Hit best{tmax, NONE, 0.0f, 0.0f, 0};
     const V3 inv = safe_inv(d);
-    if (box_t(W.S->nodes[0], o, inv, best.t) >= INF) return best;
-    trace_blas(W, o, d, first, &best);
+    if (W.S->nodes.empty() || box_t(W.S->nodes[0], o, inv, best.t) >= INF) return best;
+    if (W.S->meshes.empty()) {
+        trace_blas(W, o, d, first, &best);
+        return best;
+    }
+    uint32_t stack[32];
+    uint32_t sp = 0;
+    orc_node nd = W.S->nodes[0];
+    for (;;) {
+        if ((nd.lo.i & LEAF) != 0u) {
+            for (uint32_t s = nd.lo.i & ~LEAF; s < nd.hi.i; s++) {
+                trace_blas_inst(W, W.S->inst_order[s], o, d, first, &best);
+                if (first && best.tri != NONE) return best;
+            }
+        } else {
+            W.steps++;
+            const orc_node nl = W.S->nodes[nd.lo.i];
+            const orc_node nr = W.S->nodes[nd.hi.i];
+            const float tl = box_t(nl, o, inv, best.t);
+            const float tr = box_t(nr, o, inv, best.t);
+            if (tl < INF && tr < INF) {
+                if (tl <= tr) {
+                    stack[sp] = nd.hi.i;
+                    nd = nl;
+                } else {
+                    stack[sp] = nd.lo.i;
+                    nd = nr;
+                }
+                sp++;
+                continue;
+            }
+            if (tl < INF) {
+                nd = nl;
+                continue;
+            }
+            if (tr < INF) {
+                nd = nr;
+                continue;
+            }
+        }
+        if (sp == 0u) break;
+        sp--;
+        nd = W.S->nodes[stack[sp]];
+    }
     return best;
 }
 
@@ -267,13 +409,26 @@ float visible(World& W, V3 org, V3 l, float dist) { return trace(W, org, l, dist
 
 // ---- layout.wgsl ----
 
-Tri tri_of(const World& W, uint32_t slot) {
+// place_n (layout.wgsl:72-77): a normal under the inverse-transpose of an
+// instance's 3 x 3, unit again; a zero (flat) normal stays zero.
+V3 place_n(const Inst& in, V3 n) {
+    const V3 m = v3(in.inv[0][0], in.inv[0][1], in.inv[0][2]) * n.x + v3(in.inv[1][0], in.inv[1][1], in.inv[1][2]) * n.y +
+                 v3(in.inv[2][0], in.inv[2][1], in.inv[2][2]) * n.z;
+    const float l = length(m);
+    if (l < 1e-12f) return v3(0.0f);
+    return m / l;
+}
+
+// tri_of (layout.wgsl:114-159): the face in slot `slot`, placed in the world
+// by instance `inst` (its vertices are kept in the mesh's space).
+Tri tri_of(const World& W, uint32_t slot, uint32_t inst = 0) {
     const uint32_t* v = W.face(slot);
     const float* m = W.mat(v[3]);
     Tri t;
     t.a = W.vert(v[0]);
     t.b = W.vert(v[1]);
     t.c = W.vert(v[2]);
+    t.mirror = false;
     if (W.normals) {
         auto nv = [&](uint32_t k) {
             return v3(W.normals[4 * (size_t)k], W.normals[4 * (size_t)k + 1], W.normals[4 * (size_t)k + 2]);
@@ -283,6 +438,23 @@ Tri tri_of(const World& W, uint32_t slot) {
         t.nc = nv(v[2]);
     } else {
         t.na = t.nb = t.nc = v3(0.0f);
+    }
+    if (!W.S->insts.empty()) {
+        const Inst& in = W.S->insts[inst];
+        t.mirror = (in.flags & 4u) != 0u;
+        if ((in.flags & 1u) == 0u) {
+            auto place = [&](uint32_t k) {  // the vertex with w = 1, as the scene stores it
+                const float* q = W.verts + 4 * (size_t)k;
+                auto r = [&](const float* row) { return ((row[0] * q[0] + row[1] * q[1]) + row[2] * q[2]) + row[3]; };
+                return v3(r(in.row[0]), r(in.row[1]), r(in.row[2]));
+            };
+            t.a = place(v[0]);
+            t.b = place(v[1]);
+            t.c = place(v[2]);
+            t.na = place_n(in, t.na);
+            t.nb = place_n(in, t.nb);
+            t.nc = place_n(in, t.nc);
+        }
     }
     t.rough = m[4];
     t.metal = m[5];
@@ -300,7 +472,11 @@ Tri tri_of(const World& W, uint32_t slot) {
     return t;
 }
 
-V3 world_ng(const Tri& t) { return normalize(cross(t.b - t.a, t.c - t.a)); }
+// world_ng (layout.wgsl:97-101): turned back under a mirroring instance.
+V3 world_ng(const Tri& t) {
+    const V3 ng = normalize(cross(t.b - t.a, t.c - t.a));
+    return t.mirror ? -ng : ng;
+}
 
 // ---- brdf.wgsl ----
 
@@ -619,11 +795,11 @@ float lamp_chance(const World& W, const Hit& h) {
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2u;
         const uint32_t f = W.S->lamp_face[mid];
-        const uint32_t i = 0u;
+        const uint32_t i = W.S->lamp_inst[mid];
         if (f < h.tri || (f == h.tri && i < h.inst)) lo = mid + 1u;
         else hi = mid;
     }
-    if (W.S->lamp_face[lo] != h.tri || 0u != h.inst) return 0.0f;
+    if (W.S->lamp_face[lo] != h.tri || W.S->lamp_inst[lo] != h.inst) return 0.0f;
     const float prev = lo > 0u ? W.S->lamp_cdf[lo - 1u] : 0.0f;
     return W.S->lamp_cdf[lo] - prev;
 }
@@ -640,7 +816,7 @@ Shadowed glow_query(const World& W, const Surf& s, uint32_t* seed) {
     }
     const float prev = lo > 0u ? W.S->lamp_cdf[lo - 1u] : 0.0f;
     const float chance = fmaxw(W.S->lamp_cdf[lo] - prev, 1e-8f);
-    const Tri t = tri_of(W, W.S->lamp_face[lo]);
+    const Tri t = tri_of(W, W.S->lamp_face[lo], W.S->lamp_inst[lo]);
     float a = rnd(seed);
     float b = rnd(seed);
     if (a + b > 1.0f) {
@@ -732,7 +908,7 @@ V3 indirect(World& W, V3 pos, V3 n, uint32_t* seed, bool bounce) {
             break;
         }
         if (!bounce) break;
-        const Tri t = tri_of(W, h.tri);
+        const Tri t = tri_of(W, h.tri, h.inst);
         const V3 ng0 = normalize(cross(t.b - t.a, t.c - t.a));
         const V3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
         const V3 hit = org + dir * h.t + ng * (W.eps + h.t * 1e-5f);
@@ -769,7 +945,7 @@ V3 indirect(World& W, V3 pos, V3 n, uint32_t* seed, bool bounce) {
 }
 
 V3 bounce_light(World& W, const Hit& h, V3 org, V3 d, float min_pdf, uint32_t* seed) {
-    const Tri t = tri_of(W, h.tri);
+    const Tri t = tri_of(W, h.tri, h.inst);
     const V3 ng0 = normalize(cross(t.b - t.a, t.c - t.a));
     const V3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
     const V3 pos = org + d * h.t + ng * (W.eps + h.t * 1e-5f);
@@ -1000,7 +1176,7 @@ void shade_main(World& W, uint32_t i) {
             first_t = h.t;
             px[25 * N + i] = h.inst + 1u;
         }
-        const Tri t = tri_of(W, h.tri);
+        const Tri t = tri_of(W, h.tri, h.inst);
         const float w = 1.0f - h.u - h.v;
         const V3 hit = o + d * h.t;
         const V3 ng0 = world_ng(t);
@@ -1139,6 +1315,7 @@ void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint3
         const float p = 0.5f * std::sqrt(sq) * glow;
         if (p > 0.0f) {
             S.lamp_face.push_back(s);
+            S.lamp_inst.push_back(0u);
             pw.push_back(p);
         }
     }
@@ -1156,6 +1333,181 @@ void setup(Shared& S, World& W, const float* verts, const uint32_t* faces, uint3
         e += dk * dk;
     }
     S.extent = fmaxw(std::sqrt(e), 1e-3f);
+}
+
+// Instance::inverse and words (instance.rs): rows of the world matrix and
+// of its inverse (the upper 3 x 3 inverted, the translation undone; zero for
+// a singular matrix), and the flags.
+Inst inst_of(const phx_instance& src) {
+    Inst in;
+    const float* m = src.world;  // m[col][row] at m[4 * col + row]
+    auto a = [&](int r, int c) { return m[4 * c + r]; };
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 4; c++) in.row[r][c] = m[4 * c + r];
+    const float det = a(0, 0) * (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) - a(0, 1) * (a(1, 0) * a(2, 2) - a(1, 2) * a(2, 0)) +
+                      a(0, 2) * (a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0));
+    if (std::fabs(det) < 1e-20f) {
+        std::memset(in.inv, 0, sizeof in.inv);
+    } else {
+        const float d = 1.0f / det;
+        const float inv[3][3] = {
+            {(a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) * d, (a(0, 2) * a(2, 1) - a(0, 1) * a(2, 2)) * d,
+             (a(0, 1) * a(1, 2) - a(0, 2) * a(1, 1)) * d},
+            {(a(1, 2) * a(2, 0) - a(1, 0) * a(2, 2)) * d, (a(0, 0) * a(2, 2) - a(0, 2) * a(2, 0)) * d,
+             (a(0, 2) * a(1, 0) - a(0, 0) * a(1, 2)) * d},
+            {(a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0)) * d, (a(0, 1) * a(2, 0) - a(0, 0) * a(2, 1)) * d,
+             (a(0, 0) * a(1, 1) - a(0, 1) * a(1, 0)) * d},
+        };
+        const float t[3] = {m[12], m[13], m[14]};
+        for (int r = 0; r < 3; r++) {
+            for (int c = 0; c < 3; c++) in.inv[r][c] = inv[r][c];
+            in.inv[r][3] = -((inv[r][0] * t[0] + inv[r][1] * t[1]) + inv[r][2] * t[2]);
+        }
+    }
+    bool identity = true;
+    for (int k = 0; k < 16; k++) identity = identity && m[k] == ((k % 5 == 0) ? 1.0f : 0.0f);
+    in.mesh = src.mesh;
+    in.flags = (identity ? 1u : 0u) | (src.casts_shadow ? 0u : 2u) | (det < 0.0f ? 4u : 0u);
+    return in;
+}
+
+// Forest::retlas (forest.rs:107-121) with the LBVH: the top tree over the
+// world boxes (Instance::world_box of each mesh's root bounds) of the
+// instances whose mesh has faces, one instance a leaf; then the extent.
+void retlas(Shared& S) {
+    std::vector<uint32_t> placed;
+    std::vector<orc_aabb> boxes;
+    for (uint32_t i = 0; i < S.insts.size(); i++) {
+        const Inst& in = S.insts[i];
+        if (in.mesh >= S.meshes.size() || S.meshes[in.mesh].nodes.empty()) continue;
+        const orc_node& root = S.meshes[in.mesh].nodes[0];
+        orc_aabb b;
+        std::memset(&b, 0, sizeof b);
+        for (int k = 0; k < 3; k++) {  // Aabb::default(): [f32::MAX; 3], [f32::MIN; 3]
+            b.lo[k] = 3.40282347e38f;
+            b.hi[k] = -3.40282347e38f;
+        }
+        for (int k = 0; k < 8; k++) {
+            const float c[3] = {(k & 1) == 0 ? root.lo.p[0] : root.hi.p[0], (k & 2) == 0 ? root.lo.p[1] : root.hi.p[1],
+                                (k & 4) == 0 ? root.lo.p[2] : root.hi.p[2]};
+            for (int r = 0; r < 3; r++) {
+                const float w = ((in.row[r][0] * c[0] + in.row[r][1] * c[1]) + in.row[r][2] * c[2]) + in.row[r][3];
+                b.lo[r] = fminw(b.lo[r], w);
+                b.hi[r] = fmaxw(b.hi[r], w);
+            }
+        }
+        placed.push_back(i);
+        boxes.push_back(b);
+    }
+    const uint32_t n = (uint32_t)placed.size();
+    S.nodes.assign(n ? 2 * (size_t)n - 1 : 0, orc_node{});
+    std::vector<uint32_t> order(n);
+    uint32_t depth = 0;
+    if (n) orc_build(boxes.data(), n, 1, S.nodes.data(), order.data(), &depth);
+    S.inst_order.resize(n);
+    for (uint32_t s = 0; s < n; s++) S.inst_order[s] = placed[order[s]];
+    float e = 0.0f;
+    if (n) {
+        for (int k = 0; k < 3; k++) {
+            const float dk = S.nodes[0].hi.p[k] - S.nodes[0].lo.p[k];
+            e += dk * dk;
+        }
+    }
+    S.extent = fmaxw(std::sqrt(e), 1e-3f);
+}
+
+// lamp.rs table_of with instances: every emissive slot (slot order), once
+// for each instance of its mesh (instance order), by its world area times
+// its emitted luminance.
+void relight(Shared& S, const World& W) {
+    S.lamp_face.clear();
+    S.lamp_inst.clear();
+    S.lamp_cdf.clear();
+    std::vector<std::vector<uint32_t>> by_mesh(S.meshes.size());
+    for (uint32_t i = 0; i < S.insts.size(); i++)
+        if (S.insts[i].mesh < S.meshes.size()) by_mesh[S.insts[i].mesh].push_back(i);
+    std::vector<float> pw;
+    for (uint32_t k = 0; k < S.meshes.size(); k++) {
+        for (uint32_t s = S.meshes[k].lo; s < S.meshes[k].hi; s++) {
+            const uint32_t* q = W.faces + 4 * (size_t)S.order[s];
+            const float* m = W.mats + 32 * (size_t)q[3];
+            const float glow = 0.2126f * m[8] + 0.7152f * m[9] + 0.0722f * m[10];
+            if (glow <= 0.0f) continue;
+            for (uint32_t i : by_mesh[k]) {
+                const Inst& in = S.insts[i];
+                auto corner = [&](uint32_t v) {
+                    const float* p = W.verts + 4 * (size_t)v;
+                    auto r = [&](const float* row) { return ((row[0] * p[0] + row[1] * p[1]) + row[2] * p[2]) + row[3]; };
+                    return v3(r(in.row[0]), r(in.row[1]), r(in.row[2]));
+                };
+                const V3 a = corner(q[0]), b = corner(q[1]), c = corner(q[2]);
+                const float e1[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
+                const float e2[3] = {c.x - a.x, c.y - a.y, c.z - a.z};
+                const float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                     e1[0] * e2[1] - e1[1] * e2[0]};
+                float sq = 0.0f;
+                for (int j = 0; j < 3; j++) sq += cr[j] * cr[j];
+                const float p = 0.5f * std::sqrt(sq) * glow;
+                if (p > 0.0f) {
+                    S.lamp_face.push_back(s);
+                    S.lamp_inst.push_back(i);
+                    pw.push_back(p);
+                }
+            }
+        }
+    }
+    float total = 0.0f;
+    for (float p : pw) total += p;
+    float run = 0.0f;
+    for (float p : pw) {
+        run += p;
+        S.lamp_cdf.push_back(run / total);
+    }
+}
+
+// Forest::build (forest.rs:44-61) with each mesh's LBVH: the meshes' trees
+// in their own space, the slot order (each mesh's faces permuted within its
+// range), the instances, the top tree and the emitter table.
+void setup_instanced(Shared& S, World& W, const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
+                     const float* normals, uint32_t leaf, const phx_mesh* meshes, uint32_t nmeshes,
+                     const phx_instance* insts, uint32_t ninsts) {
+    W.S = &S;
+    W.verts = verts;
+    W.normals = normals;
+    W.faces = faces;
+    W.mats = mats;
+    S.leaf = leaf ? leaf : 4;
+    S.order.resize(nfaces);
+    for (uint32_t f = 0; f < nfaces; f++) S.order[f] = f;
+    S.meshes.assign(nmeshes, MeshTree{});
+    for (uint32_t k = 0; k < nmeshes; k++) {
+        MeshTree& mt = S.meshes[k];
+        mt.lo = meshes[k].face_lo;
+        mt.hi = meshes[k].face_hi;
+        const uint32_t n = mt.hi - mt.lo;
+        if (n == 0) continue;
+        std::vector<orc_aabb> boxes(n);
+        for (uint32_t f = 0; f < n; f++) {
+            orc_aabb b;
+            std::memset(&b, 0, sizeof b);
+            const uint32_t* q = faces + 4 * (size_t)(mt.lo + f);
+            for (int j = 0; j < 3; j++) {
+                const float a = verts[4 * (size_t)q[0] + j], bb = verts[4 * (size_t)q[1] + j], c = verts[4 * (size_t)q[2] + j];
+                b.lo[j] = fminw(fminw(a, bb), c);
+                b.hi[j] = fmaxw(fmaxw(a, bb), c);
+            }
+            boxes[f] = b;
+        }
+        mt.nodes.assign(2 * (size_t)n - 1, orc_node{});
+        std::vector<uint32_t> order(n);
+        uint32_t depth = 0;
+        orc_build(boxes.data(), n, S.leaf, mt.nodes.data(), order.data(), &depth);
+        for (uint32_t sl = 0; sl < n; sl++) S.order[mt.lo + sl] = mt.lo + order[sl];
+    }
+    S.insts.resize(ninsts);
+    for (uint32_t i = 0; i < ninsts; i++) S.insts[i] = inst_of(insts[i]);
+    retlas(S);
+    relight(S, W);
 }
 
 }  // namespace
@@ -1182,6 +1534,60 @@ void* orc_scene_new_sah(const float* verts, const uint32_t* faces, uint32_t nfac
 }
 
 void orc_scene_free(void* handle) { delete (OrcScene*)handle; }
+
+void* orc_scene_new_instanced(const float* verts, const uint32_t* faces, uint32_t nfaces, const float* mats,
+                              const float* normals, uint32_t leaf, const phx_mesh* meshes, uint32_t nmeshes,
+                              const phx_instance* insts, uint32_t ninsts) {
+    auto* h = new OrcScene();
+    setup_instanced(h->S, h->W0, verts, faces, nfaces, mats, normals, leaf, meshes, nmeshes, insts, ninsts);
+    return h;
+}
+
+// Tracer::reinstance (pose.rs:105-120): new matrices for the same instances,
+// the top tree again, the emitter table again.
+void orc_scene_reinstance(void* handle, const phx_instance* insts, uint32_t ninsts) {
+    OrcScene* h = (OrcScene*)handle;
+    for (uint32_t i = 0; i < ninsts && i < h->S.insts.size(); i++) {
+        const uint32_t mesh = h->S.insts[i].mesh;
+        h->S.insts[i] = inst_of(insts[i]);
+        h->S.insts[i].mesh = mesh;
+    }
+    retlas(h->S);
+    relight(h->S, h->W0);
+}
+
+// Primary hits and ray-buffer walks of a scene handle (as orc_primary and
+// orc_trace_rays, which build a single-instance scene of their own).
+void orc_scene_primary(void* handle, const phx_camera* cam, uint32_t frame, uint32_t* ids, float* ts, uint32_t* insts) {
+    const OrcScene* h = (const OrcScene*)handle;
+    const uint32_t n = cam->w * cam->h;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        World W = h->W0;
+        W.p = cam;
+        W.n = n;
+        uint32_t seed = hash((uint32_t)i * 9781u + frame * 6271u + 1u);
+        const CamRay cr = camera_ray(W, (uint32_t)i, &seed);
+        const Hit hh = trace(W, cr.o, cr.d, INF, false);
+        ids[i] = hh.tri == NONE ? NONE : h->S.order[hh.tri];
+        ts[i] = hh.t;
+        if (insts) insts[i] = hh.tri == NONE ? NONE : hh.inst;
+    }
+}
+
+void orc_scene_trace_rays(void* handle, const float* rays, uint32_t n, float* hits, int any_hit) {
+    const OrcScene* h = (const OrcScene*)handle;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        World W = h->W0;
+        const float* r = rays + 8 * (size_t)i;
+        const Hit hh = trace(W, v3(r[0], r[1], r[2]), v3(r[4], r[5], r[6]), r[3], any_hit != 0);
+        hits[4 * i] = hh.t;
+        hits[4 * i + 1] = f_of(hh.tri == NONE ? NONE : h->S.order[hh.tri]);
+        hits[4 * i + 2] = hh.u;
+        hits[4 * i + 3] = hh.v;
+    }
+}
 
 // adapt.wgsl and gather.wgsl: the tail after `sample` — the convergence
 // check at a step boundary past the minimum, the dilation over the four

@@ -61,6 +61,10 @@ SIGNATURES: dict[str, tuple] = {
     "phx_ctx_create": (i32, [i32, C.POINTER(vp)]),
     "phx_ctx_destroy": (i32, [vp]),
     "phx_ctx_wait": (i32, [vp, u32]),
+    "phx_tracer_create_instanced": (i32, [vp, vp, vp, u32, vp, u32, vp]),
+    "phx_tracer_reinstance": (i32, [vp, vp, u32]),
+    "phx_tracer_trace_rows": (i32, [vp, vp, u32, u32, u32, u32, u32, u32]),
+    "phx_tracer_copy_rows": (i32, [vp, u32, u32, vp, i32]),
     "phx_selftest_wait": (i32, [vp, i32, u32, i32]),
     "phx_ctx_stream": (vp, [vp]),
     "phx_ctx_set_stream": (i32, [vp, vp]),

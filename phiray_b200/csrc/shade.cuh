@@ -8,12 +8,15 @@
 // fresnel_of, dielectric_f0, under_layer(_real), env_brdf, brdf_w,
 // ggx_pdf, glossy_floor), util.wgsl (hash, rnd, unit_disk), view.wgsl.
 //
-// The scene is one identity instance (the configs place every mesh in world
-// space), so the reference's top-tree walk plus one trace_blas is a single
-// walk of the mesh tree here, in the same order: root box, near child
-// first, strict `t < best`. Features the configs do not use (textures,
-// procedural slots, environment images, depth of field, adaptive sampling,
-// the grid overlay, film transparency) are refused on the host.
+// A scene is either one identity instance (every mesh in world space: the
+// reference's top-tree walk plus one trace_blas is then a single walk of the
+// mesh tree, in the same order: root box, near child first, strict
+// `t < best`), or meshes placed by instances: a top tree over the instances'
+// world boxes, each leaf's instances walked in turn with the ray taken into
+// the mesh's space by the instance's inverse (bvh.wgsl trace, trace_blas).
+// Features the tracer does not take (textures, procedural slots,
+// environment images, depth of field, film transparency) are refused on the
+// host.
 //
 // Layout the walk reads (built from the LBVH after every build/refit):
 //   nodes  4 float4 per inner node: both children's boxes, then their refs
@@ -22,6 +25,12 @@
 //          c.xyz + flags (bit 0: last slot of its leaf; bit 1: a shadow
 //          ray passes it — glass or cut-out, bvh.wgsl:158-162)
 // so one step is one 64-byte node read and one triangle one 48-byte read.
+// With instances the top tree's records come first (a leaf ref is
+// first top slot | LEAF | INST), then each mesh's; inst_slots[s] names top
+// slot s's instance (END on the last slot of a leaf), and each instance is a
+// record of 8 float4: the world matrix's rows (3), its inverse's rows (3),
+// the mesh's root box lo with the root ref in .w, and hi with the flags in
+// .w (bit 0 at the identity, 1 casts no shadow, 2 mirrors).
 #pragma once
 
 #include "internal.cuh"
@@ -31,6 +40,8 @@ namespace phx {
 namespace shade {
 
 constexpr uint32_t LEAF = 0x80000000u;
+constexpr uint32_t INST = 0x40000000u;      // a top-tree leaf: its range is instance slots (forest.rs INST)
+constexpr uint32_t INST_END = 0x80000000u;  // the last slot of a top-tree leaf (inst_slots)
 constexpr uint32_t NONE = 0xFFFFFFFFu;
 constexpr float INF = 3.0e38f;
 constexpr float PI = 3.14159265f;
@@ -46,6 +57,9 @@ struct Scene {
     const uint32_t* __restrict__ lamp_slot;
     const float* __restrict__ lamp_cdf;
     const float4* __restrict__ info;   // root box + ref, extent, emitter count (device results of the build)
+    const float4* __restrict__ insts;  // instance records, or null: one identity instance
+    const uint32_t* __restrict__ inst_slots;  // top slot -> instance (| INST_END)
+    const uint32_t* __restrict__ lamp_inst;   // the emitter table's instance column (instanced scenes)
     uint32_t nslots;  // triangles: a leaf walk never reads past them
     uint32_t lamp_count;
     uint32_t root;  // inner node 0, or LEAF | 0 when the root is a leaf
@@ -73,6 +87,7 @@ struct Hit {
     float t;
     uint32_t tri;  // sorted slot, NONE for a miss
     float u, v;
+    uint32_t inst;  // the instance the hit came through (0 for one identity instance)
 };
 
 // Rays traced by a thread, and (STATS builds) the walk's node steps and
@@ -224,13 +239,13 @@ struct Stack {
     __device__ __forceinline__ uint32_t& at(int k) { return SMEM ? shared[k * stride] : local[k]; }
 };
 
+// One tree's walk from its root (box test first), improving `best`; true
+// when an any-hit ray found its opaque hit. Hits record `inst`.
 template <bool STATS, bool SMEM = false>
-__device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool first, Count& cnt,
-                                    uint32_t* smem_stack = nullptr, int stride = 0) {
-    cnt.rays++;
-    Hit best{tmax, NONE, 0.0f, 0.0f};
+__device__ __forceinline__ bool walk_tree(const Tree S, f3 o, f3 d, Hit& best, bool first, uint32_t inst, Count& cnt,
+                                          uint32_t* smem_stack = nullptr, int stride = 0) {
     const f3 inv = safe_inv(d);
-    if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return best;
+    if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return false;
     const RaySpace rs = ray_space(d);
     Stack<SMEM> stack;
     stack.shared = smem_stack;
@@ -250,11 +265,11 @@ __device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool f
                 if (t < best.t) {
                     if (first) {
                         if (!(flags & FLAG_PASS)) {
-                            best = Hit{t, id, u, v};
-                            return best;
+                            best = Hit{t, id, u, v, inst};
+                            return true;
                         }
                     } else {
-                        best = Hit{t, id, u, v};
+                        best = Hit{t, id, u, v, inst};
                     }
                 }
                 if (flags & FLAG_END) break;
@@ -286,7 +301,101 @@ __device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool f
         sp--;
         nd = stack.at(sp);
     }
+    return false;
+}
+
+// A ray's walk of a single-instance scene's tree.
+template <bool STATS, bool SMEM = false>
+__device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool first, Count& cnt,
+                                    uint32_t* smem_stack = nullptr, int stride = 0) {
+    cnt.rays++;
+    Hit best{tmax, NONE, 0.0f, 0.0f, 0u};
+    walk_tree<STATS, SMEM>(S, o, d, best, first, 0u, cnt, smem_stack, stride);
     return best;
+}
+
+__device__ __forceinline__ float row_point(float4 r, f3 p) { return ((r.x * p.x + r.y * p.y) + r.z * p.z) + r.w * 1.0f; }
+__device__ __forceinline__ float row_dir(float4 r, f3 d) { return (r.x * d.x + r.y * d.y) + r.z * d.z; }
+
+// trace_blas (bvh.wgsl:115-190): instance i's mesh tree, walked in the mesh's
+// space (the ray taken there by the instance's inverse, its direction left
+// unnormalised so t is the world's); a shadow ray passes an instance that
+// casts none. True when an any-hit ray found its hit.
+template <bool STATS, bool SMEM>
+__device__ __forceinline__ bool walk_instance(const Scene& S, uint32_t i, f3 ow, f3 dw, Hit& best, bool first,
+                                              Count& cnt, uint32_t* smem_stack, int stride) {
+    const float4* q = S.insts + 8 * (size_t)i;
+    const float4 lo = __ldg(q + 6), hi = __ldg(q + 7);
+    const uint32_t root = __float_as_uint(lo.w), flags = __float_as_uint(hi.w);
+    if (root == NONE) return false;
+    if (first && (flags & 2u)) return false;
+    f3 o = ow, d = dw;
+    if (!(flags & 1u)) {
+        const float4 i0 = __ldg(q + 3), i1 = __ldg(q + 4), i2 = __ldg(q + 5);
+        o = mk(row_point(i0, ow), row_point(i1, ow), row_point(i2, ow));
+        d = mk(row_dir(i0, dw), row_dir(i1, dw), row_dir(i2, dw));
+    }
+    const Tree T{S.nodes, S.tris, S.nslots, root, xyz(lo), xyz(hi)};
+    return walk_tree<STATS, SMEM>(T, o, d, best, first, i, cnt, smem_stack, stride);
+}
+
+// trace (bvh.wgsl:194-232) over a scene of instances: the top tree over
+// their world boxes, near child first; at a leaf each of its instances'
+// trees in slot order; an any-hit ray stops at its first hit. The top
+// walk's stack is a second 32-entry stack (the reference's trace and
+// trace_blas each keep one).
+template <bool STATS, bool SMEM = false>
+__device__ __forceinline__ Hit walk_forest(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt,
+                                           uint32_t* smem_stack = nullptr, int stride = 0) {
+    cnt.rays++;
+    Hit best{tmax, NONE, 0.0f, 0.0f, 0u};
+    const f3 inv = safe_inv(d);
+    if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return best;
+    uint32_t stack[STACK];
+    int sp = 0;
+    uint32_t nd = S.root;
+    for (;;) {
+        if (nd & LEAF) {
+            for (uint32_t s = nd & ~(LEAF | INST);; s++) {
+                const uint32_t e = __ldg(S.inst_slots + s);
+                if (walk_instance<STATS, SMEM>(S, e & ~INST_END, o, d, best, first, cnt, smem_stack, stride))
+                    return best;
+                if (e & INST_END) break;
+            }
+        } else {
+            if (STATS) cnt.steps++;
+            const float4* q = S.nodes + 4 * (size_t)nd;
+            const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3);
+            const float tl = box_t(mk(n0.x, n0.y, n0.z), mk(n0.w, n1.x, n1.y), o, inv, best.t);
+            const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
+            const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
+            if (tl < INF && tr < INF) {
+                if (sp < STACK) stack[sp++] = tl <= tr ? r : l;
+                nd = tl <= tr ? l : r;
+                continue;
+            }
+            if (tl < INF) {
+                nd = l;
+                continue;
+            }
+            if (tr < INF) {
+                nd = r;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        sp--;
+        nd = stack[sp];
+    }
+    return best;
+}
+
+// A ray's walk of either kind of scene.
+template <bool STATS, bool SMEM = false>
+__device__ __forceinline__ Hit walk_scene(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt,
+                                          uint32_t* smem_stack = nullptr, int stride = 0) {
+    if (S.insts) return walk_forest<STATS, SMEM>(S, o, d, tmax, first, cnt, smem_stack, stride);
+    return walk<STATS, SMEM>(tree_of(S), o, d, tmax, first, cnt, smem_stack, stride);
 }
 
 // The walk behind a call, for code with several trace sites.
@@ -294,8 +403,11 @@ template <bool STATS>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     if (S.smem_stack) {
         extern __shared__ uint32_t walk_stacks[];
+        if (S.insts)
+            return walk_forest<STATS, true>(S, o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
         return walk<STATS, true>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
     }
+    if (S.insts) return walk_forest<STATS>(S, o, d, tmax, first, cnt);
     return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 
@@ -336,9 +448,21 @@ __device__ __forceinline__ Mat mat_at(const Scene& S, uint32_t m) {
 struct Geo {
     f3 a, b, c, na, nb, nc;
     uint32_t face, mat;
+    bool mirror;  // placed by a mirroring instance: world_ng turns the face normal back
 };
 
-__device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot) {
+// place_n (layout.wgsl:72-77): a normal under the inverse-transpose of an
+// instance's 3 x 3, unit again; a zero (flat) normal stays zero.
+__device__ __forceinline__ f3 place_n(float4 i0, float4 i1, float4 i2, f3 n) {
+    const f3 m = xyz(i0) * n.x + xyz(i1) * n.y + xyz(i2) * n.z;
+    const float l = length(m);
+    if (l < 1e-12f) return mk(0.0f);
+    return m / l;
+}
+
+// tri_of (layout.wgsl:114-159): the face in `slot`, placed in the world by
+// instance `inst` (vertices are kept in the mesh's space, w = 1).
+__device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot, uint32_t inst = 0u) {
     const float4 A = __ldg(S.tris + 3 * (size_t)slot), B = __ldg(S.tris + 3 * (size_t)slot + 1),
                  Cc = __ldg(S.tris + 3 * (size_t)slot + 2);
     Geo g;
@@ -353,6 +477,22 @@ __device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot) {
         g.nc = xyz(__ldg(S.tnorm + 3 * (size_t)slot + 2));
     } else {
         g.na = g.nb = g.nc = mk(0.0f);
+    }
+    g.mirror = false;
+    if (S.insts) {
+        const float4* q = S.insts + 8 * (size_t)inst;
+        const uint32_t flags = __float_as_uint(__ldg(q + 7).w);
+        g.mirror = (flags & 4u) != 0u;
+        if (!(flags & 1u)) {
+            const float4 r0 = __ldg(q), r1 = __ldg(q + 1), r2 = __ldg(q + 2);
+            g.a = mk(row_point(r0, g.a), row_point(r1, g.a), row_point(r2, g.a));
+            g.b = mk(row_point(r0, g.b), row_point(r1, g.b), row_point(r2, g.b));
+            g.c = mk(row_point(r0, g.c), row_point(r1, g.c), row_point(r2, g.c));
+            const float4 i0 = __ldg(q + 3), i1 = __ldg(q + 4), i2 = __ldg(q + 5);
+            g.na = place_n(i0, i1, i2, g.na);
+            g.nb = place_n(i0, i1, i2, g.nb);
+            g.nc = place_n(i0, i1, i2, g.nc);
+        }
     }
     return g;
 }
@@ -654,16 +794,20 @@ __device__ __forceinline__ Shadowed lamp_query(const Frame& F, const Surf& s, ui
     return Shadowed{brdf(s, l, e) * weight, l, sqrtf(d2) * 0.999f};
 }
 
-__device__ __forceinline__ float lamp_chance(const Scene& S, uint32_t slot) {
+// lamp_chance (light.wgsl:259-271): the table share of the hit's (face,
+// instance) pair, the entries sorted by face, then instance.
+__device__ __forceinline__ float lamp_chance(const Scene& S, uint32_t slot, uint32_t inst) {
     const uint32_t count = S.lamp_count;
     if (count == 0u) return 0.0f;
     uint32_t lo = 0, hi = count - 1u;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2u;
-        if (__ldg(S.lamp_slot + mid) < slot) lo = mid + 1u;
+        const uint32_t f = __ldg(S.lamp_slot + mid);
+        const uint32_t i = S.lamp_inst ? __ldg(S.lamp_inst + mid) : 0u;
+        if (f < slot || (f == slot && i < inst)) lo = mid + 1u;
         else hi = mid;
     }
-    if (__ldg(S.lamp_slot + lo) != slot) return 0.0f;
+    if (__ldg(S.lamp_slot + lo) != slot || (S.lamp_inst ? __ldg(S.lamp_inst + lo) : 0u) != inst) return 0.0f;
     const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
     return __ldg(S.lamp_cdf + lo) - prev;
 }
@@ -681,7 +825,7 @@ __device__ __forceinline__ Shadowed glow_query(const Scene& S, const Surf& s, ui
     const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
     const float chance = fmaxf(__ldg(S.lamp_cdf + lo) - prev, 1e-8f);
     const uint32_t f = __ldg(S.lamp_slot + lo);
-    const Geo g = geo_at(S, f);
+    const Geo g = geo_at(S, f, S.lamp_inst ? __ldg(S.lamp_inst + lo) : 0u);
     const Mat t = mat_at(S, g.mat);
     float a = rnd(seed);
     float b = rnd(seed);

@@ -10,6 +10,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
+#include <cmath>
+#include <memory>
 #include <cstring>
 #include <vector>
 
@@ -63,8 +65,18 @@ __global__ void k_mark_ends(const float4* __restrict__ nodes, const uint32_t* __
     c->w = __uint_as_float(__float_as_uint(c->w) | FLAG_END);
 }
 
-// Inner node i -> both children's boxes and refs (leaf child: first | LEAF).
-__global__ void k_convert(const float4* __restrict__ nodes, uint32_t ninner, float4* __restrict__ out) {
+// A child's ref in the walk's records: an inner node's record index (its
+// Karras index + inner_base), or for a leaf its first slot + leaf_base with
+// LEAF and leaf_bits (INST for a top-tree leaf).
+__device__ __forceinline__ uint32_t child_ref(uint32_t node_word, uint32_t index, uint32_t inner_base,
+                                              uint32_t leaf_base, uint32_t leaf_bits) {
+    if (node_word & LEAF) return ((node_word & ~LEAF) + leaf_base) | LEAF | leaf_bits;
+    return index + inner_base;
+}
+
+// Inner node i -> both children's boxes and refs, into record inner_base + i.
+__global__ void k_convert(const float4* __restrict__ nodes, uint32_t ninner, float4* __restrict__ out,
+                          uint32_t inner_base, uint32_t leaf_base, uint32_t leaf_bits) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninner) return;
     const float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
@@ -72,8 +84,9 @@ __global__ void k_convert(const float4* __restrict__ nodes, uint32_t ninner, flo
     if (li & LEAF) return;  // a packed leaf: never walked as an inner node
     const float4 la = nodes[2 * (size_t)li], lb = nodes[2 * (size_t)li + 1];
     const float4 ra = nodes[2 * (size_t)ri], rb = nodes[2 * (size_t)ri + 1];
-    const uint32_t lr = (__float_as_uint(la.w) & LEAF) ? __float_as_uint(la.w) : li;
-    const uint32_t rr = (__float_as_uint(ra.w) & LEAF) ? __float_as_uint(ra.w) : ri;
+    const uint32_t lr = child_ref(__float_as_uint(la.w), li, inner_base, leaf_base, leaf_bits);
+    const uint32_t rr = child_ref(__float_as_uint(ra.w), ri, inner_base, leaf_base, leaf_bits);
+    out += 4 * (size_t)inner_base;
     float4* q = out + 4 * (size_t)i;
     q[0] = make_float4(la.x, la.y, la.z, lb.x);
     q[1] = make_float4(lb.y, lb.z, ra.x, ra.y);
@@ -82,11 +95,11 @@ __global__ void k_convert(const float4* __restrict__ nodes, uint32_t ninner, flo
 }
 
 // Root box, root ref and the scene extent (Forest::extent, forest.rs:192-200:
-// the root box's diagonal, at least 1e-3).
-__global__ void k_root(const float4* __restrict__ nodes, uint32_t n, float4* info) {
+// the root box's diagonal, at least 1e-3). leaf_bits: INST for a top tree.
+__global__ void k_root(const float4* __restrict__ nodes, uint32_t n, float4* info, uint32_t leaf_bits) {
     const float4 a = nodes[0], b = nodes[1];
     const uint32_t li = __float_as_uint(a.w);
-    const uint32_t root = (li & LEAF) ? li : 0u;
+    const uint32_t root = (li & LEAF) ? (li | leaf_bits) : 0u;
     float e = 0.0f;
     const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
     e = e + dx * dx;
@@ -164,6 +177,161 @@ __global__ void __launch_bounds__(1024) k_lamps(const float4* __restrict__ tris,
     }
 }
 
+// ---- scenes of instances (forest.rs, instance.rs, lamp.rs) ----
+
+// slot s of a mesh's range [lo, lo + n) -> the face it holds, from the
+// mesh tree's order (Forest::build's order: faces permuted within the range).
+__global__ void k_mesh_order(const uint32_t* __restrict__ order, uint32_t n, uint32_t lo, uint32_t* __restrict__ out) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) out[lo + s] = lo + order[s];
+}
+
+// A mesh's root record (2 float4): its tree's root box, the root's ref
+// (record index, or first slot | LEAF), both in the walk's numbering.
+__global__ void k_mesh_root(const float4* __restrict__ nodes, float4* __restrict__ rec, uint32_t inner_base,
+                            uint32_t leaf_base) {
+    const float4 a = nodes[0], b = nodes[1];
+    const uint32_t root = child_ref(__float_as_uint(a.w), 0u, inner_base, leaf_base, 0u);
+    rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(root));
+    rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
+}
+
+// Each instance's mesh root box and ref (words 6 and 7 of its record), with
+// its flags; a mesh with no faces has root NONE (never walked).
+__global__ void k_inst_fill(float4* __restrict__ rec, const float4* __restrict__ mesh_rec,
+                            const uint32_t* __restrict__ mesh_of, const uint32_t* __restrict__ flags, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 lo = mesh_rec[2 * (size_t)mesh_of[i]], hi = mesh_rec[2 * (size_t)mesh_of[i] + 1];
+    rec[8 * (size_t)i + 6] = lo;
+    rec[8 * (size_t)i + 7] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(flags[i]));
+}
+
+// Instance::world_box (instance.rs:118-127): the eight corners of the mesh's
+// root box placed in the world, for the placed instances (top-tree prims).
+__global__ void k_inst_boxes(const float4* __restrict__ rec, const uint32_t* __restrict__ placed, uint32_t n,
+                             phx_aabb* __restrict__ boxes) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4* q = rec + 8 * (size_t)placed[k];
+    const float4 r[3] = {q[0], q[1], q[2]};
+    const float4 lo = q[6], hi = q[7];
+    float bl[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bh[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int c = 0; c < 8; c++) {
+        const f3 p = mk((c & 1) == 0 ? lo.x : hi.x, (c & 2) == 0 ? lo.y : hi.y, (c & 4) == 0 ? lo.z : hi.z);
+        for (int j = 0; j < 3; j++) {
+            const float w = row_point(r[j], p);
+            bl[j] = fminf(bl[j], w);
+            bh[j] = fmaxf(bh[j], w);
+        }
+    }
+    phx_aabb b;
+    b.lo[0] = bl[0], b.lo[1] = bl[1], b.lo[2] = bl[2], b.pad_a = 0.0f;
+    b.hi[0] = bh[0], b.hi[1] = bh[1], b.hi[2] = bh[2], b.pad_b = 0.0f;
+    boxes[k] = b;
+}
+
+// inst_order (forest.rs:119): top slot -> instance.
+__global__ void k_inst_slots(const uint32_t* __restrict__ order, const uint32_t* __restrict__ placed, uint32_t n,
+                             uint32_t* __restrict__ slots) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) slots[s] = placed[order[s]];
+}
+
+// The last slot of every top-tree leaf gets INST_END.
+__global__ void k_inst_ends(const float4* __restrict__ nodes, const uint32_t* __restrict__ starts,
+                            const uint32_t* __restrict__ nstarts, uint32_t* slots) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *nstarts) return;
+    const uint32_t end = __float_as_uint(nodes[2 * (size_t)starts[t] + 1].w);
+    slots[end - 1] |= INST_END;
+}
+
+// lamp.rs table_of with instances: every emissive slot (slot order), once for
+// each instance of its mesh (instance order), its power the face's world
+// area times the emitted luminance; then the running share. One block:
+// counts per thread chunk, a block scan for positions, one thread sums in
+// table order so the CDF rounds as the CPU's does.
+__global__ void __launch_bounds__(1024) k_lamps_inst(const float4* __restrict__ tris, const float4* __restrict__ mats,
+                                                     const float4* __restrict__ rec,
+                                                     const uint32_t* __restrict__ slot_mesh,
+                                                     const uint32_t* __restrict__ mesh_off,
+                                                     const uint32_t* __restrict__ mesh_list, uint32_t n,
+                                                     uint32_t* __restrict__ slots, uint32_t* __restrict__ insts,
+                                                     float* __restrict__ power, float* __restrict__ cdf, float4* info) {
+    __shared__ uint32_t s_count[1024];
+    const uint32_t T = blockDim.x, t = threadIdx.x;
+    const uint32_t chunk = (n + T - 1) / T;
+    const uint32_t lo = t * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    // power of (slot s, instance i), or 0
+    auto glow = [&](uint32_t s, uint32_t i) -> float {
+        const float4 A = __ldg(tris + 3 * (size_t)s), B = __ldg(tris + 3 * (size_t)s + 1),
+                     Cc = __ldg(tris + 3 * (size_t)s + 2);
+        const uint32_t m = __float_as_uint(B.w);
+        const float4 e = __ldg(mats + 8 * (size_t)m + 2);
+        const float lum = 0.2126f * e.x + 0.7152f * e.y + 0.0722f * e.z;
+        if (!(lum > 0.0f)) return 0.0f;
+        const float4* q = rec + 8 * (size_t)i;
+        const float4 r0 = q[0], r1 = q[1], r2 = q[2];
+        const f3 a = mk(row_point(r0, xyz(A)), row_point(r1, xyz(A)), row_point(r2, xyz(A)));
+        const f3 b = mk(row_point(r0, xyz(B)), row_point(r1, xyz(B)), row_point(r2, xyz(B)));
+        const f3 c = mk(row_point(r0, xyz(Cc)), row_point(r1, xyz(Cc)), row_point(r2, xyz(Cc)));
+        const float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
+        const float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
+        const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        float sq = 0.0f;
+        sq = sq + cx * cx;
+        sq = sq + cy * cy;
+        sq = sq + cz * cz;
+        const float p = 0.5f * sqrtf(sq) * lum;
+        return p > 0.0f ? p : 0.0f;
+    };
+    uint32_t c = 0;
+    for (uint32_t s = lo; s < hi; s++) {
+        const uint32_t k = slot_mesh[s];
+        if (k == NONE) continue;
+        for (uint32_t j = mesh_off[k]; j < mesh_off[k + 1]; j++)
+            if (glow(s, mesh_list[j]) > 0.0f) c++;
+    }
+    s_count[t] = c;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < T; k++) {
+            const uint32_t v = s_count[k];
+            s_count[k] = run;
+            run += v;
+        }
+        info[2] = make_float4(__uint_as_float(run), 0.0f, 0.0f, 0.0f);
+    }
+    __syncthreads();
+    uint32_t at = s_count[t];
+    for (uint32_t s = lo; s < hi; s++) {
+        const uint32_t k = slot_mesh[s];
+        if (k == NONE) continue;
+        for (uint32_t j = mesh_off[k]; j < mesh_off[k + 1]; j++) {
+            const float p = glow(s, mesh_list[j]);
+            if (p > 0.0f) {
+                slots[at] = s;
+                insts[at] = mesh_list[j];
+                power[at] = p;
+                at++;
+            }
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        const uint32_t count = __float_as_uint(info[2].x);
+        float total = 0.0f;
+        for (uint32_t k = 0; k < count; k++) total += power[k];
+        float run = 0.0f;
+        for (uint32_t k = 0; k < count; k++) {
+            run += power[k];
+            cdf[k] = run / total;
+        }
+    }
+}
+
 // ---- the sample kernel (shade.wgsl main) ----
 
 struct Sums {
@@ -206,7 +374,7 @@ __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s,
 
 // glow_mis (integrate.wgsl:15-23).
 __device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, const Hit& h, f3 from_n, f3 dir) {
-    const float chance = lamp_chance(S, h.tri);
+    const float chance = lamp_chance(S, h.tri, h.inst);
     if (chance <= 0.0f) return emit;
     const f3 cr = cross(g.b - g.a, g.c - g.a);
     const float pl = chance * h.t * h.t / fmaxf(0.5f * length(cr) * fabsf(dot(normalize(cr), dir)), 1e-8f);
@@ -247,7 +415,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
             break;
         }
         if (!bounce) break;
-        const Geo g = geo_at(S, h.tri);
+        const Geo g = geo_at(S, h.tri, h.inst);
         const Mat t = mat_at(S, g.mat);
         const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
         const f3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
@@ -286,7 +454,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
 template <bool STATS>
 __device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const Hit& h, f3 org, f3 d,
                                            uint32_t& seed, f3 sun, Count& cnt) {
-    const Geo g = geo_at(S, h.tri);
+    const Geo g = geo_at(S, h.tri, h.inst);
     const Mat t = mat_at(S, g.mat);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
     const f3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
@@ -371,7 +539,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
             break;
         }
         if (bounce == 0u) {
-            acc.outline = 1u;
+            acc.outline = h.inst + 1u;  // outline_store(i, h.inst + 1)
             // emit's overlay term grid_over(o0, d0, first_t) is a function of
             // the first ray and hit alone: added once per sample here, where
             // they are at hand, instead of at emit (util.wgsl:101-145)
@@ -381,11 +549,12 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                 acc.cov += gr.a;
             }
         }
-        const Geo g = geo_at(S, h.tri);
+        const Geo g = geo_at(S, h.tri, h.inst);
         const Mat t = mat_at(S, g.mat);
         const float w = 1.0f - h.u - h.v;
         const f3 hit = o + d * h.t;
-        const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+        const f3 ngw = normalize(cross(g.b - g.a, g.c - g.a));
+        const f3 ng0 = g.mirror ? -ngw : ngw;  // world_ng (layout.wgsl:97-101)
         const bool front = dot(ng0, d) < 0.0f;
         const f3 ng = front ? ng0 : -ng0;
         f3 n = g.na * w + g.nb * h.u + g.nc * h.v;
@@ -890,18 +1059,19 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 return PH_EMIT_END;
             }
             if (P.bounce == 0u) {
-                acc.outline = 1u;
+                acc.outline = h.inst + 1u;
                 if (F.grid > 0.0f) {  // emit's overlay, as in sample()
                     const Over gr = grid_over(F, P.o, P.d, h.t);
                     acc.grid += gr.c;
                     acc.cov += gr.a;
                 }
             }
-            const Geo g = geo_at(S, h.tri);
+            const Geo g = geo_at(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const float w = 1.0f - h.u - h.v;
             const f3 hit = P.o + P.d * h.t;
-            const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
+            const f3 ngw = normalize(cross(g.b - g.a, g.c - g.a));
+            const f3 ng0 = g.mirror ? -ngw : ngw;  // world_ng
             const bool front = dot(ng0, P.d) < 0.0f;
             const f3 ng = front ? ng0 : -ng0;
             f3 n = g.na * w + g.nb * h.u + g.nc * h.v;
@@ -1016,7 +1186,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 P.aval = P.iacc;
                 return PH_AFTER_INDIRECT;
             }
-            const Geo g = geo_at(S, h.tri);
+            const Geo g = geo_at(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const f3 dir = P.idir;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -1097,7 +1267,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 return PH_AFTER_GLOSSY;
             }
             // bounce_light (integrate.wgsl:236-250) up to its direct().
-            const Geo g = geo_at(S, h.tri);
+            const Geo g = geo_at(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const f3 d = P.rd;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -1241,7 +1411,7 @@ __global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 su
         load_sums(px, F.n, P.i, F.frame0 > 0u, acc);
         ph = F.spp > 0u ? (uint32_t)PH_BEGIN_SAMPLE : (uint32_t)PH_FINISH_SAMPLE;
     }
-    Hit h{INF, NONE, 0.0f, 0.0f};
+    Hit h{INF, NONE, 0.0f, 0.0f, 0u};
     for (;;) {
         // run phases until the lane needs a ray or runs out of pixels
         while (ph != PH_TRACE && ph != PH_DONE) {
@@ -1267,7 +1437,7 @@ __global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 su
         }
         if (__all_sync(0xffffffffu, ph == PH_DONE)) break;
         if (ph == PH_TRACE) {
-            h = walk<STATS>(tree_of(S), P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
+            h = walk_scene<STATS>(S, P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
             ph = P.after;
         }
     }
@@ -1291,7 +1461,7 @@ __global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     Count cnt{0, 0, 0};
-    const Hit h = walk<false>(tree_of(S), cr.o, cr.d, INF, false, cnt);
+    const Hit h = walk_scene<false>(S, cr.o, cr.d, INF, false, cnt);
     ids[i] = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
     ts[i] = h.t;
 }
@@ -1304,13 +1474,13 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     Count cnt{0, 0, 0};
-    const Hit h = walk<false>(tree_of(S), cr.o, cr.d, INF, false, cnt);
+    const Hit h = walk_scene<false>(S, cr.o, cr.d, INF, false, cnt);
     if (h.tri == NONE) {
         rays[2 * (size_t)i] = make_float4(cr.o.x, cr.o.y, cr.o.z, 0.0f);
         rays[2 * (size_t)i + 1] = make_float4(cr.d.x, cr.d.y, cr.d.z, 0.0f);
         return;
     }
-    const Geo g = geo_at(S, h.tri);
+    const Geo g = geo_at(S, h.tri, h.inst);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
     const f3 ng = dot(ng0, cr.d) < 0.0f ? ng0 : -ng0;
     const f3 pos = cr.o + cr.d * h.t + ng * hit_lift(F, h.t);
@@ -1328,8 +1498,8 @@ __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict_
     Count cnt{0, 0, 0};
     if (i < n) {
         const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
-        const Hit h = walk<STATS, SMEM>(tree_of(S), mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt,
-                                        s_stack + threadIdx.x, 128);
+        const Hit h = walk_scene<STATS, SMEM>(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt,
+                                              s_stack + threadIdx.x, 128);
         const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
         hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
     }
@@ -1509,7 +1679,7 @@ __global__ void k_ray_keys(Scene S, const float4* __restrict__ rays, uint32_t n,
 template <bool ANY, bool STATS>
 void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters, bool smem,
                  cudaStream_t s, uint32_t* next = nullptr, int sms = 0, const uint32_t* order = nullptr) {
-    if (next) {
+    if (next && !S.insts) {  // (scenes of instances: a thread per ray)
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rays_fetch<ANY, STATS>, 128, 0);
         const uint32_t grid = std::min<uint32_t>((uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms, (n + 127) / 128);
@@ -1528,9 +1698,26 @@ void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, uns
 
 using namespace phx;
 
+// A scene of meshes placed by instances (phx_tracer_create_instanced): each
+// mesh's own LBVH over its faces in its own space, the top tree over the
+// placed instances' world boxes, the instance records and the emitter
+// table's instance column. Absent: one identity instance over tr->bvh.
+struct Forest {
+    std::vector<phx_mesh> meshes;
+    std::vector<std::unique_ptr<BvhWork>> trees;  // per mesh; null for a mesh with no faces
+    std::vector<uint32_t> node_base;              // per mesh: its first record in tnodes
+    std::vector<phx_instance> insts;              // as given (host)
+    std::vector<uint32_t> placed;                 // instances whose mesh has faces
+    uint32_t top_records = 1;                     // records kept for the top tree
+    uint32_t lamp_cap = 0;                        // entries the emitter table can hold
+    BvhWork top;
+    DevMem rec, flags, mesh_of, placed_dev, mesh_rec, slots, order_all, lamp_inst, slot_mesh, mesh_off, mesh_list;
+};
+
 struct phx_tracer_s {
     Ctx* ctx = nullptr;
     uint32_t nverts = 0, nfaces = 0, nmats = 0, leaf = 4;
+    std::unique_ptr<Forest> forest;
     bool has_normals = false;
     bool emissive = false;  // some material emits: the emitter table is built
     DevMem verts, vnorm, faces, mats, tnodes, tris, tnorm, lamp_slot, lamp_power, lamp_cdf, info, px, rays, cam;
@@ -1568,8 +1755,9 @@ int32_t prepare(phx_tracer tr) {
     k_mark_ends<<<(n + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr,
                                                 w.nstarts(), (float4*)tr->tris.ptr);
     if (n > 1)
-        k_convert<<<(n - 1 + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, n - 1, (float4*)tr->tnodes.ptr);
-    k_root<<<1, 1, 0, s>>>((const float4*)w.nodes.ptr, n, (float4*)tr->info.ptr);
+        k_convert<<<(n - 1 + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, n - 1, (float4*)tr->tnodes.ptr, 0u,
+                                                      0u, 0u);
+    k_root<<<1, 1, 0, s>>>((const float4*)w.nodes.ptr, n, (float4*)tr->info.ptr, 0u);
     if (tr->emissive)
         k_lamps<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, n,
                                    (uint32_t*)tr->lamp_slot.ptr, (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr,
@@ -1577,6 +1765,156 @@ int32_t prepare(phx_tracer tr) {
     else  // no material emits: an empty table (the count word of info[2])
         PHX_CUDA(cudaMemsetAsync((float4*)tr->info.ptr + 2, 0, sizeof(float4), s));
     return cuda_check(cudaGetLastError(), "tracer prepare");
+}
+
+// A float with the given bits, on the host.
+inline float host_bits(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Instance::inverse and words (instance.rs:60-157) on the host: rows of the
+// world matrix (m[col][row] -> row r = m[0..3][r]) and of its inverse (the
+// upper 3 x 3 inverted, the translation undone; zero for a singular matrix),
+// and the flags (bit 0 at the identity, 1 casts no shadow, 2 mirrors).
+void inst_words(const phx_instance& src, float4 out[6], uint32_t* flags) {
+    const float* m = src.world;
+    auto a = [&](int r, int c) { return m[4 * c + r]; };
+    float row[3][4], inv4[3][4];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 4; c++) row[r][c] = m[4 * c + r];
+    const float det = a(0, 0) * (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) - a(0, 1) * (a(1, 0) * a(2, 2) - a(1, 2) * a(2, 0)) +
+                      a(0, 2) * (a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0));
+    if (std::fabs(det) < 1e-20f) {
+        std::memset(inv4, 0, sizeof inv4);
+    } else {
+        const float d = 1.0f / det;
+        const float inv[3][3] = {
+            {(a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) * d, (a(0, 2) * a(2, 1) - a(0, 1) * a(2, 2)) * d,
+             (a(0, 1) * a(1, 2) - a(0, 2) * a(1, 1)) * d},
+            {(a(1, 2) * a(2, 0) - a(1, 0) * a(2, 2)) * d, (a(0, 0) * a(2, 2) - a(0, 2) * a(2, 0)) * d,
+             (a(0, 2) * a(1, 0) - a(0, 0) * a(1, 2)) * d},
+            {(a(1, 0) * a(2, 1) - a(1, 1) * a(2, 0)) * d, (a(0, 1) * a(2, 0) - a(0, 0) * a(2, 1)) * d,
+             (a(0, 0) * a(1, 1) - a(0, 1) * a(1, 0)) * d},
+        };
+        const float t[3] = {m[12], m[13], m[14]};
+        for (int r = 0; r < 3; r++) {
+            for (int c = 0; c < 3; c++) inv4[r][c] = inv[r][c];
+            inv4[r][3] = -((inv[r][0] * t[0] + inv[r][1] * t[1]) + inv[r][2] * t[2]);
+        }
+    }
+    bool identity = true;
+    for (int k = 0; k < 16; k++) identity = identity && m[k] == ((k % 5 == 0) ? 1.0f : 0.0f);
+    for (int r = 0; r < 3; r++) {
+        out[r] = make_float4(row[r][0], row[r][1], row[r][2], row[r][3]);
+        out[3 + r] = make_float4(inv4[r][0], inv4[r][1], inv4[r][2], inv4[r][3]);
+    }
+    *flags = (identity ? 1u : 0u) | (src.casts_shadow ? 0u : 2u) | (det < 0.0f ? 4u : 0u);
+}
+
+// The instances' matrices and flags to the device, then Forest::retlas
+// (forest.rs:107-121): the top tree over the placed instances' world boxes
+// (one instance a leaf), its records, slot table and root info.
+int32_t retlas(phx_tracer tr) {
+    Forest& F = *tr->forest;
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    const uint32_t ni = (uint32_t)F.insts.size();
+    std::vector<float4> rec(8 * (size_t)ni, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    std::vector<uint32_t> flags(ni);
+    for (uint32_t i = 0; i < ni; i++) inst_words(F.insts[i], &rec[8 * (size_t)i], &flags[i]);
+    // the rows go up (words 6 and 7, the mesh root, are filled on the device)
+    for (uint32_t i = 0; i < ni; i++)
+        PHX_CUDA(cudaMemcpyAsync((float4*)F.rec.ptr + 8 * (size_t)i, &rec[8 * (size_t)i], 6 * sizeof(float4),
+                                 cudaMemcpyHostToDevice, s));
+    PHX_CUDA(cudaMemcpyAsync(F.flags.ptr, flags.data(), 4 * (size_t)ni, cudaMemcpyHostToDevice, s));
+    PHX_TRY(wait_stream(s, 0));  // the host staging vectors go out of scope
+    k_inst_fill<<<ceil_div(ni, 128), 128, 0, s>>>((float4*)F.rec.ptr, (const float4*)F.mesh_rec.ptr,
+                                                  (const uint32_t*)F.mesh_of.ptr, (const uint32_t*)F.flags.ptr, ni);
+    const uint32_t np = (uint32_t)F.placed.size();
+    if (np == 0) {  // nothing placed: an empty world (every ray misses)
+        const float4 empty[2] = {make_float4(1.0f, 1.0f, 1.0f, host_bits(LEAF | INST)),
+                                 make_float4(-1.0f, -1.0f, -1.0f, 1e-3f)};
+        PHX_CUDA(cudaMemcpyAsync(tr->info.ptr, empty, sizeof empty, cudaMemcpyHostToDevice, s));
+        return cuda_check(cudaGetLastError(), "retlas");
+    }
+    k_inst_boxes<<<ceil_div(np, 128), 128, 0, s>>>((const float4*)F.rec.ptr, (const uint32_t*)F.placed_dev.ptr, np,
+                                                   (phx_aabb*)F.top.prims.ptr);
+    PHX_TRY(enqueue_build(c, F.top, np, 1));
+    k_inst_slots<<<ceil_div(np, 256), 256, 0, s>>>((const uint32_t*)F.top.order.ptr, (const uint32_t*)F.placed_dev.ptr,
+                                                   np, (uint32_t*)F.slots.ptr);
+    k_inst_ends<<<ceil_div(np, 256), 256, 0, s>>>((const float4*)F.top.nodes.ptr, (const uint32_t*)F.top.starts.ptr,
+                                                  F.top.nstarts(), (uint32_t*)F.slots.ptr);
+    if (np > 1)
+        k_convert<<<ceil_div(np - 1, 256), 256, 0, s>>>((const float4*)F.top.nodes.ptr, np - 1, (float4*)tr->tnodes.ptr,
+                                                        0u, 0u, INST);
+    k_root<<<1, 1, 0, s>>>((const float4*)F.top.nodes.ptr, np, (float4*)tr->info.ptr, INST);
+    return cuda_check(cudaGetLastError(), "retlas");
+}
+
+// A forest's scene preparation after its meshes' trees were built or
+// refitted (their face boxes in each tree's prims): slot order, gathered
+// triangles, leaf ends, walk records, mesh roots, the top tree, the
+// emitter table.
+int32_t prepare_forest(phx_tracer tr) {
+    Forest& F = *tr->forest;
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    const uint32_t nm = (uint32_t)F.meshes.size();
+    for (uint32_t k = 0; k < nm; k++) {
+        const BvhWork* w = F.trees[k].get();
+        if (!w) continue;
+        const uint32_t lo = F.meshes[k].face_lo, n = F.meshes[k].face_hi - lo;
+        k_mesh_order<<<ceil_div(n, 256), 256, 0, s>>>((const uint32_t*)w->order.ptr, n, lo,
+                                                      (uint32_t*)F.order_all.ptr);
+    }
+    k_gather<<<ceil_div(tr->nfaces, 256), 256, 0, s>>>(
+        (const uint32_t*)F.order_all.ptr, (const uint4*)tr->faces.ptr, (const float4*)tr->verts.ptr,
+        tr->has_normals ? (const float4*)tr->vnorm.ptr : nullptr, (const float4*)tr->mats.ptr, tr->nmats, tr->nfaces,
+        (float4*)tr->tris.ptr, tr->has_normals ? (float4*)tr->tnorm.ptr : nullptr, c->status);
+    for (uint32_t k = 0; k < nm; k++) {
+        const BvhWork* w = F.trees[k].get();
+        if (!w) continue;
+        const uint32_t lo = F.meshes[k].face_lo, n = F.meshes[k].face_hi - lo;
+        k_mark_ends<<<ceil_div(n, 256), 256, 0, s>>>((const float4*)w->nodes.ptr, (const uint32_t*)w->starts.ptr,
+                                                     w->nstarts(), (float4*)tr->tris.ptr + 3 * (size_t)lo);
+        if (n > 1)
+            k_convert<<<ceil_div(n - 1, 256), 256, 0, s>>>((const float4*)w->nodes.ptr, n - 1, (float4*)tr->tnodes.ptr,
+                                                           F.node_base[k], lo, 0u);
+        k_mesh_root<<<1, 1, 0, s>>>((const float4*)w->nodes.ptr, (float4*)F.mesh_rec.ptr + 2 * (size_t)k,
+                                    F.node_base[k], lo);
+    }
+    PHX_TRY(retlas(tr));
+    if (tr->emissive)
+        k_lamps_inst<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr,
+                                        (const float4*)F.rec.ptr, (const uint32_t*)F.slot_mesh.ptr,
+                                        (const uint32_t*)F.mesh_off.ptr, (const uint32_t*)F.mesh_list.ptr, tr->nfaces,
+                                        (uint32_t*)tr->lamp_slot.ptr, (uint32_t*)F.lamp_inst.ptr,
+                                        (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr, (float4*)tr->info.ptr);
+    else
+        PHX_CUDA(cudaMemsetAsync((float4*)tr->info.ptr + 2, 0, sizeof(float4), s));
+    return cuda_check(cudaGetLastError(), "forest prepare");
+}
+
+// Face boxes of every face (into tr->bvh.prims), then each mesh's tree over
+// its own range: a fresh build (rebuild) or a refit.
+int32_t build_forest(phx_tracer tr, bool rebuild) {
+    Forest& F = *tr->forest;
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                              (phx_aabb*)tr->bvh.prims.ptr));
+    for (size_t k = 0; k < F.meshes.size(); k++) {
+        BvhWork* w = F.trees[k].get();
+        if (!w) continue;
+        const uint32_t lo = F.meshes[k].face_lo, n = F.meshes[k].face_hi - lo;
+        PHX_CUDA(cudaMemcpyAsync(w->prims.ptr, (const phx_aabb*)tr->bvh.prims.ptr + lo, (size_t)n * sizeof(phx_aabb),
+                                 cudaMemcpyDeviceToDevice, s));
+        if (rebuild) PHX_TRY(enqueue_build(c, *w, n, tr->leaf));
+        else PHX_TRY(enqueue_refit(c, *w, n, false));
+    }
+    return prepare_forest(tr);
 }
 
 // The scene record the kernels take (build-dependent fields are read from
@@ -1591,6 +1929,11 @@ Scene scene_of(phx_tracer tr) {
     S.lamp_slot = (const uint32_t*)tr->lamp_slot.ptr;
     S.lamp_cdf = (const float*)tr->lamp_cdf.ptr;
     S.info = (const float4*)tr->info.ptr;
+    if (tr->forest) {
+        S.insts = (const float4*)tr->forest->rec.ptr;
+        S.inst_slots = (const uint32_t*)tr->forest->slots.ptr;
+        S.lamp_inst = (const uint32_t*)tr->forest->lamp_inst.ptr;
+    }
     S.nslots = tr->nfaces;
     return S;
 }
@@ -1818,8 +2161,30 @@ int32_t launch_render(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t
 
 extern "C" {
 
-int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
+}  // extern "C"
+
+namespace {
+
+// Tracer::new (single identity instance: meshes null) or a scene of meshes
+// placed by instances (forest.rs Forest::build).
+int32_t create_tracer(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, uint32_t nmeshes,
+                      const phx_instance* insts, uint32_t ninsts, phx_tracer* out) {
     if (!ctx || !sc || !out) return fail(PHX_ERR_INVALID, "null argument");
+    if (meshes) {
+        // Forest::build's assumptions: meshes name ascending, disjoint face
+        // ranges; instances name meshes.
+        if (nmeshes == 0 || ninsts == 0 || !insts) return fail(PHX_ERR_INVALID, "an instanced scene needs meshes and instances");
+        uint32_t at = 0;
+        for (uint32_t k = 0; k < nmeshes; k++) {
+            if (meshes[k].face_lo < at || meshes[k].face_hi < meshes[k].face_lo || meshes[k].face_hi > sc->nfaces)
+                return fail(PHX_ERR_INVALID, "mesh %u: faces [%u, %u) out of order or range", k, meshes[k].face_lo,
+                            meshes[k].face_hi);
+            at = meshes[k].face_hi;
+        }
+        for (uint32_t i = 0; i < ninsts; i++)
+            if (insts[i].mesh >= nmeshes) return fail(PHX_ERR_INVALID, "instance %u names mesh %u", i, insts[i].mesh);
+        if (ninsts >= (1u << 30)) return fail(PHX_ERR_INVALID, "too many instances");
+    }
     if (sc->nfaces == 0) return fail(PHX_ERR_INVALID, "a tracer needs at least one face (Tracer::new declines an empty scene)");
     if (!sc->verts || !sc->faces || !sc->mats || sc->nmats == 0 || sc->nverts == 0)
         return fail(PHX_ERR_INVALID, "scene arrays missing");
@@ -1873,6 +2238,74 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     step(tr->cam.reserve(sizeof(phx_camera)));
     step(tr->next.reserve(16));
     step(tr->bvh.reserve(sc->nfaces, ctx->c.sms));
+    if (meshes && rc == PHX_OK) {
+        tr->forest.reset(new Forest());
+        Forest& F = *tr->forest;
+        F.meshes.assign(meshes, meshes + nmeshes);
+        F.insts.assign(insts, insts + ninsts);
+        F.trees.resize(nmeshes);
+        F.node_base.assign(nmeshes, 0u);
+        std::vector<uint32_t> count(nmeshes, 0u), mesh_of(ninsts), slot_mesh(sc->nfaces, NONE);
+        for (uint32_t i = 0; i < ninsts; i++) {
+            mesh_of[i] = insts[i].mesh;
+            count[insts[i].mesh]++;
+            if (meshes[insts[i].mesh].face_hi > meshes[insts[i].mesh].face_lo) F.placed.push_back(i);
+        }
+        std::vector<uint32_t> off(nmeshes + 1, 0u), list(ninsts);
+        for (uint32_t k = 0; k < nmeshes; k++) off[k + 1] = off[k] + count[k];
+        std::vector<uint32_t> fill(off.begin(), off.end() - 1);
+        for (uint32_t i = 0; i < ninsts; i++) list[fill[insts[i].mesh]++] = i;  // instance order within a mesh
+        F.top_records = std::max<uint32_t>(ninsts > 1 ? ninsts - 1 : 1, 1u);
+        uint32_t records = F.top_records;
+        uint64_t lamps = 0;
+        for (uint32_t k = 0; k < nmeshes; k++) {
+            const uint32_t n = meshes[k].face_hi - meshes[k].face_lo;
+            for (uint32_t f = meshes[k].face_lo; f < meshes[k].face_hi; f++) slot_mesh[f] = k;
+            lamps += (uint64_t)n * count[k];
+            if (n == 0) continue;
+            F.node_base[k] = records;
+            records += n - 1;
+            F.trees[k].reset(new BvhWork());
+            step(F.trees[k]->reserve(n, ctx->c.sms));
+        }
+        if (lamps >= (1u << 30)) step(fail(PHX_ERR_INVALID, "too many emitter entries"));
+        F.lamp_cap = (uint32_t)std::max<uint64_t>(lamps, 1);
+        step(F.top.reserve(std::max<uint32_t>(ninsts, 1u), ctx->c.sms));
+        step(F.rec.reserve((size_t)ninsts * 8 * 16));
+        step(F.flags.reserve((size_t)ninsts * 4));
+        step(F.mesh_of.reserve((size_t)ninsts * 4));
+        step(F.placed_dev.reserve(std::max<size_t>(F.placed.size(), 1) * 4));
+        step(F.mesh_rec.reserve((size_t)nmeshes * 32));
+        step(F.slots.reserve((size_t)std::max<uint32_t>(ninsts, 1u) * 4));
+        step(F.order_all.reserve(n * 4));
+        step(F.lamp_inst.reserve((size_t)F.lamp_cap * 4));
+        step(F.slot_mesh.reserve(n * 4));
+        step(F.mesh_off.reserve((size_t)(nmeshes + 1) * 4));
+        step(F.mesh_list.reserve((size_t)std::max<uint32_t>(ninsts, 1u) * 4));
+        step(tr->tnodes.reserve((size_t)records * 64));
+        if (tr->emissive) {
+            step(tr->lamp_slot.reserve((size_t)F.lamp_cap * 4));
+            step(tr->lamp_power.reserve((size_t)F.lamp_cap * 4));
+            step(tr->lamp_cdf.reserve((size_t)F.lamp_cap * 4));
+        }
+        // faces outside every mesh are in no tree: their slots keep their
+        // own face, never walked
+        std::vector<uint32_t> identity(sc->nfaces);
+        for (uint32_t f = 0; f < sc->nfaces; f++) identity[f] = f;
+        std::vector<float4> mesh_rec(2 * (size_t)nmeshes, make_float4(0.0f, 0.0f, 0.0f, host_bits(NONE)));
+        auto up = [&](DevMem& d, const void* src, size_t bytes) {
+            if (rc == PHX_OK && bytes)
+                rc = cuda_check(cudaMemcpyAsync(d.ptr, src, bytes, cudaMemcpyHostToDevice, s), "upload");
+        };
+        up(F.mesh_of, mesh_of.data(), mesh_of.size() * 4);
+        up(F.placed_dev, F.placed.data(), F.placed.size() * 4);
+        up(F.mesh_rec, mesh_rec.data(), mesh_rec.size() * sizeof(float4));
+        up(F.order_all, identity.data(), identity.size() * 4);
+        up(F.slot_mesh, slot_mesh.data(), slot_mesh.size() * 4);
+        up(F.mesh_off, off.data(), off.size() * 4);
+        up(F.mesh_list, list.data(), list.size() * 4);
+        if (rc == PHX_OK) rc = wait_stream(s, 0);  // staging vectors go out of scope
+    }
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev0), "event");
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev1), "event");
     if (rc == PHX_OK)
@@ -1886,8 +2319,12 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     if (rc == PHX_OK)
         rc = launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, sc->nfaces,
                                (phx_aabb*)tr->bvh.prims.ptr);
-    if (rc == PHX_OK) rc = enqueue_build(&ctx->c, tr->bvh, sc->nfaces, tr->leaf);
-    if (rc == PHX_OK) rc = prepare(tr);
+    if (tr->forest) {
+        if (rc == PHX_OK) rc = build_forest(tr, true);
+    } else {
+        if (rc == PHX_OK) rc = enqueue_build(&ctx->c, tr->bvh, sc->nfaces, tr->leaf);
+        if (rc == PHX_OK) rc = prepare(tr);
+    }
     if (rc == PHX_OK) rc = wait_stream(s, 0);
     if (rc == PHX_OK) rc = read_status(&ctx->c);
     if (rc != PHX_OK) {
@@ -1896,6 +2333,40 @@ int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
     }
     *out = tr;
     return PHX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t phx_tracer_create(phx_ctx ctx, const phx_scene* sc, phx_tracer* out) {
+    return create_tracer(ctx, sc, nullptr, 0, nullptr, 0, out);
+}
+
+int32_t phx_tracer_create_instanced(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, uint32_t nmeshes,
+                                    const phx_instance* insts, uint32_t ninsts, phx_tracer* out) {
+    if (!meshes) return fail(PHX_ERR_INVALID, "null mesh table");
+    return create_tracer(ctx, sc, meshes, nmeshes, insts, ninsts, out);
+}
+
+int32_t phx_tracer_reinstance(phx_tracer tr, const phx_instance* insts, uint32_t ninsts) {
+    if (!tr || !insts) return fail(PHX_ERR_INVALID, "null argument");
+    if (!tr->forest) return fail(PHX_ERR_INVALID, "the tracer was not built with instances");
+    Forest& F = *tr->forest;
+    if (ninsts != F.insts.size()) return fail(PHX_ERR_INVALID, "instance count %u, the tracer holds %zu", ninsts, F.insts.size());
+    for (uint32_t i = 0; i < ninsts; i++)
+        if (insts[i].mesh != F.insts[i].mesh) return fail(PHX_ERR_INVALID, "instance %u changed its mesh", i);
+    PHX_TRY(use(tr->ctx));
+    F.insts.assign(insts, insts + ninsts);
+    PHX_TRY(retlas(tr));
+    if (tr->emissive)
+        k_lamps_inst<<<1, 1024, 0, tr->ctx->stream>>>(
+            (const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, (const float4*)F.rec.ptr,
+            (const uint32_t*)F.slot_mesh.ptr, (const uint32_t*)F.mesh_off.ptr, (const uint32_t*)F.mesh_list.ptr,
+            tr->nfaces, (uint32_t*)tr->lamp_slot.ptr, (uint32_t*)F.lamp_inst.ptr, (float*)tr->lamp_power.ptr,
+            (float*)tr->lamp_cdf.ptr, (float4*)tr->info.ptr);
+    tr->have_last = false;  // the image starts again
+    return cuda_check(cudaGetLastError(), "reinstance");
 }
 
 int32_t phx_tracer_destroy(phx_tracer tr) {
@@ -1983,6 +2454,55 @@ int32_t phx_tracer_trace(phx_tracer tr, const phx_camera* cam, uint32_t w, uint3
     tr->last = *cam;
     std::memcpy(tr->last.adapt, tr->adapt, sizeof tr->adapt);
     tr->have_last = true;
+    return PHX_OK;
+}
+
+int32_t phx_tracer_trace_rows(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t first,
+                              uint32_t spp, uint32_t row0, uint32_t rows) {
+    if (!tr || !cam) return fail(PHX_ERR_INVALID, "null argument");
+    if (row0 > h || rows > h - row0) return fail(PHX_ERR_INVALID, "rows [%u, %u) outside the %u-row frame", row0, row0 + rows, h);
+    if (tr->adapt[3] != 0.0f) return fail(PHX_ERR_INVALID, "adaptive sampling traces whole frames");
+    PHX_TRY(check_camera(cam));
+    PHX_TRY(use(tr->ctx));
+    PHX_TRY(ensure_image(tr, w, h));
+    if (spp == 0 || rows == 0) return PHX_OK;
+    Ctx* c = tr->ctx;
+    PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 8, c->stream));
+    PHX_CUDA(cudaEventRecord(tr->ev0, c->stream));
+    PHX_TRY(launch_render(tr, cam, w, h, first, spp, row0 * w, rows * w));
+    PHX_CUDA(cudaEventRecord(tr->ev1, c->stream));
+    tr->frame = first + spp - 1;
+    tr->last = *cam;
+    std::memcpy(tr->last.adapt, tr->adapt, sizeof tr->adapt);
+    tr->have_last = true;
+    return PHX_OK;
+}
+
+// The planes a traced row carries, as (first plane, words a pixel): packed,
+// linear sums, shown, albedo, normal, depth, overlay, coverage, film,
+// outline, sample count, missed (read.rs:37-56).
+static const uint32_t ROW_PLANES[12][2] = {{0, 1},  {1, 3},  {4, 3},  {7, 3},  {10, 3}, {13, 1},
+                                            {20, 3}, {23, 1}, {24, 1}, {25, 1}, {31, 1}, {33, 1}};
+
+int32_t phx_tracer_copy_rows(phx_tracer tr, uint32_t row0, uint32_t rows, uint32_t* packed, int32_t into_image) {
+    if (!tr || (rows && !packed)) return fail(PHX_ERR_INVALID, "null argument");
+    if (!tr->px.ptr) return fail(PHX_ERR_INVALID, "no image yet");
+    if (row0 > tr->h || rows > tr->h - row0) return fail(PHX_ERR_INVALID, "rows outside the frame");
+    PHX_TRY(use(tr->ctx));
+    const size_t n = (size_t)tr->w * tr->h, w = tr->w;
+    uint32_t* px = (uint32_t*)tr->px.ptr;
+    size_t at = 0;
+    for (const auto& pl : ROW_PLANES) {
+        uint32_t* img = px + pl[0] * n + (size_t)pl[1] * row0 * w;
+        const size_t words = (size_t)pl[1] * rows * w;
+        if (words) {
+            if (into_image)
+                PHX_CUDA(cudaMemcpyAsync(img, packed + at, words * 4, cudaMemcpyDeviceToDevice, tr->ctx->stream));
+            else
+                PHX_CUDA(cudaMemcpyAsync(packed + at, img, words * 4, cudaMemcpyDeviceToDevice, tr->ctx->stream));
+        }
+        at += words;
+    }
     return PHX_OK;
 }
 
@@ -2153,6 +2673,11 @@ int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebu
     cudaStream_t s = tr->ctx->stream;
     if ((const void*)verts != tr->verts.ptr)
         PHX_CUDA(cudaMemcpyAsync(tr->verts.ptr, verts, (size_t)tr->nverts * 16, cudaMemcpyDeviceToDevice, s));
+    if (tr->forest) {  // Tracer::repose: each mesh's tree refitted (or rebuilt), the top tree again
+        PHX_TRY(build_forest(tr, rebuild != 0));
+        tr->have_last = false;
+        return PHX_OK;
+    }
     PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
                               (phx_aabb*)tr->bvh.prims.ptr));
     if (rebuild) PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf));
@@ -2570,6 +3095,10 @@ int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint3
 int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
     if (!b) return fail(PHX_ERR_INVALID, "null batch");
     if (b->jobs.empty()) return fail(PHX_ERR_INVALID, "empty batch");
+    for (const BatchJob& bj : b->jobs)
+        if (bj.tr->forest)
+            return fail(PHX_ERR_INVALID, "the serving graph rebuilds single-instance scenes; trace a scene of "
+                                         "instances with phx_batch_trace");
     PHX_TRY(use(b->ctx));
     Ctx* c = b->ctx;
     PHX_TRY(wait_stream(c->stream, BATCH_WAIT_MS));

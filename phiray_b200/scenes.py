@@ -72,6 +72,30 @@ def light_area(pos, direction, right, size, size_y, power, shape=0) -> np.ndarra
     return l
 
 
+# trace::Instance as the C ABI takes it (phx_instance): object -> world in
+# Blender's layout (m[col][row] at world[4 col + row]), the mesh, whether it
+# casts shadows.
+INSTANCE = np.dtype([("world", "<f4", 16), ("mesh", "<u4"), ("casts_shadow", "<u4"), ("pad", "<u4", 6)])
+
+
+def instance(world_rows, mesh: int, casts_shadow: bool = True) -> np.ndarray:
+    """One instance record from a 4 x 4 row-major object -> world matrix."""
+    r = np.zeros(1, INSTANCE)
+    m = np.asarray(world_rows, np.float64).reshape(4, 4)
+    r["world"][0] = m.T.reshape(16).astype(np.float32)  # column-major: m[col][row]
+    r["mesh"] = mesh
+    r["casts_shadow"] = 1 if casts_shadow else 0
+    return r
+
+
+def placement(t=(0.0, 0.0, 0.0), rot_axis=(0.0, 1.0, 0.0), rot_deg=0.0, scale=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """A 4 x 4 row-major matrix: scale, then turn, then move."""
+    m = np.eye(4)
+    m[:3, :3] = _rot(np.asarray(rot_axis, np.float64), math.radians(rot_deg)) @ np.diag(scale)
+    m[:3, 3] = t
+    return m
+
+
 def light_sun(direction, power, angle=0.0) -> np.ndarray:
     """camera.wgsl Light, kind 0 (sun): colour x power arriving along
     `direction`, spread over a cone of `angle` radians (Light.size)."""
@@ -161,6 +185,8 @@ class Scene:
     meta: dict = field(default_factory=dict)
     normals: np.ndarray | None = None  # (V, 4) float32 vertex normals, or None: flat faces
     sun: tuple = (0.0, 1.0, 0.0)  # Camera.sun: the studio rig's key light direction
+    meshes: np.ndarray | None = None  # (M, 2) uint32 face ranges [lo, hi), or None: one identity instance
+    insts: np.ndarray | None = None  # INSTANCE records placing the meshes
 
     @property
     def ntris(self) -> int:
@@ -704,3 +730,98 @@ def features(kind: str, width: int = 64, height: int = 48, spp: int = 4, bounces
     lights = np.asarray(lights, np.float32).reshape(-1, LIGHT_WORDS)
     return Scene(f"features_{kind}", verts, faces, np.stack(mats).astype(np.float32), lights, view, width, height,
                  spp, bounces, env=env, normals=normals, sun=sun)
+
+
+def instanced(width: int = 64, height: int = 48, spp: int = 4, bounces: int = 4) -> Scene:
+    """Meshes placed by instances (forest.rs, instance.rs): a smooth
+    icosphere mesh shown three times — moved, turned with a non-uniform
+    scale, and mirrored (a scale of -1, world_ng's case) — one copy casting
+    no shadow; a box mesh twice; a glowing panel mesh twice (an emitter
+    entry per instance, lamp.rs table_of); the ground as its own mesh at the
+    identity; an empty mesh with an instance (never placed in the top
+    tree). Two area lamps."""
+    parts, mats, normals = [], [], []
+
+    def material(row):
+        mats.append(row)
+        return len(mats) - 1
+
+    ranges = []
+
+    def mesh(v, f, m, smooth=False):
+        lo = sum(len(p[1]) for p in parts)
+        ff = np.zeros((len(f), 4), np.uint32)
+        ff[:, :3] = f
+        ff[:, 3] = m
+        v = np.asarray(v, np.float32)
+        parts.append((v, ff))
+        normals.append(_smooth_normals(np.c_[v, np.ones(len(v))], ff[:, :3].astype(np.int64)) if smooth
+                       else np.zeros((len(v), 4), np.float32))
+        ranges.append((lo, lo + len(f)))
+        return len(ranges) - 1
+
+    g = _quad((-2.5, 0.0, -2.5), (-2.5, 0.0, 2.5), (2.5, 0.0, 2.5), (2.5, 0.0, -2.5), 0)
+    ground = mesh(g[0], g[1][:, :3], material(lambert((0.55, 0.55, 0.5))))
+    sv, sf = _icosphere(3)
+    sphere = mesh(sv * 0.3, sf, material(mat([0.7, 0.35, 0.2, 1.0], rough=0.3)), smooth=True)
+    bv, bf = _box((0.0, 0.0, 0.0), (0.3, 0.4, 0.3), 2)
+    box = mesh(bv, bf, material(mat([0.3, 0.5, 0.8, 1.0], rough=0.6, metal=0.3)))
+    pv, pf = _quad((-0.2, 0.0, -0.2), (0.2, 0.0, -0.2), (0.2, 0.0, 0.2), (-0.2, 0.0, 0.2), 0)
+    panel = mesh(pv, pf[:, :3], material(mat([0.0, 0.0, 0.0, 1.0], rough=1.0, emit=(9.0, 8.0, 7.0))))
+    empty = len(ranges)
+    at = sum(len(p[1]) for p in parts)
+    ranges.append((at, at))
+    verts, faces = _assemble(parts)
+    insts = [
+        instance(placement(), ground),
+        instance(placement((-0.6, 0.32, 0.2)), sphere),
+        instance(placement((0.1, 0.45, 0.5), (1.0, 1.0, 0.0), 35.0, (1.2, 0.7, 1.0)), sphere, casts_shadow=False),
+        instance(placement((0.75, 0.3, -0.1), scale=(-1.0, 1.0, 1.0)), sphere),
+        instance(placement((-0.2, 0.2, -0.5), (0.0, 1.0, 0.0), 30.0), box),
+        instance(placement((0.6, 0.2, 0.7), (0.0, 1.0, 0.0), -20.0, (1.0, 1.5, 1.0)), box),
+        instance(placement((-0.5, 1.4, 0.0), (1.0, 0.0, 0.0), 180.0), panel),
+        instance(placement((0.7, 1.2, 0.4), (1.0, 0.0, 0.2), 160.0, (1.5, 1.0, 0.8)), panel),
+        instance(placement((5.0, 0.0, 0.0)), empty),
+    ]
+    lights = [light_area((-0.3, 1.9, -0.6), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.5, 0.5, (10.0, 10.0, 10.0)),
+              light_area((0.9, 1.7, 0.3), (0.0, -1.0, 0.0), (1.0, 0.0, 0.0), 0.3, 0.4, (6.0, 6.0, 6.0))]
+    view = View.look((0.0, 1.0, -2.2), (0.0, -0.35, 1.0), (0.0, 1.0, 0.0), 50.0)
+    return Scene("instanced", verts, faces, np.stack(mats).astype(np.float32), np.stack(lights), view, width, height,
+                 spp, bounces, env=(0.03, 0.03, 0.04), normals=np.concatenate(normals),
+                 meshes=np.asarray(ranges, np.uint32).reshape(-1, 2), insts=np.concatenate(insts))
+
+
+def flatten(scene: Scene) -> Scene:
+    """The same world as one identity instance: every instance's faces
+    placed in world space (float64, then float32), normals turned by the
+    inverse-transpose. For sanity checks of the instanced path against the
+    flat one (close, not bit-equal: the rounding and the trees differ)."""
+    vs, fs, ns, base = [], [], [], 0
+    for r in scene.insts:
+        lo, hi = scene.meshes[r["mesh"]]
+        if hi <= lo:
+            continue
+        f = scene.faces[lo:hi]
+        used = np.unique(f[:, :3])
+        remap = np.zeros(len(scene.verts), np.int64)
+        remap[used] = np.arange(len(used)) + base
+        m = r["world"].reshape(4, 4).T.astype(np.float64)  # rows
+        p = scene.verts[used, :3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
+        nrm = scene.normals[used, :3].astype(np.float64) @ np.linalg.inv(m[:3, :3])
+        ln = np.linalg.norm(nrm, axis=1, keepdims=True)
+        nrm = np.where(ln > 1e-12, nrm / np.where(ln > 1e-12, ln, 1.0), 0.0)
+        vv = np.ones((len(used), 4), np.float32)
+        vv[:, :3] = p
+        nn = np.zeros((len(used), 4), np.float32)
+        nn[:, :3] = nrm
+        ff = f.copy()
+        ff[:, :3] = remap[f[:, :3]]
+        if np.linalg.det(m[:3, :3]) < 0:  # keep the outward winding a mirror turns over
+            ff[:, [1, 2]] = ff[:, [2, 1]]
+        vs.append(vv)
+        ns.append(nn)
+        fs.append(ff)
+        base += len(used)
+    return Scene(scene.name + "_flat", np.concatenate(vs), np.concatenate(fs).astype(np.uint32), scene.mats,
+                 scene.lights, scene.view, scene.width, scene.height, scene.spp, scene.bounces, env=scene.env,
+                 normals=np.concatenate(ns))

@@ -149,7 +149,10 @@ def depth_of(px: np.ndarray, w: int, h: int) -> np.ndarray:
 class Tracer:
     """The Rendered-mode path tracer (phiray ``Tracer``)."""
 
-    def __init__(self, gpu: Gpu, verts: np.ndarray, faces: np.ndarray, mats: np.ndarray, normals=None, leaf: int = 4):
+    def __init__(self, gpu: Gpu, verts: np.ndarray, faces: np.ndarray, mats: np.ndarray, normals=None, leaf: int = 4,
+                 meshes=None, insts=None):
+        """Tracer::new. With `meshes` ((M, 2) face ranges) and `insts`
+        (scenes.INSTANCE records): a scene of meshes placed by instances."""
         self.gpu = gpu
         self._host = [
             np.ascontiguousarray(verts, dtype=np.float32),
@@ -163,7 +166,13 @@ class Tracer:
             len(v), len(f), len(m), leaf,
         )
         h = C.c_void_p()
-        N.check(N.lib().phx_tracer_create(gpu.handle, C.byref(sc), C.byref(h)))
+        if meshes is None:
+            N.check(N.lib().phx_tracer_create(gpu.handle, C.byref(sc), C.byref(h)))
+        else:
+            ms = np.ascontiguousarray(meshes, dtype=np.uint32).reshape(-1, 2)
+            ins = np.ascontiguousarray(insts)
+            N.check(N.lib().phx_tracer_create_instanced(gpu.handle, C.byref(sc), ms.ctypes.data, len(ms),
+                                                        ins.ctypes.data, len(ins), C.byref(h)))
         self.handle = h
         self.w = self.h = 0
         gpu.adopt(self)
@@ -171,7 +180,16 @@ class Tracer:
     @classmethod
     def of(cls, gpu: Gpu, scene, **kw) -> "Tracer":
         kw.setdefault("normals", getattr(scene, "normals", None))
+        if getattr(scene, "meshes", None) is not None:
+            kw.setdefault("meshes", scene.meshes)
+            kw.setdefault("insts", scene.insts)
         return cls(gpu, scene.verts, scene.faces, scene.mats, **kw)
+
+    def reinstance(self, insts) -> None:
+        """``Tracer::reinstance``: the same instances placed anew (the top
+        tree is rebuilt on the device)."""
+        ins = np.ascontiguousarray(insts)
+        N.check(N.lib().phx_tracer_reinstance(self.handle, ins.ctypes.data, len(ins)))
 
     MEGAKERNEL = 0
     STATE_MACHINE = 1

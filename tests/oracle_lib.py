@@ -45,6 +45,10 @@ SIGS = {
     "orc_show": (None, [vp, vp]),
     "orc_trace_rays": (None, [vp, vp, u32, vp, u32, vp, u32, vp, C.c_int]),
     "orc_tri_hit": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "orc_scene_new_instanced": (vp, [vp, vp, u32, vp, vp, u32, vp, u32, vp, u32]),
+    "orc_scene_reinstance": (None, [vp, vp, u32]),
+    "orc_scene_primary": (None, [vp, vp, u32, vp, vp, vp]),
+    "orc_scene_trace_rays": (None, [vp, vp, u32, vp, C.c_int]),
     "orc_math": (None, [C.c_int, vp, vp, vp, u32]),
 }
 
@@ -197,9 +201,22 @@ class TraceOracle:
         nrm = getattr(scene, "normals", None)
         self.nrm = None if nrm is None else np.ascontiguousarray(nrm, dtype=np.float32)
         self.leaf = leaf
-        new = self.lib.orc_scene_new_sah if sah else self.lib.orc_scene_new
-        self.handle = new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data,
-                          None if self.nrm is None else self.nrm.ctypes.data, leaf)
+        meshes = getattr(scene, "meshes", None)
+        nptr = None if self.nrm is None else self.nrm.ctypes.data
+        if meshes is not None:
+            self.meshes = np.ascontiguousarray(meshes, dtype=np.uint32)
+            self.insts = np.ascontiguousarray(scene.insts)
+            self.handle = self.lib.orc_scene_new_instanced(
+                self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, nptr, leaf,
+                self.meshes.ctypes.data, len(self.meshes), self.insts.ctypes.data, len(self.insts))
+        else:
+            new = self.lib.orc_scene_new_sah if sah else self.lib.orc_scene_new
+            self.handle = new(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, nptr, leaf)
+
+    def reinstance(self, insts):
+        """Tracer::reinstance: new matrices for the same instances."""
+        self.insts = np.ascontiguousarray(insts)
+        self.lib.orc_scene_reinstance(self.handle, self.insts.ctypes.data, len(self.insts))
 
     def __del__(self):
         try:
@@ -227,20 +244,21 @@ class TraceOracle:
                                       walk.ctypes.data)
         return px, rays.value, int(walk[0]), int(walk[1])
 
-    def primary(self, cam, frame: int):
+    def primary(self, cam, frame: int, with_inst: bool = False):
+        """Primary hit (face id, t) per pixel; with_inst: also the instance."""
         n = int(cam["w"][0]) * int(cam["h"][0])
         ids = np.zeros(n, np.uint32)
         ts = np.zeros(n, np.float32)
-        self.lib.orc_primary(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, self.leaf,
-                             cam.ctypes.data, frame, ids.ctypes.data, ts.ctypes.data)
-        return ids, ts
+        inst = np.zeros(n, np.uint32)
+        self.lib.orc_scene_primary(self.handle, cam.ctypes.data, frame, ids.ctypes.data, ts.ctypes.data,
+                                   inst.ctypes.data)
+        return (ids, ts, inst) if with_inst else (ids, ts)
 
     def trace_rays(self, rays, any_hit=False):
         rays = np.ascontiguousarray(rays, dtype=np.float32)
         n = len(rays)
         hits = np.zeros((n, 4), np.float32)
-        self.lib.orc_trace_rays(self.v.ctypes.data, self.f.ctypes.data, len(self.f), self.m.ctypes.data, self.leaf,
-                                rays.ctypes.data, n, hits.ctypes.data, 1 if any_hit else 0)
+        self.lib.orc_scene_trace_rays(self.handle, rays.ctypes.data, n, hits.ctypes.data, 1 if any_hit else 0)
         return hits
 
 

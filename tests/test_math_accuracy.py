@@ -115,4 +115,5 @@ def test_device_math_equals_host_and_stays_near_cuda(orc, fn):
     ours_err = _error(fn, got, exact)
     # both near the exact value; so near each other
     assert np.all(ours_err <= _bound(fn, x, yy))
-    assert np.all(cuda_err <= CUDA_ULP[fn] + (1.0 if fn in ("sin", "cos") else 0.0)), float(cuda_err.max())
+    # (half an ulp of slack: the exact value is rounded to float32 to take its ulp)
+    assert np.all(cuda_err <= CUDA_ULP[fn] + (1.0 if fn in ("sin", "cos") else 0.5)), float(cuda_err.max())
