@@ -131,6 +131,31 @@ def whole_job_rate(units_per_rank: float, world: int, ms_max: float) -> float:
     return units_per_rank * world / (ms_max * 1e-3)
 
 
+# The c2 frame's shape, printed identically by both arms.
+C2_CONFIG = {"workload": WORKLOAD, "frame": "1920x1080", "spp": 64, "bounces": 8, "tris": 1310722}
+SAMPLE_ROWS = 48  # rows of the CPU legs' stratified sample
+
+
+def sample_rows(h: int, k: int = SAMPLE_ROWS, seed: int = 0x2545F491) -> list[int]:
+    """One row from each of k equal strata of an h-row frame, at a seeded
+    offset inside its stratum: the CPU legs' bounded, frame-wide sample
+    (both arms trace the same rows)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    edges = np.linspace(0, h, k + 1)
+    return [int(min(h - 1, np.floor(edges[i] + rng.random() * (edges[i + 1] - edges[i])))) for i in range(k)]
+
+
+def trace_sample(T, cam, px, rows) -> tuple[int, float]:
+    """The oracle over the sample rows at 1 spp: (rays, seconds)."""
+    rays_total, t_total = 0, 0.0
+    for r in rows:
+        t0 = time.perf_counter()
+        _, rays = T.trace(cam, 0, 1, px, rows=(r, 1))
+        t_total += time.perf_counter() - t0
+        rays_total += rays
+    return rays_total, t_total
+
+
 def reference_arm(args) -> None:
     """The reference's algorithm on the host cores (the oracle restatement)."""
     world, rank, _ = dist_env()
@@ -148,22 +173,20 @@ def reference_arm(args) -> None:
     # the binned SAH tree phiray's tracer walks (sah.rs), built once outside the timing
     T = oracle_lib.TraceOracle(orc, s, sah=True)
     px = np.zeros(34 * s.width * s.height + 1, np.uint32)
-    rows = 64  # a bounded sample: 64 rows of the frame, one sample each
+    rows = sample_rows(s.height)  # a bounded sample: one seeded row from each of 48 strata, one sample each
     vals = []
     for k in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        _, rays = T.trace(cam, 0, 1, px, rows=(300 + 64 * (k % 8), rows))
-        dt = time.perf_counter() - t0
+        rays, dt = trace_sample(T, cam, px, rows)
         if k >= args.warmup:
             vals.append(rays / dt / 1e6)
     v = statistics.median(vals)
     line = {
         "metric": METRIC, "value": round(v, 3), "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": dict(C2_CONFIG),
         "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{rows} rows of the 1080p frame at 1 spp per step over the SAH tree "
-                                   "(oracle/ C++ restatement, OpenMP)"},
+                         "sample": f"{len(rows)} rows of the 1080p frame (one seeded row a stratum) at 1 spp per "
+                                   "step over the SAH tree (oracle/ C++ restatement, OpenMP)"},
         "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -176,16 +199,17 @@ def cpu_baseline(scene, cam) -> dict:
     orc = oracle_lib.load()
     T = oracle_lib.TraceOracle(orc, scene, sah=True)  # phiray's tracer walks the SAH tree (sah.rs)
     px = np.zeros(34 * scene.width * scene.height + 1, np.uint32)
-    rays_total, t_total, row = 0, 0.0, 300
-    while t_total < 10.0 and row < scene.height:
-        t0 = time.perf_counter()
-        _, rays = T.trace(cam, 0, 1, px, rows=(row, 16))
-        t_total += time.perf_counter() - t0
+    rows = sample_rows(scene.height)  # the reference arm's sample
+    rays_total, t_total, passes = 0, 0.0, 0
+    while t_total < 10.0 and passes < 20:
+        rays, dt = trace_sample(T, cam, px, rows)
         rays_total += rays
-        row += 16
+        t_total += dt
+        passes += 1
     return {"value": round(rays_total / t_total / 1e6, 3), "unit": UNIT, "cores": orc.lib.orc_threads(), "kind": "port",
-            "sample": f"{row - 300} rows of the 1080p frame at 1 spp over the SAH tree ({rays_total} rays, "
-                      f"{t_total:.1f} s), oracle/ C++ OpenMP"}
+            "sample": f"{passes} x {len(rows)} rows of the 1080p frame (one seeded row a stratum, the reference "
+                      f"arm's sample) at 1 spp over the SAH tree ({rays_total} rays, {t_total:.1f} s), "
+                      "oracle/ C++ OpenMP"}
 
 
 def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
@@ -754,9 +778,10 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frame": f"{W}x{H}", "spp": args.spp, "bounces": s.bounces,
-                       "tris": nf, "parallelism": f"replicas x{world}",
-                       "l2": "scene ~300 MB of nodes/triangles/materials > 126 MB L2; the rebuild rewrites them each step"},
+            "config": dict(C2_CONFIG) if (W, H, args.spp, s.bounces, nf) == (1920, 1080, 64, 8, 1310722) else
+            {"workload": WORKLOAD, "frame": f"{W}x{H}", "spp": args.spp, "bounces": s.bounces, "tris": nf},
+            "parallelism": f"replicas x{world}",
+            "l2": "scene ~300 MB of nodes/triangles/materials > 126 MB L2; the rebuild rewrites them each step",
             "render_kernel": {"chosen": KERNEL_NAMES[chosen],
                               "ms_4spp": {KERNEL_NAMES[k]: round(v, 3) for k, v in enumerate(tune_ms)}},
             "frames_per_s": round(1000.0 / ms_step * world, 3),

@@ -490,6 +490,26 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
  * still written at its ray's index. */
 #define PHX_WALK_SORTED 2u
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
+/* Which tree the tracer walks. PHX_TREE_LBVH (the default): the device LBVH
+ * (Morton codes, stable radix sort, Karras, leaf packing; 0.6 ms at 1.3 M
+ * faces). PHX_TREE_SAH: the binned SAH tree phiray's own tracer builds
+ * (src/bvh/sah.rs:85-189, forest.rs:49), node for node, built on the device
+ * by phx_bvh_build_sah — fewer node steps and triangle tests a ray, a far
+ * longer build. Closest hits do not depend on the tree (a tie between two
+ * faces at the same t aside). Rebuilds the tree now over the current
+ * vertices (waits); the image starts over; a repose then refits or rebuilds
+ * the same kind. Single-instance scenes (scenes of instances keep LBVH mesh
+ * trees: PHX_ERR_INVALID). */
+#define PHX_TREE_LBVH 0u
+#define PHX_TREE_SAH 1u
+int32_t phx_tracer_set_tree(phx_tracer tr, uint32_t tree);
+/* The autotuner over trees: builds each (timed), traces `spp` samples of
+ * `cam` on it (timed, after a warm-up trace) and keeps the one with the lower
+ * build + frames x trace time — the SAH tree where the trace time of the
+ * frames to come outweighs its build. ms (4 floats, may be NULL): LBVH build,
+ * LBVH trace, SAH build, SAH trace. Waits; the image is overwritten. */
+int32_t phx_tracer_autotune_tree(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                                 uint32_t frames, uint32_t* chosen, float* ms);
 /* Tracer::set_samples: the sample target `sample` stops at (32 until set,
  * Tracer::SAMPLE_COUNT, src/trace/mod.rs:129). */
 int32_t phx_tracer_set_samples(phx_tracer tr, uint32_t samples);
@@ -763,8 +783,8 @@ int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint3
  * preparation; the batch trace; per job the learned denoiser with the
  * a-trous fallback (net non-NULL; one copy of the network per image shape)
  * or the a-trous Denoise, then a completion time stamp. Runs one frame
- * outside the capture first (sizing every buffer). Tracers of instances are
- * refused (PHX_ERR_INVALID): phx_batch_trace takes them. */
+ * outside the capture first (sizing every buffer). Tracers of instances or
+ * on an SAH tree are refused (PHX_ERR_INVALID): phx_batch_trace takes them. */
 int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold);
 /* Replays the captured frame; modes (HOST, one per job): 1 rebuild, 0 refit. */
 int32_t phx_batch_replay(phx_batch b, const uint32_t* modes);

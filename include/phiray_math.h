@@ -23,7 +23,7 @@
  * Accuracy against float64, measured over 400,000 arguments a function
  * (tests/test_math_accuracy.py holds these bounds): exp2 <= 1.5 ulp on
  * [-126, 127]; log2 <= 3.5 ulp on [1e-30, 1e30]; sin and cos <= 1.5 x 2^-24
- * absolute on [-100, 100]; pow(x, y) <= 5 + 1.5 |y log2 x| ulp and exp(x)
+ * absolute on [-100, 100]; pow(x, y) <= 8 + 1.5 |y log2 x| ulp and exp(x)
  * <= 3 + 1.5 |x log2 e| ulp (the product's rounding is carried into the
  * exponent: ~10 ulp for the sRGB curve's pow(x, 1/2.4), more for large
  * results). More than a path tracer needs; the point is sameness, not the

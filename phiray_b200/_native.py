@@ -64,6 +64,8 @@ SIGNATURES: dict[str, tuple] = {
     "phx_tracer_create_instanced": (i32, [vp, vp, vp, u32, vp, u32, vp]),
     "phx_tracer_reinstance": (i32, [vp, vp, u32]),
     "phx_tracer_trace_rows": (i32, [vp, vp, u32, u32, u32, u32, u32, u32]),
+    "phx_tracer_set_tree": (i32, [vp, u32]),
+    "phx_tracer_autotune_tree": (i32, [vp, vp, u32, u32, u32, u32, vp, vp]),
     "phx_tracer_copy_rows": (i32, [vp, u32, u32, vp, i32]),
     "phx_selftest_wait": (i32, [vp, i32, u32, i32]),
     "phx_ctx_stream": (vp, [vp]),

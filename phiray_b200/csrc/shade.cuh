@@ -96,6 +96,14 @@ struct Count {
     uint32_t rays, steps, tests;
 };
 
+// Render modes, a kernel's compile-time int template argument: bit 0 counts
+// node steps and triangle tests (STATS builds), bit 1 takes scenes of
+// instances. Kernels without bit 1 walk single-instance scenes only: their
+// code holds no two-level walk and no placed geometry.
+constexpr int MODE_STATS = 1;
+constexpr int MODE_INST = 2;
+constexpr int MODE_ANY = MODE_INST;  // code that takes either kind of scene
+
 struct Frame {
     uint32_t w, h, n, frame0, spp, persp, count, bounces;
     f3 right, up, back, pivot, env;
@@ -390,24 +398,43 @@ __device__ __forceinline__ Hit walk_forest(const Scene& S, f3 o, f3 d, float tma
     return best;
 }
 
+// The two-level walk behind a call of its own, so a single-instance scene's
+// trace keeps a frame of one stack.
+template <bool STATS>
+__device__ __noinline__ Hit trace_forest(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    if (S.smem_stack) {
+        extern __shared__ uint32_t walk_stacks[];
+        return walk_forest<STATS, true>(S, o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
+    }
+    return walk_forest<STATS>(S, o, d, tmax, first, cnt);
+}
+
 // A ray's walk of either kind of scene.
 template <bool STATS, bool SMEM = false>
 __device__ __forceinline__ Hit walk_scene(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt,
                                           uint32_t* smem_stack = nullptr, int stride = 0) {
-    if (S.insts) return walk_forest<STATS, SMEM>(S, o, d, tmax, first, cnt, smem_stack, stride);
+    if (S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
     return walk<STATS, SMEM>(tree_of(S), o, d, tmax, first, cnt, smem_stack, stride);
 }
 
+// A ray's walk in a render mode: the two-level walk only where the mode
+// takes instances and the scene has them.
+template <int M>
+__device__ __forceinline__ Hit walk_mode(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    constexpr bool STATS = (M & MODE_STATS) != 0;
+    if ((M & MODE_INST) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
+    return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
+}
+
 // The walk behind a call, for code with several trace sites.
-template <bool STATS>
+template <int M>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
+    constexpr bool STATS = (M & MODE_STATS) != 0;
+    if ((M & MODE_INST) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
     if (S.smem_stack) {
         extern __shared__ uint32_t walk_stacks[];
-        if (S.insts)
-            return walk_forest<STATS, true>(S, o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
         return walk<STATS, true>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
     }
-    if (S.insts) return walk_forest<STATS>(S, o, d, tmax, first, cnt);
     return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 
@@ -461,8 +488,10 @@ __device__ __forceinline__ f3 place_n(float4 i0, float4 i1, float4 i2, f3 n) {
 }
 
 // tri_of (layout.wgsl:114-159): the face in `slot`, placed in the world by
-// instance `inst` (vertices are kept in the mesh's space, w = 1).
-__device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot, uint32_t inst = 0u) {
+// instance `inst` (vertices are kept in the mesh's space, w = 1) in a mode
+// that takes instances.
+template <int M>
+__device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot, uint32_t inst) {
     const float4 A = __ldg(S.tris + 3 * (size_t)slot), B = __ldg(S.tris + 3 * (size_t)slot + 1),
                  Cc = __ldg(S.tris + 3 * (size_t)slot + 2);
     Geo g;
@@ -479,7 +508,7 @@ __device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot, uint32_t in
         g.na = g.nb = g.nc = mk(0.0f);
     }
     g.mirror = false;
-    if (S.insts) {
+    if ((M & MODE_INST) && S.insts) {
         const float4* q = S.insts + 8 * (size_t)inst;
         const uint32_t flags = __float_as_uint(__ldg(q + 7).w);
         g.mirror = (flags & 4u) != 0u;
@@ -796,22 +825,25 @@ __device__ __forceinline__ Shadowed lamp_query(const Frame& F, const Surf& s, ui
 
 // lamp_chance (light.wgsl:259-271): the table share of the hit's (face,
 // instance) pair, the entries sorted by face, then instance.
+template <int M>
 __device__ __forceinline__ float lamp_chance(const Scene& S, uint32_t slot, uint32_t inst) {
     const uint32_t count = S.lamp_count;
     if (count == 0u) return 0.0f;
+    const bool placed = (M & MODE_INST) && S.lamp_inst;
     uint32_t lo = 0, hi = count - 1u;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2u;
         const uint32_t f = __ldg(S.lamp_slot + mid);
-        const uint32_t i = S.lamp_inst ? __ldg(S.lamp_inst + mid) : 0u;
+        const uint32_t i = placed ? __ldg(S.lamp_inst + mid) : 0u;
         if (f < slot || (f == slot && i < inst)) lo = mid + 1u;
         else hi = mid;
     }
-    if (__ldg(S.lamp_slot + lo) != slot || (S.lamp_inst ? __ldg(S.lamp_inst + lo) : 0u) != inst) return 0.0f;
+    if (__ldg(S.lamp_slot + lo) != slot || (placed ? __ldg(S.lamp_inst + lo) : 0u) != inst) return 0.0f;
     const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
     return __ldg(S.lamp_cdf + lo) - prev;
 }
 
+template <int M>
 __device__ __forceinline__ Shadowed glow_query(const Scene& S, const Surf& s, uint32_t& seed) {
     const uint32_t count = S.lamp_count;
     if (count == 0u) return unshadowed();
@@ -825,7 +857,7 @@ __device__ __forceinline__ Shadowed glow_query(const Scene& S, const Surf& s, ui
     const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
     const float chance = fmaxf(__ldg(S.lamp_cdf + lo) - prev, 1e-8f);
     const uint32_t f = __ldg(S.lamp_slot + lo);
-    const Geo g = geo_at(S, f, S.lamp_inst ? __ldg(S.lamp_inst + lo) : 0u);
+    const Geo g = geo_at<M>(S, f, ((M & MODE_INST) && S.lamp_inst) ? __ldg(S.lamp_inst + lo) : 0u);
     const Mat t = mat_at(S, g.mat);
     float a = rnd(seed);
     float b = rnd(seed);

@@ -65,6 +65,18 @@ __global__ void k_mark_ends(const float4* __restrict__ nodes, const uint32_t* __
     c->w = __uint_as_float(__float_as_uint(c->w) | FLAG_END);
 }
 
+// Marks the last slot of every leaf of a tree whose nodes are all reachable
+// (the binned SAH tree's compact array).
+__global__ void k_mark_leaf_ends(const float4* __restrict__ nodes, uint32_t m, float4* tris) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
+    if (!(__float_as_uint(a.w) & LEAF)) return;
+    const uint32_t end = __float_as_uint(b.w);
+    float4* c = tris + 3 * (size_t)(end - 1) + 2;
+    c->w = __uint_as_float(__float_as_uint(c->w) | FLAG_END);
+}
+
 // A child's ref in the walk's records: an inner node's record index (its
 // Karras index + inner_base), or for a leaf its first slot + leaf_base with
 // LEAF and leaf_bits (INST for a top-tree leaf).
@@ -348,7 +360,7 @@ __device__ __forceinline__ float srgb_to_linear1(float c) {
 __device__ __forceinline__ f3 env_at(const Frame& F) { return F.env; }
 
 // direct (integrate.wgsl:66-85): every light with its shadow ray.
-template <bool STATS>
+template <int STATS>
 __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s, uint32_t& seed, bool with_env,
                                   f3 sun, Count& cnt) {
     const bool rig = uses_rig(F);
@@ -360,7 +372,7 @@ __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s,
         } else if (k == 1u) {
             if (rig) q = rig_query(F, 1u, s, seed, sun);
         } else if (k == 2u) {
-            q = glow_query(S, s, seed);
+            q = glow_query<STATS>(S, s, seed);
         }
         // k == 3: env_query needs an environment image's table (env_cdf),
         // which the host refuses; it returns unshadowed without a draw.
@@ -373,8 +385,9 @@ __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s,
 }
 
 // glow_mis (integrate.wgsl:15-23).
+template <int M>
 __device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, const Hit& h, f3 from_n, f3 dir) {
-    const float chance = lamp_chance(S, h.tri, h.inst);
+    const float chance = lamp_chance<M>(S, h.tri, h.inst);
     if (chance <= 0.0f) return emit;
     const f3 cr = cross(g.b - g.a, g.c - g.a);
     const float pl = chance * h.t * h.t / fmaxf(0.5f * length(cr) * fabsf(dot(normalize(cr), dir)), 1e-8f);
@@ -383,7 +396,7 @@ __device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, co
 }
 
 // indirect (integrate.wgsl:111-230) with no environment image.
-template <bool STATS>
+template <int STATS>
 __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f3 n, uint32_t& seed, bool bounce,
                                        f3 sun, Count& cnt) {
     const bool lit = dot(F.env, F.env) > 0.0f;
@@ -415,7 +428,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
             break;
         }
         if (!bounce) break;
-        const Geo g = geo_at(S, h.tri, h.inst);
+        const Geo g = geo_at<STATS>(S, h.tri, h.inst);
         const Mat t = mat_at(S, g.mat);
         const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
         const f3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
@@ -427,7 +440,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
         const float tw = t.trans * (1.0f - t.metal);
         f3 albedo = base * (1.0f - t.metal) * (1.0f - tw);
         if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -dir), 1e-4f));
-        acc += thr * glow_mis(S, g, t.emit, h, nrm, dir);
+        acc += thr * glow_mis<STATS>(S, g, t.emit, h, nrm, dir);
         const float near = (!lit && h.t <= F.ao) ? 0.25f : 1.0f;
         const Surf s = plain_surf(hit, ng, -dir, albedo, vmix(fd, base, metal), rough);
         acc += thr * direct<STATS>(S, F, s, seed, true, sun, cnt) * near;
@@ -451,10 +464,10 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
 }
 
 // bounce_light (integrate.wgsl:236-250).
-template <bool STATS>
+template <int STATS>
 __device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const Hit& h, f3 org, f3 d,
                                            uint32_t& seed, f3 sun, Count& cnt) {
-    const Geo g = geo_at(S, h.tri, h.inst);
+    const Geo g = geo_at<STATS>(S, h.tri, h.inst);
     const Mat t = mat_at(S, g.mat);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
     const f3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
@@ -499,7 +512,7 @@ __device__ __forceinline__ CamRay camera_ray(const Frame& F, uint32_t i, uint32_
 }
 
 // One sample of pixel i (shade.wgsl:41-373) added into `acc`.
-template <bool STATS>
+template <int STATS>
 __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t frame, f3 sun, Sums& acc,
                        Count& cnt) {
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
@@ -549,7 +562,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                 acc.cov += gr.a;
             }
         }
-        const Geo g = geo_at(S, h.tri, h.inst);
+        const Geo g = geo_at<STATS>(S, h.tri, h.inst);
         const Mat t = mat_at(S, g.mat);
         const float w = 1.0f - h.u - h.v;
         const f3 hit = o + d * h.t;
@@ -679,7 +692,7 @@ __device__ __forceinline__ void setup(Scene& S, Frame& F) {
 // SYNC: the lanes that entered wait for each other after every sample, so
 // each sample's camera ray and first bounces start together (the same sums
 // either way: a lane's own samples keep their order).
-template <bool STATS, bool SYNC = false>
+template <int STATS, bool SYNC = false>
 __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun, uint32_t* __restrict__ px,
                                           uint32_t i, Count& cnt) {
     const unsigned lanes = __activemask();
@@ -731,11 +744,11 @@ __device__ __forceinline__ void render_px(const Scene& S, const Frame& F, f3 sun
 }
 
 // Adds a warp's ray count (and STATS: steps, tests) to counters[0..2].
-template <bool STATS>
+template <int STATS>
 __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long long* counters) {
     const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counters, (unsigned long long)tot);
-    if (STATS) {
+    if (STATS & 1) {
         const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
         const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
         if ((threadIdx.x & 31) == 0) {
@@ -749,7 +762,7 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
 // (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills;
 // 5: 96, 6: 80, 8: 64, 10: 48, 12: 40, 16: 32 — more warps to hide the
 // walk's loads, more spills).
-template <bool STATS, int MINB = 4, bool SYNC = false>
+template <int STATS, int MINB = 4, bool SYNC = false>
 __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px,
                                                   uint32_t first, uint32_t count, unsigned long long* counters) {
     setup(S, F);
@@ -863,7 +876,7 @@ struct Job {
 // Registers are budgeted for 1536 resident threads an SM (40 a thread): the
 // walk is latency-bound, and the single-scene megakernel runs fastest with
 // that many warps resident although it spills more.
-template <bool STATS, int THREADS>
+template <int STATS, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
                                                                          uint32_t ntiles, uint32_t* next) {
     constexpr int WARPS = THREADS / 32;
@@ -991,6 +1004,7 @@ __device__ __forceinline__ uint32_t set_ray(Path& P, f3 o, f3 d, float tmax, boo
 }
 
 // direct() up to its shadow rays: every query (and its draws) in order.
+template <int STATS>
 __device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F, Path& P, const Surf& s, uint32_t cont,
                                                  f3 sun) {
     const bool rig = uses_rig(F);
@@ -1003,7 +1017,7 @@ __device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F,
         } else if (k == 1u) {
             if (rig) q = rig_query(F, 1u, s, P.seed, sun);
         } else if (k == 2u) {
-            q = glow_query(S, s, P.seed);
+            q = glow_query<STATS>(S, s, P.seed);
         }
         if (maxc(q.c) > 0.0f) {
             P.put(P.qn, q.c, q.dir, q.dist);
@@ -1016,7 +1030,7 @@ __device__ __forceinline__ uint32_t start_direct(const Scene& S, const Frame& F,
     return PH_DIRECT_NEXT;
 }
 
-template <bool STATS>
+template <int STATS>
 __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P, uint32_t ph, const Hit& h, f3 sun,
                                          Sums& acc) {
     const uint32_t see_through = 8u, through = 8u;
@@ -1066,7 +1080,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                     acc.cov += gr.a;
                 }
             }
-            const Geo g = geo_at(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const float w = 1.0f - h.u - h.v;
             const f3 hit = P.o + P.d * h.t;
@@ -1113,14 +1127,14 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
             P.ior = t.ior;
             P.opaque = 1.0f - t.trans * (1.0f - t.metal);
             P.c = mk(0.0f);
-            if (P.opaque > 0.0f) return start_direct(S, F, P, P.s, C_OPAQUE, sun);
+            if (P.opaque > 0.0f) return start_direct<STATS>(S, F, P, P.s, C_OPAQUE, sun);
             return PH_SHINE_OR_LOBE;
         }
         case PH_SHINE_OR_LOBE: {
             if (P.opaque < 1.0f) {
                 const Surf shine{P.s.pos, P.s.n, P.s.v, mk(0.0f), P.s.f0, P.s.rough, 0.0f, mk(1.0f), 0.0f,
                                  P.s.sheen_rough, P.s.sheen_tint, P.s.coat, P.s.coat_rough, P.s.eta, P.s.dielectric};
-                return start_direct(S, F, P, shine, C_SHINE, sun);
+                return start_direct<STATS>(S, F, P, shine, C_SHINE, sun);
             }
             return PH_LOBE;
         }
@@ -1186,7 +1200,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 P.aval = P.iacc;
                 return PH_AFTER_INDIRECT;
             }
-            const Geo g = geo_at(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const f3 dir = P.idir;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -1198,7 +1212,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
             const float tw = t.trans * (1.0f - t.metal);
             f3 albedo = base * (1.0f - t.metal) * (1.0f - tw);
             if (maxc(albedo) > 0.0f) albedo *= under_layer(fd, rough, fmaxf(dot(ng, -dir), 1e-4f));
-            P.iacc += P.ithr * glow_mis(S, g, t.emit, h, P.inrm, dir);
+            P.iacc += P.ithr * glow_mis<STATS>(S, g, t.emit, h, P.inrm, dir);
             const bool lit = dot(F.env, F.env) > 0.0f;
             P.inear = (!lit && h.t <= F.ao) ? 0.25f : 1.0f;
             P.itw = tw;
@@ -1208,7 +1222,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
             P.ing = ng;
             P.iht = h.t;
             const Surf si = plain_surf(hit, ng, -dir, albedo, vmix(fd, base, t.metal), rough);
-            return start_direct(S, F, P, si, C_IND, sun);
+            return start_direct<STATS>(S, F, P, si, C_IND, sun);
         }
         case PH_IND_AFTER_DIRECT: {
             if (P.itw > 0.0f && rnd(P.seed) < P.itw) {
@@ -1267,7 +1281,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 return PH_AFTER_GLOSSY;
             }
             // bounce_light (integrate.wgsl:236-250) up to its direct().
-            const Geo g = geo_at(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
             const Mat t = mat_at(S, g.mat);
             const f3 d = P.rd;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -1281,7 +1295,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
             const Surf s2 = plain_surf(pos, ng, -d, albedo, vmix(fd, base, t.metal), rough);
             P.balbedo = s2.albedo;
             P.bemit = t.emit;
-            return start_direct(S, F, P, s2, C_BOUNCE_LIGHT, sun);
+            return start_direct<STATS>(S, F, P, s2, C_BOUNCE_LIGHT, sun);
         }
         case PH_AFTER_GLOSSY: {
             const Surf& s = P.s;
@@ -1395,7 +1409,7 @@ __device__ __forceinline__ void store_sums(uint32_t* px, uint32_t n, uint32_t i,
 
 // Persistent: every lane takes pixels from `next` until [first, first +
 // count) is done, tracing all of a pixel's samples in frame order.
-template <bool STATS, int MINB>
+template <int STATS, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 sun, uint32_t* __restrict__ px, uint32_t first,
                                                   uint32_t count, uint32_t* next, unsigned long long* counters) {
     setup(S, F);
@@ -1437,13 +1451,13 @@ __global__ void __launch_bounds__(128, MINB) k_render_sm(Scene S, Frame F, f3 su
         }
         if (__all_sync(0xffffffffu, ph == PH_DONE)) break;
         if (ph == PH_TRACE) {
-            h = walk_scene<STATS>(S, P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
+            h = walk_mode<STATS>(S, P.ro, P.rd, P.rtmax, P.rany != 0u, cnt);
             ph = P.after;
         }
     }
     const uint32_t tot = __reduce_add_sync(0xffffffffu, cnt.rays);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(counters, (unsigned long long)tot);
-    if (STATS) {
+    if (STATS & 1) {
         const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
         const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
         if ((threadIdx.x & 31) == 0) {
@@ -1480,7 +1494,7 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
         rays[2 * (size_t)i + 1] = make_float4(cr.d.x, cr.d.y, cr.d.z, 0.0f);
         return;
     }
-    const Geo g = geo_at(S, h.tri, h.inst);
+    const Geo g = geo_at<MODE_ANY>(S, h.tri, h.inst);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
     const f3 ng = dot(ng0, cr.d) < 0.0f ? ng0 : -ng0;
     const f3 pos = cr.o + cr.d * h.t + ng * hit_lift(F, h.t);
@@ -1718,6 +1732,11 @@ struct phx_tracer_s {
     Ctx* ctx = nullptr;
     uint32_t nverts = 0, nfaces = 0, nmats = 0, leaf = 4;
     std::unique_ptr<Forest> forest;
+    // The tree the walk reads: the LBVH (tr->bvh's Karras array) or the
+    // binned SAH tree (sah.rs; its compact array in tr->bvh.nodes/order).
+    uint32_t tree = PHX_TREE_LBVH;
+    uint32_t sah_count = 0, sah_depth = 0;  // the SAH tree's nodes and depth
+    DevMem sah_alt;                          // its refit's second node array
     bool has_normals = false;
     bool emissive = false;  // some material emits: the emitter table is built
     DevMem verts, vnorm, faces, mats, tnodes, tris, tnorm, lamp_slot, lamp_power, lamp_cdf, info, px, rays, cam;
@@ -1917,6 +1936,62 @@ int32_t build_forest(phx_tracer tr, bool rebuild) {
     return prepare_forest(tr);
 }
 
+// The binned SAH tree (sah.rs:85-189, the tree phiray's tracer walks) over
+// the face boxes in tr->bvh.prims, into tr->bvh's node and order arrays,
+// then the walk's records: every node of the compact array is reachable, so
+// records are indexed by node (leaves skipped) and every leaf marks its end.
+int32_t build_sah_tree(phx_tracer tr) {
+    Ctx* c = tr->ctx;
+    const uint32_t n = tr->nfaces;
+    BvhWork& w = tr->bvh;
+    PHX_TRY(phx_bvh_build_sah((phx_ctx)((char*)c - offsetof(phx_ctx_s, c)), (const phx_aabb*)w.prims.ptr, n,
+                              tr->leaf, (phx_node*)w.nodes.ptr, (uint32_t*)w.order.ptr, &tr->sah_count,
+                              &tr->sah_depth));
+    return PHX_OK;
+}
+
+int32_t prepare_sah(phx_tracer tr) {
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    const uint32_t n = tr->nfaces, m = tr->sah_count;
+    const BvhWork& w = tr->bvh;
+    k_gather<<<ceil_div(n, 256), 256, 0, s>>>((const uint32_t*)w.order.ptr, (const uint4*)tr->faces.ptr,
+                                              (const float4*)tr->verts.ptr,
+                                              tr->has_normals ? (const float4*)tr->vnorm.ptr : nullptr,
+                                              (const float4*)tr->mats.ptr, tr->nmats, n, (float4*)tr->tris.ptr,
+                                              tr->has_normals ? (float4*)tr->tnorm.ptr : nullptr, c->status);
+    k_mark_leaf_ends<<<ceil_div(m, 256), 256, 0, s>>>((const float4*)w.nodes.ptr, m, (float4*)tr->tris.ptr);
+    k_convert<<<ceil_div(m, 256), 256, 0, s>>>((const float4*)w.nodes.ptr, m, (float4*)tr->tnodes.ptr, 0u, 0u, 0u);
+    k_root<<<1, 1, 0, s>>>((const float4*)w.nodes.ptr, n, (float4*)tr->info.ptr, 0u);
+    if (tr->emissive)
+        k_lamps<<<1, 1024, 0, s>>>((const float4*)tr->tris.ptr, (const float4*)tr->mats.ptr, n,
+                                   (uint32_t*)tr->lamp_slot.ptr, (float*)tr->lamp_power.ptr, (float*)tr->lamp_cdf.ptr,
+                                   (float4*)tr->info.ptr);
+    else
+        PHX_CUDA(cudaMemsetAsync((float4*)tr->info.ptr + 2, 0, sizeof(float4), s));
+    return cuda_check(cudaGetLastError(), "SAH prepare");
+}
+
+// The SAH tree refitted to the face boxes now in tr->bvh.prims: the
+// reference's GPU refit (kernel.rs:130-170, record_refit, gpu.rs:77-85):
+// depth + 1 Jacobi passes over every node, rounded up to even so the last
+// one lands in the node array.
+int32_t refit_sah_tree(phx_tracer tr) {
+    Ctx* c = tr->ctx;
+    BvhWork& w = tr->bvh;
+    const uint32_t m = tr->sah_count;
+    PHX_TRY(tr->sah_alt.reserve((size_t)m * 32));
+    const uint32_t passes = (tr->sah_depth + 1 + 1) & ~1u;
+    phx_refit_param p{};
+    p.n = m;
+    for (uint32_t k = 0; k < passes; k++) {
+        void* bufs[4] = {w.prims.ptr, w.order.ptr, (k & 1) ? tr->sah_alt.ptr : w.nodes.ptr,
+                         (k & 1) ? w.nodes.ptr : tr->sah_alt.ptr};
+        PHX_TRY(launch_refit_step(c->stream, &p, bufs, m));
+    }
+    return PHX_OK;
+}
+
 // The scene record the kernels take (build-dependent fields are read from
 // the device info record inside the kernel, so no host sync is needed).
 Scene scene_of(phx_tracer tr) {
@@ -2010,91 +2085,88 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
     return PHX_OK;
 }
 
+// The render kernels of one mode M (MODE_STATS, MODE_INST bits) at the
+// tracer's kernel id, over pixels [first_px, first_px + count_px).
+struct RenderLaunch {
+    Scene S;
+    Frame F;
+    f3 sun;
+    uint32_t* px;
+    uint32_t first, count;
+    unsigned long long* counters;
+    uint32_t* next;
+    int sms;
+    cudaStream_t s;
+};
+
+template <int M, int MINB>
+int32_t launch_sm(const RenderLaunch& L) {
+    int per_sm = 0;
+    PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_sm<M, MINB>, 128, 0));
+    const uint32_t grid = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)L.sms;
+    const uint32_t blocks = std::min<uint32_t>(grid, (L.count + 127) / 128);
+    PHX_CUDA(cudaMemsetAsync(L.next, 0, 4, L.s));
+    k_render_sm<M, MINB><<<blocks, 128, 0, L.s>>>(L.S, L.F, L.sun, L.px, L.first, L.count, L.next, L.counters);
+    return cuda_check(cudaGetLastError(), "render");
+}
+
+template <int M, int MINB, bool SYNC>
+int32_t launch_mk(const RenderLaunch& L) {
+    k_render<M, MINB, SYNC><<<(L.count + 127) / 128, 128, 0, L.s>>>(L.S, L.F, L.sun, L.px, L.first, L.count,
+                                                                     L.counters);
+    return cuda_check(cudaGetLastError(), "render");
+}
+
+// Single-instance scenes: every form the autotuner times.
+template <int M>
+int32_t launch_flat(uint32_t kernel, const RenderLaunch& L) {
+    switch (kernel) {
+        case PHX_KERNEL_STATE_MACHINE: return launch_sm<M, 4>(L);
+        case PHX_KERNEL_STATE_MACHINE_6: return launch_sm<M, 6>(L);
+        case PHX_KERNEL_STATE_MACHINE_8: return launch_sm<M, 8>(L);
+        case PHX_KERNEL_MEGAKERNEL_3: return launch_mk<M, 3, false>(L);
+        case PHX_KERNEL_MEGAKERNEL_2: return launch_mk<M, 2, false>(L);
+        case PHX_KERNEL_MEGAKERNEL_SYNC: return launch_mk<M, 4, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_2_SYNC: return launch_mk<M, 2, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_5: return launch_mk<M, 5, false>(L);
+        case PHX_KERNEL_MEGAKERNEL_6: return launch_mk<M, 6, false>(L);
+        case PHX_KERNEL_MEGAKERNEL_6_SYNC: return launch_mk<M, 6, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_8: return launch_mk<M, 8, false>(L);
+        case PHX_KERNEL_MEGAKERNEL_8_SYNC: return launch_mk<M, 8, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_10_SYNC: return launch_mk<M, 10, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_12_SYNC: return launch_mk<M, 12, true>(L);
+        case PHX_KERNEL_MEGAKERNEL_16_SYNC: return launch_mk<M, 16, true>(L);
+        default: return launch_mk<M, 4, false>(L);
+    }
+}
+
+// Scenes of instances: three forms — the state machine, and the
+// megakernel at the 4-block and the 16-block (per-sample wait) budgets —
+// each kernel id taking the one nearest its own (every form computes the
+// same image).
+template <int M>
+int32_t launch_placed(uint32_t kernel, const RenderLaunch& L) {
+    if (kernel >= PHX_KERNEL_STATE_MACHINE && kernel <= PHX_KERNEL_STATE_MACHINE_8) return launch_sm<M, 4>(L);
+    if (kernel >= PHX_KERNEL_MEGAKERNEL_8 && kernel <= PHX_KERNEL_MEGAKERNEL_16_SYNC) return launch_mk<M, 16, true>(L);
+    return launch_mk<M, 4, false>(L);
+}
+
 // Launches the tracer's render kernel over pixels [first_px, first_px +
 // count_px) of frame F, whose camera is already in tr->cam (no host copy:
 // the launch can be recorded into a graph).
 int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, uint32_t count_px, bool stats) {
     Ctx* c = tr->ctx;
-    const Scene S = scene_of(tr);
+    uint32_t kernel = tr->kernel;
     // Adaptive Sampling runs on the megakernel forms (the state machine
     // fetches pixels by index, not from the open list); they all compute
     // the same image, so an adaptive frame takes the default form instead.
-    const uint32_t keep_kernel = tr->kernel;
-    if (F.adapt_on && tr->kernel >= PHX_KERNEL_STATE_MACHINE && tr->kernel <= PHX_KERNEL_STATE_MACHINE_8)
-        tr->kernel = PHX_KERNEL_MEGAKERNEL;
-    struct Restore {
-        phx_tracer t;
-        uint32_t k;
-        ~Restore() { t->kernel = k; }
-    } restore{tr, keep_kernel};
-    if (tr->kernel >= PHX_KERNEL_STATE_MACHINE && tr->kernel <= PHX_KERNEL_STATE_MACHINE_8) {
-        // state machine, at 4, 6 or 8 resident blocks of 128 per SM
-        const int minb = tr->kernel == 1u ? 4 : (tr->kernel == 2u ? 6 : 8);
-        const void* fn = minb == 4 ? (const void*)k_render_sm<false, 4>
-                                   : (minb == 6 ? (const void*)k_render_sm<false, 6> : (const void*)k_render_sm<false, 8>);
-        int per_sm = 0;
-        PHX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0));
-        const uint32_t grid = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)c->sms;
-        const uint32_t blocks = std::min<uint32_t>(grid, (count_px + 127) / 128);
-        PHX_CUDA(cudaMemsetAsync(tr->next.ptr, 0, 4, c->stream));
-        uint32_t* pxp = (uint32_t*)tr->px.ptr;
-        uint32_t* nx = (uint32_t*)tr->next.ptr;
-        unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
-        if (stats) {
-            if (minb == 4) k_render_sm<true, 4><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-            else if (minb == 6) k_render_sm<true, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-            else k_render_sm<true, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-        } else {
-            if (minb == 4) k_render_sm<false, 4><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-            else if (minb == 6) k_render_sm<false, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-            else k_render_sm<false, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, nx, ct);
-        }
-        return cuda_check(cudaGetLastError(), "render");
-    }
-    const uint32_t blocks = (count_px + 127) / 128;
-    uint32_t* pxp = (uint32_t*)tr->px.ptr;
-    unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
-    if (tr->kernel == PHX_KERNEL_MEGAKERNEL_SYNC) {
-        if (stats) k_render<true, 4, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 4, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2_SYNC) {
-        if (stats) k_render<true, 2, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 2, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_3) {
-        if (stats) k_render<true, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 3><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_2) {
-        if (stats) k_render<true, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 2><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_5) {
-        if (stats) k_render<true, 5><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 5><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_6) {
-        if (stats) k_render<true, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 6><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_6_SYNC) {
-        if (stats) k_render<true, 6, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 6, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_8) {
-        if (stats) k_render<true, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 8><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_8_SYNC) {
-        if (stats) k_render<true, 8, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 8, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_10_SYNC) {
-        if (stats) k_render<true, 10, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 10, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_12_SYNC) {
-        if (stats) k_render<true, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 12, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else if (tr->kernel == PHX_KERNEL_MEGAKERNEL_16_SYNC) {
-        if (stats) k_render<true, 16, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false, 16, true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    } else {
-        if (stats) k_render<true><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-        else k_render<false><<<blocks, 128, 0, c->stream>>>(S, F, sun, pxp, first_px, count_px, ct);
-    }
-    return cuda_check(cudaGetLastError(), "render");
+    if (F.adapt_on && kernel >= PHX_KERNEL_STATE_MACHINE && kernel <= PHX_KERNEL_STATE_MACHINE_8)
+        kernel = PHX_KERNEL_MEGAKERNEL;
+    const RenderLaunch L{scene_of(tr), F,       sun,    (uint32_t*)tr->px.ptr, first_px, count_px,
+                         (unsigned long long*)tr->rays.ptr, (uint32_t*)tr->next.ptr, c->sms, c->stream};
+    if (tr->forest)
+        return stats ? launch_placed<MODE_INST | MODE_STATS>(kernel, L) : launch_placed<MODE_INST>(kernel, L);
+    return stats ? launch_flat<MODE_STATS>(kernel, L) : launch_flat<0>(kernel, L);
 }
 
 // The frame record of `cam` for tr, whose lights the kernels read from tr->cam.
@@ -2347,6 +2419,66 @@ int32_t phx_tracer_create_instanced(phx_ctx ctx, const phx_scene* sc, const phx_
                                     const phx_instance* insts, uint32_t ninsts, phx_tracer* out) {
     if (!meshes) return fail(PHX_ERR_INVALID, "null mesh table");
     return create_tracer(ctx, sc, meshes, nmeshes, insts, ninsts, out);
+}
+
+int32_t phx_tracer_set_tree(phx_tracer tr, uint32_t tree) {
+    if (!tr || (tree != PHX_TREE_LBVH && tree != PHX_TREE_SAH)) return fail(PHX_ERR_INVALID, "bad argument");
+    if (tr->forest && tree != PHX_TREE_LBVH)
+        return fail(PHX_ERR_INVALID, "scenes of instances keep LBVH mesh trees");
+    PHX_TRY(use(tr->ctx));
+    cudaStream_t s = tr->ctx->stream;
+    if (tree == PHX_TREE_SAH) PHX_TRY(tr->tnodes.reserve((size_t)(2 * tr->nfaces - 1) * 64));
+    PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                              (phx_aabb*)tr->bvh.prims.ptr));
+    tr->tree = tree;
+    if (tree == PHX_TREE_SAH) {
+        PHX_TRY(build_sah_tree(tr));
+        PHX_TRY(prepare_sah(tr));
+    } else {
+        PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf));
+        PHX_TRY(prepare(tr));
+    }
+    tr->have_last = false;
+    PHX_TRY(wait_stream(s, 0));
+    return read_status(tr->ctx);
+}
+
+int32_t phx_tracer_autotune_tree(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
+                                 uint32_t frames, uint32_t* chosen, float* ms) {
+    if (!tr || !cam || spp == 0) return fail(PHX_ERR_INVALID, "bad argument");
+    if (tr->forest) return fail(PHX_ERR_INVALID, "scenes of instances keep LBVH mesh trees");
+    PHX_TRY(use(tr->ctx));
+    cudaStream_t s = tr->ctx->stream;
+    float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    cudaEvent_t a = nullptr, b = nullptr;
+    PHX_CUDA(cudaEventCreate(&a));
+    PHX_CUDA(cudaEventCreate(&b));
+    int32_t rc = PHX_OK;
+    for (uint32_t k = 0; k < 2 && rc == PHX_OK; k++) {
+        // build (from the face boxes), then a trace of spp samples, each timed
+        const uint32_t tree = k == 0 ? PHX_TREE_LBVH : PHX_TREE_SAH;
+        rc = cuda_check(cudaEventRecord(a, s), "event");
+        if (rc == PHX_OK) rc = phx_tracer_set_tree(tr, tree);
+        if (rc == PHX_OK) rc = cuda_check(cudaEventRecord(b, s), "event");
+        if (rc == PHX_OK) rc = wait_stream(s, 0);
+        if (rc == PHX_OK) rc = cuda_check(cudaEventElapsedTime(&t[2 * k], a, b), "event");
+        if (rc == PHX_OK) rc = phx_tracer_trace(tr, cam, w, h, 0, spp);  // warms the kernel and the tree
+        if (rc == PHX_OK) rc = cuda_check(cudaEventRecord(a, s), "event");
+        if (rc == PHX_OK) rc = phx_tracer_trace(tr, cam, w, h, 0, spp);
+        if (rc == PHX_OK) rc = cuda_check(cudaEventRecord(b, s), "event");
+        if (rc == PHX_OK) rc = wait_stream(s, 0);
+        if (rc == PHX_OK) rc = cuda_check(cudaEventElapsedTime(&t[2 * k + 1], a, b), "event");
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    PHX_TRY(rc);
+    // build once, then `frames` traces of spp samples each
+    const double lbvh = t[0] + (double)frames * t[1], sah = t[2] + (double)frames * t[3];
+    const uint32_t pick = sah < lbvh ? PHX_TREE_SAH : PHX_TREE_LBVH;
+    if (pick != tr->tree) PHX_TRY(phx_tracer_set_tree(tr, pick));
+    if (chosen) *chosen = pick;
+    if (ms) std::memcpy(ms, t, sizeof t);
+    return PHX_OK;
 }
 
 int32_t phx_tracer_reinstance(phx_tracer tr, const phx_instance* insts, uint32_t ninsts) {
@@ -2680,6 +2812,13 @@ int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebu
     }
     PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
                               (phx_aabb*)tr->bvh.prims.ptr));
+    if (tr->tree == PHX_TREE_SAH) {
+        if (rebuild) PHX_TRY(build_sah_tree(tr));
+        else PHX_TRY(refit_sah_tree(tr));
+        PHX_TRY(prepare_sah(tr));
+        tr->have_last = false;
+        return PHX_OK;
+    }
     if (rebuild) PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf));
     else PHX_TRY(enqueue_refit(tr->ctx, tr->bvh, tr->nfaces, false));
     PHX_TRY(prepare(tr));
@@ -2837,10 +2976,12 @@ struct phx_batch_s {
 namespace phx {
 namespace {
 
-template <int THREADS>
-int32_t launch_batch(phx_batch b) {
+// M: MODE_INST when some job's scene is one of instances (the batch kernel
+// of that mode takes either kind).
+template <int THREADS, int M>
+int32_t launch_batch_mode(phx_batch b) {
     Ctx* c = b->ctx;
-    const void* fn = (const void*)k_render_batch<false, THREADS>;
+    const void* fn = (const void*)k_render_batch<M, THREADS>;
     const int smem = b->stack == PHX_STACK_SHARED ? STACK * 4 * THREADS : 0;
     static std::atomic<uint64_t> done{0};
     const uint64_t bit = 1ull << (c->device & 63);
@@ -2854,10 +2995,17 @@ int32_t launch_batch(phx_batch b) {
     uint32_t grid = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)c->sms;
     grid = std::min<uint32_t>(grid, (warps_needed + THREADS / 32 - 1) / (THREADS / 32));
     PHX_CUDA(cudaMemsetAsync(b->next.ptr, 0, 4, c->stream));
-    k_render_batch<false, THREADS><<<grid, THREADS, smem, c->stream>>>((const Job*)b->djobs.ptr,
-                                                                        (uint32_t)b->jobs.size(), b->ntiles,
-                                                                        (uint32_t*)b->next.ptr);
+    k_render_batch<M, THREADS><<<grid, THREADS, smem, c->stream>>>((const Job*)b->djobs.ptr,
+                                                                    (uint32_t)b->jobs.size(), b->ntiles,
+                                                                    (uint32_t*)b->next.ptr);
     return cuda_check(cudaGetLastError(), "batch render");
+}
+
+template <int THREADS>
+int32_t launch_batch(phx_batch b) {
+    for (const BatchJob& bj : b->jobs)
+        if (bj.tr->forest) return launch_batch_mode<THREADS, MODE_INST>(b);
+    return launch_batch_mode<THREADS, 0>(b);
 }
 
 // Uploads cameras and the job table (host copies: not inside a capture).
@@ -3096,9 +3244,9 @@ int32_t phx_batch_capture(phx_batch b, phx_unet net, float threshold) {
     if (!b) return fail(PHX_ERR_INVALID, "null batch");
     if (b->jobs.empty()) return fail(PHX_ERR_INVALID, "empty batch");
     for (const BatchJob& bj : b->jobs)
-        if (bj.tr->forest)
-            return fail(PHX_ERR_INVALID, "the serving graph rebuilds single-instance scenes; trace a scene of "
-                                         "instances with phx_batch_trace");
+        if (bj.tr->forest || bj.tr->tree != PHX_TREE_LBVH)
+            return fail(PHX_ERR_INVALID, "the serving graph rebuilds single-instance LBVH scenes; trace scenes "
+                                         "of instances or on an SAH tree with phx_batch_trace");
     PHX_TRY(use(b->ctx));
     Ctx* c = b->ctx;
     PHX_TRY(wait_stream(c->stream, BATCH_WAIT_MS));

@@ -185,6 +185,24 @@ class Tracer:
             kw.setdefault("insts", scene.insts)
         return cls(gpu, scene.verts, scene.faces, scene.mats, **kw)
 
+    TREE_LBVH = 0
+    TREE_SAH = 1
+
+    def set_tree(self, tree: int) -> None:
+        """Walk the device LBVH (Tracer.TREE_LBVH) or the binned SAH tree
+        phiray's tracer builds (Tracer.TREE_SAH); rebuilds now."""
+        N.check(N.lib().phx_tracer_set_tree(self.handle, tree))
+
+    def autotune_tree(self, cam: np.ndarray, w: int, h: int, spp: int, frames: int) -> tuple[int, list[float]]:
+        """Times each tree's build and an spp-sample trace; keeps the tree with
+        the lower build + frames x trace. (chosen, [lbvh build, lbvh trace,
+        sah build, sah trace] ms)."""
+        chosen = C.c_uint32()
+        ms = (C.c_float * 4)()
+        N.check(N.lib().phx_tracer_autotune_tree(self.handle, cam.ctypes.data, w, h, spp, frames, C.byref(chosen), ms))
+        self.w, self.h = w, h
+        return chosen.value, list(ms)
+
     def reinstance(self, insts) -> None:
         """``Tracer::reinstance``: the same instances placed anew (the top
         tree is rebuilt on the device)."""

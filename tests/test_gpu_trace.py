@@ -277,3 +277,65 @@ def test_show_matches_oracle(gpu, orc):
     orc.lib.orc_show(cam.ctypes.data, want.ctypes.data)
     assert np.array_equal(got, want)
     tr.close()
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 15], ids=["megakernel", "state_machine", "mk16_sync"])
+@pytest.mark.parametrize("name", list(SCENES))
+def test_sah_tree_image_matches_oracle(gpu, orc, name, kernel):
+    """The tracer walking the binned SAH tree (phx_tracer_set_tree) == the
+    oracle walking its restatement of sah.rs's tree, bit for bit."""
+    s = SCENES[name]()
+    cam = cam_of(s, s.width, s.height)
+    want, orays = oracle_lib.TraceOracle(orc, s, sah=True).trace(cam, 0, s.spp)
+    tr = px.Tracer.of(gpu, s)
+    tr.set_tree(px.Tracer.TREE_SAH)
+    tr.set_kernel(kernel)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    check_image(tr.image(), want, s.width * s.height)
+    assert tr.time()[1] == orays
+    tr.close()
+
+
+def test_sah_tree_repose_and_back_to_lbvh(gpu, orc):
+    import torch
+
+    s = SCENES["c2_small"]()
+    cam = cam_of(s, s.width, s.height)
+    moved = s.verts.copy()
+    moved[:, 0] *= np.float32(1.1)
+    tr = px.Tracer.of(gpu, s)
+    tr.set_tree(px.Tracer.TREE_SAH)
+    tr.repose_device(torch.tensor(moved, device="cuda"), rebuild=True)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    s2 = scenes.Scene(**{**s.__dict__, "verts": moved})
+    want, _ = oracle_lib.TraceOracle(orc, s2, sah=True).trace(cam, 0, s.spp)
+    check_image(tr.image(), want, s.width * s.height)
+    # a refit of the SAH tree: closest hits do not depend on the tree, so
+    # the image stays within the relMSE gate of the rebuilt one
+    back = s.verts.copy()
+    back[:, 0] *= np.float32(1.05)
+    tr.repose_device(torch.tensor(back, device="cuda"), rebuild=False)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    s3 = scenes.Scene(**{**s.__dict__, "verts": back})
+    want3, _ = oracle_lib.TraceOracle(orc, s3, sah=True).trace(cam, 0, s.spp)
+    check_image(tr.image(), want3, s.width * s.height, exact=False)
+    tr.set_tree(px.Tracer.TREE_LBVH)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    want4, _ = oracle_lib.TraceOracle(orc, s3).trace(cam, 0, s.spp)
+    check_image(tr.image(), want4, s.width * s.height)
+    tr.close()
+
+
+def test_autotune_tree_weighs_build_against_frames(gpu, orc):
+    s = SCENES["c2_small"]()
+    cam = cam_of(s, s.width, s.height)
+    tr = px.Tracer.of(gpu, s)
+    chosen, ms = tr.autotune_tree(cam, s.width, s.height, s.spp, 0)
+    assert len(ms) == 4 and all(t > 0 for t in ms)
+    assert chosen == (px.Tracer.TREE_SAH if ms[2] < ms[0] else px.Tracer.TREE_LBVH)
+    many, ms2 = tr.autotune_tree(cam, s.width, s.height, s.spp, 10 ** 6)
+    assert many == (px.Tracer.TREE_SAH if ms2[3] < ms2[1] else px.Tracer.TREE_LBVH)
+    tr.trace(cam, s.width, s.height, 0, s.spp)
+    want, _ = oracle_lib.TraceOracle(orc, s, sah=many == px.Tracer.TREE_SAH).trace(cam, 0, s.spp)
+    check_image(tr.image(), want, s.width * s.height)
+    tr.close()

@@ -53,7 +53,7 @@ def _bound(fn, x, y):
     if fn in ("sin", "cos"):
         return np.full(len(x), 1.5)
     if fn == "pow":
-        return 5.0 + 1.5 * np.abs(y.astype(np.float64) * np.log2(x.astype(np.float64)))
+        return 8.0 + 1.5 * np.abs(y.astype(np.float64) * np.log2(x.astype(np.float64)))
     return 3.0 + 1.5 * np.abs(x.astype(np.float64) * np.log2(np.e))
 
 
