@@ -97,12 +97,13 @@ struct Count {
 };
 
 // Render modes, a kernel's compile-time int template argument: bit 0 counts
-// node steps and triangle tests (STATS builds), bit 1 takes scenes of
-// instances. Kernels without bit 1 walk single-instance scenes only: their
-// code holds no two-level walk and no placed geometry.
+// node steps and triangle tests (STATS builds); bit 1 (FULL) takes scenes of
+// instances and draws the floor grid overlay. Kernels without it take
+// single-instance scenes with the grid off — every benchmark frame — and
+// hold no two-level walk, placed geometry or grid code.
 constexpr int MODE_STATS = 1;
-constexpr int MODE_INST = 2;
-constexpr int MODE_ANY = MODE_INST;  // code that takes either kind of scene
+constexpr int MODE_FULL = 2;
+constexpr int MODE_ANY = MODE_FULL;  // code that takes any scene
 
 struct Frame {
     uint32_t w, h, n, frame0, spp, persp, count, bounces;
@@ -422,7 +423,7 @@ __device__ __forceinline__ Hit walk_scene(const Scene& S, f3 o, f3 d, float tmax
 template <int M>
 __device__ __forceinline__ Hit walk_mode(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     constexpr bool STATS = (M & MODE_STATS) != 0;
-    if ((M & MODE_INST) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
+    if ((M & MODE_FULL) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
     return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 
@@ -430,7 +431,7 @@ __device__ __forceinline__ Hit walk_mode(const Scene& S, f3 o, f3 d, float tmax,
 template <int M>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     constexpr bool STATS = (M & MODE_STATS) != 0;
-    if ((M & MODE_INST) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
+    if ((M & MODE_FULL) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
     if (S.smem_stack) {
         extern __shared__ uint32_t walk_stacks[];
         return walk<STATS, true>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
@@ -508,7 +509,7 @@ __device__ __forceinline__ Geo geo_at(const Scene& S, uint32_t slot, uint32_t in
         g.na = g.nb = g.nc = mk(0.0f);
     }
     g.mirror = false;
-    if ((M & MODE_INST) && S.insts) {
+    if ((M & MODE_FULL) && S.insts) {
         const float4* q = S.insts + 8 * (size_t)inst;
         const uint32_t flags = __float_as_uint(__ldg(q + 7).w);
         g.mirror = (flags & 4u) != 0u;
@@ -829,7 +830,7 @@ template <int M>
 __device__ __forceinline__ float lamp_chance(const Scene& S, uint32_t slot, uint32_t inst) {
     const uint32_t count = S.lamp_count;
     if (count == 0u) return 0.0f;
-    const bool placed = (M & MODE_INST) && S.lamp_inst;
+    const bool placed = (M & MODE_FULL) && S.lamp_inst;
     uint32_t lo = 0, hi = count - 1u;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2u;
@@ -857,7 +858,7 @@ __device__ __forceinline__ Shadowed glow_query(const Scene& S, const Surf& s, ui
     const float prev = lo > 0u ? __ldg(S.lamp_cdf + lo - 1u) : 0.0f;
     const float chance = fmaxf(__ldg(S.lamp_cdf + lo) - prev, 1e-8f);
     const uint32_t f = __ldg(S.lamp_slot + lo);
-    const Geo g = geo_at<M>(S, f, ((M & MODE_INST) && S.lamp_inst) ? __ldg(S.lamp_inst + lo) : 0u);
+    const Geo g = geo_at<M>(S, f, ((M & MODE_FULL) && S.lamp_inst) ? __ldg(S.lamp_inst + lo) : 0u);
     const Mat t = mat_at(S, g.mat);
     float a = rnd(seed);
     float b = rnd(seed);

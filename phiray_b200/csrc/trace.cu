@@ -387,7 +387,7 @@ __device__ __noinline__ f3 direct(const Scene& S, const Frame& F, const Surf& s,
 // glow_mis (integrate.wgsl:15-23).
 template <int M>
 __device__ __forceinline__ f3 glow_mis(const Scene& S, const Geo& g, f3 emit, const Hit& h, f3 from_n, f3 dir) {
-    const float chance = lamp_chance<M>(S, h.tri, h.inst);
+    const float chance = lamp_chance<M>(S, h.tri, (M & MODE_FULL) ? h.inst : 0u);
     if (chance <= 0.0f) return emit;
     const f3 cr = cross(g.b - g.a, g.c - g.a);
     const float pl = chance * h.t * h.t / fmaxf(0.5f * length(cr) * fabsf(dot(normalize(cr), dir)), 1e-8f);
@@ -428,7 +428,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
             break;
         }
         if (!bounce) break;
-        const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+        const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
         const Mat t = mat_at(S, g.mat);
         const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
         const f3 ng = dot(ng0, dir) < 0.0f ? ng0 : -ng0;
@@ -467,7 +467,7 @@ __device__ __forceinline__ f3 indirect(const Scene& S, const Frame& F, f3 pos, f
 template <int STATS>
 __device__ __forceinline__ f3 bounce_light(const Scene& S, const Frame& F, const Hit& h, f3 org, f3 d,
                                            uint32_t& seed, f3 sun, Count& cnt) {
-    const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+    const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
     const Mat t = mat_at(S, g.mat);
     const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
     const f3 ng = dot(ng0, d) < 0.0f ? ng0 : -ng0;
@@ -539,7 +539,7 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
                 acc.film += 1.0f;
                 acc.lin += mk(0.0f);
                 if (F.adapt_on && (frame & 1u)) acc.half = acc.half + mk(0.0f) * 2.0f;
-                if (F.grid > 0.0f) {
+                if ((STATS & MODE_FULL) && F.grid > 0.0f) {
                     const Over g = grid_over(F, o, d, INF);
                     acc.grid += sky * (1.0f - g.a) + g.c;
                 } else {
@@ -552,17 +552,17 @@ __device__ void sample(const Scene& S, const Frame& F, uint32_t i, uint32_t fram
             break;
         }
         if (bounce == 0u) {
-            acc.outline = h.inst + 1u;  // outline_store(i, h.inst + 1)
+            acc.outline = ((STATS & MODE_FULL) ? h.inst : 0u) + 1u;  // outline_store(i, h.inst + 1)
             // emit's overlay term grid_over(o0, d0, first_t) is a function of
             // the first ray and hit alone: added once per sample here, where
             // they are at hand, instead of at emit (util.wgsl:101-145)
-            if (F.grid > 0.0f) {
+            if ((STATS & MODE_FULL) && F.grid > 0.0f) {
                 const Over gr = grid_over(F, o, d, h.t);
                 acc.grid += gr.c;
                 acc.cov += gr.a;
             }
         }
-        const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+        const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
         const Mat t = mat_at(S, g.mat);
         const float w = 1.0f - h.u - h.v;
         const f3 hit = o + d * h.t;
@@ -1060,7 +1060,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                     acc.count += 1u;
                     acc.film += 1.0f;
                     acc.lin += mk(0.0f);
-                    if (F.grid > 0.0f) {
+                    if ((STATS & MODE_FULL) && F.grid > 0.0f) {
                         const Over gr = grid_over(F, P.o, P.d, INF);
                         acc.grid += sky * (1.0f - gr.a) + gr.c;
                     } else {
@@ -1073,14 +1073,14 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 return PH_EMIT_END;
             }
             if (P.bounce == 0u) {
-                acc.outline = h.inst + 1u;
-                if (F.grid > 0.0f) {  // emit's overlay, as in sample()
+                acc.outline = ((STATS & MODE_FULL) ? h.inst : 0u) + 1u;
+                if ((STATS & MODE_FULL) && F.grid > 0.0f) {  // emit's overlay, as in sample()
                     const Over gr = grid_over(F, P.o, P.d, h.t);
                     acc.grid += gr.c;
                     acc.cov += gr.a;
                 }
             }
-            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
             const Mat t = mat_at(S, g.mat);
             const float w = 1.0f - h.u - h.v;
             const f3 hit = P.o + P.d * h.t;
@@ -1200,7 +1200,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 P.aval = P.iacc;
                 return PH_AFTER_INDIRECT;
             }
-            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
             const Mat t = mat_at(S, g.mat);
             const f3 dir = P.idir;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -1281,7 +1281,7 @@ __device__ __forceinline__ uint32_t step(const Scene& S, const Frame& F, Path& P
                 return PH_AFTER_GLOSSY;
             }
             // bounce_light (integrate.wgsl:236-250) up to its direct().
-            const Geo g = geo_at<STATS>(S, h.tri, h.inst);
+            const Geo g = geo_at<STATS>(S, h.tri, (STATS & MODE_FULL) ? h.inst : 0u);
             const Mat t = mat_at(S, g.mat);
             const f3 d = P.rd;
             const f3 ng0 = normalize(cross(g.b - g.a, g.c - g.a));
@@ -2085,7 +2085,7 @@ int32_t ensure_image(phx_tracer tr, uint32_t w, uint32_t h) {
     return PHX_OK;
 }
 
-// The render kernels of one mode M (MODE_STATS, MODE_INST bits) at the
+// The render kernels of one mode M (MODE_STATS, MODE_FULL bits) at the
 // tracer's kernel id, over pixels [first_px, first_px + count_px).
 struct RenderLaunch {
     Scene S;
@@ -2140,8 +2140,9 @@ int32_t launch_flat(uint32_t kernel, const RenderLaunch& L) {
     }
 }
 
-// Scenes of instances: three forms — the state machine, and the
-// megakernel at the 4-block and the 16-block (per-sample wait) budgets —
+// Scenes of instances and frames with the floor grid: three forms — the
+// state machine, and the megakernel at the 4-block and the 16-block
+// (per-sample wait) budgets —
 // each kernel id taking the one nearest its own (every form computes the
 // same image).
 template <int M>
@@ -2164,8 +2165,8 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
         kernel = PHX_KERNEL_MEGAKERNEL;
     const RenderLaunch L{scene_of(tr), F,       sun,    (uint32_t*)tr->px.ptr, first_px, count_px,
                          (unsigned long long*)tr->rays.ptr, (uint32_t*)tr->next.ptr, c->sms, c->stream};
-    if (tr->forest)
-        return stats ? launch_placed<MODE_INST | MODE_STATS>(kernel, L) : launch_placed<MODE_INST>(kernel, L);
+    if (tr->forest || F.grid > 0.0f)
+        return stats ? launch_placed<MODE_FULL | MODE_STATS>(kernel, L) : launch_placed<MODE_FULL>(kernel, L);
     return stats ? launch_flat<MODE_STATS>(kernel, L) : launch_flat<0>(kernel, L);
 }
 
@@ -2976,8 +2977,8 @@ struct phx_batch_s {
 namespace phx {
 namespace {
 
-// M: MODE_INST when some job's scene is one of instances (the batch kernel
-// of that mode takes either kind).
+// M: MODE_FULL when some job's scene is one of instances or its frame draws
+// the floor grid (the batch kernel of that mode takes every job).
 template <int THREADS, int M>
 int32_t launch_batch_mode(phx_batch b) {
     Ctx* c = b->ctx;
@@ -3004,7 +3005,7 @@ int32_t launch_batch_mode(phx_batch b) {
 template <int THREADS>
 int32_t launch_batch(phx_batch b) {
     for (const BatchJob& bj : b->jobs)
-        if (bj.tr->forest) return launch_batch_mode<THREADS, MODE_INST>(b);
+        if (bj.tr->forest || bj.cam.grid > 0.0f) return launch_batch_mode<THREADS, MODE_FULL>(b);
     return launch_batch_mode<THREADS, 0>(b);
 }
 
