@@ -42,7 +42,7 @@ WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 6
 
 KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8", "megakernel/3", "megakernel/2",
                 "megakernel/sync", "megakernel/2/sync", "megakernel/5", "megakernel/6", "megakernel/6/sync", "megakernel/8", "megakernel/8/sync",
-                "megakernel/10/sync", "megakernel/12/sync", "megakernel/16/sync"]
+                "megakernel/10/sync", "megakernel/12/sync", "megakernel/16/sync", "wavefront"]
 
 
 def peaks() -> dict:

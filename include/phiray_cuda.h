@@ -464,8 +464,14 @@ int32_t phx_tracer_destroy(phx_tracer tr);
 #define PHX_KERNEL_MEGAKERNEL_10_SYNC 13u
 #define PHX_KERNEL_MEGAKERNEL_12_SYNC 14u
 #define PHX_KERNEL_MEGAKERNEL_16_SYNC 15u
+/* The wavefront render: path state in device memory, rays queued by type
+ * (primary, extension, shadow) with ballot compaction, each queue walked by a
+ * kernel of its own (closest or any hit) between passes of the shading
+ * logic; the host polls the queues every fourth pass. Not inside a graph
+ * capture nor with adaptive sampling (the megakernel runs those frames). */
+#define PHX_KERNEL_WAVEFRONT 16u
 /* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
-#define PHX_KERNEL_COUNT 16u
+#define PHX_KERNEL_COUNT 17u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer

@@ -971,7 +971,7 @@ __device__ __forceinline__ Over z_axis_over(const Frame& F, f3 o, f3 d, float t_
 }
 
 // grid_over: nothing unless the camera turns the grid on.
-__device__ __noinline__ Over grid_over(const Frame& F, f3 o, f3 d, float t_hit) {
+static __device__ __noinline__ Over grid_over(const Frame& F, f3 o, f3 d, float t_hit) {
     const float px = 1.0f / (F.scale * F.units * (float)F.w);
     Over g = floor_over(F, o, d, t_hit, px);
     if (F.grid > 0.0f && (F.grid_hide & 8u) != 0u) {

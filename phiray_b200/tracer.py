@@ -225,7 +225,8 @@ class Tracer:
     MEGAKERNEL_10_SYNC = 13
     MEGAKERNEL_12_SYNC = 14
     MEGAKERNEL_16_SYNC = 15
-    KERNELS = 16
+    WAVEFRONT = 16
+    KERNELS = 17
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""

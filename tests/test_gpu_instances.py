@@ -25,7 +25,7 @@ def want(orc, scene):
     return (cam,) + oracle_lib.TraceOracle(orc, scene).trace(cam, 0, scene.spp)
 
 
-@pytest.mark.parametrize("kernel", list(range(16)))
+@pytest.mark.parametrize("kernel", list(range(17)))
 def test_instanced_image_matches_oracle(gpu, scene, want, kernel):
     cam, img, rays = want
     tr = px.Tracer.of(gpu, scene)

@@ -84,7 +84,7 @@ def test_emitters_closed_form_on_the_device(gpu, orc, case):
 
 
 @pytest.mark.parametrize("persp", [False, True])
-@pytest.mark.parametrize("kernel", [0, 1, 15], ids=["megakernel", "state_machine", "mk16_sync"])
+@pytest.mark.parametrize("kernel", [0, 1, 15, 16], ids=["megakernel", "state_machine", "mk16_sync", "wavefront"])
 def test_box_floor_sky_and_grid_on_the_device(gpu, orc, persp, kernel):
     scene, cam = pins.box_scene(persp)
     want, _ = pins.render_oracle(orc, scene, cam, pins.SAMPLE_COUNT)

@@ -50,9 +50,9 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("kernel", list(range(16)),
+@pytest.mark.parametrize("kernel", list(range(17)),
                          ids=["megakernel", "state_machine", "sm6", "sm8", "mk3", "mk2", "mk_sync", "mk2_sync", "mk5",
-                              "mk6", "mk6_sync", "mk8", "mk8_sync", "mk10_sync", "mk12_sync", "mk16_sync"])
+                              "mk6", "mk6_sync", "mk8", "mk8_sync", "mk10_sync", "mk12_sync", "mk16_sync", "wavefront"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_image_matches_oracle(gpu, orc, name, kernel):
     s = SCENES[name]()
@@ -163,7 +163,7 @@ def test_autotune_keeps_the_image(gpu, orc):
     cam = cam_of(s, s.width, s.height)
     tr = px.Tracer.of(gpu, s)
     chosen, ms = tr.autotune(cam, s.width, s.height, 2)
-    assert chosen in range(16) and len(ms) == 16 and all(t > 0 for t in ms)
+    assert chosen in range(17) and len(ms) == 17 and all(t > 0 for t in ms)
     tr.trace(cam, s.width, s.height, 0, s.spp)
     want, _ = oracle_lib.TraceOracle(orc, s).trace(cam, 0, s.spp)
     check_image(tr.image(), want, s.width * s.height)
@@ -279,7 +279,7 @@ def test_show_matches_oracle(gpu, orc):
     tr.close()
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 15], ids=["megakernel", "state_machine", "mk16_sync"])
+@pytest.mark.parametrize("kernel", [0, 1, 15, 16], ids=["megakernel", "state_machine", "mk16_sync", "wavefront"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_sah_tree_image_matches_oracle(gpu, orc, name, kernel):
     """The tracer walking the binned SAH tree (phx_tracer_set_tree) == the
