@@ -79,18 +79,9 @@ SAH_HD uint32_t bin_of(const float* c, const float* lo, const float* scale, int 
     return b < BINS - 1 ? b : BINS - 1;
 }
 
-// sah.rs:114-189 split: the left count after reordering slots[0, count), or
-// NONE for a leaf. Serial over the node's slots.
-SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots, uint32_t count, uint32_t leaf) {
-    if (count <= 1) return NONE;
-    Box cbox = empty_box();
-    for (uint32_t j = 0; j < count; j++) {
-        const float* c = centres + 3 * (uint64_t)slots[j];
-        Box p;
-        for (int k = 0; k < 3; k++) p.lo[k] = p.hi[k] = c[k];
-        grow(cbox, p);
-    }
-    float lo[3], scale[3];
+// Grid::of (sah.rs:40-66): the bins' origin and scale from a node's box of
+// centres; true when every centre sits in one point (no plane separates).
+SAH_HD bool grid_of(const Box& cbox, float* lo, float* scale) {
     bool flat = true;
     for (int k = 0; k < 3; k++) {
         const float e = cbox.hi[k] - cbox.lo[k];
@@ -98,26 +89,21 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
         scale[k] = e > 0.0f ? (float)BINS * (1.0f - 1e-5f) / e : 0.0f;
         if (scale[k] != 0.0f) flat = false;
     }
-    if (flat) return count > leaf ? count / 2 : NONE;
-    uint32_t bcount[3][BINS];
-    Box bbox[3][BINS];
-    for (int k = 0; k < 3; k++)
-        for (uint32_t b = 0; b < BINS; b++) {
-            bcount[k][b] = 0;
-            bbox[k][b] = empty_box();
-        }
-    for (uint32_t j = 0; j < count; j++) {
-        const uint32_t i = slots[j];
-        const Box pb = prim_box(prims + 8 * (uint64_t)i);
-        for (int k = 0; k < 3; k++) {
-            const uint32_t at = bin_of(centres + 3 * (uint64_t)i, lo, scale, k);
-            bcount[k][at] += 1;
-            grow(bbox[k][at], pb);
-        }
-    }
+    return !flat;
+}
+
+// What split does with a node once its bins are filled (sah.rs:150-181):
+// the cheapest plane over the three axes' sweeps, then the leaf rule.
+enum Cut : uint32_t { CUT_LEAF = 0, CUT_HALF = 1, CUT_PLANE = 2 };
+struct Decision {
+    uint32_t cut, axis, at;
+};
+
+SAH_HD Decision decide(const uint32_t (*bcount)[BINS], const Box (*bbox)[BINS], const float* scale, uint32_t count,
+                       uint32_t leaf) {
     bool have = false;
     float best = 0.0f;
-    int best_k = 0;
+    uint32_t best_k = 0;
     uint32_t best_at = 0;
     for (int k = 0; k < 3; k++) {
         if (scale[k] == 0.0f) continue;
@@ -142,19 +128,54 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
             if (!have || cost < best) {
                 have = true;
                 best = cost;
-                best_k = k;
+                best_k = (uint32_t)k;
                 best_at = at;
             }
         }
     }
     Box bounds = empty_box();
     for (uint32_t b = 0; b < BINS; b++) grow(bounds, bbox[0][b]);
-    if (!have) return count > leaf ? count / 2 : NONE;
+    if (!have) return Decision{count > leaf ? (uint32_t)CUT_HALF : (uint32_t)CUT_LEAF, 0u, 0u};
     const float parent = rmax(area(bounds), 1.17549435e-38f);  // f32::MIN_POSITIVE
-    if (count <= leaf && TRAVERSE + best / parent >= (float)count) return NONE;
+    if (count <= leaf && TRAVERSE + best / parent >= (float)count) return Decision{CUT_LEAF, 0u, 0u};
+    return Decision{CUT_PLANE, best_k, best_at};
+}
+
+// sah.rs:114-189 split: the left count after reordering slots[0, count), or
+// NONE for a leaf. Serial over the node's slots.
+SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots, uint32_t count, uint32_t leaf) {
+    if (count <= 1) return NONE;
+    Box cbox = empty_box();
+    for (uint32_t j = 0; j < count; j++) {
+        const float* c = centres + 3 * (uint64_t)slots[j];
+        Box p;
+        for (int k = 0; k < 3; k++) p.lo[k] = p.hi[k] = c[k];
+        grow(cbox, p);
+    }
+    float lo[3], scale[3];
+    if (!grid_of(cbox, lo, scale)) return count > leaf ? count / 2 : NONE;
+    uint32_t bcount[3][BINS];
+    Box bbox[3][BINS];
+    for (int k = 0; k < 3; k++)
+        for (uint32_t b = 0; b < BINS; b++) {
+            bcount[k][b] = 0;
+            bbox[k][b] = empty_box();
+        }
+    for (uint32_t j = 0; j < count; j++) {
+        const uint32_t i = slots[j];
+        const Box pb = prim_box(prims + 8 * (uint64_t)i);
+        for (int k = 0; k < 3; k++) {
+            const uint32_t at = bin_of(centres + 3 * (uint64_t)i, lo, scale, k);
+            bcount[k][at] += 1;
+            grow(bbox[k][at], pb);
+        }
+    }
+    const Decision d = decide(bcount, bbox, scale, count, leaf);
+    if (d.cut == CUT_LEAF) return NONE;
+    if (d.cut == CUT_HALF) return count / 2;
     uint32_t m = 0;
     for (uint32_t j = 0; j < count; j++) {
-        if (bin_of(centres + 3 * (uint64_t)slots[j], lo, scale, best_k) <= best_at) {
+        if (bin_of(centres + 3 * (uint64_t)slots[j], lo, scale, (int)d.axis) <= d.at) {
             const uint32_t t = slots[j];
             slots[j] = slots[m];
             slots[m] = t;

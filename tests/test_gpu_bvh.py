@@ -206,6 +206,28 @@ def test_sah_build_equals_the_reference_tree(gpu, orc, n, leaf):
     assert np.array_equal(got.nodes.view(np.uint32), want_nodes.view(np.uint32))
 
 
+def test_sah_build_of_many_big_nodes(gpu, orc):
+    """300,000 boxes (a spread, a dense clump, and 9,000 copies of one box):
+    many levels of nodes cut over blocks, with several such nodes a level,
+    flat ones among them, == the restatement word for word."""
+    from phiray_b200.bvh import build_sah
+
+    rng = np.random.default_rng(11)
+    n = 300_000
+    lo = rng.uniform(0.0, 100.0, (n, 3)).astype(np.float32)
+    lo[: n // 4] = rng.normal(40.0, 0.5, (n // 4, 3)).astype(np.float32)
+    size = rng.uniform(0.01, 2.0, (n, 3)).astype(np.float32)
+    p = np.zeros((n, 8), np.float32)
+    p[:, 0:3], p[:, 4:7] = lo, lo + size
+    p[n - 9000:, 0:3], p[n - 9000:, 4:7] = 7.0, 7.5
+    p = p[rng.permutation(n)]
+    want_nodes, want_order, want_depth = orc.build_sah(p, 4)
+    got = build_sah(gpu, p, 4)
+    assert got.depth == want_depth
+    assert np.array_equal(got.order, want_order)
+    assert np.array_equal(got.nodes.view(np.uint32), want_nodes.view(np.uint32))
+
+
 def test_sah_build_on_a_mesh(gpu, orc):
     from phiray_b200.bvh import build_sah
 
