@@ -37,7 +37,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "1080p frames/s at equal relMSE vs 4096spp: denoised low-spp vs plain; Mrays/s"
 UNIT = "Mrays/s"
-WORKLOAD = "c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 64 spp, 8 bounces, LBVH rebuild + trace + denoise per frame"
+WORKLOAD = ("c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 64 spp, 8 bounces, "
+            "tree rebuild (the autotuner's pick of LBVH or binned SAH) + trace + denoise per frame")
 
 
 KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8", "megakernel/3", "megakernel/2",
@@ -444,6 +445,38 @@ def run_c5(args) -> None:
     gpu.close()
 
 
+def timed_fn(gpu, stream, fn, reps: int) -> float:
+    """Mean device ms of fn over reps calls (after one untimed call), by
+    CUDA events on the library's stream."""
+    import torch
+
+    fn()
+    gpu.wait(60000)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        fn()
+    b.record(stream)
+    gpu.wait(60000)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def count_launches(fn) -> int:
+    """Kernels one call of fn launches, counted by the CUDA activity trace
+    of torch.profiler (every kernel of the process, the library's included)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    evs = [e for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA and
+           not e.name.startswith(("Memcpy", "Memset", "[memory]"))]
+    return len(evs)
+
+
 def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
     """The headline comparison at 1080p against a 4096-spp render of the same
     frame: plain tracing + the a-trous Denoise at `plain` spp against the
@@ -659,7 +692,17 @@ def main() -> None:
         gpu.close()
         return
 
+    # The tree for this step: the SAH tree where its build costs less than
+    # the trace time it saves over the step's samples (build + spp/4 frames
+    # of 4 spp each), else the LBVH; then the render kernel on that tree.
+    nf = s.ntris
+    build_ms = timed_fn(gpu, stream, lambda: tr.repose_device(verts_dev, rebuild=True), 10)
+    refit_ms = timed_fn(gpu, stream, lambda: tr.repose_device(verts_dev, rebuild=False), 10)
+    tree, tree_ms = tr.autotune_tree(cam, W, H, 4, max(1, args.spp // 4))
+    sah_build_ms = timed_fn(gpu, stream, lambda: tr.set_tree(px.Tracer.TREE_SAH), 3)
+    tr.set_tree(tree)
     chosen, tune_ms = tr.autotune(cam, W, H, 4)  # the render kernel for this scene (keeps the image contract)
+    launches = count_launches(step)
     for _ in range(args.warmup):
         step()
     barrier()
@@ -677,20 +720,9 @@ def main() -> None:
 
     # Phase timings (same device, outside the headline loop).
     def timed(fn, reps):
-        fn()
-        gpu.wait(60000)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            fn()
-        b.record(stream)
-        gpu.wait(60000)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / reps
+        return timed_fn(gpu, stream, fn, reps)
 
-    nf = s.ntris
-    build_ms = timed(lambda: tr.repose_device(verts_dev, rebuild=True), 10)
-    refit_ms = timed(lambda: tr.repose_device(verts_dev, rebuild=False), 10)
+    tree_build_ms = timed(lambda: tr.repose_device(verts_dev, rebuild=True), 5)
     tr.trace(cam, W, H, 0, args.spp)
     trace_ms, trace_rays = tr.time()
     denoise_ms = timed(lambda: tr.denoise(), 5)
@@ -710,14 +742,23 @@ def main() -> None:
     tr.secondary_rays(cam, W, H, 0, rays)
     walk_ms = {}
     walks = {"thread_per_ray": px.Tracer.WALK_THREAD, "persistent_fetch": px.Tracer.WALK_FETCH,
-             "sorted_fetch": px.Tracer.WALK_SORTED}
-    for name, mode in walks.items():
-        tr.set_walk(mode)
-        walk_ms[name] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)  # the sort is inside the timing
-    inc_ms = min(walk_ms.values())
-    tr.set_walk(walks[min(walk_ms, key=walk_ms.get)])
+             "sorted_fetch": px.Tracer.WALK_SORTED, "wide_fetch": px.Tracer.WALK_WIDE}
+    tree_names = {px.Tracer.TREE_LBVH: "lbvh", px.Tracer.TREE_SAH: "sah"}
+    for t_kind in (px.Tracer.TREE_LBVH, px.Tracer.TREE_SAH):
+        tr.set_tree(t_kind)
+        for name, mode in walks.items():
+            tr.set_walk(mode)
+            tr.trace_rays(rays, n, hits, False)  # (the wide walk collapses its tree here, untimed)
+            walk_ms[f"{tree_names[t_kind]}/{name}"] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
+    best_walk = min(walk_ms, key=walk_ms.get)
+    inc_ms = walk_ms[best_walk]
+    tr.set_tree({"lbvh": px.Tracer.TREE_LBVH, "sah": px.Tracer.TREE_SAH}[best_walk.split("/")[0]])
+    tr.set_walk(walks[best_walk.split("/")[1]])
     _, inc_steps, inc_tests = tr.trace_rays_stats(rays, n, hits, False)
-    inc_bytes = inc_steps * 64 + inc_tests * 48
+    node_bytes = 128 if best_walk.endswith("wide_fetch") else 64
+    inc_bytes = inc_steps * node_bytes + inc_tests * 48
+    tr.set_walk(px.Tracer.WALK_THREAD)
+    tr.set_tree(tree)
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
     ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
     prim_ms = timed(lambda: tr.primary(cam, W, H, 0, ids, ts), 10)
@@ -734,6 +775,8 @@ def main() -> None:
     def e2e_step():
         t0 = time.perf_counter()
         t = px.Tracer(gpu, hv, hf, hm)
+        if tree != px.Tracer.TREE_LBVH:
+            t.set_tree(tree)  # the tree the autotuner picked (rebuilt over the uploaded faces)
         t.set_kernel(chosen)  # the render kernel the autotuner picked for this scene
         gpu.wait(60000)
         t1 = time.perf_counter()
@@ -786,13 +829,19 @@ def main() -> None:
                               "ms_4spp": {KERNEL_NAMES[k]: round(v, 3) for k, v in enumerate(tune_ms)}},
             "frames_per_s": round(1000.0 / ms_step * world, 3),
             "rays_per_frame": int(rays_per_frame),
+            "tree": {"chosen": tree_names[tree],
+                     "autotune_ms": dict(zip(("lbvh_build", "lbvh_trace_4spp", "sah_build", "sah_trace_4spp"),
+                                             [round(v, 3) for v in tree_ms])),
+                     "frames_weighed": max(1, args.spp // 4)},
             "phases_ms": {"lbvh_build": round(build_ms, 3), "lbvh_refit": round(refit_ms, 3),
+                          "sah_build": round(sah_build_ms, 3), "tree_rebuild_in_step": round(tree_build_ms, 3),
                           "trace": round(trace_ms, 3), "denoise": round(denoise_ms, 3)},
             "lbvh_build_gbs": round(412 * nf / (build_ms * 1e-3) / 1e9, 1),
             "lbvh_refit_gbs": round(172 * nf / (refit_ms * 1e-3) / 1e9, 1),
             "incoherent_grays": round(n / (inc_ms * 1e-3) / 1e9, 3),
             "incoherent_grays_by_walk": {k: round(n / (v * 1e-3) / 1e9, 3) for k, v in walk_ms.items()},
-            "incoherent_walk": {"steps_per_ray": round(inc_steps / n, 2), "tests_per_ray": round(inc_tests / n, 2),
+            "incoherent_walk": {"best": best_walk, "node_bytes": node_bytes,
+                                "steps_per_ray": round(inc_steps / n, 2), "tests_per_ray": round(inc_tests / n, 2),
                                 "achieved_gbs": round(inc_bytes / (inc_ms * 1e-3) / 1e9, 1),
                                 "frac_of_hbm": round(inc_bytes / (inc_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)},
             "primary_grays": round(n / (prim_ms * 1e-3) / 1e9, 3),
@@ -804,7 +853,7 @@ def main() -> None:
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "phases_ms": {k: round(v / max(2, args.steps // 2), 1) for k, v in e2e_parts.items()}},
             "denoised": denoised,
-            "gpu_launches": 21 * args.steps,
+            "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(out), flush=True)

@@ -495,6 +495,14 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
  * radix sort by (direction octant, Morton code of the origin), each hit
  * still written at its ray's index. */
 #define PHX_WALK_SORTED 2u
+/* PHX_WALK_WIDE: persistent warps over a 4-wide tree collapsed on the
+ * device from the binary tree (the LBVH or the SAH tree; its boxes and leaf
+ * ranges unchanged), at about half the steps a ray, four slab tests a step.
+ * The wide tree is made when first walked after a build, refit or tree
+ * switch (waits). Closest hits equal the binary walk's but for the face
+ * named at a tie (two faces at one t); any-hit rays report the same
+ * hit-or-miss. Single-instance scenes. */
+#define PHX_WALK_WIDE 3u
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
 /* Which tree the tracer walks. PHX_TREE_LBVH (the default): the device LBVH
  * (Morton codes, stable radix sort, Karras, leaf packing; 0.6 ms at 1.3 M

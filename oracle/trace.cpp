@@ -1684,8 +1684,10 @@ static void scene_trace(void* handle, const phx_camera* cam, uint32_t first, uin
     const float eps = S.extent * 1e-5f;
     const uint32_t r1 = rows ? (row0 + rows < hh ? row0 + rows : hh) : hh;
     uint64_t total = 0;
-#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total, steps_sum, tests_sum)
-    for (int64_t y = row0; y < (int64_t)r1; y++) {
+    // Pixels are independent: threads take runs of 32 pixels, so a band of
+    // one row keeps every thread busy too.
+#pragma omp parallel reduction(+ : total, steps_sum, tests_sum)
+    {
         World W = h->W0;  // the scene is shared; counters are per thread
         W.p = cam;
         W.n = n;
@@ -1693,11 +1695,11 @@ static void scene_trace(void* handle, const phx_camera* cam, uint32_t first, uin
         W.ao = ao;
         W.eps = eps;
         W.rays = 0;
-        for (uint32_t x = 0; x < w; x++) {
-            const uint32_t i = (uint32_t)y * w + x;
+#pragma omp for schedule(dynamic, 32)
+        for (int64_t i = (int64_t)row0 * w; i < (int64_t)r1 * w; i++) {
             for (uint32_t f = first; f < first + spp; f++) {
                 W.frame = f;
-                shade_main(W, i);
+                shade_main(W, (uint32_t)i);
             }
         }
         total += W.rays;

@@ -62,6 +62,16 @@ int32_t render_batch(int threads, bool full, bool smem_stack, int device, int sm
                      uint32_t ntiles, uint32_t* next, cudaStream_t s);
 // sizeof the batch kernel's job record.
 size_t batch_job_bytes();
+// The 4-wide tree collapsed from the tracer's binary records `bin` (wide.cu):
+// at most `ninner` 128-byte wide records (0: the root is a leaf, nothing to
+// build); jobs_a/jobs_b hold ninner (wide id, record) pairs each, counts 2
+// words. Waits on `s` once a level.
+int32_t build_wide(const float4* bin, uint32_t ninner, float4* wide, uint2* jobs_a, uint2* jobs_b, uint32_t* counts,
+                   cudaStream_t s, uint32_t* nodes_out, uint32_t* levels_out);
+// Persistent walks of n rays over the wide tree (counters: rays, steps,
+// tests, or null; next: one word of scratch).
+int32_t launch_rays_wide(const Scene& S, const float4* wide, const float* rays, uint32_t n, float* hits, bool any,
+                         unsigned long long* counters, uint32_t* next, int sms, cudaStream_t s);
 
 namespace {
 

@@ -628,6 +628,10 @@ struct phx_tracer_s {
     bool smem_stack = false;                     // ray walks keep their stack in shared memory
     uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, persistent warps, sorted first
     DevMem rkeys, rsorted, rorder, ralt_k, ralt_v, rzero;  // the sorted walk's keys and radix-sort scratch
+    // The 4-wide tree of PHX_WALK_WIDE, collapsed from the binary tree when
+    // first walked after tree_gen moved (every build, refit or tree switch).
+    DevMem wide, wide_jobs_a, wide_jobs_b, wide_counts;
+    uint32_t tree_gen = 0, wide_gen = 0xFFFFFFFFu, wide_nodes = 0, wide_levels = 0;
     bool have_last = false;
     // Adaptive Sampling, [threshold, min samples, step, on] (Tracer::adapt,
     // set_adaptive): every frame this tracer traces takes it in place of the
@@ -642,6 +646,7 @@ namespace {
 int32_t prepare(phx_tracer tr) {
     // After a build or refit: face boxes are in tr->bvh; gather, mark leaf
     // ends, convert nodes, root info, emitter table.
+    tr->tree_gen++;
     Ctx* c = tr->ctx;
     cudaStream_t s = c->stream;
     const uint32_t n = tr->nfaces;
@@ -831,6 +836,7 @@ int32_t build_sah_tree(phx_tracer tr) {
 }
 
 int32_t prepare_sah(phx_tracer tr) {
+    tr->tree_gen++;
     Ctx* c = tr->ctx;
     cudaStream_t s = c->stream;
     const uint32_t n = tr->nfaces, m = tr->sah_count;
@@ -1412,7 +1418,9 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
 
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (mode > PHX_WALK_SORTED) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
+    if (mode > PHX_WALK_WIDE) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
+    if (mode == PHX_WALK_WIDE && tr->forest)
+        return fail(PHX_ERR_INVALID, "the wide walk takes single-instance scenes");
     tr->walk = mode;
     return PHX_OK;
 }
@@ -1729,11 +1737,45 @@ int32_t sort_rays(phx_tracer tr, const Scene& S, const float* rays, uint32_t n, 
 }  // namespace
 }  // namespace phx
 
+namespace phx {
+namespace {
+// The wide tree of the binary tree the tracer walks now (collapsed on the
+// device when the tree changed since the last collapse; waits).
+int32_t ensure_wide(phx_tracer tr) {
+    if (tr->wide_gen == tr->tree_gen) return PHX_OK;
+    Ctx* c = tr->ctx;
+    float4 root{};
+    PHX_CUDA(cudaMemcpyAsync(&root, tr->info.ptr, sizeof root, cudaMemcpyDeviceToHost, c->stream));
+    PHX_TRY(wait_stream(c->stream, 0));
+    uint32_t root_ref = 0;
+    std::memcpy(&root_ref, &root.w, 4);
+    const bool leaf_root = (root_ref & LEAF) != 0;
+    const uint32_t ninner = (leaf_root || tr->nfaces < 2) ? 0u : tr->nfaces - 1;
+    if (ninner) {
+        PHX_TRY(tr->wide.reserve((size_t)ninner * 128));
+        PHX_TRY(tr->wide_jobs_a.reserve((size_t)ninner * 8));
+        PHX_TRY(tr->wide_jobs_b.reserve((size_t)ninner * 8));
+        PHX_TRY(tr->wide_counts.reserve(8));
+    }
+    PHX_TRY(build_wide((const float4*)tr->tnodes.ptr, ninner, (float4*)tr->wide.ptr, (uint2*)tr->wide_jobs_a.ptr,
+                       (uint2*)tr->wide_jobs_b.ptr, (uint32_t*)tr->wide_counts.ptr, c->stream, &tr->wide_nodes,
+                       &tr->wide_levels));
+    tr->wide_gen = tr->tree_gen;
+    return read_status(c);
+}
+}  // namespace
+}  // namespace phx
+
 int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit) {
     if (!tr || (n && (!rays || !hits))) return fail(PHX_ERR_INVALID, "null argument");
     if (n == 0) return PHX_OK;
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
+    if (tr->walk == PHX_WALK_WIDE) {
+        PHX_TRY(ensure_wide(tr));
+        return launch_rays_wide(S, (const float4*)tr->wide.ptr, rays, n, hits, any_hit != 0, nullptr,
+                                (uint32_t*)tr->next.ptr, tr->ctx->sms, tr->ctx->stream);
+    }
     uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
     const uint32_t* order = nullptr;
     if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));
@@ -1751,7 +1793,11 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
     cudaStream_t s = tr->ctx->stream;
     PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
     const Scene S = scene_of(tr);
-    if (n) {
+    if (n && tr->walk == PHX_WALK_WIDE) {
+        PHX_TRY(ensure_wide(tr));
+        PHX_TRY(launch_rays_wide(S, (const float4*)tr->wide.ptr, rays, n, hits, any_hit != 0,
+                                 (unsigned long long*)tr->rays.ptr, (uint32_t*)tr->next.ptr, tr->ctx->sms, s));
+    } else if (n) {
         uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
         const uint32_t* order = nullptr;
         if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));

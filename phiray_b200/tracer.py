@@ -247,12 +247,15 @@ class Tracer:
     WALK_THREAD = 0
     WALK_FETCH = 1
     WALK_SORTED = 2
+    WALK_WIDE = 3
 
     def set_walk(self, mode: int) -> None:
         """Ray-buffer walks: Tracer.WALK_THREAD (a thread per ray),
-        Tracer.WALK_FETCH (persistent warps refilling idle lanes) or
+        Tracer.WALK_FETCH (persistent warps refilling idle lanes),
         Tracer.WALK_SORTED (the same over rays sorted by direction octant and
-        origin); same hits."""
+        origin), all with the same hits; or Tracer.WALK_WIDE (persistent
+        warps over a 4-wide tree collapsed from the binary one: the same
+        closest t, the face at a tie may differ)."""
         N.check(N.lib().phx_tracer_set_walk(self.handle, mode))
 
     def set_samples(self, n: int) -> None:

@@ -158,6 +158,64 @@ def test_ray_buffer_walks(gpu, orc, walk):
             assert np.array_equal(got[hit], want[hit])
 
 
+def _same_closest_hits(got, want):
+    """The closest t of every ray equal bit for bit; the face equal wherever
+    no other face sits at that t (a tie is the only freedom the wide walk
+    has), so at most a few in 10,000 rays may name another face."""
+    gt, wt = got[:, 0], want[:, 0]
+    assert np.array_equal(gt.view(np.uint32), wt.view(np.uint32))
+    diff = got.view(np.uint32)[:, 1] != want.view(np.uint32)[:, 1]
+    assert diff.sum() <= max(2, len(got) // 10000), diff.sum()
+
+
+@pytest.mark.parametrize("tree", [0, 1], ids=["lbvh", "sah"])
+def test_wide_walk(gpu, orc, tree):
+    """PHX_WALK_WIDE over the 4-wide tree collapsed from either binary tree:
+    closest hits == the oracle's binary walk (ties aside), any-hit rays hit
+    or miss as the oracle's do; after a repose the wide tree follows the
+    refitted binary one."""
+    import torch
+
+    s = SCENES["c2_small"]()
+    rng = np.random.default_rng(9)
+    n = 20000
+    o = rng.uniform(-1.0, 1.0, (n, 3)).astype(np.float32)
+    d = rng.standard_normal((n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3], rays[:, 4:7] = o, 3.0e38, d
+    rays[::5, 3] = 0.3
+    tr = px.Tracer.of(gpu, s)
+    tr.set_tree(tree)
+    tr.set_walk(px.Tracer.WALK_WIDE)
+    dr = torch.tensor(rays, device="cuda")
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    T = oracle_lib.TraceOracle(orc, s, sah=bool(tree))
+    for any_hit in (False, True):
+        tr.trace_rays(dr, n, hits, any_hit)
+        gpu.wait()
+        got, want = hits.cpu().numpy(), T.trace_rays(rays, any_hit)
+        if any_hit:
+            assert np.array_equal(got.view(np.uint32)[:, 1] != 0xFFFFFFFF, want.view(np.uint32)[:, 1] != 0xFFFFFFFF)
+        else:
+            _same_closest_hits(got, want)
+    c = tr.trace_rays_stats(dr, n, hits)
+    tr.set_walk(px.Tracer.WALK_FETCH)
+    c2 = tr.trace_rays_stats(dr, n, hits)
+    assert c[0] == c2[0] == n and c[1] < c2[1]  # fewer (wider) steps
+    moved = s.verts.copy()
+    moved[:, 1] *= np.float32(1.07)
+    tr.repose_device(torch.tensor(moved, device="cuda"), rebuild=False)
+    tr.trace_rays(dr, n, hits)
+    gpu.wait()
+    binary = hits.cpu().numpy().copy()
+    tr.set_walk(px.Tracer.WALK_WIDE)
+    tr.trace_rays(dr, n, hits)
+    gpu.wait()
+    _same_closest_hits(hits.cpu().numpy(), binary)
+    tr.close()
+
+
 def test_autotune_keeps_the_image(gpu, orc):
     s = SCENES["c2_small"]()
     cam = cam_of(s, s.width, s.height)
