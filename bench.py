@@ -498,7 +498,8 @@ def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
     if not os.path.exists(WEIGHTS):
         return {"unavailable": f"no trained weights at {os.path.relpath(WEIGHTS, ROOT)}"}
     W, H, n = s.width, s.height, s.width * s.height
-    learned_spp = [1, 2, 4, 8, 16, 20, 24, 28, 32, 48, 64]
+    learned_spp = [1, 2, 4, 8, 16, 20, 24, 26, 28, 30, 32, 36, 40, 48, 64]
+    flip_counts = [1, 2, 4]  # the learned result averaged over this many mirrored network passes
     plain_spp = [64, 128, 256, 512]
     tr = px.Tracer.of(gpu, s)
     tr.set_kernel(kernel)
@@ -536,19 +537,30 @@ def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
             kernels.denoise(gpu, buf, W, H)
             rel_plain.setdefault(spp, []).append(T.relmse(T.radiance(buf.read(np.uint32), W, H), ref))
             if spp in learned_spp:
-                buf.write(noisy)
                 if half is not None:
                     hbuf.write(half)
-                kept.setdefault(spp, []).append(
-                    net.denoise_px(buf, W, H, half=hbuf if half is not None else None, tile=TILE,
-                                   threshold=THRESHOLD, count=True) / tiles)
-                rel_learned.setdefault(spp, []).append(T.relmse(T.radiance(buf.read(np.uint32), W, H), ref))
+                for fl in flip_counts:
+                    net.set_flips(fl)
+                    buf.write(noisy)
+                    kept.setdefault((fl, spp), []).append(
+                        net.denoise_px(buf, W, H, half=hbuf if half is not None else None, tile=TILE,
+                                       threshold=THRESHOLD, count=True) / tiles)
+                    rel_learned.setdefault((fl, spp), []).append(
+                        T.relmse(T.radiance(buf.read(np.uint32), W, H), ref))
     buf.free()
-    spread = {"plain": {str(k): [round(x, 6) for x in v] for k, v in rel_plain.items() if k == args.plain_spp},
-              "learned": {str(k): [round(x, 6) for x in v] for k, v in rel_learned.items() if k in (24, 32, 48)}}
+    rel_plain_frames = rel_plain
     rel_plain = {k: float(np.mean(v)) for k, v in rel_plain.items()}
-    rel_learned = {k: float(np.mean(v)) for k, v in rel_learned.items()}
-    kept = {k: float(np.mean(v)) for k, v in kept.items()}
+    target = rel_plain[args.plain_spp]
+    # the flip count with the fewest samples to reach the plain figure (ties: fewer passes)
+    best_fl = min(flip_counts, key=lambda fl: (next((p for p in learned_spp
+                                                      if np.mean(rel_learned[(fl, p)]) <= target), 1 << 30), fl))
+    spread = {"plain": {str(k): [round(x, 6) for x in v] for k, v in rel_plain_frames.items() if k == args.plain_spp},
+              "learned": {str(k): [round(x, 6) for x in rel_learned[(best_fl, k)]] for k in (24, 28, 32, 48)}}
+    by_flips = {str(fl): {str(p): round(float(np.mean(rel_learned[(fl, p)])), 6) for p in learned_spp}
+                for fl in flip_counts}
+    kept = {p: float(np.mean(kept[(best_fl, p)])) for p in learned_spp}
+    rel_learned = {p: float(np.mean(rel_learned[(best_fl, p)])) for p in learned_spp}
+    net.set_flips(best_fl)
 
     def frame_ms(spp, learned, reps):
         def once():
@@ -575,7 +587,6 @@ def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
         return a.elapsed_time(b) / reps
 
     t_plain = frame_ms(args.plain_spp, False, 2)
-    target = rel_plain[args.plain_spp]
     match = next((p for p in learned_spp if rel_learned[p] <= target), None)
     out = {
         "reference_spp": args.ref_spp,
@@ -585,6 +596,8 @@ def equal_relmse(args, gpu, s, cam, stream, kernel: int = 0) -> dict:
                   "frames_per_s": round(1000.0 / t_plain, 3)},
         "relmse_plain_denoise": {str(k): round(v, 6) for k, v in rel_plain.items()},
         "relmse_learned": {str(k): round(v, 6) for k, v in rel_learned.items()},
+        "flips": best_fl,
+        "relmse_learned_by_flips": by_flips,
         "fallback_tile_share": {str(k): round(v, 4) for k, v in kept.items()},
         "threshold": THRESHOLD,
     }
@@ -796,11 +809,12 @@ def main() -> None:
     barrier()
     for k in e2e_parts:
         e2e_parts[k] = 0.0
+    e2e_steps = max(3, args.steps)
     t0 = time.perf_counter()
-    for _ in range(max(2, args.steps // 2)):
+    for _ in range(e2e_steps):
         e2e_step()
     barrier()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(2, args.steps // 2), f"cuda:{local}")
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, f"cuda:{local}")
     e2e = whole_job_rate(rays_per_frame, world, e2e_s * 1e3) / 1e6
 
     denoised = None if args.no_denoised else equal_relmse(args, gpu, s, cam, stream, chosen)
@@ -851,7 +865,8 @@ def main() -> None:
                          "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "phases_ms": {k: round(v / max(2, args.steps // 2), 1) for k, v in e2e_parts.items()}},
+                    "steps": e2e_steps,
+                    "phases_ms": {k: round(v / e2e_steps, 1) for k, v in e2e_parts.items()}},
             "denoised": denoised,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),

@@ -747,6 +747,12 @@ int32_t phx_unet_logits(phx_unet net, float** logits);
 /* Whether phx_unet_denoise_px's predicted kernels filter the irradiance
  * after phx_nn_firefly (on) or as it is (0, the default). */
 int32_t phx_unet_set_clamp(phx_unet net, int32_t on);
+/* Test-time flip average of phx_unet_denoise_px / phx_tracer_denoise_learned:
+ * the filtered image and its error estimate are the mean over `images`
+ * network passes, the frame (1, the default), also mirrored in x (2), and
+ * mirrored in y and in both (4); each mirrored pass's kernels filter its
+ * own mirrored irradiance. Costs one network pass an image. */
+int32_t phx_unet_set_flips(phx_unet net, int32_t images);
 /* Denoises a traced px image in place (`half`: nullable snapshot, as
  * phx_nn_features): features, network (its kernels filtering the
  * firefly-clamped irradiance if phx_unet_set_clamp turned that on), the a-trous

@@ -131,6 +131,7 @@ SIGNATURES: dict[str, tuple] = {
     "phx_unet_logits": (i32, [vp, C.POINTER(vp)]),
     "phx_unet_grad_arena": (i32, [vp, C.POINTER(vp), C.POINTER(C.c_uint64)]),
     "phx_unet_set_clamp": (i32, [vp, i32]),
+    "phx_unet_set_flips": (i32, [vp, i32]),
     "phx_unet_denoise_px": (i32, [vp, vp, vp, u32, u32, f32p, i32, C.c_float, i32, C.POINTER(u32)]),
     "phx_tracer_snapshot": (i32, [vp, vp]),
     "phx_tracer_denoise_learned": (i32, [vp, vp, vp, i32, C.c_float, i32, C.POINTER(u32)]),

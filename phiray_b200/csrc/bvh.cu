@@ -367,9 +367,40 @@ __global__ void __launch_bounds__(256) k_karras(const uint32_t* __restrict__ cod
     }
 }
 
+// ---- depth of every inner node by pointer jumping ----
+
+// anc[i] starts as i's parent (the root its own), dist[i] as 1 (the root 0);
+// each round doubles the hops: dist[i] += dist[anc[i]], anc[i] = anc[anc[i]].
+// After DEPTH_ROUNDS rounds a node within 2^DEPTH_ROUNDS = STACK hops of the
+// root has anc 0 and dist its depth; any deeper node has anc != 0.
+constexpr int DEPTH_ROUNDS = 5;
+static_assert((1u << DEPTH_ROUNDS) == STACK, "the jumps cover the stack's depth");
+
+__global__ void __launch_bounds__(256) k_depth_init(const uint32_t* __restrict__ parent, uint32_t ninner,
+                                                    uint32_t* __restrict__ anc, uint32_t* __restrict__ dist,
+                                                    Gate gate) {
+    if (gate.off()) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninner) return;
+    anc[i] = i == 0 ? 0u : __ldg(parent + i);
+    dist[i] = i == 0 ? 0u : 1u;
+}
+
+__global__ void __launch_bounds__(256) k_depth_jump(const uint32_t* __restrict__ anc, const uint32_t* __restrict__ dist,
+                                                    uint32_t ninner, uint32_t* __restrict__ anc_out,
+                                                    uint32_t* __restrict__ dist_out, Gate gate) {
+    if (gate.off()) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ninner) return;
+    const uint32_t a = __ldg(anc + i);
+    dist_out[i] = __ldg(dist + i) + __ldg(dist + a);
+    anc_out[i] = __ldg(anc + a);
+}
+
 // ---- pack + depth (Bvh::assemble without the DFS) ----
 
 __global__ void __launch_bounds__(256) k_pack(const uint4* __restrict__ links, const uint32_t* __restrict__ parent,
+                                              const uint32_t* __restrict__ anc, const uint32_t* __restrict__ dist,
                                               uint32_t n, uint32_t leaf, float4* __restrict__ nodes,
                                               uint32_t* __restrict__ starts, uint32_t* __restrict__ nstarts,
                                               uint32_t* __restrict__ depth_out, Gate gate) {
@@ -398,13 +429,9 @@ __global__ void __launch_bounds__(256) k_pack(const uint4* __restrict__ links, c
             const uint32_t p = __ldg(parent + i);
             const uint4 Lp = __ldg(links + p);
             if (Lp.w - Lp.z >= leaf) {
-                // depth(p): climb to the root. Past 31 hops p is cand and
-                // i unreachable, so the climb stops there.
-                uint32_t dp = 0, q = p;
-                while (q != 0 && dp < STACK) {
-                    q = __ldg(parent + q);
-                    dp++;
-                }
+                // depth(p), or STACK for any depth past it (p is then cand
+                // and i unreachable)
+                const uint32_t dp = __ldg(anc + p) == 0 ? __ldg(dist + p) : STACK;
                 if (dp + 1 < STACK) {
                     reach = true;
                     dep = dp + 1;
@@ -425,17 +452,30 @@ __global__ void __launch_bounds__(256) k_pack(const uint4* __restrict__ links, c
         nodes[2 * (size_t)i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(lo_i));
         nodes[2 * (size_t)i + 1] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(hi_i));
     }
+    // One atomic a block for the depth and one for the start list (a warp's
+    // atomics on the two words serialised the kernel).
+    __shared__ uint32_t s_max[8], s_cnt[8], s_base;
     const uint32_t dmax = __reduce_max_sync(0xffffffffu, reach ? dep : 0u);
-    const int lane = threadIdx.x & 31;
-    if (lane == 0 && dmax) atomicMax(depth_out, dmax);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t m = __ballot_sync(0xffffffffu, start);
-    if (m) {
-        const int leader = __ffs(m) - 1;
-        uint32_t b = 0;
-        if (lane == leader) b = atomicAdd(nstarts, __popc(m));
-        b = __shfl_sync(0xffffffffu, b, leader);
-        if (start) starts[b + __popc(m & ((1u << lane) - 1u))] = i;
+    if (lane == 0) {
+        s_max[warp] = dmax;
+        s_cnt[warp] = __popc(m);
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t bm = 0, total = 0;
+        for (int k = 0; k < 8; k++) {
+            bm = bm > s_max[k] ? bm : s_max[k];
+            const uint32_t c = s_cnt[k];
+            s_cnt[k] = total;
+            total += c;
+        }
+        if (bm) atomicMax(depth_out, bm);
+        s_base = total ? atomicAdd(nstarts, total) : 0u;
+    }
+    __syncthreads();
+    if (start) starts[s_base + s_cnt[warp] + __popc(m & ((1u << lane) - 1u))] = i;
 }
 
 // ---- refit: atomic bottom-up (Bvh::refit's bounds, Warp's refit pattern) ----
@@ -648,8 +688,25 @@ int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate) 
     k_karras<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>((const uint32_t*)w.sorted.ptr, n, (uint4*)w.links.ptr,
                                                         (uint32_t*)w.parent.ptr, gate);
     PHX_TRY(zero(c, w.counters.ptr, (size_t)n * 4, gate));
+    // Inner nodes' depths (the unsorted codes and the sort's ping-pong
+    // arrays are free now; the depth rounds end in alt_keys / alt_vals).
+    uint32_t* anc_a = (uint32_t*)w.codes.ptr;
+    uint32_t* dist_a = (uint32_t*)w.starts.ptr;
+    uint32_t* anc_b = (uint32_t*)w.alt_keys.ptr;
+    uint32_t* dist_b = (uint32_t*)w.alt_vals.ptr;
+    const uint32_t ninner = n - 1;
+    if (ninner) {
+        k_depth_init<<<grid_for(ninner, 256, 1u << 30), 256, 0, s>>>((const uint32_t*)w.parent.ptr, ninner, anc_a,
+                                                                    dist_a, gate);
+        for (int r = 0; r < DEPTH_ROUNDS; r++) {
+            k_depth_jump<<<grid_for(ninner, 256, 1u << 30), 256, 0, s>>>(anc_a, dist_a, ninner, anc_b, dist_b, gate);
+            std::swap(anc_a, anc_b);
+            std::swap(dist_a, dist_b);
+        }
+    }
+    static_assert(DEPTH_ROUNDS % 2 == 1, "the last round writes alt_keys / alt_vals, not starts");
     k_pack<<<grid_for(2ull * n - 1, 256, 1u << 30), 256, 0, s>>>((const uint4*)w.links.ptr,
-                                                                (const uint32_t*)w.parent.ptr, n, leaf,
+                                                                (const uint32_t*)w.parent.ptr, anc_a, dist_a, n, leaf,
                                                                 (float4*)w.nodes.ptr, (uint32_t*)w.starts.ptr,
                                                                 w.nstarts(), w.depth(), gate);
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>(prims, (const uint32_t*)w.order.ptr,

@@ -9,10 +9,11 @@
 // down) give every node the index the reference's work stack hands out,
 // and a last bottom-up pass writes the nodes with their bounds.
 //
-// Small nodes are one thread each, running the per-node code of
-// sah_core.cuh. Nodes of BIG slots or more — the top levels, where a
-// thread per node would leave the GPU idle — are cut over blocks of CHUNK
-// slots: the box of centres and the bins are min/max and count reductions
+// Nodes under MID slots are one thread each, running the per-node code of
+// sah_core.cuh; nodes of MID to BIG slots a warp each (bins by shared-memory
+// atomics, the swap loop over shared memory). Nodes of BIG slots or more —
+// the top levels, where a node a thread or warp would leave the GPU idle —
+// are cut over blocks of CHUNK slots: the box of centres and the bins are min/max and count reductions
 // (exact in any order) merged with atomics; one thread a node then makes
 // the reference's decision from those bins (sah_core.cuh decide); and the
 // reference's in-place swap partition is reproduced in parallel. That loop
@@ -34,12 +35,6 @@ namespace {
 
 using sah::TNode;
 
-__device__ uint32_t atomic_add(uint32_t* p, uint32_t v) { return atomicAdd(p, v); }
-
-struct DeviceAdd {
-    __device__ uint32_t operator()(uint32_t* p, uint32_t v) const { return atomic_add(p, v); }
-};
-
 __global__ void k_sah_init(const float* __restrict__ prims, uint32_t n, float* __restrict__ centres,
                            uint32_t* __restrict__ order) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -47,14 +42,6 @@ __global__ void k_sah_init(const float* __restrict__ prims, uint32_t n, float* _
     // Aabb::center (node.rs:90-92)
     for (int k = 0; k < 3; k++) centres[3 * (uint64_t)i + k] = 0.5f * (prims[8 * (uint64_t)i + k] + prims[8 * (uint64_t)i + 4 + k]);
     order[i] = i;
-}
-
-__global__ void k_sah_level(const uint32_t* __restrict__ list, uint32_t count, TNode* tn, const float* __restrict__ prims,
-                            const float* __restrict__ centres, uint32_t* order, uint32_t leaf, uint32_t* tcount,
-                            uint32_t* next, uint32_t* next_count) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    sah::process(list[k], tn, prims, centres, order, leaf, tcount, next, next_count, DeviceAdd{});
 }
 
 __global__ void k_sah_count(const uint32_t* __restrict__ list, uint32_t count, const TNode* __restrict__ tn,
@@ -136,16 +123,170 @@ __device__ __forceinline__ uint32_t block_sum_exclusive(uint32_t v, uint32_t* to
     return before;
 }
 
+// ---- nodes of MID to BIG slots: a warp a node ----
+
+constexpr uint32_t MID = 128;
+
+constexpr uint32_t NODE_WARPS = 4;  // warps (nodes) a block
+// A warp's shared memory: bin counts, bin boxes (ordered words), the node's
+// slots and their left flags.
+constexpr uint32_t WARP_WORDS = HBINS + 6 * HBINS + BIG + BIG / 4;
+
+// sah_core.cuh process for one node, by a warp: the box of centres by warp
+// reductions, the bins by shared-memory atomics (min, max and counts are
+// exact in any order), the reference's decision by lane 0 (decide), and the
+// reference's swap loop by lane 0 over the slots staged in shared memory
+// (the flag of the slot at position j when the loop reaches j is that of the
+// slot first there: the loop only swaps positions at or before j).
+__global__ void __launch_bounds__(NODE_WARPS * 32, 4) k_sah_warp(const uint32_t* __restrict__ list, uint32_t count,
+                                                              TNode* tn, const float* __restrict__ prims,
+                                                              const float* __restrict__ centres, uint32_t* order,
+                                                              uint32_t leaf, uint32_t* tcount, uint32_t* next,
+                                                              uint32_t* next_count) {
+    extern __shared__ uint32_t s_words[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t k = blockIdx.x * NODE_WARPS + warp;
+    if (k >= count) return;  // (whole warps)
+    uint32_t* s_count = s_words + warp * WARP_WORDS;
+    uint32_t* s_box = s_count + HBINS;
+    uint32_t* s_slot = s_box + 6 * HBINS;
+    uint8_t* s_flag = (uint8_t*)(s_slot + BIG);
+    const uint32_t t = list[k];
+    TNode nd = tn[t];
+    const uint32_t n = nd.end - nd.start;
+    uint32_t m = sah::NONE;
+    if (nd.depth + 1 < sah::MAX_DEPTH && n > 1 && n <= BIG) {
+        const uint32_t* slots = order + nd.start;
+        float lo[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
+        float hi[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+        for (uint32_t j = lane; j < n; j += 32) {
+            const uint32_t i = slots[j];
+            s_slot[j] = i;
+            const float* c = centres + 3 * (uint64_t)i;
+            for (int e = 0; e < 3; e++) {
+                lo[e] = fminf(lo[e], c[e]);
+                hi[e] = fmaxf(hi[e], c[e]);
+            }
+        }
+        for (int e = 0; e < 3; e++)
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[e] = fminf(lo[e], __shfl_xor_sync(0xffffffffu, lo[e], o));
+                hi[e] = fmaxf(hi[e], __shfl_xor_sync(0xffffffffu, hi[e], o));
+            }
+        sah::Box cbox;
+        for (int e = 0; e < 3; e++) {
+            cbox.lo[e] = lo[e];
+            cbox.hi[e] = hi[e];
+        }
+        float glo[3], scale[3];
+        if (!sah::grid_of(cbox, glo, scale)) {
+            m = n > leaf ? n / 2 : sah::NONE;
+        } else {
+            for (uint32_t i = lane; i < HBINS; i += 32) s_count[i] = 0;
+            for (uint32_t i = lane; i < 6 * HBINS; i += 32)
+                s_box[i] = ord((i % 6) < 3 ? 3.402823466e38f : -3.402823466e38f);
+            __syncwarp();
+            for (uint32_t j = lane; j < n; j += 32) {
+                const uint32_t i = s_slot[j];
+                const float* p = prims + 8 * (uint64_t)i;
+                for (int e = 0; e < 3; e++) {
+                    const uint32_t at = e * sah::BINS + sah::bin_of(centres + 3 * (uint64_t)i, glo, scale, e);
+                    atomicAdd(&s_count[at], 1u);
+                    for (int f = 0; f < 3; f++) {  // a NaN bound loses, as in f32::min / max
+                        if (p[f] == p[f]) atomicMin(&s_box[6 * at + f], ord(p[f]));
+                        if (p[4 + f] == p[4 + f]) atomicMax(&s_box[6 * at + 3 + f], ord(p[4 + f]));
+                    }
+                }
+            }
+            __syncwarp();
+            uint32_t cut = 0, axis = 0, at = 0;
+            if (lane == 0) {
+                uint32_t bcount[3][sah::BINS];
+                sah::Box bbox[3][sah::BINS];
+                for (int e = 0; e < 3; e++)
+                    for (uint32_t a = 0; a < sah::BINS; a++) {
+                        const uint32_t i = e * sah::BINS + a;
+                        bcount[e][a] = s_count[i];
+                        for (int f = 0; f < 3; f++) {
+                            bbox[e][a].lo[f] = unord(s_box[6 * i + f]);
+                            bbox[e][a].hi[f] = unord(s_box[6 * i + 3 + f]);
+                        }
+                    }
+                const sah::Decision d = sah::decide(bcount, bbox, scale, n, leaf);
+                cut = d.cut;
+                axis = d.axis;
+                at = d.at;
+            }
+            cut = __shfl_sync(0xffffffffu, cut, 0);
+            axis = __shfl_sync(0xffffffffu, axis, 0);
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (cut == sah::CUT_HALF) m = n / 2;
+            if (cut == sah::CUT_PLANE) {
+                for (uint32_t j = lane; j < n; j += 32)
+                    s_flag[j] = sah::bin_of(centres + 3 * (uint64_t)s_slot[j], glo, scale, (int)axis) <= at ? 1 : 0;
+                __syncwarp();
+                if (lane == 0) {
+                    uint32_t q = 0;
+                    for (uint32_t j = 0; j < n; j++) {
+                        if (s_flag[j]) {
+                            const uint32_t x = s_slot[j];
+                            s_slot[j] = s_slot[q];
+                            s_slot[q] = x;
+                            q++;
+                        }
+                    }
+                    m = (q == 0 || q == n) ? n / 2 : q;
+                }
+                m = __shfl_sync(0xffffffffu, m, 0);
+                __syncwarp();
+                for (uint32_t j = lane; j < n; j += 32) order[nd.start + j] = s_slot[j];
+            }
+        }
+    }
+    if (lane != 0) return;
+    if (m == sah::NONE) {
+        nd.left = nd.right = sah::NONE;
+    } else {
+        const uint32_t c = atomicAdd(tcount, 2u);
+        tn[c] = TNode{nd.start, nd.start + m, nd.depth + 1, sah::NONE, sah::NONE};
+        tn[c + 1] = TNode{nd.start + m, nd.end, nd.depth + 1, sah::NONE, sah::NONE};
+        nd.left = c;
+        nd.right = c + 1;
+        const uint32_t p = atomicAdd(next_count, 2u);
+        next[p] = c;
+        next[p + 1] = c + 1;
+    }
+    tn[t] = nd;
+}
+
 // The level's open nodes, split into the big ones (BIG slots or more, not
 // at the depth cap) and the rest.
+// (counts: small, big, mid.)
 __global__ void k_sah_classify(const uint32_t* __restrict__ list, uint32_t count, const TNode* __restrict__ tn,
-                               uint32_t* small, uint32_t* big, uint32_t* counts) {
+                               uint32_t* small, uint32_t* big, uint32_t* mid, uint32_t* counts) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const uint32_t t = list[k];
     const TNode nd = tn[t];
-    if (nd.end - nd.start >= BIG && nd.depth + 1 < sah::MAX_DEPTH) big[atomicAdd(counts + 1, 1u)] = t;
+    const uint32_t n = nd.end - nd.start;
+    const bool open = nd.depth + 1 < sah::MAX_DEPTH;
+    if (open && n >= BIG) big[atomicAdd(counts + 1, 1u)] = t;
+    else if (open && n >= MID) mid[atomicAdd(counts + 2, 1u)] = t;
     else small[atomicAdd(counts, 1u)] = t;
+}
+
+// Nodes under MID slots (and nodes at the depth cap): a thread a node,
+// sah_core.cuh process as it is.
+struct DeviceAdd {
+    __device__ uint32_t operator()(uint32_t* p, uint32_t v) const { return atomicAdd(p, v); }
+};
+
+__global__ void k_sah_thread(const uint32_t* __restrict__ list, uint32_t count, TNode* tn,
+                             const float* __restrict__ prims, const float* __restrict__ centres, uint32_t* order,
+                             uint32_t leaf, uint32_t* tcount, uint32_t* next, uint32_t* next_count) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    sah::process(list[k], tn, prims, centres, order, leaf, tcount, next, next_count, DeviceAdd{});
 }
 
 __global__ void k_big_setup(const uint32_t* __restrict__ big, uint32_t nb, const TNode* __restrict__ tn,
@@ -345,20 +486,17 @@ __global__ void __launch_bounds__(CHUNK_THREADS) k_part_flags(const Chunk* __res
     if ((threadIdx.x & 31u) == 0 && first != 0xFFFFFFFFu) atomicMin(&B.first_right, first);
 }
 
-// Partition, step 2 (one thread): each chunk's left count before it within
-// its node (the table lists a node's chunks in order).
+// Partition, step 2 (a thread a chunk): the chunk's left count before it
+// within its node (the table lists a node's chunks in order, so they are the
+// chunks before it with the same node).
 __global__ void k_part_chunks(const Chunk* __restrict__ chunks, uint32_t nchunks, const uint32_t* __restrict__ lefts,
                               uint32_t* offs) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    uint32_t run = 0, node = 0xFFFFFFFFu;
-    for (uint32_t c = 0; c < nchunks; c++) {
-        if (chunks[c].b != node) {
-            node = chunks[c].b;
-            run = 0;
-        }
-        offs[c] = run;
-        run += lefts[c];
-    }
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    const uint32_t node = chunks[c].b;
+    uint32_t run = 0;
+    for (uint32_t k = c; k-- > 0 && chunks[k].b == node;) run += lefts[k];
+    offs[c] = run;
 }
 
 // Partition, step 3: left slots to their places; from the first right slot
@@ -474,12 +612,14 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
     // Big-node work arrays (sized for the widest level: at most n / BIG big
     // nodes, n / CHUNK + n / BIG chunks).
     const uint32_t max_big = n / BIG + 1, max_chunks = n / CHUNK + max_big + 1;
-    DevMem small_list, big_list, lcounts, bnodes, spans, chunks, rank_w, lefts, offs, out_w, ptr_a, ptr_b, val_w;
+    DevMem small_list, mid_list, big_list, lcounts, bnodes, spans, chunks, rank_w, lefts, offs, out_w, ptr_a, ptr_b,
+        val_w;
+    PHX_TRY(small_list.reserve((size_t)cap * 4));
+    PHX_TRY(mid_list.reserve((size_t)(n / MID + 1) * 4));
+    PHX_TRY(lcounts.reserve(12));
     if (n >= BIG) {
         PHX_TRY(spans.reserve((size_t)max_big * 8));
-        PHX_TRY(small_list.reserve((size_t)cap * 4));
         PHX_TRY(big_list.reserve((size_t)max_big * 4));
-        PHX_TRY(lcounts.reserve(8));
         PHX_TRY(bnodes.reserve((size_t)max_big * sizeof(BigNode)));
         PHX_TRY(chunks.reserve((size_t)max_chunks * sizeof(Chunk)));
         PHX_TRY(rank_w.reserve((size_t)n * 4));
@@ -496,18 +636,19 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
     for (uint32_t lv = 0; lv < sah::MAX_DEPTH; lv++) {
         const uint32_t next = off[lv] + len[lv];
         PHX_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, s));
-        const uint32_t* level = L + off[lv];
-        uint32_t nsmall = len[lv];
-        if (n >= BIG) {
-            PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 8, s));
-            k_sah_classify<<<blocks_of(len[lv], 256), 256, 0, s>>>(level, len[lv], T, (uint32_t*)small_list.ptr,
-                                                                   (uint32_t*)big_list.ptr, (uint32_t*)lcounts.ptr);
-            uint32_t lc[2] = {0, 0};
-            PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 8, cudaMemcpyDeviceToHost, s));
+        const uint32_t* level = (const uint32_t*)small_list.ptr;
+        uint32_t nsmall = 0, nmid = 0;
+        {
+            PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 12, s));
+            k_sah_classify<<<blocks_of(len[lv], 256), 256, 0, s>>>(L + off[lv], len[lv], T, (uint32_t*)small_list.ptr,
+                                                                   (uint32_t*)big_list.ptr, (uint32_t*)mid_list.ptr,
+                                                                   (uint32_t*)lcounts.ptr);
+            uint32_t lc[3] = {0, 0, 0};
+            PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 12, cudaMemcpyDeviceToHost, s));
             PHX_TRY(wait_stream(s, 0));
             nsmall = lc[0];
+            nmid = lc[2];
             const uint32_t nb = lc[1];
-            level = (const uint32_t*)small_list.ptr;
             if (nb) {
                 BigNode* BN = (BigNode*)bnodes.ptr;
                 k_big_setup<<<nb, 256, 0, s>>>((const uint32_t*)big_list.ptr, nb, T, BN, (uint2*)spans.ptr);
@@ -532,7 +673,8 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
                 k_big_choose<<<blocks_of(nb, 64), 64, 0, s>>>(BN, nb, T, leaf, cnt, L + next, cnt + 1);
                 uint32_t* R = (uint32_t*)rank_w.ptr;
                 k_part_flags<<<nc, CHUNK_THREADS, 0, s>>>(CH, BN, Cc, order, R, (uint32_t*)lefts.ptr);
-                k_part_chunks<<<1, 32, 0, s>>>(CH, nc, (const uint32_t*)lefts.ptr, (uint32_t*)offs.ptr);
+                k_part_chunks<<<blocks_of(nc, 128), 128, 0, s>>>(CH, nc, (const uint32_t*)lefts.ptr,
+                                                                 (uint32_t*)offs.ptr);
                 uint32_t* pa = (uint32_t*)ptr_a.ptr;
                 uint32_t* pb = (uint32_t*)ptr_b.ptr;
                 k_part_scatter<<<nc, CHUNK_THREADS, 0, s>>>(CH, BN, Cc, order, R, (const uint32_t*)offs.ptr,
@@ -549,9 +691,13 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
                 PHX_CUDA(cudaGetLastError());
             }
         }
+        if (nmid)
+            k_sah_warp<<<blocks_of(nmid, NODE_WARPS), NODE_WARPS * 32, NODE_WARPS * WARP_WORDS * 4, s>>>(
+                (const uint32_t*)mid_list.ptr, nmid, T, P, (const float*)centres.ptr, order, leaf, cnt, L + next,
+                cnt + 1);
         if (nsmall)
-            k_sah_level<<<blocks_of(nsmall, 64), 64, 0, s>>>(level, nsmall, T, P, (const float*)centres.ptr, order,
-                                                             leaf, cnt, L + next, cnt + 1);
+            k_sah_thread<<<blocks_of(nsmall, 64), 64, 0, s>>>(level, nsmall, T, P, (const float*)centres.ptr, order,
+                                                              leaf, cnt, L + next, cnt + 1);
         PHX_CUDA(cudaGetLastError());
         uint32_t opened = 0;
         PHX_CUDA(cudaMemcpyAsync(&opened, cnt + 1, 4, cudaMemcpyDeviceToHost, s));

@@ -91,7 +91,9 @@ struct phx_unet_s {
     phx::DevMem dA[5], dcat[4], dpool[5], dB4, dDa[4], dDb[4], dlogits;
     // tracer-facing scratch
     phx::DevMem feat, irr, irr_clamped, alb, out, err, tile_err, fallback;
+    phx::DevMem ffeat, firr, falb, fout, ferr;  // the mirrored inputs and outputs of the flip average
     bool clamp = false;  // firefly clamp on the irradiance the predicted kernels filter
+    int flips = 1;       // images the result is averaged over: 1, 2 (+ mirrored in x) or 4 (+ in y, both)
     int step = 0;
     float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
 };
@@ -332,6 +334,47 @@ int32_t check_shape(const Shape& s) {
     return PHX_OK;
 }
 
+// Pixel (x, y) of the image mirrored by `flip` (bit 0: in x, bit 1: in y);
+// padding outside w x h stays where it is.
+__device__ __forceinline__ size_t mirrored(int x, int y, int w, int h, int Wp, int flip) {
+    if (x < w && y < h) {
+        if (flip & 1) x = w - 1 - x;
+        if (flip & 2) y = h - 1 - y;
+    }
+    return (size_t)y * Wp + x;
+}
+
+// The network's inputs of the mirrored image: features (FEAT bf16 a pixel,
+// moved as 16-bit words), irradiance and albedo (3 floats a pixel).
+__global__ void k_flip_inputs(const uint4* __restrict__ feat, const float* __restrict__ irr,
+                              const float* __restrict__ alb, uint4* __restrict__ ffeat, float* __restrict__ firr,
+                              float* __restrict__ falb, int w, int h, int Hp, int Wp, int flip) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Hp * Wp) return;
+    const int x = i % Wp, y = i / Wp;
+    const size_t j = mirrored(x, y, w, h, Wp, flip);
+    static_assert(FEAT * 2 == 2 * sizeof(uint4), "a pixel's features are two uint4");
+    ffeat[2 * (size_t)i] = feat[2 * j];
+    ffeat[2 * (size_t)i + 1] = feat[2 * j + 1];
+    for (int c = 0; c < 3; c++) {
+        firr[3 * (size_t)i + c] = irr[3 * j + c];
+        falb[3 * (size_t)i + c] = alb[3 * j + c];
+    }
+}
+
+// Adds the mirrored image's filtered result and error estimate back in the
+// frame's own pixel order; `scale` on the last image makes the sum a mean.
+__global__ void k_flip_add(float* __restrict__ out, float* __restrict__ err, const float* __restrict__ fout,
+                           const float* __restrict__ ferr, int w, int h, int Wp, int flip, float scale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w * h) return;
+    const int x = i % w, y = i / w;
+    const size_t p = (size_t)y * Wp + x;
+    const size_t j = mirrored(x, y, w, h, Wp, flip);
+    for (int c = 0; c < 3; c++) out[3 * p + c] = (out[3 * p + c] + fout[3 * j + c]) * scale;
+    err[p] = (err[p] + ferr[j]) * scale;
+}
+
 }  // namespace
 }  // namespace phx
 
@@ -504,6 +547,13 @@ int32_t phx_unet_set_clamp(phx_unet net, int32_t on) {
     return PHX_OK;
 }
 
+int32_t phx_unet_set_flips(phx_unet net, int32_t images) {
+    if (!net) return fail(PHX_ERR_INVALID, "null network");
+    if (images != 1 && images != 2 && images != 4) return fail(PHX_ERR_INVALID, "unet: flips %d (1, 2 or 4)", images);
+    net->flips = images;
+    return PHX_OK;
+}
+
 int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint32_t w, uint32_t h,
                             const float view[4], int32_t tile, float threshold, int32_t keep, uint32_t* fallback) {
     if (!net || !px || !view) return fail(PHX_ERR_INVALID, "null argument");
@@ -534,6 +584,31 @@ int32_t phx_unet_denoise_px(phx_unet net, uint32_t* px, const float* half, uint3
     }
     PHX_TRY(phx_unet_forward(net, net->feat.ptr, filtered, (const float*)net->alb.ptr, 1, Hp, Wp, (int)h, (int)w,
                              (float*)net->out.ptr, (float*)net->err.ptr));
+    // The mean over mirrored images (the network trained on mirrored crops):
+    // each mirrored image's kernels filter its own mirrored irradiance.
+    for (int f = 1; f < net->flips; f++) {
+        if (f == 1) {
+            PHX_TRY(net->ffeat.reserve(P * FEAT * 2));
+            PHX_TRY(net->firr.reserve(P * 12));
+            PHX_TRY(net->falb.reserve(P * 12));
+            PHX_TRY(net->fout.reserve(P * 12));
+            PHX_TRY(net->ferr.reserve(P * 4));
+        }
+        cudaStream_t s = net->ctx->stream;
+        k_flip_inputs<<<(int)((P + 255) / 256), 256, 0, s>>>((const uint4*)net->feat.ptr, filtered,
+                                                              (const float*)net->alb.ptr, (uint4*)net->ffeat.ptr,
+                                                              (float*)net->firr.ptr, (float*)net->falb.ptr, (int)w,
+                                                              (int)h, Hp, Wp, f);
+        PHX_CUDA(cudaGetLastError());
+        PHX_TRY(phx_unet_forward(net, net->ffeat.ptr, (const float*)net->firr.ptr, (const float*)net->falb.ptr, 1, Hp,
+                                 Wp, (int)h, (int)w, (float*)net->fout.ptr, (float*)net->ferr.ptr));
+        const float scale = f + 1 == net->flips ? 1.0f / (float)net->flips : 1.0f;
+        k_flip_add<<<(int)(((size_t)w * h + 255) / 256), 256, 0, s>>>((float*)net->out.ptr, (float*)net->err.ptr,
+                                                                      (const float*)net->fout.ptr,
+                                                                      (const float*)net->ferr.ptr, (int)w, (int)h, Wp,
+                                                                      f, scale);
+        PHX_CUDA(cudaGetLastError());
+    }
     // The a-trous filter everywhere first; the learned result then replaces it
     // on every tile whose estimate is within the threshold.
     const float strength[4] = {64.0f, 8.0f, 40.0f, 7.0f};

@@ -144,6 +144,11 @@ class Unet:
         or the irradiance as it is (the default; phx_unet_set_clamp)."""
         N.check(N.lib().phx_unet_set_clamp(self.handle, 1 if on else 0))
 
+    def set_flips(self, images: int) -> None:
+        """Average the denoised result over 1, 2 (also mirrored in x) or 4
+        (also in y and both) network passes (phx_unet_set_flips)."""
+        N.check(N.lib().phx_unet_set_flips(self.handle, images))
+
     def denoise(self, tracer, half=None, tile: int = TILE, threshold: float = THRESHOLD, keep: bool = False,
                 count: bool = False) -> int | None:
         """Learned ``Tracer::denoise``; `half`: a snapshot (``Tracer.snapshot``)

@@ -719,3 +719,64 @@ def test_learned_denoise_with_the_clamp_filters_clamped_irradiance(gpu):
     assert np.allclose(rad[live], o[:h, :w][live], rtol=1e-6, atol=1e-7)
     net.close()
     tr.close()
+
+
+@pytest.mark.parametrize("flips", [2, 4])
+def test_learned_denoise_flip_average(gpu, flips):
+    """phx_unet_set_flips: the learned result is the mean of the network run
+    on the frame and on its mirror images (in x; for 4 also in y and both),
+    each mirrored result mirrored back (no tile falling back)."""
+    import torch
+
+    import phiray_b200 as px
+    from phiray_b200 import scenes
+    from phiray_b200.denoiser import Unet, padded
+
+    s = scenes.c1_plain(ntris=4096, width=72, height=40, spp=4)
+    cam = px.camera(s)
+    w, h = s.width, s.height
+    tr = px.Tracer.of(gpu, s)
+    net = Unet(gpu, seed=3)
+    net.set_flips(flips)
+    tr.trace(cam, w, h, 0, 4)
+    noisy = tr.image()
+    Hp, Wp = padded(h), padded(w)
+    feat = torch.empty((Hp, Wp, 16), dtype=torch.bfloat16, device="cuda")
+    irr = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    alb = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+    pptr, _ = tr.device_image()
+    torch.cuda.synchronize()
+    px.denoiser.features(gpu, pptr, w, h, Hp, Wp, feat, irr, alb)
+    _sync(gpu)
+
+    def mirror(t, f):
+        m = t.clone()
+        part = t[:h, :w]
+        if f & 1:
+            part = part.flip(1)
+        if f & 2:
+            part = part.flip(0)
+        m[:h, :w] = part
+        return m
+
+    acc = None
+    for f in range(flips):
+        out = torch.empty((Hp, Wp, 3), dtype=torch.float32, device="cuda")
+        err = torch.empty((Hp, Wp), dtype=torch.float32, device="cuda")
+        net.forward(mirror(feat, f), mirror(irr, f), mirror(alb, f), 1, Hp, Wp, h, w, out, err)
+        _sync(gpu)
+        back = mirror(out, f)
+        acc = back if acc is None else acc + back
+    want = (acc * (1.0 / flips)).cpu().numpy()
+    assert net.denoise(tr, tile=16, threshold=1e30, count=True) == 0
+    rad = tr.lit()
+    n = w * h
+    cnt = np.maximum(noisy[31 * n:32 * n].astype(np.float64), 1)
+    gone = noisy.view(np.float32)[33 * n:34 * n]
+    live = (1.0 - gone / cnt > 0.5 / cnt).reshape(h, w)
+    assert np.allclose(rad[live], want[:h, :w][live], rtol=1e-6, atol=1e-7)
+    net.set_flips(1)
+    with pytest.raises(px.PhxError):
+        net.set_flips(3)
+    net.close()
+    tr.close()
