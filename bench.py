@@ -647,7 +647,9 @@ def main() -> None:
     ap.add_argument("--no-denoised", action="store_true", help="skip the equal-relMSE comparison")
     ap.add_argument("--relmse-frames", type=int, default=5,
                     help="independent frames each equal-relMSE figure is averaged over")
-    ap.add_argument("--walk", type=int, default=0, help="ray walk of --phase rays: 0 a thread per ray, 1 persistent")
+    ap.add_argument("--walk", type=int, default=0,
+                    help="ray walk of --phase rays: 0 a thread per ray, 1 persistent, 2 sorted, 3 the 4-wide tree")
+    ap.add_argument("--tree", type=int, default=0, help="tree of --phase runs: 0 the LBVH, 1 the binned SAH tree")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="render kernel id of --phase render (KERNEL_NAMES order; default: the tracer's default)")
     ap.add_argument("--phase", default="all", choices=["all", "render", "rays", "build", "nn"],
@@ -701,6 +703,7 @@ def main() -> None:
         torch.cuda.synchronize()
 
     if args.phase != "all":
+        tr.set_tree(args.tree)
         profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local)
         gpu.close()
         return

@@ -201,18 +201,21 @@ __global__ void __launch_bounds__(NODE_WARPS * 32, 4) k_sah_warp(const uint32_t*
             __syncwarp();
             uint32_t cut = 0, axis = 0, at = 0;
             if (lane == 0) {
+                uint32_t mask[3] = {0u, 0u, 0u};
                 uint32_t bcount[3][sah::BINS];
                 sah::Box bbox[3][sah::BINS];
                 for (int e = 0; e < 3; e++)
                     for (uint32_t a = 0; a < sah::BINS; a++) {
                         const uint32_t i = e * sah::BINS + a;
+                        if (!s_count[i]) continue;
+                        mask[e] |= 1u << a;
                         bcount[e][a] = s_count[i];
                         for (int f = 0; f < 3; f++) {
                             bbox[e][a].lo[f] = unord(s_box[6 * i + f]);
                             bbox[e][a].hi[f] = unord(s_box[6 * i + 3 + f]);
                         }
                     }
-                const sah::Decision d = sah::decide(bcount, bbox, scale, n, leaf);
+                const sah::Decision d = sah::decide_occupied(mask, bcount, bbox, scale, n, leaf);
                 cut = d.cut;
                 axis = d.axis;
                 at = d.at;

@@ -141,8 +141,70 @@ SAH_HD Decision decide(const uint32_t (*bcount)[BINS], const Box (*bbox)[BINS], 
     return Decision{CUT_PLANE, best_k, best_at};
 }
 
+SAH_HD uint32_t lowest_bit(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)(__ffs((int)x) - 1);
+#else
+    return (uint32_t)__builtin_ctz(x);
+#endif
+}
+
+// decide over the occupied bins only (mask[k] bit b: bin b of axis k holds
+// a slot; the entries of empty bins are never read). The same decision as
+// decide: an empty bin adds nothing to a union or a count, so every plane
+// between two occupied bins prices as the plane at the lower one, which the
+// sweep (ascending, strict `<`) meets first; planes below the first
+// occupied bin or at and above the last have an empty side and are skipped.
+SAH_HD Decision decide_occupied(const uint32_t* mask, const uint32_t (*bcount)[BINS], const Box (*bbox)[BINS],
+                                const float* scale, uint32_t count, uint32_t leaf) {
+    bool have = false;
+    float best = 0.0f;
+    uint32_t best_k = 0;
+    uint32_t best_at = 0;
+    for (int k = 0; k < 3; k++) {
+        if (scale[k] == 0.0f) continue;
+        float right_area[BINS];
+        uint32_t right_count[BINS];
+        Box b = empty_box();
+        uint32_t c = 0;
+        for (uint32_t at = BINS; at-- > 0;) {
+            if (!((mask[k] >> at) & 1u)) continue;
+            grow(b, bbox[k][at]);
+            c += bcount[k][at];
+            right_area[at] = area(b);
+            right_count[at] = c;
+        }
+        b = empty_box();
+        c = 0;
+        for (uint32_t at = 0; at + 1 < BINS; at++) {
+            if (!((mask[k] >> at) & 1u)) continue;
+            grow(b, bbox[k][at]);
+            c += bcount[k][at];
+            const uint32_t above = mask[k] & ~((2u << at) - 1u);  // occupied bins past `at`
+            if (!above) break;
+            const uint32_t nxt = lowest_bit(above);
+            const float cost = area(b) * (float)c + right_area[nxt] * (float)right_count[nxt];
+            if (!have || cost < best) {
+                have = true;
+                best = cost;
+                best_k = (uint32_t)k;
+                best_at = at;
+            }
+        }
+    }
+    Box bounds = empty_box();
+    for (uint32_t b = 0; b < BINS; b++)
+        if ((mask[0] >> b) & 1u) grow(bounds, bbox[0][b]);
+    if (!have) return Decision{count > leaf ? (uint32_t)CUT_HALF : (uint32_t)CUT_LEAF, 0u, 0u};
+    const float parent = rmax(area(bounds), 1.17549435e-38f);  // f32::MIN_POSITIVE
+    if (count <= leaf && TRAVERSE + best / parent >= (float)count) return Decision{CUT_LEAF, 0u, 0u};
+    return Decision{CUT_PLANE, best_k, best_at};
+}
+
 // sah.rs:114-189 split: the left count after reordering slots[0, count), or
-// NONE for a leaf. Serial over the node's slots.
+// NONE for a leaf. Serial over the node's slots; a bin's entries are set
+// when the first slot lands in it (so a small node touches only its
+// occupied bins).
 SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots, uint32_t count, uint32_t leaf) {
     if (count <= 1) return NONE;
     Box cbox = empty_box();
@@ -154,23 +216,24 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
     }
     float lo[3], scale[3];
     if (!grid_of(cbox, lo, scale)) return count > leaf ? count / 2 : NONE;
+    uint32_t mask[3] = {0u, 0u, 0u};
     uint32_t bcount[3][BINS];
     Box bbox[3][BINS];
-    for (int k = 0; k < 3; k++)
-        for (uint32_t b = 0; b < BINS; b++) {
-            bcount[k][b] = 0;
-            bbox[k][b] = empty_box();
-        }
     for (uint32_t j = 0; j < count; j++) {
         const uint32_t i = slots[j];
         const Box pb = prim_box(prims + 8 * (uint64_t)i);
         for (int k = 0; k < 3; k++) {
             const uint32_t at = bin_of(centres + 3 * (uint64_t)i, lo, scale, k);
+            if (!((mask[k] >> at) & 1u)) {
+                mask[k] |= 1u << at;
+                bcount[k][at] = 0;
+                bbox[k][at] = empty_box();
+            }
             bcount[k][at] += 1;
             grow(bbox[k][at], pb);
         }
     }
-    const Decision d = decide(bcount, bbox, scale, count, leaf);
+    const Decision d = decide_occupied(mask, bcount, bbox, scale, count, leaf);
     if (d.cut == CUT_LEAF) return NONE;
     if (d.cut == CUT_HALF) return count / 2;
     uint32_t m = 0;

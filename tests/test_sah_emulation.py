@@ -55,3 +55,23 @@ def test_device_steps_on_flat_and_mesh_input(orc, emul):
         b = emul(p, 4)
         assert a[2] == b[2] and np.array_equal(a[1], b[1])
         assert np.array_equal(a[0].view(np.uint32), b[0].view(np.uint32))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_device_steps_on_random_boxes(orc, emul, seed):
+    """Spread boxes, a dense clump and repeated boxes: nodes whose slots
+    fill few of the 16 bins, the case the occupied-bin sweep shortens."""
+    rng = np.random.default_rng(seed)
+    n = 20000
+    lo = rng.uniform(0.0, 10.0, (n, 3)).astype(np.float32)
+    lo[: n // 3] = rng.normal(4.0, 0.05, (n // 3, 3)).astype(np.float32)
+    size = rng.uniform(0.0, 0.5, (n, 3)).astype(np.float32)
+    p = np.zeros((n, 8), np.float32)
+    p[:, 0:3], p[:, 4:7] = lo, lo + size
+    p[n - 500:, 0:3], p[n - 500:, 4:7] = 2.0, 2.25
+    p = p[rng.permutation(n)]
+    for leaf in (1, 4):
+        a = orc.build_sah(p, leaf)
+        b = emul(p, leaf)
+        assert a[2] == b[2] and np.array_equal(a[1], b[1])
+        assert np.array_equal(a[0].view(np.uint32), b[0].view(np.uint32))
