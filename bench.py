@@ -648,7 +648,8 @@ def main() -> None:
     ap.add_argument("--relmse-frames", type=int, default=5,
                     help="independent frames each equal-relMSE figure is averaged over")
     ap.add_argument("--walk", type=int, default=0,
-                    help="ray walk of --phase rays: 0 a thread per ray, 1 persistent, 2 sorted, 3 the 4-wide tree")
+                    help="ray walk of --phase rays: 0 a thread per ray, 1 persistent, 2 sorted, 3 the 4-wide tree "
+                         "(persistent), 4 the 4-wide tree (a thread per ray)")
     ap.add_argument("--tree", type=int, default=0, help="tree of --phase runs: 0 the LBVH, 1 the binned SAH tree")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="render kernel id of --phase render (KERNEL_NAMES order; default: the tracer's default)")
@@ -758,7 +759,8 @@ def main() -> None:
     tr.secondary_rays(cam, W, H, 0, rays)
     walk_ms = {}
     walks = {"thread_per_ray": px.Tracer.WALK_THREAD, "persistent_fetch": px.Tracer.WALK_FETCH,
-             "sorted_fetch": px.Tracer.WALK_SORTED, "wide_fetch": px.Tracer.WALK_WIDE}
+             "sorted_fetch": px.Tracer.WALK_SORTED, "wide_fetch": px.Tracer.WALK_WIDE,
+             "wide_thread_per_ray": px.Tracer.WALK_WIDE_THREAD}
     tree_names = {px.Tracer.TREE_LBVH: "lbvh", px.Tracer.TREE_SAH: "sah"}
     for t_kind in (px.Tracer.TREE_LBVH, px.Tracer.TREE_SAH):
         tr.set_tree(t_kind)
@@ -771,7 +773,7 @@ def main() -> None:
     tr.set_tree({"lbvh": px.Tracer.TREE_LBVH, "sah": px.Tracer.TREE_SAH}[best_walk.split("/")[0]])
     tr.set_walk(walks[best_walk.split("/")[1]])
     _, inc_steps, inc_tests = tr.trace_rays_stats(rays, n, hits, False)
-    node_bytes = 128 if best_walk.endswith("wide_fetch") else 64
+    node_bytes = 128 if "/wide" in best_walk else 64
     inc_bytes = inc_steps * node_bytes + inc_tests * 48
     tr.set_walk(px.Tracer.WALK_THREAD)
     tr.set_tree(tree)

@@ -503,6 +503,8 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
  * named at a tie (two faces at one t); any-hit rays report the same
  * hit-or-miss. Single-instance scenes. */
 #define PHX_WALK_WIDE 3u
+/* PHX_WALK_WIDE_THREAD: the same walk of the wide tree, a thread per ray. */
+#define PHX_WALK_WIDE_THREAD 4u
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
 /* Which tree the tracer walks. PHX_TREE_LBVH (the default): the device LBVH
  * (Morton codes, stable radix sort, Karras, leaf packing; 0.6 ms at 1.3 M

@@ -68,8 +68,9 @@ size_t batch_job_bytes();
 // words. Waits on `s` once a level.
 int32_t build_wide(const float4* bin, uint32_t ninner, float4* wide, uint2* jobs_a, uint2* jobs_b, uint32_t* counts,
                    cudaStream_t s, uint32_t* nodes_out, uint32_t* levels_out);
-// Persistent walks of n rays over the wide tree (counters: rays, steps,
-// tests, or null; next: one word of scratch).
+// Walks of n rays over the wide tree: persistent warps (next: one word of
+// scratch) or, with next null, a thread a ray (counters: rays, steps, tests,
+// or null).
 int32_t launch_rays_wide(const Scene& S, const float4* wide, const float* rays, uint32_t n, float* hits, bool any,
                          unsigned long long* counters, uint32_t* next, int sms, cudaStream_t s);
 

@@ -399,6 +399,90 @@ __device__ __forceinline__ Hit walk_forest(const Scene& S, f3 o, f3 d, float tma
     return best;
 }
 
+// ---- the 4-wide tree of the ray-buffer walks (wide.cu builds it from the
+// binary records; inside the 32-register render kernels its larger frame
+// cost more than its fewer steps saved, so the frame walks stay binary) ----
+// Record: 8 float4 = lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of children 0-3,
+// their refs (inner wide record, first slot | LEAF, or NONE), a spare.
+
+constexpr int WSTACK = 96;  // 3 pushes a wide level, 31 levels at most
+
+__device__ __forceinline__ void order2(float& ta, uint32_t& ra, float& tb, uint32_t& rb) {
+    if (tb < ta) {
+        const float t = ta;
+        ta = tb;
+        tb = t;
+        const uint32_t r = ra;
+        ra = rb;
+        rb = r;
+    }
+}
+
+// One ray's walk of the wide tree: each node's hit children sorted by entry
+// distance (a 5-comparator network), the nearest taken, the rest pushed
+// farthest first. `first`: any hit, as walk_tree. The closest t equals the
+// binary walk's; only which face a tie of two faces at one t names may
+// differ.
+template <bool STATS>
+__device__ __forceinline__ Hit walk_wide(const Tree& T, const float4* __restrict__ wide, f3 o, f3 d, float tmax,
+                                         bool first, Count& cnt) {
+    cnt.rays++;
+    Hit best{tmax, NONE, 0.0f, 0.0f, 0u};
+    const f3 inv = safe_inv(d);
+    if (box_t(T.root_lo, T.root_hi, o, inv, best.t) >= INF) return best;
+    const RaySpace rs = ray_space(d);
+    uint32_t stack[WSTACK];
+    int sp = 0;
+    uint32_t nd = (T.root & LEAF) ? T.root : 0u;
+    for (;;) {
+        if (nd & LEAF) {
+            for (uint32_t id = nd & ~LEAF; id < T.nslots; id++) {
+                const float4 A = __ldg(T.tris + 3 * (size_t)id);
+                const float4 B = __ldg(T.tris + 3 * (size_t)id + 1);
+                const float4 Cc = __ldg(T.tris + 3 * (size_t)id + 2);
+                const uint32_t flags = __float_as_uint(Cc.w);
+                if (STATS) cnt.tests++;
+                float u, v;
+                const float t = tri_t(xyz(A), xyz(B), xyz(Cc), o, rs, u, v);
+                if (t < best.t) {
+                    if (first) {
+                        if (!(flags & FLAG_PASS)) return Hit{t, id, u, v, 0u};
+                    } else {
+                        best = Hit{t, id, u, v, 0u};
+                    }
+                }
+                if (flags & FLAG_END) break;
+            }
+        } else {
+            if (STATS) cnt.steps++;
+            const float4* q = wide + 8 * (size_t)nd;
+            const float4 lx = __ldg(q), hx = __ldg(q + 1), ly = __ldg(q + 2), hy = __ldg(q + 3);
+            const float4 lz = __ldg(q + 4), hz = __ldg(q + 5), rf = __ldg(q + 6);
+            uint32_t r0 = __float_as_uint(rf.x), r1 = __float_as_uint(rf.y);
+            uint32_t r2 = __float_as_uint(rf.z), r3 = __float_as_uint(rf.w);
+            float t0 = box_t(mk(lx.x, ly.x, lz.x), mk(hx.x, hy.x, hz.x), o, inv, best.t);
+            float t1 = box_t(mk(lx.y, ly.y, lz.y), mk(hx.y, hy.y, hz.y), o, inv, best.t);
+            float t2 = r2 == NONE ? INF : box_t(mk(lx.z, ly.z, lz.z), mk(hx.z, hy.z, hz.z), o, inv, best.t);
+            float t3 = r3 == NONE ? INF : box_t(mk(lx.w, ly.w, lz.w), mk(hx.w, hy.w, hz.w), o, inv, best.t);
+            order2(t0, r0, t1, r1);
+            order2(t2, r2, t3, r3);
+            order2(t0, r0, t2, r2);
+            order2(t1, r1, t3, r3);
+            order2(t1, r1, t2, r2);
+            if (t0 < INF) {
+                if (t3 < INF && sp < WSTACK) stack[sp++] = r3;
+                if (t2 < INF && sp < WSTACK) stack[sp++] = r2;
+                if (t1 < INF && sp < WSTACK) stack[sp++] = r1;
+                nd = r0;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        nd = stack[--sp];
+    }
+    return best;
+}
+
 // The two-level walk behind a call of its own, so a single-instance scene's
 // trace keeps a frame of one stack.
 template <bool STATS>

@@ -995,15 +995,41 @@ int32_t wf_buffers(phx_tracer tr, uint32_t count, WfBuffers& B) {
 // Launches the tracer's render kernel over pixels [first_px, first_px +
 // count_px) of frame F, whose camera is already in tr->cam (no host copy:
 // the launch can be recorded into a graph).
+// The wide tree of the binary tree the tracer walks now (collapsed on the
+// device when the tree changed since the last collapse; waits).
+int32_t ensure_wide(phx_tracer tr) {
+    if (tr->wide_gen == tr->tree_gen) return PHX_OK;
+    Ctx* c = tr->ctx;
+    float4 root{};
+    PHX_CUDA(cudaMemcpyAsync(&root, tr->info.ptr, sizeof root, cudaMemcpyDeviceToHost, c->stream));
+    PHX_TRY(wait_stream(c->stream, 0));
+    uint32_t root_ref = 0;
+    std::memcpy(&root_ref, &root.w, 4);
+    const bool leaf_root = (root_ref & LEAF) != 0;
+    const uint32_t ninner = (leaf_root || tr->nfaces < 2) ? 0u : tr->nfaces - 1;
+    if (ninner) {
+        PHX_TRY(tr->wide.reserve((size_t)ninner * 128));
+        PHX_TRY(tr->wide_jobs_a.reserve((size_t)ninner * 8));
+        PHX_TRY(tr->wide_jobs_b.reserve((size_t)ninner * 8));
+        PHX_TRY(tr->wide_counts.reserve(8));
+    }
+    PHX_TRY(build_wide((const float4*)tr->tnodes.ptr, ninner, (float4*)tr->wide.ptr, (uint2*)tr->wide_jobs_a.ptr,
+                       (uint2*)tr->wide_jobs_b.ptr, (uint32_t*)tr->wide_counts.ptr, c->stream, &tr->wide_nodes,
+                       &tr->wide_levels));
+    tr->wide_gen = tr->tree_gen;
+    return read_status(c);
+}
+
 int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, uint32_t count_px, bool stats) {
     Ctx* c = tr->ctx;
     uint32_t kernel = tr->kernel;
+    const Scene S = scene_of(tr);
     // Adaptive Sampling runs on the megakernel forms (the state machine
     // fetches pixels by index, not from the open list); they all compute
     // the same image, so an adaptive frame takes the default form instead.
     if (F.adapt_on && kernel >= PHX_KERNEL_STATE_MACHINE && kernel <= PHX_KERNEL_STATE_MACHINE_8)
         kernel = PHX_KERNEL_MEGAKERNEL;
-    const RenderLaunch L{scene_of(tr), F,       sun,    (uint32_t*)tr->px.ptr, first_px, count_px,
+    const RenderLaunch L{S,        F,       sun,    (uint32_t*)tr->px.ptr, first_px, count_px,
                          (unsigned long long*)tr->rays.ptr, (uint32_t*)tr->next.ptr, c->sms, c->stream};
     const bool full = tr->forest || F.grid > 0.0f;
     if (kernel == PHX_KERNEL_WAVEFRONT) {
@@ -1418,8 +1444,8 @@ int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
 
 int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (mode > PHX_WALK_WIDE) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
-    if (mode == PHX_WALK_WIDE && tr->forest)
+    if (mode > PHX_WALK_WIDE_THREAD) return fail(PHX_ERR_INVALID, "unknown walk mode %u", mode);
+    if (mode >= PHX_WALK_WIDE && tr->forest)
         return fail(PHX_ERR_INVALID, "the wide walk takes single-instance scenes");
     tr->walk = mode;
     return PHX_OK;
@@ -1737,44 +1763,17 @@ int32_t sort_rays(phx_tracer tr, const Scene& S, const float* rays, uint32_t n, 
 }  // namespace
 }  // namespace phx
 
-namespace phx {
-namespace {
-// The wide tree of the binary tree the tracer walks now (collapsed on the
-// device when the tree changed since the last collapse; waits).
-int32_t ensure_wide(phx_tracer tr) {
-    if (tr->wide_gen == tr->tree_gen) return PHX_OK;
-    Ctx* c = tr->ctx;
-    float4 root{};
-    PHX_CUDA(cudaMemcpyAsync(&root, tr->info.ptr, sizeof root, cudaMemcpyDeviceToHost, c->stream));
-    PHX_TRY(wait_stream(c->stream, 0));
-    uint32_t root_ref = 0;
-    std::memcpy(&root_ref, &root.w, 4);
-    const bool leaf_root = (root_ref & LEAF) != 0;
-    const uint32_t ninner = (leaf_root || tr->nfaces < 2) ? 0u : tr->nfaces - 1;
-    if (ninner) {
-        PHX_TRY(tr->wide.reserve((size_t)ninner * 128));
-        PHX_TRY(tr->wide_jobs_a.reserve((size_t)ninner * 8));
-        PHX_TRY(tr->wide_jobs_b.reserve((size_t)ninner * 8));
-        PHX_TRY(tr->wide_counts.reserve(8));
-    }
-    PHX_TRY(build_wide((const float4*)tr->tnodes.ptr, ninner, (float4*)tr->wide.ptr, (uint2*)tr->wide_jobs_a.ptr,
-                       (uint2*)tr->wide_jobs_b.ptr, (uint32_t*)tr->wide_counts.ptr, c->stream, &tr->wide_nodes,
-                       &tr->wide_levels));
-    tr->wide_gen = tr->tree_gen;
-    return read_status(c);
-}
-}  // namespace
-}  // namespace phx
 
 int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits, int32_t any_hit) {
     if (!tr || (n && (!rays || !hits))) return fail(PHX_ERR_INVALID, "null argument");
     if (n == 0) return PHX_OK;
     PHX_TRY(use(tr->ctx));
     const Scene S = scene_of(tr);
-    if (tr->walk == PHX_WALK_WIDE) {
+    if (tr->walk >= PHX_WALK_WIDE) {
         PHX_TRY(ensure_wide(tr));
         return launch_rays_wide(S, (const float4*)tr->wide.ptr, rays, n, hits, any_hit != 0, nullptr,
-                                (uint32_t*)tr->next.ptr, tr->ctx->sms, tr->ctx->stream);
+                                tr->walk == PHX_WALK_WIDE ? (uint32_t*)tr->next.ptr : nullptr, tr->ctx->sms,
+                                tr->ctx->stream);
     }
     uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
     const uint32_t* order = nullptr;
@@ -1793,10 +1792,11 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
     cudaStream_t s = tr->ctx->stream;
     PHX_CUDA(cudaMemsetAsync(tr->rays.ptr, 0, 24, s));
     const Scene S = scene_of(tr);
-    if (n && tr->walk == PHX_WALK_WIDE) {
+    if (n && tr->walk >= PHX_WALK_WIDE) {
         PHX_TRY(ensure_wide(tr));
         PHX_TRY(launch_rays_wide(S, (const float4*)tr->wide.ptr, rays, n, hits, any_hit != 0,
-                                 (unsigned long long*)tr->rays.ptr, (uint32_t*)tr->next.ptr, tr->ctx->sms, s));
+                                 (unsigned long long*)tr->rays.ptr,
+                                 tr->walk == PHX_WALK_WIDE ? (uint32_t*)tr->next.ptr : nullptr, tr->ctx->sms, s));
     } else if (n) {
         uint32_t* nx = tr->walk != PHX_WALK_THREAD ? (uint32_t*)tr->next.ptr : nullptr;
         const uint32_t* order = nullptr;

@@ -31,8 +31,6 @@ namespace {
 
 using namespace shade;
 
-constexpr int WSTACK = 96;  // 3 pushes a wide level, 31 levels at most
-
 __device__ __forceinline__ float half_area(float lx, float ly, float lz, float hx, float hy, float hz) {
     const float dx = fmaxf(hx - lx, 0.0f), dy = fmaxf(hy - ly, 0.0f), dz = fmaxf(hz - lz, 0.0f);
     return dx * dy + dy * dz + dz * dx;
@@ -118,14 +116,28 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ b
     o[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-__device__ __forceinline__ void order2(float& ta, uint32_t& ra, float& tb, uint32_t& rb) {
-    if (tb < ta) {
-        const float t = ta;
-        ta = tb;
-        tb = t;
-        const uint32_t r = ra;
-        ra = rb;
-        rb = r;
+template <bool ANY, bool STATS>
+__global__ void __launch_bounds__(128, 8) k_rays_wide_thread(Scene S, const float4* __restrict__ wide,
+                                                             const float4* __restrict__ rays, uint32_t n,
+                                                             float4* __restrict__ hits,
+                                                             unsigned long long* counters) {
+    load_info(S);
+    const Tree T = tree_of(S);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    Count cnt{0, 0, 0};
+    if (i < n) {
+        const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+        const Hit h = walk_wide<STATS>(T, wide, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt);
+        const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(T.tris + 3 * (size_t)h.tri).w);
+        hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
+    }
+    if (STATS) {
+        const uint32_t st = __reduce_add_sync(0xffffffffu, cnt.steps);
+        const uint32_t te = __reduce_add_sync(0xffffffffu, cnt.tests);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + 1, (unsigned long long)st);
+            atomicAdd(counters + 2, (unsigned long long)te);
+        }
     }
 }
 
@@ -296,6 +308,19 @@ int32_t build_wide(const float4* bin, uint32_t ninner, float4* wide, uint2* jobs
 
 int32_t launch_rays_wide(const Scene& S, const float4* wide, const float* rays, uint32_t n, float* hits, bool any,
                          unsigned long long* counters, uint32_t* next, int sms, cudaStream_t s) {
+    if (!next) {  // a thread a ray
+        const uint32_t blocks = (n + 127) / 128;
+        const float4* R = (const float4*)rays;
+        float4* H = (float4*)hits;
+        if (any) {
+            if (counters) k_rays_wide_thread<true, true><<<blocks, 128, 0, s>>>(S, wide, R, n, H, counters);
+            else k_rays_wide_thread<true, false><<<blocks, 128, 0, s>>>(S, wide, R, n, H, counters);
+        } else {
+            if (counters) k_rays_wide_thread<false, true><<<blocks, 128, 0, s>>>(S, wide, R, n, H, counters);
+            else k_rays_wide_thread<false, false><<<blocks, 128, 0, s>>>(S, wide, R, n, H, counters);
+        }
+        return cuda_check(cudaGetLastError(), "wide ray walk");
+    }
     int per_sm = 0;
     const bool st = counters != nullptr;
     if (any) {

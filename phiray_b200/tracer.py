@@ -248,6 +248,7 @@ class Tracer:
     WALK_FETCH = 1
     WALK_SORTED = 2
     WALK_WIDE = 3
+    WALK_WIDE_THREAD = 4
 
     def set_walk(self, mode: int) -> None:
         """Ray-buffer walks: Tracer.WALK_THREAD (a thread per ray),
@@ -255,7 +256,8 @@ class Tracer:
         Tracer.WALK_SORTED (the same over rays sorted by direction octant and
         origin), all with the same hits; or Tracer.WALK_WIDE (persistent
         warps over a 4-wide tree collapsed from the binary one: the same
-        closest t, the face at a tie may differ)."""
+        closest t, the face at a tie may differ) and Tracer.WALK_WIDE_THREAD
+        (the same walk, a thread per ray)."""
         N.check(N.lib().phx_tracer_set_walk(self.handle, mode))
 
     def set_samples(self, n: int) -> None:

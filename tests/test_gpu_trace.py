@@ -168,8 +168,9 @@ def _same_closest_hits(got, want):
     assert diff.sum() <= max(2, len(got) // 10000), diff.sum()
 
 
+@pytest.mark.parametrize("mode", [3, 4], ids=["persistent", "thread_per_ray"])
 @pytest.mark.parametrize("tree", [0, 1], ids=["lbvh", "sah"])
-def test_wide_walk(gpu, orc, tree):
+def test_wide_walk(gpu, orc, tree, mode):
     """PHX_WALK_WIDE over the 4-wide tree collapsed from either binary tree:
     closest hits == the oracle's binary walk (ties aside), any-hit rays hit
     or miss as the oracle's do; after a repose the wide tree follows the
@@ -187,7 +188,7 @@ def test_wide_walk(gpu, orc, tree):
     rays[::5, 3] = 0.3
     tr = px.Tracer.of(gpu, s)
     tr.set_tree(tree)
-    tr.set_walk(px.Tracer.WALK_WIDE)
+    tr.set_walk(mode)
     dr = torch.tensor(rays, device="cuda")
     hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
     T = oracle_lib.TraceOracle(orc, s, sah=bool(tree))
@@ -209,7 +210,7 @@ def test_wide_walk(gpu, orc, tree):
     tr.trace_rays(dr, n, hits)
     gpu.wait()
     binary = hits.cpu().numpy().copy()
-    tr.set_walk(px.Tracer.WALK_WIDE)
+    tr.set_walk(mode)
     tr.trace_rays(dr, n, hits)
     gpu.wait()
     _same_closest_hits(hits.cpu().numpy(), binary)
