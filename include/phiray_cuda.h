@@ -782,6 +782,10 @@ typedef struct phx_batch_s* phx_batch;
  * bit for bit its tracer's own phx_tracer_trace. */
 #define PHX_BATCH_PERSISTENT 0u
 #define PHX_BATCH_PER_SCENE 1u
+/* PHX_BATCH_PERSISTENT_DENSE: the persistent launch with registers budgeted
+ * for every thread slot of an SM resident (32 a thread; PHX_BATCH_PERSISTENT
+ * budgets 1,536 threads, 40 registers). */
+#define PHX_BATCH_PERSISTENT_DENSE 2u
 int32_t phx_batch_create(phx_ctx ctx, phx_batch* out);
 int32_t phx_batch_destroy(phx_batch b);
 /* A job: frames [first, first + spp) of `cam` at w x h into tracer tr's image
@@ -795,8 +799,9 @@ int32_t phx_batch_set_config(phx_batch b, uint32_t kind, uint32_t threads, uint3
 /* Every job's frame, stream-ordered. */
 int32_t phx_batch_trace(phx_batch b);
 /* The autotuner: times the persistent launch at each block size and stack
- * placement, and per-scene launches of the megakernel and of the state
- * machine, on the batch; keeps the fastest. ms (>= 8 floats, may be NULL)
+ * placement, the dense persistent launch at 128 and 256 threads, and
+ * per-scene launches of the megakernel (4 and 16 resident blocks) and of the
+ * state machine, on the batch; keeps the fastest. ms (>= 11 floats, may be NULL)
  * gets each configuration's time, *nconfigs their number. Waits. */
 int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint32_t* stack, float* ms,
                            uint32_t* nconfigs);

@@ -14,11 +14,13 @@ from .gpu import Gpu
 
 PERSISTENT = 0
 PER_SCENE = 1
+PERSISTENT_DENSE = 2
 STACK_LOCAL = 0
 STACK_SHARED = 1
 
 CONFIG_NAMES = [f"persistent/{t}/{'shared' if s else 'local'}" for t in (64, 128, 256) for s in (0, 1)] + [
-    "per-scene/megakernel", "per-scene/state-machine"]
+    "per-scene/megakernel", "per-scene/state-machine", "persistent-dense/128/local", "persistent-dense/256/local",
+    "per-scene/megakernel-16-sync"]
 
 
 class Batch:

@@ -57,9 +57,10 @@ int32_t render_full(uint32_t kernel, bool stats, const RenderLaunch& L);
 // The wavefront render (render_wf.cu).
 int32_t render_wavefront(bool full, bool stats, const RenderLaunch& L, const WfBuffers& B);
 // The batched persistent launch over a device job table (render_batch.cu):
-// `threads` 64, 128 or 256, the walk stacks in shared memory when smem_stack.
-int32_t render_batch(int threads, bool full, bool smem_stack, int device, int sms, const void* jobs, uint32_t njobs,
-                     uint32_t ntiles, uint32_t* next, cudaStream_t s);
+// `threads` 64, 128 or 256, the walk stacks in shared memory when smem_stack,
+// registers for 2048 resident threads an SM when dense (else 1536).
+int32_t render_batch(int threads, bool full, bool smem_stack, bool dense, int device, int sms, const void* jobs,
+                     uint32_t njobs, uint32_t ntiles, uint32_t* next, cudaStream_t s);
 // sizeof the batch kernel's job record.
 size_t batch_job_bytes();
 // The 4-wide tree collapsed from the tracer's binary records `bin` (wide.cu):
@@ -605,12 +606,12 @@ struct Job {
     uint32_t npx;
 };
 
-// Registers are budgeted for 1536 resident threads an SM (40 a thread): the
-// walk is latency-bound, and the single-scene megakernel runs fastest with
-// that many warps resident although it spills more.
-template <int STATS, int THREADS>
-__global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
-                                                                         uint32_t ntiles, uint32_t* next) {
+// Registers are budgeted for RES resident threads an SM: 1536 (40 a
+// thread) or every thread slot, 2048 (32 a thread). The walk is
+// latency-bound, so more resident warps pay although they spill more.
+template <int STATS, int THREADS, int RES>
+__global__ void __launch_bounds__(THREADS, RES / THREADS) k_render_batch(const Job* __restrict__ jobs, uint32_t njobs,
+                                                                        uint32_t ntiles, uint32_t* next) {
     constexpr int WARPS = THREADS / 32;
     constexpr int WORDS = (int)(sizeof(Job) / 4);
     __shared__ __align__(16) Job sj[WARPS];

@@ -1881,8 +1881,8 @@ int32_t launch_batch(phx_batch b) {
     bool full = false;
     for (const BatchJob& bj : b->jobs) full = full || bj.tr->forest || bj.cam.grid > 0.0f;
     Ctx* c = b->ctx;
-    return render_batch(THREADS, full, b->stack == PHX_STACK_SHARED, c->device, c->sms, b->djobs.ptr,
-                        (uint32_t)b->jobs.size(), b->ntiles, (uint32_t*)b->next.ptr, c->stream);
+    return render_batch(THREADS, full, b->stack == PHX_STACK_SHARED, b->kind == PHX_BATCH_PERSISTENT_DENSE, c->device,
+                        c->sms, b->djobs.ptr, (uint32_t)b->jobs.size(), b->ntiles, (uint32_t*)b->next.ptr, c->stream);
 }
 
 // Uploads cameras and the job table (host copies: not inside a capture).
@@ -2036,7 +2036,7 @@ int32_t phx_batch_add(phx_batch b, phx_tracer tr, const phx_camera* cam, uint32_
 
 int32_t phx_batch_set_config(phx_batch b, uint32_t kind, uint32_t threads, uint32_t stack) {
     if (!b) return fail(PHX_ERR_INVALID, "null batch");
-    if (kind > PHX_BATCH_PER_SCENE) return fail(PHX_ERR_INVALID, "unknown batch kind %u", kind);
+    if (kind > PHX_BATCH_PERSISTENT_DENSE) return fail(PHX_ERR_INVALID, "unknown batch kind %u", kind);
     if (threads != 64 && threads != 128 && threads != 256) return fail(PHX_ERR_INVALID, "block size %u", threads);
     if (stack > PHX_STACK_SHARED) return fail(PHX_ERR_INVALID, "stack placement %u", stack);
     batch_drop_graph(b);
@@ -2069,6 +2069,9 @@ int32_t phx_batch_autotune(phx_batch b, uint32_t* kind, uint32_t* threads, uint3
         for (uint32_t st : {PHX_STACK_LOCAL, PHX_STACK_SHARED}) cfgs.push_back({PHX_BATCH_PERSISTENT, t, st, 0});
     cfgs.push_back({PHX_BATCH_PER_SCENE, 128, PHX_STACK_LOCAL, PHX_KERNEL_MEGAKERNEL});
     cfgs.push_back({PHX_BATCH_PER_SCENE, 128, PHX_STACK_LOCAL, PHX_KERNEL_STATE_MACHINE});
+    // every thread slot resident (32 registers): the single-scene winner's budget
+    for (uint32_t t : {128u, 256u}) cfgs.push_back({PHX_BATCH_PERSISTENT_DENSE, t, PHX_STACK_LOCAL, 0});
+    cfgs.push_back({PHX_BATCH_PER_SCENE, 128, PHX_STACK_LOCAL, PHX_KERNEL_MEGAKERNEL_16_SYNC});
     std::vector<uint32_t> saved;
     for (const BatchJob& bj : b->jobs) saved.push_back(bj.tr->kernel);
     cudaEvent_t e0, e1;

@@ -8,7 +8,7 @@ import pytest
 
 import phiray_b200 as px
 from phiray_b200 import scenes
-from phiray_b200.batch import PER_SCENE, PERSISTENT, STACK_LOCAL, STACK_SHARED, Batch
+from phiray_b200.batch import PER_SCENE, PERSISTENT, PERSISTENT_DENSE, STACK_LOCAL, STACK_SHARED, Batch
 
 pytestmark = pytest.mark.gpu
 
@@ -38,7 +38,8 @@ def _single(gpu, jobs):
 
 @pytest.mark.parametrize("kind,threads,stack", [(PERSISTENT, 64, STACK_LOCAL), (PERSISTENT, 128, STACK_SHARED),
                                                 (PERSISTENT, 256, STACK_LOCAL), (PERSISTENT, 256, STACK_SHARED),
-                                                (PER_SCENE, 128, STACK_LOCAL)])
+                                                (PER_SCENE, 128, STACK_LOCAL), (PERSISTENT_DENSE, 128, STACK_LOCAL),
+                                                (PERSISTENT_DENSE, 256, STACK_SHARED)])
 def test_batch_equals_single_traces(gpu, kind, threads, stack):
     jobs = _jobs()
     want = _single(gpu, jobs)
@@ -70,7 +71,7 @@ def test_batch_autotune_and_captured_frame(gpu):
         trs.append(tr)
         b.add(tr, cam, s.width, s.height, first, s.spp)
     cfg, ms = b.autotune()
-    assert len(ms) == 8 and all(v > 0 for v in ms.values())
+    assert len(ms) == 11 and all(v > 0 for v in ms.values())
     net = Unet(gpu, seed=5)
     b.capture(net, threshold=0.1)
     modes = [1, 0, 0, 1]
