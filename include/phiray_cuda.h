@@ -266,9 +266,9 @@ int32_t phx_sort_codes(phx_ctx ctx, const uint32_t* codes, uint32_t n, uint32_t*
  * array compiled into the library (~9.4 MB, held on every GPU that loads it
  * until the process exits), so n is at most PHX_SORT_STATIC_MAX (larger n:
  * PHX_ERR_INVALID, nothing launched). The first call on a device looks up
- * that array's device address and keeps it for the life of the process: make
- * that first call before any stream capture, and do not reset the device
- * (cudaDeviceReset) while the library is loaded. Stream-ordered and does not
+ * that array's device address and keeps it for the life of the process: do
+ * not reset the device (cudaDeviceReset) while the library is loaded.
+ * Stream-ordered and does not
  * wait: synchronise before reading order/sorted. A failure inside the sort's
  * kernels (a look-back wait that gave up) is reported by the next call that
  * reads the context's status, such as phx_ctx_wait. All calls share the

@@ -39,8 +39,8 @@ std::mutex g_lock;
 uint32_t* g_addr[64] = {};
 
 // The device address of the array on the current device, looked up once per
-// device (the first call on a device does this; make that first call before
-// any stream capture, since the lookup is not a stream operation).
+// device (by the first call on a device; the lookup is a host-side query,
+// not a stream operation).
 int32_t device_scratch(int device, uint32_t** out) {
     if (device < 0 || device >= 64) return phx::fail(PHX_ERR_INVALID, "device %d out of range", device);
     std::lock_guard<std::mutex> g(g_lock);
