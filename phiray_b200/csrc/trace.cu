@@ -26,6 +26,31 @@ namespace {
 
 // ---- scene preparation ----
 
+// The scene checks Tracer::new's callers rely on, run over the uploaded
+// arrays before any kernel indexes through them: out[0] the first face that
+// names a vertex or material out of range, out[1] the first material with a
+// texture or map (Mat words 12-16 not NO_TEX), out[2] the first with a
+// second lobe (word 30 not NO_MAT), all 0xFFFFFFFF when none; out[3] != 0
+// when some material emits (luminance of words 8-10 above zero).
+__global__ void __launch_bounds__(256) k_check_scene(const uint4* __restrict__ faces, uint32_t nfaces, uint32_t nverts,
+                                                     const float* __restrict__ mats, uint32_t nmats,
+                                                     uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nfaces) {
+        const uint4 q = __ldg(faces + i);
+        if (q.x >= nverts || q.y >= nverts || q.z >= nverts || q.w >= nmats) atomicMin(out, i);
+    }
+    if (i < nmats) {
+        const float* m = mats + 32 * (size_t)i;
+        const uint32_t* w = (const uint32_t*)m;
+        bool tex = false;
+        for (int k = 12; k <= 16; k++) tex = tex || __ldg(w + k) != 0xFFFFFFFFu;
+        if (tex) atomicMin(out + 1, i);
+        if (__ldg(w + 30) != 0xFFFFFFFFu) atomicMin(out + 2, i);
+        if (0.2126f * __ldg(m + 8) + 0.7152f * __ldg(m + 9) + 0.0722f * __ldg(m + 10) > 0.0f) atomicOr(out + 3, 1u);
+    }
+}
+
 // tris in slot order (sorted by Morton code): positions, face id, material,
 // and the shadow-pass flag from the material (bvh.wgsl:158-162).
 __global__ void k_gather(const uint32_t* __restrict__ order, const uint4* __restrict__ faces,
@@ -1144,24 +1169,7 @@ int32_t create_tracer(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, 
     if (!sc->verts || !sc->faces || !sc->mats || sc->nmats == 0 || sc->nverts == 0)
         return fail(PHX_ERR_INVALID, "scene arrays missing");
     if (sc->nfaces >= (1u << 30)) return fail(PHX_ERR_INVALID, "too many faces");
-    // Faces index vertices and materials: check on the host once.
-    for (uint32_t f = 0; f < sc->nfaces; f++) {
-        const uint32_t* q = sc->faces + 4 * (size_t)f;
-        if (q[0] >= sc->nverts || q[1] >= sc->nverts || q[2] >= sc->nverts || q[3] >= sc->nmats)
-            return fail(PHX_ERR_INVALID, "face %u names a vertex or material out of range", f);
-    }
-    for (uint32_t m = 0; m < sc->nmats; m++) {
-        const uint32_t* q = (const uint32_t*)(sc->mats + 32 * (size_t)m);
-        // tex, nmap, maps (Mat words 12..16) must be NO_TEX; second (30) NO_MAT.
-        for (int k = 12; k <= 16; k++)
-            if (q[k] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u uses a texture (not supported)", m);
-        if (q[30] != 0xFFFFFFFFu) return fail(PHX_ERR_INVALID, "material %u has a second lobe (not supported)", m);
-    }
-    bool emissive = false;
-    for (uint32_t m = 0; m < sc->nmats && !emissive; m++) {
-        const float* e = sc->mats + 32 * (size_t)m + 8;
-        emissive = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2] > 0.0f;
-    }
+    if (sc->nmats >= (1u << 30)) return fail(PHX_ERR_INVALID, "too many materials");
     PHX_TRY(use(&ctx->c));
     auto* tr = new phx_tracer_s();
     tr->ctx = &ctx->c;
@@ -1170,7 +1178,6 @@ int32_t create_tracer(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, 
     tr->nmats = sc->nmats;
     tr->leaf = sc->leaf ? sc->leaf : 4;
     tr->has_normals = sc->normals != nullptr;
-    tr->emissive = emissive;
     ctx->c.live++;
     cudaStream_t s = ctx->c.stream;
     const size_t n = sc->nfaces;
@@ -1193,6 +1200,37 @@ int32_t create_tracer(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, 
     step(tr->cam.reserve(sizeof(phx_camera)));
     step(tr->next.reserve(16));
     step(tr->bvh.reserve(sc->nfaces, ctx->c.sms));
+    // Upload, then check the arrays on the device before any kernel indexes
+    // through them (faces name vertices and materials; materials take no
+    // textures, maps or second lobes) and learn whether some material emits.
+    if (rc == PHX_OK)
+        rc = cuda_check(cudaMemcpyAsync(tr->verts.ptr, sc->verts, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK && tr->has_normals)
+        rc = cuda_check(cudaMemcpyAsync(tr->vnorm.ptr, sc->normals, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK) rc = cuda_check(cudaMemcpyAsync(tr->faces.ptr, sc->faces, n * 16, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK)
+        rc = cuda_check(cudaMemcpyAsync(tr->mats.ptr, sc->mats, (size_t)sc->nmats * 128, cudaMemcpyHostToDevice, s), "upload");
+    if (rc == PHX_OK) {
+        const uint32_t init[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u};
+        uint32_t found[4] = {0, 0, 0, 0};
+        rc = cuda_check(cudaMemcpyAsync(tr->rays.ptr, init, 16, cudaMemcpyHostToDevice, s), "upload");
+        const uint32_t items = std::max<uint32_t>(sc->nfaces, sc->nmats);
+        if (rc == PHX_OK) {
+            k_check_scene<<<(items + 255) / 256, 256, 0, s>>>((const uint4*)tr->faces.ptr, sc->nfaces, sc->nverts,
+                                                               (const float*)tr->mats.ptr, sc->nmats,
+                                                               (uint32_t*)tr->rays.ptr);
+            rc = cuda_check(cudaGetLastError(), "scene check");
+        }
+        if (rc == PHX_OK) rc = cuda_check(cudaMemcpyAsync(found, tr->rays.ptr, 16, cudaMemcpyDeviceToHost, s), "check");
+        if (rc == PHX_OK) rc = wait_stream(s, 0);
+        if (rc == PHX_OK && found[0] != 0xFFFFFFFFu)
+            rc = fail(PHX_ERR_INVALID, "face %u names a vertex or material out of range", found[0]);
+        if (rc == PHX_OK && found[1] != 0xFFFFFFFFu)
+            rc = fail(PHX_ERR_INVALID, "material %u uses a texture (not supported)", found[1]);
+        if (rc == PHX_OK && found[2] != 0xFFFFFFFFu)
+            rc = fail(PHX_ERR_INVALID, "material %u has a second lobe (not supported)", found[2]);
+        tr->emissive = found[3] != 0;
+    }
     if (meshes && rc == PHX_OK) {
         tr->forest.reset(new Forest());
         Forest& F = *tr->forest;
@@ -1263,14 +1301,7 @@ int32_t create_tracer(phx_ctx ctx, const phx_scene* sc, const phx_mesh* meshes, 
     }
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev0), "event");
     if (rc == PHX_OK) rc = cuda_check(cudaEventCreate(&tr->ev1), "event");
-    if (rc == PHX_OK)
-        rc = cuda_check(cudaMemcpyAsync(tr->verts.ptr, sc->verts, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
-    if (rc == PHX_OK && tr->has_normals)
-        rc = cuda_check(cudaMemcpyAsync(tr->vnorm.ptr, sc->normals, (size_t)sc->nverts * 16, cudaMemcpyHostToDevice, s), "upload");
-    if (rc == PHX_OK) rc = cuda_check(cudaMemcpyAsync(tr->faces.ptr, sc->faces, n * 16, cudaMemcpyHostToDevice, s), "upload");
-    if (rc == PHX_OK)
-        rc = cuda_check(cudaMemcpyAsync(tr->mats.ptr, sc->mats, (size_t)sc->nmats * 128, cudaMemcpyHostToDevice, s), "upload");
-    if (rc == PHX_OK) rc = cuda_check(cudaMemsetAsync(tr->rays.ptr, 0, 8, s), "zero");
+    if (rc == PHX_OK) rc = cuda_check(cudaMemsetAsync(tr->rays.ptr, 0, 24, s), "zero");
     if (rc == PHX_OK)
         rc = launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, sc->nfaces,
                                (phx_aabb*)tr->bvh.prims.ptr);

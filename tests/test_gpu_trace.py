@@ -398,3 +398,29 @@ def test_autotune_tree_weighs_build_against_frames(gpu, orc):
     want, _ = oracle_lib.TraceOracle(orc, s, sah=many == px.Tracer.TREE_SAH).trace(cam, 0, s.spp)
     check_image(tr.image(), want, s.width * s.height)
     tr.close()
+
+
+def test_create_refuses_scenes_the_tracer_does_not_take(gpu):
+    """The device check at create: a face naming a vertex or material out of
+    range, a material with a texture or map word set, or one with a second
+    lobe, each refused with PHX_ERR_INVALID; the scene otherwise builds."""
+    s = SCENES["c1_small"]()
+    px.Tracer.of(gpu, s).close()
+    cases = []
+    f = s.faces.copy()
+    f[17, 1] = len(s.verts)
+    cases.append((s.verts, f, s.mats, "vertex"))
+    f = s.faces.copy()
+    f[5, 3] = len(s.mats)
+    cases.append((s.verts, f, s.mats, "material index"))
+    m = s.mats.copy()
+    m.view(np.uint32).reshape(len(m), -1)[len(m) - 1, 13] = 0
+    cases.append((s.verts, s.faces, m, "texture"))
+    m = s.mats.copy()
+    m.view(np.uint32).reshape(len(m), -1)[0, 30] = 0
+    cases.append((s.verts, s.faces, m, "second lobe"))
+    for v, f, m, what in cases:
+        with pytest.raises(px.PhxError) as e:
+            px.Tracer(gpu, v, f, m)
+        assert e.value.code == px._native.PHX_ERR_INVALID, what
+    px.Tracer.of(gpu, s).close()  # the context is still good
