@@ -10,8 +10,8 @@
 // and a last bottom-up pass writes the nodes with their bounds.
 //
 // Nodes under MID slots are one thread each, running the per-node code of
-// sah_core.cuh; nodes of MID to BIG slots a warp each (bins by shared-memory
-// atomics, the swap loop over shared memory). Nodes of BIG slots or more —
+// sah_core.cuh; nodes of MID to BIG slots a block each (bins by shared-memory
+// atomics, the swap loop's result by the queue model below, in shared memory). Nodes of BIG slots or more —
 // the top levels, where a node a thread or warp would leave the GPU idle —
 // are cut over blocks of CHUNK slots: the box of centres and the bins are min/max and count reductions
 // (exact in any order) merged with atomics; one thread a node then makes
@@ -123,74 +123,91 @@ __device__ __forceinline__ uint32_t block_sum_exclusive(uint32_t v, uint32_t* to
     return before;
 }
 
-// ---- nodes of MID to BIG slots: a warp a node ----
+// ---- nodes of MID to BIG slots: a block a node ----
 
 constexpr uint32_t MID = 128;
+constexpr uint32_t NODE_THREADS = 256;
+constexpr uint32_t NODE_ITEMS = BIG / NODE_THREADS;  // slots a thread holds
+static_assert(NODE_THREADS * NODE_ITEMS == BIG, "a block holds a node of up to BIG slots");
+static_assert(NODE_THREADS == CHUNK_THREADS, "block_sum_exclusive is written for CHUNK_THREADS");
 
-constexpr uint32_t NODE_WARPS = 4;  // warps (nodes) a block
-// A warp's shared memory: bin counts, bin boxes (ordered words), the node's
-// slots and their left flags.
-constexpr uint32_t WARP_WORDS = HBINS + 6 * HBINS + BIG + BIG / 4;
-
-// sah_core.cuh process for one node, by a warp: the box of centres by warp
-// reductions, the bins by shared-memory atomics (min, max and counts are
-// exact in any order), the reference's decision by lane 0 (decide), and the
-// reference's swap loop by lane 0 over the slots staged in shared memory
-// (the flag of the slot at position j when the loop reaches j is that of the
-// slot first there: the loop only swaps positions at or before j).
-__global__ void __launch_bounds__(NODE_WARPS * 32, 4) k_sah_warp(const uint32_t* __restrict__ list, uint32_t count,
-                                                              TNode* tn, const float* __restrict__ prims,
-                                                              const float* __restrict__ centres, uint32_t* order,
-                                                              uint32_t leaf, uint32_t* tcount, uint32_t* next,
-                                                              uint32_t* next_count) {
-    extern __shared__ uint32_t s_words[];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t k = blockIdx.x * NODE_WARPS + warp;
-    if (k >= count) return;  // (whole warps)
-    uint32_t* s_count = s_words + warp * WARP_WORDS;
-    uint32_t* s_box = s_count + HBINS;
-    uint32_t* s_slot = s_box + 6 * HBINS;
-    uint8_t* s_flag = (uint8_t*)(s_slot + BIG);
-    const uint32_t t = list[k];
+// sah_core.cuh process for one node by a block: each thread holds 8 of the
+// node's slots in registers; the box of centres by block reduction, the bins
+// by shared-memory atomics on ordered words (min, max and counts are exact
+// in any order), one thread an axis sweeps (sweep_axis) and thread 0 decides
+// (decide_from); the reference's swap loop is reproduced in shared memory by
+// the queue model (block scan for each slot's rank among the lefts, the
+// log's links, pointer jumping in place: a link only ever moves to an
+// ancestor on its own chain, so reading a neighbour's already-updated link
+// only shortens the chase).
+__global__ void __launch_bounds__(NODE_THREADS, 2) k_sah_block(const uint32_t* __restrict__ list, TNode* tn,
+                                                            const float* __restrict__ prims,
+                                                            const float* __restrict__ centres, uint32_t* order,
+                                                            uint32_t leaf, uint32_t* tcount, uint32_t* next,
+                                                            uint32_t* next_count) {
+    __shared__ uint32_t s_count[HBINS];
+    __shared__ uint32_t s_box[6 * HBINS];
+    __shared__ uint16_t s_ptr[BIG];
+    __shared__ uint32_t s_val[BIG];
+    __shared__ float s_red[6][NODE_THREADS / 32];
+    __shared__ sah::AxisBest s_axis[3];
+    __shared__ uint32_t s_cut, s_axis_k, s_at, s_first;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t t = list[blockIdx.x];
     TNode nd = tn[t];
     const uint32_t n = nd.end - nd.start;
     uint32_t m = sah::NONE;
     if (nd.depth + 1 < sah::MAX_DEPTH && n > 1 && n <= BIG) {
-        const uint32_t* slots = order + nd.start;
+        uint32_t slot[NODE_ITEMS];
+        const uint32_t j0 = tid * NODE_ITEMS;
         float lo[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
         float hi[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
-        for (uint32_t j = lane; j < n; j += 32) {
-            const uint32_t i = slots[j];
-            s_slot[j] = i;
-            const float* c = centres + 3 * (uint64_t)i;
-            for (int e = 0; e < 3; e++) {
-                lo[e] = fminf(lo[e], c[e]);
-                hi[e] = fmaxf(hi[e], c[e]);
+#pragma unroll
+        for (uint32_t e = 0; e < NODE_ITEMS; e++) {
+            slot[e] = j0 + e < n ? order[nd.start + j0 + e] : 0u;
+            if (j0 + e < n) {
+                const float* c = centres + 3 * (uint64_t)slot[e];
+                for (int k = 0; k < 3; k++) {
+                    lo[k] = fminf(lo[k], c[k]);
+                    hi[k] = fmaxf(hi[k], c[k]);
+                }
             }
         }
-        for (int e = 0; e < 3; e++)
+        for (int k = 0; k < 3; k++)
             for (int o = 16; o > 0; o >>= 1) {
-                lo[e] = fminf(lo[e], __shfl_xor_sync(0xffffffffu, lo[e], o));
-                hi[e] = fmaxf(hi[e], __shfl_xor_sync(0xffffffffu, hi[e], o));
+                lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+                hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
             }
+        if (lane == 0)
+            for (int k = 0; k < 3; k++) {
+                s_red[k][warp] = lo[k];
+                s_red[3 + k][warp] = hi[k];
+            }
+        for (uint32_t i = tid; i < HBINS; i += NODE_THREADS) s_count[i] = 0;
+        for (uint32_t i = tid; i < 6 * HBINS; i += NODE_THREADS)
+            s_box[i] = ord((i % 6) < 3 ? 3.402823466e38f : -3.402823466e38f);
+        if (tid == 0) s_first = 0xFFFFFFFFu;
+        __syncthreads();
         sah::Box cbox;
-        for (int e = 0; e < 3; e++) {
-            cbox.lo[e] = lo[e];
-            cbox.hi[e] = hi[e];
+        for (int k = 0; k < 3; k++) {
+            cbox.lo[k] = s_red[k][0];
+            cbox.hi[k] = s_red[3 + k][0];
+            for (uint32_t w = 1; w < NODE_THREADS / 32; w++) {
+                cbox.lo[k] = fminf(cbox.lo[k], s_red[k][w]);
+                cbox.hi[k] = fmaxf(cbox.hi[k], s_red[3 + k][w]);
+            }
         }
         float glo[3], scale[3];
         if (!sah::grid_of(cbox, glo, scale)) {
             m = n > leaf ? n / 2 : sah::NONE;
         } else {
-            for (uint32_t i = lane; i < HBINS; i += 32) s_count[i] = 0;
-            for (uint32_t i = lane; i < 6 * HBINS; i += 32)
-                s_box[i] = ord((i % 6) < 3 ? 3.402823466e38f : -3.402823466e38f);
-            __syncwarp();
-            for (uint32_t j = lane; j < n; j += 32) {
-                const uint32_t i = s_slot[j];
+#pragma unroll
+            for (uint32_t e = 0; e < NODE_ITEMS; e++) {
+                if (j0 + e >= n) continue;
+                const uint32_t i = slot[e];
                 const float* p = prims + 8 * (uint64_t)i;
-                for (int e = 0; e < 3; e++) {
-                    const uint32_t at = e * sah::BINS + sah::bin_of(centres + 3 * (uint64_t)i, glo, scale, e);
+                for (int k = 0; k < 3; k++) {
+                    const uint32_t at = k * sah::BINS + sah::bin_of(centres + 3 * (uint64_t)i, glo, scale, k);
                     atomicAdd(&s_count[at], 1u);
                     for (int f = 0; f < 3; f++) {  // a NaN bound loses, as in f32::min / max
                         if (p[f] == p[f]) atomicMin(&s_box[6 * at + f], ord(p[f]));
@@ -198,55 +215,93 @@ __global__ void __launch_bounds__(NODE_WARPS * 32, 4) k_sah_warp(const uint32_t*
                     }
                 }
             }
-            __syncwarp();
-            uint32_t cut = 0, axis = 0, at = 0;
-            if (lane == 0) {
-                uint32_t mask[3] = {0u, 0u, 0u};
-                uint32_t bcount[3][sah::BINS];
-                sah::Box bbox[3][sah::BINS];
-                for (int e = 0; e < 3; e++)
-                    for (uint32_t a = 0; a < sah::BINS; a++) {
-                        const uint32_t i = e * sah::BINS + a;
-                        if (!s_count[i]) continue;
-                        mask[e] |= 1u << a;
-                        bcount[e][a] = s_count[i];
-                        for (int f = 0; f < 3; f++) {
-                            bbox[e][a].lo[f] = unord(s_box[6 * i + f]);
-                            bbox[e][a].hi[f] = unord(s_box[6 * i + 3 + f]);
-                        }
+            __syncthreads();
+            if (tid < 3) {
+                const int k = (int)tid;
+                uint32_t mask = 0, bc[sah::BINS];
+                sah::Box bb[sah::BINS];
+                for (uint32_t a = 0; a < sah::BINS; a++) {
+                    const uint32_t i = k * sah::BINS + a;
+                    if (!s_count[i]) continue;
+                    mask |= 1u << a;
+                    bc[a] = s_count[i];
+                    for (int f = 0; f < 3; f++) {
+                        bb[a].lo[f] = unord(s_box[6 * i + f]);
+                        bb[a].hi[f] = unord(s_box[6 * i + 3 + f]);
                     }
-                const sah::Decision d = sah::decide_occupied(mask, bcount, bbox, scale, n, leaf);
-                cut = d.cut;
-                axis = d.axis;
-                at = d.at;
+                }
+                s_axis[k] = scale[k] == 0.0f ? sah::AxisBest{false, 0.0f, 0u} : sah::sweep_axis(mask, bc, bb);
             }
-            cut = __shfl_sync(0xffffffffu, cut, 0);
-            axis = __shfl_sync(0xffffffffu, axis, 0);
-            at = __shfl_sync(0xffffffffu, at, 0);
+            __syncthreads();
+            if (tid == 0) {
+                sah::Box bounds = sah::empty_box();
+                for (uint32_t a = 0; a < sah::BINS; a++) {
+                    if (!s_count[a]) continue;
+                    sah::Box b;
+                    for (int f = 0; f < 3; f++) {
+                        b.lo[f] = unord(s_box[6 * a + f]);
+                        b.hi[f] = unord(s_box[6 * a + 3 + f]);
+                    }
+                    sah::grow(bounds, b);
+                }
+                const sah::Decision d = sah::decide_from(s_axis, scale, bounds, n, leaf);
+                s_cut = d.cut;
+                s_axis_k = d.axis;
+                s_at = d.at;
+            }
+            __syncthreads();
+            const uint32_t cut = s_cut, axis = s_axis_k, at = s_at;
             if (cut == sah::CUT_HALF) m = n / 2;
             if (cut == sah::CUT_PLANE) {
-                for (uint32_t j = lane; j < n; j += 32)
-                    s_flag[j] = sah::bin_of(centres + 3 * (uint64_t)s_slot[j], glo, scale, (int)axis) <= at ? 1 : 0;
-                __syncwarp();
-                if (lane == 0) {
-                    uint32_t q = 0;
-                    for (uint32_t j = 0; j < n; j++) {
-                        if (s_flag[j]) {
-                            const uint32_t x = s_slot[j];
-                            s_slot[j] = s_slot[q];
-                            s_slot[q] = x;
-                            q++;
-                        }
-                    }
-                    m = (q == 0 || q == n) ? n / 2 : q;
+                bool left[NODE_ITEMS];
+                uint32_t mine = 0;
+#pragma unroll
+                for (uint32_t e = 0; e < NODE_ITEMS; e++) {
+                    left[e] = j0 + e < n &&
+                              sah::bin_of(centres + 3 * (uint64_t)slot[e], glo, scale, (int)axis) <= at;
+                    mine += left[e] ? 1u : 0u;
+                    if (j0 + e < n && !left[e]) atomicMin(&s_first, j0 + e);
                 }
-                m = __shfl_sync(0xffffffffu, m, 0);
-                __syncwarp();
-                for (uint32_t j = lane; j < n; j += 32) order[nd.start + j] = s_slot[j];
+                uint32_t total = 0;
+                uint32_t lr = block_sum_exclusive(mine, &total);  // (syncs; s_first is settled after it)
+                const uint32_t q = total;
+                if (q == 0 || q == n) {
+                    m = n / 2;  // no left slot or no right one: the swap loop moved nothing
+                } else {
+                    m = q;
+                    const uint32_t first = s_first;
+#pragma unroll
+                    for (uint32_t e = 0; e < NODE_ITEMS; e++) {
+                        const uint32_t j = j0 + e;
+                        if (j >= n) continue;
+                        if (left[e]) order[nd.start + lr] = slot[e];
+                        if (j >= first) {
+                            const uint32_t p = j - first;
+                            if (left[e]) {
+                                s_ptr[p] = (uint16_t)(lr - first);
+                            } else {
+                                s_ptr[p] = (uint16_t)p;
+                                s_val[p] = slot[e];
+                            }
+                        }
+                        if (left[e]) lr++;
+                    }
+                    __syncthreads();
+                    const uint32_t entries = n - first;
+                    uint32_t rounds = 1;
+                    while ((1u << rounds) < entries) rounds++;
+                    for (uint32_t r = 0; r <= rounds; r++) {
+                        for (uint32_t x = tid; x < entries; x += NODE_THREADS) s_ptr[x] = s_ptr[s_ptr[x]];
+                        __syncthreads();
+                    }
+                    const uint32_t rotations = m - first;
+                    for (uint32_t r = tid; r < n - m; r += NODE_THREADS)
+                        order[nd.start + m + r] = s_val[s_ptr[rotations + r]];
+                }
             }
         }
     }
-    if (lane != 0) return;
+    if (tid != 0) return;
     if (m == sah::NONE) {
         nd.left = nd.right = sah::NONE;
     } else {
@@ -695,9 +750,8 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
             }
         }
         if (nmid)
-            k_sah_warp<<<blocks_of(nmid, NODE_WARPS), NODE_WARPS * 32, NODE_WARPS * WARP_WORDS * 4, s>>>(
-                (const uint32_t*)mid_list.ptr, nmid, T, P, (const float*)centres.ptr, order, leaf, cnt, L + next,
-                cnt + 1);
+            k_sah_block<<<nmid, NODE_THREADS, 0, s>>>((const uint32_t*)mid_list.ptr, T, P, (const float*)centres.ptr,
+                                                      order, leaf, cnt, L + next, cnt + 1);
         if (nsmall)
             k_sah_thread<<<blocks_of(nsmall, 64), 64, 0, s>>>(level, nsmall, T, P, (const float*)centres.ptr, order,
                                                               leaf, cnt, L + next, cnt + 1);

@@ -149,56 +149,81 @@ SAH_HD uint32_t lowest_bit(uint32_t x) {
 #endif
 }
 
-// decide over the occupied bins only (mask[k] bit b: bin b of axis k holds
-// a slot; the entries of empty bins are never read). The same decision as
-// decide: an empty bin adds nothing to a union or a count, so every plane
-// between two occupied bins prices as the plane at the lower one, which the
-// sweep (ascending, strict `<`) meets first; planes below the first
-// occupied bin or at and above the last have an empty side and are skipped.
-SAH_HD Decision decide_occupied(const uint32_t* mask, const uint32_t (*bcount)[BINS], const Box (*bbox)[BINS],
-                                const float* scale, uint32_t count, uint32_t leaf) {
+// One axis of the sweep (sah.rs:150-170) over the occupied bins only
+// (mask bit b: bin b holds a slot; the entries of empty bins are never
+// read): the first plane of least cost in ascending order. An empty bin adds
+// nothing to a union or a count, so every plane between two occupied bins
+// prices as the plane at the lower one, which the ascending strict-`<` sweep
+// meets first; planes below the first occupied bin or at and above the last
+// have an empty side and are skipped.
+struct AxisBest {
+    bool have;
+    float cost;
+    uint32_t at;
+};
+
+SAH_HD AxisBest sweep_axis(uint32_t mask, const uint32_t* bcount, const Box* bbox) {
+    AxisBest r{false, 0.0f, 0u};
+    float right_area[BINS];
+    uint32_t right_count[BINS];
+    Box b = empty_box();
+    uint32_t c = 0;
+    for (uint32_t at = BINS; at-- > 0;) {
+        if (!((mask >> at) & 1u)) continue;
+        grow(b, bbox[at]);
+        c += bcount[at];
+        right_area[at] = area(b);
+        right_count[at] = c;
+    }
+    b = empty_box();
+    c = 0;
+    for (uint32_t at = 0; at + 1 < BINS; at++) {
+        if (!((mask >> at) & 1u)) continue;
+        grow(b, bbox[at]);
+        c += bcount[at];
+        const uint32_t above = mask & ~((2u << at) - 1u);  // occupied bins past `at`
+        if (!above) break;
+        const uint32_t nxt = lowest_bit(above);
+        const float cost = area(b) * (float)c + right_area[nxt] * (float)right_count[nxt];
+        if (!r.have || cost < r.cost) r = AxisBest{true, cost, at};
+    }
+    return r;
+}
+
+// The decision from the three axes' sweeps (axis k skipped where scale[k]
+// is 0): the reference keeps the first plane of least cost over the axes in
+// order (strict `<`), i.e. the axis with the least cost, the lower axis on a
+// tie; then the leaf rule against the node's bounds.
+SAH_HD Decision decide_from(const AxisBest* axes, const float* scale, const Box& bounds, uint32_t count,
+                            uint32_t leaf) {
     bool have = false;
     float best = 0.0f;
-    uint32_t best_k = 0;
-    uint32_t best_at = 0;
+    uint32_t best_k = 0, best_at = 0;
     for (int k = 0; k < 3; k++) {
-        if (scale[k] == 0.0f) continue;
-        float right_area[BINS];
-        uint32_t right_count[BINS];
-        Box b = empty_box();
-        uint32_t c = 0;
-        for (uint32_t at = BINS; at-- > 0;) {
-            if (!((mask[k] >> at) & 1u)) continue;
-            grow(b, bbox[k][at]);
-            c += bcount[k][at];
-            right_area[at] = area(b);
-            right_count[at] = c;
-        }
-        b = empty_box();
-        c = 0;
-        for (uint32_t at = 0; at + 1 < BINS; at++) {
-            if (!((mask[k] >> at) & 1u)) continue;
-            grow(b, bbox[k][at]);
-            c += bcount[k][at];
-            const uint32_t above = mask[k] & ~((2u << at) - 1u);  // occupied bins past `at`
-            if (!above) break;
-            const uint32_t nxt = lowest_bit(above);
-            const float cost = area(b) * (float)c + right_area[nxt] * (float)right_count[nxt];
-            if (!have || cost < best) {
-                have = true;
-                best = cost;
-                best_k = (uint32_t)k;
-                best_at = at;
-            }
+        if (scale[k] == 0.0f || !axes[k].have) continue;
+        if (!have || axes[k].cost < best) {
+            have = true;
+            best = axes[k].cost;
+            best_k = (uint32_t)k;
+            best_at = axes[k].at;
         }
     }
-    Box bounds = empty_box();
-    for (uint32_t b = 0; b < BINS; b++)
-        if ((mask[0] >> b) & 1u) grow(bounds, bbox[0][b]);
     if (!have) return Decision{count > leaf ? (uint32_t)CUT_HALF : (uint32_t)CUT_LEAF, 0u, 0u};
     const float parent = rmax(area(bounds), 1.17549435e-38f);  // f32::MIN_POSITIVE
     if (count <= leaf && TRAVERSE + best / parent >= (float)count) return Decision{CUT_LEAF, 0u, 0u};
     return Decision{CUT_PLANE, best_k, best_at};
+}
+
+// decide over the occupied bins only (mask[k] for axis k).
+SAH_HD Decision decide_occupied(const uint32_t* mask, const uint32_t (*bcount)[BINS], const Box (*bbox)[BINS],
+                                const float* scale, uint32_t count, uint32_t leaf) {
+    AxisBest axes[3];
+    for (int k = 0; k < 3; k++)
+        axes[k] = scale[k] == 0.0f ? AxisBest{false, 0.0f, 0u} : sweep_axis(mask[k], bcount[k], bbox[k]);
+    Box bounds = empty_box();
+    for (uint32_t b = 0; b < BINS; b++)
+        if ((mask[0] >> b) & 1u) grow(bounds, bbox[0][b]);
+    return decide_from(axes, scale, bounds, count, leaf);
 }
 
 // sah.rs:114-189 split: the left count after reordering slots[0, count), or
