@@ -218,7 +218,7 @@ typedef struct phx_bvh_s* phx_bvh;
  * numbering, bounds refit bottom up. All pointers are DEVICE memory:
  * prims (n phx_aabb), nodes (room for 2n - 1), order (n). Writes the node
  * count and depth; stream-ordered, waits once or twice per tree level.
- * Nodes under 128 slots are a thread's, 128-2,047 a warp's, larger ones are
+ * Nodes under 128 slots are a thread's, 128-2,047 a block's, larger ones are
  * cut over blocks of 2,048 slots (1.3 M prims: ~10 ms). */
 int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t leaf, phx_node* nodes,
                           uint32_t* order, uint32_t* node_count, uint32_t* depth);
