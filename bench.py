@@ -735,6 +735,51 @@ def main() -> None:
     ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps, f"cuda:{local}")
     value = whole_job_rate(rays_per_frame, world, ms_step) / 1e6
 
+    # End to end through the public API from pinned host memory.
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
+           (("v", s.verts), ("f", s.faces.view(np.int32)), ("m", s.mats))}
+    hv, hf, hm = pin["v"].numpy(), pin["f"].numpy().view(np.uint32), pin["m"].numpy()
+    h2d = hv.nbytes + hf.nbytes + hm.nbytes + cam.nbytes
+    d2h = n * 4
+
+    e2e_parts = {"create_ms": 0.0, "trace_denoise_ms": 0.0, "read_ms": 0.0, "close_ms": 0.0}
+
+    def e2e_step():
+        t0 = time.perf_counter()
+        t = px.Tracer(gpu, hv, hf, hm)
+        if tree != px.Tracer.TREE_LBVH:
+            t.set_tree(tree)  # the tree the autotuner picked (rebuilt over the uploaded faces)
+        t.set_kernel(chosen)  # the render kernel the autotuner picked for this scene
+        gpu.wait(60000)
+        t1 = time.perf_counter()
+        t.trace(cam, W, H, 0, args.spp)
+        t.denoise()
+        gpu.wait(60000)
+        t2 = time.perf_counter()
+        img = t.pixels()
+        t3 = time.perf_counter()
+        t.close()
+        t4 = time.perf_counter()
+        for k, a, b in (("create_ms", t0, t1), ("trace_denoise_ms", t1, t2), ("read_ms", t2, t3), ("close_ms", t3, t4)):
+            e2e_parts[k] += (b - a) * 1e3
+        return img
+
+    e2e_step()
+    barrier()
+    for k in e2e_parts:
+        e2e_parts[k] = 0.0
+    e2e_steps = max(3, args.steps)
+    e2e_each = []
+    with Clocks(local) as e2e_clk:
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ts = time.perf_counter()
+            e2e_step()
+            e2e_each.append((time.perf_counter() - ts) * 1e3)
+        barrier()
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, f"cuda:{local}")
+    e2e = whole_job_rate(rays_per_frame, world, e2e_s * 1e3) / 1e6
+
     # Phase timings (same device, outside the headline loop).
     def timed(fn, reps):
         return timed_fn(gpu, stream, fn, reps)
@@ -780,47 +825,6 @@ def main() -> None:
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
     ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")
     prim_ms = timed(lambda: tr.primary(cam, W, H, 0, ids, ts), 10)
-
-    # End to end through the public API from pinned host memory.
-    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in
-           (("v", s.verts), ("f", s.faces.view(np.int32)), ("m", s.mats))}
-    hv, hf, hm = pin["v"].numpy(), pin["f"].numpy().view(np.uint32), pin["m"].numpy()
-    h2d = hv.nbytes + hf.nbytes + hm.nbytes + cam.nbytes
-    d2h = n * 4
-
-    e2e_parts = {"create_ms": 0.0, "trace_denoise_ms": 0.0, "read_ms": 0.0, "close_ms": 0.0}
-
-    def e2e_step():
-        t0 = time.perf_counter()
-        t = px.Tracer(gpu, hv, hf, hm)
-        if tree != px.Tracer.TREE_LBVH:
-            t.set_tree(tree)  # the tree the autotuner picked (rebuilt over the uploaded faces)
-        t.set_kernel(chosen)  # the render kernel the autotuner picked for this scene
-        gpu.wait(60000)
-        t1 = time.perf_counter()
-        t.trace(cam, W, H, 0, args.spp)
-        t.denoise()
-        gpu.wait(60000)
-        t2 = time.perf_counter()
-        img = t.pixels()
-        t3 = time.perf_counter()
-        t.close()
-        t4 = time.perf_counter()
-        for k, a, b in (("create_ms", t0, t1), ("trace_denoise_ms", t1, t2), ("read_ms", t2, t3), ("close_ms", t3, t4)):
-            e2e_parts[k] += (b - a) * 1e3
-        return img
-
-    e2e_step()
-    barrier()
-    for k in e2e_parts:
-        e2e_parts[k] = 0.0
-    e2e_steps = max(3, args.steps)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    barrier()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, f"cuda:{local}")
-    e2e = whole_job_rate(rays_per_frame, world, e2e_s * 1e3) / 1e6
 
     denoised = None if args.no_denoised else equal_relmse(args, gpu, s, cam, stream, chosen)
 
@@ -870,8 +874,9 @@ def main() -> None:
                          "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "steps": e2e_steps,
-                    "phases_ms": {k: round(v / e2e_steps, 1) for k, v in e2e_parts.items()}},
+                    "steps": e2e_steps, "step_ms": [round(v, 1) for v in e2e_each],
+                    "phases_ms": {k: round(v / e2e_steps, 1) for k, v in e2e_parts.items()},
+                    "clocks": e2e_clk.summary()},
             "denoised": denoised,
             "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
