@@ -1,8 +1,9 @@
 """Parity at the benchmark configurations' own sizes.
 
 C2 as the bench times it — the 1,310,722-face displaced icosphere, 1920 x
-1080, 8 bounces — traced whole on the GPU and compared with the oracle on
-a band of rows spread over the frame (every px plane word of those rows),
+1080, 8 bounces, on the LBVH and on the binned SAH tree — traced whole on
+the GPU and compared with the oracle on a band of rows spread over the
+frame (every px plane word of those rows),
 plus every primary hit id of the 1080p frame. C3 as configured — 500,000
 vertices (+ 4 of the ground), 999,002 faces, 64 bones, 1-4 influences a vertex — Skin, face
 boxes and the LBVH refit, each bit for bit against the oracle, and the
@@ -41,16 +42,20 @@ def c2():
     return scenes.c2_mesh()
 
 
-def test_c2_1080p_rows_match_oracle(gpu, orc, c2):
+@pytest.mark.parametrize("tree", [0, 1], ids=["lbvh", "sah"])
+def test_c2_1080p_rows_match_oracle(gpu, orc, c2, tree):
+    """On either tree; the SAH tree is the one the bench's autotuner picks
+    for this frame, so this is the headline step's image."""
     s = c2
     w, h, spp = 1920, 1080, 2
     cam = cam_of(s, w, h)
     rows = np.linspace(0, h - 1, 40).round().astype(int).tolist()
-    T = oracle_lib.TraceOracle(orc, s)
+    T = oracle_lib.TraceOracle(orc, s, sah=bool(tree))
     want = np.zeros(34 * w * h + 1, np.uint32)
     for r in rows:
         T.trace(cam, 0, spp, px=want, rows=(r, 1))
     tr = px.Tracer.of(gpu, s)
+    tr.set_tree(tree)
     tr.autotune(cam, w, h, 1)  # the form the bench picks
     tr.trace(cam, w, h, 0, spp)
     rows_equal(tr.image(), want, w, w * h, rows)
