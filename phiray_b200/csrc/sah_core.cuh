@@ -233,6 +233,7 @@ SAH_HD Decision decide_occupied(const uint32_t* mask, const uint32_t (*bcount)[B
 SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots, uint32_t count, uint32_t leaf) {
     if (count <= 1) return NONE;
     Box cbox = empty_box();
+#pragma unroll 4
     for (uint32_t j = 0; j < count; j++) {
         const float* c = centres + 3 * (uint64_t)slots[j];
         Box p;
@@ -244,6 +245,7 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
     uint32_t mask[3] = {0u, 0u, 0u};
     uint32_t bcount[3][BINS];
     Box bbox[3][BINS];
+#pragma unroll 4
     for (uint32_t j = 0; j < count; j++) {
         const uint32_t i = slots[j];
         const Box pb = prim_box(prims + 8 * (uint64_t)i);
@@ -261,13 +263,25 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
     const Decision d = decide_occupied(mask, bcount, bbox, scale, count, leaf);
     if (d.cut == CUT_LEAF) return NONE;
     if (d.cut == CUT_HALF) return count / 2;
+    // The swap loop, 32 positions at a time: the flags of a run are taken
+    // before its swaps (independent loads), which is exact because the loop
+    // only swaps positions at or before the one it stands on, so a position
+    // still holds its first slot when the loop reaches it.
     uint32_t m = 0;
-    for (uint32_t j = 0; j < count; j++) {
-        if (bin_of(centres + 3 * (uint64_t)slots[j], lo, scale, (int)d.axis) <= d.at) {
-            const uint32_t t = slots[j];
-            slots[j] = slots[m];
-            slots[m] = t;
-            m++;
+    for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t run = count - base < 32u ? count - base : 32u;
+        uint32_t flags = 0;
+#pragma unroll 8
+        for (uint32_t e = 0; e < run; e++)
+            if (bin_of(centres + 3 * (uint64_t)slots[base + e], lo, scale, (int)d.axis) <= d.at) flags |= 1u << e;
+        for (uint32_t e = 0; e < run; e++) {
+            if ((flags >> e) & 1u) {
+                const uint32_t j = base + e;
+                const uint32_t t = slots[j];
+                slots[j] = slots[m];
+                slots[m] = t;
+                m++;
+            }
         }
     }
     return (m == 0 || m == count) ? count / 2 : m;
