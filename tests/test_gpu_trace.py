@@ -424,3 +424,28 @@ def test_create_refuses_scenes_the_tracer_does_not_take(gpu):
             px.Tracer(gpu, v, f, m)
         assert e.value.code == px._native.PHX_ERR_INVALID, what
     px.Tracer.of(gpu, s).close()  # the context is still good
+
+
+@pytest.mark.parametrize("mode", [3, 4], ids=["persistent", "thread_per_ray"])
+def test_wide_walk_when_the_root_is_a_leaf(gpu, orc, mode):
+    """A scene of one face: the tree is a single leaf, the wide tree has no
+    node, and the wide walks test the leaf as the binary walk does."""
+    import torch
+
+    from tests import pins
+
+    a, _ = pins.card()
+    s = pins.single_triangle_scene(a)
+    rays = np.zeros((len(pins.edge_rays(2000)), 8), np.float32)
+    for k, (o, d) in enumerate(pins.edge_rays(2000)):
+        rays[k, 0:3], rays[k, 3], rays[k, 4:7] = o, 3.0e38, d
+    tr = px.Tracer.of(gpu, s)
+    tr.set_walk(mode)
+    n = len(rays)
+    dr = torch.tensor(rays, device="cuda")
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    tr.trace_rays(dr, n, hits)
+    gpu.wait()
+    want = oracle_lib.TraceOracle(orc, s).trace_rays(rays)
+    assert np.array_equal(hits.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    tr.close()
