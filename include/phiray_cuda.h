@@ -218,8 +218,8 @@ typedef struct phx_bvh_s* phx_bvh;
  * numbering, bounds refit bottom up. All pointers are DEVICE memory:
  * prims (n phx_aabb), nodes (room for 2n - 1), order (n). Writes the node
  * count and depth; stream-ordered, waits once or twice per tree level.
- * Nodes under 128 slots are a thread's, 128-2,047 a block's, larger ones are
- * cut over blocks of 2,048 slots (1.3 M prims: ~10 ms). */
+ * Nodes under 64 slots are a thread's, 64-2,047 a block's, larger ones are
+ * cut over blocks of 2,048 slots (1.3 M prims: ~9 ms). */
 int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32_t leaf, phx_node* nodes,
                           uint32_t* order, uint32_t* node_count, uint32_t* depth);
 
@@ -512,7 +512,7 @@ int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
  * faces). PHX_TREE_SAH: the binned SAH tree phiray's own tracer builds
  * (src/bvh/sah.rs:85-189, forest.rs:49), node for node, built on the device
  * by phx_bvh_build_sah — fewer node steps and triangle tests a ray, a
- * longer build (1.3 M faces: ~10 ms against 0.5 ms). Closest hits do not
+ * longer build (1.3 M faces: ~9 ms against 0.5 ms). Closest hits do not
  * depend on the tree (a tie between two
  * faces at the same t aside). Rebuilds the tree now over the current
  * vertices (waits); the image starts over; a repose then refits or rebuilds

@@ -10,8 +10,9 @@
 // and a last bottom-up pass writes the nodes with their bounds.
 //
 // Nodes under MID slots are one thread each, running the per-node code of
-// sah_core.cuh; nodes of MID to BIG slots a block each (bins by shared-memory
-// atomics, the swap loop's result by the queue model below, in shared memory). Nodes of BIG slots or more —
+// sah_core.cuh; nodes of MID to BIG slots a block each (64 threads up to
+// LARGE slots, 256 above; bins by shared-memory atomics, the swap loop's
+// result by the queue model below, in shared memory). Nodes of BIG slots or more —
 // the top levels, where a node a thread or warp would leave the GPU idle —
 // are cut over blocks of CHUNK slots: the box of centres and the bins are min/max and count reductions
 // (exact in any order) merged with atomics; one thread a node then makes
@@ -98,8 +99,9 @@ __device__ __forceinline__ float unord(uint32_t w) {
     return __uint_as_float((w & 0x80000000u) ? (w & 0x7FFFFFFFu) : ~w);
 }
 
+template <int THREADS = CHUNK_THREADS>
 __device__ __forceinline__ uint32_t block_sum_exclusive(uint32_t v, uint32_t* total) {
-    __shared__ uint32_t s_warp[CHUNK_THREADS / 32];
+    __shared__ uint32_t s_warp[THREADS / 32];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t x = v;
     for (int o = 1; o < 32; o <<= 1) {
@@ -109,27 +111,28 @@ __device__ __forceinline__ uint32_t block_sum_exclusive(uint32_t v, uint32_t* to
     if (lane == 31) s_warp[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < CHUNK_THREADS / 32 ? s_warp[lane] : 0u;
+        uint32_t w = lane < THREADS / 32 ? s_warp[lane] : 0u;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= (uint32_t)o) w += y;
         }
-        if (lane < CHUNK_THREADS / 32) s_warp[lane] = w;
+        if (lane < THREADS / 32) s_warp[lane] = w;
     }
     __syncthreads();
     const uint32_t before = (warp ? s_warp[warp - 1] : 0u) + x - v;
-    *total = s_warp[CHUNK_THREADS / 32 - 1];
+    *total = s_warp[THREADS / 32 - 1];
     __syncthreads();
     return before;
 }
 
 // ---- nodes of MID to BIG slots: a block a node ----
 
-constexpr uint32_t MID = 128;
-constexpr uint32_t NODE_THREADS = 256;
-constexpr uint32_t NODE_ITEMS = BIG / NODE_THREADS;  // slots a thread holds
-static_assert(NODE_THREADS * NODE_ITEMS == BIG, "a block holds a node of up to BIG slots");
-static_assert(NODE_THREADS == CHUNK_THREADS, "block_sum_exclusive is written for CHUNK_THREADS");
+// Two block forms: 256 threads for nodes of LARGE to BIG slots, 64 threads
+// for nodes of MID to LARGE (8 slots a thread either way).
+constexpr uint32_t MID = 64;
+constexpr uint32_t LARGE = 512;
+constexpr uint32_t NODE_ITEMS = 8;  // slots a thread holds
+static_assert(256 * NODE_ITEMS == BIG && 64 * NODE_ITEMS == LARGE, "a block holds its largest node");
 
 // sah_core.cuh process for one node by a block: each thread holds 8 of the
 // node's slots in registers; the box of centres by block reduction, the bins
@@ -140,15 +143,15 @@ static_assert(NODE_THREADS == CHUNK_THREADS, "block_sum_exclusive is written for
 // log's links, pointer jumping in place: a link only ever moves to an
 // ancestor on its own chain, so reading a neighbour's already-updated link
 // only shortens the chase).
-__global__ void __launch_bounds__(NODE_THREADS, 2) k_sah_block(const uint32_t* __restrict__ list, TNode* tn,
-                                                            const float* __restrict__ prims,
-                                                            const float* __restrict__ centres, uint32_t* order,
-                                                            uint32_t leaf, uint32_t* tcount, uint32_t* next,
-                                                            uint32_t* next_count) {
+template <int NODE_THREADS>
+__global__ void __launch_bounds__(NODE_THREADS, 512 / NODE_THREADS) k_sah_block(
+    const uint32_t* __restrict__ list, TNode* tn, const float* __restrict__ prims, const float* __restrict__ centres,
+    uint32_t* order, uint32_t leaf, uint32_t* tcount, uint32_t* next, uint32_t* next_count) {
+    constexpr uint32_t CAP = NODE_THREADS * NODE_ITEMS;  // slots the block can hold
     __shared__ uint32_t s_count[HBINS];
     __shared__ uint32_t s_box[6 * HBINS];
-    __shared__ uint16_t s_ptr[BIG];
-    __shared__ uint32_t s_val[BIG];
+    __shared__ uint16_t s_ptr[CAP];
+    __shared__ uint32_t s_val[CAP];
     __shared__ float s_red[6][NODE_THREADS / 32];
     __shared__ sah::AxisBest s_axis[3];
     __shared__ uint32_t s_cut, s_axis_k, s_at, s_first;
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(NODE_THREADS, 2) k_sah_block(const uint32_t* _
     TNode nd = tn[t];
     const uint32_t n = nd.end - nd.start;
     uint32_t m = sah::NONE;
-    if (nd.depth + 1 < sah::MAX_DEPTH && n > 1 && n <= BIG) {
+    if (nd.depth + 1 < sah::MAX_DEPTH && n > 1 && n <= CAP) {
         uint32_t slot[NODE_ITEMS];
         const uint32_t j0 = tid * NODE_ITEMS;
         float lo[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(NODE_THREADS, 2) k_sah_block(const uint32_t* _
                     if (j0 + e < n && !left[e]) atomicMin(&s_first, j0 + e);
                 }
                 uint32_t total = 0;
-                uint32_t lr = block_sum_exclusive(mine, &total);  // (syncs; s_first is settled after it)
+                uint32_t lr = block_sum_exclusive<NODE_THREADS>(mine, &total);  // (syncs; s_first settles)
                 const uint32_t q = total;
                 if (q == 0 || q == n) {
                     m = n / 2;  // no left slot or no right one: the swap loop moved nothing
@@ -319,9 +322,9 @@ __global__ void __launch_bounds__(NODE_THREADS, 2) k_sah_block(const uint32_t* _
 
 // The level's open nodes, split into the big ones (BIG slots or more, not
 // at the depth cap) and the rest.
-// (counts: small, big, mid.)
+// (counts: small, big, mid, large.)
 __global__ void k_sah_classify(const uint32_t* __restrict__ list, uint32_t count, const TNode* __restrict__ tn,
-                               uint32_t* small, uint32_t* big, uint32_t* mid, uint32_t* counts) {
+                               uint32_t* small, uint32_t* big, uint32_t* mid, uint32_t* large, uint32_t* counts) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const uint32_t t = list[k];
@@ -329,6 +332,7 @@ __global__ void k_sah_classify(const uint32_t* __restrict__ list, uint32_t count
     const uint32_t n = nd.end - nd.start;
     const bool open = nd.depth + 1 < sah::MAX_DEPTH;
     if (open && n >= BIG) big[atomicAdd(counts + 1, 1u)] = t;
+    else if (open && n >= LARGE) large[atomicAdd(counts + 3, 1u)] = t;
     else if (open && n >= MID) mid[atomicAdd(counts + 2, 1u)] = t;
     else small[atomicAdd(counts, 1u)] = t;
 }
@@ -670,11 +674,12 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
     // Big-node work arrays (sized for the widest level: at most n / BIG big
     // nodes, n / CHUNK + n / BIG chunks).
     const uint32_t max_big = n / BIG + 1, max_chunks = n / CHUNK + max_big + 1;
-    DevMem small_list, mid_list, big_list, lcounts, bnodes, spans, chunks, rank_w, lefts, offs, out_w, ptr_a, ptr_b,
-        val_w;
+    DevMem small_list, mid_list, large_list, big_list, lcounts, bnodes, spans, chunks, rank_w, lefts, offs, out_w,
+        ptr_a, ptr_b, val_w;
     PHX_TRY(small_list.reserve((size_t)cap * 4));
     PHX_TRY(mid_list.reserve((size_t)(n / MID + 1) * 4));
-    PHX_TRY(lcounts.reserve(12));
+    PHX_TRY(large_list.reserve((size_t)(n / LARGE + 1) * 4));
+    PHX_TRY(lcounts.reserve(16));
     if (n >= BIG) {
         PHX_TRY(spans.reserve((size_t)max_big * 8));
         PHX_TRY(big_list.reserve((size_t)max_big * 4));
@@ -695,17 +700,18 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
         const uint32_t next = off[lv] + len[lv];
         PHX_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, s));
         const uint32_t* level = (const uint32_t*)small_list.ptr;
-        uint32_t nsmall = 0, nmid = 0;
+        uint32_t nsmall = 0, nmid = 0, nlarge = 0;
         {
-            PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 12, s));
+            PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 16, s));
             k_sah_classify<<<blocks_of(len[lv], 256), 256, 0, s>>>(L + off[lv], len[lv], T, (uint32_t*)small_list.ptr,
                                                                    (uint32_t*)big_list.ptr, (uint32_t*)mid_list.ptr,
-                                                                   (uint32_t*)lcounts.ptr);
-            uint32_t lc[3] = {0, 0, 0};
-            PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 12, cudaMemcpyDeviceToHost, s));
+                                                                   (uint32_t*)large_list.ptr, (uint32_t*)lcounts.ptr);
+            uint32_t lc[4] = {0, 0, 0, 0};
+            PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 16, cudaMemcpyDeviceToHost, s));
             PHX_TRY(wait_stream(s, 0));
             nsmall = lc[0];
             nmid = lc[2];
+            nlarge = lc[3];
             const uint32_t nb = lc[1];
             if (nb) {
                 BigNode* BN = (BigNode*)bnodes.ptr;
@@ -749,9 +755,12 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
                 PHX_CUDA(cudaGetLastError());
             }
         }
+        if (nlarge)
+            k_sah_block<256><<<nlarge, 256, 0, s>>>((const uint32_t*)large_list.ptr, T, P, (const float*)centres.ptr,
+                                                    order, leaf, cnt, L + next, cnt + 1);
         if (nmid)
-            k_sah_block<<<nmid, NODE_THREADS, 0, s>>>((const uint32_t*)mid_list.ptr, T, P, (const float*)centres.ptr,
-                                                      order, leaf, cnt, L + next, cnt + 1);
+            k_sah_block<64><<<nmid, 64, 0, s>>>((const uint32_t*)mid_list.ptr, T, P, (const float*)centres.ptr, order,
+                                                leaf, cnt, L + next, cnt + 1);
         if (nsmall)
             k_sah_thread<<<blocks_of(nsmall, 64), 64, 0, s>>>(level, nsmall, T, P, (const float*)centres.ptr, order,
                                                               leaf, cnt, L + next, cnt + 1);
