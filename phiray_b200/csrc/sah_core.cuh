@@ -242,25 +242,36 @@ SAH_HD uint32_t split(const float* prims, const float* centres, uint32_t* slots,
     }
     float lo[3], scale[3];
     if (!grid_of(cbox, lo, scale)) return count > leaf ? count / 2 : NONE;
-    uint32_t mask[3] = {0u, 0u, 0u};
-    uint32_t bcount[3][BINS];
-    Box bbox[3][BINS];
+    // One axis at a time (its 16 bins, then its sweep), so a thread keeps a
+    // third of the bins live; the bins of an axis and the decision are those
+    // of all three filled together.
+    AxisBest axes[3];
+    Box bounds = empty_box();
+    for (int k = 0; k < 3; k++) {
+        axes[k] = AxisBest{false, 0.0f, 0u};
+        if (scale[k] == 0.0f && k != 0) continue;  // (axis 0's bins give the node's bounds)
+        uint32_t mask = 0u;
+        uint32_t bcount[BINS];
+        Box bbox[BINS];
 #pragma unroll 4
-    for (uint32_t j = 0; j < count; j++) {
-        const uint32_t i = slots[j];
-        const Box pb = prim_box(prims + 8 * (uint64_t)i);
-        for (int k = 0; k < 3; k++) {
+        for (uint32_t j = 0; j < count; j++) {
+            const uint32_t i = slots[j];
             const uint32_t at = bin_of(centres + 3 * (uint64_t)i, lo, scale, k);
-            if (!((mask[k] >> at) & 1u)) {
-                mask[k] |= 1u << at;
-                bcount[k][at] = 0;
-                bbox[k][at] = empty_box();
+            const Box pb = prim_box(prims + 8 * (uint64_t)i);
+            if (!((mask >> at) & 1u)) {
+                mask |= 1u << at;
+                bcount[at] = 0;
+                bbox[at] = empty_box();
             }
-            bcount[k][at] += 1;
-            grow(bbox[k][at], pb);
+            bcount[at] += 1;
+            grow(bbox[at], pb);
         }
+        if (k == 0)
+            for (uint32_t b = 0; b < BINS; b++)
+                if ((mask >> b) & 1u) grow(bounds, bbox[b]);
+        if (scale[k] != 0.0f) axes[k] = sweep_axis(mask, bcount, bbox);
     }
-    const Decision d = decide_occupied(mask, bcount, bbox, scale, count, leaf);
+    const Decision d = decide_from(axes, scale, bounds, count, leaf);
     if (d.cut == CUT_LEAF) return NONE;
     if (d.cut == CUT_HALF) return count / 2;
     // The swap loop, 32 positions at a time: the flags of a run are taken
