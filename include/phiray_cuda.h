@@ -521,7 +521,7 @@ int32_t phx_tracer_set_walk(phx_tracer tr, uint32_t mode);
 #define PHX_TREE_LBVH 0u
 #define PHX_TREE_SAH 1u
 int32_t phx_tracer_set_tree(phx_tracer tr, uint32_t tree);
-/* The autotuner over trees: builds each (timed), traces `spp` samples of
+/* The autotuner over trees: builds each (timed, after an untimed build), traces `spp` samples of
  * `cam` on it (timed, after a warm-up trace) and keeps the one with the lower
  * build + frames x trace time — the SAH tree where the trace time of the
  * frames to come outweighs its build. ms (4 floats, may be NULL): LBVH build,

@@ -1370,8 +1370,11 @@ int32_t phx_tracer_autotune_tree(phx_tracer tr, const phx_camera* cam, uint32_t 
     int32_t rc = PHX_OK;
     for (uint32_t k = 0; k < 2 && rc == PHX_OK; k++) {
         // build (from the face boxes), then a trace of spp samples, each timed
+        // after an untimed one (a process's first build of a kind also pays
+        // one-time costs: kernel loading, pool growth)
         const uint32_t tree = k == 0 ? PHX_TREE_LBVH : PHX_TREE_SAH;
-        rc = cuda_check(cudaEventRecord(a, s), "event");
+        rc = phx_tracer_set_tree(tr, tree);
+        if (rc == PHX_OK) rc = cuda_check(cudaEventRecord(a, s), "event");
         if (rc == PHX_OK) rc = phx_tracer_set_tree(tr, tree);
         if (rc == PHX_OK) rc = cuda_check(cudaEventRecord(b, s), "event");
         if (rc == PHX_OK) rc = wait_stream(s, 0);
