@@ -191,7 +191,7 @@ def test_pass_replays_reference_kernels(gpu, orc):
     assert ps.compiled() == 1
 
 
-@pytest.mark.parametrize("n", [1, 2, 7, 5000, 70000])
+@pytest.mark.parametrize("n", [1, 2, 7, 100, 600, 5000, 70000])
 @pytest.mark.parametrize("leaf", [0, 1, 4])
 def test_sah_build_equals_the_reference_tree(gpu, orc, n, leaf):
     """phx_bvh_build_sah == Bvh::build_sah's restatement, word for word:
