@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128, 8) k_rays_wide_thread(Scene S, const floa
     }
 }
 
-constexpr int WIDE_STEPS = 12;
+constexpr int WIDE_STEPS = 20;  // visits a round: 12-24 swept on the C2 bounce rays, 20 fastest
 
 // k_rays_fetch's persistent warps over the wide tree: each lane walks one
 // ray nearest child first (four slab tests a step, the hit children sorted
