@@ -243,7 +243,8 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
 def run_c3(args) -> None:
     """The skinned-animation configuration: 500k vertices / ~1M faces, 64
     bones; per frame Skin -> face boxes -> LBVH refit (or full rebuild) ->
-    trace 1080p at 16 spp. Prints per-stage ms per frame (device events)."""
+    trace 1080p at 16 spp, and the same on the binned SAH tree. Prints
+    per-stage ms per frame (device events)."""
     import torch
 
     import phiray_b200 as px
@@ -262,8 +263,13 @@ def run_c3(args) -> None:
     bones = [torch.tensor(rig.bones(f), device="cuda") for f in range(frames)]
     gpu.wait(60000)
     torch.cuda.synchronize()
+    # the render kernel for this scene, as the C2 leg picks it (same image)
+    chosen, _ = tr.autotune(cam, s.width, s.height, 4)
     res = {}
-    for mode in ("refit", "rebuild"):
+    # the configuration's LBVH refit and rebuild, then the same over the
+    # binned SAH tree (its Jacobi refit, its device rebuild)
+    for mode in ("refit", "rebuild", "sah_refit", "sah_rebuild"):
+        tr.set_tree(px.Tracer.TREE_SAH if mode.startswith("sah") else px.Tracer.TREE_LBVH)
         ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(frames)]
         rays = 0
         for f in range(frames + args.warmup):
@@ -274,7 +280,7 @@ def run_c3(args) -> None:
             px.skin(gpu, dev["rest"], dev["offsets"], dev["pairs"], bones[f % frames], rig.nbones, vptr, nv, 1e-4)
             if e:
                 e[1].record(st)
-            tr.repose_device(vptr, rebuild=(mode == "rebuild"))
+            tr.repose_device(vptr, rebuild=mode.endswith("rebuild"))
             if e:
                 e[2].record(st)
             tr.trace(cam, s.width, s.height, 0, s.spp)
@@ -292,7 +298,7 @@ def run_c3(args) -> None:
                      "frame_ms": round(statistics.mean(skin) + statistics.mean(bvh) + statistics.mean(trace), 3)}
     nb = len(rig.rest)
     out = {"workload": "c3_skinned: 500k verts / 999k tris, 64 bones, 1-4 influences, 1080p 16 spp",
-           "frames": frames, "per_frame": res,
+           "frames": frames, "per_frame": res, "render_kernel": KERNEL_NAMES[chosen],
            "skin_gbs": round((16 + 4 + 16 * len(rig.pairs) / nb + 16) * nb / (res["refit"]["skin_ms"] * 1e-3) / 1e9, 1)}
     print(json.dumps(out), flush=True)
     gpu.close()
