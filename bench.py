@@ -774,7 +774,7 @@ def main() -> None:
     barrier()
     for k in e2e_parts:
         e2e_parts[k] = 0.0
-    e2e_steps = max(3, args.steps)
+    e2e_steps = max(7, args.steps)
     e2e_each = []
     with Clocks(local) as e2e_clk:
         t0 = time.perf_counter()
@@ -783,8 +783,13 @@ def main() -> None:
             e2e_step()
             e2e_each.append((time.perf_counter() - ts) * 1e3)
         barrier()
-        e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, f"cuda:{local}")
+        e2e_mean_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, f"cuda:{local}")
+        # the median step: one step held up by something outside this process
+        # (seen once at 906 ms against 219 ms, clocks steady) does not decide
+        # the figure; the mean is printed beside it
+        e2e_s = max_over_ranks(statistics.median(e2e_each) * 1e-3, f"cuda:{local}")
     e2e = whole_job_rate(rays_per_frame, world, e2e_s * 1e3) / 1e6
+    e2e_mean = whole_job_rate(rays_per_frame, world, e2e_mean_s * 1e3) / 1e6
 
     # Phase timings (same device, outside the headline loop).
     def timed(fn, reps):
@@ -880,6 +885,7 @@ def main() -> None:
                          "algorithmic": f"{counts[1]} node steps x 64 B + {counts[2]} triangle tests x 48 B per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "statistic": "median step", "mean_value": round(e2e_mean, 2),
                     "steps": e2e_steps, "step_ms": [round(v, 1) for v in e2e_each],
                     "phases_ms": {k: round(v / e2e_steps, 1) for k, v in e2e_parts.items()},
                     "clocks": e2e_clk.summary()},
