@@ -322,10 +322,16 @@ __global__ void __launch_bounds__(NODE_THREADS, 512 / NODE_THREADS) k_sah_block(
 
 // The level's open nodes, split into the big ones (BIG slots or more, not
 // at the depth cap) and the rest.
-// (counts: small, big, mid, large.)
-__global__ void k_sah_classify(const uint32_t* __restrict__ list, uint32_t count, const TNode* __restrict__ tn,
-                               uint32_t* small, uint32_t* big, uint32_t* mid, uint32_t* large, uint32_t* counts) {
+// (counts: small, big, mid, large, and in counts[4] the level's length.)
+// The length is `count`, or *dcount when given: the children the level
+// before opened, so the host learns them with this level's counts, in one
+// wait; the grid then covers an upper bound.
+__global__ void k_sah_classify(const uint32_t* __restrict__ list, uint32_t count, const uint32_t* dcount,
+                               const TNode* __restrict__ tn, uint32_t* small, uint32_t* big, uint32_t* mid,
+                               uint32_t* large, uint32_t* counts) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (dcount) count = *dcount;
+    if (k == 0) counts[4] = count;
     if (k >= count) return;
     const uint32_t t = list[k];
     const TNode nd = tn[t];
@@ -679,7 +685,7 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
     PHX_TRY(small_list.reserve((size_t)cap * 4));
     PHX_TRY(mid_list.reserve((size_t)(n / MID + 1) * 4));
     PHX_TRY(large_list.reserve((size_t)(n / LARGE + 1) * 4));
-    PHX_TRY(lcounts.reserve(16));
+    PHX_TRY(lcounts.reserve(20));
     if (n >= BIG) {
         PHX_TRY(spans.reserve((size_t)max_big * 8));
         PHX_TRY(big_list.reserve((size_t)max_big * 4));
@@ -696,19 +702,29 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
     std::vector<uint32_t> off{0}, len{1};
     std::vector<uint2> host_big;
     std::vector<Chunk> host_chunks;
+    // Level 0's classification; each level then classifies the next one
+    // right behind its own kernels, and one wait a level reads both the
+    // children opened and their classes.
+    PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 16, s));
+    k_sah_classify<<<1, 256, 0, s>>>(L, 1u, nullptr, T, (uint32_t*)small_list.ptr, (uint32_t*)big_list.ptr,
+                                     (uint32_t*)mid_list.ptr, (uint32_t*)large_list.ptr, (uint32_t*)lcounts.ptr);
     for (uint32_t lv = 0; lv < sah::MAX_DEPTH; lv++) {
+        uint32_t lc[5] = {0, 0, 0, 0, 0};
+        PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 20, cudaMemcpyDeviceToHost, s));
+        PHX_TRY(wait_stream(s, 0));
+        if (lv > 0) {
+            // lc[4]: the children the level before opened (this level's length)
+            if (lc[4] == 0) break;
+            const uint32_t at = off[lv - 1] + len[lv - 1];
+            if (at + lc[4] > cap) return fail(PHX_ERR_DEVICE, "SAH build: more nodes than 2n - 1");
+            off.push_back(at);
+            len.push_back(lc[4]);
+        }
         const uint32_t next = off[lv] + len[lv];
         PHX_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, s));
         const uint32_t* level = (const uint32_t*)small_list.ptr;
         uint32_t nsmall = 0, nmid = 0, nlarge = 0;
         {
-            PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 16, s));
-            k_sah_classify<<<blocks_of(len[lv], 256), 256, 0, s>>>(L + off[lv], len[lv], T, (uint32_t*)small_list.ptr,
-                                                                   (uint32_t*)big_list.ptr, (uint32_t*)mid_list.ptr,
-                                                                   (uint32_t*)large_list.ptr, (uint32_t*)lcounts.ptr);
-            uint32_t lc[4] = {0, 0, 0, 0};
-            PHX_CUDA(cudaMemcpyAsync(lc, lcounts.ptr, 16, cudaMemcpyDeviceToHost, s));
-            PHX_TRY(wait_stream(s, 0));
             nsmall = lc[0];
             nmid = lc[2];
             nlarge = lc[3];
@@ -765,13 +781,13 @@ int32_t phx_bvh_build_sah(phx_ctx ctx, const phx_aabb* prims, uint32_t n, uint32
             k_sah_thread<<<blocks_of(nsmall, 64), 64, 0, s>>>(level, nsmall, T, P, (const float*)centres.ptr, order,
                                                               leaf, cnt, L + next, cnt + 1);
         PHX_CUDA(cudaGetLastError());
-        uint32_t opened = 0;
-        PHX_CUDA(cudaMemcpyAsync(&opened, cnt + 1, 4, cudaMemcpyDeviceToHost, s));
-        PHX_TRY(wait_stream(s, 0));
-        if (opened == 0) break;
-        if (next + opened > cap) return fail(PHX_ERR_DEVICE, "SAH build: more nodes than 2n - 1");
-        off.push_back(next);
-        len.push_back(opened);
+        // the next level: its length is the children just opened (cnt[1]);
+        // at most two a node of this level
+        PHX_CUDA(cudaMemsetAsync(lcounts.ptr, 0, 16, s));
+        k_sah_classify<<<blocks_of(2 * len[lv], 256), 256, 0, s>>>(
+            L + next, 0u, cnt + 1, T, (uint32_t*)small_list.ptr, (uint32_t*)big_list.ptr, (uint32_t*)mid_list.ptr,
+            (uint32_t*)large_list.ptr, (uint32_t*)lcounts.ptr);
+        PHX_CUDA(cudaGetLastError());
     }
     const uint32_t levels = (uint32_t)len.size();
     for (uint32_t lv = levels; lv-- > 0;)
