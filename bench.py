@@ -43,7 +43,8 @@ WORKLOAD = ("c2_mesh: icosphere L8 (1,310,722 tris) + 4 area lights, 1920x1080, 
 
 KERNEL_NAMES = ["megakernel", "state-machine/4", "state-machine/6", "state-machine/8", "megakernel/3", "megakernel/2",
                 "megakernel/sync", "megakernel/2/sync", "megakernel/5", "megakernel/6", "megakernel/6/sync", "megakernel/8", "megakernel/8/sync",
-                "megakernel/10/sync", "megakernel/12/sync", "megakernel/16/sync", "wavefront"]
+                "megakernel/10/sync", "megakernel/12/sync", "megakernel/16/sync", "wavefront",
+                "megakernel/reg8", "megakernel/8/sync/reg1", "megakernel/16/sync/reg1"]
 
 
 def peaks() -> dict:
@@ -229,6 +230,7 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
         hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
         tr.secondary_rays(cam, W, H, 0, rays)
         tr.set_walk(args.walk)
+        tr.set_stack(args.stack)
         fn = lambda: tr.trace_rays(rays, n, hits, False)  # noqa: E731
     for _ in range(args.warmup):
         fn()
@@ -656,6 +658,8 @@ def main() -> None:
     ap.add_argument("--walk", type=int, default=0,
                     help="ray walk of --phase rays: 0 a thread per ray, 1 persistent, 2 sorted, 3 the 4-wide tree "
                          "(persistent), 4 the 4-wide tree (a thread per ray)")
+    ap.add_argument("--stack", type=int, default=0,
+                    help="stack placement of --phase rays thread-per-ray walks: 0 local, 1 shared, 2 registers")
     ap.add_argument("--tree", type=int, default=0, help="tree of --phase runs: 0 the LBVH, 1 the binned SAH tree")
     ap.add_argument("--kernel", type=int, default=-1,
                     help="render kernel id of --phase render (KERNEL_NAMES order; default: the tracer's default)")
@@ -814,24 +818,32 @@ def main() -> None:
     hits = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
     tr.secondary_rays(cam, W, H, 0, rays)
     walk_ms = {}
-    walks = {"thread_per_ray": px.Tracer.WALK_THREAD, "persistent_fetch": px.Tracer.WALK_FETCH,
-             "sorted_fetch": px.Tracer.WALK_SORTED, "wide_fetch": px.Tracer.WALK_WIDE,
-             "wide_thread_per_ray": px.Tracer.WALK_WIDE_THREAD}
+    # (walk schedule, stack placement of the thread-per-ray walk)
+    walks = {"thread_per_ray": (px.Tracer.WALK_THREAD, px.Tracer.STACK_LOCAL),
+             "thread_per_ray_shared_stack": (px.Tracer.WALK_THREAD, px.Tracer.STACK_SHARED),
+             "thread_per_ray_register_stack": (px.Tracer.WALK_THREAD, px.Tracer.STACK_REGISTER),
+             "persistent_fetch": (px.Tracer.WALK_FETCH, px.Tracer.STACK_LOCAL),
+             "sorted_fetch": (px.Tracer.WALK_SORTED, px.Tracer.STACK_LOCAL),
+             "wide_fetch": (px.Tracer.WALK_WIDE, px.Tracer.STACK_LOCAL),
+             "wide_thread_per_ray": (px.Tracer.WALK_WIDE_THREAD, px.Tracer.STACK_LOCAL)}
     tree_names = {px.Tracer.TREE_LBVH: "lbvh", px.Tracer.TREE_SAH: "sah"}
     for t_kind in (px.Tracer.TREE_LBVH, px.Tracer.TREE_SAH):
         tr.set_tree(t_kind)
-        for name, mode in walks.items():
+        for name, (mode, place) in walks.items():
             tr.set_walk(mode)
+            tr.set_stack(place)
             tr.trace_rays(rays, n, hits, False)  # (the wide walk collapses its tree here, untimed)
             walk_ms[f"{tree_names[t_kind]}/{name}"] = timed(lambda: tr.trace_rays(rays, n, hits, False), 10)
     best_walk = min(walk_ms, key=walk_ms.get)
     inc_ms = walk_ms[best_walk]
     tr.set_tree({"lbvh": px.Tracer.TREE_LBVH, "sah": px.Tracer.TREE_SAH}[best_walk.split("/")[0]])
-    tr.set_walk(walks[best_walk.split("/")[1]])
+    tr.set_walk(walks[best_walk.split("/")[1]][0])
+    tr.set_stack(walks[best_walk.split("/")[1]][1])
     _, inc_steps, inc_tests = tr.trace_rays_stats(rays, n, hits, False)
     node_bytes = 128 if "/wide" in best_walk else 64
     inc_bytes = inc_steps * node_bytes + inc_tests * 48
     tr.set_walk(px.Tracer.WALK_THREAD)
+    tr.set_stack(px.Tracer.STACK_LOCAL)
     tr.set_tree(tree)
     ids = torch.empty(n, dtype=torch.int32, device=f"cuda:{local}")
     ts = torch.empty(n, dtype=torch.float32, device=f"cuda:{local}")

@@ -471,8 +471,16 @@ int32_t phx_tracer_destroy(phx_tracer tr);
  * logic; the host polls the queues every fourth pass. Not inside a graph
  * capture nor with adaptive sampling (the megakernel runs those frames). */
 #define PHX_KERNEL_WAVEFRONT 16u
+/* The megakernel whose walk keeps the top of its 32-entry stack in
+ * registers (older entries spill to local memory, a pop refilling the
+ * registers ahead of use): 8 register entries at 4 resident blocks (128
+ * registers a thread), the top entry at 8 and at 16 resident blocks with the
+ * per-sample warp wait. */
+#define PHX_KERNEL_MEGAKERNEL_REG 17u
+#define PHX_KERNEL_MEGAKERNEL_8_SYNC_REG 18u
+#define PHX_KERNEL_MEGAKERNEL_16_SYNC_REG 19u
 /* Number of render kernel ids (the length of phx_tracer_autotune's ms). */
-#define PHX_KERNEL_COUNT 17u
+#define PHX_KERNEL_COUNT 20u
 int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
 /* The autotuner: times every render kernel (and register budget) above on
  * `spp` samples of this scene and camera, keeps the fastest for the tracer
@@ -480,11 +488,16 @@ int32_t phx_tracer_set_kernel(phx_tracer tr, uint32_t kernel);
  * image is overwritten (the next sample starts over). Waits. */
 int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, uint32_t h, uint32_t spp,
                             uint32_t* chosen, float* ms);
-/* Where ray-buffer walks (phx_trace_rays) keep their 32-entry stack:
- * PHX_STACK_LOCAL (per-thread local memory, the default) or PHX_STACK_SHARED
- * (a column of a block-wide shared-memory array). Same hits either way. */
+/* Where thread-per-ray walks (phx_trace_rays under PHX_WALK_THREAD) keep
+ * their 32-entry stack: PHX_STACK_LOCAL (per-thread local memory, the
+ * default), PHX_STACK_SHARED (a column of a block-wide shared-memory array)
+ * or PHX_STACK_REGISTER (the top entry in a register, the older ones in
+ * local memory, a pop loading the next entry ahead of use). Same hits in
+ * every placement. Batches take LOCAL or
+ * SHARED (phx_batch_set_config). */
 #define PHX_STACK_LOCAL 0u
 #define PHX_STACK_SHARED 1u
+#define PHX_STACK_REGISTER 2u
 int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place);
 /* How ray-buffer walks (phx_trace_rays) are scheduled: PHX_WALK_THREAD, one
  * thread per ray (the default); PHX_WALK_FETCH, persistent warps whose idle

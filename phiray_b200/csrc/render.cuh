@@ -47,10 +47,12 @@ constexpr uint32_t WF_SLOTS = 1u << 20;  // path slots of the wavefront render (
 uint32_t wf_slot_words();
 
 // The single-instance render kernels by id: ids 0 and 4-8 (render_flat_a.cu),
-// 9-12 (render_flat_b.cu), 13-15 (render_flat_c.cu), 1-3 (render_sm.cu).
+// 9-12 (render_flat_b.cu), 13-15 (render_flat_c.cu), 17-19 (render_flat_r.cu),
+// 1-3 (render_sm.cu).
 int32_t render_flat_a(uint32_t kernel, bool stats, const RenderLaunch& L);
 int32_t render_flat_b(uint32_t kernel, bool stats, const RenderLaunch& L);
 int32_t render_flat_c(uint32_t kernel, bool stats, const RenderLaunch& L);
+int32_t render_flat_r(uint32_t kernel, bool stats, const RenderLaunch& L);
 int32_t render_flat_sm(uint32_t kernel, bool stats, const RenderLaunch& L);
 // Scenes of instances and frames with the floor grid (render_full.cu).
 int32_t render_full(uint32_t kernel, bool stats, const RenderLaunch& L);
@@ -1441,7 +1443,9 @@ int32_t launch_wf(const RenderLaunch& L, const WfBuffers& B) {
 template <int M>
 int32_t launch_placed(uint32_t kernel, const RenderLaunch& L) {
     if (kernel >= PHX_KERNEL_STATE_MACHINE && kernel <= PHX_KERNEL_STATE_MACHINE_8) return launch_sm<M, 4>(L);
-    if (kernel >= PHX_KERNEL_MEGAKERNEL_8 && kernel <= PHX_KERNEL_MEGAKERNEL_16_SYNC) return launch_mk<M, 16, true>(L);
+    if ((kernel >= PHX_KERNEL_MEGAKERNEL_8 && kernel <= PHX_KERNEL_MEGAKERNEL_16_SYNC) ||
+        kernel == PHX_KERNEL_MEGAKERNEL_8_SYNC_REG || kernel == PHX_KERNEL_MEGAKERNEL_16_SYNC_REG)
+        return launch_mk<M, 16, true>(L);
     return launch_mk<M, 4, false>(L);
 }
 

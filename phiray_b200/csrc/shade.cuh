@@ -104,6 +104,19 @@ struct Count {
 constexpr int MODE_STATS = 1;
 constexpr int MODE_FULL = 2;
 constexpr int MODE_ANY = MODE_FULL;  // code that takes any scene
+// Bits 2 and 3 place the single-instance walk's stack: its top entry (REG)
+// or top 8 entries (REG | REG8) in registers, the rest in local memory.
+constexpr int MODE_REG = 4;
+constexpr int MODE_REG8 = 8;
+
+// Where a walk keeps its 32-entry stack: a per-thread local array, this
+// thread's column of a block-wide shared array, or a short stack of R
+// registers over a local array (place REG_BASE + R).
+constexpr int PLACE_LOCAL = 0;
+constexpr int PLACE_SHARED = 1;
+constexpr int PLACE_REG_BASE = 16;
+template <int M>
+constexpr int PLACE_OF_MODE = (M & MODE_REG) ? PLACE_REG_BASE + ((M & MODE_REG8) ? 8 : 1) : PLACE_LOCAL;
 
 struct Frame {
     uint32_t w, h, n, frame0, spp, persp, count, bounces;
@@ -238,28 +251,80 @@ __device__ __forceinline__ Tree tree_of(const Scene& S) {
     return Tree{S.nodes, S.tris, S.nslots, S.root, S.root_lo, S.root_hi};
 }
 
-// The traversal stack: a per-thread array in local memory, or (SMEM) this
-// thread's column of a block-wide shared array, entry k at stk[k * stride].
-template <bool SMEM>
+// The traversal stack at placement P: a per-thread array in local memory,
+// this thread's column of a block-wide shared array (entry k at
+// shared[k * stride]), or a short stack whose top R entries sit in registers
+// and whose older entries spill to a local array. Every placement pops in
+// the same last-in first-out order and holds at most STACK entries (a push
+// onto a full stack is dropped), so the walk visits the same nodes.
+template <int P, bool REG = (P >= PLACE_REG_BASE)>
 struct Stack {
-    uint32_t local[SMEM ? 1 : STACK];
+    static constexpr int SPILL = 1;  // the caller's spill array: unused here
+    uint32_t local[P == PLACE_SHARED ? 1 : STACK];
     uint32_t* shared;
     int stride;
-    __device__ __forceinline__ uint32_t& at(int k) { return SMEM ? shared[k * stride] : local[k]; }
+    int sp = 0;
+    __device__ __forceinline__ void bind(uint32_t*, uint32_t* smem, int smem_stride) {
+        shared = smem;
+        stride = smem_stride;
+    }
+    __device__ __forceinline__ bool empty() const { return sp == 0; }
+    __device__ __forceinline__ void push(uint32_t x) {
+        if (sp >= STACK) return;
+        if (P == PLACE_SHARED) shared[sp++ * stride] = x;
+        else local[sp++] = x;
+    }
+    __device__ __forceinline__ uint32_t pop() {
+        sp--;
+        return P == PLACE_SHARED ? shared[sp * stride] : local[sp];
+    }
+};
+
+// The register placement keeps its spill array outside the struct (the
+// caller's local array), so the struct's own fields stay in registers. A
+// pop refills the registers from the spill array at once, so that load's
+// latency passes while the popped subtree is walked.
+template <int P>
+struct Stack<P, true> {
+    static constexpr int R = P - PLACE_REG_BASE;
+    static constexpr int SPILL = STACK - R;
+    uint32_t reg[R];
+    uint32_t* spill;
+    int sp = 0;  // entries in the spill array
+    int nr = 0;  // entries in registers
+    __device__ __forceinline__ void bind(uint32_t* s, uint32_t*, int) { spill = s; }
+    __device__ __forceinline__ bool empty() const { return sp + nr == 0; }
+    __device__ __forceinline__ void push(uint32_t x) {
+        if (sp + nr >= STACK) return;
+        // the oldest register entry spills once all R are held
+        if (nr == R) spill[sp++] = reg[R - 1];
+        else nr++;
+#pragma unroll
+        for (int k = R - 1; k > 0; k--) reg[k] = reg[k - 1];
+        reg[0] = x;
+    }
+    __device__ __forceinline__ uint32_t pop() {
+        const uint32_t x = reg[0];
+#pragma unroll
+        for (int k = 0; k < R - 1; k++) reg[k] = reg[k + 1];
+        // the spill array holds entries only while every register is full
+        if (sp > 0) reg[R - 1] = spill[--sp];
+        else nr--;
+        return x;
+    }
 };
 
 // One tree's walk from its root (box test first), improving `best`; true
 // when an any-hit ray found its opaque hit. Hits record `inst`.
-template <bool STATS, bool SMEM = false>
+template <bool STATS, int P = PLACE_LOCAL>
 __device__ __forceinline__ bool walk_tree(const Tree S, f3 o, f3 d, Hit& best, bool first, uint32_t inst, Count& cnt,
                                           uint32_t* smem_stack = nullptr, int stride = 0) {
     const f3 inv = safe_inv(d);
     if (box_t(S.root_lo, S.root_hi, o, inv, best.t) >= INF) return false;
     const RaySpace rs = ray_space(d);
-    Stack<SMEM> stack;
-    stack.shared = smem_stack;
-    stack.stride = stride;
-    int sp = 0;
+    uint32_t spill[Stack<P>::SPILL];
+    Stack<P> stack;
+    stack.bind(spill, smem_stack, stride);
     uint32_t nd = S.root;
     for (;;) {
         if (nd & LEAF) {
@@ -291,9 +356,9 @@ __device__ __forceinline__ bool walk_tree(const Tree S, f3 o, f3 d, Hit& best, b
             const float tr = box_t(mk(n1.z, n1.w, n2.x), mk(n2.y, n2.z, n2.w), o, inv, best.t);
             const uint32_t l = __float_as_uint(n3.x), r = __float_as_uint(n3.y);
             if (tl < INF && tr < INF) {
-                // Depth <= 31 keeps sp below STACK; the check only guards a
-                // corrupt tree from writing past the stack.
-                if (sp < STACK) stack.at(sp++) = tl <= tr ? r : l;
+                // Depth <= 31 keeps the stack below STACK entries; push's
+                // check only guards a corrupt tree from writing past it.
+                stack.push(tl <= tr ? r : l);
                 nd = tl <= tr ? l : r;
                 continue;
             }
@@ -306,20 +371,19 @@ __device__ __forceinline__ bool walk_tree(const Tree S, f3 o, f3 d, Hit& best, b
                 continue;
             }
         }
-        if (sp == 0) break;
-        sp--;
-        nd = stack.at(sp);
+        if (stack.empty()) break;
+        nd = stack.pop();
     }
     return false;
 }
 
 // A ray's walk of a single-instance scene's tree.
-template <bool STATS, bool SMEM = false>
+template <bool STATS, int P = PLACE_LOCAL>
 __device__ __forceinline__ Hit walk(const Tree S, f3 o, f3 d, float tmax, bool first, Count& cnt,
                                     uint32_t* smem_stack = nullptr, int stride = 0) {
     cnt.rays++;
     Hit best{tmax, NONE, 0.0f, 0.0f, 0u};
-    walk_tree<STATS, SMEM>(S, o, d, best, first, 0u, cnt, smem_stack, stride);
+    walk_tree<STATS, P>(S, o, d, best, first, 0u, cnt, smem_stack, stride);
     return best;
 }
 
@@ -330,7 +394,7 @@ __device__ __forceinline__ float row_dir(float4 r, f3 d) { return (r.x * d.x + r
 // space (the ray taken there by the instance's inverse, its direction left
 // unnormalised so t is the world's); a shadow ray passes an instance that
 // casts none. True when an any-hit ray found its hit.
-template <bool STATS, bool SMEM>
+template <bool STATS, int P>
 __device__ __forceinline__ bool walk_instance(const Scene& S, uint32_t i, f3 ow, f3 dw, Hit& best, bool first,
                                               Count& cnt, uint32_t* smem_stack, int stride) {
     const float4* q = S.insts + 8 * (size_t)i;
@@ -345,7 +409,7 @@ __device__ __forceinline__ bool walk_instance(const Scene& S, uint32_t i, f3 ow,
         d = mk(row_dir(i0, dw), row_dir(i1, dw), row_dir(i2, dw));
     }
     const Tree T{S.nodes, S.tris, S.nslots, root, xyz(lo), xyz(hi)};
-    return walk_tree<STATS, SMEM>(T, o, d, best, first, i, cnt, smem_stack, stride);
+    return walk_tree<STATS, P>(T, o, d, best, first, i, cnt, smem_stack, stride);
 }
 
 // trace (bvh.wgsl:194-232) over a scene of instances: the top tree over
@@ -353,7 +417,7 @@ __device__ __forceinline__ bool walk_instance(const Scene& S, uint32_t i, f3 ow,
 // trees in slot order; an any-hit ray stops at its first hit. The top
 // walk's stack is a second 32-entry stack (the reference's trace and
 // trace_blas each keep one).
-template <bool STATS, bool SMEM = false>
+template <bool STATS, int P = PLACE_LOCAL>
 __device__ __forceinline__ Hit walk_forest(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt,
                                            uint32_t* smem_stack = nullptr, int stride = 0) {
     cnt.rays++;
@@ -367,7 +431,7 @@ __device__ __forceinline__ Hit walk_forest(const Scene& S, f3 o, f3 d, float tma
         if (nd & LEAF) {
             for (uint32_t s = nd & ~(LEAF | INST);; s++) {
                 const uint32_t e = __ldg(S.inst_slots + s);
-                if (walk_instance<STATS, SMEM>(S, e & ~INST_END, o, d, best, first, cnt, smem_stack, stride))
+                if (walk_instance<STATS, P>(S, e & ~INST_END, o, d, best, first, cnt, smem_stack, stride))
                     return best;
                 if (e & INST_END) break;
             }
@@ -489,17 +553,17 @@ template <bool STATS>
 __device__ __noinline__ Hit trace_forest(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     if (S.smem_stack) {
         extern __shared__ uint32_t walk_stacks[];
-        return walk_forest<STATS, true>(S, o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
+        return walk_forest<STATS, PLACE_SHARED>(S, o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
     }
     return walk_forest<STATS>(S, o, d, tmax, first, cnt);
 }
 
 // A ray's walk of either kind of scene.
-template <bool STATS, bool SMEM = false>
+template <bool STATS, int P = PLACE_LOCAL>
 __device__ __forceinline__ Hit walk_scene(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt,
                                           uint32_t* smem_stack = nullptr, int stride = 0) {
     if (S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
-    return walk<STATS, SMEM>(tree_of(S), o, d, tmax, first, cnt, smem_stack, stride);
+    return walk<STATS, P>(tree_of(S), o, d, tmax, first, cnt, smem_stack, stride);
 }
 
 // A ray's walk in a render mode: the two-level walk only where the mode
@@ -508,7 +572,7 @@ template <int M>
 __device__ __forceinline__ Hit walk_mode(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     constexpr bool STATS = (M & MODE_STATS) != 0;
     if ((M & MODE_FULL) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
-    return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
+    return walk<STATS, PLACE_OF_MODE<M>>(tree_of(S), o, d, tmax, first, cnt);
 }
 
 // The walk behind a call, for code with several trace sites.
@@ -516,11 +580,16 @@ template <int M>
 __device__ __noinline__ Hit trace(const Scene& S, f3 o, f3 d, float tmax, bool first, Count& cnt) {
     constexpr bool STATS = (M & MODE_STATS) != 0;
     if ((M & MODE_FULL) && S.insts) return trace_forest<STATS>(S, o, d, tmax, first, cnt);
-    if (S.smem_stack) {
-        extern __shared__ uint32_t walk_stacks[];
-        return walk<STATS, true>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x, (int)blockDim.x);
+    if constexpr ((M & MODE_REG) != 0) {
+        return walk<STATS, PLACE_OF_MODE<M>>(tree_of(S), o, d, tmax, first, cnt);
+    } else {
+        if (S.smem_stack) {
+            extern __shared__ uint32_t walk_stacks[];
+            return walk<STATS, PLACE_SHARED>(tree_of(S), o, d, tmax, first, cnt, walk_stacks + threadIdx.x,
+                                             (int)blockDim.x);
+        }
+        return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
     }
-    return walk<STATS>(tree_of(S), o, d, tmax, first, cnt);
 }
 
 // ---- scene records ----

@@ -405,16 +405,16 @@ __global__ void k_secondary(Scene S, Frame F, uint32_t frame, float4* __restrict
     rays[2 * (size_t)i + 1] = make_float4(dir.x, dir.y, dir.z, 0.0f);
 }
 
-template <bool ANY, bool STATS, bool SMEM>
+template <bool ANY, bool STATS, int P>
 __global__ void __launch_bounds__(128) k_rays(Scene S, const float4* __restrict__ rays, uint32_t n,
                                               float4* __restrict__ hits, unsigned long long* counters) {
-    __shared__ uint32_t s_stack[SMEM ? STACK * 128 : 1];
+    __shared__ uint32_t s_stack[P == PLACE_SHARED ? STACK * 128 : 1];
     load_info(S);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Count cnt{0, 0, 0};
     if (i < n) {
         const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
-        const Hit h = walk_scene<STATS, SMEM>(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt,
+        const Hit h = walk_scene<STATS, P>(S, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, ANY, cnt,
                                               s_stack + threadIdx.x, 128);
         const uint32_t face = h.tri == NONE ? NONE : __float_as_uint(__ldg(S.tris + 3 * (size_t)h.tri).w);
         hits[i] = make_float4(h.t, __uint_as_float(face), h.u, h.v);
@@ -593,8 +593,8 @@ __global__ void k_ray_keys(Scene S, const float4* __restrict__ rays, uint32_t n,
 }
 
 template <bool ANY, bool STATS>
-void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters, bool smem,
-                 cudaStream_t s, uint32_t* next = nullptr, int sms = 0, const uint32_t* order = nullptr) {
+void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, unsigned long long* counters,
+                 uint32_t place, cudaStream_t s, uint32_t* next = nullptr, int sms = 0, const uint32_t* order = nullptr) {
     if (next && !S.insts) {  // (scenes of instances: a thread per ray)
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rays_fetch<ANY, STATS>, 128, 0);
@@ -603,10 +603,14 @@ void launch_rays(const Scene& S, const float* rays, uint32_t n, float* hits, uns
         k_rays_fetch<ANY, STATS><<<grid, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters, next, order);
         return;
     }
-    if (smem)
-        k_rays<ANY, STATS, true><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters);
+    const uint32_t blocks = (n + 127) / 128;
+    const float4* r = (const float4*)rays;
+    if (place == PHX_STACK_SHARED)
+        k_rays<ANY, STATS, PLACE_SHARED><<<blocks, 128, 0, s>>>(S, r, n, (float4*)hits, counters);
+    else if (place == PHX_STACK_REGISTER)
+        k_rays<ANY, STATS, PLACE_REG_BASE + 1><<<blocks, 128, 0, s>>>(S, r, n, (float4*)hits, counters);
     else
-        k_rays<ANY, STATS, false><<<(n + 127) / 128, 128, 0, s>>>(S, (const float4*)rays, n, (float4*)hits, counters);
+        k_rays<ANY, STATS, PLACE_LOCAL><<<blocks, 128, 0, s>>>(S, r, n, (float4*)hits, counters);
 }
 
 }  // namespace
@@ -650,7 +654,7 @@ struct phx_tracer_s {
     uint32_t frame = 0, target = 32;  // Tracer::SAMPLE_COUNT (src/trace/mod.rs:129) until set_samples
     uint32_t kernel = PHX_KERNEL_MEGAKERNEL;  // which render kernel traces a frame (the fastest measured)
     DevMem next;                                 // the state-machine kernel's pixel counter
-    bool smem_stack = false;                     // ray walks keep their stack in shared memory
+    uint32_t stack_place = PHX_STACK_LOCAL;      // where thread-per-ray walks keep their stack
     uint32_t walk = PHX_WALK_THREAD;             // ray walks: a thread per ray, persistent warps, sorted first
     DevMem rkeys, rsorted, rorder, ralt_k, ralt_v, rzero;  // the sorted walk's keys and radix-sort scratch
     // The 4-wide tree of PHX_WALK_WIDE, collapsed from the binary tree when
@@ -1074,6 +1078,8 @@ int32_t launch_frame(phx_tracer tr, const Frame& F, f3 sun, uint32_t first_px, u
     if (kernel >= PHX_KERNEL_MEGAKERNEL_6 && kernel <= PHX_KERNEL_MEGAKERNEL_8_SYNC) return render_flat_b(kernel, stats, L);
     if (kernel >= PHX_KERNEL_MEGAKERNEL_10_SYNC && kernel <= PHX_KERNEL_MEGAKERNEL_16_SYNC)
         return render_flat_c(kernel, stats, L);
+    if (kernel >= PHX_KERNEL_MEGAKERNEL_REG && kernel <= PHX_KERNEL_MEGAKERNEL_16_SYNC_REG)
+        return render_flat_r(kernel, stats, L);
     return render_flat_a(kernel, stats, L);
 }
 
@@ -1471,8 +1477,8 @@ int32_t phx_tracer_autotune(phx_tracer tr, const phx_camera* cam, uint32_t w, ui
 
 int32_t phx_tracer_set_stack(phx_tracer tr, uint32_t place) {
     if (!tr) return fail(PHX_ERR_INVALID, "null tracer");
-    if (place > PHX_STACK_SHARED) return fail(PHX_ERR_INVALID, "unknown stack placement %u", place);
-    tr->smem_stack = place == PHX_STACK_SHARED;
+    if (place > PHX_STACK_REGISTER) return fail(PHX_ERR_INVALID, "unknown stack placement %u", place);
+    tr->stack_place = place;
     return PHX_OK;
 }
 
@@ -1813,9 +1819,9 @@ int32_t phx_trace_rays(phx_tracer tr, const float* rays, uint32_t n, float* hits
     const uint32_t* order = nullptr;
     if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));
     if (any_hit)
-        launch_rays<true, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms, order);
+        launch_rays<true, false>(S, rays, n, hits, nullptr, tr->stack_place, tr->ctx->stream, nx, tr->ctx->sms, order);
     else
-        launch_rays<false, false>(S, rays, n, hits, nullptr, tr->smem_stack, tr->ctx->stream, nx, tr->ctx->sms, order);
+        launch_rays<false, false>(S, rays, n, hits, nullptr, tr->stack_place, tr->ctx->stream, nx, tr->ctx->sms, order);
     return cuda_check(cudaGetLastError(), "trace rays");
 }
 
@@ -1836,8 +1842,8 @@ int32_t phx_trace_rays_stats(phx_tracer tr, const float* rays, uint32_t n, float
         const uint32_t* order = nullptr;
         if (tr->walk == PHX_WALK_SORTED) PHX_TRY(sort_rays(tr, S, rays, n, &order));
         unsigned long long* ct = (unsigned long long*)tr->rays.ptr;
-        if (any_hit) launch_rays<true, true>(S, rays, n, hits, ct, tr->smem_stack, s, nx, tr->ctx->sms, order);
-        else launch_rays<false, true>(S, rays, n, hits, ct, tr->smem_stack, s, nx, tr->ctx->sms, order);
+        if (any_hit) launch_rays<true, true>(S, rays, n, hits, ct, tr->stack_place, s, nx, tr->ctx->sms, order);
+        else launch_rays<false, true>(S, rays, n, hits, ct, tr->stack_place, s, nx, tr->ctx->sms, order);
         PHX_CUDA(cudaGetLastError());
     }
     PHX_CUDA(cudaMemcpyAsync(counts, tr->rays.ptr, 24, cudaMemcpyDeviceToHost, s));

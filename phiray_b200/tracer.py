@@ -226,7 +226,10 @@ class Tracer:
     MEGAKERNEL_12_SYNC = 14
     MEGAKERNEL_16_SYNC = 15
     WAVEFRONT = 16
-    KERNELS = 17
+    MEGAKERNEL_REG = 17
+    MEGAKERNEL_8_SYNC_REG = 18
+    MEGAKERNEL_16_SYNC_REG = 19
+    KERNELS = 20
 
     def autotune(self, cam: np.ndarray, w: int, h: int, spp: int = 1) -> tuple[int, list[float]]:
         """Times every render kernel on this scene; keeps and returns the fastest."""
@@ -240,9 +243,14 @@ class Tracer:
         """Render kernel: Tracer.MEGAKERNEL or Tracer.STATE_MACHINE (same image)."""
         N.check(N.lib().phx_tracer_set_kernel(self.handle, kind))
 
-    def set_stack(self, shared: bool) -> None:
-        """Ray-buffer walks keep their stack in shared (True) or local memory."""
-        N.check(N.lib().phx_tracer_set_stack(self.handle, 1 if shared else 0))
+    STACK_LOCAL = 0
+    STACK_SHARED = 1
+    STACK_REGISTER = 2
+
+    def set_stack(self, place: int) -> None:
+        """Where thread-per-ray walks keep their stack: STACK_LOCAL,
+        STACK_SHARED (True also means shared) or STACK_REGISTER."""
+        N.check(N.lib().phx_tracer_set_stack(self.handle, int(place)))
 
     WALK_THREAD = 0
     WALK_FETCH = 1

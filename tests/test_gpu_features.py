@@ -17,7 +17,7 @@ from tests.test_gpu_trace import cam_of, check_image
 pytestmark = pytest.mark.gpu
 
 KINDS = ["lamps", "rig", "glass", "layers"]
-KERNELS = list(range(17))
+KERNELS = list(range(20))
 
 
 @pytest.fixture(scope="module")

@@ -50,9 +50,10 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("kernel", list(range(17)),
+@pytest.mark.parametrize("kernel", list(range(20)),
                          ids=["megakernel", "state_machine", "sm6", "sm8", "mk3", "mk2", "mk_sync", "mk2_sync", "mk5",
-                              "mk6", "mk6_sync", "mk8", "mk8_sync", "mk10_sync", "mk12_sync", "mk16_sync", "wavefront"])
+                              "mk6", "mk6_sync", "mk8", "mk8_sync", "mk10_sync", "mk12_sync", "mk16_sync", "wavefront",
+                              "mk_reg8", "mk8_sync_reg1", "mk16_sync_reg1"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_image_matches_oracle(gpu, orc, name, kernel):
     s = SCENES[name]()
@@ -127,6 +128,62 @@ def test_primary_hit_ids(gpu, orc, name):
     got = ids.cpu().numpy().view(np.uint32)
     assert np.array_equal(got, want_ids)
     assert np.array_equal(ts.cpu().numpy(), want_t)
+
+
+def _chain_scene():
+    """40 parallel triangles at x = 2^-k, overlapping in y and z: a tree 13
+    levels deep whose boxes a ray along x nearly all enters, so it pushes at
+    nearly every level (more entries than the register stack holds: its
+    spill and refill)."""
+    from tests import pins
+
+    k = np.arange(40)
+    x = (2.0 ** -k.astype(np.float64)).astype(np.float32)
+    v = np.ones((120, 4), np.float32)
+    v[0::3, :3] = np.stack([x, -np.ones(40), -np.ones(40)], 1)
+    v[1::3, :3] = np.stack([x, np.ones(40), -np.ones(40)], 1)
+    v[2::3, :3] = np.stack([x, np.zeros(40), np.ones(40)], 1)
+    f = np.zeros((40, 4), np.uint32)
+    f[:, 0], f[:, 1], f[:, 2] = 3 * k, 3 * k + 1, 3 * k + 2
+    return scenes.Scene("chain", v, f, np.stack([scenes.lambert((0.5, 0.5, 0.5))]),
+                        np.stack([scenes.light_off()]), None, pins.W, pins.W, 1, 1)
+
+
+@pytest.mark.parametrize("place", [0, 1, 2], ids=["local", "shared", "register"])
+@pytest.mark.parametrize("name", ["c2_small", "chain"])
+def test_ray_walk_stack_placements(gpu, orc, name, place):
+    """Thread-per-ray walks with the stack in local memory, shared memory or
+    registers over a spill array: the oracle's hits, word for word."""
+    import torch
+
+    s = _chain_scene() if name == "chain" else SCENES[name]()
+    rng = np.random.default_rng(21)
+    n = 8000
+    rays = np.zeros((n, 8), np.float32)
+    if name == "chain":
+        rays[:, 0] = np.where(np.arange(n) % 2 == 0, -1.0, 2.0)
+        rays[:, 1:3] = rng.uniform(-0.3, 0.3, (n, 2))
+        d = np.zeros((n, 3), np.float32)
+        d[:, 0] = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+        d[:, 1:3] = rng.uniform(-0.05, 0.05, (n, 2))
+    else:
+        rays[:, 0:3] = rng.uniform(-1.0, 1.0, (n, 3))
+        d = rng.standard_normal((n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3], rays[:, 4:7] = 3.0e38, d
+    tr = px.Tracer.of(gpu, s)
+    tr.set_stack(place)
+    dr = torch.tensor(rays, device="cuda")
+    hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    T = oracle_lib.TraceOracle(orc, s)
+    for any_hit in (False, True):
+        tr.trace_rays(dr, n, hits, any_hit)
+        gpu.wait()
+        got, want = hits.cpu().numpy(), T.trace_rays(rays, any_hit)
+        assert np.array_equal(got.view(np.uint32)[:, 1], want.view(np.uint32)[:, 1])
+        if not any_hit:
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    tr.close()
 
 
 @pytest.mark.parametrize("walk", [0, 1, 2], ids=["thread_per_ray", "persistent_fetch", "sorted"])
@@ -222,7 +279,7 @@ def test_autotune_keeps_the_image(gpu, orc):
     cam = cam_of(s, s.width, s.height)
     tr = px.Tracer.of(gpu, s)
     chosen, ms = tr.autotune(cam, s.width, s.height, 2)
-    assert chosen in range(17) and len(ms) == 17 and all(t > 0 for t in ms)
+    assert chosen in range(20) and len(ms) == 20 and all(t > 0 for t in ms)
     tr.trace(cam, s.width, s.height, 0, s.spp)
     want, _ = oracle_lib.TraceOracle(orc, s).trace(cam, 0, s.spp)
     check_image(tr.image(), want, s.width * s.height)
@@ -338,7 +395,8 @@ def test_show_matches_oracle(gpu, orc):
     tr.close()
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 15, 16], ids=["megakernel", "state_machine", "mk16_sync", "wavefront"])
+@pytest.mark.parametrize("kernel", [0, 1, 15, 16, 19],
+                         ids=["megakernel", "state_machine", "mk16_sync", "wavefront", "mk16_sync_reg1"])
 @pytest.mark.parametrize("name", list(SCENES))
 def test_sah_tree_image_matches_oracle(gpu, orc, name, kernel):
     """The tracer walking the binned SAH tree (phx_tracer_set_tree) == the
