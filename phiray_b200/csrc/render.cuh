@@ -493,6 +493,20 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
     }
 }
 
+// Thread k's pixel offset: over a whole frame whose sides are multiples of
+// 16 and 8, each 128-thread block takes a 16 x 8 region and each warp an
+// 8 x 4 tile of it, so a warp's camera rays (and the paths they start)
+// stay close together; otherwise pixel k. Which thread traces a pixel does
+// not change what is traced there.
+__device__ __forceinline__ uint32_t tile_px(const Frame& F, uint32_t k, uint32_t first, uint32_t count) {
+    if (first != 0u || count != F.w * F.h || (F.w & 15u) != 0u || (F.h & 7u) != 0u) return k;
+    const uint32_t block = k >> 7, warp = (k >> 5) & 3u, lane = k & 31u;
+    const uint32_t bx = block % (F.w >> 4), by = block / (F.w >> 4);
+    const uint32_t x = bx * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t y = by * 8u + (warp >> 1) * 4u + (lane >> 3);
+    return y * F.w + x;
+}
+
 // MINB: resident 128-thread blocks per SM the register budget is set for
 // (4: 128 registers a thread; 3: 168; 2: 255 — fewer warps, fewer spills;
 // 5: 96, 6: 80, 8: 64, 10: 48, 12: 40, 16: 32 — more warps to hide the
@@ -507,7 +521,7 @@ __global__ void __launch_bounds__(128, MINB) k_render(Scene S, Frame F, f3 sun, 
         // shade.wgsl:44-50: thread k takes the k-th pixel still open
         if (k < px[34u * F.n]) render_px<STATS, SYNC>(S, F, sun, px, px[32u * F.n + k], cnt);
     } else if (k < count) {
-        render_px<STATS, SYNC>(S, F, sun, px, first + k, cnt);
+        render_px<STATS, SYNC>(S, F, sun, px, first + tile_px(F, k, first, count), cnt);
     }
     flush_counts<STATS>(cnt, counters);
 }
@@ -608,6 +622,15 @@ struct Job {
     uint32_t npx;
 };
 
+// Lane `lane` of a job's warp tile q: an 8 x 4 block of pixels when the
+// image's sides are multiples of 8 and 4 (q counts the blocks row by row),
+// else the 32 pixels from q * 32 on.
+__device__ __forceinline__ uint32_t warp_tile_px(const Frame& F, uint32_t q, uint32_t lane) {
+    if ((F.w & 7u) != 0u || (F.h & 3u) != 0u) return q * 32u + lane;
+    const uint32_t across = F.w >> 3;
+    return ((q / across) * 4u + (lane >> 3)) * F.w + (q % across) * 8u + (lane & 7u);
+}
+
 // Registers are budgeted for RES resident threads an SM: 1536 (40 a
 // thread) or every thread slot, 2048 (32 a thread). The walk is
 // latency-bound, so more resident warps pay although they spill more.
@@ -641,7 +664,7 @@ __global__ void __launch_bounds__(THREADS, RES / THREADS) k_render_batch(const J
             __syncwarp();
             cur = lo;
         }
-        const uint32_t p = (t - J.tile0) * 32u + (uint32_t)lane;
+        const uint32_t p = warp_tile_px(J.F, t - J.tile0, (uint32_t)lane);
         Count cnt{0, 0, 0};
         if (p < J.npx) render_px<STATS>(J.S, J.F, J.sun, J.px, p, cnt);
         flush_counts<STATS>(cnt, J.counters);

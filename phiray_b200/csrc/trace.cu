@@ -369,11 +369,13 @@ __global__ void __launch_bounds__(1024) k_lamps_inst(const float4* __restrict__ 
     }
 }
 
-// Primary ray of each pixel: face id and t.
+// Primary ray of each pixel: face id and t (a warp's pixels an 8 x 4 tile
+// where the frame's sides allow, as in k_render).
 __global__ void k_primary(Scene S, Frame F, uint32_t frame, uint32_t* __restrict__ ids, float* __restrict__ ts) {
     setup(S, F);
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= F.n) return;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= F.n) return;
+    const uint32_t i = tile_px(F, k, 0u, F.n);
     uint32_t seed = hash(i * 9781u + frame * 6271u + 1u);
     const CamRay cr = camera_ray(F, i, seed);
     Count cnt{0, 0, 0};
