@@ -515,12 +515,14 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims,
             return;
         }
         const uint32_t p = __ldg(parent + i);
+        // p's child links (fixed during a refit) are read before the
+        // arrival count, so the sibling is known when the count returns
+        const uint32_t l = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p) + 3);
+        const uint32_t r = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p + 1) + 3);
         __threadfence();
         const uint32_t old = atomicAdd(counters + p, 1u);
         if ((old & 1u) == 0) return;  // first child here: the sibling finishes p
         __threadfence();
-        const float4 pa = __ldcg(nodes + 2 * (size_t)p), pb = __ldcg(nodes + 2 * (size_t)p + 1);
-        const uint32_t l = __float_as_uint(pa.w), r = __float_as_uint(pb.w);
         const bool is_left = (l == i);
         const uint32_t sib = is_left ? r : l;
         const float4 sa = __ldcg(nodes + 2 * (size_t)sib), sb = __ldcg(nodes + 2 * (size_t)sib + 1);
@@ -539,8 +541,8 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims,
             hy = fmaxf(sb.y, hy);
             hz = fmaxf(sb.z, hz);
         }
-        nodes[2 * (size_t)p] = make_float4(lx, ly, lz, pa.w);
-        nodes[2 * (size_t)p + 1] = make_float4(hx, hy, hz, pb.w);
+        nodes[2 * (size_t)p] = make_float4(lx, ly, lz, __uint_as_float(l));
+        nodes[2 * (size_t)p + 1] = make_float4(hx, hy, hz, __uint_as_float(r));
         i = p;
     }
 }
