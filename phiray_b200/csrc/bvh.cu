@@ -507,44 +507,7 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ prims,
     }
     nodes[2 * (size_t)i] = make_float4(lx, ly, lz, a.w);
     nodes[2 * (size_t)i + 1] = make_float4(hx, hy, hz, b.w);
-    // A Karras tree is at most 65 levels deep (delta grows strictly from
-    // -1 to 64 going down); a longer climb means a corrupt parent array.
-    for (int hops = 0; i != 0; hops++) {
-        if (hops > 80) {
-            atomicOr(status, STATUS_BAD_INDEX);
-            return;
-        }
-        const uint32_t p = __ldg(parent + i);
-        // p's child links (fixed during a refit) are read before the
-        // arrival count, so the sibling is known when the count returns
-        const uint32_t l = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p) + 3);
-        const uint32_t r = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p + 1) + 3);
-        __threadfence();
-        const uint32_t old = atomicAdd(counters + p, 1u);
-        if ((old & 1u) == 0) return;  // first child here: the sibling finishes p
-        __threadfence();
-        const bool is_left = (l == i);
-        const uint32_t sib = is_left ? r : l;
-        const float4 sa = __ldcg(nodes + 2 * (size_t)sib), sb = __ldcg(nodes + 2 * (size_t)sib + 1);
-        if (is_left) {
-            lx = fminf(lx, sa.x);
-            ly = fminf(ly, sa.y);
-            lz = fminf(lz, sa.z);
-            hx = fmaxf(hx, sb.x);
-            hy = fmaxf(hy, sb.y);
-            hz = fmaxf(hz, sb.z);
-        } else {
-            lx = fminf(sa.x, lx);
-            ly = fminf(sa.y, ly);
-            lz = fminf(sa.z, lz);
-            hx = fmaxf(sb.x, hx);
-            hy = fmaxf(sb.y, hy);
-            hz = fmaxf(sb.z, hz);
-        }
-        nodes[2 * (size_t)p] = make_float4(lx, ly, lz, __uint_as_float(l));
-        nodes[2 * (size_t)p + 1] = make_float4(hx, hy, hz, __uint_as_float(r));
-        i = p;
-    }
+    refit_climb(i, lx, ly, lz, hx, hy, hz, parent, nodes, counters, status);
 }
 
 // The reference's Jacobi Refit step (kernel.rs:130-170), for Pass replay.
@@ -675,7 +638,7 @@ int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* or
 }
 
 // Every stage of Bvh::build over w.prims[0..n) on the context's stream.
-int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate) {
+int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate, bool refit) {
     cudaStream_t s = c->stream;
     PHX_TRY(zero(c, w.scalars.ptr, 64, gate));
     if (n == 0) return PHX_OK;
@@ -711,6 +674,7 @@ int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate) 
                                                                 (const uint32_t*)w.parent.ptr, anc_a, dist_a, n, leaf,
                                                                 (float4*)w.nodes.ptr, (uint32_t*)w.starts.ptr,
                                                                 w.nstarts(), w.depth(), gate);
+    if (!refit) return cuda_check(cudaGetLastError(), "bvh build");
     k_refit<<<grid_for(n, 256, 1u << 30), 256, 0, s>>>(prims, (const uint32_t*)w.order.ptr,
                                                        (const uint32_t*)w.parent.ptr, (float4*)w.nodes.ptr,
                                                        (const uint32_t*)w.starts.ptr, w.nstarts(),

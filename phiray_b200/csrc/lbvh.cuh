@@ -65,6 +65,54 @@ __device__ __forceinline__ uint32_t lookback_prefix(const uint32_t* lookback, ui
     }
     return prefix;
 }
+
+// The climb of the atomic bottom-up refit (Bvh::refit's bounds, build.rs:
+// 180-194) from node i, whose box (lx .. hz) is already stored: at each
+// parent the first arriving child stops and the second unions its box with
+// its sibling's (left box first) and carries on up. counters[] start even
+// and every reachable inner node gets exactly two arrivals, so they need no
+// reset between refits. A climb longer than any Karras tree (65 levels)
+// means a corrupt parent array: STATUS_BAD_INDEX, and the climb stops.
+__device__ __forceinline__ void refit_climb(uint32_t i, float lx, float ly, float lz, float hx, float hy, float hz,
+                                            const uint32_t* __restrict__ parent, float4* nodes, uint32_t* counters,
+                                            uint32_t* status) {
+    for (int hops = 0; i != 0; hops++) {
+        if (hops > 80) {
+            atomicOr(status, STATUS_BAD_INDEX);
+            return;
+        }
+        const uint32_t p = __ldg(parent + i);
+        // p's child links (fixed during a refit) are read before the
+        // arrival count, so the sibling is known when the count returns
+        const uint32_t l = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p) + 3);
+        const uint32_t r = __ldcg((const uint32_t*)(nodes + 2 * (size_t)p + 1) + 3);
+        __threadfence();
+        const uint32_t old = atomicAdd(counters + p, 1u);
+        if ((old & 1u) == 0) return;  // first child here: the sibling finishes p
+        __threadfence();
+        const bool is_left = (l == i);
+        const uint32_t sib = is_left ? r : l;
+        const float4 sa = __ldcg(nodes + 2 * (size_t)sib), sb = __ldcg(nodes + 2 * (size_t)sib + 1);
+        if (is_left) {
+            lx = fminf(lx, sa.x);
+            ly = fminf(ly, sa.y);
+            lz = fminf(lz, sa.z);
+            hx = fmaxf(hx, sb.x);
+            hy = fmaxf(hy, sb.y);
+            hz = fmaxf(hz, sb.z);
+        } else {
+            lx = fminf(sa.x, lx);
+            ly = fminf(sa.y, ly);
+            lz = fminf(sa.z, lz);
+            hx = fmaxf(sb.x, hx);
+            hy = fmaxf(sb.y, hy);
+            hz = fmaxf(sb.z, hz);
+        }
+        nodes[2 * (size_t)p] = make_float4(lx, ly, lz, __uint_as_float(l));
+        nodes[2 * (size_t)p + 1] = make_float4(hx, hy, hz, __uint_as_float(r));
+        i = p;
+    }
+}
 #endif
 
 struct BvhWork {
@@ -91,8 +139,10 @@ int32_t enqueue_sort_raw(Ctx* c, const uint32_t* codes, uint32_t n, uint32_t* or
                          uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* hist, uint32_t* tickets, uint32_t* lookback,
                          uint32_t stride);
 
-// Every stage of Bvh::build over w.prims[0..n) on the context's stream.
-int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate = Gate{});
+// Every stage of Bvh::build over w.prims[0..n) on the context's stream;
+// refit = false leaves out the last one, the bounds (the caller runs a
+// refit of its own, which must climb as refit_climb does).
+int32_t enqueue_build(Ctx* c, BvhWork& w, uint32_t n, uint32_t leaf, Gate gate = Gate{}, bool refit = true);
 // Bvh::refit (slots = false: prims through order; true: prims already in
 // slot order, Bvh::refit_slots).
 int32_t enqueue_refit(Ctx* c, BvhWork& w, uint32_t n, bool slots, Gate gate = Gate{});

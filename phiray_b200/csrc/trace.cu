@@ -90,6 +90,59 @@ __global__ void k_mark_ends(const float4* __restrict__ nodes, const uint32_t* __
     c->w = __uint_as_float(__float_as_uint(c->w) | FLAG_END);
 }
 
+// The refit (k_refit's leaf part and climb) fused with the triangle gather
+// for a single-mesh LBVH tree: the thread of each reachable leaf computes
+// its faces' boxes from the vertices (Aabb::of_tri, as k_face_boxes), writes
+// their slots' triangle records (as k_gather) with the last slot marked (as
+// k_mark_ends), stores the leaf's box and climbs. The nodes, triangles and
+// flags are those of the separate kernels; the vertices are read once.
+__global__ void __launch_bounds__(256) k_refit_gather(const uint32_t* __restrict__ order,
+                                                      const uint4* __restrict__ faces,
+                                                      const float4* __restrict__ verts,
+                                                      const float4* __restrict__ vnorm,
+                                                      const float4* __restrict__ mats, uint32_t nmats,
+                                                      float4* __restrict__ tris, float4* __restrict__ tnorm,
+                                                      const uint32_t* __restrict__ parent, float4* nodes,
+                                                      const uint32_t* __restrict__ starts,
+                                                      const uint32_t* __restrict__ nstarts, uint32_t* counters,
+                                                      uint32_t* status) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *nstarts) return;
+    const uint32_t i = starts[t];
+    const float4 na = nodes[2 * (size_t)i], nb = nodes[2 * (size_t)i + 1];
+    const uint32_t first = __float_as_uint(na.w) & ~LEAF, end = __float_as_uint(nb.w);
+    float lx = FLT_MAX, ly = FLT_MAX, lz = FLT_MAX, hx = -FLT_MAX, hy = -FLT_MAX, hz = -FLT_MAX;
+    for (uint32_t s = first; s < end; s++) {
+        const uint32_t f = __ldg(order + s);
+        const uint4 v = __ldg(faces + f);
+        const float4 a = __ldg(verts + v.x), b = __ldg(verts + v.y), c = __ldg(verts + v.z);
+        lx = fminf(lx, fminf(fminf(a.x, b.x), c.x));
+        ly = fminf(ly, fminf(fminf(a.y, b.y), c.y));
+        lz = fminf(lz, fminf(fminf(a.z, b.z), c.z));
+        hx = fmaxf(hx, fmaxf(fmaxf(a.x, b.x), c.x));
+        hy = fmaxf(hy, fmaxf(fmaxf(a.y, b.y), c.y));
+        hz = fmaxf(hz, fmaxf(fmaxf(a.z, b.z), c.z));
+        uint32_t m = v.w;
+        if (m >= nmats) {
+            atomicOr(status, STATUS_BAD_INDEX);
+            m = 0;
+        }
+        const float4 m0 = __ldg(mats + 8 * (size_t)m), m1 = __ldg(mats + 8 * (size_t)m + 1);
+        const uint32_t flags = ((m1.z > 0.5f || m0.w < 0.5f) ? FLAG_PASS : 0u) | (s + 1 == end ? FLAG_END : 0u);
+        tris[3 * (size_t)s] = make_float4(a.x, a.y, a.z, __uint_as_float(f));
+        tris[3 * (size_t)s + 1] = make_float4(b.x, b.y, b.z, __uint_as_float(m));
+        tris[3 * (size_t)s + 2] = make_float4(c.x, c.y, c.z, __uint_as_float(flags));
+        if (tnorm) {
+            tnorm[3 * (size_t)s] = __ldg(vnorm + v.x);
+            tnorm[3 * (size_t)s + 1] = __ldg(vnorm + v.y);
+            tnorm[3 * (size_t)s + 2] = __ldg(vnorm + v.z);
+        }
+    }
+    nodes[2 * (size_t)i] = make_float4(lx, ly, lz, na.w);
+    nodes[2 * (size_t)i + 1] = make_float4(hx, hy, hz, nb.w);
+    refit_climb(i, lx, ly, lz, hx, hy, hz, parent, nodes, counters, status);
+}
+
 // Marks the last slot of every leaf of a tree whose nodes are all reachable
 // (the binned SAH tree's compact array).
 __global__ void k_mark_leaf_ends(const float4* __restrict__ nodes, uint32_t m, float4* tris) {
@@ -674,10 +727,11 @@ struct phx_tracer_s {
 
 namespace {
 
+int32_t prepare_nodes(phx_tracer tr);
+
 int32_t prepare(phx_tracer tr) {
     // After a build or refit: face boxes are in tr->bvh; gather, mark leaf
-    // ends, convert nodes, root info, emitter table.
-    tr->tree_gen++;
+    // ends, then the walk's nodes, root info and emitter table.
     Ctx* c = tr->ctx;
     cudaStream_t s = c->stream;
     const uint32_t n = tr->nfaces;
@@ -689,6 +743,35 @@ int32_t prepare(phx_tracer tr) {
                                              tr->has_normals ? (float4*)tr->tnorm.ptr : nullptr, c->status);
     k_mark_ends<<<(n + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr,
                                                 w.nstarts(), (float4*)tr->tris.ptr);
+    return prepare_nodes(tr);
+}
+
+// The LBVH's bounds by k_refit_gather (triangles gathered on the way), after
+// enqueue_build(..., refit = false) or on its own for a refit; then the
+// walk's nodes as prepare.
+int32_t refit_gather(phx_tracer tr) {
+    Ctx* c = tr->ctx;
+    const uint32_t n = tr->nfaces;
+    BvhWork& w = tr->bvh;
+    if (n > 0) {
+        k_refit_gather<<<(n + 255) / 256, 256, 0, c->stream>>>(
+            (const uint32_t*)w.order.ptr, (const uint4*)tr->faces.ptr, (const float4*)tr->verts.ptr,
+            tr->has_normals ? (const float4*)tr->vnorm.ptr : nullptr, (const float4*)tr->mats.ptr, tr->nmats,
+            (float4*)tr->tris.ptr, tr->has_normals ? (float4*)tr->tnorm.ptr : nullptr, (const uint32_t*)w.parent.ptr,
+            (float4*)w.nodes.ptr, (const uint32_t*)w.starts.ptr, w.nstarts(), (uint32_t*)w.counters.ptr, c->status);
+        PHX_CUDA(cudaGetLastError());
+    }
+    return prepare_nodes(tr);
+}
+
+// The walk's inner-node records, root info and emitter table from tr->bvh
+// and the gathered triangles.
+int32_t prepare_nodes(phx_tracer tr) {
+    tr->tree_gen++;
+    Ctx* c = tr->ctx;
+    cudaStream_t s = c->stream;
+    const uint32_t n = tr->nfaces;
+    const BvhWork& w = tr->bvh;
     if (n > 1)
         k_convert<<<(n - 1 + 255) / 256, 256, 0, s>>>((const float4*)w.nodes.ptr, n - 1, (float4*)tr->tnodes.ptr, 0u,
                                                       0u, 0u);
@@ -1738,18 +1821,25 @@ int32_t phx_tracer_repose_device(phx_tracer tr, const float* verts, int32_t rebu
         tr->have_last = false;
         return PHX_OK;
     }
-    PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
-                              (phx_aabb*)tr->bvh.prims.ptr));
     if (tr->tree == PHX_TREE_SAH) {
+        PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                                  (phx_aabb*)tr->bvh.prims.ptr));
         if (rebuild) PHX_TRY(build_sah_tree(tr));
         else PHX_TRY(refit_sah_tree(tr));
         PHX_TRY(prepare_sah(tr));
         tr->have_last = false;
         return PHX_OK;
     }
-    if (rebuild) PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf));
-    else PHX_TRY(enqueue_refit(tr->ctx, tr->bvh, tr->nfaces, false));
-    PHX_TRY(prepare(tr));
+    // The LBVH: a rebuild sorts the face boxes; its bounds, like a refit's,
+    // come from k_refit_gather, which takes each face's box from the
+    // vertices (so a refit leaves tr->bvh.prims as it was: every user of
+    // the face boxes computes them first).
+    if (rebuild) {
+        PHX_TRY(launch_face_boxes(s, (const float*)tr->verts.ptr, (const uint32_t*)tr->faces.ptr, tr->nfaces,
+                                  (phx_aabb*)tr->bvh.prims.ptr));
+        PHX_TRY(enqueue_build(tr->ctx, tr->bvh, tr->nfaces, tr->leaf, Gate{}, false));
+    }
+    PHX_TRY(refit_gather(tr));
     tr->have_last = false;  // a new pose starts the image over
     return PHX_OK;
 }
