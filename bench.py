@@ -222,6 +222,9 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
     if args.phase == "render":
         if args.kernel >= 0:
             tr.set_kernel(args.kernel)
+        if args.adapt:
+            thr, lo, step = (float(v) for v in args.adapt.split(","))
+            tr.set_adaptive([thr, lo, step, 1.0])
         fn = lambda: tr.trace(cam, W, H, 0, args.spp)  # noqa: E731
     elif args.phase == "build":
         fn = lambda: tr.repose_device(verts_dev, rebuild=True)  # noqa: E731
@@ -239,7 +242,13 @@ def profile_phase(args, tr, gpu, cam, verts_dev, W, H, n, local) -> None:
     for _ in range(args.steps):
         fn()
     gpu.wait(60000)
-    print(json.dumps({"phase": args.phase, "steps": args.steps, "ms": (time.perf_counter() - t0) * 1e3 / args.steps}))
+    line = {"phase": args.phase, "steps": args.steps, "ms": (time.perf_counter() - t0) * 1e3 / args.steps}
+    if args.phase == "render":
+        gpu_ms, rays = tr.time()  # the last frame: device time and rays traced
+        line.update({"gpu_ms": round(gpu_ms, 3), "rays": int(rays), "mrays_s": round(rays / gpu_ms / 1e3, 1)})
+        if args.adapt:
+            line["unconverged"] = tr.unconverged()
+    print(json.dumps(line))
 
 
 def run_c3(args) -> None:
@@ -658,6 +667,8 @@ def main() -> None:
     ap.add_argument("--walk", type=int, default=0,
                     help="ray walk of --phase rays: 0 a thread per ray, 1 persistent, 2 sorted, 3 the 4-wide tree "
                          "(persistent), 4 the 4-wide tree (a thread per ray)")
+    ap.add_argument("--adapt", default="",
+                    help="--phase render with Adaptive Sampling: 'threshold,min samples,step' (off by default)")
     ap.add_argument("--stack", type=int, default=0,
                     help="stack placement of --phase rays thread-per-ray walks: 0 local, 1 shared, 2 registers")
     ap.add_argument("--tree", type=int, default=0, help="tree of --phase runs: 0 the LBVH, 1 the binned SAH tree")

@@ -493,18 +493,23 @@ __device__ __forceinline__ void flush_counts(const Count& cnt, unsigned long lon
     }
 }
 
-// Thread k's pixel offset: over a whole frame whose sides are multiples of
-// 16 and 8, each 128-thread block takes a 16 x 8 region and each warp an
-// 8 x 4 tile of it, so a warp's camera rays (and the paths they start)
-// stay close together; otherwise pixel k. Which thread traces a pixel does
-// not change what is traced there.
-__device__ __forceinline__ uint32_t tile_px(const Frame& F, uint32_t k, uint32_t first, uint32_t count) {
-    if (first != 0u || count != F.w * F.h || (F.w & 15u) != 0u || (F.h & 7u) != 0u) return k;
+// The k-th pixel of a w x h image in warp-tile order: when the sides are
+// multiples of 16 and 8, each run of 128 takes a 16 x 8 region and each run
+// of 32 an 8 x 4 tile of it, so a warp's camera rays (and the paths they
+// start) stay close together; otherwise pixel k. Which thread traces a
+// pixel does not change what is traced there. tile_px: thread k's pixel
+// offset in a launch, tiled only over a whole frame.
+__device__ __forceinline__ uint32_t tile_order(uint32_t w, uint32_t h, uint32_t k) {
+    if ((w & 15u) != 0u || (h & 7u) != 0u) return k;
     const uint32_t block = k >> 7, warp = (k >> 5) & 3u, lane = k & 31u;
-    const uint32_t bx = block % (F.w >> 4), by = block / (F.w >> 4);
+    const uint32_t bx = block % (w >> 4), by = block / (w >> 4);
     const uint32_t x = bx * 16u + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t y = by * 8u + (warp >> 1) * 4u + (lane >> 3);
-    return y * F.w + x;
+    return y * w + x;
+}
+__device__ __forceinline__ uint32_t tile_px(const Frame& F, uint32_t k, uint32_t first, uint32_t count) {
+    if (first != 0u || count != F.w * F.h) return k;
+    return tile_order(F.w, F.h, k);
 }
 
 // MINB: resident 128-thread blocks per SM the register budget is set for
@@ -583,14 +588,18 @@ __global__ void k_adapt_dilate(uint32_t* __restrict__ px, uint32_t w, uint32_t h
 }
 
 // gather.wgsl: the list of pixels not settled, each block appending its
-// open pixels as one run in the order they lie (the list's order decides
-// only which thread traces which pixel, never a result).
-__global__ void __launch_bounds__(256) k_adapt_gather(uint32_t* __restrict__ px, uint32_t n) {
+// open pixels as one run in the order it visits them — the warp tiles'
+// order (tile_order), so a warp of the list launch traces neighbouring
+// pixels while most are open. The list's order decides only which thread
+// traces which pixel, never a result.
+__global__ void __launch_bounds__(256) k_adapt_gather(uint32_t* __restrict__ px, uint32_t w, uint32_t h) {
     __shared__ uint32_t held, run;
     if (threadIdx.x == 0) held = 0u;
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool open = i < n && px[30u * n + i] == 0u;
+    const uint32_t n = w * h;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = k < n ? tile_order(w, h, k) : k;
+    const bool open = k < n && px[30u * n + i] == 0u;
     const unsigned ballot = __ballot_sync(0xffffffffu, open);
     const int lane = threadIdx.x & 31;
     uint32_t base = 0;

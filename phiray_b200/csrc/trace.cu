@@ -1190,7 +1190,7 @@ int32_t adapt_tail(phx_tracer tr, const Frame& F, bool check, uint32_t sample) {
     if (check && adapt_boundary(F, sample)) k_adapt_check<<<blocks, 256, 0, s>>>(px, F.n, F.adapt_thr);
     k_adapt_dilate<<<blocks, 256, 0, s>>>(px, F.w, F.h);
     PHX_CUDA(cudaMemsetAsync(px + 34ull * F.n, 0, 4, s));
-    k_adapt_gather<<<blocks, 256, 0, s>>>(px, F.n);
+    k_adapt_gather<<<blocks, 256, 0, s>>>(px, F.w, F.h);
     return cuda_check(cudaGetLastError(), "adaptive sampling tail");
 }
 
